@@ -1,0 +1,459 @@
+#!/usr/bin/env python
+"""Benchmark: batched table NUFFT forward + adjoint on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c2|c2s|c1|c3]
+    python bench.py --impl reference ...
+
+One step = the forward NUFFT (deapodise + zero-pad, oversampled FFT, table
+gather) and the adjoint NUFFT (table spread, inverse FFT, crop + deapodise)
+of one batch of slices x coils.  Unit: Msamples/s = sample-coil pairs
+processed (forward + adjoint) per second, over all ranks.  Inputs are
+resident in HBM for `value`; `e2e` times the same step through the host-buffer
+C ABI (mirt_nufft_forward_host / _adjoint_host) with the copies inside.
+
+Default workload (c2): 64 slices, golden-angle radial with U{100..400} spokes
+x 512 samples, 32 coils, N = 256^2, K = 512^2, J = 6, L = 1024, all slices in
+one launch per kernel.  Data are seeded synthetic ellipse phantoms times
+Gaussian-bump coil maps.  Inputs exceed L2 (126 MB), so L2 is not flushed.
+
+--impl reference times the reference's own CPU path on the host cores: the
+table kernels nufft/table/interp2_table1_{for,adj}.c (oracle/_ref, built from
+the reference sources) with one coil column per thread, scipy.fft for the
+oversampled FFT and numpy for the deapodisation, on a bounded sample of the
+same workload.
+
+Multi-GPU (torchrun): each rank runs its own batch (weak scaling, no
+collective in the data path); time = max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "NUFFT fwd+adj Msamples/s & %HBM peak; CG-SENSE s to NRMSE 1e-3, learned vs plain"
+UNIT = "Msamples/s"
+
+WORKLOADS = {
+    "c2": dict(D=2, N=256, K=512, J=6, L=1024, ncoil=32, nslice=64, spokes=(100, 400), nro=512),
+    "c2s": dict(D=2, N=256, K=512, J=6, L=1024, ncoil=32, nslice=4, spokes=(100, 400), nro=512),
+    "c1": dict(D=2, N=64, K=128, J=6, L=1024, ncoil=1, nslice=1, spokes=(64, 64), nro=128),
+    "c3": dict(D=3, N=128, K=256, J=6, L=512, ncoil=8, nslice=1, spokes=(16384, 16384), nro=256),
+    "c3s": dict(D=3, N=128, K=256, J=6, L=512, ncoil=8, nslice=1, spokes=(2048, 2048), nro=256),
+}
+
+
+def describe(name, w):
+    if w["D"] == 2:
+        sp = (f"{w['spokes'][0]}" if w["spokes"][0] == w["spokes"][1]
+              else f"U{{{w['spokes'][0]}..{w['spokes'][1]}}}")
+        return (f"batched 2D multicoil table NUFFT fwd+adj: {w['nslice']} slices x {sp} "
+                f"golden-angle spokes x {w['nro']}, {w['ncoil']} coils, N={w['N']}^2, "
+                f"K={w['K']}^2, J={w['J']}, L={w['L']}")
+    return (f"3D table NUFFT fwd+adj: kooshball {w['spokes'][0]} spokes x {w['nro']}, "
+            f"{w['ncoil']} coils, N={w['N']}^3, K={w['K']}^3, J={w['J']}, L={w['L']}")
+
+
+def make_trajectory(w, rng):
+    from mirt_b200 import workloads as wl
+    if w["D"] == 2:
+        om, moff, _ = wl.batch_ga_radial(w["nslice"], w["spokes"][0], w["spokes"][1], w["nro"], rng)
+        return om, moff
+    om = wl.kooshball(w["spokes"][0], w["nro"])
+    return om, np.array([0, len(om)], np.int64)
+
+
+def make_images(w, rng, nslice=None):
+    """complex64 [nslice, N.., ncoil] in device layout: phantom x coil maps."""
+    from mirt_b200 import workloads as wl
+    S = w["nslice"] if nslice is None else nslice
+    N, C = w["N"], w["ncoil"]
+    if w["D"] == 2:
+        maps = wl.coil_maps((N, N), C, rng)                       # [n1, n2, c]
+        out = np.empty((S, N, N, C), np.complex64)                # [s, n2, n1, c]
+        for s in range(S):
+            ph = wl.ellipses(N, 10, rng).astype(np.complex64)      # [n1, n2]
+            out[s] = np.transpose(ph[:, :, None] * maps, (1, 0, 2))
+        return out
+    maps = wl.coil_maps((N, N, N), C, rng)
+    vol = wl.ellipsoids(N, 20, rng)
+    return np.transpose(vol[..., None] * maps, (2, 1, 0, 3))[None].copy()
+
+
+# ---------------------------------------------------------------------------
+# clocks
+# ---------------------------------------------------------------------------
+class Clocks:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            out, _ = self.p.communicate(timeout=10)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+            out, _ = self.p.communicate()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def physical_gpu_index(dev):
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        ids = [v.strip() for v in vis.split(",") if v.strip()]
+        if dev < len(ids) and ids[dev].isdigit():
+            return int(ids[dev])
+    return dev
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def traffic_from_profiles(kernel, workload):
+    """dram bytes per launch recorded from an ncu capture (profiles/traffic.json)."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            t = json.load(f)
+        return t.get(workload, {}).get(kernel)
+    except (OSError, ValueError):
+        return None
+
+
+# ---------------------------------------------------------------------------
+# CPU path of the reference (oracle/_ref kernels + scipy FFT + numpy glue)
+# ---------------------------------------------------------------------------
+class CpuReference:
+    def __init__(self, w, om, moff, n_shift):
+        import oracle
+        from oracle import nufft_ref as nr
+        self.oracle = oracle
+        self.impl = "ref" if oracle.ref_available() else "port"
+        self.kind = "reference" if self.impl == "ref" else "port"
+        self.w = w
+        D = w["D"]
+        self.Nd = (w["N"],) * D
+        self.Kd = (w["K"],) * D
+        self.Jd = (w["J"],) * D
+        self.Ld = (w["L"],) * D
+        self.h = [nr.table_1d(w["N"], w["J"], w["K"], w["L"])] * D
+        self.sn = nr.scaling_factors(self.Nd, self.Jd, self.Kd)
+        self.om, self.moff, self.n_shift = om, moff, np.asarray(n_shift, float)
+        self.threads = oracle.ref_max_threads() if self.impl == "ref" else 1
+
+    def step(self, s, x):
+        """forward + adjoint of slice s; x [N.., C] (MATLAB order).  Returns #sample-coils."""
+        import scipy.fft as sf
+        om = self.om[self.moff[s]:self.moff[s + 1]]
+        tm = np.stack([om[:, d] / (2 * np.pi / self.Kd[d]) for d in range(len(self.Kd))], 1)
+        ph = np.exp(1j * (om @ self.n_shift))
+        C = x.shape[-1]
+        D = len(self.Kd)
+        ax = tuple(range(D))
+        xs = x * self.sn[..., None]
+        Xk = sf.fftn(xs, s=self.Kd, axes=ax, workers=self.threads)
+        ck = Xk.reshape(-1, C, order="F")
+        if self.impl == "ref":
+            X = self.oracle.interp_for(ck, self.h, self.Jd, self.Ld, tm, self.Kd, 0,
+                                       impl="ref", nthreads=self.threads)
+        else:
+            X = self.oracle.interp_for(ck, self.h, self.Jd, self.Ld, tm, self.Kd, 0, impl="port")
+        X = X * ph[:, None]
+        Y = X * np.conj(ph)[:, None]
+        if self.impl == "ref":
+            ck2 = self.oracle.interp_adj(Y, self.h, self.Jd, self.Ld, tm, self.Kd, 0,
+                                         impl="ref", nthreads=self.threads)
+        else:
+            ck2 = self.oracle.interp_adj(Y, self.h, self.Jd, self.Ld, tm, self.Kd, 0, impl="port")
+        g = sf.ifftn(ck2.reshape(self.Kd + (C,), order="F"), axes=ax, norm="forward",
+                     workers=self.threads)
+        xa = g[tuple(slice(0, n) for n in self.Nd)] * np.conj(self.sn)[..., None]
+        assert np.isfinite(xa).all()
+        return 2 * len(om) * C
+
+    def timed_sample(self, images, target_s=12.0, max_slices=None):
+        """Time slices until ~target_s of CPU work; returns (Msamples/s, sample description)."""
+        S = len(self.moff) - 1
+        limit = S if max_slices is None else min(S, max_slices)
+        units, t0, n = 0, time.perf_counter(), 0
+        while n < limit:
+            x = self._image(images, n)
+            units += self.step(n, x)
+            n += 1
+            if time.perf_counter() - t0 >= target_s:
+                break
+        t = time.perf_counter() - t0
+        return units / t / 1e6, n, units, t
+
+    def _image(self, images, s):
+        D = len(self.Kd)
+        axes = tuple(range(D - 1, -1, -1)) + (D,)
+        return np.transpose(images[s % len(images)], axes).astype(np.complex128)
+
+
+def run_reference(args, w):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    rng = np.random.default_rng(1234)
+    om, moff = make_trajectory(w, rng)
+    images = make_images(w, np.random.default_rng(99), nslice=min(4, w["nslice"]))
+    n_shift = [w["N"] / 2] * w["D"]
+    ref = CpuReference(w, om, moff, n_shift)
+    S = len(moff) - 1
+    for i in range(args.warmup):
+        ref.step(i % S, ref._image(images, i))
+    times, units = [], 0
+    for i in range(args.steps):
+        s = (args.warmup + i) % S
+        t0 = time.perf_counter()
+        u = ref.step(s, ref._image(images, s))
+        times.append(time.perf_counter() - t0)
+        units += u
+    total = sum(times)
+    value = units / total / 1e6
+    sample = (f"per step one slice (forward + adjoint, {w['ncoil']} coils) of the workload; "
+              f"{args.steps} steps")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000 * total / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": describe(args.workload, w)},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": ref.threads, "kind": ref.kind,
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# GPU path
+# ---------------------------------------------------------------------------
+def run_gpu(args, w):
+    import torch
+    import torch.distributed as dist
+
+    import mirt_b200 as mb
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    rng = np.random.default_rng(1234 + rank)
+    om, moff = make_trajectory(w, rng)
+    Mtot = len(om)
+    C = w["ncoil"]
+    D = w["D"]
+    n_shift = [w["N"] / 2] * D
+    plan = mb.NufftPlan(om, (w["N"],) * D, (w["J"],) * D, (w["K"],) * D, n_shift=n_shift,
+                        Ld=w["L"], ncol=C, slice_moff=moff)
+    img_np = make_images(w, np.random.default_rng(99 + rank))
+    if img_np.shape[0] != plan.nslice:
+        reps = -(-plan.nslice // img_np.shape[0])
+        img_np = np.concatenate([img_np] * reps)[:plan.nslice]
+    x = torch.from_numpy(img_np).to(dev)
+    X = torch.empty(plan.sample_shape, dtype=torch.complex64, device=dev)
+    xa = torch.empty(plan.image_shape, dtype=torch.complex64, device=dev)
+    stream = torch.cuda.current_stream()
+
+    def step():
+        plan.forward(x, out=X)
+        plan.adjoint(X, out=xa)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(physical_gpu_index(local))
+    clocks.start()
+    time.sleep(0.3)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    t_local = e0.elapsed_time(e1) / 1000.0
+    units_local = 2.0 * Mtot * C * args.steps
+    if world > 1:
+        tt = torch.tensor([t_local], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        uu = torch.tensor([units_local], device=dev, dtype=torch.float64)
+        dist.all_reduce(uu, op=dist.ReduceOp.SUM)
+        t, units = float(tt.item()), float(uu.item())
+    else:
+        t, units = t_local, units_local
+    value = units / t / 1e6
+
+    # --- roofline of the interpolation kernels (device buffers, same plan) ---
+    ip = plan.lib.mirt_nufft_interp_plan(plan.handle)
+    import ctypes as Cc
+    grid = torch.randn((plan.nslice,) + (w["K"],) * D + (C,), dtype=torch.complex64, device=dev)
+    sptr = Cc.c_void_p(stream.cuda_stream)
+    reps = 5
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / 1000.0 / reps
+
+    from mirt_b200._lib import check
+    t_gather = timed(lambda: check(plan.lib.mirt_interp_plan_forward(
+        ip, Cc.c_void_p(grid.data_ptr()), Cc.c_void_p(X.data_ptr()), sptr)))
+    t_spread = timed(lambda: check(plan.lib.mirt_interp_plan_adjoint(
+        ip, Cc.c_void_p(X.data_ptr()), Cc.c_void_p(grid.data_ptr()), sptr)))
+    nk = w["K"] ** D
+    B = 8.0 * C * nk * plan.nslice + 8.0 * C * Mtot + 4.0 * D * Mtot
+    peak, peak_kind = measured_peak()
+    dom, tdom = ("spread", t_spread) if t_spread >= t_gather else ("gather", t_gather)
+    achieved = B / tdom / 1e9
+    roof = {"bound": "hbm", "kernel": f"{dom}_kernel", "achieved": achieved, "peak": peak,
+            "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+            "traffic": traffic_from_profiles(f"{dom}_kernel", args.workload),
+            "algorithmic_bytes": B,
+            "gather": {"ms": 1e3 * t_gather, "GBps": B / t_gather / 1e9,
+                       "frac": B / t_gather / 1e9 / peak},
+            "spread": {"ms": 1e3 * t_spread, "GBps": B / t_spread / 1e9,
+                       "frac": B / t_spread / 1e9 / peak}}
+    del grid
+
+    # --- e2e through the host-buffer C ABI ---
+    e2e = None
+    if not args.no_e2e:
+        xh = torch.empty(plan.image_shape, dtype=torch.complex64, pin_memory=True)
+        Xh = torch.empty(plan.sample_shape, dtype=torch.complex64, pin_memory=True)
+        xh.copy_(x)
+        xhn, Xhn = xh.numpy(), Xh.numpy()
+        xa_h = torch.empty(plan.image_shape, dtype=torch.complex64, pin_memory=True).numpy()
+        ke = max(1, min(args.steps, 5))
+        plan.forward_host(xhn, out=Xhn)
+        plan.adjoint_host(Xhn, out=xa_h)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(ke):
+            plan.forward_host(xhn, out=Xhn)
+            plan.adjoint_host(Xhn, out=xa_h)
+        te = time.perf_counter() - t0
+        if world > 1:
+            tt = torch.tensor([te], device=dev, dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            te = float(tt.item())
+        nbx, nbX = xhn.nbytes, Xhn.nbytes
+        e2e = {"value": (2.0 * Mtot * C * ke * world) / te / 1e6, "unit": UNIT,
+               "h2d_bytes_per_step": nbx + nbX, "d2h_bytes_per_step": nbX + nbx}
+
+    # --- CPU baseline (rank 0, N = 1 only) ---
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        ref = CpuReference(w, om, moff, n_shift)
+        v, ns, u, tc = ref.timed_sample(img_np, target_s=args.cpu_seconds)
+        cpu = {"value": v, "unit": UNIT, "cores": ref.threads, "kind": ref.kind,
+               "sample": f"{ns} of {plan.nslice} slices, forward + adjoint, {C} coils "
+                         f"({u:.3g} sample-coils in {tc:.1f} s)"}
+
+    launches_per_step = 4  # deapod_pad, gather, spread, crop_deapod (cuFFT not counted)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "c64 (f32 arithmetic, f64 table-index selection)", "data": "synthetic",
+            "config": {"workload": describe(args.workload, w), "samples_per_rank": Mtot,
+                       "coils": C, "slices_per_rank": plan.nslice,
+                       "l2": "inputs larger than L2; no flush",
+                       "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
+            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": launches_per_step * args.steps, "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    plan.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="mirt", choices=["mirt", "reference"])
+    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    args = ap.parse_args()
+    w = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        return run_reference(args, w)
+    return run_gpu(args, w)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

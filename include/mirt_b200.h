@@ -1,0 +1,234 @@
+/*
+ * mirt_b200.h -- C ABI of the B200 (sm_100a) implementation of MIRT's
+ * table-based NUFFT interpolation (JeffFessler/mirt, nufft/table/).
+ *
+ * Three layers, all plain C types:
+ *
+ *  1. Drop-ins for the six mex gateways.  Same arguments, in the same order,
+ *     as the MATLAB calls
+ *        fm = interpD_table_mex(ck, h1..hD, J, L, tm, [order, flips])
+ *        ck = interpD_table_adj_mex(fm, h1..hD, J, L, tm, K, [order, flips])
+ *     with each mxArray passed as its data pointers (split real/imag FP64,
+ *     column-major) and its dimensions.  An optional argument that the MATLAB
+ *     call omits is passed as a NULL pointer.  The caller allocates the output
+ *     (the gateway's mxCreateDoubleMatrix(..., mxCOMPLEX)) and passes its two
+ *     data pointers.  Calls are synchronous; inputs are read-only.  Device
+ *     arithmetic is FP32 with FP64 table-index selection, so the output agrees
+ *     with the reference's FP64 kernels to FP32 rounding (relative L2 ~1e-7).
+ *
+ *  2. A device-resident interpolation plan: tables and trajectory are
+ *     uploaded and bin-sorted once, then forward / adjoint run on float2
+ *     (complex64) device buffers with the column (coil) index innermost.
+ *
+ *  3. A device-resident NUFFT (nufft.m / nufft_adj.m with 'table' and
+ *     'minmax:kb'): tables and scaling factors built here in FP64, the
+ *     oversampled FFT by cuFFT, deapodisation and phase fused around it.
+ *
+ * Every function returns MIRT_OK (0) or an error code; mirt_last_error()
+ * gives the message of the last failure on the calling thread.  Argument
+ * errors carry the reference gateway's own diagnostic, e.g.
+ * "interp2_table_mex failed: h1 size problem".
+ */
+#ifndef MIRT_B200_H
+#define MIRT_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MIRT_OK 0
+#define MIRT_ERR_ARG 1    /* invalid argument (reference: Fail() / mexFail()) */
+#define MIRT_ERR_CUDA 2   /* CUDA runtime error, or no CUDA device */
+#define MIRT_ERR_ALLOC 3  /* device allocation failed */
+#define MIRT_ERR_FFT 4    /* cuFFT error */
+
+/* Message of the last failing call on this thread ("" if none). */
+const char *mirt_last_error(void);
+
+/* Library version, major * 10000 + minor * 100 + patch. */
+int mirt_version(void);
+
+/* ------------------------------------------------------------------------
+ * 1. mex gateway drop-ins
+ *
+ * Common conventions:
+ *   *_re / *_im   data of a complex double mxArray (mxGetPr / mxGetPi).
+ *                 An `_im` of NULL means a real mxArray: for a table this
+ *                 selects the real-table kernels; for ck / fm it is the
+ *                 reference's "mxIsComplexDouble" failure.
+ *   *_rows/_cols  mxGetM / mxGetN of the array.
+ *   J, L, K       int32 arrays with their element counts (mxGetM*mxGetN).
+ *   order, flips  int32 arrays with element counts, or NULL when omitted.
+ *   tm            real double [M, D], column-major.
+ * ---------------------------------------------------------------------- */
+
+/* fm = interp1_table_mex(ck, h, J, L, tm, [order, flips])
+ * replaces nufft/table/interp1_table_mex.c:21-121 (gateway :126-149) and the
+ * kernels of nufft/table/interp1_table1_for.c:19,70,126.
+ * ck [K1, N] (ck_rows = K1, ck_cols = N); fm [M, N]. */
+int mirt_interp1_table_mex(
+	const double *ck_re, const double *ck_im, int64_t ck_rows, int64_t ck_cols,
+	const double *h_re, const double *h_im, int64_t h_rows, int64_t h_cols,
+	const int32_t *J, int64_t J_numel,
+	const int32_t *L, int64_t L_numel,
+	const double *tm, int64_t tm_rows, int64_t tm_cols,
+	const int32_t *order, int64_t order_numel,
+	const int32_t *flips, int64_t flips_numel,
+	double *fm_re, double *fm_im);
+
+/* fm = interp2_table_mex(ck, h1, h2, J, L, tm, [order, flips])
+ * replaces nufft/table/interp2_table_mex.c:14-128 (gateway :132-154) and the
+ * kernels of nufft/table/interp2_table1_for.c:24,106,198.
+ * ck has dimensions ck_dims[0..ck_ndim-1] = [K1 K2 N] (N = 1 if absent). */
+int mirt_interp2_table_mex(
+	const double *ck_re, const double *ck_im, const int64_t *ck_dims, int32_t ck_ndim,
+	const double *h1_re, const double *h1_im, int64_t h1_rows, int64_t h1_cols,
+	const double *h2_re, const double *h2_im, int64_t h2_rows, int64_t h2_cols,
+	const int32_t *J, int64_t J_numel,
+	const int32_t *L, int64_t L_numel,
+	const double *tm, int64_t tm_rows, int64_t tm_cols,
+	const int32_t *order, int64_t order_numel,
+	const int32_t *flips, int64_t flips_numel,
+	double *fm_re, double *fm_im);
+
+/* fm = interp3_table_mex(ck, h1, h2, h3, J, L, tm, [order, flips])
+ * replaces nufft/table/interp3_table_mex.c:14-146 (gateway :150-175) and the
+ * kernels of nufft/table/interp3_table1_for.c:24,134,258.
+ * ck dimensions [K1 K2 K3 N].  The reference gateway rejects N > 1
+ * ("N=1 done only", :85-86); this drop-in accepts any N. */
+int mirt_interp3_table_mex(
+	const double *ck_re, const double *ck_im, const int64_t *ck_dims, int32_t ck_ndim,
+	const double *h1_re, const double *h1_im, int64_t h1_rows, int64_t h1_cols,
+	const double *h2_re, const double *h2_im, int64_t h2_rows, int64_t h2_cols,
+	const double *h3_re, const double *h3_im, int64_t h3_rows, int64_t h3_cols,
+	const int32_t *J, int64_t J_numel,
+	const int32_t *L, int64_t L_numel,
+	const double *tm, int64_t tm_rows, int64_t tm_cols,
+	const int32_t *order, int64_t order_numel,
+	const int32_t *flips, int64_t flips_numel,
+	double *fm_re, double *fm_im);
+
+/* ck = interp1_table_adj_mex(fm, h, J, L, tm, K, [order, flips])
+ * replaces nufft/table/interp1_table_adj_mex.c:21-126 (gateway :131-154) and
+ * nufft/table/interp1_table1_adj.c:20,69,123.  fm [M, N]; ck [K1, N]. */
+int mirt_interp1_table_adj_mex(
+	const double *fm_re, const double *fm_im, int64_t fm_rows, int64_t fm_cols,
+	const double *h_re, const double *h_im, int64_t h_rows, int64_t h_cols,
+	const int32_t *J, int64_t J_numel,
+	const int32_t *L, int64_t L_numel,
+	const double *tm, int64_t tm_rows, int64_t tm_cols,
+	const int32_t *K, int64_t K_numel,
+	const int32_t *order, int64_t order_numel,
+	const int32_t *flips, int64_t flips_numel,
+	double *ck_re, double *ck_im);
+
+/* ck = interp2_table_adj_mex(fm, h1, h2, J, L, tm, K, [order, flips])
+ * replaces nufft/table/interp2_table_adj_mex.c:17-131 (gateway :135-159) and
+ * nufft/table/interp2_table1_adj.c:24,102,190.  ck [K1*K2, N]. */
+int mirt_interp2_table_adj_mex(
+	const double *fm_re, const double *fm_im, int64_t fm_rows, int64_t fm_cols,
+	const double *h1_re, const double *h1_im, int64_t h1_rows, int64_t h1_cols,
+	const double *h2_re, const double *h2_im, int64_t h2_rows, int64_t h2_cols,
+	const int32_t *J, int64_t J_numel,
+	const int32_t *L, int64_t L_numel,
+	const double *tm, int64_t tm_rows, int64_t tm_cols,
+	const int32_t *K, int64_t K_numel,
+	const int32_t *order, int64_t order_numel,
+	const int32_t *flips, int64_t flips_numel,
+	double *ck_re, double *ck_im);
+
+/* ck = interp3_table_adj_mex(fm, h1, h2, h3, J, L, tm, K, [order, flips])
+ * replaces nufft/table/interp3_table_adj_mex.c:17-149 (gateway :153-179) and
+ * nufft/table/interp3_table1_adj.c:24,127,243.  ck [K1*K2*K3, N]. */
+int mirt_interp3_table_adj_mex(
+	const double *fm_re, const double *fm_im, int64_t fm_rows, int64_t fm_cols,
+	const double *h1_re, const double *h1_im, int64_t h1_rows, int64_t h1_cols,
+	const double *h2_re, const double *h2_im, int64_t h2_rows, int64_t h2_cols,
+	const double *h3_re, const double *h3_im, int64_t h3_rows, int64_t h3_cols,
+	const int32_t *J, int64_t J_numel,
+	const int32_t *L, int64_t L_numel,
+	const double *tm, int64_t tm_rows, int64_t tm_cols,
+	const int32_t *K, int64_t K_numel,
+	const int32_t *order, int64_t order_numel,
+	const int32_t *flips, int64_t flips_numel,
+	double *ck_re, double *ck_im);
+
+/* ------------------------------------------------------------------------
+ * 2. device-resident interpolation plan (no reference counterpart: the
+ *    reference re-reads its tables and tm on every mex call)
+ *
+ * A plan covers `nslice` trajectories of slice_moff[s+1]-slice_moff[s]
+ * samples each, sharing geometry, tables and the column count `ncol`.
+ * Device layouts (float2 = complex64):
+ *   grid    ck[s][k][c]  k = k1 + K1*(k2 + K2*k3), c < ncol
+ *   samples fm[m][c]     m over all slices (slice s owns [moff[s], moff[s+1]))
+ * ---------------------------------------------------------------------- */
+typedef struct mirt_interp_plan mirt_interp_plan;
+
+/* tm: host FP64 [Mtot, D] column-major (t = omega / (2 pi / K)).
+ * h_re[d] / h_im[d]: host FP64 tables of length J[d]*L[d]+1; h_im == NULL or
+ * h_im[0] == NULL selects real tables.  slice_moff: nslice+1 offsets
+ * (NULL when nslice == 1).  phase_re/phase_im: optional host FP64 per-sample
+ * factor applied after the gather and conjugated before the spread (NULL for
+ * none).  stream: cudaStream_t used for the set-up work (NULL = default). */
+int mirt_interp_plan_create(mirt_interp_plan **plan, int32_t D,
+	const int32_t *K, const int32_t *J, const int32_t *L,
+	const double *const *h_re, const double *const *h_im, int32_t order,
+	const double *tm, int64_t Mtot, const int64_t *slice_moff, int32_t nslice,
+	int32_t ncol, const double *phase_re, const double *phase_im, void *stream);
+
+/* fm = interp(ck) on device buffers, asynchronous on `stream`. */
+int mirt_interp_plan_forward(mirt_interp_plan *plan, const void *ck, void *fm, void *stream);
+
+/* ck = interp_adj(fm) on device buffers; overwrites all of ck. */
+int mirt_interp_plan_adjoint(mirt_interp_plan *plan, const void *fm, void *ck, void *stream);
+
+int mirt_interp_plan_destroy(mirt_interp_plan *plan);
+
+/* ------------------------------------------------------------------------
+ * 3. device-resident NUFFT with min-max:KB tables
+ *    forward = nufft/nufft.m:128-165, adjoint = nufft/nufft_adj.m:32-80,
+ *    set-up = nufft/nufft_init.m:93-95 -> nufft/nufft_table_init.m:38-134
+ *
+ * om: host FP64 [Mtot, D] column-major, radians.  n_shift: D values.
+ * Device layouts:  image x[s][n][c] (n = n1 + N1*(n2 + N2*n3)),
+ *                  samples X[m][c].
+ * ---------------------------------------------------------------------- */
+typedef struct mirt_nufft mirt_nufft;
+
+int mirt_nufft_create(mirt_nufft **out, int32_t D, const int32_t *Nd, const int32_t *Kd,
+	const int32_t *Jd, const int32_t *Ld, const double *n_shift,
+	const double *om, int64_t Mtot, const int64_t *slice_moff, int32_t nslice,
+	int32_t ncol, void *stream);
+
+int mirt_nufft_forward(mirt_nufft *p, const void *x, void *X, void *stream);
+int mirt_nufft_adjoint(mirt_nufft *p, const void *X, void *x, void *stream);
+
+/* Same, from and to HOST complex64 buffers (interleaved re/im float pairs in
+ * the device layouts above); copies in and out are part of the call, which
+ * returns when the result is in host memory. */
+int mirt_nufft_forward_host(mirt_nufft *p, const float *x, float *X, void *stream);
+int mirt_nufft_adjoint_host(mirt_nufft *p, const float *X, float *x, void *stream);
+
+/* The interpolation plan inside a NUFFT (for direct gather/spread calls). */
+mirt_interp_plan *mirt_nufft_interp_plan(mirt_nufft *p);
+
+int mirt_nufft_destroy(mirt_nufft *p);
+
+/* Host FP64 builders used by mirt_nufft_create, exported for callers that
+ * build their own plans (st.h{d} and the 1D factors of st.sn):
+ *   table: length J*L+1 complex, nufft/nufft_table_init.m:111-134
+ *   scale: length N complex,  nufft/nufft_scale.m:54-75 with
+ *          nufft/nufft_alpha_kb_fit.m (st.sn = outer product of conj()). */
+int mirt_minmax_kb_table(int32_t N, int32_t J, int32_t K, int32_t L,
+	double *h_re, double *h_im);
+int mirt_minmax_kb_scale(int32_t N, int32_t J, int32_t K,
+	double *sn_re, double *sn_im);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MIRT_B200_H */

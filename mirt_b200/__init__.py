@@ -1,0 +1,24 @@
+"""mirt_b200 -- B200 (sm_100a) implementation of MIRT's table-based NUFFT
+interpolation (JeffFessler/mirt nufft/table/) behind the reference's own
+interfaces.
+
+* ``mirt_b200.mex``: the six mex gateways (interp{1,2,3}_table[_adj]_mex)
+* ``mirt_b200.nufft``: device plans, nufft_init / nufft / nufft_adj
+* ``include/mirt_b200.h``: the C ABI of libmirt_b200.so underneath both
+
+All compute runs in libmirt_b200.so; importing the package does not load it,
+calling any compute function does, and fails loudly if it has not been built.
+"""
+from ._lib import MirtError, load
+from .mex import (MexError, interp1_table_adj_mex, interp1_table_mex, interp2_table_adj_mex,
+                  interp2_table_mex, interp3_table_adj_mex, interp3_table_mex)
+from .nufft import (InterpPlan, NufftPlan, minmax_kb_scale, minmax_kb_table, nufft, nufft_adj,
+                    nufft_init)
+
+__all__ = [
+    "MirtError", "MexError", "load",
+    "interp1_table_mex", "interp2_table_mex", "interp3_table_mex",
+    "interp1_table_adj_mex", "interp2_table_adj_mex", "interp3_table_adj_mex",
+    "InterpPlan", "NufftPlan", "minmax_kb_table", "minmax_kb_scale",
+    "nufft_init", "nufft", "nufft_adj",
+]

@@ -1,0 +1,1115 @@
+// capi.cu -- the C ABI of include/mirt_b200.h.
+//
+// The mex drop-ins reproduce the gateways' argument checks and messages
+// (nufft/table/interp{1,2,3}_table{,_adj}_mex.c) and their column semantics,
+// then run the whole call on the GPU: FP64 split-complex host arrays are
+// copied in, converted to the device's interleaved FP32 layout, bin-sorted,
+// interpolated, converted back and copied out before the call returns.
+#include "../../include/mirt_b200.h"
+
+#include <cufft.h>
+
+#include <cmath>
+#include <complex>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <set>
+#include <string>
+#include <vector>
+
+#include "glue.cuh"
+#include "interp.cuh"
+
+namespace mirt {
+bool minmax_kb_table(int N, int J, int K, int L, std::vector<std::complex<double>> &h);
+void alpha_kb_fit(int N, int J, int K, std::vector<double> &alphas, double &beta);
+std::vector<std::complex<double>> scale1(int N, int K, const std::vector<double> &alpha,
+                                         double beta);
+}  // namespace mirt
+
+using namespace mirt;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string &msg) {
+  g_err = msg;
+  return code;
+}
+
+#define CK(call)                                                                      \
+  do {                                                                                \
+    cudaError_t e_ = (call);                                                          \
+    if (e_ != cudaSuccess)                                                            \
+      return fail(e_ == cudaErrorMemoryAllocation ? MIRT_ERR_ALLOC : MIRT_ERR_CUDA,   \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));                \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// caching device allocator: blocks are rounded up to a power of two and kept
+// for reuse, so repeated mex calls do not pay cudaMalloc / cudaFree.
+// ---------------------------------------------------------------------------
+std::mutex g_cache_mu;
+std::multimap<std::pair<int, size_t>, void *> g_free;
+
+size_t round_block(size_t b) {
+  size_t r = 256;
+  while (r < b) r <<= 1;
+  return r;
+}
+
+cudaError_t dalloc(void **p, size_t bytes) {
+  *p = nullptr;
+  if (bytes == 0) return cudaSuccess;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const size_t r = round_block(bytes);
+  {
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    auto it = g_free.find({dev, r});
+    if (it != g_free.end()) {
+      *p = it->second;
+      g_free.erase(it);
+      return cudaSuccess;
+    }
+  }
+  cudaError_t e = cudaMalloc(p, r);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    // release the cache and retry once
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    for (auto &kv : g_free) cudaFree(kv.second);
+    g_free.clear();
+    e = cudaMalloc(p, r);
+  }
+  return e;
+}
+
+void dfree(void *p, size_t bytes) {
+  if (!p) return;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(g_cache_mu);
+  g_free.insert({{dev, round_block(bytes)}, p});
+}
+
+struct DMem {
+  void *p = nullptr;
+  size_t bytes = 0;
+  DMem() = default;
+  DMem(const DMem &) = delete;
+  DMem &operator=(const DMem &) = delete;
+  ~DMem() { release(); }
+  void release() {
+    dfree(p, bytes);
+    p = nullptr;
+    bytes = 0;
+  }
+  cudaError_t alloc(size_t b) {
+    release();
+    bytes = b;
+    return dalloc(&p, b);
+  }
+  template <class T>
+  T *as() const {
+    return static_cast<T *>(p);
+  }
+};
+
+cudaStream_t as_stream(void *s) { return static_cast<cudaStream_t>(s); }
+
+int device_ok() {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    return fail(MIRT_ERR_CUDA, "no CUDA device available");
+  }
+  return MIRT_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// interpolation plan
+// ---------------------------------------------------------------------------
+struct mirt_interp_plan {
+  InterpArgs a{};
+  Tiling t{};
+  Launch lg{}, ls{};
+  DMem tm, slice, perm, bin_start, tab[MIRT_DMAX], phase, src[MIRT_DMAX], nsrc[MIRT_DMAX];
+  DMem keys, sorttmp, moff;
+  std::vector<long long> moff_host;
+};
+
+namespace {
+
+// Tile extents and launch shapes: heuristics sized for ~64 KB of shared
+// accumulator per spread CTA with the coil lanes innermost.
+void choose_config(mirt_interp_plan *P) {
+  InterpArgs &a = P->a;
+  Tiling &t = P->t;
+  const int C = a.C, D = a.g.D;
+  const int cw = C >= 32 ? 32 : C >= 8 ? 8 : C >= 4 ? 4 : 1;
+  const int threads = 256;
+  const int ngroups = threads / cw;
+  size_t tabb = 0;
+  for (int d = 0; d < D; d++) tabb += ((size_t)a.g.tlen[d] * (a.real_tab ? 4 : 8) + 15) & ~15ull;
+
+  Launch &lg = P->lg;
+  lg.threads = threads;
+  lg.cw = cw;
+  int sb = ngroups * 4;
+  if (sb < 32) sb = 32;
+  if (sb > 256) sb = 256;
+  lg.sb = sb;
+  lg.tab_smem = tabb <= 112 * 1024 ? 1 : 0;
+  lg.grid = 0;
+
+  const int npts_target = 65536 / (cw * 8);
+  int T[MIRT_DMAX] = {1, 1, 1};
+  if (D == 1) {
+    T[0] = npts_target;
+  } else if (D == 2) {
+    int t1 = 1;
+    while (t1 * t1 < npts_target) t1 <<= 1;
+    T[0] = t1;
+    T[1] = npts_target / t1;
+  } else {
+    int t1 = 1;
+    while (t1 * t1 * t1 < npts_target) t1 <<= 1;
+    T[0] = t1;
+    int rest = npts_target / t1;
+    int t2 = 1;
+    while (t2 * t2 < rest) t2 <<= 1;
+    T[1] = t2;
+    T[2] = rest / t2;
+  }
+  int P3[MIRT_DMAX] = {1, 1, 1};
+  if (D == 1) {
+    P3[0] = ngroups;
+  } else if (D == 2) {
+    P3[0] = ngroups < 8 ? ngroups : 8;
+    P3[1] = ngroups / P3[0];
+  } else {
+    P3[0] = ngroups < 4 ? ngroups : 4;
+    const int r = ngroups / P3[0];
+    P3[1] = r < 4 ? r : 4;
+    P3[2] = r / P3[1];
+  }
+  for (int d = 0; d < D; d++) {
+    if (T[d] > a.g.K[d]) T[d] = a.g.K[d];
+    if (T[d] < 1) T[d] = 1;
+  }
+  Launch &ls = P->ls;
+  ls.threads = threads;
+  ls.cw = cw;
+  ls.sb = 64;
+  for (int d = 0; d < MIRT_DMAX; d++) ls.P[d] = P3[d];
+  int npts = 1;
+  for (int d = 0; d < D; d++) npts *= T[d];
+  int SJ = 0;
+  for (int d = 0; d < D; d++) SJ += a.g.J[d];
+  const size_t rest = (size_t)npts * cw * 8 + (size_t)ls.sb * SJ * 12 + (size_t)ls.sb * 8 +
+                      (size_t)ls.sb * cw * 8 + 64;
+  ls.tab_smem = (tabb + rest) <= 200 * 1024 ? 1 : 0;
+  for (int d = 0; d < MIRT_DMAX; d++) {
+    t.T[d] = d < D ? T[d] : 1;
+    t.nb[d] = d < D ? (a.g.K[d] + T[d] - 1) / T[d] : 1;
+  }
+  t.ntiles = t.nb[0] * t.nb[1] * t.nb[2];
+}
+
+// Source bins per dimension: tiles whose samples (binned by the first tap
+// koff mod K) can have a tap inside tile b, i.e. koff in [lo-J+1, hi-1] mod K.
+int build_sources(mirt_interp_plan *P, cudaStream_t st) {
+  const InterpArgs &a = P->a;
+  Tiling &t = P->t;
+  for (int d = 0; d < MIRT_DMAX; d++) {
+    const int nb = t.nb[d];
+    std::vector<int> src((size_t)nb * MIRT_SRCMAX, 0), nsrc(nb, 1);
+    if (d < a.g.D) {
+      const int K = a.g.K[d], T = t.T[d], J = a.g.J[d];
+      for (int b = 0; b < nb; b++) {
+        const int lo = b * T, hi = std::min(lo + T, K);
+        const long long n = (long long)(hi - lo) + J - 1;
+        std::vector<int> list;
+        if (n >= K) {
+          for (int i = 0; i < nb; i++) list.push_back(i);
+        } else {
+          int x0 = ((lo - J + 1) % K + K) % K;
+          std::set<int> seen;
+          for (long long i = 0; i < n; i++) {
+            const int x = (int)((x0 + i) % K);
+            const int bb = x / T;
+            if (!seen.count(bb)) {
+              seen.insert(bb);
+              list.push_back(bb);
+            }
+          }
+        }
+        if ((int)list.size() > MIRT_SRCMAX)
+          return fail(MIRT_ERR_ARG, "tile too small for the interpolator width");
+        nsrc[b] = (int)list.size();
+        for (size_t i = 0; i < list.size(); i++) src[(size_t)b * MIRT_SRCMAX + i] = list[i];
+      }
+    } else {
+      src[0] = 0;
+    }
+    CK(P->src[d].alloc(src.size() * sizeof(int)));
+    CK(P->nsrc[d].alloc(nsrc.size() * sizeof(int)));
+    CK(cudaMemcpyAsync(P->src[d].p, src.data(), src.size() * sizeof(int),
+                       cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(P->nsrc[d].p, nsrc.data(), nsrc.size() * sizeof(int),
+                       cudaMemcpyHostToDevice, st));
+    t.src[d] = P->src[d].as<int>();
+    t.nsrc[d] = P->nsrc[d].as<int>();
+  }
+  // the host vectors above are released at scope exit: wait for the copies
+  CK(cudaStreamSynchronize(st));
+  return MIRT_OK;
+}
+
+// Fill geometry and upload tables.  Tables arrive as host FP64.
+int plan_geometry(mirt_interp_plan *P, int D, const int *K, const int *J, const int *L,
+                  const double *const *h_re, const double *const *h_im, int order, int C,
+                  cudaStream_t st) {
+  InterpArgs &a = P->a;
+  a.g.D = D;
+  long long stride = 1;
+  const bool cplx = h_im != nullptr && h_im[0] != nullptr;
+  a.real_tab = cplx ? 0 : 1;
+  a.order = order;
+  a.C = C;
+  for (int d = 0; d < MIRT_DMAX; d++) {
+    if (d < D) {
+      a.g.K[d] = K[d];
+      a.g.J[d] = J[d];
+      a.g.L[d] = L[d];
+      a.g.ncenter[d] = (int)std::floor(J[d] * L[d] / 2.);
+      a.g.tlen[d] = J[d] * L[d] + 1;
+      a.g.kstride[d] = stride;
+      stride *= K[d];
+    } else {
+      a.g.K[d] = 1;
+      a.g.J[d] = 1;
+      a.g.L[d] = 1;
+      a.g.ncenter[d] = 0;
+      a.g.tlen[d] = 1;
+      a.g.kstride[d] = stride;
+    }
+  }
+  a.grid_elems = stride * C;
+  for (int d = 0; d < D; d++) {
+    const int n = a.g.tlen[d];
+    if (cplx) {
+      std::vector<float2> h(n);
+      for (int i = 0; i < n; i++) h[i] = make_float2((float)h_re[d][i], (float)h_im[d][i]);
+      CK(P->tab[d].alloc(n * sizeof(float2)));
+      CK(cudaMemcpyAsync(P->tab[d].p, h.data(), n * sizeof(float2), cudaMemcpyHostToDevice, st));
+      CK(cudaStreamSynchronize(st));
+    } else {
+      std::vector<float> h(n);
+      for (int i = 0; i < n; i++) h[i] = (float)h_re[d][i];
+      CK(P->tab[d].alloc(n * sizeof(float)));
+      CK(cudaMemcpyAsync(P->tab[d].p, h.data(), n * sizeof(float), cudaMemcpyHostToDevice, st));
+      CK(cudaStreamSynchronize(st));
+    }
+    a.tab[d] = P->tab[d].p;
+  }
+  return MIRT_OK;
+}
+
+// Slices, tiling, bin sort.  P->tm must hold the FP64 coordinates on device.
+int plan_finish(mirt_interp_plan *P, long long Mtot, const long long *moff, int nslice,
+                cudaStream_t st) {
+  InterpArgs &a = P->a;
+  a.Mtot = Mtot;
+  a.tm = P->tm.as<double>();
+  P->t.nslice = nslice;
+  P->moff_host.assign(moff, moff + nslice + 1);
+  if (nslice > 1) {
+    CK(P->moff.alloc((nslice + 1) * sizeof(long long)));
+    CK(cudaMemcpyAsync(P->moff.p, moff, (nslice + 1) * sizeof(long long),
+                       cudaMemcpyHostToDevice, st));
+    CK(P->slice.alloc(Mtot * sizeof(int)));
+    CK(launch_fill_slice(P->moff.as<long long>(), nslice, Mtot, P->slice.as<int>(), st));
+    a.slice_id = P->slice.as<int>();
+  } else {
+    a.slice_id = nullptr;
+  }
+  choose_config(P);
+  int rc = build_sources(P, st);
+  if (rc) return rc;
+  const long long nbins = (long long)P->t.ntiles * nslice;
+  if (nbins >= (1ll << 31)) return fail(MIRT_ERR_ARG, "too many grid tiles");
+  CK(P->keys.alloc(std::max<long long>(Mtot, 1) * sizeof(uint32_t)));
+  CK(P->perm.alloc(std::max<long long>(Mtot, 1) * sizeof(int)));
+  CK(P->bin_start.alloc((nbins + 1) * sizeof(int)));
+  CK(P->sorttmp.alloc(radix_sort_tmp_bytes(Mtot)));
+  CK(launch_bin_keys(a, P->t, P->keys.as<uint32_t>(), st));
+  CK(radix_sort_bins(P->keys.as<uint32_t>(), Mtot, (int)nbins, P->sorttmp.p, P->perm.as<int>(),
+                     P->bin_start.as<int>(), st));
+  a.perm = P->perm.as<int>();
+  P->sorttmp.release();
+  CK(query_gather_grid(a, P->lg));
+  return MIRT_OK;
+}
+
+int validate_geometry(int D, const int *K, const int *J, const int *L, int order, bool cplx,
+                      long long Mtot, int C) {
+  if (D < 1 || D > MIRT_DMAX) return fail(MIRT_ERR_ARG, "D must be 1, 2 or 3");
+  for (int d = 0; d < D; d++) {
+    if (K[d] < 1) return fail(MIRT_ERR_ARG, "K must be positive");
+    if (J[d] < 1 || J[d] > MIRT_JMAX) return fail(MIRT_ERR_ARG, "J must be in 1..16");
+    if (L[d] < 1) return fail(MIRT_ERR_ARG, "L must be positive");
+    if ((long long)J[d] * L[d] + 1 > (1ll << 30)) return fail(MIRT_ERR_ARG, "table too long");
+  }
+  if (order != 0 && order != 1) return fail(MIRT_ERR_ARG, "bad order");
+  if (cplx && order) return fail(MIRT_ERR_ARG, "only 0th order implemented for complex");
+  if (Mtot < 0 || Mtot >= (1ll << 31)) return fail(MIRT_ERR_ARG, "too many samples");
+  if (C < 0) return fail(MIRT_ERR_ARG, "bad column count");
+  long long g = C;
+  for (int d = 0; d < D; d++) g *= K[d];
+  if (g >= (1ll << 31)) return fail(MIRT_ERR_ARG, "grid too large for one slice");
+  return MIRT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *mirt_last_error(void) { return g_err.c_str(); }
+
+int mirt_version(void) { return 100; }
+
+int mirt_interp_plan_create(mirt_interp_plan **plan, int32_t D, const int32_t *K,
+                            const int32_t *J, const int32_t *L, const double *const *h_re,
+                            const double *const *h_im, int32_t order, const double *tm,
+                            int64_t Mtot, const int64_t *slice_moff, int32_t nslice,
+                            int32_t ncol, const double *phase_re, const double *phase_im,
+                            void *stream) {
+  if (!plan) return fail(MIRT_ERR_ARG, "plan pointer is NULL");
+  *plan = nullptr;
+  int rc = device_ok();
+  if (rc) return rc;
+  const bool cplx = h_im != nullptr && h_im[0] != nullptr;
+  if (nslice < 1) return fail(MIRT_ERR_ARG, "nslice must be >= 1");
+  rc = validate_geometry(D, K, J, L, order, cplx, Mtot, ncol);
+  if (rc) return rc;
+  std::vector<long long> moff(nslice + 1);
+  if (slice_moff) {
+    for (int s = 0; s <= nslice; s++) moff[s] = slice_moff[s];
+    if (moff[0] != 0 || moff[nslice] != Mtot)
+      return fail(MIRT_ERR_ARG, "slice offsets must start at 0 and end at Mtot");
+    for (int s = 0; s < nslice; s++)
+      if (moff[s + 1] < moff[s]) return fail(MIRT_ERR_ARG, "slice offsets must not decrease");
+  } else {
+    if (nslice != 1) return fail(MIRT_ERR_ARG, "slice offsets required for nslice > 1");
+    moff[0] = 0;
+    moff[1] = Mtot;
+  }
+  cudaStream_t st = as_stream(stream);
+  auto *P = new mirt_interp_plan();
+  rc = plan_geometry(P, D, K, J, L, h_re, h_im, order, ncol, st);
+  if (!rc) {
+    cudaError_t e = P->tm.alloc(std::max<long long>(Mtot, 1) * D * sizeof(double));
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(P->tm.p, tm, Mtot * D * sizeof(double), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && phase_re) {
+      std::vector<float2> ph(Mtot);
+      for (long long m = 0; m < Mtot; m++)
+        ph[m] = make_float2((float)phase_re[m], phase_im ? (float)phase_im[m] : 0.f);
+      e = P->phase.alloc(std::max<long long>(Mtot, 1) * sizeof(float2));
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(P->phase.p, ph.data(), Mtot * sizeof(float2), cudaMemcpyHostToDevice,
+                            st);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+      P->a.phase = P->phase.as<float2>();
+    }
+    if (e != cudaSuccess) rc = fail(MIRT_ERR_CUDA, std::string("plan upload: ") + cudaGetErrorString(e));
+  }
+  if (!rc) rc = plan_finish(P, Mtot, moff.data(), nslice, st);
+  if (!rc) {
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) rc = fail(MIRT_ERR_CUDA, std::string("plan: ") + cudaGetErrorString(e));
+  }
+  if (rc) {
+    delete P;
+    return rc;
+  }
+  *plan = P;
+  return MIRT_OK;
+}
+
+int mirt_interp_plan_forward(mirt_interp_plan *P, const void *ck, void *fm, void *stream) {
+  if (!P) return fail(MIRT_ERR_ARG, "plan is NULL");
+  CK(launch_gather(P->a, P->lg, static_cast<const float2 *>(ck), static_cast<float2 *>(fm),
+                   as_stream(stream)));
+  return MIRT_OK;
+}
+
+int mirt_interp_plan_adjoint(mirt_interp_plan *P, const void *fm, void *ck, void *stream) {
+  if (!P) return fail(MIRT_ERR_ARG, "plan is NULL");
+  CK(launch_spread(P->a, P->t, P->ls, P->bin_start.as<int>(), static_cast<const float2 *>(fm),
+                   static_cast<float2 *>(ck), as_stream(stream)));
+  return MIRT_OK;
+}
+
+int mirt_interp_plan_destroy(mirt_interp_plan *P) {
+  if (P) {
+    cudaDeviceSynchronize();
+    delete P;
+  }
+  return MIRT_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// mex gateway drop-ins
+// ---------------------------------------------------------------------------
+namespace {
+
+struct Tab {
+  const double *re, *im;
+  int64_t rows, cols;
+};
+
+struct MexCall {
+  const char *gateway;  // the gateway's mexFail() text
+  int D;
+  bool adj;
+  int K[MIRT_DMAX], J[MIRT_DMAX], L[MIRT_DMAX];
+  Tab h[MIRT_DMAX];
+  int order;
+  long long M;
+  int N;
+  const double *tm;
+  const double *in_re, *in_im;
+  double *out_re, *out_im;
+};
+
+int mex_fail(const MexCall &c, const std::string &why) {
+  return fail(MIRT_ERR_ARG, std::string(c.gateway) + ": " + why);
+}
+
+std::mutex g_mex_mu;
+cudaStream_t g_mex_stream = nullptr;
+
+// Table kind and order checks shared by all gateways, in the gateways' order
+// (e.g. nufft/table/interp2_table_mex.c:78-126).
+int mex_check_tables(MexCall &c, const int32_t *flips, int64_t flips_numel) {
+  bool all_cx = true, all_re = true;
+  for (int d = 0; d < c.D; d++) {
+    if (c.h[d].im) all_re = false;
+    else all_cx = false;
+  }
+  if (all_cx) {
+    if (c.order) return mex_fail(c, "only 0th order implemented for complex");
+  } else if (all_re) {
+    if (c.order != 0 && c.order != 1) return mex_fail(c, "bad order");
+    if (flips)
+      for (int64_t i = 0; i < flips_numel; i++)
+        if (flips[i]) return mex_fail(c, "flip not compiled");
+  } else {
+    return mex_fail(c, "h must be real or complex double (preferably real)");
+  }
+  for (int d = 0; d < c.D; d++) {
+    if (c.J[d] < 1 || c.J[d] > MIRT_JMAX)
+      return mex_fail(c, "J outside 1..16 is not supported by the GPU kernels");
+    if (c.L[d] < 1) return mex_fail(c, "L must be positive");
+    if (c.K[d] < 1) return mex_fail(c, "K must be positive");
+  }
+  return MIRT_OK;
+}
+
+int mex_run(MexCall &c) {
+  int rc = device_ok();
+  if (rc) return rc;
+  std::lock_guard<std::mutex> lk(g_mex_mu);
+  if (!g_mex_stream) CK(cudaStreamCreateWithFlags(&g_mex_stream, cudaStreamNonBlocking));
+  cudaStream_t st = g_mex_stream;
+  long long nk = 1;
+  for (int d = 0; d < c.D; d++) nk *= c.K[d];
+  const long long M = c.M;
+  const int N = c.N;
+  {
+    long long g = (long long)N;
+    for (int d = 0; d < c.D; d++) g *= c.K[d];
+    if (g >= (1ll << 31)) return mex_fail(c, "grid times columns too large");
+    if (M >= (1ll << 31)) return mex_fail(c, "too many samples");
+  }
+  const bool cplx = c.h[0].im != nullptr;
+  const double *hr[MIRT_DMAX] = {nullptr, nullptr, nullptr};
+  const double *hi[MIRT_DMAX] = {nullptr, nullptr, nullptr};
+  for (int d = 0; d < c.D; d++) {
+    hr[d] = c.h[d].re;
+    hi[d] = c.h[d].im;
+  }
+  mirt_interp_plan P;
+  rc = plan_geometry(&P, c.D, c.K, c.J, c.L, hr, cplx ? hi : nullptr, c.order, N, st);
+  if (rc) return rc;
+  CK(P.tm.alloc(std::max<long long>(M, 1) * c.D * sizeof(double)));
+  if (M) CK(cudaMemcpyAsync(P.tm.p, c.tm, M * c.D * sizeof(double), cudaMemcpyHostToDevice, st));
+  const long long moff[2] = {0, M};
+  rc = plan_finish(&P, M, moff, 1, st);
+  if (rc) return rc;
+
+  const long long nin = c.adj ? M : nk;
+  const long long nout = c.adj ? nk : M;
+  DMem in_split, in_il, out_il, out_split;
+  CK(in_split.alloc(std::max<long long>(nin * N, 1) * 2 * sizeof(double)));
+  CK(in_il.alloc(std::max<long long>(nin * N, 1) * sizeof(float2)));
+  CK(out_il.alloc(std::max<long long>(nout * N, 1) * sizeof(float2)));
+  CK(out_split.alloc(std::max<long long>(nout * N, 1) * 2 * sizeof(double)));
+  double *ir = in_split.as<double>(), *ii = ir + nin * N;
+  double *orr = out_split.as<double>(), *oi = orr + nout * N;
+  if (nin * N) {
+    CK(cudaMemcpyAsync(ir, c.in_re, nin * N * sizeof(double), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(ii, c.in_im, nin * N * sizeof(double), cudaMemcpyHostToDevice, st));
+  }
+  CK(launch_split_to_il(ir, ii, nin, N, in_il.as<float2>(), st));
+  if (c.adj)
+    CK(launch_spread(P.a, P.t, P.ls, P.bin_start.as<int>(), in_il.as<float2>(),
+                     out_il.as<float2>(), st));
+  else
+    CK(launch_gather(P.a, P.lg, in_il.as<float2>(), out_il.as<float2>(), st));
+  CK(launch_il_to_split(out_il.as<float2>(), nout, N, orr, oi, st));
+  if (nout * N) {
+    CK(cudaMemcpyAsync(c.out_re, orr, nout * N * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(c.out_im, oi, nout * N * sizeof(double), cudaMemcpyDeviceToHost, st));
+  }
+  CK(cudaStreamSynchronize(st));
+  return MIRT_OK;
+}
+
+// table size check of the gateways: "hD size problem" (2D/3D) / "h size problem" (1D)
+bool tab_len_ok(const Tab &h, int J, int L) { return h.rows == (int64_t)J * L + 1 && h.cols == 1; }
+
+}  // namespace
+
+extern "C" {
+
+int mirt_interp1_table_mex(const double *ck_re, const double *ck_im, int64_t ck_rows,
+                           int64_t ck_cols, const double *h_re, const double *h_im,
+                           int64_t h_rows, int64_t h_cols, const int32_t *J, int64_t J_numel,
+                           const int32_t *L, int64_t L_numel, const double *tm, int64_t tm_rows,
+                           int64_t tm_cols, const int32_t *order, int64_t order_numel,
+                           const int32_t *flips, int64_t flips_numel, double *fm_re,
+                           double *fm_im) {
+  MexCall c{};
+  c.gateway = "interp1_table_mex() failed";
+  c.D = 1;
+  c.adj = false;
+  if (!ck_re || !ck_im) return mex_fail(c, "mxIsComplexDouble");
+  if (!tm) return mex_fail(c, "mxIsRealDouble");
+  if (!J || J_numel != 1) return mex_fail(c, "J must be scalar int32");
+  if (!L || L_numel != 1) return mex_fail(c, "L must be scalar int32");
+  if (order && order_numel != 1) return mex_fail(c, "order must be scalar int32 (0 | 1)");
+  if (flips && flips_numel != 1) return mex_fail(c, "flips must be scalar int32 (0 | 1)");
+  c.J[0] = J[0];
+  c.L[0] = L[0];
+  c.h[0] = Tab{h_re, h_im, h_rows, h_cols};
+  if (!h_re || !tab_len_ok(c.h[0], c.J[0], c.L[0])) return mex_fail(c, "h size problem");
+  if (tm_cols != 1) return mex_fail(c, "t_m must be col vector.");
+  c.K[0] = (int)ck_rows;
+  c.N = (int)ck_cols;
+  c.M = tm_rows;
+  c.order = order ? order[0] : 0;
+  int rc = mex_check_tables(c, flips, flips_numel);
+  if (rc) return rc;
+  c.tm = tm;
+  c.in_re = ck_re;
+  c.in_im = ck_im;
+  c.out_re = fm_re;
+  c.out_im = fm_im;
+  return mex_run(c);
+}
+
+int mirt_interp2_table_mex(const double *ck_re, const double *ck_im, const int64_t *ck_dims,
+                           int32_t ck_ndim, const double *h1_re, const double *h1_im,
+                           int64_t h1_rows, int64_t h1_cols, const double *h2_re,
+                           const double *h2_im, int64_t h2_rows, int64_t h2_cols,
+                           const int32_t *J, int64_t J_numel, const int32_t *L, int64_t L_numel,
+                           const double *tm, int64_t tm_rows, int64_t tm_cols,
+                           const int32_t *order, int64_t order_numel, const int32_t *flips,
+                           int64_t flips_numel, double *fm_re, double *fm_im) {
+  MexCall c{};
+  c.gateway = "interp2_table_mex failed";
+  c.D = 2;
+  c.adj = false;
+  if (!ck_re || !ck_im) return mex_fail(c, "mxIsComplexDouble");
+  if (!tm) return mex_fail(c, "mxIsRealDouble");
+  if (!J || J_numel != 2) return mex_fail(c, "J must be [1,2]");
+  if (!L || L_numel != 2) return mex_fail(c, "L must be [1,2]");
+  if (order && order_numel != 1) return mex_fail(c, "order must be scalar int32 (0 | 1)");
+  if (flips && flips_numel != 2) return mex_fail(c, "flips must be [1 2] int32 (0 | 1)");
+  for (int d = 0; d < 2; d++) {
+    c.J[d] = J[d];
+    c.L[d] = L[d];
+  }
+  c.h[0] = Tab{h1_re, h1_im, h1_rows, h1_cols};
+  c.h[1] = Tab{h2_re, h2_im, h2_rows, h2_cols};
+  if (!h1_re || !tab_len_ok(c.h[0], c.J[0], c.L[0])) return mex_fail(c, "h1 size problem");
+  if (!h2_re || !tab_len_ok(c.h[1], c.J[1], c.L[1])) return mex_fail(c, "h2 size problem");
+  if (tm_cols != 2) return mex_fail(c, "tm must have 2 columns");
+  c.K[0] = ck_ndim > 0 ? (int)ck_dims[0] : 1;
+  c.K[1] = ck_ndim > 1 ? (int)ck_dims[1] : 1;
+  c.N = ck_ndim > 2 ? (int)ck_dims[2] : 1;
+  c.M = tm_rows;
+  c.order = order ? order[0] : 0;
+  int rc = mex_check_tables(c, flips, flips_numel);
+  if (rc) return rc;
+  c.tm = tm;
+  c.in_re = ck_re;
+  c.in_im = ck_im;
+  c.out_re = fm_re;
+  c.out_im = fm_im;
+  return mex_run(c);
+}
+
+int mirt_interp3_table_mex(const double *ck_re, const double *ck_im, const int64_t *ck_dims,
+                           int32_t ck_ndim, const double *h1_re, const double *h1_im,
+                           int64_t h1_rows, int64_t h1_cols, const double *h2_re,
+                           const double *h2_im, int64_t h2_rows, int64_t h2_cols,
+                           const double *h3_re, const double *h3_im, int64_t h3_rows,
+                           int64_t h3_cols, const int32_t *J, int64_t J_numel, const int32_t *L,
+                           int64_t L_numel, const double *tm, int64_t tm_rows, int64_t tm_cols,
+                           const int32_t *order, int64_t order_numel, const int32_t *flips,
+                           int64_t flips_numel, double *fm_re, double *fm_im) {
+  MexCall c{};
+  c.gateway = "interp3_table_mex failed";
+  c.D = 3;
+  c.adj = false;
+  if (!ck_re || !ck_im) return mex_fail(c, "mxIsComplexDouble");
+  if (!tm) return mex_fail(c, "mxIsRealDouble");
+  if (!J || J_numel != 3) return mex_fail(c, "J must be [1,3]");
+  if (!L || L_numel != 3) return mex_fail(c, "L must be [1,3]");
+  if (order && order_numel != 1) return mex_fail(c, "order must be scalar int32 (0 | 1)");
+  if (flips && flips_numel != 3) return mex_fail(c, "flips must be [1 3] int32 (0 | 1)");
+  for (int d = 0; d < 3; d++) {
+    c.J[d] = J[d];
+    c.L[d] = L[d];
+  }
+  c.h[0] = Tab{h1_re, h1_im, h1_rows, h1_cols};
+  c.h[1] = Tab{h2_re, h2_im, h2_rows, h2_cols};
+  c.h[2] = Tab{h3_re, h3_im, h3_rows, h3_cols};
+  if (!h1_re || !tab_len_ok(c.h[0], c.J[0], c.L[0])) return mex_fail(c, "h1 size problem");
+  if (!h2_re || !tab_len_ok(c.h[1], c.J[1], c.L[1])) return mex_fail(c, "h2 size problem");
+  if (!h3_re || !tab_len_ok(c.h[2], c.J[2], c.L[2])) return mex_fail(c, "h3 size problem");
+  if (tm_cols != 3) return mex_fail(c, "tm must have 3 columns");
+  c.K[0] = ck_ndim > 0 ? (int)ck_dims[0] : 1;
+  c.K[1] = ck_ndim > 1 ? (int)ck_dims[1] : 1;
+  c.K[2] = ck_ndim > 2 ? (int)ck_dims[2] : 1;
+  c.N = ck_ndim > 3 ? (int)ck_dims[3] : 1;
+  c.M = tm_rows;
+  c.order = order ? order[0] : 0;
+  int rc = mex_check_tables(c, flips, flips_numel);
+  if (rc) return rc;
+  c.tm = tm;
+  c.in_re = ck_re;
+  c.in_im = ck_im;
+  c.out_re = fm_re;
+  c.out_im = fm_im;
+  return mex_run(c);
+}
+
+int mirt_interp1_table_adj_mex(const double *fm_re, const double *fm_im, int64_t fm_rows,
+                               int64_t fm_cols, const double *h_re, const double *h_im,
+                               int64_t h_rows, int64_t h_cols, const int32_t *J, int64_t J_numel,
+                               const int32_t *L, int64_t L_numel, const double *tm,
+                               int64_t tm_rows, int64_t tm_cols, const int32_t *K,
+                               int64_t K_numel, const int32_t *order, int64_t order_numel,
+                               const int32_t *flips, int64_t flips_numel, double *ck_re,
+                               double *ck_im) {
+  MexCall c{};
+  c.gateway = "interp1_table_adj_mex() failed";
+  c.D = 1;
+  c.adj = true;
+  if (!fm_re || !fm_im) return mex_fail(c, "mxIsComplexDouble");
+  if (!tm) return mex_fail(c, "mxIsRealDouble");
+  if (!J || J_numel != 1) return mex_fail(c, "J must be scalar int32");
+  if (!K || K_numel != 1) return mex_fail(c, "K must be scalar int32");
+  if (!L || L_numel != 1) return mex_fail(c, "L must be scalar int32");
+  if (order && order_numel != 1) return mex_fail(c, "order must be scalar int32 (0 | 1)");
+  if (flips && flips_numel != 1) return mex_fail(c, "flips must be scalar int32 (0 | 1)");
+  c.J[0] = J[0];
+  c.L[0] = L[0];
+  c.K[0] = K[0];
+  c.h[0] = Tab{h_re, h_im, h_rows, h_cols};
+  if (!h_re || h_rows != (int64_t)c.J[0] * c.L[0] + 1) return mex_fail(c, "h size problem");
+  if (h_cols != 1) return mex_fail(c, "h must be col vector");
+  if (fm_rows != tm_rows || tm_cols != 1) return mex_fail(c, "t_m must be Mx1 col vector");
+  c.M = fm_rows;
+  c.N = (int)fm_cols;
+  c.order = order ? order[0] : 0;
+  int rc = mex_check_tables(c, flips, flips_numel);
+  if (rc) return rc;
+  c.tm = tm;
+  c.in_re = fm_re;
+  c.in_im = fm_im;
+  c.out_re = ck_re;
+  c.out_im = ck_im;
+  return mex_run(c);
+}
+
+int mirt_interp2_table_adj_mex(const double *fm_re, const double *fm_im, int64_t fm_rows,
+                               int64_t fm_cols, const double *h1_re, const double *h1_im,
+                               int64_t h1_rows, int64_t h1_cols, const double *h2_re,
+                               const double *h2_im, int64_t h2_rows, int64_t h2_cols,
+                               const int32_t *J, int64_t J_numel, const int32_t *L,
+                               int64_t L_numel, const double *tm, int64_t tm_rows,
+                               int64_t tm_cols, const int32_t *K, int64_t K_numel,
+                               const int32_t *order, int64_t order_numel, const int32_t *flips,
+                               int64_t flips_numel, double *ck_re, double *ck_im) {
+  MexCall c{};
+  c.gateway = "interp2_table_adj_mex() failed";
+  c.D = 2;
+  c.adj = true;
+  if (!fm_re || !fm_im) return mex_fail(c, "mxIsComplexDouble");
+  if (!tm) return mex_fail(c, "mxIsRealDouble");
+  if (!J || J_numel != 2) return mex_fail(c, "J must be int32 [1,2]");
+  if (!L || L_numel != 2) return mex_fail(c, "L must be int32 [1,2]");
+  if (!K || K_numel != 2) return mex_fail(c, "K must be int32 [1,2]");
+  if (order && order_numel != 1) return mex_fail(c, "order must be scalar int32 (0 | 1)");
+  if (flips && flips_numel != 2) return mex_fail(c, "flips must be [1 2] int32 (0 | 1)");
+  for (int d = 0; d < 2; d++) {
+    c.J[d] = J[d];
+    c.L[d] = L[d];
+    c.K[d] = K[d];
+  }
+  c.h[0] = Tab{h1_re, h1_im, h1_rows, h1_cols};
+  c.h[1] = Tab{h2_re, h2_im, h2_rows, h2_cols};
+  if (!h1_re || !tab_len_ok(c.h[0], c.J[0], c.L[0])) return mex_fail(c, "h1 size problem");
+  if (!h2_re || !tab_len_ok(c.h[1], c.J[1], c.L[1])) return mex_fail(c, "h2 size problem");
+  if (fm_rows != tm_rows || tm_cols != 2) return mex_fail(c, "t_m must be Mx2 matrix");
+  c.M = fm_rows;
+  c.N = (int)fm_cols;
+  c.order = order ? order[0] : 0;
+  int rc = mex_check_tables(c, flips, flips_numel);
+  if (rc) return rc;
+  c.tm = tm;
+  c.in_re = fm_re;
+  c.in_im = fm_im;
+  c.out_re = ck_re;
+  c.out_im = ck_im;
+  return mex_run(c);
+}
+
+int mirt_interp3_table_adj_mex(const double *fm_re, const double *fm_im, int64_t fm_rows,
+                               int64_t fm_cols, const double *h1_re, const double *h1_im,
+                               int64_t h1_rows, int64_t h1_cols, const double *h2_re,
+                               const double *h2_im, int64_t h2_rows, int64_t h2_cols,
+                               const double *h3_re, const double *h3_im, int64_t h3_rows,
+                               int64_t h3_cols, const int32_t *J, int64_t J_numel,
+                               const int32_t *L, int64_t L_numel, const double *tm,
+                               int64_t tm_rows, int64_t tm_cols, const int32_t *K,
+                               int64_t K_numel, const int32_t *order, int64_t order_numel,
+                               const int32_t *flips, int64_t flips_numel, double *ck_re,
+                               double *ck_im) {
+  MexCall c{};
+  c.gateway = "interp3_table_adj_mex() failed";
+  c.D = 3;
+  c.adj = true;
+  if (!fm_re || !fm_im) return mex_fail(c, "mxIsComplexDouble");
+  if (!tm) return mex_fail(c, "mxIsRealDouble");
+  if (!J || J_numel != 3) return mex_fail(c, "J must be int32 [1,3]");
+  if (!L || L_numel != 3) return mex_fail(c, "L must be int32 [1,3]");
+  if (!K || K_numel != 3) return mex_fail(c, "K must be int32 [1,3]");
+  if (order && order_numel != 1) return mex_fail(c, "order must be scalar int32 (0 | 1)");
+  if (flips && flips_numel != 3) return mex_fail(c, "flips must be [1 3] int32 (0 | 1)");
+  for (int d = 0; d < 3; d++) {
+    c.J[d] = J[d];
+    c.L[d] = L[d];
+    c.K[d] = K[d];
+  }
+  c.h[0] = Tab{h1_re, h1_im, h1_rows, h1_cols};
+  c.h[1] = Tab{h2_re, h2_im, h2_rows, h2_cols};
+  c.h[2] = Tab{h3_re, h3_im, h3_rows, h3_cols};
+  if (!h1_re || !tab_len_ok(c.h[0], c.J[0], c.L[0])) return mex_fail(c, "h1 size problem");
+  if (!h2_re || !tab_len_ok(c.h[1], c.J[1], c.L[1])) return mex_fail(c, "h2 size problem");
+  if (!h3_re || !tab_len_ok(c.h[2], c.J[2], c.L[2])) return mex_fail(c, "h3 size problem");
+  if (fm_rows != tm_rows || tm_cols != 3) return mex_fail(c, "t_m must be Mx3 matrix");
+  c.M = fm_rows;
+  c.N = (int)fm_cols;
+  c.order = order ? order[0] : 0;
+  int rc = mex_check_tables(c, flips, flips_numel);
+  if (rc) return rc;
+  c.tm = tm;
+  c.in_re = fm_re;
+  c.in_im = fm_im;
+  c.out_re = ck_re;
+  c.out_im = ck_im;
+  return mex_run(c);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// NUFFT
+// ---------------------------------------------------------------------------
+struct mirt_nufft {
+  mirt_interp_plan *ip = nullptr;
+  GlueGeom gg{};
+  int C = 0, nslice = 0;
+  long long Mtot = 0;
+  DMem sn, grid, hx, hX;
+  cufftHandle fft = 0;
+  bool fft_ok = false;
+  ~mirt_nufft() {
+    if (fft_ok) cufftDestroy(fft);
+    delete ip;
+  }
+};
+
+namespace {
+
+#define CF(call)                                                                   \
+  do {                                                                             \
+    cufftResult r_ = (call);                                                       \
+    if (r_ != CUFFT_SUCCESS)                                                       \
+      return fail(MIRT_ERR_FFT, std::string(#call) + " failed: " + std::to_string((int)r_)); \
+  } while (0)
+
+int nufft_fft(mirt_nufft *p, int dir, cudaStream_t st) {
+  CF(cufftSetStream(p->fft, st));
+  const long long per = p->gg.ngrid * p->C;
+  for (int s = 0; s < p->nslice; s++) {
+    cufftComplex *g = reinterpret_cast<cufftComplex *>(p->grid.as<float2>() + s * per);
+    CF(cufftExecC2C(p->fft, g, g, dir));
+  }
+  return MIRT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mirt_minmax_kb_table(int32_t N, int32_t J, int32_t K, int32_t L, double *h_re, double *h_im) {
+  if (N < 1 || J < 1 || K < 1 || L < 1) return fail(MIRT_ERR_ARG, "N, J, K, L must be positive");
+  std::vector<std::complex<double>> h;
+  if (!minmax_kb_table(N, J, K, L, h)) return fail(MIRT_ERR_ARG, "singular min-max system");
+  for (size_t i = 0; i < h.size(); i++) {
+    h_re[i] = h[i].real();
+    h_im[i] = h[i].imag();
+  }
+  return MIRT_OK;
+}
+
+int mirt_minmax_kb_scale(int32_t N, int32_t J, int32_t K, double *sn_re, double *sn_im) {
+  if (N < 1 || J < 1 || K < 1) return fail(MIRT_ERR_ARG, "N, J, K must be positive");
+  std::vector<double> alpha;
+  double beta;
+  alpha_kb_fit(N, J, K, alpha, beta);
+  std::vector<std::complex<double>> s = scale1(N, K, alpha, beta);
+  for (int i = 0; i < N; i++) {
+    sn_re[i] = s[i].real();
+    sn_im[i] = s[i].imag();
+  }
+  return MIRT_OK;
+}
+
+int mirt_nufft_create(mirt_nufft **out, int32_t D, const int32_t *Nd, const int32_t *Kd,
+                      const int32_t *Jd, const int32_t *Ld, const double *n_shift,
+                      const double *om, int64_t Mtot, const int64_t *slice_moff, int32_t nslice,
+                      int32_t ncol, void *stream) {
+  if (!out) return fail(MIRT_ERR_ARG, "output pointer is NULL");
+  *out = nullptr;
+  int rc = device_ok();
+  if (rc) return rc;
+  if (nslice < 1) return fail(MIRT_ERR_ARG, "nslice must be >= 1");
+  rc = validate_geometry(D, Kd, Jd, Ld, 0, true, Mtot, ncol);
+  if (rc) return rc;
+  for (int d = 0; d < D; d++)
+    if (Nd[d] < 1 || Nd[d] > Kd[d]) return fail(MIRT_ERR_ARG, "need 1 <= N <= K per dimension");
+  std::vector<long long> moff(nslice + 1);
+  if (slice_moff) {
+    for (int s = 0; s <= nslice; s++) moff[s] = slice_moff[s];
+    if (moff[0] != 0 || moff[nslice] != Mtot)
+      return fail(MIRT_ERR_ARG, "slice offsets must start at 0 and end at Mtot");
+    for (int s = 0; s < nslice; s++)
+      if (moff[s + 1] < moff[s]) return fail(MIRT_ERR_ARG, "slice offsets must not decrease");
+  } else {
+    if (nslice != 1) return fail(MIRT_ERR_ARG, "slice offsets required for nslice > 1");
+    moff[0] = 0;
+    moff[1] = Mtot;
+  }
+  cudaStream_t st = as_stream(stream);
+  auto *p = new mirt_nufft();
+  p->C = ncol;
+  p->nslice = nslice;
+  p->Mtot = Mtot;
+  p->gg.D = D;
+  p->gg.npix = 1;
+  p->gg.ngrid = 1;
+  for (int d = 0; d < 3; d++) {
+    p->gg.N[d] = d < D ? Nd[d] : 1;
+    p->gg.K[d] = d < D ? Kd[d] : 1;
+    p->gg.npix *= p->gg.N[d];
+    p->gg.ngrid *= p->gg.K[d];
+  }
+  auto bail = [&](int code) {
+    delete p;
+    return code;
+  };
+  // tables (FP64 host), scaling factors as the outer product of conj(1D factors)
+  std::vector<std::vector<double>> hre(D), him(D);
+  std::vector<std::complex<double>> sn(1, 1.0);
+  for (int d = 0; d < D; d++) {
+    std::vector<std::complex<double>> h;
+    if (!minmax_kb_table(Nd[d], Jd[d], Kd[d], Ld[d], h))
+      return bail(fail(MIRT_ERR_ARG, "singular min-max system"));
+    hre[d].resize(h.size());
+    him[d].resize(h.size());
+    for (size_t i = 0; i < h.size(); i++) {
+      hre[d][i] = h[i].real();
+      him[d][i] = h[i].imag();
+    }
+    std::vector<double> alpha;
+    double beta;
+    alpha_kb_fit(Nd[d], Jd[d], Kd[d], alpha, beta);
+    std::vector<std::complex<double>> s1 = scale1(Nd[d], Kd[d], alpha, beta);
+    std::vector<std::complex<double>> nsn(sn.size() * Nd[d]);
+    for (int n = 0; n < Nd[d]; n++)
+      for (size_t i = 0; i < sn.size(); i++) nsn[i + sn.size() * n] = sn[i] * std::conj(s1[n]);
+    sn.swap(nsn);
+  }
+  const double *hr[MIRT_DMAX] = {nullptr, nullptr, nullptr};
+  const double *hi[MIRT_DMAX] = {nullptr, nullptr, nullptr};
+  for (int d = 0; d < D; d++) {
+    hr[d] = hre[d].data();
+    hi[d] = him[d].data();
+  }
+  p->ip = new mirt_interp_plan();
+  mirt_interp_plan *P = p->ip;
+  rc = plan_geometry(P, D, Kd, Jd, Ld, hr, hi, 0, ncol, st);
+  if (rc) return bail(rc);
+  {
+    std::vector<float2> snf(sn.size());
+    for (size_t i = 0; i < sn.size(); i++)
+      snf[i] = make_float2((float)sn[i].real(), (float)sn[i].imag());
+    cudaError_t e = p->sn.alloc(snf.size() * sizeof(float2));
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(p->sn.p, snf.data(), snf.size() * sizeof(float2),
+                          cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return bail(fail(MIRT_ERR_CUDA, cudaGetErrorString(e)));
+  }
+  // om -> tm (FP64, om / (2 pi / K)) and the n_shift phase on the device
+  bool any_shift = false;
+  double gam[3] = {1, 1, 1}, ns[3] = {0, 0, 0};
+  for (int d = 0; d < D; d++) {
+    gam[d] = 2 * M_PI / Kd[d];
+    ns[d] = n_shift ? n_shift[d] : 0.0;
+    if (ns[d] != 0) any_shift = true;
+  }
+  {
+    DMem om_d, par;
+    cudaError_t e = om_d.alloc(std::max<long long>(Mtot, 1) * D * sizeof(double));
+    if (e == cudaSuccess) e = par.alloc(6 * sizeof(double));
+    if (e == cudaSuccess) e = P->tm.alloc(std::max<long long>(Mtot, 1) * D * sizeof(double));
+    if (e == cudaSuccess && any_shift) e = P->phase.alloc(std::max<long long>(Mtot, 1) * sizeof(float2));
+    double hp[6] = {gam[0], gam[1], gam[2], ns[0], ns[1], ns[2]};
+    if (e == cudaSuccess && Mtot)
+      e = cudaMemcpyAsync(om_d.p, om, Mtot * D * sizeof(double), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(par.p, hp, sizeof hp, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+      e = launch_om_to_tm(om_d.as<double>(), Mtot, D, par.as<double>(), par.as<double>() + 3,
+                          any_shift ? 1 : 0, P->tm.as<double>(), P->phase.as<float2>(), st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return bail(fail(MIRT_ERR_CUDA, cudaGetErrorString(e)));
+    P->a.phase = any_shift ? P->phase.as<float2>() : nullptr;
+  }
+  rc = plan_finish(P, Mtot, moff.data(), nslice, st);
+  if (rc) return bail(rc);
+  {
+    cudaError_t e = p->grid.alloc((size_t)nslice * p->gg.ngrid * ncol * sizeof(float2));
+    if (e != cudaSuccess) return bail(fail(MIRT_ERR_ALLOC, "NUFFT grid buffer"));
+  }
+  int n[3];
+  for (int d = 0; d < D; d++) n[d] = Kd[D - 1 - d];
+  if (ncol > 0) {
+    cufftResult r = cufftPlanMany(&p->fft, D, n, n, ncol, 1, n, ncol, 1, CUFFT_C2C, ncol);
+    if (r != CUFFT_SUCCESS)
+      return bail(fail(MIRT_ERR_FFT, "cufftPlanMany failed: " + std::to_string((int)r)));
+    p->fft_ok = true;
+  }
+  {
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return bail(fail(MIRT_ERR_CUDA, cudaGetErrorString(e)));
+  }
+  *out = p;
+  return MIRT_OK;
+}
+
+int mirt_nufft_forward(mirt_nufft *p, const void *x, void *X, void *stream) {
+  if (!p) return fail(MIRT_ERR_ARG, "nufft is NULL");
+  if (p->C == 0) return MIRT_OK;
+  cudaStream_t st = as_stream(stream);
+  CK(launch_deapod_pad(static_cast<const float2 *>(x), p->sn.as<float2>(), p->grid.as<float2>(),
+                       p->gg, p->C, p->nslice, st));
+  int rc = nufft_fft(p, CUFFT_FORWARD, st);
+  if (rc) return rc;
+  CK(launch_gather(p->ip->a, p->ip->lg, p->grid.as<float2>(), static_cast<float2 *>(X), st));
+  return MIRT_OK;
+}
+
+int mirt_nufft_adjoint(mirt_nufft *p, const void *X, void *x, void *stream) {
+  if (!p) return fail(MIRT_ERR_ARG, "nufft is NULL");
+  if (p->C == 0) return MIRT_OK;
+  cudaStream_t st = as_stream(stream);
+  mirt_interp_plan *P = p->ip;
+  CK(launch_spread(P->a, P->t, P->ls, P->bin_start.as<int>(), static_cast<const float2 *>(X),
+                   p->grid.as<float2>(), st));
+  int rc = nufft_fft(p, CUFFT_INVERSE, st);
+  if (rc) return rc;
+  CK(launch_crop_deapod(p->grid.as<float2>(), p->sn.as<float2>(), static_cast<float2 *>(x), p->gg,
+                        p->C, p->nslice, st));
+  return MIRT_OK;
+}
+
+int mirt_nufft_forward_host(mirt_nufft *p, const float *x, float *X, void *stream) {
+  if (!p) return fail(MIRT_ERR_ARG, "nufft is NULL");
+  cudaStream_t st = as_stream(stream);
+  const size_t bx = (size_t)p->nslice * p->gg.npix * p->C * sizeof(float2);
+  const size_t bX = (size_t)p->Mtot * p->C * sizeof(float2);
+  if (p->hx.bytes < bx) CK(p->hx.alloc(bx));
+  if (p->hX.bytes < bX) CK(p->hX.alloc(bX));
+  CK(cudaMemcpyAsync(p->hx.p, x, bx, cudaMemcpyHostToDevice, st));
+  int rc = mirt_nufft_forward(p, p->hx.p, p->hX.p, stream);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(X, p->hX.p, bX, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return MIRT_OK;
+}
+
+int mirt_nufft_adjoint_host(mirt_nufft *p, const float *X, float *x, void *stream) {
+  if (!p) return fail(MIRT_ERR_ARG, "nufft is NULL");
+  cudaStream_t st = as_stream(stream);
+  const size_t bx = (size_t)p->nslice * p->gg.npix * p->C * sizeof(float2);
+  const size_t bX = (size_t)p->Mtot * p->C * sizeof(float2);
+  if (p->hx.bytes < bx) CK(p->hx.alloc(bx));
+  if (p->hX.bytes < bX) CK(p->hX.alloc(bX));
+  CK(cudaMemcpyAsync(p->hX.p, X, bX, cudaMemcpyHostToDevice, st));
+  int rc = mirt_nufft_adjoint(p, p->hX.p, p->hx.p, stream);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(x, p->hx.p, bx, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return MIRT_OK;
+}
+
+mirt_interp_plan *mirt_nufft_interp_plan(mirt_nufft *p) { return p ? p->ip : nullptr; }
+
+int mirt_nufft_destroy(mirt_nufft *p) {
+  if (p) {
+    cudaDeviceSynchronize();
+    delete p;
+  }
+  return MIRT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,214 @@
+// glue.cu -- elementwise kernels around the interpolation and the FFT.
+//
+//   deapod_pad   x .* sn, zero-padded at the end of every dimension to Kd
+//                (nufft/nufft.m:139-140, nufft/fftn_fast.m:22-26)
+//   crop_deapod  crop [Kd] -> [Nd] and multiply by conj(sn)
+//                (nufft/nufft_adj.m:63-80)
+//   om_to_tm     tm = om / (2 pi / K) in FP64 and the n_shift phase
+//                exp(i om . n_shift) (nufft/nufft_table_interp.m:36-40,
+//                nufft/nufft_table_init.m:48-50)
+//   split <-> interleaved conversions for the FP64 split-complex mex layout
+//                (column n of [*, N] <-> innermost column of the device layout)
+#include "glue.cuh"
+
+namespace mirt {
+
+__global__ void deapod_pad_kernel(const float2 *__restrict__ x, const float2 *__restrict__ sn,
+                                  float2 *__restrict__ grid, GlueGeom g, int C, int nslice) {
+  const long long total = g.ngrid * C;
+  const long long per = total;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < per * nslice;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long s = i / per;
+    const long long r = i - s * per;
+    const long long k = r / C;
+    const int c = (int)(r - k * C);
+    long long rem = k;
+    long long n = 0, nstr = 1;
+    bool inside = true;
+    for (int d = 0; d < g.D; d++) {
+      const long long kd = rem % g.K[d];
+      rem /= g.K[d];
+      if (kd >= g.N[d]) inside = false;
+      n += kd * nstr;
+      nstr *= g.N[d];
+    }
+    float2 v = make_float2(0.f, 0.f);
+    if (inside) {
+      const float2 a = x[(s * g.npix + n) * C + c];
+      const float2 b = sn[n];
+      v = make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+    }
+    grid[i] = v;
+  }
+}
+
+__global__ void crop_deapod_kernel(const float2 *__restrict__ grid, const float2 *__restrict__ sn,
+                                   float2 *__restrict__ x, GlueGeom g, int C, int nslice) {
+  const long long per = g.npix * C;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < per * nslice;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long s = i / per;
+    const long long r = i - s * per;
+    const long long n = r / C;
+    const int c = (int)(r - n * C);
+    long long rem = n, k = 0, kstr = 1;
+    for (int d = 0; d < g.D; d++) {
+      const long long nd = rem % g.N[d];
+      rem /= g.N[d];
+      k += nd * kstr;
+      kstr *= g.K[d];
+    }
+    const float2 a = grid[(s * g.ngrid + k) * C + c];
+    const float2 b = sn[n];
+    // a * conj(b)
+    x[i] = make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+  }
+}
+
+__global__ void om_to_tm_kernel(const double *__restrict__ om, long long M, int D,
+                                const double *gam, const double *n_shift, int want_phase,
+                                double *__restrict__ tm, float2 *__restrict__ phase) {
+  const long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (m >= M) return;
+  double arg = 0.0;
+  for (int d = 0; d < D; d++) {
+    const double o = om[d * M + m];
+    tm[d * M + m] = o / gam[d];
+    arg += o * n_shift[d];
+  }
+  if (want_phase) {
+    double s, c;
+    sincos(arg, &s, &c);
+    phase[m] = make_float2((float)c, (float)s);
+  }
+}
+
+// split FP64 [npts, N] (column n contiguous) -> float2 [npts][N]
+__global__ void split_to_il_kernel(const double *__restrict__ re, const double *__restrict__ im,
+                                   long long npts, int N, float2 *__restrict__ out) {
+  __shared__ float2 tile[32][33];
+  const long long p0 = (long long)blockIdx.x * 32;
+  const int n0 = blockIdx.y * 32;
+  const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
+  for (int r = ty; r < 32; r += 8) {
+    const long long p = p0 + tx;
+    const int n = n0 + r;
+    if (p < npts && n < N) {
+      const long long idx = (long long)n * npts + p;
+      tile[r][tx] = make_float2((float)re[idx], im ? (float)im[idx] : 0.f);
+    }
+  }
+  __syncthreads();
+  for (int r = ty; r < 32; r += 8) {
+    const long long p = p0 + r;
+    const int n = n0 + tx;
+    if (p < npts && n < N) out[p * N + n] = tile[tx][r];
+  }
+}
+
+// float2 [npts][N] -> split FP64 [npts, N]
+__global__ void il_to_split_kernel(const float2 *__restrict__ in, long long npts, int N,
+                                   double *__restrict__ re, double *__restrict__ im) {
+  __shared__ float2 tile[32][33];
+  const long long p0 = (long long)blockIdx.x * 32;
+  const int n0 = blockIdx.y * 32;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  for (int r = ty; r < 32; r += 8) {
+    const long long p = p0 + r;
+    const int n = n0 + tx;
+    if (p < npts && n < N) tile[r][tx] = in[p * N + n];
+  }
+  __syncthreads();
+  for (int r = ty; r < 32; r += 8) {
+    const long long p = p0 + tx;
+    const int n = n0 + r;
+    if (p < npts && n < N) {
+      const long long idx = (long long)n * npts + p;
+      const float2 v = tile[tx][r];
+      re[idx] = (double)v.x;
+      im[idx] = (double)v.y;
+    }
+  }
+}
+
+__global__ void tab_to_f32_kernel(const double *__restrict__ re, const double *__restrict__ im,
+                                  int n, void *__restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (im)
+    static_cast<float2 *>(out)[i] = make_float2((float)re[i], (float)im[i]);
+  else
+    static_cast<float *>(out)[i] = (float)re[i];
+}
+
+__global__ void fill_slice_kernel(const long long *moff, int nslice, int *slice_id) {
+  const int s = blockIdx.y;
+  if (s >= nslice) return;
+  const long long beg = moff[s], end = moff[s + 1];
+  for (long long m = beg + blockIdx.x * (long long)blockDim.x + threadIdx.x; m < end;
+       m += (long long)gridDim.x * blockDim.x)
+    slice_id[m] = s;
+}
+
+static unsigned grid_for(long long n, int thr, int maxb = 148 * 32) {
+  long long b = (n + thr - 1) / thr;
+  if (b > maxb) b = maxb;
+  if (b < 1) b = 1;
+  return (unsigned)b;
+}
+
+cudaError_t launch_deapod_pad(const float2 *x, const float2 *sn, float2 *grid, const GlueGeom &g,
+                              int C, int nslice, cudaStream_t st) {
+  const long long n = g.ngrid * C * nslice;
+  deapod_pad_kernel<<<grid_for(n, 256), 256, 0, st>>>(x, sn, grid, g, C, nslice);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_crop_deapod(const float2 *grid, const float2 *sn, float2 *x, const GlueGeom &g,
+                               int C, int nslice, cudaStream_t st) {
+  const long long n = g.npix * C * nslice;
+  crop_deapod_kernel<<<grid_for(n, 256), 256, 0, st>>>(grid, sn, x, g, C, nslice);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_om_to_tm(const double *om, long long M, int D, const double *gam_dev,
+                            const double *nshift_dev, int want_phase, double *tm, float2 *phase,
+                            cudaStream_t st) {
+  if (M == 0) return cudaSuccess;
+  om_to_tm_kernel<<<(unsigned)((M + 255) / 256), 256, 0, st>>>(om, M, D, gam_dev, nshift_dev,
+                                                              want_phase, tm, phase);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_split_to_il(const double *re, const double *im, long long npts, int N,
+                               float2 *out, cudaStream_t st) {
+  if (npts == 0 || N == 0) return cudaSuccess;
+  dim3 grid((unsigned)((npts + 31) / 32), (unsigned)((N + 31) / 32));
+  split_to_il_kernel<<<grid, dim3(32, 8), 0, st>>>(re, im, npts, N, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_il_to_split(const float2 *in, long long npts, int N, double *re, double *im,
+                               cudaStream_t st) {
+  if (npts == 0 || N == 0) return cudaSuccess;
+  dim3 grid((unsigned)((npts + 31) / 32), (unsigned)((N + 31) / 32));
+  il_to_split_kernel<<<grid, dim3(32, 8), 0, st>>>(in, npts, N, re, im);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_tab_to_f32(const double *re, const double *im, int n, void *out,
+                              cudaStream_t st) {
+  tab_to_f32_kernel<<<(n + 255) / 256, 256, 0, st>>>(re, im, n, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fill_slice(const long long *moff_dev, int nslice, long long Mtot, int *slice_id,
+                              cudaStream_t st) {
+  if (Mtot == 0) return cudaSuccess;
+  dim3 grid(64, (unsigned)nslice);
+  fill_slice_kernel<<<grid, 256, 0, st>>>(moff_dev, nslice, slice_id);
+  return cudaGetLastError();
+}
+
+}  // namespace mirt

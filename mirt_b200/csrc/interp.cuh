@@ -1,0 +1,74 @@
+// interp.cuh -- host-side interface of the table-interpolation kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "common.cuh"
+
+namespace mirt {
+
+// Everything the gather / spread kernels need about one batch of samples.
+// A batch is nslice independent trajectories ("slices") sharing K, J, L,
+// tables and column count C.  Slice s owns grid block s (prod(K)*C points)
+// and samples [moff[s], moff[s+1]) of the concatenated coordinate array.
+struct InterpArgs {
+  Geom g;
+  int real_tab;          // 1: real tables (order 0 or 1); 0: complex tables
+  int order;             // 0 or 1 (1 only with real tables)
+  int C;                 // columns (coils) per slice
+  long long Mtot;        // samples over all slices
+  const double *tm;      // [D][Mtot] FP64 coordinates t = om / (2 pi / K)
+  const int *slice_id;   // [Mtot] slice of each sample, or nullptr (all 0)
+  const int *perm;       // [Mtot] processing order (sorted), or nullptr
+  const void *tab[MIRT_DMAX];  // device tables: float2 (complex) or float (real)
+  const float2 *phase;   // [Mtot] per-sample phase (nullptr = none)
+  long long grid_elems;  // prod(K) * C  (one slice's grid, in float2)
+};
+
+// Tiling of the grid used by the bin sort and the spread.
+struct Tiling {
+  int T[MIRT_DMAX];      // tile extent per dimension
+  int nb[MIRT_DMAX];     // tiles per dimension
+  int ntiles;            // prod(nb)
+  int nslice;
+  // source-bin lists per dimension: for tile index b of dimension d,
+  // src[d][b*MIRT_SRCMAX + i], i < nsrc[d][b], are the tiles whose samples
+  // (binned by their first tap) can reach tile b.
+  const int *src[MIRT_DMAX];
+  const int *nsrc[MIRT_DMAX];
+};
+#define MIRT_SRCMAX 8
+
+// Launch tuning chosen by the host (autotuned per geometry).
+struct Launch {
+  int threads;   // CTA size
+  int cw;        // lanes per sample group (= coils handled in parallel)
+  int sb;        // samples per staged batch
+  int grid;      // CTAs for the gather (persistent)
+  int P[MIRT_DMAX];  // spread: owner groups per dimension (prod * cw = threads)
+  int tab_smem;  // 1: stage tables in shared memory
+};
+
+// Compute the sort key of every sample: slice * ntiles + tile of its first tap.
+cudaError_t launch_bin_keys(const InterpArgs &a, const Tiling &t, uint32_t *keys,
+                            cudaStream_t st);
+
+// Stable LSD radix sort of (keys, 0..n-1) by key; writes the permutation
+// (sorted position -> sample) and bin_start[nbins+1].  tmp must hold
+// radix_sort_tmp_bytes(n) bytes.
+size_t radix_sort_tmp_bytes(long long n);
+cudaError_t radix_sort_bins(const uint32_t *keys, long long n, int nbins, void *tmp,
+                            int *perm, int *bin_start, cudaStream_t st);
+
+// Size the persistent gather grid (l.grid) from the kernel's occupancy.
+cudaError_t query_gather_grid(const InterpArgs &a, Launch &l);
+
+// fm[m][c] = sum_taps h * ck   for every sample (forward gather)
+cudaError_t launch_gather(const InterpArgs &a, const Launch &l, const float2 *ck,
+                          float2 *fm, cudaStream_t st);
+
+// ck = adjoint of the gather; deterministic owner-computes spread over tiles
+cudaError_t launch_spread(const InterpArgs &a, const Tiling &t, const Launch &l,
+                          const int *bin_start, const float2 *fm, float2 *ck,
+                          cudaStream_t st);
+
+}  // namespace mirt

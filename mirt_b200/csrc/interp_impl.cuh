@@ -1,0 +1,523 @@
+// interp_impl.cuh -- device templates of the gather and spread kernels and
+// the launch dispatch, included by one translation unit per dimension
+// (interp_d1.cu, interp_d2.cu, interp_d3.cu) so that they compile in parallel.
+//
+// Forward gather replaces nufft/table/interp{1,2,3}_table1_for.c; the
+// adjoint spread replaces nufft/table/interp{1,2,3}_table1_adj.c.
+// Table-entry selection and grid wrap are FP64, exactly as the reference
+// (common.cuh); taps are accumulated in FP32.
+//
+// Both kernels stage, per CTA, a batch of `sb` samples: one thread per
+// (sample, dimension, tap) computes the table coefficient and the wrapped grid
+// coordinate once, so that the FP64 index arithmetic is not repeated by every
+// coil lane.  Coil lanes then run the taps with coalesced column accesses.
+#pragma once
+#include "interp.cuh"
+
+namespace mirt {
+namespace detail {
+
+// ------------------------------------------------------------------------
+// shared-memory staging
+// ------------------------------------------------------------------------
+struct Stage {
+  float2 *W;   // [sb][SJ] tap coefficients (real tables: .y = 0)
+  int *KI;     // [sb][SJ] wrapped grid coordinate of each tap
+  int *mid;    // [sb] sample index
+  int *sid;    // [sb] slice index
+};
+
+// Copy the D tables into shared memory when requested; returns pointers to use.
+template <bool REAL>
+__device__ void stage_tables(const InterpArgs &a, int use_smem, unsigned char *buf,
+                             const void *tp[MIRT_DMAX]) {
+  size_t off = 0;
+  for (int d = 0; d < a.g.D; d++) {
+    if (!use_smem) {
+      tp[d] = a.tab[d];
+      continue;
+    }
+    if (REAL) {
+      float *dst = reinterpret_cast<float *>(buf + off);
+      const float *src = static_cast<const float *>(a.tab[d]);
+      for (int i = threadIdx.x; i < a.g.tlen[d]; i += blockDim.x) dst[i] = src[i];
+      tp[d] = dst;
+      off += ((size_t)a.g.tlen[d] * 4 + 15) & ~(size_t)15;
+    } else {
+      float2 *dst = reinterpret_cast<float2 *>(buf + off);
+      const float2 *src = static_cast<const float2 *>(a.tab[d]);
+      for (int i = threadIdx.x; i < a.g.tlen[d]; i += blockDim.x) dst[i] = src[i];
+      tp[d] = dst;
+      off += ((size_t)a.g.tlen[d] * 8 + 15) & ~(size_t)15;
+    }
+  }
+  __syncthreads();
+}
+
+// Coefficient of tap (d, k) for coordinate t: the reference's 0th-order
+// lookup or 1st-order linear interpolation of the table.  The index is
+// clamped into the table, which changes nothing for |t - k| <= J/2.
+template <bool REAL>
+__device__ __forceinline__ float2 tap_coef(const InterpArgs &a, const void *const tp[MIRT_DMAX],
+                                           int d, double t, int k) {
+  const int L = a.g.L[d];
+  const int nc = a.g.ncenter[d];
+  const int tl = a.g.tlen[d];
+  if (REAL) {
+    const float *h = static_cast<const float *>(tp[d]);
+    if (a.order == 0) {
+      int n = nc + tab0_index(t, k, L);
+      n = min(max(n, 0), tl - 1);
+      return make_float2(h[n], 0.f);
+    }
+    float alf;
+    int n = nc + tab1_index(t, k, L, &alf);
+    n = min(max(n, 0), tl - 1);
+    const float h0 = h[n];
+    // the reference reads one entry past the table end here, times alf = 0
+    const float h1 = (n + 1 < tl) ? h[n + 1] : 0.f;
+    return make_float2((1.f - alf) * h0 + alf * h1, 0.f);
+  } else {
+    const float2 *h = static_cast<const float2 *>(tp[d]);
+    int n = nc + tab0_index(t, k, L);
+    n = min(max(n, 0), tl - 1);
+    return h[n];
+  }
+}
+
+// Fill the stage for samples at sorted positions [pos0, pos0 + nb).
+template <bool REAL>
+__device__ void stage_batch(const InterpArgs &a, const void *const tp[MIRT_DMAX], const Stage &s,
+                            long long pos0, int nb, int SJ) {
+  const int D = a.g.D;
+  for (int e = threadIdx.x; e < nb * SJ; e += blockDim.x) {
+    const int sl = e / SJ;
+    const int r = e - sl * SJ;
+    int d = 0;
+    int j = r;
+    while (d + 1 < D && j >= a.g.J[d]) {
+      j -= a.g.J[d];
+      d++;
+    }
+    const long long pos = pos0 + sl;
+    const int m = a.perm ? a.perm[pos] : (int)pos;
+    const double t = a.tm[(long long)d * a.Mtot + m];
+    const int k = koff_of(t, a.g.J[d]) + j;
+    s.W[e] = tap_coef<REAL>(a, tp, d, t, k);
+    s.KI[e] = wrapk(k, a.g.K[d]);
+    if (r == 0) {
+      s.mid[sl] = m;
+      s.sid[sl] = a.slice_id ? a.slice_id[m] : 0;
+    }
+  }
+}
+
+template <bool REAL>
+__device__ __forceinline__ void mac(float2 &acc, float2 w, float2 v) {
+  if (REAL) {
+    acc.x = fmaf(w.x, v.x, acc.x);
+    acc.y = fmaf(w.x, v.y, acc.y);
+  } else {
+    acc.x += w.x * v.x - w.y * v.y;
+    acc.y += w.x * v.y + w.y * v.x;
+  }
+}
+
+// conj(w) * v
+template <bool REAL>
+__device__ __forceinline__ float2 cw_mul(float2 w, float2 v) {
+  if (REAL) return make_float2(w.x * v.x, w.x * v.y);
+  return cmulc(w, v);
+}
+
+__host__ __device__ inline size_t table_smem_bytes(const InterpArgs &a) {
+  size_t b = 0;
+  for (int d = 0; d < a.g.D; d++)
+    b += ((size_t)a.g.tlen[d] * (a.real_tab ? 4 : 8) + 15) & ~(size_t)15;
+  return b;
+}
+
+// ------------------------------------------------------------------------
+// forward gather
+// ------------------------------------------------------------------------
+// Persistent CTAs walk batches of the bin-sorted samples.  A group of CW
+// lanes serves one sample at a time; lane li handles columns li, li+CW, ...
+// and reads each tap as one coalesced column segment of the grid.
+template <int D, int CW, int JT, bool REAL>
+__global__ void __launch_bounds__(256) gather_kernel(InterpArgs a, Launch l,
+                                                     const float2 *__restrict__ ck,
+                                                     float2 *__restrict__ fm) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const Geom &g = a.g;
+  const size_t tab_bytes = l.tab_smem ? table_smem_bytes(a) : 0;
+  const void *tp[MIRT_DMAX];
+  stage_tables<REAL>(a, l.tab_smem, smem, tp);
+
+  int Jd[MIRT_DMAX] = {1, 1, 1};
+#pragma unroll
+  for (int d = 0; d < D; d++) Jd[d] = JT > 0 ? JT : g.J[d];
+  const int SJ = Jd[0] + (D > 1 ? Jd[1] : 0) + (D > 2 ? Jd[2] : 0);
+  const int sb = l.sb;
+  Stage s;
+  s.W = reinterpret_cast<float2 *>(smem + tab_bytes);
+  s.KI = reinterpret_cast<int *>(s.W + sb * SJ);
+  s.mid = s.KI + sb * SJ;
+  s.sid = s.mid + sb;
+
+  const int ngroups = blockDim.x / CW;
+  const int grp = threadIdx.x / CW;
+  const int li = threadIdx.x % CW;
+  const int C = a.C;
+  int ostr[MIRT_DMAX] = {0, 0, 0};
+#pragma unroll
+  for (int d = 0; d < D; d++) ostr[d] = (int)(g.kstride[d] * C);
+
+  const long long nbatch = (a.Mtot + sb - 1) / sb;
+  for (long long bi = blockIdx.x; bi < nbatch; bi += gridDim.x) {
+    const long long pos0 = bi * sb;
+    const int nb = (int)min((long long)sb, a.Mtot - pos0);
+    stage_batch<REAL>(a, tp, s, pos0, nb, SJ);
+    __syncthreads();
+    for (int sl = grp; sl < nb; sl += ngroups) {
+      const int m = s.mid[sl];
+      const float2 *gb = ck + (long long)s.sid[sl] * a.grid_elems;
+      const float2 ph = a.phase ? a.phase[m] : make_float2(1.f, 0.f);
+      const float2 *Ws = s.W + sl * SJ;
+      const int *Ks = s.KI + sl * SJ;
+      if constexpr (JT > 0) {
+        // fixed J: tap coefficients and offsets in registers, taps unrolled
+        float2 w[D][JT];
+        int o[D][JT];
+#pragma unroll
+        for (int d = 0; d < D; d++)
+#pragma unroll
+          for (int j = 0; j < JT; j++) {
+            w[d][j] = Ws[d * JT + j];
+            o[d][j] = Ks[d * JT + j] * ostr[d];
+          }
+        for (int c = li; c < C; c += CW) {
+          const float2 *gc = gb + c;
+          float2 acc = make_float2(0.f, 0.f);
+          if constexpr (D == 1) {
+#pragma unroll
+            for (int j1 = 0; j1 < JT; j1++) mac<REAL>(acc, w[0][j1], __ldg(gc + o[0][j1]));
+          } else if constexpr (D == 2) {
+#pragma unroll
+            for (int j2 = 0; j2 < JT; j2++) {
+              float2 s1 = make_float2(0.f, 0.f);
+              const float2 *row = gc + o[1][j2];
+#pragma unroll
+              for (int j1 = 0; j1 < JT; j1++) mac<REAL>(s1, w[0][j1], __ldg(row + o[0][j1]));
+              mac<false>(acc, w[1][j2], s1);
+            }
+          } else {
+#pragma unroll
+            for (int j3 = 0; j3 < JT; j3++) {
+              float2 s2 = make_float2(0.f, 0.f);
+              const float2 *pl = gc + o[2][j3];
+#pragma unroll
+              for (int j2 = 0; j2 < JT; j2++) {
+                float2 s1 = make_float2(0.f, 0.f);
+                const float2 *row = pl + o[1][j2];
+#pragma unroll
+                for (int j1 = 0; j1 < JT; j1++) mac<REAL>(s1, w[0][j1], __ldg(row + o[0][j1]));
+                mac<false>(s2, w[1][j2], s1);
+              }
+              mac<false>(acc, w[2][j3], s2);
+            }
+          }
+          if (a.phase) acc = cmul(acc, ph);
+          fm[(long long)m * C + c] = acc;
+        }
+      } else {
+        // any J: coefficients read from shared memory, runtime loops
+        for (int c = li; c < C; c += CW) {
+          const float2 *gc = gb + c;
+          float2 acc = make_float2(0.f, 0.f);
+          if constexpr (D == 1) {
+            for (int j1 = 0; j1 < Jd[0]; j1++)
+              mac<REAL>(acc, Ws[j1], __ldg(gc + Ks[j1] * ostr[0]));
+          } else if constexpr (D == 2) {
+            for (int j2 = 0; j2 < Jd[1]; j2++) {
+              float2 s1 = make_float2(0.f, 0.f);
+              const float2 *row = gc + Ks[Jd[0] + j2] * ostr[1];
+              for (int j1 = 0; j1 < Jd[0]; j1++)
+                mac<REAL>(s1, Ws[j1], __ldg(row + Ks[j1] * ostr[0]));
+              mac<false>(acc, Ws[Jd[0] + j2], s1);
+            }
+          } else {
+            for (int j3 = 0; j3 < Jd[2]; j3++) {
+              float2 s2 = make_float2(0.f, 0.f);
+              const float2 *pl = gc + Ks[Jd[0] + Jd[1] + j3] * ostr[2];
+              for (int j2 = 0; j2 < Jd[1]; j2++) {
+                float2 s1 = make_float2(0.f, 0.f);
+                const float2 *row = pl + Ks[Jd[0] + j2] * ostr[1];
+                for (int j1 = 0; j1 < Jd[0]; j1++)
+                  mac<REAL>(s1, Ws[j1], __ldg(row + Ks[j1] * ostr[0]));
+                mac<false>(s2, Ws[Jd[0] + j2], s1);
+              }
+              mac<false>(acc, Ws[Jd[0] + Jd[1] + j3], s2);
+            }
+          }
+          if (a.phase) acc = cmul(acc, ph);
+          fm[(long long)m * C + c] = acc;
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------------------
+// adjoint spread: owner-computes over grid tiles, deterministic
+// ------------------------------------------------------------------------
+// CTA (tile, slice, coil chunk) accumulates its tile in shared memory.  Thread
+// (group, lane) owns coil c0 + lane of every tile point whose local
+// coordinates are congruent to the group's (g1, g2, g3) modulo (P1, P2, P3),
+// so each accumulator has one writer.  All groups walk the same samples (the
+// tile's source bins in fixed order, samples in stable bin-sorted order), so
+// the summation order at every grid point is fixed: no atomics, bitwise
+// reproducible.  The tile is written once; there is no halo merge pass,
+// because the samples of neighbouring bins are read instead.
+template <int D, int CW, int JT, bool REAL>
+__global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t, Launch l,
+                                                     const int *__restrict__ bin_start,
+                                                     const float2 *__restrict__ fm,
+                                                     float2 *__restrict__ ck) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const Geom &g = a.g;
+  const size_t tab_bytes = l.tab_smem ? table_smem_bytes(a) : 0;
+  const void *tp[MIRT_DMAX];
+  stage_tables<REAL>(a, l.tab_smem, smem, tp);
+
+  int npts = 1;
+#pragma unroll
+  for (int d = 0; d < D; d++) npts *= t.T[d];
+  float2 *acc = reinterpret_cast<float2 *>(smem + tab_bytes);
+  int Jd[MIRT_DMAX] = {1, 1, 1};
+#pragma unroll
+  for (int d = 0; d < D; d++) Jd[d] = JT > 0 ? JT : g.J[d];
+  const int SJ = Jd[0] + (D > 1 ? Jd[1] : 0) + (D > 2 ? Jd[2] : 0);
+  const int sb = l.sb;
+  Stage s;
+  s.W = acc + (size_t)npts * CW;
+  s.KI = reinterpret_cast<int *>(s.W + sb * SJ);
+  s.mid = s.KI + sb * SJ;
+  s.sid = s.mid + sb;
+  // [sb][CW] sample values; sb is even, so this stays 8-byte aligned
+  float2 *F = reinterpret_cast<float2 *>(s.sid + sb);
+
+  const int tile = blockIdx.x % t.ntiles;
+  const int slice = blockIdx.x / t.ntiles;
+  const int c0 = blockIdx.y * CW;
+  int b[MIRT_DMAX] = {0, 0, 0}, lo[MIRT_DMAX] = {0, 0, 0}, ext[MIRT_DMAX] = {1, 1, 1};
+  {
+    int r = tile;
+#pragma unroll
+    for (int d = 0; d < D; d++) {
+      b[d] = r % t.nb[d];
+      r /= t.nb[d];
+      lo[d] = b[d] * t.T[d];
+      ext[d] = min(t.T[d], g.K[d] - lo[d]);
+    }
+  }
+  const int grp = threadIdx.x / CW;
+  const int li = threadIdx.x % CW;
+  int gq[MIRT_DMAX] = {0, 0, 0};
+  {
+    int r = grp;
+#pragma unroll
+    for (int d = 0; d < D; d++) {
+      gq[d] = r % l.P[d];
+      r /= l.P[d];
+    }
+  }
+  for (int e = threadIdx.x; e < npts * CW; e += blockDim.x) acc[e] = make_float2(0.f, 0.f);
+
+  int ns[MIRT_DMAX] = {1, 1, 1};
+#pragma unroll
+  for (int d = 0; d < D; d++) ns[d] = t.nsrc[d][b[d]];
+  const int nsrc_tot = ns[0] * ns[1] * ns[2];
+  const int C = a.C;
+  const int T0 = t.T[0];
+  const int T1 = D > 1 ? t.T[1] : 1;
+
+  for (int si = 0; si < nsrc_tot; si++) {
+    int r = si, stile = 0, mul = 1;
+#pragma unroll
+    for (int d = 0; d < D; d++) {
+      const int i = r % ns[d];
+      r /= ns[d];
+      stile += t.src[d][b[d] * MIRT_SRCMAX + i] * mul;
+      mul *= t.nb[d];
+    }
+    const int bin = slice * t.ntiles + stile;
+    const long long beg = bin_start[bin], end = bin_start[bin + 1];
+    for (long long pos0 = beg; pos0 < end; pos0 += sb) {
+      const int nb = (int)min((long long)sb, end - pos0);
+      __syncthreads();
+      stage_batch<REAL>(a, tp, s, pos0, nb, SJ);
+      for (int e = threadIdx.x; e < nb * CW; e += blockDim.x) {
+        const int sl = e / CW, cc = e - sl * CW;
+        const int m = a.perm ? a.perm[pos0 + sl] : (int)(pos0 + sl);
+        float2 f = make_float2(0.f, 0.f);
+        if (c0 + cc < C) {
+          f = fm[(long long)m * C + c0 + cc];
+          if (a.phase) f = cmulc(a.phase[m], f);
+        }
+        F[e] = f;
+      }
+      __syncthreads();
+      for (int sl = 0; sl < nb; sl++) {
+        const float2 *Ws = s.W + sl * SJ;
+        const int *Ks = s.KI + sl * SJ;
+        const float2 f = F[sl * CW + li];
+#pragma unroll 1
+        for (int j1 = 0; j1 < Jd[0]; j1++) {
+          const int l1 = Ks[j1] - lo[0];
+          if ((unsigned)l1 >= (unsigned)ext[0] || (l1 % l.P[0]) != gq[0]) continue;
+          const float2 w1 = Ws[j1];
+          if constexpr (D == 1) {
+            const float2 v = cw_mul<REAL>(w1, f);
+            float2 &A = acc[(size_t)l1 * CW + li];
+            A.x += v.x;
+            A.y += v.y;
+          } else {
+#pragma unroll 1
+            for (int j2 = 0; j2 < Jd[1]; j2++) {
+              const int l2 = Ks[Jd[0] + j2] - lo[1];
+              if ((unsigned)l2 >= (unsigned)ext[1] || (l2 % l.P[1]) != gq[1]) continue;
+              const float2 w2 = Ws[Jd[0] + j2];
+              if constexpr (D == 2) {
+                const float2 v = cw_mul<REAL>(w1, cw_mul<REAL>(w2, f));
+                float2 &A = acc[((size_t)l2 * T0 + l1) * CW + li];
+                A.x += v.x;
+                A.y += v.y;
+              } else {
+#pragma unroll 1
+                for (int j3 = 0; j3 < Jd[2]; j3++) {
+                  const int l3 = Ks[Jd[0] + Jd[1] + j3] - lo[2];
+                  if ((unsigned)l3 >= (unsigned)ext[2] || (l3 % l.P[2]) != gq[2]) continue;
+                  const float2 w3 = Ws[Jd[0] + Jd[1] + j3];
+                  const float2 v = cw_mul<REAL>(w1, cw_mul<REAL>(w2, cw_mul<REAL>(w3, f)));
+                  float2 &A = acc[(((size_t)l3 * T1 + l2) * T0 + l1) * CW + li];
+                  A.x += v.x;
+                  A.y += v.y;
+                }
+              }
+            }
+          }
+        }
+      }
+    }
+  }
+  __syncthreads();
+  float2 *gout = ck + (long long)slice * a.grid_elems;
+  for (int e = threadIdx.x; e < npts * CW; e += blockDim.x) {
+    const int pt = e / CW, cc = e - pt * CW;
+    const int l1 = pt % T0;
+    const int l2 = D > 1 ? (pt / T0) % T1 : 0;
+    const int l3 = D > 2 ? pt / (T0 * T1) : 0;
+    if (l1 >= ext[0] || l2 >= ext[1] || l3 >= ext[2] || c0 + cc >= C) continue;
+    long long kk = lo[0] + l1;
+    if (D > 1) kk += (long long)(lo[1] + l2) * g.kstride[1];
+    if (D > 2) kk += (long long)(lo[2] + l3) * g.kstride[2];
+    gout[kk * C + c0 + cc] = acc[e];
+  }
+}
+
+// ------------------------------------------------------------------------
+// launch dispatch
+// ------------------------------------------------------------------------
+enum What { GATHER = 0, GATHER_GRID = 1, SPREAD = 2 };
+
+struct Req {
+  What what;
+  const InterpArgs *a;
+  const Tiling *t;
+  Launch *l;
+  const int *bin_start;
+  const float2 *in;
+  float2 *out;
+  cudaStream_t st;
+};
+
+inline size_t stage_bytes(const InterpArgs &a, int sb) {
+  int SJ = 0;
+  for (int d = 0; d < a.g.D; d++) SJ += a.g.J[d];
+  return (size_t)sb * SJ * (8 + 4) + (size_t)sb * 8 + 16;
+}
+
+template <int D, int CW, int JT, bool REAL>
+cudaError_t run(Req &r) {
+  const InterpArgs &a = *r.a;
+  Launch &l = *r.l;
+  if (r.what == GATHER || r.what == GATHER_GRID) {
+    const size_t sm = (l.tab_smem ? table_smem_bytes(a) : 0) + stage_bytes(a, l.sb);
+    auto kern = gather_kernel<D, CW, JT, REAL>;
+    cudaError_t e =
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    if (r.what == GATHER_GRID || l.grid <= 0) {
+      int per_sm = 0, dev = 0, nsm = 0;
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, l.threads, sm);
+      if (e != cudaSuccess) return e;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+      const long long nbatch = (a.Mtot + l.sb - 1) / l.sb;
+      long long gsz = (long long)nsm * (per_sm > 0 ? per_sm : 1);
+      if (gsz > nbatch) gsz = nbatch;
+      l.grid = (int)(gsz > 0 ? gsz : 1);
+      if (r.what == GATHER_GRID) return cudaSuccess;
+    }
+    kern<<<l.grid, l.threads, sm, r.st>>>(a, l, r.in, r.out);
+    return cudaGetLastError();
+  }
+  const Tiling &t = *r.t;
+  int npts = 1;
+  for (int d = 0; d < D; d++) npts *= t.T[d];
+  const size_t sm = (l.tab_smem ? table_smem_bytes(a) : 0) + (size_t)npts * CW * 8 +
+                    stage_bytes(a, l.sb) + (size_t)l.sb * CW * 8 + 16;
+  auto kern = spread_kernel<D, CW, JT, REAL>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return e;
+  dim3 grid((unsigned)(t.ntiles * t.nslice), (unsigned)((a.C + CW - 1) / CW));
+  kern<<<grid, l.threads, sm, r.st>>>(a, t, l, r.bin_start, r.in, r.out);
+  return cudaGetLastError();
+}
+
+template <int D, int CW, int JT>
+cudaError_t by_real(Req &r) {
+  return r.a->real_tab ? run<D, CW, JT, true>(r) : run<D, CW, JT, false>(r);
+}
+
+inline bool all_j(const Geom &g, int j) {
+  for (int d = 0; d < g.D; d++)
+    if (g.J[d] != j) return false;
+  return true;
+}
+
+template <int D, int CW>
+cudaError_t by_j(Req &r) {
+  if (all_j(r.a->g, 6)) return by_real<D, CW, 6>(r);
+  return by_real<D, CW, 0>(r);
+}
+
+template <int D>
+cudaError_t by_cw(Req &r) {
+  switch (r.l->cw) {
+    case 1: return by_j<D, 1>(r);
+    case 4: return by_j<D, 4>(r);
+    case 8: return by_j<D, 8>(r);
+    case 32: return by_j<D, 32>(r);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+// one per dimension, each in its own translation unit
+cudaError_t dispatch_d1(Req &r);
+cudaError_t dispatch_d2(Req &r);
+cudaError_t dispatch_d3(Req &r);
+
+}  // namespace detail
+}  // namespace mirt

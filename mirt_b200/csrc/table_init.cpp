@@ -1,0 +1,238 @@
+// table_init.cpp -- host FP64 construction of the min-max:KB interpolation
+// tables and scaling factors, as st = nufft_init(om, Nd, Jd, Kd, n_shift,
+// 'table', Ld, 'minmax:kb') builds them.
+//
+// Reference lines followed:
+//   alpha/beta fit     nufft/nufft_alpha_kb_fit.m:13-54
+//   KB FT              nufft/kaiser_bessel_ft.m:70-73 (kb_m = 0, d = 1)
+//   KB shape           nufft/kaiser_bessel.m:119-140, nufft/param-data/kaiser,m=0.mat
+//   scaling factors    nufft/nufft_scale.m:54-75, outer product nufft/nufft_init.m:214-232
+//   T, r, offset       nufft/private/nufft_T.m:45-75, nufft_r.m:32-50, nufft_offset.m:18-19
+//   sinc "diric"       nufft/nufft_diric.m:38-40, nufft/nufft_sinc.m
+//   1D table           nufft/nufft_table_init.m:111-134 with nufft/nufft_init.m:234-263,287-288
+//
+// MATLAB built-ins are replaced: mldivide by a Householder QR least-squares
+// solve, inv by Gauss-Jordan with partial pivoting, besseli(0, .) by its power
+// series, and besselj(1/2, z) / z^(1/2) by the closed form sqrt(2/pi) sin(z)/z.
+#include <cmath>
+#include <complex>
+#include <cstdint>
+#include <cstdio>
+#include <vector>
+
+namespace mirt {
+
+using cd = std::complex<double>;
+
+namespace {
+
+// abest.zn of nufft/param-data/kaiser,m=0.mat for J = 2..16 (alpha = J * zn
+// at K/N = 2).  Data that must match the reference's file for sn parity.
+const double kKbZn[15] = {2.5, 2.27, 2.31, 2.34, 2.32, 2.32, 2.35, 2.34,
+                          2.34, 2.35, 2.34, 2.35, 2.35, 2.35, 2.33};
+
+double kb_alpha_best(int J, double K_N) {
+  if (K_N != 2.0) return 2.34 * J;
+  int idx = J - 2;
+  if (idx < 0) idx = 0;
+  if (idx > 14) idx = 14;
+  return J * kKbZn[idx];
+}
+
+// I0(x) by its power series sum (x^2/4)^k / (k!)^2
+double bessel_i0(double x) {
+  const double q = x * x / 4.0;
+  double term = 1.0, sum = 1.0;
+  for (int k = 1; k < 500; k++) {
+    term *= q / ((double)k * (double)k);
+    sum += term;
+    if (term < sum * 1e-17) break;
+  }
+  return sum;
+}
+
+// FT of the KB function with kb_m = 0, d = 1:
+//   (2 pi)^(1/2) (J/2) / I0(alpha) * J_{1/2}(z) / z^(1/2),  z = sqrt((pi J u)^2 - alpha^2)
+// and J_{1/2}(z)/z^(1/2) = sqrt(2/pi) sin(z)/z (sinh for imaginary z).
+double kb_ft(double u, int J, double alpha) {
+  const double a = 2 * M_PI * (J / 2.0) * u;
+  const double z2 = a * a - alpha * alpha;
+  double s;
+  if (z2 > 0) {
+    const double z = std::sqrt(z2);
+    s = std::sin(z) / z;
+  } else if (z2 < 0) {
+    const double y = std::sqrt(-z2);
+    s = std::sinh(y) / y;
+  } else {
+    s = 1.0;
+  }
+  return std::sqrt(2 * M_PI) * (J / 2.0) / bessel_i0(alpha) * std::sqrt(2 / M_PI) * s;
+}
+
+// least squares min ||X c - y|| for X [n x p] column-major by Householder QR
+std::vector<double> lstsq(std::vector<double> X, int n, int p, std::vector<double> y) {
+  for (int k = 0; k < p; k++) {
+    double nrm = 0;
+    for (int i = k; i < n; i++) nrm += X[i + k * n] * X[i + k * n];
+    nrm = std::sqrt(nrm);
+    if (nrm == 0) continue;
+    const double alpha = X[k + k * n] > 0 ? -nrm : nrm;
+    std::vector<double> v(n, 0.0);
+    for (int i = k; i < n; i++) v[i] = X[i + k * n];
+    v[k] -= alpha;
+    double vn = 0;
+    for (int i = k; i < n; i++) vn += v[i] * v[i];
+    if (vn == 0) continue;
+    for (int j = k; j < p; j++) {
+      double dot = 0;
+      for (int i = k; i < n; i++) dot += v[i] * X[i + j * n];
+      const double f = 2 * dot / vn;
+      for (int i = k; i < n; i++) X[i + j * n] -= f * v[i];
+    }
+    double dot = 0;
+    for (int i = k; i < n; i++) dot += v[i] * y[i];
+    const double f = 2 * dot / vn;
+    for (int i = k; i < n; i++) y[i] -= f * v[i];
+  }
+  std::vector<double> c(p, 0.0);
+  for (int k = p - 1; k >= 0; k--) {
+    double s = y[k];
+    for (int j = k + 1; j < p; j++) s -= X[k + j * n] * c[j];
+    c[k] = X[k + k * n] != 0 ? s / X[k + k * n] : 0.0;
+  }
+  return c;
+}
+
+// in-place inverse of a J x J real matrix (row-major), Gauss-Jordan with pivoting
+bool invert(std::vector<double> &A, int J) {
+  std::vector<double> I(J * J, 0.0);
+  for (int i = 0; i < J; i++) I[i * J + i] = 1;
+  for (int c = 0; c < J; c++) {
+    int piv = c;
+    for (int r = c + 1; r < J; r++)
+      if (std::fabs(A[r * J + c]) > std::fabs(A[piv * J + c])) piv = r;
+    if (A[piv * J + c] == 0) return false;
+    if (piv != c)
+      for (int k = 0; k < J; k++) {
+        std::swap(A[c * J + k], A[piv * J + k]);
+        std::swap(I[c * J + k], I[piv * J + k]);
+      }
+    const double d = A[c * J + c];
+    for (int k = 0; k < J; k++) {
+      A[c * J + k] /= d;
+      I[c * J + k] /= d;
+    }
+    for (int r = 0; r < J; r++) {
+      if (r == c) continue;
+      const double f = A[r * J + c];
+      if (f == 0) continue;
+      for (int k = 0; k < J; k++) {
+        A[r * J + k] -= f * A[c * J + k];
+        I[r * J + k] -= f * I[c * J + k];
+      }
+    }
+  }
+  A = I;
+  return true;
+}
+
+double nufft_sinc(double x) {
+  if (x == 0) return 1.0;
+  return std::sin(M_PI * x) / (M_PI * x);
+}
+
+double diric(double k, int N, int K) { return nufft_sinc(k / ((double)K / (double)N)); }
+
+}  // namespace
+
+// alphas (L+1 real coefficients) and beta of nufft_alpha_kb_fit(N, J, K)
+void alpha_kb_fit(int N, int J, int K, std::vector<double> &alphas, double &beta) {
+  beta = 1.0;
+  const double Nmid = (N - 1) / 2.0;
+  const int L = N > 40 ? 13 : (int)std::ceil(N / 3.0);
+  double kb_a = kb_alpha_best(J, (double)K / (double)N);
+  // kaiser_bessel_ft('inline', ...) prints alpha with %g into its kernel string
+  char buf[64];
+  std::snprintf(buf, sizeof buf, "%g", kb_a);
+  kb_a = std::atof(buf);
+  std::vector<double> sn_kaiser(N), X((size_t)N * (L + 1));
+  const double gam = 2 * M_PI / K;
+  for (int i = 0; i < N; i++) {
+    const double nl = i - Nmid;
+    sn_kaiser[i] = 1.0 / kb_ft(nl / K, J, kb_a);
+    for (int l = 0; l <= L; l++) X[i + (size_t)l * N] = std::cos((beta * gam * nl) * (double)l);
+  }
+  std::vector<double> coef = lstsq(X, N, L + 1, sn_kaiser);
+  alphas.assign(L + 1, 0.0);
+  alphas[0] = coef[0];
+  for (int l = 1; l <= L; l++) alphas[l] = coef[l] / 2;
+}
+
+// 1D scaling factors nufft_scale1(N, K, alpha, beta, (N-1)/2)
+std::vector<cd> scale1(int N, int K, const std::vector<double> &alpha, double beta) {
+  const int L = (int)alpha.size() - 1;
+  const double Nmid = (N - 1) / 2.0;
+  std::vector<cd> sn(N, cd(0, 0));
+  for (int n = 0; n < N; n++) {
+    const double g = (2 * M_PI / K) * (n - Nmid) * beta;
+    cd s(0, 0);
+    for (int l1 = -L; l1 <= L; l1++) {
+      const double alf = alpha[std::abs(l1)];  // real alpha: conj is a no-op
+      s += alf * std::exp(cd(0, g * l1));
+    }
+    sn[n] = s;
+  }
+  return sn;
+}
+
+// Complex min-max:KB table for one dimension, length J*L+1.
+bool minmax_kb_table(int N, int J, int K, int L, std::vector<cd> &h) {
+  std::vector<double> alpha;
+  double beta;
+  alpha_kb_fit(N, J, K, alpha, beta);
+  const int La = (int)alpha.size() - 1;
+  // T = inv(C'SS'C)   (tol = 0 in nufft_init)
+  std::vector<double> T(J * J, 0.0);
+  for (int a = 0; a < J; a++)
+    for (int b = 0; b < J; b++) {
+      double s = 0;
+      for (int l1 = -La; l1 <= La; l1++)
+        for (int l2 = -La; l2 <= La; l2++) {
+          const double tmp = (double)(b - a) + beta * (double)(l1 - l2);
+          s += alpha[std::abs(l1)] * alpha[std::abs(l2)] * diric(tmp, N, K);
+        }
+      T[a * J + b] = s;
+    }
+  if (!invert(T, J)) return false;
+  const double gam = 2 * M_PI / K;
+  std::vector<cd> p((size_t)L * J, cd(0, 0));  // used columns 0..J-1 of p [L, K]
+  std::vector<double> r(J), arg(J);
+  for (int l = 0; l < L; l++) {
+    const double t1 = (J / 2.0 - 1) + (double)l / L;
+    const double om = t1 * 2 * M_PI / K;
+    const double koff = std::floor(om / gam - J / 2.0);
+    const double dk = om / gam - koff;
+    for (int j = 0; j < J; j++) {
+      arg[j] = -(double)(j + 1) + dk;
+      double s = 0;
+      for (int l1 = -La; l1 <= La; l1++) s += alpha[std::abs(l1)] * diric(arg[j] + l1 * beta, N, K);
+      r[j] = s;
+    }
+    for (int j = 0; j < J; j++) {
+      double c = 0;
+      for (int i = 0; i < J; i++) c += T[j * J + i] * r[i];
+      const cd ud = std::exp(cd(0, gam * (N - 1) / 2 * arg[j])) * c;
+      long long col = (long long)(koff + (j + 1));
+      col = ((col % K) + K) % K;
+      if (col < J) p[(size_t)l + (size_t)col * L] += std::conj(ud);
+    }
+  }
+  h.assign((size_t)J * L + 1, cd(0, 0));
+  for (int jj = J - 1, blk = 0; jj >= 0; jj--, blk++)
+    for (int l = 0; l < L; l++) h[(size_t)blk * L + l] = p[(size_t)l + (size_t)jj * L];
+  h[(size_t)J * L] = 0;
+  return true;
+}
+
+}  // namespace mirt

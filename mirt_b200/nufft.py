@@ -1,0 +1,274 @@
+"""Device-resident interpolation plans and the table NUFFT, over torch tensors.
+
+The MATLAB-style entry points mirror the reference's NUFFT interface:
+
+    st = nufft_init(om, Nd, Jd, Kd, n_shift, 'table', Ld, 'minmax:kb')
+    X  = nufft(x, st)        # nufft/nufft.m:128-165
+    x  = nufft_adj(X, st)    # nufft/nufft_adj.m:32-80
+
+with numpy inputs and outputs in MATLAB index order (x[n1, n2, (n3), coil]).
+``NufftPlan`` and ``InterpPlan`` are the device-resident forms used by the
+solvers and the benchmark: complex64 torch tensors on the GPU with the coil
+index innermost.  torch provides device memory and streams only; all compute
+runs in libmirt_b200.so.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._lib import check, load
+
+_dp = C.POINTER(C.c_double)
+_fp = C.POINTER(C.c_float)
+_i32p = C.POINTER(C.c_int32)
+_i64p = C.POINTER(C.c_int64)
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _stream_ptr(stream=None):
+    torch = _torch()
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return C.c_void_p(s.cuda_stream)
+
+
+def _i32(v):
+    return np.ascontiguousarray(np.asarray(v, dtype=np.int32).ravel())
+
+
+def _moff(slice_moff, Mtot):
+    if slice_moff is None:
+        return None, 1
+    mo = np.ascontiguousarray(np.asarray(slice_moff, dtype=np.int64))
+    if mo[0] != 0 or mo[-1] != Mtot:
+        raise ValueError("slice offsets must start at 0 and end at Mtot")
+    return mo, len(mo) - 1
+
+
+def minmax_kb_table(N: int, J: int, K: int, L: int) -> np.ndarray:
+    """Complex min-max:KB table st.h{d} (length J*L+1) built by the library in FP64."""
+    n = J * L + 1
+    re, im = np.zeros(n), np.zeros(n)
+    check(load().mirt_minmax_kb_table(N, J, K, L, re.ctypes.data_as(_dp), im.ctypes.data_as(_dp)))
+    return re + 1j * im
+
+
+def minmax_kb_scale(N: int, J: int, K: int) -> np.ndarray:
+    """1D scaling factors nufft_scale(N, K, alpha, beta) with the min-max:KB fit."""
+    re, im = np.zeros(N), np.zeros(N)
+    check(load().mirt_minmax_kb_scale(N, J, K, re.ctypes.data_as(_dp), im.ctypes.data_as(_dp)))
+    return re + 1j * im
+
+
+class InterpPlan:
+    """Plan of the table gather / spread for fixed tables and trajectory.
+
+    tm: [Mtot, D] float64 (t = omega / (2 pi / K)); tables: list of D arrays
+    (complex128 or float64).  Device tensors: grid [nslice, K_D, ..., K_1, ncol]
+    and samples [Mtot, ncol], complex64, contiguous.
+    """
+
+    def __init__(self, K, J, L, tables, tm, ncol, order=0, slice_moff=None, phase=None,
+                 stream=None):
+        torch = _torch()
+        self.lib = load()
+        tm = np.asarray(tm, dtype=np.float64)
+        if tm.ndim == 1:
+            tm = tm[:, None]
+        self.D = tm.shape[1]
+        self.K, self.J, self.L = _i32(K), _i32(J), _i32(L)
+        self.Mtot = tm.shape[0]
+        self.ncol = int(ncol)
+        mo, self.nslice = _moff(slice_moff, self.Mtot)
+        is_cx = any(np.iscomplexobj(h) for h in tables)
+        self._keep = []
+        hr = (_dp * 3)()
+        hi = (_dp * 3)() if is_cx else None
+        for d, h in enumerate(tables):
+            r = np.ascontiguousarray(np.real(h), dtype=np.float64)
+            self._keep.append(r)
+            hr[d] = r.ctypes.data_as(_dp)
+            if is_cx:
+                i = np.ascontiguousarray(np.imag(h), dtype=np.float64)
+                self._keep.append(i)
+                hi[d] = i.ctypes.data_as(_dp)
+        tmf = np.ascontiguousarray(tm.ravel(order="F"))
+        pr = pi = None
+        if phase is not None:
+            phase = np.asarray(phase, dtype=np.complex128)
+            pr = np.ascontiguousarray(phase.real)
+            pi = np.ascontiguousarray(phase.imag)
+        h = C.c_void_p()
+        check(self.lib.mirt_interp_plan_create(
+            C.byref(h), self.D, self.K.ctypes.data_as(_i32p), self.J.ctypes.data_as(_i32p),
+            self.L.ctypes.data_as(_i32p), hr, hi, int(order), tmf.ctypes.data_as(_dp),
+            self.Mtot, None if mo is None else mo.ctypes.data_as(_i64p), self.nslice,
+            self.ncol, None if pr is None else pr.ctypes.data_as(_dp),
+            None if pi is None else pi.ctypes.data_as(_dp), _stream_ptr(stream)))
+        self.handle = h
+        self._keep = []
+        self.grid_shape = (self.nslice,) + tuple(int(k) for k in self.K[::-1]) + (self.ncol,)
+        self.sample_shape = (self.Mtot, self.ncol)
+        self.device = torch.device("cuda", torch.cuda.current_device())
+
+    def forward(self, ck, out=None, stream=None):
+        torch = _torch()
+        if out is None:
+            out = torch.empty(self.sample_shape, dtype=torch.complex64, device=ck.device)
+        assert ck.is_contiguous() and ck.dtype == torch.complex64
+        check(self.lib.mirt_interp_plan_forward(self.handle, C.c_void_p(ck.data_ptr()),
+                                                C.c_void_p(out.data_ptr()), _stream_ptr(stream)))
+        return out
+
+    def adjoint(self, fm, out=None, stream=None):
+        torch = _torch()
+        if out is None:
+            out = torch.empty(self.grid_shape, dtype=torch.complex64, device=fm.device)
+        assert fm.is_contiguous() and fm.dtype == torch.complex64
+        check(self.lib.mirt_interp_plan_adjoint(self.handle, C.c_void_p(fm.data_ptr()),
+                                                C.c_void_p(out.data_ptr()), _stream_ptr(stream)))
+        return out
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.mirt_interp_plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class NufftPlan:
+    """Table NUFFT with min-max:KB tables built in FP64 by the library.
+
+    om: [Mtot, D] radians; Nd, Jd, Kd, Ld per dimension; n_shift (default 0).
+    Device tensors: image [nslice, N_D, ..., N_1, ncol], samples [Mtot, ncol].
+    """
+
+    def __init__(self, om, Nd, Jd, Kd, n_shift=None, Ld=1024, ncol=1, slice_moff=None,
+                 stream=None):
+        torch = _torch()
+        self.lib = load()
+        om = np.asarray(om, dtype=np.float64)
+        if om.ndim == 1:
+            om = om[:, None]
+        self.D = om.shape[1]
+        D = self.D
+        self.Nd, self.Jd, self.Kd = _i32(Nd), _i32(Jd), _i32(Kd)
+        self.Ld = _i32(Ld if np.ndim(Ld) else [Ld] * D)
+        self.n_shift = np.ascontiguousarray(
+            np.zeros(D) if n_shift is None else np.asarray(n_shift, dtype=np.float64).ravel())
+        self.Mtot = om.shape[0]
+        self.ncol = int(ncol)
+        mo, self.nslice = _moff(slice_moff, self.Mtot)
+        omf = np.ascontiguousarray(om.ravel(order="F"))
+        h = C.c_void_p()
+        check(self.lib.mirt_nufft_create(
+            C.byref(h), D, self.Nd.ctypes.data_as(_i32p), self.Kd.ctypes.data_as(_i32p),
+            self.Jd.ctypes.data_as(_i32p), self.Ld.ctypes.data_as(_i32p),
+            self.n_shift.ctypes.data_as(_dp), omf.ctypes.data_as(_dp), self.Mtot,
+            None if mo is None else mo.ctypes.data_as(_i64p), self.nslice, self.ncol,
+            _stream_ptr(stream)))
+        self.handle = h
+        self.image_shape = (self.nslice,) + tuple(int(n) for n in self.Nd[::-1]) + (self.ncol,)
+        self.sample_shape = (self.Mtot, self.ncol)
+
+    def forward(self, x, out=None, stream=None):
+        torch = _torch()
+        if out is None:
+            out = torch.empty(self.sample_shape, dtype=torch.complex64, device=x.device)
+        assert x.is_contiguous() and x.dtype == torch.complex64
+        check(self.lib.mirt_nufft_forward(self.handle, C.c_void_p(x.data_ptr()),
+                                          C.c_void_p(out.data_ptr()), _stream_ptr(stream)))
+        return out
+
+    def adjoint(self, X, out=None, stream=None):
+        torch = _torch()
+        if out is None:
+            out = torch.empty(self.image_shape, dtype=torch.complex64, device=X.device)
+        assert X.is_contiguous() and X.dtype == torch.complex64
+        check(self.lib.mirt_nufft_adjoint(self.handle, C.c_void_p(X.data_ptr()),
+                                          C.c_void_p(out.data_ptr()), _stream_ptr(stream)))
+        return out
+
+    def forward_host(self, x: np.ndarray, out: np.ndarray | None = None, stream=None):
+        """host complex64 image (device layout) -> host complex64 samples."""
+        x = np.ascontiguousarray(x, dtype=np.complex64)
+        if out is None:
+            out = np.empty(self.sample_shape, dtype=np.complex64)
+        check(self.lib.mirt_nufft_forward_host(self.handle, x.ctypes.data_as(_fp),
+                                               out.ctypes.data_as(_fp), _stream_ptr(stream)))
+        return out
+
+    def adjoint_host(self, X: np.ndarray, out: np.ndarray | None = None, stream=None):
+        X = np.ascontiguousarray(X, dtype=np.complex64)
+        if out is None:
+            out = np.empty(self.image_shape, dtype=np.complex64)
+        check(self.lib.mirt_nufft_adjoint_host(self.handle, X.ctypes.data_as(_fp),
+                                               out.ctypes.data_as(_fp), _stream_ptr(stream)))
+        return out
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.mirt_nufft_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------------------
+# MATLAB-style interface
+# ---------------------------------------------------------------------------
+def nufft_init(om, Nd, Jd, Kd, n_shift=None, *args):
+    """st = nufft_init(om, Nd, Jd, Kd, n_shift, 'table', Ld, 'minmax:kb').
+
+    Only the table mode with the min-max:KB interpolator (the reference's
+    default for 'table', nufft/nufft_init.m:93-95) is provided.
+    """
+    args = list(args)
+    Ld = 1024
+    if args and args[0] == "table":
+        Ld = args[1] if len(args) > 1 else Ld
+        ktype = args[2] if len(args) > 2 else "minmax:kb"
+    else:
+        ktype = args[0] if args else "minmax:kb"
+    if ktype != "minmax:kb":
+        raise ValueError(f"only 'minmax:kb' tables are provided, not {ktype!r}")
+    ncol = 1
+    return NufftPlan(om, Nd, Jd, Kd, n_shift=n_shift, Ld=Ld, ncol=ncol)
+
+
+def _to_device_image(x, D, ncol):
+    torch = _torch()
+    x = np.asarray(x, dtype=np.complex64)
+    if x.ndim == D:
+        x = x[..., None]
+    axes = tuple(range(D - 1, -1, -1)) + (D,)
+    return torch.from_numpy(np.ascontiguousarray(np.transpose(x, axes))[None]).cuda()
+
+
+def nufft(x, st: NufftPlan):
+    """X = nufft(x, st) for a numpy image x[n1, n2, ...] (one column)."""
+    xd = _to_device_image(x, st.D, st.ncol)
+    X = st.forward(xd)
+    return X.cpu().numpy()[:, 0].astype(np.complex128)
+
+
+def nufft_adj(X, st: NufftPlan):
+    """x = nufft_adj(X, st) for numpy samples X[M] (one column)."""
+    torch = _torch()
+    Xd = torch.from_numpy(np.asarray(X, dtype=np.complex64).reshape(-1, 1).copy()).cuda()
+    x = st.adjoint(Xd).cpu().numpy()[0, ..., 0]
+    return np.transpose(x, tuple(range(st.D - 1, -1, -1))).astype(np.complex128)

@@ -1,0 +1,101 @@
+"""Seeded synthetic inputs for the benchmark configurations.
+
+No public dataset is involved: every array here is generated from a seed with
+the shapes and value distributions the configurations name.
+
+* radial trajectories: uniformly spaced spokes, and golden-angle spokes with
+  the angle step pi*(sqrt(5)-1)/2 from pi/2 and readout positions
+  (-(Nro/2-1) .. Nro/2)/Nro in cycles/sample (the sampling of
+  mri/ir_mri_kspace_ga_radial.m:34-53), scaled to radians
+* 3D kooshball: spokes through the centre along directions on a Fibonacci
+  sphere
+* phantoms: random ellipses / ellipsoids with amplitude U[0,1] and phase
+  U[-pi, pi)
+* coil maps: smooth complex Gaussian bumps with seeded centres and widths
+"""
+from __future__ import annotations
+
+import numpy as np
+
+GOLDEN_ANGLE = np.pi * (np.sqrt(5) - 1) / 2
+
+
+def radial(nspoke: int, nread: int) -> np.ndarray:
+    """[nspoke*nread, 2] radians, spokes at angles k*pi/nspoke, readout [-pi, pi)."""
+    r = np.linspace(-np.pi, np.pi, nread, endpoint=False)
+    ang = np.arange(nspoke) * np.pi / nspoke
+    return np.stack([np.outer(np.cos(ang), r).ravel(), np.outer(np.sin(ang), r).ravel()], 1)
+
+
+def ga_radial(nspoke: int, nro: int, start: float = np.pi / 2) -> np.ndarray:
+    """[nro*nspoke, 2] radians, golden-angle spokes, readout fastest."""
+    phi = np.arange(nspoke) * GOLDEN_ANGLE + start
+    rho = np.arange(-(nro // 2 - 1), nro // 2 + 1) / nro
+    kx = np.outer(rho, np.cos(phi))
+    ky = np.outer(rho, np.sin(-phi))
+    return 2 * np.pi * np.stack([kx.ravel(order="F"), ky.ravel(order="F")], 1)
+
+
+def kooshball(nspoke: int, nro: int) -> np.ndarray:
+    """[nspoke*nro, 3] radians: spokes along Fibonacci-sphere directions."""
+    i = np.arange(nspoke) + 0.5
+    z = 1 - 2 * i / nspoke
+    r = np.sqrt(1 - z * z)
+    th = np.pi * (1 + np.sqrt(5)) * i
+    dirs = np.stack([r * np.cos(th), r * np.sin(th), z], 1)
+    rho = np.arange(-(nro // 2 - 1), nro // 2 + 1) / nro * 2 * np.pi
+    return (dirs[:, None, :] * rho[None, :, None]).reshape(-1, 3)
+
+
+def ellipses(N: int, n: int, rng: np.random.Generator) -> np.ndarray:
+    """[N, N] complex image (index [n1, n2]) of n random ellipses."""
+    x, y = np.meshgrid(np.linspace(-1, 1, N), np.linspace(-1, 1, N), indexing="ij")
+    img = np.zeros((N, N), complex)
+    for _ in range(n):
+        cx, cy = rng.uniform(-0.5, 0.5, 2)
+        rx, ry = rng.uniform(0.05, 0.4, 2)
+        th = rng.uniform(0, np.pi)
+        a = rng.uniform(0, 1) * np.exp(1j * rng.uniform(-np.pi, np.pi))
+        xr = (x - cx) * np.cos(th) + (y - cy) * np.sin(th)
+        yr = -(x - cx) * np.sin(th) + (y - cy) * np.cos(th)
+        img[(xr / rx) ** 2 + (yr / ry) ** 2 <= 1] += a
+    return img
+
+
+def ellipsoids(N: int, n: int, rng: np.random.Generator) -> np.ndarray:
+    """[N, N, N] complex volume of n random ellipsoids."""
+    g = np.linspace(-1, 1, N, dtype=np.float32)
+    x, y, z = np.meshgrid(g, g, g, indexing="ij")
+    vol = np.zeros((N, N, N), np.complex64)
+    for _ in range(n):
+        c = rng.uniform(-0.4, 0.4, 3)
+        r = rng.uniform(0.05, 0.35, 3)
+        a = rng.uniform(0, 1) * np.exp(1j * rng.uniform(-np.pi, np.pi))
+        inside = (((x - c[0]) / r[0]) ** 2 + ((y - c[1]) / r[1]) ** 2
+                  + ((z - c[2]) / r[2]) ** 2) <= 1
+        vol[inside] += a
+    return vol
+
+
+def coil_maps(shape, ncoil: int, rng: np.random.Generator) -> np.ndarray:
+    """[*shape, ncoil] smooth complex Gaussian-bump sensitivities."""
+    axes = [np.linspace(-1, 1, n, dtype=np.float32) for n in shape]
+    grids = np.meshgrid(*axes, indexing="ij")
+    maps = np.empty(tuple(shape) + (ncoil,), np.complex64)
+    for c in range(ncoil):
+        ang = 2 * np.pi * c / ncoil
+        centre = [1.2 * np.cos(ang), 1.2 * np.sin(ang)] + [rng.uniform(-0.5, 0.5)] * (len(shape) - 2)
+        width = rng.uniform(0.6, 1.2)
+        d2 = sum((g - c0) ** 2 for g, c0 in zip(grids, centre))
+        phase = rng.uniform(-np.pi, np.pi) + 0.5 * grids[0] * rng.uniform(-1, 1)
+        maps[..., c] = np.exp(-d2 / (2 * width ** 2)) * np.exp(1j * phase)
+    return maps
+
+
+def batch_ga_radial(nslice: int, spoke_lo: int, spoke_hi: int, nro: int,
+                    rng: np.random.Generator):
+    """Uneven golden-angle slices: (om [Mtot, 2], slice offsets [nslice+1], spokes)."""
+    spokes = rng.integers(spoke_lo, spoke_hi + 1, nslice)
+    oms = [ga_radial(int(s), nro, start=np.pi / 2 + rng.uniform(0, np.pi)) for s in spokes]
+    moff = np.concatenate([[0], np.cumsum([len(o) for o in oms])]).astype(np.int64)
+    return np.concatenate(oms), moff, spokes

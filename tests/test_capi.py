@@ -1,0 +1,113 @@
+"""CPU: the C-ABI library loads, exports every declared symbol, builds its
+FP64 tables like the oracle, and rejects bad arguments with the reference
+gateways' messages (no GPU work is started by any of these calls)."""
+from __future__ import annotations
+
+import os
+import re
+
+import numpy as np
+import pytest
+
+import mirt_b200 as mb
+from mirt_b200 import _lib
+from oracle import nufft_ref as nr
+from conftest import ROOT
+
+
+def _declared():
+    src = open(os.path.join(ROOT, "include", "mirt_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(mirt_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_exports_every_declared_symbol():
+    lib = mb.load()
+    names = _declared()
+    assert len(names) >= 20
+    for n in names:
+        assert hasattr(lib, n), n
+    assert set(names) == set(_lib.exported_names())
+
+
+def test_version():
+    assert mb.load().mirt_version() >= 100
+
+
+@pytest.mark.parametrize("N,J,K,L", [(64, 6, 128, 1024), (256, 6, 512, 1024),
+                                     (128, 6, 256, 512), (60, 5, 120, 64), (30, 4, 64, 32)])
+def test_tables_match_oracle(N, J, K, L):
+    h = mb.minmax_kb_table(N, J, K, L)
+    ho = nr.table_1d(N, J, K, L)
+    assert np.abs(h - ho).max() <= 1e-10 * np.abs(ho).max()
+    s = mb.minmax_kb_scale(N, J, K)
+    a, b = nr.nufft_alpha_kb_fit(N, J, K)
+    so = nr.nufft_scale1(N, K, a, b)
+    assert np.abs(s - so).max() <= 1e-12 * np.abs(so).max()
+
+
+def _args2(**kw):
+    a = dict(ck=np.zeros((8, 8), complex), h1=np.zeros(6 * 4 + 1), h2=np.zeros(6 * 4 + 1),
+             J=np.array([6, 6], np.int32), L=np.array([4, 4], np.int32), tm=np.zeros((3, 2)))
+    a.update(kw)
+    return a
+
+
+@pytest.mark.parametrize("kw,msg", [
+    (dict(ck=np.zeros((8, 8))), "interp2_table_mex failed: mxIsComplexDouble"),
+    (dict(J=np.array([6, 6, 6], np.int32)), "interp2_table_mex failed: J must be [1,2]"),
+    (dict(J=np.array([6, 6], np.int64)), "interp2_table_mex failed: J must be [1,2]"),
+    (dict(L=np.array([4], np.int32)), "interp2_table_mex failed: L must be [1,2]"),
+    (dict(h1=np.zeros(6 * 4)), "interp2_table_mex failed: h1 size problem"),
+    (dict(h2=np.zeros((6 * 4 + 1, 2))), "interp2_table_mex failed: h2 size problem"),
+    (dict(tm=np.zeros((3, 3))), "interp2_table_mex failed: tm must have 2 columns"),
+    (dict(h1=np.zeros(25, complex)), "h must be real or complex double (preferably real)"),
+])
+def test_interp2_argument_errors(kw, msg):
+    with pytest.raises(mb.MexError, match=re.escape(msg)):
+        mb.interp2_table_mex(**_args2(**kw))
+
+
+def test_order_and_flip_errors():
+    a = _args2(h1=np.zeros(25, complex), h2=np.zeros(25, complex))
+    with pytest.raises(mb.MexError, match="only 0th order implemented for complex"):
+        mb.interp2_table_mex(**a, order=np.array([1], np.int32))
+    with pytest.raises(mb.MexError, match="bad order"):
+        mb.interp2_table_mex(**_args2(), order=np.array([2], np.int32))
+    with pytest.raises(mb.MexError, match="flip not compiled"):
+        mb.interp2_table_mex(**_args2(), order=np.array([0], np.int32),
+                             flips=np.array([1, 0], np.int32))
+    with pytest.raises(mb.MexError, match=re.escape("order must be scalar int32 (0 | 1)")):
+        mb.interp2_table_mex(**_args2(), order=np.array([0, 1], np.int32))
+
+
+def test_adjoint_and_1d_3d_errors():
+    h = np.zeros(25)
+    J2, L2, K2 = (np.array([6, 6], np.int32), np.array([4, 4], np.int32),
+                  np.array([8, 8], np.int32))
+    with pytest.raises(mb.MexError, match=re.escape("interp2_table_adj_mex() failed: t_m must be Mx2 matrix")):
+        mb.interp2_table_adj_mex(np.zeros((3, 1), complex), h, h, J2, L2, np.zeros((4, 2)), K2)
+    with pytest.raises(mb.MexError, match=re.escape("interp2_table_adj_mex() failed: K must be int32 [1,2]")):
+        mb.interp2_table_adj_mex(np.zeros((3, 1), complex), h, h, J2, L2, np.zeros((3, 2)),
+                                 np.array([8], np.int32))
+    J1, L1 = np.array([6], np.int32), np.array([4], np.int32)
+    with pytest.raises(mb.MexError, match=re.escape("interp1_table_mex() failed: t_m must be col vector.")):
+        mb.interp1_table_mex(np.zeros((8, 1), complex), h, J1, L1, np.zeros((3, 2)))
+    with pytest.raises(mb.MexError, match=re.escape("interp1_table_adj_mex() failed: h must be col vector")):
+        mb.interp1_table_adj_mex(np.zeros((3, 1), complex), np.zeros((25, 2)), J1, L1,
+                                 np.zeros((3, 1)), np.array([8], np.int32))
+    J3, L3 = np.array([6, 6, 6], np.int32), np.array([4, 4, 4], np.int32)
+    with pytest.raises(mb.MexError, match=re.escape("interp3_table_mex failed: h3 size problem")):
+        mb.interp3_table_mex(np.zeros((8, 8, 8), complex), h, h, np.zeros(3), J3, L3,
+                             np.zeros((3, 3)))
+    with pytest.raises(mb.MexError, match=re.escape("interp3_table_adj_mex() failed: L must be int32 [1,3]")):
+        mb.interp3_table_adj_mex(np.zeros((3, 1), complex), h, h, h, J3, L2, np.zeros((3, 3)),
+                                 np.array([8, 8, 8], np.int32))
+
+
+def test_valid_call_without_gpu_fails_loudly():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(mb.MirtError, match="no CUDA device"):
+        mb.interp2_table_mex(**_args2())
