@@ -146,8 +146,9 @@ struct mirt_interp_plan {
 
 namespace {
 
-// Tile extents and launch shapes: heuristics sized for ~64 KB of shared
-// accumulator per spread CTA with the coil lanes innermost.
+// Tile extents and launch shapes.  The spread accumulates a tile of
+// npts points x CW coils in shared memory (~64 KB); its warps own bands of
+// the slowest tiled dimension, so that dimension is a multiple of 8 rows.
 void choose_config(mirt_interp_plan *P) {
   InterpArgs &a = P->a;
   Tiling &t = P->t;
@@ -155,8 +156,6 @@ void choose_config(mirt_interp_plan *P) {
   const int cw = C >= 32 ? 32 : C >= 8 ? 8 : C >= 4 ? 4 : 1;
   const int threads = 256;
   const int ngroups = threads / cw;
-  size_t tabb = 0;
-  for (int d = 0; d < D; d++) tabb += ((size_t)a.g.tlen[d] * (a.real_tab ? 4 : 8) + 15) & ~15ull;
 
   Launch &lg = P->lg;
   lg.threads = threads;
@@ -165,39 +164,26 @@ void choose_config(mirt_interp_plan *P) {
   if (sb < 32) sb = 32;
   if (sb > 256) sb = 256;
   lg.sb = sb;
-  lg.tab_smem = tabb <= 112 * 1024 ? 1 : 0;
+  lg.tab_smem = 0;
   lg.grid = 0;
 
-  const int npts_target = 65536 / (cw * 8);
   int T[MIRT_DMAX] = {1, 1, 1};
   if (D == 1) {
-    T[0] = npts_target;
+    T[0] = 65536 / (cw * 8);
   } else if (D == 2) {
-    int t1 = 1;
-    while (t1 * t1 < npts_target) t1 <<= 1;
-    T[0] = t1;
-    T[1] = npts_target / t1;
+    switch (cw) {
+      case 32: T[0] = 16; T[1] = 16; break;
+      case 8: T[0] = 32; T[1] = 32; break;
+      case 4: T[0] = 32; T[1] = 32; break;
+      default: T[0] = 64; T[1] = 64; break;
+    }
   } else {
-    int t1 = 1;
-    while (t1 * t1 * t1 < npts_target) t1 <<= 1;
-    T[0] = t1;
-    int rest = npts_target / t1;
-    int t2 = 1;
-    while (t2 * t2 < rest) t2 <<= 1;
-    T[1] = t2;
-    T[2] = rest / t2;
-  }
-  int P3[MIRT_DMAX] = {1, 1, 1};
-  if (D == 1) {
-    P3[0] = ngroups;
-  } else if (D == 2) {
-    P3[0] = ngroups < 8 ? ngroups : 8;
-    P3[1] = ngroups / P3[0];
-  } else {
-    P3[0] = ngroups < 4 ? ngroups : 4;
-    const int r = ngroups / P3[0];
-    P3[1] = r < 4 ? r : 4;
-    P3[2] = r / P3[1];
+    switch (cw) {
+      case 32: T[0] = 8; T[1] = 4; T[2] = 8; break;
+      case 8: T[0] = 16; T[1] = 8; T[2] = 8; break;
+      case 4: T[0] = 16; T[1] = 16; T[2] = 8; break;
+      default: T[0] = 32; T[1] = 16; T[2] = 16; break;
+    }
   }
   for (int d = 0; d < D; d++) {
     if (T[d] > a.g.K[d]) T[d] = a.g.K[d];
@@ -207,14 +193,8 @@ void choose_config(mirt_interp_plan *P) {
   ls.threads = threads;
   ls.cw = cw;
   ls.sb = 64;
-  for (int d = 0; d < MIRT_DMAX; d++) ls.P[d] = P3[d];
-  int npts = 1;
-  for (int d = 0; d < D; d++) npts *= T[d];
-  int SJ = 0;
-  for (int d = 0; d < D; d++) SJ += a.g.J[d];
-  const size_t rest = (size_t)npts * cw * 8 + (size_t)ls.sb * SJ * 12 + (size_t)ls.sb * 8 +
-                      (size_t)ls.sb * cw * 8 + 64;
-  ls.tab_smem = (tabb + rest) <= 200 * 1024 ? 1 : 0;
+  ls.tab_smem = 0;
+  for (int d = 0; d < MIRT_DMAX; d++) ls.P[d] = 1;
   for (int d = 0; d < MIRT_DMAX; d++) {
     t.T[d] = d < D ? T[d] : 1;
     t.nb[d] = d < D ? (a.g.K[d] + T[d] - 1) / T[d] : 1;
@@ -353,6 +333,8 @@ int plan_finish(mirt_interp_plan *P, long long Mtot, const long long *moff, int 
   CK(radix_sort_bins(P->keys.as<uint32_t>(), Mtot, (int)nbins, P->sorttmp.p, P->perm.as<int>(),
                      P->bin_start.as<int>(), st));
   a.perm = P->perm.as<int>();
+  // the sort scratch returns to the shared cache: let the sort finish first
+  CK(cudaStreamSynchronize(st));
   P->sorttmp.release();
   CK(query_gather_grid(a, P->lg));
   return MIRT_OK;

@@ -271,29 +271,82 @@ __global__ void __launch_bounds__(256) gather_kernel(InterpArgs a, Launch l,
 // ------------------------------------------------------------------------
 // adjoint spread: owner-computes over grid tiles, deterministic
 // ------------------------------------------------------------------------
-// CTA (tile, slice, coil chunk) accumulates its tile in shared memory.  Thread
-// (group, lane) owns coil c0 + lane of every tile point whose local
-// coordinates are congruent to the group's (g1, g2, g3) modulo (P1, P2, P3),
-// so each accumulator has one writer.  All groups walk the same samples (the
-// tile's source bins in fixed order, samples in stable bin-sorted order), so
-// the summation order at every grid point is fixed: no atomics, bitwise
-// reproducible.  The tile is written once; there is no halo merge pass,
-// because the samples of neighbouring bins are read instead.
+// CTA (tile, slice, coil chunk) accumulates its tile in shared memory and
+// writes it once.  Ownership of the accumulators:
+//   * warp w owns a contiguous band of the tile's slowest tiled dimension
+//     (rows l2 in 2D, planes l3 in 3D, columns l1 in 1D);
+//   * lane (s, c), s < SUB = 32/CW, c < CW, owns coil c0 + c of the columns
+//     l1 = s (mod SUB).
+// Every accumulator therefore has exactly one writer, and every warp walks the
+// tile's samples in the same fixed order (source bins in fixed order, samples
+// in stable bin-sorted order).  The sum at each grid point is formed in a
+// fixed order: no atomics, bitwise reproducible.  A warp skips a sample whose
+// taps miss its band with one warp-uniform test.  There is no halo merge
+// pass: samples of neighbouring bins whose taps reach into the tile are read.
+
+// Mask of taps j < J whose local coordinate lies in [lo_b, hi_b) and, when
+// SUB > 1, is congruent to s modulo SUB.  The taps of a sample are the grid
+// points k0w + j (mod K), which in tile-local coordinates form at most two
+// runs: base + j before the periodic wrap and base - K + j after it.
+template <int SUB>
+__host__ __device__ __forceinline__ unsigned tap_mask(int k0w, int J, int K, int lo_tile, int lo_b,
+                                             int hi_b, int s) {
+  const int base = k0w - lo_tile;
+  const int jw = K - k0w;  // first tap index after the wrap
+  unsigned m = 0;
+  {
+    const int ja = max(0, lo_b - base), jb = min(min(J, jw), hi_b - base);
+    if (jb > ja) m |= ((1u << jb) - 1u) & ~((1u << ja) - 1u);
+  }
+  {
+    const int b2 = base - K;
+    const int ja = max(jw, lo_b - b2), jb = min(J, hi_b - b2);
+    if (jb > ja) m |= ((1u << jb) - 1u) & ~((1u << ja) - 1u);
+  }
+  if (SUB > 1 && m) {
+    // bit j kept iff (base + j) = s (mod SUB); after the wrap base - K + j,
+    // and K need not be a multiple of SUB, so test each run separately
+    unsigned keep = 0;
+    const unsigned all = (J >= 32) ? 0xffffffffu : ((1u << J) - 1u);
+    const unsigned pre = (jw >= 32) ? all : (all & ((1u << max(jw, 0)) - 1u));
+    {
+      const int r = (s - base) & (SUB - 1);
+      unsigned p = 0;
+      for (int j = r; j < 32; j += SUB) p |= 1u << j;
+      keep |= p & pre;
+    }
+    {
+      const int r = (s - (base - K)) & (SUB - 1);
+      unsigned p = 0;
+      for (int j = r; j < 32; j += SUB) p |= 1u << j;
+      keep |= p & ~pre;
+    }
+    m &= keep;
+  }
+  return m;
+}
+
+__host__ __device__ __forceinline__ int tap_local(int k0w, int j, int K, int lo_tile) {
+  int x = k0w + j;
+  if (x >= K) x -= K;
+  return x - lo_tile;
+}
+
 template <int D, int CW, int JT, bool REAL>
 __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t, Launch l,
                                                      const int *__restrict__ bin_start,
                                                      const float2 *__restrict__ fm,
                                                      float2 *__restrict__ ck) {
+  constexpr int SUB = 32 / CW;
   extern __shared__ __align__(16) unsigned char smem[];
   const Geom &g = a.g;
-  const size_t tab_bytes = l.tab_smem ? table_smem_bytes(a) : 0;
   const void *tp[MIRT_DMAX];
-  stage_tables<REAL>(a, l.tab_smem, smem, tp);
+  stage_tables<REAL>(a, 0, smem, tp);
 
   int npts = 1;
 #pragma unroll
   for (int d = 0; d < D; d++) npts *= t.T[d];
-  float2 *acc = reinterpret_cast<float2 *>(smem + tab_bytes);
+  float2 *acc = reinterpret_cast<float2 *>(smem);
   int Jd[MIRT_DMAX] = {1, 1, 1};
 #pragma unroll
   for (int d = 0; d < D; d++) Jd[d] = JT > 0 ? JT : g.J[d];
@@ -321,17 +374,15 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t, Lau
       ext[d] = min(t.T[d], g.K[d] - lo[d]);
     }
   }
-  const int grp = threadIdx.x / CW;
-  const int li = threadIdx.x % CW;
-  int gq[MIRT_DMAX] = {0, 0, 0};
-  {
-    int r = grp;
-#pragma unroll
-    for (int d = 0; d < D; d++) {
-      gq[d] = r % l.P[d];
-      r /= l.P[d];
-    }
-  }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nwarp = blockDim.x >> 5;
+  const int ls = lane / CW;   // column class
+  const int lc = lane % CW;   // coil within the chunk
+  // this warp's band of the slowest tiled dimension
+  constexpr int BD = D - 1;
+  const int per = (t.T[BD] + nwarp - 1) / nwarp;
+  const int band_lo = min(warp * per, ext[BD]);
+  const int band_hi = min(band_lo + per, ext[BD]);
   for (int e = threadIdx.x; e < npts * CW; e += blockDim.x) acc[e] = make_float2(0.f, 0.f);
 
   int ns[MIRT_DMAX] = {1, 1, 1};
@@ -368,42 +419,73 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t, Lau
         F[e] = f;
       }
       __syncthreads();
+      if (band_lo >= band_hi) continue;
       for (int sl = 0; sl < nb; sl++) {
         const float2 *Ws = s.W + sl * SJ;
         const int *Ks = s.KI + sl * SJ;
-        const float2 f = F[sl * CW + li];
-#pragma unroll 1
-        for (int j1 = 0; j1 < Jd[0]; j1++) {
-          const int l1 = Ks[j1] - lo[0];
-          if ((unsigned)l1 >= (unsigned)ext[0] || (l1 % l.P[0]) != gq[0]) continue;
-          const float2 w1 = Ws[j1];
-          if constexpr (D == 1) {
-            const float2 v = cw_mul<REAL>(w1, f);
-            float2 &A = acc[(size_t)l1 * CW + li];
+        // warp-uniform: taps of the band dimension inside this warp's band
+        const int jb0 = D == 1 ? 0 : (D == 2 ? Jd[0] : Jd[0] + Jd[1]);  // first tap of dim BD
+        const unsigned mb = tap_mask<1>(Ks[jb0], Jd[BD], g.K[BD], lo[BD], band_lo, band_hi, 0);
+        if (!mb) continue;
+        // lane: its columns (1D: inside the band; otherwise the whole tile)
+        const unsigned m1 = (D == 1) ? tap_mask<SUB>(Ks[0], Jd[0], g.K[0], lo[0], band_lo,
+                                                     band_hi, ls)
+                                     : tap_mask<SUB>(Ks[0], Jd[0], g.K[0], lo[0], 0, ext[0], ls);
+        const float2 f = F[sl * CW + lc];
+        if constexpr (D == 1) {
+          unsigned mm = m1;
+          while (mm) {
+            const int j1 = __ffs(mm) - 1;
+            mm &= mm - 1;
+            const int l1 = tap_local(Ks[0], j1, g.K[0], lo[0]);
+            const float2 v = cw_mul<REAL>(Ws[j1], f);
+            float2 &A = acc[(size_t)l1 * CW + lc];
             A.x += v.x;
             A.y += v.y;
-          } else {
-#pragma unroll 1
-            for (int j2 = 0; j2 < Jd[1]; j2++) {
-              const int l2 = Ks[Jd[0] + j2] - lo[1];
-              if ((unsigned)l2 >= (unsigned)ext[1] || (l2 % l.P[1]) != gq[1]) continue;
-              const float2 w2 = Ws[Jd[0] + j2];
-              if constexpr (D == 2) {
-                const float2 v = cw_mul<REAL>(w1, cw_mul<REAL>(w2, f));
-                float2 &A = acc[((size_t)l2 * T0 + l1) * CW + li];
+          }
+        } else if constexpr (D == 2) {
+          unsigned m2 = mb;
+          while (m2) {
+            const int j2 = __ffs(m2) - 1;
+            m2 &= m2 - 1;
+            const int l2 = tap_local(Ks[Jd[0]], j2, g.K[1], lo[1]);
+            const float2 v2 = cw_mul<REAL>(Ws[Jd[0] + j2], f);
+            float2 *row = acc + (size_t)l2 * T0 * CW + lc;
+            unsigned mm = m1;
+            while (mm) {
+              const int j1 = __ffs(mm) - 1;
+              mm &= mm - 1;
+              const int l1 = tap_local(Ks[0], j1, g.K[0], lo[0]);
+              const float2 v = cw_mul<REAL>(Ws[j1], v2);
+              float2 &A = row[(size_t)l1 * CW];
+              A.x += v.x;
+              A.y += v.y;
+            }
+          }
+        } else {
+          const unsigned m2all = tap_mask<1>(Ks[Jd[0]], Jd[1], g.K[1], lo[1], 0, ext[1], 0);
+          unsigned m3 = mb;
+          while (m3) {
+            const int j3 = __ffs(m3) - 1;
+            m3 &= m3 - 1;
+            const int l3 = tap_local(Ks[jb0], j3, g.K[2], lo[2]);
+            const float2 v3 = cw_mul<REAL>(Ws[jb0 + j3], f);
+            unsigned m2 = m2all;
+            while (m2) {
+              const int j2 = __ffs(m2) - 1;
+              m2 &= m2 - 1;
+              const int l2 = tap_local(Ks[Jd[0]], j2, g.K[1], lo[1]);
+              const float2 v2 = cw_mul<REAL>(Ws[Jd[0] + j2], v3);
+              float2 *row = acc + ((size_t)l3 * T1 + l2) * T0 * CW + lc;
+              unsigned mm = m1;
+              while (mm) {
+                const int j1 = __ffs(mm) - 1;
+                mm &= mm - 1;
+                const int l1 = tap_local(Ks[0], j1, g.K[0], lo[0]);
+                const float2 v = cw_mul<REAL>(Ws[j1], v2);
+                float2 &A = row[(size_t)l1 * CW];
                 A.x += v.x;
                 A.y += v.y;
-              } else {
-#pragma unroll 1
-                for (int j3 = 0; j3 < Jd[2]; j3++) {
-                  const int l3 = Ks[Jd[0] + Jd[1] + j3] - lo[2];
-                  if ((unsigned)l3 >= (unsigned)ext[2] || (l3 % l.P[2]) != gq[2]) continue;
-                  const float2 w3 = Ws[Jd[0] + Jd[1] + j3];
-                  const float2 v = cw_mul<REAL>(w1, cw_mul<REAL>(w2, cw_mul<REAL>(w3, f)));
-                  float2 &A = acc[(((size_t)l3 * T1 + l2) * T0 + l1) * CW + li];
-                  A.x += v.x;
-                  A.y += v.y;
-                }
               }
             }
           }
@@ -425,7 +507,6 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t, Lau
     gout[kk * C + c0 + cc] = acc[e];
   }
 }
-
 // ------------------------------------------------------------------------
 // launch dispatch
 // ------------------------------------------------------------------------
@@ -476,8 +557,8 @@ cudaError_t run(Req &r) {
   const Tiling &t = *r.t;
   int npts = 1;
   for (int d = 0; d < D; d++) npts *= t.T[d];
-  const size_t sm = (l.tab_smem ? table_smem_bytes(a) : 0) + (size_t)npts * CW * 8 +
-                    stage_bytes(a, l.sb) + (size_t)l.sb * CW * 8 + 16;
+  // the spread reads its tables from global memory (L1) in the staging phase
+  const size_t sm = (size_t)npts * CW * 8 + stage_bytes(a, l.sb) + (size_t)l.sb * CW * 8 + 16;
   auto kern = spread_kernel<D, CW, JT, REAL>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;

@@ -90,7 +90,8 @@ def interp_for(ck, h, J, L, tm, K, order=0, impl="port", nthreads=1):
     ck = np.asarray(ck, dtype=np.complex128)
     if ck.ndim == 1:
         ck = ck[:, None]
-    tm = np.asfortranarray(np.asarray(tm, dtype=np.float64).reshape(len(tm), -1))
+    tm = np.asarray(tm, dtype=np.float64)
+    tm = np.asfortranarray(tm.reshape(tm.shape[0], -1) if tm.ndim != 2 else tm)
     D = tm.shape[1]
     M, N = tm.shape[0], ck.shape[1]
     keep, hr, hi = _tables(h)
@@ -124,7 +125,8 @@ def interp_adj(fm, h, J, L, tm, K, order=0, impl="port", nthreads=1):
     fm = np.asarray(fm, dtype=np.complex128)
     if fm.ndim == 1:
         fm = fm[:, None]
-    tm = np.asfortranarray(np.asarray(tm, dtype=np.float64).reshape(len(tm), -1))
+    tm = np.asarray(tm, dtype=np.float64)
+    tm = np.asfortranarray(tm.reshape(tm.shape[0], -1) if tm.ndim != 2 else tm)
     D = tm.shape[1]
     M, N = fm.shape
     nk = int(np.prod(K))
