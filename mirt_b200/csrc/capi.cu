@@ -11,6 +11,7 @@
 
 #include <cmath>
 #include <complex>
+#include <algorithm>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -118,6 +119,11 @@ struct DMem {
   }
 };
 
+void swap_mem(DMem &x, DMem &y) {
+  std::swap(x.p, y.p);
+  std::swap(x.bytes, y.bytes);
+}
+
 cudaStream_t as_stream(void *s) { return static_cast<cudaStream_t>(s); }
 
 int device_ok() {
@@ -140,7 +146,7 @@ struct mirt_interp_plan {
   Tiling t{};
   Launch lg{}, ls{};
   DMem tm, slice, perm, bin_start, tab[MIRT_DMAX], phase, src[MIRT_DMAX], nsrc[MIRT_DMAX];
-  DMem keys, sorttmp, moff;
+  DMem keys, sorttmp, moff, task_order;
   std::vector<long long> moff_host;
 };
 
@@ -160,7 +166,7 @@ void choose_config(mirt_interp_plan *P) {
   Launch &lg = P->lg;
   lg.threads = threads;
   lg.cw = cw;
-  int sb = ngroups * 4;
+  int sb = ngroups * 16;
   if (sb < 32) sb = 32;
   if (sb > 256) sb = 256;
   lg.sb = sb;
@@ -302,6 +308,59 @@ int plan_geometry(mirt_interp_plan *P, int D, const int *K, const int *J, const 
   return MIRT_OK;
 }
 
+// Spread CTAs in order of decreasing work (samples over each tile's source
+// bins), so that the dense k-space centre tiles start first and do not form
+// the tail of the launch.
+int build_task_order(mirt_interp_plan *P, cudaStream_t st) {
+  const Tiling &t = P->t;
+  const int D = P->a.g.D;
+  const long long ntask = (long long)t.ntiles * t.nslice;
+  std::vector<int> bs(ntask + 1);
+  CK(cudaMemcpyAsync(bs.data(), P->bin_start.p, (ntask + 1) * sizeof(int), cudaMemcpyDeviceToHost,
+                     st));
+  std::vector<int> src[MIRT_DMAX], nsrc[MIRT_DMAX];
+  for (int d = 0; d < MIRT_DMAX; d++) {
+    src[d].resize((size_t)t.nb[d] * MIRT_SRCMAX);
+    nsrc[d].resize(t.nb[d]);
+    CK(cudaMemcpyAsync(src[d].data(), t.src[d], src[d].size() * sizeof(int),
+                       cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(nsrc[d].data(), t.nsrc[d], nsrc[d].size() * sizeof(int),
+                       cudaMemcpyDeviceToHost, st));
+  }
+  CK(cudaStreamSynchronize(st));
+  std::vector<std::pair<long long, int>> work(ntask);
+  for (long long task = 0; task < ntask; task++) {
+    const int tile = (int)(task % t.ntiles);
+    const long long slice = task / t.ntiles;
+    int b[MIRT_DMAX] = {0, 0, 0}, r = tile;
+    for (int d = 0; d < D; d++) {
+      b[d] = r % t.nb[d];
+      r /= t.nb[d];
+    }
+    long long w = 0;
+    const int n0 = nsrc[0][b[0]], n1 = D > 1 ? nsrc[1][b[1]] : 1, n2 = D > 2 ? nsrc[2][b[2]] : 1;
+    for (int i2 = 0; i2 < n2; i2++)
+      for (int i1 = 0; i1 < n1; i1++)
+        for (int i0 = 0; i0 < n0; i0++) {
+          long long st_ = src[0][b[0] * MIRT_SRCMAX + i0];
+          if (D > 1) st_ += (long long)src[1][b[1] * MIRT_SRCMAX + i1] * t.nb[0];
+          if (D > 2) st_ += (long long)src[2][b[2] * MIRT_SRCMAX + i2] * t.nb[0] * t.nb[1];
+          const long long bin = slice * t.ntiles + st_;
+          w += bs[bin + 1] - bs[bin];
+        }
+    work[task] = {-w, (int)task};
+  }
+  std::stable_sort(work.begin(), work.end());
+  std::vector<int> order(ntask);
+  for (long long i = 0; i < ntask; i++) order[i] = work[i].second;
+  CK(P->task_order.alloc(std::max<long long>(ntask, 1) * sizeof(int)));
+  CK(cudaMemcpyAsync(P->task_order.p, order.data(), ntask * sizeof(int), cudaMemcpyHostToDevice,
+                     st));
+  CK(cudaStreamSynchronize(st));
+  P->t.task_order = P->task_order.as<int>();
+  return MIRT_OK;
+}
+
 // Slices, tiling, bin sort.  P->tm must hold the FP64 coordinates on device.
 int plan_finish(mirt_interp_plan *P, long long Mtot, const long long *moff, int nslice,
                 cudaStream_t st) {
@@ -332,10 +391,30 @@ int plan_finish(mirt_interp_plan *P, long long Mtot, const long long *moff, int 
   CK(launch_bin_keys(a, P->t, P->keys.as<uint32_t>(), st));
   CK(radix_sort_bins(P->keys.as<uint32_t>(), Mtot, (int)nbins, P->sorttmp.p, P->perm.as<int>(),
                      P->bin_start.as<int>(), st));
+  // per-sample arrays into sorted order, so that staging reads are coalesced
+  {
+    DMem tm2, sl2, ph2;
+    CK(tm2.alloc(std::max<long long>(Mtot, 1) * a.g.D * sizeof(double)));
+    if (a.slice_id) CK(sl2.alloc(std::max<long long>(Mtot, 1) * sizeof(int)));
+    if (a.phase) CK(ph2.alloc(std::max<long long>(Mtot, 1) * sizeof(float2)));
+    CK(launch_permute_samples(a.tm, a.slice_id, a.phase, P->perm.as<int>(), Mtot, a.g.D,
+                              tm2.as<double>(), sl2.as<int>(), ph2.as<float2>(), st));
+    CK(cudaStreamSynchronize(st));
+    swap_mem(P->tm, tm2);
+    a.tm = P->tm.as<double>();
+    if (a.slice_id) {
+      swap_mem(P->slice, sl2);
+      a.slice_id = P->slice.as<int>();
+    }
+    if (a.phase) {
+      swap_mem(P->phase, ph2);
+      a.phase = P->phase.as<float2>();
+    }
+  }
   a.perm = P->perm.as<int>();
-  // the sort scratch returns to the shared cache: let the sort finish first
-  CK(cudaStreamSynchronize(st));
   P->sorttmp.release();
+  int rc2 = build_task_order(P, st);
+  if (rc2) return rc2;
   CK(query_gather_grid(a, P->lg));
   return MIRT_OK;
 }

@@ -151,6 +151,21 @@ __global__ void fill_slice_kernel(const long long *moff, int nslice, int *slice_
     slice_id[m] = s;
 }
 
+// gather the per-sample arrays into bin-sorted order: out[pos] = in[perm[pos]]
+__global__ void permute_samples_kernel(const double *__restrict__ tm_in,
+                                       const int *__restrict__ slice_in,
+                                       const float2 *__restrict__ ph_in,
+                                       const int *__restrict__ perm, long long M, int D,
+                                       double *__restrict__ tm_out, int *__restrict__ slice_out,
+                                       float2 *__restrict__ ph_out) {
+  const long long pos = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (pos >= M) return;
+  const int m = perm[pos];
+  for (int d = 0; d < D; d++) tm_out[d * M + pos] = tm_in[d * M + m];
+  if (slice_in) slice_out[pos] = slice_in[m];
+  if (ph_in) ph_out[pos] = ph_in[m];
+}
+
 static unsigned grid_for(long long n, int thr, int maxb = 148 * 32) {
   long long b = (n + thr - 1) / thr;
   if (b > maxb) b = maxb;
@@ -200,6 +215,15 @@ cudaError_t launch_il_to_split(const float2 *in, long long npts, int N, double *
 cudaError_t launch_tab_to_f32(const double *re, const double *im, int n, void *out,
                               cudaStream_t st) {
   tab_to_f32_kernel<<<(n + 255) / 256, 256, 0, st>>>(re, im, n, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_permute_samples(const double *tm_in, const int *slice_in, const float2 *ph_in,
+                                   const int *perm, long long M, int D, double *tm_out,
+                                   int *slice_out, float2 *ph_out, cudaStream_t st) {
+  if (M == 0) return cudaSuccess;
+  permute_samples_kernel<<<(unsigned)((M + 255) / 256), 256, 0, st>>>(
+      tm_in, slice_in, ph_in, perm, M, D, tm_out, slice_out, ph_out);
   return cudaGetLastError();
 }
 

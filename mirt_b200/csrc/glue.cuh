@@ -26,6 +26,9 @@ cudaError_t launch_il_to_split(const float2 *in, long long npts, int N, double *
                                cudaStream_t st);
 cudaError_t launch_tab_to_f32(const double *re, const double *im, int n, void *out,
                               cudaStream_t st);
+cudaError_t launch_permute_samples(const double *tm_in, const int *slice_in, const float2 *ph_in,
+                                   const int *perm, long long M, int D, double *tm_out,
+                                   int *slice_out, float2 *ph_out, cudaStream_t st);
 cudaError_t launch_fill_slice(const long long *moff_dev, int nslice, long long Mtot, int *slice_id,
                               cudaStream_t st);
 

@@ -16,9 +16,13 @@ struct InterpArgs {
   int order;             // 0 or 1 (1 only with real tables)
   int C;                 // columns (coils) per slice
   long long Mtot;        // samples over all slices
+  // Per-sample arrays are indexed by processing position pos.  Before the
+  // bin sort perm == nullptr and pos is the sample index; after it the plan
+  // stores tm / slice_id / phase permuted into sorted order and perm[pos]
+  // gives the caller's sample index (the row of fm).
   const double *tm;      // [D][Mtot] FP64 coordinates t = om / (2 pi / K)
   const int *slice_id;   // [Mtot] slice of each sample, or nullptr (all 0)
-  const int *perm;       // [Mtot] processing order (sorted), or nullptr
+  const int *perm;       // [Mtot] caller's sample index of each position, or nullptr
   const void *tab[MIRT_DMAX];  // device tables: float2 (complex) or float (real)
   const float2 *phase;   // [Mtot] per-sample phase (nullptr = none)
   long long grid_elems;  // prod(K) * C  (one slice's grid, in float2)
@@ -35,12 +39,14 @@ struct Tiling {
   // (binned by their first tap) can reach tile b.
   const int *src[MIRT_DMAX];
   const int *nsrc[MIRT_DMAX];
+  // spread CTA order: task = slice * ntiles + tile, heaviest first (or nullptr)
+  const int *task_order;
 };
 #define MIRT_SRCMAX 8
 
 // Launch tuning chosen by the host (autotuned per geometry).
 struct Launch {
-  int threads;   // CTA size
+  int threads;   // CTA size (multiple of 32)
   int cw;        // lanes per sample group (= coils handled in parallel)
   int sb;        // samples per staged batch
   int grid;      // CTAs for the gather (persistent)

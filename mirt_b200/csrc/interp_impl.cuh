@@ -5,7 +5,7 @@
 // Forward gather replaces nufft/table/interp{1,2,3}_table1_for.c; the
 // adjoint spread replaces nufft/table/interp{1,2,3}_table1_adj.c.
 // Table-entry selection and grid wrap are FP64, exactly as the reference
-// (common.cuh); taps are accumulated in FP32.
+// (common.cuh); taps are accumulated in FP32 with packed FP32x2 FMAs.
 //
 // Both kernels stage, per CTA, a batch of `sb` samples: one thread per
 // (sample, dimension, tap) computes the table coefficient and the wrapped grid
@@ -18,77 +18,56 @@ namespace mirt {
 namespace detail {
 
 // ------------------------------------------------------------------------
-// shared-memory staging
+// small helpers
 // ------------------------------------------------------------------------
 struct Stage {
   float2 *W;   // [sb][SJ] tap coefficients (real tables: .y = 0)
   int *KI;     // [sb][SJ] wrapped grid coordinate of each tap
-  int *mid;    // [sb] sample index
+  int *mid;    // [sb] caller's sample index (row of fm)
   int *sid;    // [sb] slice index
 };
 
-// Copy the D tables into shared memory when requested; returns pointers to use.
-template <bool REAL>
-__device__ void stage_tables(const InterpArgs &a, int use_smem, unsigned char *buf,
-                             const void *tp[MIRT_DMAX]) {
-  size_t off = 0;
-  for (int d = 0; d < a.g.D; d++) {
-    if (!use_smem) {
-      tp[d] = a.tab[d];
-      continue;
-    }
-    if (REAL) {
-      float *dst = reinterpret_cast<float *>(buf + off);
-      const float *src = static_cast<const float *>(a.tab[d]);
-      for (int i = threadIdx.x; i < a.g.tlen[d]; i += blockDim.x) dst[i] = src[i];
-      tp[d] = dst;
-      off += ((size_t)a.g.tlen[d] * 4 + 15) & ~(size_t)15;
-    } else {
-      float2 *dst = reinterpret_cast<float2 *>(buf + off);
-      const float2 *src = static_cast<const float2 *>(a.tab[d]);
-      for (int i = threadIdx.x; i < a.g.tlen[d]; i += blockDim.x) dst[i] = src[i];
-      tp[d] = dst;
-      off += ((size_t)a.g.tlen[d] * 8 + 15) & ~(size_t)15;
-    }
-  }
-  __syncthreads();
+// k mod K for any k, cheap when k is within one period of [0, K)
+__device__ __forceinline__ int wrap_fast(int k, int K) {
+  if (k < 0) k += K;
+  else if (k >= K) k -= K;
+  if ((unsigned)k >= (unsigned)K) k = wrapk(k, K);
+  return k;
 }
 
 // Coefficient of tap (d, k) for coordinate t: the reference's 0th-order
 // lookup or 1st-order linear interpolation of the table.  The index is
 // clamped into the table, which changes nothing for |t - k| <= J/2.
 template <bool REAL>
-__device__ __forceinline__ float2 tap_coef(const InterpArgs &a, const void *const tp[MIRT_DMAX],
-                                           int d, double t, int k) {
+__device__ __forceinline__ float2 tap_coef(const InterpArgs &a, int d, double t, int k) {
   const int L = a.g.L[d];
   const int nc = a.g.ncenter[d];
   const int tl = a.g.tlen[d];
   if (REAL) {
-    const float *h = static_cast<const float *>(tp[d]);
+    const float *h = static_cast<const float *>(a.tab[d]);
     if (a.order == 0) {
       int n = nc + tab0_index(t, k, L);
       n = min(max(n, 0), tl - 1);
-      return make_float2(h[n], 0.f);
+      return make_float2(__ldg(h + n), 0.f);
     }
     float alf;
     int n = nc + tab1_index(t, k, L, &alf);
     n = min(max(n, 0), tl - 1);
-    const float h0 = h[n];
+    const float h0 = __ldg(h + n);
     // the reference reads one entry past the table end here, times alf = 0
-    const float h1 = (n + 1 < tl) ? h[n + 1] : 0.f;
+    const float h1 = (n + 1 < tl) ? __ldg(h + n + 1) : 0.f;
     return make_float2((1.f - alf) * h0 + alf * h1, 0.f);
   } else {
-    const float2 *h = static_cast<const float2 *>(tp[d]);
+    const float2 *h = static_cast<const float2 *>(a.tab[d]);
     int n = nc + tab0_index(t, k, L);
     n = min(max(n, 0), tl - 1);
-    return h[n];
+    return __ldg(h + n);
   }
 }
 
-// Fill the stage for samples at sorted positions [pos0, pos0 + nb).
+// Fill the stage for positions [pos0, pos0 + nb).
 template <bool REAL>
-__device__ void stage_batch(const InterpArgs &a, const void *const tp[MIRT_DMAX], const Stage &s,
-                            long long pos0, int nb, int SJ) {
+__device__ void stage_batch(const InterpArgs &a, const Stage &s, long long pos0, int nb, int SJ) {
   const int D = a.g.D;
   for (int e = threadIdx.x; e < nb * SJ; e += blockDim.x) {
     const int sl = e / SJ;
@@ -100,27 +79,36 @@ __device__ void stage_batch(const InterpArgs &a, const void *const tp[MIRT_DMAX]
       d++;
     }
     const long long pos = pos0 + sl;
-    const int m = a.perm ? a.perm[pos] : (int)pos;
-    const double t = a.tm[(long long)d * a.Mtot + m];
+    const double t = a.tm[(long long)d * a.Mtot + pos];
     const int k = koff_of(t, a.g.J[d]) + j;
-    s.W[e] = tap_coef<REAL>(a, tp, d, t, k);
-    s.KI[e] = wrapk(k, a.g.K[d]);
+    s.W[e] = tap_coef<REAL>(a, d, t, k);
+    s.KI[e] = wrap_fast(k, a.g.K[d]);
     if (r == 0) {
-      s.mid[sl] = m;
-      s.sid[sl] = a.slice_id ? a.slice_id[m] : 0;
+      s.mid[sl] = a.perm ? a.perm[pos] : (int)pos;
+      s.sid[sl] = a.slice_id ? a.slice_id[pos] : 0;
     }
   }
 }
 
+// Complex accumulator held as two packed pairs: with w = (wr, wi) and
+// v = (vr, vi), A += (wr, wr) * v and B += (wi, wi) * v, so that
+// sum w * v = (A.x - B.y, A.y + B.x).  Two FFMA2 per complex MAC.
+struct CAcc {
+  float2 A, B;
+};
+__device__ __forceinline__ void cacc_zero(CAcc &c) {
+  c.A = make_float2(0.f, 0.f);
+  c.B = make_float2(0.f, 0.f);
+}
 template <bool REAL>
-__device__ __forceinline__ void mac(float2 &acc, float2 w, float2 v) {
-  if (REAL) {
-    acc.x = fmaf(w.x, v.x, acc.x);
-    acc.y = fmaf(w.x, v.y, acc.y);
-  } else {
-    acc.x += w.x * v.x - w.y * v.y;
-    acc.y += w.x * v.y + w.y * v.x;
-  }
+__device__ __forceinline__ void cacc_mac(CAcc &c, float2 w, float2 v) {
+  c.A = __ffma2_rn(make_float2(w.x, w.x), v, c.A);
+  if (!REAL) c.B = __ffma2_rn(make_float2(w.y, w.y), v, c.B);
+}
+template <bool REAL>
+__device__ __forceinline__ float2 cacc_get(const CAcc &c) {
+  if (REAL) return c.A;
+  return make_float2(c.A.x - c.B.y, c.A.y + c.B.x);
 }
 
 // conj(w) * v
@@ -130,11 +118,12 @@ __device__ __forceinline__ float2 cw_mul(float2 w, float2 v) {
   return cmulc(w, v);
 }
 
-__host__ __device__ inline size_t table_smem_bytes(const InterpArgs &a) {
-  size_t b = 0;
-  for (int d = 0; d < a.g.D; d++)
-    b += ((size_t)a.g.tlen[d] * (a.real_tab ? 4 : 8) + 15) & ~(size_t)15;
-  return b;
+// A += conj(w) * v as two FFMA2: (wr, wr) * (vr, vi) + (wi, -wi) * (vi, vr)
+template <bool REAL>
+__device__ __forceinline__ float2 cw_fma(float2 w, float2 v, float2 vs, float2 A) {
+  A = __ffma2_rn(make_float2(w.x, w.x), v, A);
+  if (!REAL) A = __ffma2_rn(make_float2(w.y, -w.y), vs, A);
+  return A;
 }
 
 // ------------------------------------------------------------------------
@@ -142,24 +131,22 @@ __host__ __device__ inline size_t table_smem_bytes(const InterpArgs &a) {
 // ------------------------------------------------------------------------
 // Persistent CTAs walk batches of the bin-sorted samples.  A group of CW
 // lanes serves one sample at a time; lane li handles columns li, li+CW, ...
-// and reads each tap as one coalesced column segment of the grid.
-template <int D, int CW, int JT, bool REAL>
+// and reads each tap as one coalesced column segment of the grid.  When the
+// J1 taps of a row do not wrap, they sit at a constant stride from one row
+// pointer (a compile-time stride when C == CW, CX).
+template <int D, int CW, int JT, bool REAL, bool CX>
 __global__ void __launch_bounds__(256) gather_kernel(InterpArgs a, Launch l,
                                                      const float2 *__restrict__ ck,
                                                      float2 *__restrict__ fm) {
   extern __shared__ __align__(16) unsigned char smem[];
   const Geom &g = a.g;
-  const size_t tab_bytes = l.tab_smem ? table_smem_bytes(a) : 0;
-  const void *tp[MIRT_DMAX];
-  stage_tables<REAL>(a, l.tab_smem, smem, tp);
-
   int Jd[MIRT_DMAX] = {1, 1, 1};
 #pragma unroll
   for (int d = 0; d < D; d++) Jd[d] = JT > 0 ? JT : g.J[d];
   const int SJ = Jd[0] + (D > 1 ? Jd[1] : 0) + (D > 2 ? Jd[2] : 0);
   const int sb = l.sb;
   Stage s;
-  s.W = reinterpret_cast<float2 *>(smem + tab_bytes);
+  s.W = reinterpret_cast<float2 *>(smem);
   s.KI = reinterpret_cast<int *>(s.W + sb * SJ);
   s.mid = s.KI + sb * SJ;
   s.sid = s.mid + sb;
@@ -168,99 +155,116 @@ __global__ void __launch_bounds__(256) gather_kernel(InterpArgs a, Launch l,
   const int grp = threadIdx.x / CW;
   const int li = threadIdx.x % CW;
   const int C = a.C;
-  int ostr[MIRT_DMAX] = {0, 0, 0};
-#pragma unroll
-  for (int d = 0; d < D; d++) ostr[d] = (int)(g.kstride[d] * C);
+  const int cstr = CX ? CW : C;  // grid stride between neighbouring k1
+  const long long rstr = (long long)g.kstride[D > 1 ? 1 : 0] * C;
+  const long long pstr = (long long)g.kstride[D > 2 ? 2 : 0] * C;
 
   const long long nbatch = (a.Mtot + sb - 1) / sb;
   for (long long bi = blockIdx.x; bi < nbatch; bi += gridDim.x) {
     const long long pos0 = bi * sb;
     const int nb = (int)min((long long)sb, a.Mtot - pos0);
-    stage_batch<REAL>(a, tp, s, pos0, nb, SJ);
+    stage_batch<REAL>(a, s, pos0, nb, SJ);
     __syncthreads();
     for (int sl = grp; sl < nb; sl += ngroups) {
       const int m = s.mid[sl];
       const float2 *gb = ck + (long long)s.sid[sl] * a.grid_elems;
-      const float2 ph = a.phase ? a.phase[m] : make_float2(1.f, 0.f);
       const float2 *Ws = s.W + sl * SJ;
       const int *Ks = s.KI + sl * SJ;
+      const float2 ph = a.phase ? a.phase[pos0 + sl] : make_float2(1.f, 0.f);
       if constexpr (JT > 0) {
-        // fixed J: tap coefficients and offsets in registers, taps unrolled
-        float2 w[D][JT];
-        int o[D][JT];
+        float2 w1[JT];
+        int o1[JT];
 #pragma unroll
-        for (int d = 0; d < D; d++)
-#pragma unroll
-          for (int j = 0; j < JT; j++) {
-            w[d][j] = Ws[d * JT + j];
-            o[d][j] = Ks[d * JT + j] * ostr[d];
-          }
+        for (int j = 0; j < JT; j++) {
+          w1[j] = Ws[j];
+          o1[j] = Ks[j] * C;
+        }
+        const int k10 = Ks[0];
+        const bool fast = k10 + JT <= g.K[0];
+        const int c10 = k10 * C;
         for (int c = li; c < C; c += CW) {
           const float2 *gc = gb + c;
-          float2 acc = make_float2(0.f, 0.f);
-          if constexpr (D == 1) {
+          // sum over j1 of one grid row (the reference's innermost loop)
+          auto rowsum = [&](const float2 *row) -> float2 {
+            CAcc s1;
+            cacc_zero(s1);
+            if (fast) {
+              const float2 *p = row + c10;
 #pragma unroll
-            for (int j1 = 0; j1 < JT; j1++) mac<REAL>(acc, w[0][j1], __ldg(gc + o[0][j1]));
+              for (int j1 = 0; j1 < JT; j1++) cacc_mac<REAL>(s1, w1[j1], __ldg(p + j1 * cstr));
+            } else {
+#pragma unroll
+              for (int j1 = 0; j1 < JT; j1++) cacc_mac<REAL>(s1, w1[j1], __ldg(row + o1[j1]));
+            }
+            return cacc_get<REAL>(s1);
+          };
+          float2 out;
+          if constexpr (D == 1) {
+            out = rowsum(gc);
           } else if constexpr (D == 2) {
+            CAcc s2;
+            cacc_zero(s2);
 #pragma unroll
             for (int j2 = 0; j2 < JT; j2++) {
-              float2 s1 = make_float2(0.f, 0.f);
-              const float2 *row = gc + o[1][j2];
-#pragma unroll
-              for (int j1 = 0; j1 < JT; j1++) mac<REAL>(s1, w[0][j1], __ldg(row + o[0][j1]));
-              mac<false>(acc, w[1][j2], s1);
+              const float2 r = rowsum(gc + Ks[JT + j2] * rstr);
+              cacc_mac<false>(s2, Ws[JT + j2], r);
             }
+            out = cacc_get<false>(s2);
           } else {
-#pragma unroll
+            CAcc s3;
+            cacc_zero(s3);
+#pragma unroll 1
             for (int j3 = 0; j3 < JT; j3++) {
-              float2 s2 = make_float2(0.f, 0.f);
-              const float2 *pl = gc + o[2][j3];
+              const float2 *pl = gc + Ks[2 * JT + j3] * pstr;
+              CAcc s2;
+              cacc_zero(s2);
 #pragma unroll
               for (int j2 = 0; j2 < JT; j2++) {
-                float2 s1 = make_float2(0.f, 0.f);
-                const float2 *row = pl + o[1][j2];
-#pragma unroll
-                for (int j1 = 0; j1 < JT; j1++) mac<REAL>(s1, w[0][j1], __ldg(row + o[0][j1]));
-                mac<false>(s2, w[1][j2], s1);
+                const float2 r = rowsum(pl + Ks[JT + j2] * rstr);
+                cacc_mac<false>(s2, Ws[JT + j2], r);
               }
-              mac<false>(acc, w[2][j3], s2);
+              cacc_mac<false>(s3, Ws[2 * JT + j3], cacc_get<false>(s2));
             }
+            out = cacc_get<false>(s3);
           }
-          if (a.phase) acc = cmul(acc, ph);
-          fm[(long long)m * C + c] = acc;
+          if (a.phase) out = cmul(out, ph);
+          fm[(long long)m * C + c] = out;
         }
       } else {
         // any J: coefficients read from shared memory, runtime loops
         for (int c = li; c < C; c += CW) {
           const float2 *gc = gb + c;
-          float2 acc = make_float2(0.f, 0.f);
-          if constexpr (D == 1) {
+          auto rowsum = [&](const float2 *row) -> float2 {
+            CAcc s1;
+            cacc_zero(s1);
             for (int j1 = 0; j1 < Jd[0]; j1++)
-              mac<REAL>(acc, Ws[j1], __ldg(gc + Ks[j1] * ostr[0]));
+              cacc_mac<REAL>(s1, Ws[j1], __ldg(row + (long long)Ks[j1] * C));
+            return cacc_get<REAL>(s1);
+          };
+          float2 out;
+          if constexpr (D == 1) {
+            out = rowsum(gc);
           } else if constexpr (D == 2) {
-            for (int j2 = 0; j2 < Jd[1]; j2++) {
-              float2 s1 = make_float2(0.f, 0.f);
-              const float2 *row = gc + Ks[Jd[0] + j2] * ostr[1];
-              for (int j1 = 0; j1 < Jd[0]; j1++)
-                mac<REAL>(s1, Ws[j1], __ldg(row + Ks[j1] * ostr[0]));
-              mac<false>(acc, Ws[Jd[0] + j2], s1);
-            }
+            CAcc s2;
+            cacc_zero(s2);
+            for (int j2 = 0; j2 < Jd[1]; j2++)
+              cacc_mac<false>(s2, Ws[Jd[0] + j2], rowsum(gc + Ks[Jd[0] + j2] * rstr));
+            out = cacc_get<false>(s2);
           } else {
+            CAcc s3;
+            cacc_zero(s3);
             for (int j3 = 0; j3 < Jd[2]; j3++) {
-              float2 s2 = make_float2(0.f, 0.f);
-              const float2 *pl = gc + Ks[Jd[0] + Jd[1] + j3] * ostr[2];
-              for (int j2 = 0; j2 < Jd[1]; j2++) {
-                float2 s1 = make_float2(0.f, 0.f);
-                const float2 *row = pl + Ks[Jd[0] + j2] * ostr[1];
-                for (int j1 = 0; j1 < Jd[0]; j1++)
-                  mac<REAL>(s1, Ws[j1], __ldg(row + Ks[j1] * ostr[0]));
-                mac<false>(s2, Ws[Jd[0] + j2], s1);
-              }
-              mac<false>(acc, Ws[Jd[0] + Jd[1] + j3], s2);
+              const float2 *pl = gc + Ks[Jd[0] + Jd[1] + j3] * pstr;
+              CAcc s2;
+              cacc_zero(s2);
+              for (int j2 = 0; j2 < Jd[1]; j2++)
+                cacc_mac<false>(s2, Ws[Jd[0] + j2], rowsum(pl + Ks[Jd[0] + j2] * rstr));
+              cacc_mac<false>(s3, Ws[Jd[0] + Jd[1] + j3], cacc_get<false>(s2));
             }
+            out = cacc_get<false>(s3);
           }
-          if (a.phase) acc = cmul(acc, ph);
-          fm[(long long)m * C + c] = acc;
+          if (a.phase) out = cmul(out, ph);
+          fm[(long long)m * C + c] = out;
         }
       }
     }
@@ -290,7 +294,7 @@ __global__ void __launch_bounds__(256) gather_kernel(InterpArgs a, Launch l,
 // runs: base + j before the periodic wrap and base - K + j after it.
 template <int SUB>
 __host__ __device__ __forceinline__ unsigned tap_mask(int k0w, int J, int K, int lo_tile, int lo_b,
-                                             int hi_b, int s) {
+                                                      int hi_b, int s) {
   const int base = k0w - lo_tile;
   const int jw = K - k0w;  // first tap index after the wrap
   unsigned m = 0;
@@ -332,6 +336,44 @@ __host__ __device__ __forceinline__ int tap_local(int k0w, int j, int K, int lo_
   return x - lo_tile;
 }
 
+// One grid row of the tile for one sample: acc[l1][lane coil] += conj(w1) v2
+// for the lane's taps.  Fast path when all J1 taps lie inside the tile.
+template <int CW, int JT, bool REAL>
+__device__ __forceinline__ void spread_row(float2 *row, const float2 *Ws, int J1, bool fast1,
+                                           int l10, unsigned m1, int k10, int K1, int lo1,
+                                           int ls, float2 v2) {
+  constexpr int SUB = 32 / CW;
+  const float2 v2s = make_float2(v2.y, v2.x);
+  if (fast1) {
+    if constexpr (JT > 0 && SUB == 1) {
+      float2 *p = row + l10 * CW;
+#pragma unroll
+      for (int j1 = 0; j1 < JT; j1++) {
+        float2 A = p[j1 * CW];
+        A = cw_fma<REAL>(Ws[j1], v2, v2s, A);
+        p[j1 * CW] = A;
+      }
+    } else {
+      for (int j1 = (ls - l10) & (SUB - 1); j1 < J1; j1 += SUB) {
+        float2 *p = row + (l10 + j1) * CW;
+        float2 A = *p;
+        A = cw_fma<REAL>(Ws[j1], v2, v2s, A);
+        *p = A;
+      }
+    }
+  } else {
+    unsigned mm = m1;
+    while (mm) {
+      const int j1 = __ffs(mm) - 1;
+      mm &= mm - 1;
+      float2 *p = row + tap_local(k10, j1, K1, lo1) * CW;
+      float2 A = *p;
+      A = cw_fma<REAL>(Ws[j1], v2, v2s, A);
+      *p = A;
+    }
+  }
+}
+
 template <int D, int CW, int JT, bool REAL>
 __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t, Launch l,
                                                      const int *__restrict__ bin_start,
@@ -340,8 +382,6 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t, Lau
   constexpr int SUB = 32 / CW;
   extern __shared__ __align__(16) unsigned char smem[];
   const Geom &g = a.g;
-  const void *tp[MIRT_DMAX];
-  stage_tables<REAL>(a, 0, smem, tp);
 
   int npts = 1;
 #pragma unroll
@@ -360,8 +400,9 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t, Lau
   // [sb][CW] sample values; sb is even, so this stays 8-byte aligned
   float2 *F = reinterpret_cast<float2 *>(s.sid + sb);
 
-  const int tile = blockIdx.x % t.ntiles;
-  const int slice = blockIdx.x / t.ntiles;
+  const int task = t.task_order ? t.task_order[blockIdx.x] : (int)blockIdx.x;
+  const int tile = task % t.ntiles;
+  const int slice = task / t.ntiles;
   const int c0 = blockIdx.y * CW;
   int b[MIRT_DMAX] = {0, 0, 0}, lo[MIRT_DMAX] = {0, 0, 0}, ext[MIRT_DMAX] = {1, 1, 1};
   {
@@ -378,8 +419,7 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t, Lau
   const int nwarp = blockDim.x >> 5;
   const int ls = lane / CW;   // column class
   const int lc = lane % CW;   // coil within the chunk
-  // this warp's band of the slowest tiled dimension
-  constexpr int BD = D - 1;
+  constexpr int BD = D - 1;   // band dimension
   const int per = (t.T[BD] + nwarp - 1) / nwarp;
   const int band_lo = min(warp * per, ext[BD]);
   const int band_hi = min(band_lo + per, ext[BD]);
@@ -392,6 +432,7 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t, Lau
   const int C = a.C;
   const int T0 = t.T[0];
   const int T1 = D > 1 ? t.T[1] : 1;
+  const int jb0 = D == 1 ? 0 : (D == 2 ? Jd[0] : Jd[0] + Jd[1]);  // first tap of dim BD
 
   for (int si = 0; si < nsrc_tot; si++) {
     int r = si, stile = 0, mul = 1;
@@ -407,14 +448,15 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t, Lau
     for (long long pos0 = beg; pos0 < end; pos0 += sb) {
       const int nb = (int)min((long long)sb, end - pos0);
       __syncthreads();
-      stage_batch<REAL>(a, tp, s, pos0, nb, SJ);
+      stage_batch<REAL>(a, s, pos0, nb, SJ);
       for (int e = threadIdx.x; e < nb * CW; e += blockDim.x) {
         const int sl = e / CW, cc = e - sl * CW;
-        const int m = a.perm ? a.perm[pos0 + sl] : (int)(pos0 + sl);
+        const long long pos = pos0 + sl;
+        const int m = a.perm ? a.perm[pos] : (int)pos;
         float2 f = make_float2(0.f, 0.f);
         if (c0 + cc < C) {
           f = fm[(long long)m * C + c0 + cc];
-          if (a.phase) f = cmulc(a.phase[m], f);
+          if (a.phase) f = cmulc(a.phase[pos], f);
         }
         F[e] = f;
       }
@@ -424,68 +466,48 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t, Lau
         const float2 *Ws = s.W + sl * SJ;
         const int *Ks = s.KI + sl * SJ;
         // warp-uniform: taps of the band dimension inside this warp's band
-        const int jb0 = D == 1 ? 0 : (D == 2 ? Jd[0] : Jd[0] + Jd[1]);  // first tap of dim BD
         const unsigned mb = tap_mask<1>(Ks[jb0], Jd[BD], g.K[BD], lo[BD], band_lo, band_hi, 0);
         if (!mb) continue;
-        // lane: its columns (1D: inside the band; otherwise the whole tile)
-        const unsigned m1 = (D == 1) ? tap_mask<SUB>(Ks[0], Jd[0], g.K[0], lo[0], band_lo,
-                                                     band_hi, ls)
-                                     : tap_mask<SUB>(Ks[0], Jd[0], g.K[0], lo[0], 0, ext[0], ls);
+        const int k10 = Ks[0];
+        const int l10 = k10 - lo[0];
         const float2 f = F[sl * CW + lc];
         if constexpr (D == 1) {
-          unsigned mm = m1;
-          while (mm) {
-            const int j1 = __ffs(mm) - 1;
-            mm &= mm - 1;
-            const int l1 = tap_local(Ks[0], j1, g.K[0], lo[0]);
-            const float2 v = cw_mul<REAL>(Ws[j1], f);
-            float2 &A = acc[(size_t)l1 * CW + lc];
-            A.x += v.x;
-            A.y += v.y;
-          }
-        } else if constexpr (D == 2) {
-          unsigned m2 = mb;
-          while (m2) {
-            const int j2 = __ffs(m2) - 1;
-            m2 &= m2 - 1;
-            const int l2 = tap_local(Ks[Jd[0]], j2, g.K[1], lo[1]);
-            const float2 v2 = cw_mul<REAL>(Ws[Jd[0] + j2], f);
-            float2 *row = acc + (size_t)l2 * T0 * CW + lc;
-            unsigned mm = m1;
-            while (mm) {
-              const int j1 = __ffs(mm) - 1;
-              mm &= mm - 1;
-              const int l1 = tap_local(Ks[0], j1, g.K[0], lo[0]);
-              const float2 v = cw_mul<REAL>(Ws[j1], v2);
-              float2 &A = row[(size_t)l1 * CW];
-              A.x += v.x;
-              A.y += v.y;
-            }
-          }
+          const unsigned m1 = tap_mask<SUB>(k10, Jd[0], g.K[0], lo[0], band_lo, band_hi, ls);
+          spread_row<CW, JT, REAL>(acc + lc, Ws, Jd[0], false, l10, m1, k10, g.K[0], lo[0], ls,
+                                   f);
         } else {
-          const unsigned m2all = tap_mask<1>(Ks[Jd[0]], Jd[1], g.K[1], lo[1], 0, ext[1], 0);
-          unsigned m3 = mb;
-          while (m3) {
-            const int j3 = __ffs(m3) - 1;
-            m3 &= m3 - 1;
-            const int l3 = tap_local(Ks[jb0], j3, g.K[2], lo[2]);
-            const float2 v3 = cw_mul<REAL>(Ws[jb0 + j3], f);
-            unsigned m2 = m2all;
+          // lane's columns: fast when the J1 taps do not leave the tile
+          const bool fast1 = l10 >= 0 && l10 + Jd[0] <= ext[0];
+          const unsigned m1 =
+              fast1 ? 0u : tap_mask<SUB>(k10, Jd[0], g.K[0], lo[0], 0, ext[0], ls);
+          if (!fast1 && !m1) continue;
+          if constexpr (D == 2) {
+            unsigned m2 = mb;
             while (m2) {
               const int j2 = __ffs(m2) - 1;
               m2 &= m2 - 1;
               const int l2 = tap_local(Ks[Jd[0]], j2, g.K[1], lo[1]);
-              const float2 v2 = cw_mul<REAL>(Ws[Jd[0] + j2], v3);
-              float2 *row = acc + ((size_t)l3 * T1 + l2) * T0 * CW + lc;
-              unsigned mm = m1;
-              while (mm) {
-                const int j1 = __ffs(mm) - 1;
-                mm &= mm - 1;
-                const int l1 = tap_local(Ks[0], j1, g.K[0], lo[0]);
-                const float2 v = cw_mul<REAL>(Ws[j1], v2);
-                float2 &A = row[(size_t)l1 * CW];
-                A.x += v.x;
-                A.y += v.y;
+              const float2 v2 = cw_mul<REAL>(Ws[Jd[0] + j2], f);
+              spread_row<CW, JT, REAL>(acc + (size_t)l2 * T0 * CW + lc, Ws, Jd[0], fast1, l10, m1,
+                                       k10, g.K[0], lo[0], ls, v2);
+            }
+          } else {
+            const unsigned m2all = tap_mask<1>(Ks[Jd[0]], Jd[1], g.K[1], lo[1], 0, ext[1], 0);
+            if (!m2all) continue;
+            unsigned m3 = mb;
+            while (m3) {
+              const int j3 = __ffs(m3) - 1;
+              m3 &= m3 - 1;
+              const int l3 = tap_local(Ks[jb0], j3, g.K[2], lo[2]);
+              const float2 v3 = cw_mul<REAL>(Ws[jb0 + j3], f);
+              unsigned m2 = m2all;
+              while (m2) {
+                const int j2 = __ffs(m2) - 1;
+                m2 &= m2 - 1;
+                const int l2 = tap_local(Ks[Jd[0]], j2, g.K[1], lo[1]);
+                const float2 v2 = cw_mul<REAL>(Ws[Jd[0] + j2], v3);
+                spread_row<CW, JT, REAL>(acc + ((size_t)l3 * T1 + l2) * T0 * CW + lc, Ws, Jd[0],
+                                         fast1, l10, m1, k10, g.K[0], lo[0], ls, v2);
               }
             }
           }
@@ -507,6 +529,7 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t, Lau
     gout[kk * C + c0 + cc] = acc[e];
   }
 }
+
 // ------------------------------------------------------------------------
 // launch dispatch
 // ------------------------------------------------------------------------
@@ -529,13 +552,19 @@ inline size_t stage_bytes(const InterpArgs &a, int sb) {
   return (size_t)sb * SJ * (8 + 4) + (size_t)sb * 8 + 16;
 }
 
-template <int D, int CW, int JT, bool REAL>
+inline size_t spread_smem_bytes(const InterpArgs &a, const Tiling &t, const Launch &l) {
+  size_t npts = 1;
+  for (int d = 0; d < a.g.D; d++) npts *= t.T[d];
+  return npts * l.cw * 8 + stage_bytes(a, l.sb) + (size_t)l.sb * l.cw * 8 + 16;
+}
+
+template <int D, int CW, int JT, bool REAL, bool CX>
 cudaError_t run(Req &r) {
   const InterpArgs &a = *r.a;
   Launch &l = *r.l;
   if (r.what == GATHER || r.what == GATHER_GRID) {
-    const size_t sm = (l.tab_smem ? table_smem_bytes(a) : 0) + stage_bytes(a, l.sb);
-    auto kern = gather_kernel<D, CW, JT, REAL>;
+    const size_t sm = stage_bytes(a, l.sb);
+    auto kern = gather_kernel<D, CW, JT, REAL, CX>;
     cudaError_t e =
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
@@ -554,22 +583,30 @@ cudaError_t run(Req &r) {
     kern<<<l.grid, l.threads, sm, r.st>>>(a, l, r.in, r.out);
     return cudaGetLastError();
   }
-  const Tiling &t = *r.t;
-  int npts = 1;
-  for (int d = 0; d < D; d++) npts *= t.T[d];
-  // the spread reads its tables from global memory (L1) in the staging phase
-  const size_t sm = (size_t)npts * CW * 8 + stage_bytes(a, l.sb) + (size_t)l.sb * CW * 8 + 16;
-  auto kern = spread_kernel<D, CW, JT, REAL>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  if (e != cudaSuccess) return e;
-  dim3 grid((unsigned)(t.ntiles * t.nslice), (unsigned)((a.C + CW - 1) / CW));
-  kern<<<grid, l.threads, sm, r.st>>>(a, t, l, r.bin_start, r.in, r.out);
-  return cudaGetLastError();
+  if constexpr (CX) {
+    return cudaErrorInvalidValue;  // the spread has no CX variant
+  } else {
+    const Tiling &t = *r.t;
+    const size_t sm = spread_smem_bytes(a, t, l);
+    auto kern = spread_kernel<D, CW, JT, REAL>;
+    cudaError_t e =
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    dim3 grid((unsigned)(t.ntiles * t.nslice), (unsigned)((a.C + CW - 1) / CW));
+    kern<<<grid, l.threads, sm, r.st>>>(a, t, l, r.bin_start, r.in, r.out);
+    return cudaGetLastError();
+  }
+}
+
+template <int D, int CW, int JT, bool REAL>
+cudaError_t by_cx(Req &r) {
+  if (r.what != SPREAD && JT > 0 && r.a->C == CW) return run<D, CW, JT, REAL, true>(r);
+  return run<D, CW, JT, REAL, false>(r);
 }
 
 template <int D, int CW, int JT>
 cudaError_t by_real(Req &r) {
-  return r.a->real_tab ? run<D, CW, JT, true>(r) : run<D, CW, JT, false>(r);
+  return r.a->real_tab ? by_cx<D, CW, JT, true>(r) : by_cx<D, CW, JT, false>(r);
 }
 
 inline bool all_j(const Geom &g, int j) {
@@ -590,6 +627,7 @@ cudaError_t by_cw(Req &r) {
     case 1: return by_j<D, 1>(r);
     case 4: return by_j<D, 4>(r);
     case 8: return by_j<D, 8>(r);
+    case 16: return by_j<D, 16>(r);
     case 32: return by_j<D, 32>(r);
     default: return cudaErrorInvalidValue;
   }
