@@ -299,6 +299,9 @@ def run_gpu(args, w):
     n_shift = [w["N"] / 2] * D
     plan = mb.NufftPlan(om, (w["N"],) * D, (w["J"],) * D, (w["K"],) * D, n_shift=n_shift,
                         Ld=w["L"], ncol=C, slice_moff=moff)
+    t0 = time.perf_counter()
+    tuned = plan.autotune() if not args.no_autotune else plan.config()
+    t_tune = time.perf_counter() - t0
     img_np = make_images(w, np.random.default_rng(99 + rank))
     if img_np.shape[0] != plan.nslice:
         reps = -(-plan.nslice // img_np.shape[0])
@@ -426,6 +429,7 @@ def run_gpu(args, w):
             "config": {"workload": describe(args.workload, w), "samples_per_rank": Mtot,
                        "coils": C, "slices_per_rank": plan.nslice,
                        "l2": "inputs larger than L2; no flush",
+                       "launch": tuned, "autotune_s": round(t_tune, 2),
                        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": launches_per_step * args.steps, "clocks": clk,
@@ -447,6 +451,7 @@ def main():
     ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     args = ap.parse_args()
     w = WORKLOADS[args.workload]

@@ -185,6 +185,18 @@ int mirt_interp_plan_forward(mirt_interp_plan *plan, const void *ck, void *fm, v
 /* ck = interp_adj(fm) on device buffers; overwrites all of ck. */
 int mirt_interp_plan_adjoint(mirt_interp_plan *plan, const void *fm, void *ck, void *stream);
 
+/* Autotune: time candidate spread tile shapes (multiples of the 8-point sort
+ * bins), warps per spread CTA and staged batch sizes, and gather CTA / batch
+ * sizes, on this plan's trajectory; keep the fastest.  Allocates a scratch
+ * grid and sample buffer for the duration of the call.  Results stay
+ * bitwise deterministic for any choice. */
+int mirt_interp_plan_autotune(mirt_interp_plan *plan, void *stream);
+
+/* Current launch configuration: up to 12 values
+ * {T1, T2, T3, spread threads, spread batch, coil lanes, gather threads,
+ *  gather batch, gather CTAs, B1, B2, B3}. */
+int mirt_interp_plan_config(mirt_interp_plan *plan, int32_t *out, int32_t n);
+
 int mirt_interp_plan_destroy(mirt_interp_plan *plan);
 
 /* ------------------------------------------------------------------------
@@ -214,6 +226,9 @@ int mirt_nufft_adjoint_host(mirt_nufft *p, const float *X, float *x, void *strea
 
 /* The interpolation plan inside a NUFFT (for direct gather/spread calls). */
 mirt_interp_plan *mirt_nufft_interp_plan(mirt_nufft *p);
+
+/* mirt_interp_plan_autotune on the NUFFT's interpolation plan. */
+int mirt_nufft_autotune(mirt_nufft *p, void *stream);
 
 int mirt_nufft_destroy(mirt_nufft *p);
 

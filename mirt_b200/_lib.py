@@ -57,6 +57,8 @@ _SIGS = {
                                  _i32, _dp, _dp, _vp], C.c_int),
     "mirt_interp_plan_forward": ([_vp, _vp, _vp, _vp], C.c_int),
     "mirt_interp_plan_adjoint": ([_vp, _vp, _vp, _vp], C.c_int),
+    "mirt_interp_plan_autotune": ([_vp, _vp], C.c_int),
+    "mirt_interp_plan_config": ([_vp, _i32p, _i32], C.c_int),
     "mirt_interp_plan_destroy": ([_vp], C.c_int),
     "mirt_nufft_create": ([C.POINTER(_vp), _i32, _i32p, _i32p, _i32p, _i32p, _dp, _dp, _i64,
                            _i64p, _i32, _i32, _vp], C.c_int),
@@ -65,6 +67,7 @@ _SIGS = {
     "mirt_nufft_forward_host": ([_vp, _fp, _fp, _vp], C.c_int),
     "mirt_nufft_adjoint_host": ([_vp, _fp, _fp, _vp], C.c_int),
     "mirt_nufft_interp_plan": ([_vp], _vp),
+    "mirt_nufft_autotune": ([_vp, _vp], C.c_int),
     "mirt_nufft_destroy": ([_vp], C.c_int),
     "mirt_minmax_kb_table": ([_i32, _i32, _i32, _i32, _dp, _dp], C.c_int),
     "mirt_minmax_kb_scale": ([_i32, _i32, _i32, _dp, _dp], C.c_int),

@@ -152,9 +152,9 @@ struct mirt_interp_plan {
 
 namespace {
 
-// Tile extents and launch shapes.  The spread accumulates a tile of
-// npts points x CW coils in shared memory (~64 KB); its warps own bands of
-// the slowest tiled dimension, so that dimension is a multiple of 8 rows.
+// Launch shapes and tiling.  Samples are binned on 8-point bins (64 in 1D);
+// the spread runs one warp per tile (lanes = coils; the tile accumulator is
+// sized to keep several CTAs resident per SM).
 void choose_config(mirt_interp_plan *P) {
   InterpArgs &a = P->a;
   Tiling &t = P->t;
@@ -170,90 +170,90 @@ void choose_config(mirt_interp_plan *P) {
   if (sb < 32) sb = 32;
   if (sb > 256) sb = 256;
   lg.sb = sb;
-  lg.tab_smem = 0;
   lg.grid = 0;
 
-  int T[MIRT_DMAX] = {1, 1, 1};
+  int B[MIRT_DMAX] = {1, 1, 1}, T[MIRT_DMAX] = {1, 1, 1};
   if (D == 1) {
-    T[0] = 65536 / (cw * 8);
+    B[0] = 64;
+    T[0] = cw == 32 ? 64 : 256;
   } else if (D == 2) {
-    switch (cw) {
-      case 32: T[0] = 16; T[1] = 16; break;
-      case 8: T[0] = 32; T[1] = 32; break;
-      case 4: T[0] = 32; T[1] = 32; break;
-      default: T[0] = 64; T[1] = 64; break;
-    }
+    B[0] = B[1] = 8;
+    const int e = cw == 32 ? 8 : cw == 8 ? 16 : 32;
+    T[0] = T[1] = e;
   } else {
-    switch (cw) {
-      case 32: T[0] = 8; T[1] = 4; T[2] = 8; break;
-      case 8: T[0] = 16; T[1] = 8; T[2] = 8; break;
-      case 4: T[0] = 16; T[1] = 16; T[2] = 8; break;
-      default: T[0] = 32; T[1] = 16; T[2] = 16; break;
-    }
+    B[0] = B[1] = B[2] = 8;
+    T[0] = T[1] = T[2] = 8;
+    if (cw <= 4) T[0] = 16;
   }
   for (int d = 0; d < D; d++) {
-    if (T[d] > a.g.K[d]) T[d] = a.g.K[d];
-    if (T[d] < 1) T[d] = 1;
+    if (B[d] > a.g.K[d]) B[d] = a.g.K[d];
+    const int kr = (a.g.K[d] + B[d] - 1) / B[d] * B[d];
+    if (T[d] > kr) T[d] = kr;
+    T[d] = (T[d] + B[d] - 1) / B[d] * B[d];
   }
   Launch &ls = P->ls;
-  ls.threads = threads;
+  ls.threads = 32;
   ls.cw = cw;
-  ls.sb = 64;
-  ls.tab_smem = 0;
-  for (int d = 0; d < MIRT_DMAX; d++) ls.P[d] = 1;
+  ls.sb = cw == 32 ? 16 : 32;
+  ls.grid = 0;
+  t.nbins = 1;
+  t.ntiles = 1;
   for (int d = 0; d < MIRT_DMAX; d++) {
+    t.B[d] = d < D ? B[d] : 1;
+    t.nbin[d] = d < D ? (a.g.K[d] + B[d] - 1) / B[d] : 1;
     t.T[d] = d < D ? T[d] : 1;
     t.nb[d] = d < D ? (a.g.K[d] + T[d] - 1) / T[d] : 1;
+    t.nbins *= t.nbin[d];
+    t.ntiles *= t.nb[d];
   }
-  t.ntiles = t.nb[0] * t.nb[1] * t.nb[2];
 }
 
-// Source bins per dimension: tiles whose samples (binned by the first tap
+// Source bins per dimension: bins whose samples (binned by the first tap
 // koff mod K) can have a tap inside tile b, i.e. koff in [lo-J+1, hi-1] mod K.
 int build_sources(mirt_interp_plan *P, cudaStream_t st) {
   const InterpArgs &a = P->a;
   Tiling &t = P->t;
+  std::vector<int> src[MIRT_DMAX], nsrc[MIRT_DMAX];
   for (int d = 0; d < MIRT_DMAX; d++) {
     const int nb = t.nb[d];
-    std::vector<int> src((size_t)nb * MIRT_SRCMAX, 0), nsrc(nb, 1);
-    if (d < a.g.D) {
-      const int K = a.g.K[d], T = t.T[d], J = a.g.J[d];
-      for (int b = 0; b < nb; b++) {
-        const int lo = b * T, hi = std::min(lo + T, K);
-        const long long n = (long long)(hi - lo) + J - 1;
-        std::vector<int> list;
-        if (n >= K) {
-          for (int i = 0; i < nb; i++) list.push_back(i);
-        } else {
-          int x0 = ((lo - J + 1) % K + K) % K;
-          std::set<int> seen;
-          for (long long i = 0; i < n; i++) {
-            const int x = (int)((x0 + i) % K);
-            const int bb = x / T;
-            if (!seen.count(bb)) {
-              seen.insert(bb);
-              list.push_back(bb);
-            }
+    src[d].assign((size_t)nb * MIRT_SRCMAX, 0);
+    nsrc[d].assign(nb, 1);
+    if (d >= a.g.D) continue;
+    const int K = a.g.K[d], T = t.T[d], B = t.B[d], J = a.g.J[d];
+    for (int b = 0; b < nb; b++) {
+      const int lo = b * T, hi = std::min(lo + T, K);
+      const long long n = (long long)(hi - lo) + J - 1;
+      std::vector<int> list;
+      if (n >= K) {
+        for (int i = 0; i < t.nbin[d]; i++) list.push_back(i);
+      } else {
+        const int x0 = ((lo - J + 1) % K + K) % K;
+        std::set<int> seen;
+        for (long long i = 0; i < n; i++) {
+          const int bb = (int)((x0 + i) % K) / B;
+          if (!seen.count(bb)) {
+            seen.insert(bb);
+            list.push_back(bb);
           }
         }
-        if ((int)list.size() > MIRT_SRCMAX)
-          return fail(MIRT_ERR_ARG, "tile too small for the interpolator width");
-        nsrc[b] = (int)list.size();
-        for (size_t i = 0; i < list.size(); i++) src[(size_t)b * MIRT_SRCMAX + i] = list[i];
       }
-    } else {
-      src[0] = 0;
+      if ((int)list.size() > MIRT_SRCMAX)
+        return fail(MIRT_ERR_ARG, "spread tile spans too many sort bins");
+      nsrc[d][b] = (int)list.size();
+      for (size_t i = 0; i < list.size(); i++) src[d][(size_t)b * MIRT_SRCMAX + i] = list[i];
     }
-    CK(P->src[d].alloc(src.size() * sizeof(int)));
-    CK(P->nsrc[d].alloc(nsrc.size() * sizeof(int)));
-    CK(cudaMemcpyAsync(P->src[d].p, src.data(), src.size() * sizeof(int),
+  }
+  for (int d = 0; d < MIRT_DMAX; d++) {
+    CK(P->src[d].alloc(src[d].size() * sizeof(int)));
+    CK(P->nsrc[d].alloc(nsrc[d].size() * sizeof(int)));
+    CK(cudaMemcpyAsync(P->src[d].p, src[d].data(), src[d].size() * sizeof(int),
                        cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(P->nsrc[d].p, nsrc.data(), nsrc.size() * sizeof(int),
+    CK(cudaMemcpyAsync(P->nsrc[d].p, nsrc[d].data(), nsrc[d].size() * sizeof(int),
                        cudaMemcpyHostToDevice, st));
     t.src[d] = P->src[d].as<int>();
     t.nsrc[d] = P->nsrc[d].as<int>();
   }
-  // the host vectors above are released at scope exit: wait for the copies
+  // the host vectors are released at scope exit: wait for the copies
   CK(cudaStreamSynchronize(st));
   return MIRT_OK;
 }
@@ -315,9 +315,10 @@ int build_task_order(mirt_interp_plan *P, cudaStream_t st) {
   const Tiling &t = P->t;
   const int D = P->a.g.D;
   const long long ntask = (long long)t.ntiles * t.nslice;
-  std::vector<int> bs(ntask + 1);
-  CK(cudaMemcpyAsync(bs.data(), P->bin_start.p, (ntask + 1) * sizeof(int), cudaMemcpyDeviceToHost,
-                     st));
+  const long long nbin_all = (long long)t.nbins * t.nslice;
+  std::vector<int> bs(nbin_all + 1);
+  CK(cudaMemcpyAsync(bs.data(), P->bin_start.p, (nbin_all + 1) * sizeof(int),
+                     cudaMemcpyDeviceToHost, st));
   std::vector<int> src[MIRT_DMAX], nsrc[MIRT_DMAX];
   for (int d = 0; d < MIRT_DMAX; d++) {
     src[d].resize((size_t)t.nb[d] * MIRT_SRCMAX);
@@ -343,9 +344,9 @@ int build_task_order(mirt_interp_plan *P, cudaStream_t st) {
       for (int i1 = 0; i1 < n1; i1++)
         for (int i0 = 0; i0 < n0; i0++) {
           long long st_ = src[0][b[0] * MIRT_SRCMAX + i0];
-          if (D > 1) st_ += (long long)src[1][b[1] * MIRT_SRCMAX + i1] * t.nb[0];
-          if (D > 2) st_ += (long long)src[2][b[2] * MIRT_SRCMAX + i2] * t.nb[0] * t.nb[1];
-          const long long bin = slice * t.ntiles + st_;
+          if (D > 1) st_ += (long long)src[1][b[1] * MIRT_SRCMAX + i1] * t.nbin[0];
+          if (D > 2) st_ += (long long)src[2][b[2] * MIRT_SRCMAX + i2] * t.nbin[0] * t.nbin[1];
+          const long long bin = slice * t.nbins + st_;
           w += bs[bin + 1] - bs[bin];
         }
     work[task] = {-w, (int)task};
@@ -382,7 +383,7 @@ int plan_finish(mirt_interp_plan *P, long long Mtot, const long long *moff, int 
   choose_config(P);
   int rc = build_sources(P, st);
   if (rc) return rc;
-  const long long nbins = (long long)P->t.ntiles * nslice;
+  const long long nbins = (long long)P->t.nbins * nslice;
   if (nbins >= (1ll << 31)) return fail(MIRT_ERR_ARG, "too many grid tiles");
   CK(P->keys.alloc(std::max<long long>(Mtot, 1) * sizeof(uint32_t)));
   CK(P->perm.alloc(std::max<long long>(Mtot, 1) * sizeof(int)));
@@ -416,6 +417,54 @@ int plan_finish(mirt_interp_plan *P, long long Mtot, const long long *moff, int 
   int rc2 = build_task_order(P, st);
   if (rc2) return rc2;
   CK(query_gather_grid(a, P->lg));
+  return MIRT_OK;
+}
+
+// Re-tile the spread (tiles of T[d] points, multiples of the sort bins) and
+// rebuild its source lists and CTA order; the sort itself is unchanged.
+int set_spread_tiles(mirt_interp_plan *P, const int *T, cudaStream_t st) {
+  Tiling &t = P->t;
+  const int D = P->a.g.D;
+  t.ntiles = 1;
+  for (int d = 0; d < MIRT_DMAX; d++) {
+    t.T[d] = d < D ? T[d] : 1;
+    t.nb[d] = d < D ? (P->a.g.K[d] + t.T[d] - 1) / t.T[d] : 1;
+    t.ntiles *= t.nb[d];
+  }
+  int rc = build_sources(P, st);
+  if (rc) return rc;
+  return build_task_order(P, st);
+}
+
+struct SpreadCand {
+  int T[MIRT_DMAX];
+  int threads, sb;
+};
+
+// Time `fn` (one launch) on the stream: one warm-up, then the best of 3.
+template <class F>
+int time_launch(F fn, cudaStream_t st, float *ms) {
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  *ms = 1e30f;
+  for (int it = 0; it < 4; it++) {
+    CK(cudaEventRecord(e0, st));
+    cudaError_t e = fn();
+    if (e != cudaSuccess) {
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      cudaGetLastError();
+      return fail(MIRT_ERR_CUDA, std::string("autotune launch: ") + cudaGetErrorString(e));
+    }
+    CK(cudaEventRecord(e1, st));
+    CK(cudaEventSynchronize(e1));
+    float t = 0;
+    CK(cudaEventElapsedTime(&t, e0, e1));
+    if (it > 0 && t < *ms) *ms = t;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
   return MIRT_OK;
 }
 
@@ -516,6 +565,116 @@ int mirt_interp_plan_adjoint(mirt_interp_plan *P, const void *fm, void *ck, void
   if (!P) return fail(MIRT_ERR_ARG, "plan is NULL");
   CK(launch_spread(P->a, P->t, P->ls, P->bin_start.as<int>(), static_cast<const float2 *>(fm),
                    static_cast<float2 *>(ck), as_stream(stream)));
+  return MIRT_OK;
+}
+
+int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
+  if (!P) return fail(MIRT_ERR_ARG, "plan is NULL");
+  cudaStream_t st = as_stream(stream);
+  const InterpArgs &a = P->a;
+  const int D = a.g.D, cw = P->ls.cw;
+  const long long ngrid = (long long)P->t.nslice * a.grid_elems;
+  const long long nsamp = a.Mtot * (long long)a.C;
+  if (ngrid == 0 || nsamp == 0) return MIRT_OK;
+  DMem grid, samp;
+  CK(grid.alloc(ngrid * sizeof(float2)));
+  CK(samp.alloc(nsamp * sizeof(float2)));
+  CK(cudaMemsetAsync(samp.p, 0, nsamp * sizeof(float2), st));
+  CK(cudaMemsetAsync(grid.p, 0, ngrid * sizeof(float2), st));
+  // spread candidates: tile shape (multiples of the 8-point bins), warps, batch
+  std::vector<SpreadCand> cands;
+  auto add = [&](int t0, int t1, int t2, int threads, int sb) {
+    SpreadCand c{{t0, t1, t2}, threads, sb};
+    for (int d = 0; d < D; d++) {
+      const int kr = (a.g.K[d] + P->t.B[d] - 1) / P->t.B[d] * P->t.B[d];
+      if (c.T[d] > kr) c.T[d] = kr;
+      c.T[d] = (c.T[d] + P->t.B[d] - 1) / P->t.B[d] * P->t.B[d];
+    }
+    size_t npts = 1;
+    for (int d = 0; d < D; d++) npts *= c.T[d];
+    int SJ = 0;
+    for (int d = 0; d < D; d++) SJ += a.g.J[d];
+    const size_t sm = npts * cw * 8 + (size_t)sb * SJ * 12 + (size_t)sb * 8 + 16 + (size_t)sb * cw * 8 + 16;
+    if (sm <= 200 * 1024) cands.push_back(c);
+  };
+  if (D == 1) {
+    for (int t0 : {64, 128, 256, 512})
+      for (int th : {32, 64}) add(t0, 1, 1, th, 32);
+  } else if (D == 2) {
+    const int sbs = cw == 32 ? 16 : 32;
+    for (int t0 : {8, 16, 32})
+      for (int t1 : {8, 16, 32}) {
+        add(t0, t1, 1, 32, sbs);
+        if (t1 >= 16) add(t0, t1, 1, 64, sbs);
+        if (t1 >= 32) add(t0, t1, 1, 128, sbs);
+      }
+    add(8, 8, 1, 32, 2 * sbs);
+  } else {
+    for (int t0 : {8, 16})
+      for (int t1 : {8, 16})
+        for (int t2 : {8, 16}) {
+          add(t0, t1, t2, 32, 32);
+          if (t2 >= 16) add(t0, t1, t2, 64, 32);
+        }
+  }
+  SpreadCand best{};
+  float best_ms = 1e30f;
+  for (const SpreadCand &c : cands) {
+    int rc = set_spread_tiles(P, c.T, st);
+    if (rc) continue;
+    P->ls.threads = c.threads;
+    P->ls.sb = c.sb;
+    float ms = 0;
+    rc = time_launch([&]() {
+      return launch_spread(P->a, P->t, P->ls, P->bin_start.as<int>(), samp.as<float2>(),
+                           grid.as<float2>(), st);
+    }, st, &ms);
+    if (rc) return rc;
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = c;
+    }
+  }
+  if (best_ms < 1e30f) {
+    int rc = set_spread_tiles(P, best.T, st);
+    if (rc) return rc;
+    P->ls.threads = best.threads;
+    P->ls.sb = best.sb;
+  }
+  // gather candidates: CTA size and staged batch
+  Launch bestg = P->lg;
+  float bestg_ms = 1e30f;
+  for (int threads : {128, 256}) {
+    for (int per : {8, 16, 32}) {
+      Launch l = P->lg;
+      l.threads = threads;
+      int sb = threads / l.cw * per;
+      if (sb < 32) sb = 32;
+      if (sb > 512) continue;
+      l.sb = sb;
+      l.grid = 0;
+      CK(query_gather_grid(P->a, l));
+      float ms = 0;
+      int rc = time_launch([&]() {
+        return launch_gather(P->a, l, grid.as<float2>(), samp.as<float2>(), st);
+      }, st, &ms);
+      if (rc) return rc;
+      if (ms < bestg_ms) {
+        bestg_ms = ms;
+        bestg = l;
+      }
+    }
+  }
+  P->lg = bestg;
+  CK(cudaStreamSynchronize(st));
+  return MIRT_OK;
+}
+
+int mirt_interp_plan_config(mirt_interp_plan *P, int32_t *out, int32_t n) {
+  if (!P || !out) return fail(MIRT_ERR_ARG, "NULL argument");
+  const int32_t v[12] = {P->t.T[0], P->t.T[1], P->t.T[2], P->ls.threads, P->ls.sb, P->ls.cw,
+                         P->lg.threads, P->lg.sb, P->lg.grid, P->t.B[0], P->t.B[1], P->t.B[2]};
+  for (int i = 0; i < n && i < 12; i++) out[i] = v[i];
   return MIRT_OK;
 }
 
@@ -1164,6 +1323,11 @@ int mirt_nufft_adjoint_host(mirt_nufft *p, const float *X, float *x, void *strea
 }
 
 mirt_interp_plan *mirt_nufft_interp_plan(mirt_nufft *p) { return p ? p->ip : nullptr; }
+
+int mirt_nufft_autotune(mirt_nufft *p, void *stream) {
+  if (!p) return fail(MIRT_ERR_ARG, "nufft is NULL");
+  return mirt_interp_plan_autotune(p->ip, stream);
+}
 
 int mirt_nufft_destroy(mirt_nufft *p) {
   if (p) {

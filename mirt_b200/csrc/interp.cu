@@ -10,15 +10,15 @@ namespace mirt {
 __global__ void bin_keys_kernel(InterpArgs a, Tiling t, uint32_t *keys) {
   const long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (m >= a.Mtot) return;
-  int tile = 0, mul = 1;
+  int bin = 0, mul = 1;
   for (int d = 0; d < a.g.D; d++) {
     const double td = a.tm[(long long)d * a.Mtot + m];
     const int k0 = wrapk(koff_of(td, a.g.J[d]), a.g.K[d]);
-    tile += (k0 / t.T[d]) * mul;
-    mul *= t.nb[d];
+    bin += (k0 / t.B[d]) * mul;
+    mul *= t.nbin[d];
   }
   const int s = a.slice_id ? a.slice_id[m] : 0;
-  keys[m] = (uint32_t)s * (uint32_t)t.ntiles + (uint32_t)tile;
+  keys[m] = (uint32_t)s * (uint32_t)t.nbins + (uint32_t)bin;
 }
 
 cudaError_t launch_bin_keys(const InterpArgs &a, const Tiling &t, uint32_t *keys,

@@ -28,33 +28,37 @@ struct InterpArgs {
   long long grid_elems;  // prod(K) * C  (one slice's grid, in float2)
 };
 
-// Tiling of the grid used by the bin sort and the spread.
+// Tiling of the grid.  Samples are sorted into bins of B[d] grid points per
+// dimension (by the slice and the wrapped first tap of each sample); the
+// spread works on tiles of T[d] = multiple of B[d] points, so the tile shape
+// can be tuned without re-sorting.
 struct Tiling {
-  int T[MIRT_DMAX];      // tile extent per dimension
+  int B[MIRT_DMAX];      // bin extent per dimension
+  int nbin[MIRT_DMAX];   // bins per dimension
+  int nbins;             // prod(nbin): bins per slice
+  int T[MIRT_DMAX];      // spread tile extent per dimension (multiple of B)
   int nb[MIRT_DMAX];     // tiles per dimension
-  int ntiles;            // prod(nb)
+  int ntiles;            // prod(nb): tiles per slice
   int nslice;
   // source-bin lists per dimension: for tile index b of dimension d,
-  // src[d][b*MIRT_SRCMAX + i], i < nsrc[d][b], are the tiles whose samples
-  // (binned by their first tap) can reach tile b.
+  // src[d][b*MIRT_SRCMAX + i], i < nsrc[d][b], are the bins whose samples
+  // (binned by their first tap) can have a tap in tile b.
   const int *src[MIRT_DMAX];
   const int *nsrc[MIRT_DMAX];
   // spread CTA order: task = slice * ntiles + tile, heaviest first (or nullptr)
   const int *task_order;
 };
-#define MIRT_SRCMAX 8
+#define MIRT_SRCMAX 16
 
 // Launch tuning chosen by the host (autotuned per geometry).
 struct Launch {
-  int threads;   // CTA size (multiple of 32)
-  int cw;        // lanes per sample group (= coils handled in parallel)
-  int sb;        // samples per staged batch
-  int grid;      // CTAs for the gather (persistent)
-  int P[MIRT_DMAX];  // spread: owner groups per dimension (prod * cw = threads)
-  int tab_smem;  // 1: stage tables in shared memory
+  int threads;   // CTA size (multiple of 32); the spread gives each warp a band
+  int cw;        // coil lanes per sample group
+  int sb;        // samples per staged batch (even)
+  int grid;      // CTAs for the persistent gather (0: size from occupancy)
 };
 
-// Compute the sort key of every sample: slice * ntiles + tile of its first tap.
+// Compute the sort key of every sample: slice * nbins + bin of its first tap.
 cudaError_t launch_bin_keys(const InterpArgs &a, const Tiling &t, uint32_t *keys,
                             cudaStream_t st);
 

@@ -441,9 +441,9 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t, Lau
       const int i = r % ns[d];
       r /= ns[d];
       stile += t.src[d][b[d] * MIRT_SRCMAX + i] * mul;
-      mul *= t.nb[d];
+      mul *= t.nbin[d];
     }
-    const int bin = slice * t.ntiles + stile;
+    const int bin = slice * t.nbins + stile;
     const long long beg = bin_start[bin], end = bin_start[bin + 1];
     for (long long pos0 = beg; pos0 < end; pos0 += sb) {
       const int nb = (int)min((long long)sb, end - pos0);
@@ -482,6 +482,37 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t, Lau
               fast1 ? 0u : tap_mask<SUB>(k10, Jd[0], g.K[0], lo[0], 0, ext[0], ls);
           if (!fast1 && !m1) continue;
           if constexpr (D == 2) {
+            if constexpr (JT > 0 && SUB == 1) {
+              if (fast1) {
+                // all J1 columns inside the tile: coefficient pairs in registers,
+                // LDS.64 + 2 FFMA2 + STS.64 per tap at compile-time strides
+                float2 wr[JT], wi[JT];
+#pragma unroll
+                for (int j1 = 0; j1 < JT; j1++) {
+                  const float2 w = Ws[j1];
+                  wr[j1] = make_float2(w.x, w.x);
+                  wi[j1] = make_float2(w.y, -w.y);
+                }
+                float2 *base = acc + l10 * CW + lc;
+                unsigned m2 = mb;
+                while (m2) {
+                  const int j2 = __ffs(m2) - 1;
+                  m2 &= m2 - 1;
+                  const int l2 = tap_local(Ks[Jd[0]], j2, g.K[1], lo[1]);
+                  const float2 v2 = cw_mul<REAL>(Ws[Jd[0] + j2], f);
+                  const float2 v2s = make_float2(v2.y, v2.x);
+                  float2 *p = base + (size_t)l2 * T0 * CW;
+#pragma unroll
+                  for (int j1 = 0; j1 < JT; j1++) {
+                    float2 A = p[j1 * CW];
+                    A = __ffma2_rn(wr[j1], v2, A);
+                    if (!REAL) A = __ffma2_rn(wi[j1], v2s, A);
+                    p[j1 * CW] = A;
+                  }
+                }
+                continue;
+              }
+            }
             unsigned m2 = mb;
             while (m2) {
               const int j2 = __ffs(m2) - 1;

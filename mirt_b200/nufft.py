@@ -65,6 +65,14 @@ def minmax_kb_scale(N: int, J: int, K: int) -> np.ndarray:
     return re + 1j * im
 
 
+def _plan_config(lib, handle) -> dict:
+    v = (C.c_int32 * 12)()
+    check(lib.mirt_interp_plan_config(handle, v, 12))
+    return {"spread_tile": [v[0], v[1], v[2]], "spread_threads": v[3], "spread_batch": v[4],
+            "coil_lanes": v[5], "gather_threads": v[6], "gather_batch": v[7],
+            "gather_ctas": v[8], "sort_bin": [v[9], v[10], v[11]]}
+
+
 class InterpPlan:
     """Plan of the table gather / spread for fixed tables and trajectory.
 
@@ -134,6 +142,14 @@ class InterpPlan:
                                                 C.c_void_p(out.data_ptr()), _stream_ptr(stream)))
         return out
 
+    def autotune(self, stream=None):
+        """Pick the fastest gather / spread launch shapes for this trajectory."""
+        check(self.lib.mirt_interp_plan_autotune(self.handle, _stream_ptr(stream)))
+        return self.config()
+
+    def config(self):
+        return _plan_config(self.lib, self.handle)
+
     def close(self):
         if getattr(self, "handle", None):
             self.lib.mirt_interp_plan_destroy(self.handle)
@@ -198,6 +214,14 @@ class NufftPlan:
         check(self.lib.mirt_nufft_adjoint(self.handle, C.c_void_p(X.data_ptr()),
                                           C.c_void_p(out.data_ptr()), _stream_ptr(stream)))
         return out
+
+    def autotune(self, stream=None):
+        """Pick the fastest gather / spread launch shapes for this trajectory."""
+        check(self.lib.mirt_nufft_autotune(self.handle, _stream_ptr(stream)))
+        return self.config()
+
+    def config(self):
+        return _plan_config(self.lib, self.lib.mirt_nufft_interp_plan(self.handle))
 
     def forward_host(self, x: np.ndarray, out: np.ndarray | None = None, stream=None):
         """host complex64 image (device layout) -> host complex64 samples."""

@@ -180,3 +180,36 @@ def test_plan_multislice_uneven():
         else:
             assert not got_a.any()
     plan.close()
+
+
+@pytest.mark.parametrize("C", [1, 8, 32])
+def test_autotuned_plan_keeps_parity(C):
+    """Every tile shape the autotuner may pick gives the same (correct) result."""
+    import torch
+    rng = np.random.default_rng(31 + C)
+    K, J, L = [128, 96], [6, 6], [1024, 1024]
+    h = [mb.minmax_kb_table(64, 6, 128, 1024), mb.minmax_kb_table(48, 6, 96, 1024)]
+    counts = [3000, 1700]
+    moff = np.concatenate([[0], np.cumsum(counts)])
+    tm = np.concatenate([rng.uniform(-70, 70, (c, 2)) for c in counts])
+    plan = mb.InterpPlan(K, J, L, h, tm, C, slice_moff=moff)
+    fm = rng.standard_normal((len(tm), C)) + 1j * rng.standard_normal((len(tm), C))
+    fm_d = torch.from_numpy(fm.astype(np.complex64)).cuda()
+    before = plan.adjoint(fm_d).cpu().numpy()
+    cfg = plan.autotune()
+    assert cfg["spread_threads"] % 32 == 0
+    after = plan.adjoint(fm_d).cpu().numpy()
+    for s in range(2):
+        sl = slice(moff[s], moff[s + 1])
+        ref = oracle.interp_adj(fm[sl], h, J, L, tm[sl], K, 0, impl=ref_impl())
+        got = np.transpose(after[s], (1, 0, 2)).reshape(-1, C, order="F")
+        assert rel_l2(got, ref) <= ADJ_TOL
+    assert rel_l2(after, before) <= ADJ_TOL
+    ck = rng.standard_normal(plan.grid_shape) + 1j * rng.standard_normal(plan.grid_shape)
+    out = plan.forward(torch.from_numpy(ck.astype(np.complex64)).cuda()).cpu().numpy()
+    for s in range(2):
+        sl = slice(moff[s], moff[s + 1])
+        cks = np.transpose(ck[s], (1, 0, 2)).reshape(-1, C, order="F")
+        ref = oracle.interp_for(cks, h, J, L, tm[sl], K, 0, impl=ref_impl())
+        assert rel_l2(out[sl], ref) <= FWD_TOL
+    plan.close()
