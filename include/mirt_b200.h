@@ -186,15 +186,16 @@ int mirt_interp_plan_forward(mirt_interp_plan *plan, const void *ck, void *fm, v
 int mirt_interp_plan_adjoint(mirt_interp_plan *plan, const void *fm, void *ck, void *stream);
 
 /* Autotune: time candidate spread tile shapes (multiples of the 8-point sort
- * bins), warps per spread CTA and staged batch sizes, and gather CTA / batch
- * sizes, on this plan's trajectory; keep the fastest.  Allocates a scratch
+ * bins), warps per spread CTA, staged batch sizes and the split size of dense
+ * tiles, and gather CTA / batch sizes, on this plan's trajectory; keep the
+ * fastest.  Allocates a scratch
  * grid and sample buffer for the duration of the call.  Results stay
  * bitwise deterministic for any choice. */
 int mirt_interp_plan_autotune(mirt_interp_plan *plan, void *stream);
 
-/* Current launch configuration: up to 12 values
+/* Current launch configuration: up to 14 values
  * {T1, T2, T3, spread threads, spread batch, coil lanes, gather threads,
- *  gather batch, gather CTAs, B1, B2, B3}. */
+ *  gather batch, gather CTAs, B1, B2, B3, split chunk, spread tasks}. */
 int mirt_interp_plan_config(mirt_interp_plan *plan, int32_t *out, int32_t n);
 
 int mirt_interp_plan_destroy(mirt_interp_plan *plan);

@@ -146,7 +146,9 @@ struct mirt_interp_plan {
   Tiling t{};
   Launch lg{}, ls{};
   DMem tm, slice, perm, bin_start, tab[MIRT_DMAX], phase, src[MIRT_DMAX], nsrc[MIRT_DMAX];
-  DMem keys, sorttmp, moff, task_order;
+  DMem keys, sorttmp, moff;
+  DMem task_tile, task_range, task_slot, red, scratch;
+  int split_chunk = 1024;  // sample visits per spread task before a tile is split
   std::vector<long long> moff_host;
 };
 
@@ -308,13 +310,15 @@ int plan_geometry(mirt_interp_plan *P, int D, const int *K, const int *J, const 
   return MIRT_OK;
 }
 
-// Spread CTAs in order of decreasing work (samples over each tile's source
-// bins), so that the dense k-space centre tiles start first and do not form
-// the tail of the launch.
-int build_task_order(mirt_interp_plan *P, cudaStream_t st) {
-  const Tiling &t = P->t;
+// Spread work list.  The work of a tile is the number of sample visits over
+// its source bins.  Tiles with more than split_chunk visits (the dense k-space
+// centre of radial and kooshball trajectories) are split into tasks of
+// split_chunk visits whose partial tiles a reduction sums in fixed order, so
+// no single CTA serialises a dense tile.  Tasks run heaviest first.
+int build_tasks(mirt_interp_plan *P, cudaStream_t st) {
+  Tiling &t = P->t;
   const int D = P->a.g.D;
-  const long long ntask = (long long)t.ntiles * t.nslice;
+  const long long ntile_all = (long long)t.ntiles * t.nslice;
   const long long nbin_all = (long long)t.nbins * t.nslice;
   std::vector<int> bs(nbin_all + 1);
   CK(cudaMemcpyAsync(bs.data(), P->bin_start.p, (nbin_all + 1) * sizeof(int),
@@ -329,8 +333,15 @@ int build_task_order(mirt_interp_plan *P, cudaStream_t st) {
                        cudaMemcpyDeviceToHost, st));
   }
   CK(cudaStreamSynchronize(st));
-  std::vector<std::pair<long long, int>> work(ntask);
-  for (long long task = 0; task < ntask; task++) {
+  const long long chunk = std::max(32, P->split_chunk);
+  struct Task {
+    long long work;
+    int tile, v0, v1, slot;
+  };
+  std::vector<Task> tasks;
+  std::vector<int4> red;
+  int nslot = 0;
+  for (long long task = 0; task < ntile_all; task++) {
     const int tile = (int)(task % t.ntiles);
     const long long slice = task / t.ntiles;
     int b[MIRT_DMAX] = {0, 0, 0}, r = tile;
@@ -349,16 +360,55 @@ int build_task_order(mirt_interp_plan *P, cudaStream_t st) {
           const long long bin = slice * t.nbins + st_;
           w += bs[bin + 1] - bs[bin];
         }
-    work[task] = {-w, (int)task};
+    if (w >= (1ll << 31)) return fail(MIRT_ERR_ARG, "too many samples in one tile");
+    if (w <= chunk) {
+      tasks.push_back({w, (int)task, 0, (int)w, -1});
+    } else {
+      const int np = (int)((w + chunk - 1) / chunk);
+      red.push_back(make_int4((int)task, nslot, np, 0));
+      for (int i = 0; i < np; i++) {
+        const long long v0 = i * chunk, v1 = std::min(w, v0 + chunk);
+        tasks.push_back({v1 - v0, (int)task, (int)v0, (int)v1, nslot + i});
+      }
+      nslot += np;
+    }
   }
-  std::stable_sort(work.begin(), work.end());
-  std::vector<int> order(ntask);
-  for (long long i = 0; i < ntask; i++) order[i] = work[i].second;
-  CK(P->task_order.alloc(std::max<long long>(ntask, 1) * sizeof(int)));
-  CK(cudaMemcpyAsync(P->task_order.p, order.data(), ntask * sizeof(int), cudaMemcpyHostToDevice,
-                     st));
+  std::stable_sort(tasks.begin(), tasks.end(),
+                   [](const Task &x, const Task &y) { return x.work > y.work; });
+  const size_t nt = tasks.size();
+  std::vector<int> tt(nt), ts(nt);
+  std::vector<int2> tr(nt);
+  for (size_t i = 0; i < nt; i++) {
+    tt[i] = tasks[i].tile;
+    tr[i] = make_int2(tasks[i].v0, tasks[i].v1);
+    ts[i] = tasks[i].slot;
+  }
+  CK(P->task_tile.alloc(std::max<size_t>(nt, 1) * sizeof(int)));
+  CK(P->task_range.alloc(std::max<size_t>(nt, 1) * sizeof(int2)));
+  CK(P->task_slot.alloc(std::max<size_t>(nt, 1) * sizeof(int)));
+  CK(P->red.alloc(std::max<size_t>(red.size(), 1) * sizeof(int4)));
+  if (nt) {
+    CK(cudaMemcpyAsync(P->task_tile.p, tt.data(), nt * sizeof(int), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(P->task_range.p, tr.data(), nt * sizeof(int2), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(P->task_slot.p, ts.data(), nt * sizeof(int), cudaMemcpyHostToDevice, st));
+  }
+  if (!red.empty())
+    CK(cudaMemcpyAsync(P->red.p, red.data(), red.size() * sizeof(int4), cudaMemcpyHostToDevice,
+                       st));
+  size_t npts = 1;
+  for (int d = 0; d < D; d++) npts *= t.T[d];
+  const int cw = P->ls.cw;
+  const size_t nchunk = (P->a.C + cw - 1) / cw;
+  const size_t sbytes = (size_t)nslot * nchunk * npts * cw * sizeof(float2);
+  if (P->scratch.bytes < sbytes) CK(P->scratch.alloc(sbytes));
   CK(cudaStreamSynchronize(st));
-  P->t.task_order = P->task_order.as<int>();
+  t.ntask = (int)nt;
+  t.task_tile = P->task_tile.as<int>();
+  t.task_range = P->task_range.as<int2>();
+  t.task_slot = P->task_slot.as<int>();
+  t.nred = (int)red.size();
+  t.red = P->red.as<int4>();
+  t.scratch = P->scratch.as<float2>();
   return MIRT_OK;
 }
 
@@ -414,7 +464,7 @@ int plan_finish(mirt_interp_plan *P, long long Mtot, const long long *moff, int 
   }
   a.perm = P->perm.as<int>();
   P->sorttmp.release();
-  int rc2 = build_task_order(P, st);
+  int rc2 = build_tasks(P, st);
   if (rc2) return rc2;
   CK(query_gather_grid(a, P->lg));
   return MIRT_OK;
@@ -433,7 +483,7 @@ int set_spread_tiles(mirt_interp_plan *P, const int *T, cudaStream_t st) {
   }
   int rc = build_sources(P, st);
   if (rc) return rc;
-  return build_task_order(P, st);
+  return build_tasks(P, st);
 }
 
 struct SpreadCand {
@@ -641,6 +691,29 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
     P->ls.threads = best.threads;
     P->ls.sb = best.sb;
   }
+  // split size of heavy tiles (sample visits per spread task)
+  {
+    int best_chunk = P->split_chunk;
+    float bc_ms = 1e30f;
+    for (int chunk : {256, 512, 1024, 2048, 4096, 16384}) {
+      P->split_chunk = chunk;
+      int rc = build_tasks(P, st);
+      if (rc) return rc;
+      float ms = 0;
+      rc = time_launch([&]() {
+        return launch_spread(P->a, P->t, P->ls, P->bin_start.as<int>(), samp.as<float2>(),
+                             grid.as<float2>(), st);
+      }, st, &ms);
+      if (rc) return rc;
+      if (ms < bc_ms) {
+        bc_ms = ms;
+        best_chunk = chunk;
+      }
+    }
+    P->split_chunk = best_chunk;
+    int rc = build_tasks(P, st);
+    if (rc) return rc;
+  }
   // gather candidates: CTA size and staged batch
   Launch bestg = P->lg;
   float bestg_ms = 1e30f;
@@ -672,9 +745,10 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
 
 int mirt_interp_plan_config(mirt_interp_plan *P, int32_t *out, int32_t n) {
   if (!P || !out) return fail(MIRT_ERR_ARG, "NULL argument");
-  const int32_t v[12] = {P->t.T[0], P->t.T[1], P->t.T[2], P->ls.threads, P->ls.sb, P->ls.cw,
-                         P->lg.threads, P->lg.sb, P->lg.grid, P->t.B[0], P->t.B[1], P->t.B[2]};
-  for (int i = 0; i < n && i < 12; i++) out[i] = v[i];
+  const int32_t v[14] = {P->t.T[0], P->t.T[1], P->t.T[2], P->ls.threads, P->ls.sb, P->ls.cw,
+                         P->lg.threads, P->lg.sb, P->lg.grid, P->t.B[0], P->t.B[1], P->t.B[2],
+                         P->split_chunk, P->t.ntask};
+  for (int i = 0; i < n && i < 14; i++) out[i] = v[i];
   return MIRT_OK;
 }
 

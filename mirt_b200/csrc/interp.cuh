@@ -45,8 +45,20 @@ struct Tiling {
   // (binned by their first tap) can have a tap in tile b.
   const int *src[MIRT_DMAX];
   const int *nsrc[MIRT_DMAX];
-  // spread CTA order: task = slice * ntiles + tile, heaviest first (or nullptr)
-  const int *task_order;
+  // Spread work list, heaviest first.  Task i covers the sample visits
+  // [task_range[i].x, task_range[i].y) of tile task_tile[i] (= slice * ntiles
+  // + tile; a tile's visits are its source bins' samples in fixed order).  A
+  // tile with one task is written to the grid directly (task_slot = -1);
+  // a heavy tile split into several tasks writes partial tiles to
+  // scratch[slot] and reduction item r sums its red[r].z partials from slot
+  // red[r].y in order into tile red[r].x.  Fixed at plan time: deterministic.
+  int ntask;
+  const int *task_tile;
+  const int2 *task_range;
+  const int *task_slot;
+  int nred;
+  const int4 *red;
+  float2 *scratch;       // [slots][coil chunks][prod(T)][cw]
 };
 #define MIRT_SRCMAX 16
 

@@ -400,7 +400,9 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t, Lau
   // [sb][CW] sample values; sb is even, so this stays 8-byte aligned
   float2 *F = reinterpret_cast<float2 *>(s.sid + sb);
 
-  const int task = t.task_order ? t.task_order[blockIdx.x] : (int)blockIdx.x;
+  const int task = t.task_tile[blockIdx.x];
+  const int2 vr = t.task_range[blockIdx.x];
+  const int slot = t.task_slot[blockIdx.x];
   const int tile = task % t.ntiles;
   const int slice = task / t.ntiles;
   const int c0 = blockIdx.y * CW;
@@ -434,7 +436,8 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t, Lau
   const int T1 = D > 1 ? t.T[1] : 1;
   const int jb0 = D == 1 ? 0 : (D == 2 ? Jd[0] : Jd[0] + Jd[1]);  // first tap of dim BD
 
-  for (int si = 0; si < nsrc_tot; si++) {
+  long long vbase = 0;
+  for (int si = 0; si < nsrc_tot && vbase < vr.y; si++) {
     int r = si, stile = 0, mul = 1;
 #pragma unroll
     for (int d = 0; d < D; d++) {
@@ -444,7 +447,11 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t, Lau
       mul *= t.nbin[d];
     }
     const int bin = slice * t.nbins + stile;
-    const long long beg = bin_start[bin], end = bin_start[bin + 1];
+    const long long b0 = bin_start[bin], b1 = bin_start[bin + 1];
+    // this task's share of the tile's visit sequence
+    const long long beg = b0 + max(0ll, (long long)vr.x - vbase);
+    const long long end = b0 + min(b1 - b0, (long long)vr.y - vbase);
+    vbase += b1 - b0;
     for (long long pos0 = beg; pos0 < end; pos0 += sb) {
       const int nb = (int)min((long long)sb, end - pos0);
       __syncthreads();
@@ -547,6 +554,12 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t, Lau
     }
   }
   __syncthreads();
+  if (slot >= 0) {
+    // partial tile of a split heavy tile: summed later in fixed order
+    float2 *part = t.scratch + ((size_t)slot * gridDim.y + blockIdx.y) * npts * CW;
+    for (int e = threadIdx.x; e < npts * CW; e += blockDim.x) part[e] = acc[e];
+    return;
+  }
   float2 *gout = ck + (long long)slice * a.grid_elems;
   for (int e = threadIdx.x; e < npts * CW; e += blockDim.x) {
     const int pt = e / CW, cc = e - pt * CW;
@@ -558,6 +571,53 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t, Lau
     if (D > 1) kk += (long long)(lo[1] + l2) * g.kstride[1];
     if (D > 2) kk += (long long)(lo[2] + l3) * g.kstride[2];
     gout[kk * C + c0 + cc] = acc[e];
+  }
+}
+
+// Sum the partial tiles of each split heavy tile, in slot order, into the grid.
+template <int D, int CW>
+__global__ void __launch_bounds__(256) spread_reduce_kernel(InterpArgs a, Tiling t,
+                                                            float2 *__restrict__ ck) {
+  const int4 it = t.red[blockIdx.x];
+  const int task = it.x, first = it.y, nparts = it.z;
+  const int tile = task % t.ntiles;
+  const int slice = task / t.ntiles;
+  const Geom &g = a.g;
+  int npts = 1;
+  int lo[MIRT_DMAX] = {0, 0, 0}, ext[MIRT_DMAX] = {1, 1, 1};
+  {
+    int r = tile;
+#pragma unroll
+    for (int d = 0; d < D; d++) {
+      const int bd = r % t.nb[d];
+      r /= t.nb[d];
+      lo[d] = bd * t.T[d];
+      ext[d] = min(t.T[d], g.K[d] - lo[d]);
+      npts *= t.T[d];
+    }
+  }
+  const int T0 = t.T[0];
+  const int T1 = D > 1 ? t.T[1] : 1;
+  const int c0 = blockIdx.y * CW;
+  const size_t stride = (size_t)gridDim.y * npts * CW;
+  const float2 *part = t.scratch + ((size_t)first * gridDim.y + blockIdx.y) * npts * CW;
+  float2 *gout = ck + (long long)slice * a.grid_elems;
+  for (int e = threadIdx.x; e < npts * CW; e += blockDim.x) {
+    const int pt = e / CW, cc = e - pt * CW;
+    const int l1 = pt % T0;
+    const int l2 = D > 1 ? (pt / T0) % T1 : 0;
+    const int l3 = D > 2 ? pt / (T0 * T1) : 0;
+    if (l1 >= ext[0] || l2 >= ext[1] || l3 >= ext[2] || c0 + cc >= a.C) continue;
+    float2 v = part[e];
+    for (int p = 1; p < nparts; p++) {
+      const float2 w = part[p * stride + e];
+      v.x += w.x;
+      v.y += w.y;
+    }
+    long long kk = lo[0] + l1;
+    if (D > 1) kk += (long long)(lo[1] + l2) * g.kstride[1];
+    if (D > 2) kk += (long long)(lo[2] + l3) * g.kstride[2];
+    gout[kk * a.C + c0 + cc] = v;
   }
 }
 
@@ -623,9 +683,18 @@ cudaError_t run(Req &r) {
     cudaError_t e =
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
-    dim3 grid((unsigned)(t.ntiles * t.nslice), (unsigned)((a.C + CW - 1) / CW));
-    kern<<<grid, l.threads, sm, r.st>>>(a, t, l, r.bin_start, r.in, r.out);
-    return cudaGetLastError();
+    const unsigned nchunk = (unsigned)((a.C + CW - 1) / CW);
+    if (t.ntask > 0) {
+      kern<<<dim3((unsigned)t.ntask, nchunk), l.threads, sm, r.st>>>(a, t, l, r.bin_start, r.in,
+                                                                     r.out);
+      e = cudaGetLastError();
+      if (e != cudaSuccess) return e;
+    }
+    if (t.nred > 0) {
+      spread_reduce_kernel<D, CW><<<dim3((unsigned)t.nred, nchunk), 256, 0, r.st>>>(a, t, r.out);
+      e = cudaGetLastError();
+    }
+    return e;
   }
 }
 
