@@ -147,7 +147,7 @@ struct mirt_interp_plan {
   Launch lg{}, ls{};
   DMem tm, slice, perm, bin_start, tab[MIRT_DMAX], phase, src[MIRT_DMAX], nsrc[MIRT_DMAX];
   DMem keys, sorttmp, moff;
-  DMem task_tile, task_range, task_slot, red, scratch;
+  DMem task_tile, task_range, task_slot, red, scratch, wtap, k0tap;
   int split_chunk = 1024;  // sample visits per spread task before a tile is split
   std::vector<long long> moff_host;
 };
@@ -163,15 +163,10 @@ void choose_config(mirt_interp_plan *P) {
   const int C = a.C, D = a.g.D;
   const int cw = C >= 32 ? 32 : C >= 8 ? 8 : C >= 4 ? 4 : 1;
   const int threads = 256;
-  const int ngroups = threads / cw;
-
   Launch &lg = P->lg;
   lg.threads = threads;
   lg.cw = cw;
-  int sb = ngroups * 16;
-  if (sb < 32) sb = 32;
-  if (sb > 256) sb = 256;
-  lg.sb = sb;
+  lg.sb = 0;
   lg.grid = 0;
 
   int B[MIRT_DMAX] = {1, 1, 1}, T[MIRT_DMAX] = {1, 1, 1};
@@ -196,7 +191,7 @@ void choose_config(mirt_interp_plan *P) {
   Launch &ls = P->ls;
   ls.threads = 32;
   ls.cw = cw;
-  ls.sb = cw == 32 ? 16 : 32;
+  ls.sb = 0;
   ls.grid = 0;
   t.nbins = 1;
   t.ntiles = 1;
@@ -464,6 +459,14 @@ int plan_finish(mirt_interp_plan *P, long long Mtot, const long long *moff, int 
   }
   a.perm = P->perm.as<int>();
   P->sorttmp.release();
+  // tap coefficients and first taps of every position, once per trajectory
+  a.SJ = 0;
+  for (int d = 0; d < a.g.D; d++) a.SJ += a.g.J[d];
+  CK(P->wtap.alloc(std::max<long long>(Mtot, 1) * a.SJ * sizeof(float2)));
+  CK(P->k0tap.alloc(std::max<long long>(Mtot, 1) * sizeof(int4)));
+  CK(launch_prep_taps(a, P->wtap.as<float2>(), P->k0tap.as<int4>(), st));
+  a.W = P->wtap.as<float2>();
+  a.K0 = P->k0tap.as<int4>();
   int rc2 = build_tasks(P, st);
   if (rc2) return rc2;
   CK(query_gather_grid(a, P->lg));
@@ -631,10 +634,10 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
   CK(samp.alloc(nsamp * sizeof(float2)));
   CK(cudaMemsetAsync(samp.p, 0, nsamp * sizeof(float2), st));
   CK(cudaMemsetAsync(grid.p, 0, ngrid * sizeof(float2), st));
-  // spread candidates: tile shape (multiples of the 8-point bins), warps, batch
+  // spread candidates: tile shape (multiples of the 8-point bins), warps
   std::vector<SpreadCand> cands;
-  auto add = [&](int t0, int t1, int t2, int threads, int sb) {
-    SpreadCand c{{t0, t1, t2}, threads, sb};
+  auto add = [&](int t0, int t1, int t2, int threads) {
+    SpreadCand c{{t0, t1, t2}, threads, 0};
     for (int d = 0; d < D; d++) {
       const int kr = (a.g.K[d] + P->t.B[d] - 1) / P->t.B[d] * P->t.B[d];
       if (c.T[d] > kr) c.T[d] = kr;
@@ -642,29 +645,24 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
     }
     size_t npts = 1;
     for (int d = 0; d < D; d++) npts *= c.T[d];
-    int SJ = 0;
-    for (int d = 0; d < D; d++) SJ += a.g.J[d];
-    const size_t sm = npts * cw * 8 + (size_t)sb * SJ * 12 + (size_t)sb * 8 + 16 + (size_t)sb * cw * 8 + 16;
-    if (sm <= 200 * 1024) cands.push_back(c);
+    if (npts * cw * 8 <= 160 * 1024) cands.push_back(c);
   };
   if (D == 1) {
     for (int t0 : {64, 128, 256, 512})
-      for (int th : {32, 64}) add(t0, 1, 1, th, 32);
+      for (int th : {32, 64}) add(t0, 1, 1, th);
   } else if (D == 2) {
-    const int sbs = cw == 32 ? 16 : 32;
     for (int t0 : {8, 16, 32})
       for (int t1 : {8, 16, 32}) {
-        add(t0, t1, 1, 32, sbs);
-        if (t1 >= 16) add(t0, t1, 1, 64, sbs);
-        if (t1 >= 32) add(t0, t1, 1, 128, sbs);
+        add(t0, t1, 1, 32);
+        if (t1 >= 16) add(t0, t1, 1, 64);
+        if (t1 >= 32) add(t0, t1, 1, 128);
       }
-    add(8, 8, 1, 32, 2 * sbs);
   } else {
     for (int t0 : {8, 16})
       for (int t1 : {8, 16})
         for (int t2 : {8, 16}) {
-          add(t0, t1, t2, 32, 32);
-          if (t2 >= 16) add(t0, t1, t2, 64, 32);
+          add(t0, t1, t2, 32);
+          if (t2 >= 16) add(t0, t1, t2, 64);
         }
   }
   SpreadCand best{};
@@ -673,7 +671,6 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
     int rc = set_spread_tiles(P, c.T, st);
     if (rc) continue;
     P->ls.threads = c.threads;
-    P->ls.sb = c.sb;
     float ms = 0;
     rc = time_launch([&]() {
       return launch_spread(P->a, P->t, P->ls, P->bin_start.as<int>(), samp.as<float2>(),
@@ -689,7 +686,6 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
     int rc = set_spread_tiles(P, best.T, st);
     if (rc) return rc;
     P->ls.threads = best.threads;
-    P->ls.sb = best.sb;
   }
   // split size of heavy tiles (sample visits per spread task)
   {
@@ -714,28 +710,22 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
     int rc = build_tasks(P, st);
     if (rc) return rc;
   }
-  // gather candidates: CTA size and staged batch
+  // gather candidates: CTA size
   Launch bestg = P->lg;
   float bestg_ms = 1e30f;
-  for (int threads : {128, 256}) {
-    for (int per : {8, 16, 32}) {
-      Launch l = P->lg;
-      l.threads = threads;
-      int sb = threads / l.cw * per;
-      if (sb < 32) sb = 32;
-      if (sb > 512) continue;
-      l.sb = sb;
-      l.grid = 0;
-      CK(query_gather_grid(P->a, l));
-      float ms = 0;
-      int rc = time_launch([&]() {
-        return launch_gather(P->a, l, grid.as<float2>(), samp.as<float2>(), st);
-      }, st, &ms);
-      if (rc) return rc;
-      if (ms < bestg_ms) {
-        bestg_ms = ms;
-        bestg = l;
-      }
+  for (int threads : {64, 128, 256}) {
+    Launch l = P->lg;
+    l.threads = threads;
+    l.grid = 0;
+    CK(query_gather_grid(P->a, l));
+    float ms = 0;
+    int rc = time_launch([&]() {
+      return launch_gather(P->a, l, grid.as<float2>(), samp.as<float2>(), st);
+    }, st, &ms);
+    if (rc) return rc;
+    if (ms < bestg_ms) {
+      bestg_ms = ms;
+      bestg = l;
     }
   }
   P->lg = bestg;

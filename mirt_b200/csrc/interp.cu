@@ -172,6 +172,19 @@ cudaError_t radix_sort_bins(const uint32_t *keys, long long n, int nbins, void *
 }
 
 // ------------------------------------------------------------------------
+// per-position tap data
+// ------------------------------------------------------------------------
+cudaError_t launch_prep_taps(const InterpArgs &a, float2 *W, int4 *K0, cudaStream_t st) {
+  if (a.Mtot == 0) return cudaSuccess;
+  const unsigned blocks = (unsigned)((a.Mtot + 255) / 256);
+  if (a.real_tab)
+    detail::prep_taps_kernel<true><<<blocks, 256, 0, st>>>(a, W, K0);
+  else
+    detail::prep_taps_kernel<false><<<blocks, 256, 0, st>>>(a, W, K0);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------
 // public launchers
 // ------------------------------------------------------------------------
 namespace {

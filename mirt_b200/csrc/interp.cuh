@@ -26,6 +26,13 @@ struct InterpArgs {
   const void *tab[MIRT_DMAX];  // device tables: float2 (complex) or float (real)
   const float2 *phase;   // [Mtot] per-sample phase (nullptr = none)
   long long grid_elems;  // prod(K) * C  (one slice's grid, in float2)
+  // Per-position tap data, computed once per trajectory by prep_taps():
+  //   W[pos * SJ + (sum of J[<d]) + j]  coefficient of tap j of dimension d
+  //                                     (real tables: .y = 0)
+  //   K0[pos] = (first tap k1, k2, k3 wrapped into [0, K), slice)
+  int SJ;                // J[0] + ... + J[D-1]
+  const float2 *W;
+  const int4 *K0;
 };
 
 // Tiling of the grid.  Samples are sorted into bins of B[d] grid points per
@@ -73,6 +80,10 @@ struct Launch {
 // Compute the sort key of every sample: slice * nbins + bin of its first tap.
 cudaError_t launch_bin_keys(const InterpArgs &a, const Tiling &t, uint32_t *keys,
                             cudaStream_t st);
+
+// Tap coefficients (FP64 index selection, FP32 table values) and wrapped
+// first taps of every position, in the plan's sorted order.
+cudaError_t launch_prep_taps(const InterpArgs &a, float2 *W, int4 *K0, cudaStream_t st);
 
 // Stable LSD radix sort of (keys, 0..n-1) by key; writes the permutation
 // (sorted position -> sample) and bin_start[nbins+1].  tmp must hold

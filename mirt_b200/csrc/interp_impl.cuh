@@ -20,19 +20,18 @@ namespace detail {
 // ------------------------------------------------------------------------
 // small helpers
 // ------------------------------------------------------------------------
-struct Stage {
-  float2 *W;   // [sb][SJ] tap coefficients (real tables: .y = 0)
-  int *KI;     // [sb][SJ] wrapped grid coordinate of each tap
-  int *mid;    // [sb] caller's sample index (row of fm)
-  int *sid;    // [sb] slice index
-};
-
 // k mod K for any k, cheap when k is within one period of [0, K)
 __device__ __forceinline__ int wrap_fast(int k, int K) {
   if (k < 0) k += K;
   else if (k >= K) k -= K;
   if ((unsigned)k >= (unsigned)K) k = wrapk(k, K);
   return k;
+}
+
+// k0 + j for a wrapped first tap k0 in [0, K) and 0 <= j < J <= K
+__device__ __forceinline__ int tap_k(int k0, int j, int K) {
+  const int x = k0 + j;
+  return x >= K ? x - K : x;
 }
 
 // Coefficient of tap (d, k) for coordinate t: the reference's 0th-order
@@ -65,29 +64,20 @@ __device__ __forceinline__ float2 tap_coef(const InterpArgs &a, int d, double t,
   }
 }
 
-// Fill the stage for positions [pos0, pos0 + nb).
+// One thread per position: every tap coefficient and the wrapped first taps.
 template <bool REAL>
-__device__ void stage_batch(const InterpArgs &a, const Stage &s, long long pos0, int nb, int SJ) {
-  const int D = a.g.D;
-  for (int e = threadIdx.x; e < nb * SJ; e += blockDim.x) {
-    const int sl = e / SJ;
-    const int r = e - sl * SJ;
-    int d = 0;
-    int j = r;
-    while (d + 1 < D && j >= a.g.J[d]) {
-      j -= a.g.J[d];
-      d++;
-    }
-    const long long pos = pos0 + sl;
+__global__ void prep_taps_kernel(InterpArgs a, float2 *__restrict__ W, int4 *__restrict__ K0) {
+  const long long pos = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (pos >= a.Mtot) return;
+  int k0[MIRT_DMAX] = {0, 0, 0};
+  float2 *w = W + pos * a.SJ;
+  for (int d = 0; d < a.g.D; d++) {
     const double t = a.tm[(long long)d * a.Mtot + pos];
-    const int k = koff_of(t, a.g.J[d]) + j;
-    s.W[e] = tap_coef<REAL>(a, d, t, k);
-    s.KI[e] = wrap_fast(k, a.g.K[d]);
-    if (r == 0) {
-      s.mid[sl] = a.perm ? a.perm[pos] : (int)pos;
-      s.sid[sl] = a.slice_id ? a.slice_id[pos] : 0;
-    }
+    const int koff = koff_of(t, a.g.J[d]);
+    for (int j = 0; j < a.g.J[d]; j++) *w++ = tap_coef<REAL>(a, d, t, koff + j);
+    k0[d] = wrap_fast(koff, a.g.K[d]);
   }
+  K0[pos] = make_int4(k0[0], k0[1], k0[2], a.slice_id ? a.slice_id[pos] : 0);
 }
 
 // Complex accumulator held as two packed pairs: with w = (wr, wi) and
@@ -129,146 +119,151 @@ __device__ __forceinline__ float2 cw_fma(float2 w, float2 v, float2 vs, float2 A
 // ------------------------------------------------------------------------
 // forward gather
 // ------------------------------------------------------------------------
-// Persistent CTAs walk batches of the bin-sorted samples.  A group of CW
-// lanes serves one sample at a time; lane li handles columns li, li+CW, ...
-// and reads each tap as one coalesced column segment of the grid.  When the
-// J1 taps of a row do not wrap, they sit at a constant stride from one row
-// pointer (a compile-time stride when C == CW, CX).
+// Persistent CTAs sweep the bin-sorted positions; a group of CW lanes serves
+// one position at a time, lane li the columns li, li+CW, ..., and each tap is
+// one coalesced column segment of the grid.  The tap coefficients come from
+// the plan's per-position table (one broadcast load each).  When the J1 taps
+// of a row do not wrap they sit at a constant stride from one row pointer (a
+// compile-time stride when C == CW, CX).
 template <int D, int CW, int JT, bool REAL, bool CX>
-__global__ void __launch_bounds__(256) gather_kernel(InterpArgs a, Launch l,
-                                                     const float2 *__restrict__ ck,
+__global__ void __launch_bounds__(256) gather_kernel(InterpArgs a, const float2 *__restrict__ ck,
                                                      float2 *__restrict__ fm) {
-  extern __shared__ __align__(16) unsigned char smem[];
   const Geom &g = a.g;
   int Jd[MIRT_DMAX] = {1, 1, 1};
 #pragma unroll
   for (int d = 0; d < D; d++) Jd[d] = JT > 0 ? JT : g.J[d];
-  const int SJ = Jd[0] + (D > 1 ? Jd[1] : 0) + (D > 2 ? Jd[2] : 0);
-  const int sb = l.sb;
-  Stage s;
-  s.W = reinterpret_cast<float2 *>(smem);
-  s.KI = reinterpret_cast<int *>(s.W + sb * SJ);
-  s.mid = s.KI + sb * SJ;
-  s.sid = s.mid + sb;
-
-  const int ngroups = blockDim.x / CW;
-  const int grp = threadIdx.x / CW;
+  const int SJ = a.SJ;
+  const int gpc = blockDim.x / CW;
   const int li = threadIdx.x % CW;
+  const long long ngr = (long long)gridDim.x * gpc;
   const int C = a.C;
   const int cstr = CX ? CW : C;  // grid stride between neighbouring k1
   const long long rstr = (long long)g.kstride[D > 1 ? 1 : 0] * C;
   const long long pstr = (long long)g.kstride[D > 2 ? 2 : 0] * C;
+  const int K1 = g.K[0];
+  const int K2 = g.K[D > 1 ? 1 : 0];
+  const int K3 = g.K[D > 2 ? 2 : 0];
 
-  const long long nbatch = (a.Mtot + sb - 1) / sb;
-  for (long long bi = blockIdx.x; bi < nbatch; bi += gridDim.x) {
-    const long long pos0 = bi * sb;
-    const int nb = (int)min((long long)sb, a.Mtot - pos0);
-    stage_batch<REAL>(a, s, pos0, nb, SJ);
-    __syncthreads();
-    for (int sl = grp; sl < nb; sl += ngroups) {
-      const int m = s.mid[sl];
-      const float2 *gb = ck + (long long)s.sid[sl] * a.grid_elems;
-      const float2 *Ws = s.W + sl * SJ;
-      const int *Ks = s.KI + sl * SJ;
-      const float2 ph = a.phase ? a.phase[pos0 + sl] : make_float2(1.f, 0.f);
-      if constexpr (JT > 0) {
-        float2 w1[JT];
-        int o1[JT];
+  for (long long pos = (long long)blockIdx.x * gpc + threadIdx.x / CW; pos < a.Mtot;
+       pos += ngr) {
+    const int4 k0 = a.K0[pos];
+    const int m = a.perm ? a.perm[pos] : (int)pos;
+    const float2 *Ws = a.W + pos * SJ;
+    const float2 *gb = ck + (long long)k0.w * a.grid_elems;
+    const float2 ph = a.phase ? a.phase[pos] : make_float2(1.f, 0.f);
+    if constexpr (JT > 0) {
+      float2 w1[JT], w2[D > 1 ? JT : 1], w3[D > 2 ? JT : 1];
+      const float4 *W4 = reinterpret_cast<const float4 *>(Ws);
+      // coefficient loads (SJ float2; pairs as float4 when 16-byte aligned)
+      if ((SJ & 1) == 0) {
+        float2 tmp[3 * JT];
+#pragma unroll
+        for (int q = 0; q < D * JT / 2; q++) {
+          const float4 v = __ldg(W4 + q);
+          tmp[2 * q] = make_float2(v.x, v.y);
+          tmp[2 * q + 1] = make_float2(v.z, v.w);
+        }
 #pragma unroll
         for (int j = 0; j < JT; j++) {
-          w1[j] = Ws[j];
-          o1[j] = Ks[j] * C;
+          w1[j] = tmp[j];
+          if (D > 1) w2[j] = tmp[JT + j];
+          if (D > 2) w3[j] = tmp[2 * JT + j];
         }
-        const int k10 = Ks[0];
-        const bool fast = k10 + JT <= g.K[0];
-        const int c10 = k10 * C;
-        for (int c = li; c < C; c += CW) {
-          const float2 *gc = gb + c;
-          // sum over j1 of one grid row (the reference's innermost loop)
-          auto rowsum = [&](const float2 *row) -> float2 {
-            CAcc s1;
-            cacc_zero(s1);
-            if (fast) {
-              const float2 *p = row + c10;
+      } else {
 #pragma unroll
-              for (int j1 = 0; j1 < JT; j1++) cacc_mac<REAL>(s1, w1[j1], __ldg(p + j1 * cstr));
-            } else {
+        for (int j = 0; j < JT; j++) {
+          w1[j] = __ldg(Ws + j);
+          if (D > 1) w2[j] = __ldg(Ws + JT + j);
+          if (D > 2) w3[j] = __ldg(Ws + 2 * JT + j);
+        }
+      }
+      const bool fast = k0.x + JT <= K1;
+      int o1[JT];
 #pragma unroll
-              for (int j1 = 0; j1 < JT; j1++) cacc_mac<REAL>(s1, w1[j1], __ldg(row + o1[j1]));
-            }
-            return cacc_get<REAL>(s1);
-          };
-          float2 out;
-          if constexpr (D == 1) {
-            out = rowsum(gc);
-          } else if constexpr (D == 2) {
+      for (int j = 0; j < JT; j++) o1[j] = tap_k(k0.x, j, K1) * C;
+      const int c10 = k0.x * C;
+      for (int c = li; c < C; c += CW) {
+        const float2 *gc = gb + c;
+        // sum over j1 of one grid row (the reference's innermost loop)
+        auto rowsum = [&](const float2 *row) -> float2 {
+          CAcc s1;
+          cacc_zero(s1);
+          if (fast) {
+            const float2 *p = row + c10;
+#pragma unroll
+            for (int j1 = 0; j1 < JT; j1++) cacc_mac<REAL>(s1, w1[j1], __ldg(p + j1 * cstr));
+          } else {
+#pragma unroll
+            for (int j1 = 0; j1 < JT; j1++) cacc_mac<REAL>(s1, w1[j1], __ldg(row + o1[j1]));
+          }
+          return cacc_get<REAL>(s1);
+        };
+        float2 out;
+        if constexpr (D == 1) {
+          out = rowsum(gc);
+        } else if constexpr (D == 2) {
+          CAcc s2;
+          cacc_zero(s2);
+#pragma unroll
+          for (int j2 = 0; j2 < JT; j2++)
+            cacc_mac<false>(s2, w2[j2], rowsum(gc + tap_k(k0.y, j2, K2) * rstr));
+          out = cacc_get<false>(s2);
+        } else {
+          CAcc s3;
+          cacc_zero(s3);
+#pragma unroll 1
+          for (int j3 = 0; j3 < JT; j3++) {
+            const float2 *pl = gc + tap_k(k0.z, j3, K3) * pstr;
             CAcc s2;
             cacc_zero(s2);
 #pragma unroll
-            for (int j2 = 0; j2 < JT; j2++) {
-              const float2 r = rowsum(gc + Ks[JT + j2] * rstr);
-              cacc_mac<false>(s2, Ws[JT + j2], r);
-            }
-            out = cacc_get<false>(s2);
-          } else {
-            CAcc s3;
-            cacc_zero(s3);
-#pragma unroll 1
-            for (int j3 = 0; j3 < JT; j3++) {
-              const float2 *pl = gc + Ks[2 * JT + j3] * pstr;
-              CAcc s2;
-              cacc_zero(s2);
-#pragma unroll
-              for (int j2 = 0; j2 < JT; j2++) {
-                const float2 r = rowsum(pl + Ks[JT + j2] * rstr);
-                cacc_mac<false>(s2, Ws[JT + j2], r);
-              }
-              cacc_mac<false>(s3, Ws[2 * JT + j3], cacc_get<false>(s2));
-            }
-            out = cacc_get<false>(s3);
+            for (int j2 = 0; j2 < JT; j2++)
+              cacc_mac<false>(s2, w2[j2], rowsum(pl + tap_k(k0.y, j2, K2) * rstr));
+            cacc_mac<false>(s3, w3[j3], cacc_get<false>(s2));
           }
-          if (a.phase) out = cmul(out, ph);
-          fm[(long long)m * C + c] = out;
+          out = cacc_get<false>(s3);
         }
-      } else {
-        // any J: coefficients read from shared memory, runtime loops
-        for (int c = li; c < C; c += CW) {
-          const float2 *gc = gb + c;
-          auto rowsum = [&](const float2 *row) -> float2 {
-            CAcc s1;
-            cacc_zero(s1);
-            for (int j1 = 0; j1 < Jd[0]; j1++)
-              cacc_mac<REAL>(s1, Ws[j1], __ldg(row + (long long)Ks[j1] * C));
-            return cacc_get<REAL>(s1);
-          };
-          float2 out;
-          if constexpr (D == 1) {
-            out = rowsum(gc);
-          } else if constexpr (D == 2) {
+        if (a.phase) out = cmul(out, ph);
+        fm[(long long)m * C + c] = out;
+      }
+    } else {
+      // any J: coefficients read per tap, runtime loops
+      for (int c = li; c < C; c += CW) {
+        const float2 *gc = gb + c;
+        auto rowsum = [&](const float2 *row) -> float2 {
+          CAcc s1;
+          cacc_zero(s1);
+          for (int j1 = 0; j1 < Jd[0]; j1++)
+            cacc_mac<REAL>(s1, __ldg(Ws + j1), __ldg(row + (long long)tap_k(k0.x, j1, K1) * C));
+          return cacc_get<REAL>(s1);
+        };
+        float2 out;
+        if constexpr (D == 1) {
+          out = rowsum(gc);
+        } else if constexpr (D == 2) {
+          CAcc s2;
+          cacc_zero(s2);
+          for (int j2 = 0; j2 < Jd[1]; j2++)
+            cacc_mac<false>(s2, __ldg(Ws + Jd[0] + j2), rowsum(gc + tap_k(k0.y, j2, K2) * rstr));
+          out = cacc_get<false>(s2);
+        } else {
+          CAcc s3;
+          cacc_zero(s3);
+          for (int j3 = 0; j3 < Jd[2]; j3++) {
+            const float2 *pl = gc + tap_k(k0.z, j3, K3) * pstr;
             CAcc s2;
             cacc_zero(s2);
             for (int j2 = 0; j2 < Jd[1]; j2++)
-              cacc_mac<false>(s2, Ws[Jd[0] + j2], rowsum(gc + Ks[Jd[0] + j2] * rstr));
-            out = cacc_get<false>(s2);
-          } else {
-            CAcc s3;
-            cacc_zero(s3);
-            for (int j3 = 0; j3 < Jd[2]; j3++) {
-              const float2 *pl = gc + Ks[Jd[0] + Jd[1] + j3] * pstr;
-              CAcc s2;
-              cacc_zero(s2);
-              for (int j2 = 0; j2 < Jd[1]; j2++)
-                cacc_mac<false>(s2, Ws[Jd[0] + j2], rowsum(pl + Ks[Jd[0] + j2] * rstr));
-              cacc_mac<false>(s3, Ws[Jd[0] + Jd[1] + j3], cacc_get<false>(s2));
-            }
-            out = cacc_get<false>(s3);
+              cacc_mac<false>(s2, __ldg(Ws + Jd[0] + j2),
+                              rowsum(pl + tap_k(k0.y, j2, K2) * rstr));
+            cacc_mac<false>(s3, __ldg(Ws + Jd[0] + Jd[1] + j3), cacc_get<false>(s2));
           }
-          if (a.phase) out = cmul(out, ph);
-          fm[(long long)m * C + c] = out;
+          out = cacc_get<false>(s3);
         }
+        if (a.phase) out = cmul(out, ph);
+        fm[(long long)m * C + c] = out;
       }
     }
-    __syncthreads();
   }
 }
 
@@ -345,21 +340,11 @@ __device__ __forceinline__ void spread_row(float2 *row, const float2 *Ws, int J1
   constexpr int SUB = 32 / CW;
   const float2 v2s = make_float2(v2.y, v2.x);
   if (fast1) {
-    if constexpr (JT > 0 && SUB == 1) {
-      float2 *p = row + l10 * CW;
-#pragma unroll
-      for (int j1 = 0; j1 < JT; j1++) {
-        float2 A = p[j1 * CW];
-        A = cw_fma<REAL>(Ws[j1], v2, v2s, A);
-        p[j1 * CW] = A;
-      }
-    } else {
-      for (int j1 = (ls - l10) & (SUB - 1); j1 < J1; j1 += SUB) {
-        float2 *p = row + (l10 + j1) * CW;
-        float2 A = *p;
-        A = cw_fma<REAL>(Ws[j1], v2, v2s, A);
-        *p = A;
-      }
+    for (int j1 = (ls - l10) & (SUB - 1); j1 < J1; j1 += SUB) {
+      float2 *p = row + (l10 + j1) * CW;
+      float2 A = *p;
+      A = cw_fma<REAL>(__ldg(Ws + j1), v2, v2s, A);
+      *p = A;
     }
   } else {
     unsigned mm = m1;
@@ -368,14 +353,14 @@ __device__ __forceinline__ void spread_row(float2 *row, const float2 *Ws, int J1
       mm &= mm - 1;
       float2 *p = row + tap_local(k10, j1, K1, lo1) * CW;
       float2 A = *p;
-      A = cw_fma<REAL>(Ws[j1], v2, v2s, A);
+      A = cw_fma<REAL>(__ldg(Ws + j1), v2, v2s, A);
       *p = A;
     }
   }
 }
 
 template <int D, int CW, int JT, bool REAL>
-__global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t, Launch l,
+__global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t,
                                                      const int *__restrict__ bin_start,
                                                      const float2 *__restrict__ fm,
                                                      float2 *__restrict__ ck) {
@@ -390,15 +375,7 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t, Lau
   int Jd[MIRT_DMAX] = {1, 1, 1};
 #pragma unroll
   for (int d = 0; d < D; d++) Jd[d] = JT > 0 ? JT : g.J[d];
-  const int SJ = Jd[0] + (D > 1 ? Jd[1] : 0) + (D > 2 ? Jd[2] : 0);
-  const int sb = l.sb;
-  Stage s;
-  s.W = acc + (size_t)npts * CW;
-  s.KI = reinterpret_cast<int *>(s.W + sb * SJ);
-  s.mid = s.KI + sb * SJ;
-  s.sid = s.mid + sb;
-  // [sb][CW] sample values; sb is even, so this stays 8-byte aligned
-  float2 *F = reinterpret_cast<float2 *>(s.sid + sb);
+  const int SJ = a.SJ;
 
   const int task = t.task_tile[blockIdx.x];
   const int2 vr = t.task_range[blockIdx.x];
@@ -426,6 +403,7 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t, Lau
   const int band_lo = min(warp * per, ext[BD]);
   const int band_hi = min(band_lo + per, ext[BD]);
   for (int e = threadIdx.x; e < npts * CW; e += blockDim.x) acc[e] = make_float2(0.f, 0.f);
+  __syncthreads();
 
   int ns[MIRT_DMAX] = {1, 1, 1};
 #pragma unroll
@@ -435,9 +413,10 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t, Lau
   const int T0 = t.T[0];
   const int T1 = D > 1 ? t.T[1] : 1;
   const int jb0 = D == 1 ? 0 : (D == 2 ? Jd[0] : Jd[0] + Jd[1]);  // first tap of dim BD
+  const bool lane_on = c0 + lc < C;
 
   long long vbase = 0;
-  for (int si = 0; si < nsrc_tot && vbase < vr.y; si++) {
+  for (int si = 0; si < nsrc_tot && vbase < vr.y && band_lo < band_hi; si++) {
     int r = si, stile = 0, mul = 1;
 #pragma unroll
     for (int d = 0; d < D; d++) {
@@ -452,101 +431,94 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t, Lau
     const long long beg = b0 + max(0ll, (long long)vr.x - vbase);
     const long long end = b0 + min(b1 - b0, (long long)vr.y - vbase);
     vbase += b1 - b0;
-    for (long long pos0 = beg; pos0 < end; pos0 += sb) {
-      const int nb = (int)min((long long)sb, end - pos0);
-      __syncthreads();
-      stage_batch<REAL>(a, s, pos0, nb, SJ);
-      for (int e = threadIdx.x; e < nb * CW; e += blockDim.x) {
-        const int sl = e / CW, cc = e - sl * CW;
-        const long long pos = pos0 + sl;
-        const int m = a.perm ? a.perm[pos] : (int)pos;
-        float2 f = make_float2(0.f, 0.f);
-        if (c0 + cc < C) {
-          f = fm[(long long)m * C + c0 + cc];
-          if (a.phase) f = cmulc(a.phase[pos], f);
-        }
-        F[e] = f;
+    if (beg >= end) continue;
+    // one position ahead: its first taps and sample index are in flight
+    int4 kn = a.K0[beg];
+    int mn = a.perm ? a.perm[beg] : (int)beg;
+    for (long long pos = beg; pos < end; pos++) {
+      const int4 k = kn;
+      const int m = mn;
+      if (pos + 1 < end) {
+        kn = a.K0[pos + 1];
+        mn = a.perm ? a.perm[pos + 1] : (int)(pos + 1);
       }
-      __syncthreads();
-      if (band_lo >= band_hi) continue;
-      for (int sl = 0; sl < nb; sl++) {
-        const float2 *Ws = s.W + sl * SJ;
-        const int *Ks = s.KI + sl * SJ;
-        // warp-uniform: taps of the band dimension inside this warp's band
-        const unsigned mb = tap_mask<1>(Ks[jb0], Jd[BD], g.K[BD], lo[BD], band_lo, band_hi, 0);
-        if (!mb) continue;
-        const int k10 = Ks[0];
-        const int l10 = k10 - lo[0];
-        const float2 f = F[sl * CW + lc];
-        if constexpr (D == 1) {
-          const unsigned m1 = tap_mask<SUB>(k10, Jd[0], g.K[0], lo[0], band_lo, band_hi, ls);
-          spread_row<CW, JT, REAL>(acc + lc, Ws, Jd[0], false, l10, m1, k10, g.K[0], lo[0], ls,
-                                   f);
-        } else {
-          // lane's columns: fast when the J1 taps do not leave the tile
-          const bool fast1 = l10 >= 0 && l10 + Jd[0] <= ext[0];
-          const unsigned m1 =
-              fast1 ? 0u : tap_mask<SUB>(k10, Jd[0], g.K[0], lo[0], 0, ext[0], ls);
-          if (!fast1 && !m1) continue;
-          if constexpr (D == 2) {
-            if constexpr (JT > 0 && SUB == 1) {
-              if (fast1) {
-                // all J1 columns inside the tile: coefficient pairs in registers,
-                // LDS.64 + 2 FFMA2 + STS.64 per tap at compile-time strides
-                float2 wr[JT], wi[JT];
+      const int kb = D == 1 ? k.x : (D == 2 ? k.y : k.z);
+      // warp-uniform: taps of the band dimension inside this warp's band
+      const unsigned mb = tap_mask<1>(kb, Jd[BD], g.K[BD], lo[BD], band_lo, band_hi, 0);
+      if (!mb) continue;
+      const float2 *Ws = a.W + pos * SJ;
+      float2 f = make_float2(0.f, 0.f);
+      if (lane_on) {
+        f = __ldg(fm + (long long)m * C + c0 + lc);
+        if (a.phase) f = cmulc(__ldg(a.phase + pos), f);
+      }
+      const int l10 = k.x - lo[0];
+      if constexpr (D == 1) {
+        const unsigned m1 = tap_mask<SUB>(k.x, Jd[0], g.K[0], lo[0], band_lo, band_hi, ls);
+        spread_row<CW, JT, REAL>(acc + lc, Ws, Jd[0], false, l10, m1, k.x, g.K[0], lo[0], ls, f);
+      } else {
+        // lane's columns: fast when the J1 taps do not leave the tile
+        const bool fast1 = l10 >= 0 && l10 + Jd[0] <= ext[0];
+        const unsigned m1 = fast1 ? 0u : tap_mask<SUB>(k.x, Jd[0], g.K[0], lo[0], 0, ext[0], ls);
+        if (!fast1 && !m1) continue;
+        if constexpr (D == 2) {
+          if constexpr (JT > 0 && SUB == 1) {
+            if (fast1) {
+              // all J1 columns inside the tile: coefficient pairs in registers,
+              // LDS.64 + 2 FFMA2 + STS.64 per tap at compile-time strides
+              float2 wr[JT], wi[JT];
 #pragma unroll
-                for (int j1 = 0; j1 < JT; j1++) {
-                  const float2 w = Ws[j1];
-                  wr[j1] = make_float2(w.x, w.x);
-                  wi[j1] = make_float2(w.y, -w.y);
-                }
-                float2 *base = acc + l10 * CW + lc;
-                unsigned m2 = mb;
-                while (m2) {
-                  const int j2 = __ffs(m2) - 1;
-                  m2 &= m2 - 1;
-                  const int l2 = tap_local(Ks[Jd[0]], j2, g.K[1], lo[1]);
-                  const float2 v2 = cw_mul<REAL>(Ws[Jd[0] + j2], f);
-                  const float2 v2s = make_float2(v2.y, v2.x);
-                  float2 *p = base + (size_t)l2 * T0 * CW;
-#pragma unroll
-                  for (int j1 = 0; j1 < JT; j1++) {
-                    float2 A = p[j1 * CW];
-                    A = __ffma2_rn(wr[j1], v2, A);
-                    if (!REAL) A = __ffma2_rn(wi[j1], v2s, A);
-                    p[j1 * CW] = A;
-                  }
-                }
-                continue;
+              for (int j1 = 0; j1 < JT; j1++) {
+                const float2 w = __ldg(Ws + j1);
+                wr[j1] = make_float2(w.x, w.x);
+                wi[j1] = make_float2(w.y, -w.y);
               }
-            }
-            unsigned m2 = mb;
-            while (m2) {
-              const int j2 = __ffs(m2) - 1;
-              m2 &= m2 - 1;
-              const int l2 = tap_local(Ks[Jd[0]], j2, g.K[1], lo[1]);
-              const float2 v2 = cw_mul<REAL>(Ws[Jd[0] + j2], f);
-              spread_row<CW, JT, REAL>(acc + (size_t)l2 * T0 * CW + lc, Ws, Jd[0], fast1, l10, m1,
-                                       k10, g.K[0], lo[0], ls, v2);
-            }
-          } else {
-            const unsigned m2all = tap_mask<1>(Ks[Jd[0]], Jd[1], g.K[1], lo[1], 0, ext[1], 0);
-            if (!m2all) continue;
-            unsigned m3 = mb;
-            while (m3) {
-              const int j3 = __ffs(m3) - 1;
-              m3 &= m3 - 1;
-              const int l3 = tap_local(Ks[jb0], j3, g.K[2], lo[2]);
-              const float2 v3 = cw_mul<REAL>(Ws[jb0 + j3], f);
-              unsigned m2 = m2all;
+              float2 *base = acc + l10 * CW + lc;
+              unsigned m2 = mb;
               while (m2) {
                 const int j2 = __ffs(m2) - 1;
                 m2 &= m2 - 1;
-                const int l2 = tap_local(Ks[Jd[0]], j2, g.K[1], lo[1]);
-                const float2 v2 = cw_mul<REAL>(Ws[Jd[0] + j2], v3);
-                spread_row<CW, JT, REAL>(acc + ((size_t)l3 * T1 + l2) * T0 * CW + lc, Ws, Jd[0],
-                                         fast1, l10, m1, k10, g.K[0], lo[0], ls, v2);
+                const int l2 = tap_local(k.y, j2, g.K[1], lo[1]);
+                const float2 v2 = cw_mul<REAL>(__ldg(Ws + JT + j2), f);
+                const float2 v2s = make_float2(v2.y, v2.x);
+                float2 *p = base + (size_t)l2 * T0 * CW;
+#pragma unroll
+                for (int j1 = 0; j1 < JT; j1++) {
+                  float2 A = p[j1 * CW];
+                  A = __ffma2_rn(wr[j1], v2, A);
+                  if (!REAL) A = __ffma2_rn(wi[j1], v2s, A);
+                  p[j1 * CW] = A;
+                }
               }
+              continue;
+            }
+          }
+          unsigned m2 = mb;
+          while (m2) {
+            const int j2 = __ffs(m2) - 1;
+            m2 &= m2 - 1;
+            const int l2 = tap_local(k.y, j2, g.K[1], lo[1]);
+            const float2 v2 = cw_mul<REAL>(__ldg(Ws + Jd[0] + j2), f);
+            spread_row<CW, JT, REAL>(acc + (size_t)l2 * T0 * CW + lc, Ws, Jd[0], fast1, l10, m1,
+                                     k.x, g.K[0], lo[0], ls, v2);
+          }
+        } else {
+          const unsigned m2all = tap_mask<1>(k.y, Jd[1], g.K[1], lo[1], 0, ext[1], 0);
+          if (!m2all) continue;
+          unsigned m3 = mb;
+          while (m3) {
+            const int j3 = __ffs(m3) - 1;
+            m3 &= m3 - 1;
+            const int l3 = tap_local(k.z, j3, g.K[2], lo[2]);
+            const float2 v3 = cw_mul<REAL>(__ldg(Ws + jb0 + j3), f);
+            unsigned m2 = m2all;
+            while (m2) {
+              const int j2 = __ffs(m2) - 1;
+              m2 &= m2 - 1;
+              const int l2 = tap_local(k.y, j2, g.K[1], lo[1]);
+              const float2 v2 = cw_mul<REAL>(__ldg(Ws + Jd[0] + j2), v3);
+              spread_row<CW, JT, REAL>(acc + ((size_t)l3 * T1 + l2) * T0 * CW + lc, Ws, Jd[0],
+                                       fast1, l10, m1, k.x, g.K[0], lo[0], ls, v2);
             }
           }
         }
@@ -637,16 +609,10 @@ struct Req {
   cudaStream_t st;
 };
 
-inline size_t stage_bytes(const InterpArgs &a, int sb) {
-  int SJ = 0;
-  for (int d = 0; d < a.g.D; d++) SJ += a.g.J[d];
-  return (size_t)sb * SJ * (8 + 4) + (size_t)sb * 8 + 16;
-}
-
 inline size_t spread_smem_bytes(const InterpArgs &a, const Tiling &t, const Launch &l) {
   size_t npts = 1;
   for (int d = 0; d < a.g.D; d++) npts *= t.T[d];
-  return npts * l.cw * 8 + stage_bytes(a, l.sb) + (size_t)l.sb * l.cw * 8 + 16;
+  return npts * l.cw * 8;
 }
 
 template <int D, int CW, int JT, bool REAL, bool CX>
@@ -654,24 +620,21 @@ cudaError_t run(Req &r) {
   const InterpArgs &a = *r.a;
   Launch &l = *r.l;
   if (r.what == GATHER || r.what == GATHER_GRID) {
-    const size_t sm = stage_bytes(a, l.sb);
     auto kern = gather_kernel<D, CW, JT, REAL, CX>;
-    cudaError_t e =
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    if (e != cudaSuccess) return e;
+    cudaError_t e = cudaSuccess;
     if (r.what == GATHER_GRID || l.grid <= 0) {
       int per_sm = 0, dev = 0, nsm = 0;
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, l.threads, sm);
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, l.threads, 0);
       if (e != cudaSuccess) return e;
       cudaGetDevice(&dev);
       cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-      const long long nbatch = (a.Mtot + l.sb - 1) / l.sb;
+      const long long groups = (a.Mtot + (l.threads / CW) - 1) / (l.threads / CW);
       long long gsz = (long long)nsm * (per_sm > 0 ? per_sm : 1);
-      if (gsz > nbatch) gsz = nbatch;
+      if (gsz > groups) gsz = groups;
       l.grid = (int)(gsz > 0 ? gsz : 1);
       if (r.what == GATHER_GRID) return cudaSuccess;
     }
-    kern<<<l.grid, l.threads, sm, r.st>>>(a, l, r.in, r.out);
+    kern<<<l.grid, l.threads, 0, r.st>>>(a, r.in, r.out);
     return cudaGetLastError();
   }
   if constexpr (CX) {
@@ -685,7 +648,7 @@ cudaError_t run(Req &r) {
     if (e != cudaSuccess) return e;
     const unsigned nchunk = (unsigned)((a.C + CW - 1) / CW);
     if (t.ntask > 0) {
-      kern<<<dim3((unsigned)t.ntask, nchunk), l.threads, sm, r.st>>>(a, t, l, r.bin_start, r.in,
+      kern<<<dim3((unsigned)t.ntask, nchunk), l.threads, sm, r.st>>>(a, t, r.bin_start, r.in,
                                                                      r.out);
       e = cudaGetLastError();
       if (e != cudaSuccess) return e;
