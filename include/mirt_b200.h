@@ -194,8 +194,9 @@ int mirt_interp_plan_adjoint(mirt_interp_plan *plan, const void *fm, void *ck, v
 int mirt_interp_plan_autotune(mirt_interp_plan *plan, void *stream);
 
 /* Current launch configuration: up to 14 values
- * {T1, T2, T3, spread threads, spread batch, coil lanes, gather threads,
- *  gather batch, gather CTAs, B1, B2, B3, split chunk, spread tasks}. */
+ * {T1, T2, T3, spread threads, spread heavy-first order, coil lanes,
+ *  gather threads, (unused), gather CTAs, B1, B2, B3, split chunk,
+ *  spread tasks}. */
 int mirt_interp_plan_config(mirt_interp_plan *plan, int32_t *out, int32_t n);
 
 int mirt_interp_plan_destroy(mirt_interp_plan *plan);

@@ -149,6 +149,7 @@ struct mirt_interp_plan {
   DMem keys, sorttmp, moff;
   DMem task_tile, task_range, task_slot, red, scratch, wtap, k0tap;
   int split_chunk = 1024;  // sample visits per spread task before a tile is split
+  int heavy_first = 1;     // spread task order: 1 heaviest first, 0 grid order
   std::vector<long long> moff_host;
 };
 
@@ -368,8 +369,9 @@ int build_tasks(mirt_interp_plan *P, cudaStream_t st) {
       nslot += np;
     }
   }
-  std::stable_sort(tasks.begin(), tasks.end(),
-                   [](const Task &x, const Task &y) { return x.work > y.work; });
+  if (P->heavy_first)
+    std::stable_sort(tasks.begin(), tasks.end(),
+                     [](const Task &x, const Task &y) { return x.work > y.work; });
   const size_t nt = tasks.size();
   std::vector<int> tt(nt), ts(nt);
   std::vector<int2> tr(nt);
@@ -707,6 +709,20 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
       }
     }
     P->split_chunk = best_chunk;
+    // task order: heaviest first (load balance) or grid order (L2 reuse of
+    // neighbouring bins)
+    float order_ms[2] = {1e30f, 1e30f};
+    for (int hf = 0; hf < 2; hf++) {
+      P->heavy_first = hf;
+      int rc = build_tasks(P, st);
+      if (rc) return rc;
+      rc = time_launch([&]() {
+        return launch_spread(P->a, P->t, P->ls, P->bin_start.as<int>(), samp.as<float2>(),
+                             grid.as<float2>(), st);
+      }, st, &order_ms[hf]);
+      if (rc) return rc;
+    }
+    P->heavy_first = order_ms[1] <= order_ms[0] ? 1 : 0;
     int rc = build_tasks(P, st);
     if (rc) return rc;
   }
@@ -735,7 +751,7 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
 
 int mirt_interp_plan_config(mirt_interp_plan *P, int32_t *out, int32_t n) {
   if (!P || !out) return fail(MIRT_ERR_ARG, "NULL argument");
-  const int32_t v[14] = {P->t.T[0], P->t.T[1], P->t.T[2], P->ls.threads, P->ls.sb, P->ls.cw,
+  const int32_t v[14] = {P->t.T[0], P->t.T[1], P->t.T[2], P->ls.threads, P->heavy_first, P->ls.cw,
                          P->lg.threads, P->lg.sb, P->lg.grid, P->t.B[0], P->t.B[1], P->t.B[2],
                          P->split_chunk, P->t.ntask};
   for (int i = 0; i < n && i < 14; i++) out[i] = v[i];

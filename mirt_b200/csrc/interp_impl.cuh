@@ -126,7 +126,7 @@ __device__ __forceinline__ float2 cw_fma(float2 w, float2 v, float2 vs, float2 A
 // of a row do not wrap they sit at a constant stride from one row pointer (a
 // compile-time stride when C == CW, CX).
 template <int D, int CW, int JT, bool REAL, bool CX>
-__global__ void __launch_bounds__(256) gather_kernel(InterpArgs a, const float2 *__restrict__ ck,
+__global__ void __launch_bounds__(256, 3) gather_kernel(InterpArgs a, const float2 *__restrict__ ck,
                                                      float2 *__restrict__ fm) {
   const Geom &g = a.g;
   int Jd[MIRT_DMAX] = {1, 1, 1};
@@ -152,35 +152,22 @@ __global__ void __launch_bounds__(256) gather_kernel(InterpArgs a, const float2 
     const float2 *gb = ck + (long long)k0.w * a.grid_elems;
     const float2 ph = a.phase ? a.phase[pos] : make_float2(1.f, 0.f);
     if constexpr (JT > 0) {
-      float2 w1[JT], w2[D > 1 ? JT : 1], w3[D > 2 ? JT : 1];
-      const float4 *W4 = reinterpret_cast<const float4 *>(Ws);
-      // coefficient loads (SJ float2; pairs as float4 when 16-byte aligned)
-      if ((SJ & 1) == 0) {
-        float2 tmp[3 * JT];
+      // column coefficients stay in registers; row / plane coefficients are
+      // loaded per row (broadcast L1 hits), keeping register pressure low
+      float2 w1[JT];
+      if constexpr ((JT & 1) == 0) {
+        const float4 *W4 = reinterpret_cast<const float4 *>(Ws);
 #pragma unroll
-        for (int q = 0; q < D * JT / 2; q++) {
+        for (int q = 0; q < JT / 2; q++) {
           const float4 v = __ldg(W4 + q);
-          tmp[2 * q] = make_float2(v.x, v.y);
-          tmp[2 * q + 1] = make_float2(v.z, v.w);
-        }
-#pragma unroll
-        for (int j = 0; j < JT; j++) {
-          w1[j] = tmp[j];
-          if (D > 1) w2[j] = tmp[JT + j];
-          if (D > 2) w3[j] = tmp[2 * JT + j];
+          w1[2 * q] = make_float2(v.x, v.y);
+          w1[2 * q + 1] = make_float2(v.z, v.w);
         }
       } else {
 #pragma unroll
-        for (int j = 0; j < JT; j++) {
-          w1[j] = __ldg(Ws + j);
-          if (D > 1) w2[j] = __ldg(Ws + JT + j);
-          if (D > 2) w3[j] = __ldg(Ws + 2 * JT + j);
-        }
+        for (int j = 0; j < JT; j++) w1[j] = __ldg(Ws + j);
       }
       const bool fast = k0.x + JT <= K1;
-      int o1[JT];
-#pragma unroll
-      for (int j = 0; j < JT; j++) o1[j] = tap_k(k0.x, j, K1) * C;
       const int c10 = k0.x * C;
       for (int c = li; c < C; c += CW) {
         const float2 *gc = gb + c;
@@ -194,7 +181,8 @@ __global__ void __launch_bounds__(256) gather_kernel(InterpArgs a, const float2 
             for (int j1 = 0; j1 < JT; j1++) cacc_mac<REAL>(s1, w1[j1], __ldg(p + j1 * cstr));
           } else {
 #pragma unroll
-            for (int j1 = 0; j1 < JT; j1++) cacc_mac<REAL>(s1, w1[j1], __ldg(row + o1[j1]));
+            for (int j1 = 0; j1 < JT; j1++)
+              cacc_mac<REAL>(s1, w1[j1], __ldg(row + tap_k(k0.x, j1, K1) * C));
           }
           return cacc_get<REAL>(s1);
         };
@@ -204,9 +192,9 @@ __global__ void __launch_bounds__(256) gather_kernel(InterpArgs a, const float2 
         } else if constexpr (D == 2) {
           CAcc s2;
           cacc_zero(s2);
-#pragma unroll
+#pragma unroll 3
           for (int j2 = 0; j2 < JT; j2++)
-            cacc_mac<false>(s2, w2[j2], rowsum(gc + tap_k(k0.y, j2, K2) * rstr));
+            cacc_mac<false>(s2, __ldg(Ws + JT + j2), rowsum(gc + tap_k(k0.y, j2, K2) * rstr));
           out = cacc_get<false>(s2);
         } else {
           CAcc s3;
@@ -216,10 +204,10 @@ __global__ void __launch_bounds__(256) gather_kernel(InterpArgs a, const float2 
             const float2 *pl = gc + tap_k(k0.z, j3, K3) * pstr;
             CAcc s2;
             cacc_zero(s2);
-#pragma unroll
+#pragma unroll 3
             for (int j2 = 0; j2 < JT; j2++)
-              cacc_mac<false>(s2, w2[j2], rowsum(pl + tap_k(k0.y, j2, K2) * rstr));
-            cacc_mac<false>(s3, w3[j3], cacc_get<false>(s2));
+              cacc_mac<false>(s2, __ldg(Ws + JT + j2), rowsum(pl + tap_k(k0.y, j2, K2) * rstr));
+            cacc_mac<false>(s3, __ldg(Ws + 2 * JT + j3), cacc_get<false>(s2));
           }
           out = cacc_get<false>(s3);
         }
@@ -453,6 +441,66 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t,
         if (a.phase) f = cmulc(__ldg(a.phase + pos), f);
       }
       const int l10 = k.x - lo[0];
+      if constexpr (JT > 0 && D >= 2) {
+        // patch without periodic wrap: the in-tile taps of each dimension are
+        // one index range, walked with unrolled predicated loops
+        const int kr = D == 2 ? k.y : k.z;  // row (2D) / plane (3D) first tap
+        if (k.x + JT <= g.K[0] && k.y + JT <= g.K[1] && (D == 2 || k.z + JT <= g.K[2])) {
+          const int ja1 = max(0, -l10), jb1 = min(JT, ext[0] - l10);
+          const int lb = kr - lo[BD];
+          const int jab = max(0, band_lo - lb), jbb = min(JT, band_hi - lb);
+          float2 wr[JT], wi[JT];
+          if constexpr (SUB == 1) {
+#pragma unroll
+            for (int j1 = 0; j1 < JT; j1++) {
+              const float2 w = __ldg(Ws + j1);
+              wr[j1] = make_float2(w.x, w.x);
+              wi[j1] = make_float2(w.y, -w.y);
+            }
+          }
+          // lane's first column tap (class ls of SUB), then every SUB-th
+          const int j1s = ja1 + ((ls - l10 - ja1) & (SUB - 1));
+          auto row = [&](float2 *p, float2 v2) {
+            const float2 v2s = make_float2(v2.y, v2.x);
+            if constexpr (SUB == 1) {
+#pragma unroll
+              for (int j1 = 0; j1 < JT; j1++) {
+                if (j1 >= ja1 && j1 < jb1) {
+                  float2 A = p[j1 * CW];
+                  A = __ffma2_rn(wr[j1], v2, A);
+                  if (!REAL) A = __ffma2_rn(wi[j1], v2s, A);
+                  p[j1 * CW] = A;
+                }
+              }
+            } else {
+              for (int j1 = j1s; j1 < jb1; j1 += SUB) {
+                float2 A = p[j1 * CW];
+                A = cw_fma<REAL>(__ldg(Ws + j1), v2, v2s, A);
+                p[j1 * CW] = A;
+              }
+            }
+          };
+          float2 *base = acc + l10 * CW + lc;
+          if constexpr (D == 2) {
+            for (int j2 = jab; j2 < jbb; j2++) {
+              const float2 v2 = cw_mul<REAL>(__ldg(Ws + JT + j2), f);
+              row(base + (size_t)(lb + j2) * T0 * CW, v2);
+            }
+          } else {
+            const int l20 = k.y - lo[1];
+            const int ja2 = max(0, -l20), jb2 = min(JT, ext[1] - l20);
+            for (int j3 = jab; j3 < jbb; j3++) {
+              const float2 v3 = cw_mul<REAL>(__ldg(Ws + 2 * JT + j3), f);
+              float2 *pl = base + (size_t)(lb + j3) * T1 * T0 * CW;
+              for (int j2 = ja2; j2 < jb2; j2++) {
+                const float2 v2 = cw_mul<REAL>(__ldg(Ws + JT + j2), v3);
+                row(pl + (size_t)(l20 + j2) * T0 * CW, v2);
+              }
+            }
+          }
+          continue;
+        }
+      }
       if constexpr (D == 1) {
         const unsigned m1 = tap_mask<SUB>(k.x, Jd[0], g.K[0], lo[0], band_lo, band_hi, ls);
         spread_row<CW, JT, REAL>(acc + lc, Ws, Jd[0], false, l10, m1, k.x, g.K[0], lo[0], ls, f);

@@ -68,8 +68,8 @@ def minmax_kb_scale(N: int, J: int, K: int) -> np.ndarray:
 def _plan_config(lib, handle) -> dict:
     v = (C.c_int32 * 14)()
     check(lib.mirt_interp_plan_config(handle, v, 14))
-    return {"spread_tile": [v[0], v[1], v[2]], "spread_threads": v[3], "spread_batch": v[4],
-            "coil_lanes": v[5], "gather_threads": v[6], "gather_batch": v[7],
+    return {"spread_tile": [v[0], v[1], v[2]], "spread_threads": v[3], "spread_heavy_first": v[4],
+            "coil_lanes": v[5], "gather_threads": v[6],
             "gather_ctas": v[8], "sort_bin": [v[9], v[10], v[11]], "split_chunk": v[12],
             "spread_tasks": v[13]}
 
