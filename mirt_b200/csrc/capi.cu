@@ -155,7 +155,7 @@ struct mirt_interp_plan {
 
 namespace {
 
-// Launch shapes and tiling.  Samples are binned on 8-point bins (64 in 1D);
+// Launch shapes and tiling.  Samples are binned on 4-point bins (64 in 1D);
 // the spread runs one warp per tile (lanes = coils; the tile accumulator is
 // sized to keep several CTAs resident per SM).
 void choose_config(mirt_interp_plan *P) {
@@ -175,11 +175,11 @@ void choose_config(mirt_interp_plan *P) {
     B[0] = 64;
     T[0] = cw == 32 ? 64 : 256;
   } else if (D == 2) {
-    B[0] = B[1] = 8;
+    B[0] = B[1] = 4;
     const int e = cw == 32 ? 8 : cw == 8 ? 16 : 32;
     T[0] = T[1] = e;
   } else {
-    B[0] = B[1] = B[2] = 8;
+    B[0] = B[1] = B[2] = 4;
     T[0] = T[1] = T[2] = 8;
     if (cw <= 4) T[0] = 16;
   }

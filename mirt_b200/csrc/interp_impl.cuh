@@ -126,7 +126,7 @@ __device__ __forceinline__ float2 cw_fma(float2 w, float2 v, float2 vs, float2 A
 // of a row do not wrap they sit at a constant stride from one row pointer (a
 // compile-time stride when C == CW, CX).
 template <int D, int CW, int JT, bool REAL, bool CX>
-__global__ void __launch_bounds__(256, 3) gather_kernel(InterpArgs a, const float2 *__restrict__ ck,
+__global__ void __launch_bounds__(256, D == 3 ? 2 : 4) gather_kernel(InterpArgs a, const float2 *__restrict__ ck,
                                                      float2 *__restrict__ fm) {
   const Geom &g = a.g;
   int Jd[MIRT_DMAX] = {1, 1, 1};
@@ -431,24 +431,24 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t,
         mn = a.perm ? a.perm[pos + 1] : (int)(pos + 1);
       }
       const int kb = D == 1 ? k.x : (D == 2 ? k.y : k.z);
-      // warp-uniform: taps of the band dimension inside this warp's band
-      const unsigned mb = tap_mask<1>(kb, Jd[BD], g.K[BD], lo[BD], band_lo, band_hi, 0);
-      if (!mb) continue;
-      const float2 *Ws = a.W + pos * SJ;
-      float2 f = make_float2(0.f, 0.f);
-      if (lane_on) {
-        f = __ldg(fm + (long long)m * C + c0 + lc);
-        if (a.phase) f = cmulc(__ldg(a.phase + pos), f);
-      }
       const int l10 = k.x - lo[0];
+      const float2 *Ws = a.W + pos * SJ;
       if constexpr (JT > 0 && D >= 2) {
         // patch without periodic wrap: the in-tile taps of each dimension are
-        // one index range, walked with unrolled predicated loops
-        const int kr = D == 2 ? k.y : k.z;  // row (2D) / plane (3D) first tap
+        // one index range, walked with unrolled predicated loops.  A visit
+        // whose ranges are empty ends before any coefficient is loaded.
         if (k.x + JT <= g.K[0] && k.y + JT <= g.K[1] && (D == 2 || k.z + JT <= g.K[2])) {
           const int ja1 = max(0, -l10), jb1 = min(JT, ext[0] - l10);
-          const int lb = kr - lo[BD];
+          const int lb = kb - lo[BD];
           const int jab = max(0, band_lo - lb), jbb = min(JT, band_hi - lb);
+          const int l20 = k.y - lo[1];
+          const int ja2 = D == 3 ? max(0, -l20) : 0, jb2 = D == 3 ? min(JT, ext[1] - l20) : 1;
+          if (ja1 >= jb1 || jab >= jbb || ja2 >= jb2) continue;
+          float2 f = make_float2(0.f, 0.f);
+          if (lane_on) {
+            f = __ldg(fm + (long long)m * C + c0 + lc);
+            if (a.phase) f = cmulc(__ldg(a.phase + pos), f);
+          }
           float2 wr[JT], wi[JT];
           if constexpr (SUB == 1) {
 #pragma unroll
@@ -487,8 +487,6 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t,
               row(base + (size_t)(lb + j2) * T0 * CW, v2);
             }
           } else {
-            const int l20 = k.y - lo[1];
-            const int ja2 = max(0, -l20), jb2 = min(JT, ext[1] - l20);
             for (int j3 = jab; j3 < jbb; j3++) {
               const float2 v3 = cw_mul<REAL>(__ldg(Ws + 2 * JT + j3), f);
               float2 *pl = base + (size_t)(lb + j3) * T1 * T0 * CW;
@@ -500,6 +498,14 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t,
           }
           continue;
         }
+      }
+      // general path (periodic wrap inside the patch, or any J)
+      const unsigned mb = tap_mask<1>(kb, Jd[BD], g.K[BD], lo[BD], band_lo, band_hi, 0);
+      if (!mb) continue;
+      float2 f = make_float2(0.f, 0.f);
+      if (lane_on) {
+        f = __ldg(fm + (long long)m * C + c0 + lc);
+        if (a.phase) f = cmulc(__ldg(a.phase + pos), f);
       }
       if constexpr (D == 1) {
         const unsigned m1 = tap_mask<SUB>(k.x, Jd[0], g.K[0], lo[0], band_lo, band_hi, ls);
