@@ -367,11 +367,13 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t,
 #pragma unroll
   for (int d = 0; d < D; d++) Jd[d] = JT > 0 ? JT : g.J[d];
   const int SJ = a.SJ;
-  // staging chunk of SCH positions after the accumulator tile
-  int4 *Ks_s = reinterpret_cast<int4 *>(acc + (size_t)npts * CW);
-  float2 *F_s = reinterpret_cast<float2 *>(Ks_s + SCH);   // [SCH][CW]
-  float2 *W_s = F_s + SCH * CW;                            // [SCH][SJ]
-  int *M_s = reinterpret_cast<int *>(W_s + SCH * SJ);      // [SCH]
+  // staging chunk of SCH positions after the accumulator tile, whose size
+  // (npts * CW float2) need not be a multiple of 16 bytes: round up for int4
+  const size_t acc_bytes = ((size_t)npts * CW * sizeof(float2) + 15) & ~(size_t)15;
+  int4 *Ks_s = reinterpret_cast<int4 *>(smem + acc_bytes);  // [SCH]
+  float2 *F_s = reinterpret_cast<float2 *>(Ks_s + SCH);     // [SCH][CW]
+  float2 *W_s = F_s + SCH * CW;                              // [SCH][SJ]
+  int *M_s = reinterpret_cast<int *>(W_s + SCH * SJ);        // [SCH] sample index, -1: no tap here
 
   const int task = t.task_tile[blockIdx.x];
   const int2 vr = t.task_range[blockIdx.x];
@@ -431,21 +433,32 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t,
     const int nch = (int)min((long long)SCH, end - cp);
     // stage the chunk: every load below is independent, so all are in flight
     // together (one memory latency per chunk rather than per position)
+    // positions whose taps miss the tile (neighbouring-bin samples) are
+    // flagged here, so their coefficients and sample values are not loaded
     for (int e = threadIdx.x; e < nch; e += blockDim.x) {
-      Ks_s[e] = a.K0[cp + e];
-      M_s[e] = a.perm ? a.perm[cp + e] : (int)(cp + e);
-    }
-    {
-      const float2 *Wg = a.W + cp * SJ;
-      for (int e = threadIdx.x; e < nch * SJ; e += blockDim.x) W_s[e] = __ldg(Wg + e);
+      const int4 k = __ldg(a.K0 + cp + e);
+      bool hit = tap_mask<1>(k.x, Jd[0], g.K[0], lo[0], 0, ext[0], 0) != 0;
+      if (D > 1) hit = hit && tap_mask<1>(k.y, Jd[D > 1 ? 1 : 0], g.K[D > 1 ? 1 : 0], lo[D > 1 ? 1 : 0], 0,
+                                          ext[D > 1 ? 1 : 0], 0) != 0;
+      if (D > 2) hit = hit && tap_mask<1>(k.z, Jd[D > 2 ? 2 : 0], g.K[D > 2 ? 2 : 0], lo[D > 2 ? 2 : 0], 0,
+                                          ext[D > 2 ? 2 : 0], 0) != 0;
+      Ks_s[e] = k;
+      M_s[e] = hit ? (a.perm ? a.perm[cp + e] : (int)(cp + e)) : -1;
     }
     __syncthreads();
+    {
+      const float2 *Wg = a.W + cp * SJ;
+      for (int e = threadIdx.x; e < nch * SJ; e += blockDim.x)
+        if (M_s[e / SJ] >= 0) W_s[e] = __ldg(Wg + e);
+    }
 #pragma unroll 4
     for (int e = threadIdx.x; e < nch * CW; e += blockDim.x) {
       const int j = e / CW, cc = e - j * CW;
+      const int mj = M_s[j];
+      if (mj < 0) continue;
       float2 f = make_float2(0.f, 0.f);
       if (c0 + cc < C) {
-        f = __ldg(fm + (long long)M_s[j] * C + c0 + cc);
+        f = __ldg(fm + (long long)mj * C + c0 + cc);
         if (a.phase) f = cmulc(__ldg(a.phase + cp + j), f);
       }
       F_s[e] = f;
@@ -453,6 +466,7 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t,
     __syncthreads();
     for (int jc = 0; jc < nch; jc++) {
       const long long pos = cp + jc;
+      if (M_s[jc] < 0) continue;
       const int4 k = Ks_s[jc];
       const int kb = D == 1 ? k.x : (D == 2 ? k.y : k.z);
       const int l10 = k.x - lo[0];
@@ -685,7 +699,8 @@ struct Req {
 inline size_t spread_smem_bytes(const InterpArgs &a, const Tiling &t, const Launch &l) {
   size_t npts = 1;
   for (int d = 0; d < a.g.D; d++) npts *= t.T[d];
-  return npts * l.cw * 8 + (size_t)SCH * (16 + (size_t)l.cw * 8 + (size_t)a.SJ * 8 + 4) + 16;
+  return ((npts * l.cw * 8 + 15) & ~(size_t)15) +
+         (size_t)SCH * (16 + (size_t)l.cw * 8 + (size_t)a.SJ * 8 + 4) + 16;
 }
 
 template <int D, int CW, int JT, bool REAL, bool CX>
