@@ -331,7 +331,7 @@ __device__ __forceinline__ void spread_row(float2 *row, const float2 *Ws, int J1
     for (int j1 = (ls - l10) & (SUB - 1); j1 < J1; j1 += SUB) {
       float2 *p = row + (l10 + j1) * CW;
       float2 A = *p;
-      A = cw_fma<REAL>(Ws[j1], v2, v2s, A);
+      A = cw_fma<REAL>(__ldg(Ws + j1), v2, v2s, A);
       *p = A;
     }
   } else {
@@ -341,14 +341,11 @@ __device__ __forceinline__ void spread_row(float2 *row, const float2 *Ws, int J1
       mm &= mm - 1;
       float2 *p = row + tap_local(k10, j1, K1, lo1) * CW;
       float2 A = *p;
-      A = cw_fma<REAL>(Ws[j1], v2, v2s, A);
+      A = cw_fma<REAL>(__ldg(Ws + j1), v2, v2s, A);
       *p = A;
     }
   }
 }
-
-// positions staged per chunk by the spread
-constexpr int SCH = 32;
 
 template <int D, int CW, int JT, bool REAL>
 __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t,
@@ -367,13 +364,6 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t,
 #pragma unroll
   for (int d = 0; d < D; d++) Jd[d] = JT > 0 ? JT : g.J[d];
   const int SJ = a.SJ;
-  // staging chunk of SCH positions after the accumulator tile, whose size
-  // (npts * CW float2) need not be a multiple of 16 bytes: round up for int4
-  const size_t acc_bytes = ((size_t)npts * CW * sizeof(float2) + 15) & ~(size_t)15;
-  int4 *Ks_s = reinterpret_cast<int4 *>(smem + acc_bytes);  // [SCH]
-  float2 *F_s = reinterpret_cast<float2 *>(Ks_s + SCH);     // [SCH][CW]
-  float2 *W_s = F_s + SCH * CW;                              // [SCH][SJ]
-  int *M_s = reinterpret_cast<int *>(W_s + SCH * SJ);        // [SCH] sample index, -1: no tap here
 
   const int task = t.task_tile[blockIdx.x];
   const int2 vr = t.task_range[blockIdx.x];
@@ -411,6 +401,7 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t,
   const int T0 = t.T[0];
   const int T1 = D > 1 ? t.T[1] : 1;
   const int jb0 = D == 1 ? 0 : (D == 2 ? Jd[0] : Jd[0] + Jd[1]);  // first tap of dim BD
+  const bool lane_on = c0 + lc < C;
 
   long long vbase = 0;
   for (int si = 0; si < nsrc_tot && vbase < vr.y && band_lo < band_hi; si++) {
@@ -429,49 +420,19 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t,
     const long long end = b0 + min(b1 - b0, (long long)vr.y - vbase);
     vbase += b1 - b0;
     if (beg >= end) continue;
-    for (long long cp = beg; cp < end; cp += SCH) {
-    const int nch = (int)min((long long)SCH, end - cp);
-    // stage the chunk: every load below is independent, so all are in flight
-    // together (one memory latency per chunk rather than per position)
-    // positions whose taps miss the tile (neighbouring-bin samples) are
-    // flagged here, so their coefficients and sample values are not loaded
-    for (int e = threadIdx.x; e < nch; e += blockDim.x) {
-      const int4 k = __ldg(a.K0 + cp + e);
-      bool hit = tap_mask<1>(k.x, Jd[0], g.K[0], lo[0], 0, ext[0], 0) != 0;
-      if (D > 1) hit = hit && tap_mask<1>(k.y, Jd[D > 1 ? 1 : 0], g.K[D > 1 ? 1 : 0], lo[D > 1 ? 1 : 0], 0,
-                                          ext[D > 1 ? 1 : 0], 0) != 0;
-      if (D > 2) hit = hit && tap_mask<1>(k.z, Jd[D > 2 ? 2 : 0], g.K[D > 2 ? 2 : 0], lo[D > 2 ? 2 : 0], 0,
-                                          ext[D > 2 ? 2 : 0], 0) != 0;
-      Ks_s[e] = k;
-      M_s[e] = hit ? (a.perm ? a.perm[cp + e] : (int)(cp + e)) : -1;
-    }
-    __syncthreads();
-    {
-      const float2 *Wg = a.W + cp * SJ;
-      for (int e = threadIdx.x; e < nch * SJ; e += blockDim.x)
-        if (M_s[e / SJ] >= 0) W_s[e] = __ldg(Wg + e);
-    }
-#pragma unroll 4
-    for (int e = threadIdx.x; e < nch * CW; e += blockDim.x) {
-      const int j = e / CW, cc = e - j * CW;
-      const int mj = M_s[j];
-      if (mj < 0) continue;
-      float2 f = make_float2(0.f, 0.f);
-      if (c0 + cc < C) {
-        f = __ldg(fm + (long long)mj * C + c0 + cc);
-        if (a.phase) f = cmulc(__ldg(a.phase + cp + j), f);
+    // one position ahead: its first taps and sample index are in flight
+    int4 kn = a.K0[beg];
+    int mn = a.perm ? a.perm[beg] : (int)beg;
+    for (long long pos = beg; pos < end; pos++) {
+      const int4 k = kn;
+      const int m = mn;
+      if (pos + 1 < end) {
+        kn = a.K0[pos + 1];
+        mn = a.perm ? a.perm[pos + 1] : (int)(pos + 1);
       }
-      F_s[e] = f;
-    }
-    __syncthreads();
-    for (int jc = 0; jc < nch; jc++) {
-      const long long pos = cp + jc;
-      if (M_s[jc] < 0) continue;
-      const int4 k = Ks_s[jc];
       const int kb = D == 1 ? k.x : (D == 2 ? k.y : k.z);
       const int l10 = k.x - lo[0];
-      const float2 *Ws = W_s + jc * SJ;
-      (void)pos;
+      const float2 *Ws = a.W + pos * SJ;
       if constexpr (JT > 0 && D >= 2) {
         // patch without periodic wrap: the in-tile taps of each dimension are
         // one index range, walked with unrolled predicated loops.  A visit
@@ -483,12 +444,16 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t,
           const int l20 = k.y - lo[1];
           const int ja2 = D == 3 ? max(0, -l20) : 0, jb2 = D == 3 ? min(JT, ext[1] - l20) : 1;
           if (ja1 >= jb1 || jab >= jbb || ja2 >= jb2) continue;
-          const float2 f = F_s[jc * CW + lc];
+          float2 f = make_float2(0.f, 0.f);
+          if (lane_on) {
+            f = __ldg(fm + (long long)m * C + c0 + lc);
+            if (a.phase) f = cmulc(__ldg(a.phase + pos), f);
+          }
           float2 wr[JT], wi[JT];
           if constexpr (SUB == 1) {
 #pragma unroll
             for (int j1 = 0; j1 < JT; j1++) {
-              const float2 w = Ws[j1];
+              const float2 w = __ldg(Ws + j1);
               wr[j1] = make_float2(w.x, w.x);
               wi[j1] = make_float2(w.y, -w.y);
             }
@@ -510,7 +475,7 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t,
             } else {
               for (int j1 = j1s; j1 < jb1; j1 += SUB) {
                 float2 A = p[j1 * CW];
-                A = cw_fma<REAL>(Ws[j1], v2, v2s, A);
+                A = cw_fma<REAL>(__ldg(Ws + j1), v2, v2s, A);
                 p[j1 * CW] = A;
               }
             }
@@ -518,15 +483,15 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t,
           float2 *base = acc + l10 * CW + lc;
           if constexpr (D == 2) {
             for (int j2 = jab; j2 < jbb; j2++) {
-              const float2 v2 = cw_mul<REAL>(Ws[JT + j2], f);
+              const float2 v2 = cw_mul<REAL>(__ldg(Ws + JT + j2), f);
               row(base + (size_t)(lb + j2) * T0 * CW, v2);
             }
           } else {
             for (int j3 = jab; j3 < jbb; j3++) {
-              const float2 v3 = cw_mul<REAL>(Ws[2 * JT + j3], f);
+              const float2 v3 = cw_mul<REAL>(__ldg(Ws + 2 * JT + j3), f);
               float2 *pl = base + (size_t)(lb + j3) * T1 * T0 * CW;
               for (int j2 = ja2; j2 < jb2; j2++) {
-                const float2 v2 = cw_mul<REAL>(Ws[JT + j2], v3);
+                const float2 v2 = cw_mul<REAL>(__ldg(Ws + JT + j2), v3);
                 row(pl + (size_t)(l20 + j2) * T0 * CW, v2);
               }
             }
@@ -537,7 +502,11 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t,
       // general path (periodic wrap inside the patch, or any J)
       const unsigned mb = tap_mask<1>(kb, Jd[BD], g.K[BD], lo[BD], band_lo, band_hi, 0);
       if (!mb) continue;
-      const float2 f = F_s[jc * CW + lc];
+      float2 f = make_float2(0.f, 0.f);
+      if (lane_on) {
+        f = __ldg(fm + (long long)m * C + c0 + lc);
+        if (a.phase) f = cmulc(__ldg(a.phase + pos), f);
+      }
       if constexpr (D == 1) {
         const unsigned m1 = tap_mask<SUB>(k.x, Jd[0], g.K[0], lo[0], band_lo, band_hi, ls);
         spread_row<CW, JT, REAL>(acc + lc, Ws, Jd[0], false, l10, m1, k.x, g.K[0], lo[0], ls, f);
@@ -554,7 +523,7 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t,
               float2 wr[JT], wi[JT];
 #pragma unroll
               for (int j1 = 0; j1 < JT; j1++) {
-                const float2 w = Ws[j1];
+                const float2 w = __ldg(Ws + j1);
                 wr[j1] = make_float2(w.x, w.x);
                 wi[j1] = make_float2(w.y, -w.y);
               }
@@ -564,7 +533,7 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t,
                 const int j2 = __ffs(m2) - 1;
                 m2 &= m2 - 1;
                 const int l2 = tap_local(k.y, j2, g.K[1], lo[1]);
-                const float2 v2 = cw_mul<REAL>(Ws[JT + j2], f);
+                const float2 v2 = cw_mul<REAL>(__ldg(Ws + JT + j2), f);
                 const float2 v2s = make_float2(v2.y, v2.x);
                 float2 *p = base + (size_t)l2 * T0 * CW;
 #pragma unroll
@@ -583,7 +552,7 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t,
             const int j2 = __ffs(m2) - 1;
             m2 &= m2 - 1;
             const int l2 = tap_local(k.y, j2, g.K[1], lo[1]);
-            const float2 v2 = cw_mul<REAL>(Ws[Jd[0] + j2], f);
+            const float2 v2 = cw_mul<REAL>(__ldg(Ws + Jd[0] + j2), f);
             spread_row<CW, JT, REAL>(acc + (size_t)l2 * T0 * CW + lc, Ws, Jd[0], fast1, l10, m1,
                                      k.x, g.K[0], lo[0], ls, v2);
           }
@@ -595,21 +564,19 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t,
             const int j3 = __ffs(m3) - 1;
             m3 &= m3 - 1;
             const int l3 = tap_local(k.z, j3, g.K[2], lo[2]);
-            const float2 v3 = cw_mul<REAL>(Ws[jb0 + j3], f);
+            const float2 v3 = cw_mul<REAL>(__ldg(Ws + jb0 + j3), f);
             unsigned m2 = m2all;
             while (m2) {
               const int j2 = __ffs(m2) - 1;
               m2 &= m2 - 1;
               const int l2 = tap_local(k.y, j2, g.K[1], lo[1]);
-              const float2 v2 = cw_mul<REAL>(Ws[Jd[0] + j2], v3);
+              const float2 v2 = cw_mul<REAL>(__ldg(Ws + Jd[0] + j2), v3);
               spread_row<CW, JT, REAL>(acc + ((size_t)l3 * T1 + l2) * T0 * CW + lc, Ws, Jd[0],
                                        fast1, l10, m1, k.x, g.K[0], lo[0], ls, v2);
             }
           }
         }
       }
-    }
-    __syncthreads();
     }
   }
   __syncthreads();
@@ -699,8 +666,7 @@ struct Req {
 inline size_t spread_smem_bytes(const InterpArgs &a, const Tiling &t, const Launch &l) {
   size_t npts = 1;
   for (int d = 0; d < a.g.D; d++) npts *= t.T[d];
-  return ((npts * l.cw * 8 + 15) & ~(size_t)15) +
-         (size_t)SCH * (16 + (size_t)l.cw * 8 + (size_t)a.SJ * 8 + 4) + 16;
+  return npts * l.cw * 8;
 }
 
 template <int D, int CW, int JT, bool REAL, bool CX>
