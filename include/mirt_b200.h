@@ -234,6 +234,35 @@ int mirt_nufft_autotune(mirt_nufft *p, void *stream);
 
 int mirt_nufft_destroy(mirt_nufft *p);
 
+/* ------------------------------------------------------------------------
+ * 4. forward gather for callers that cannot allocate device memory (no
+ *    counterpart in the reference, whose mex files run on the host)
+ *
+ * Code that runs during CUDA-graph stream capture, hosts whose device memory
+ * belongs to their own pool, and real-time loops that must not stall on an
+ * allocation cannot call cudaMalloc.  This entry point runs the table gather
+ * fm = interp(ck) on the caller's device buffers and allocates nothing: its
+ * scratch (per-sample tap coefficients and first taps) is a fixed array of
+ * MIRT_NOALLOC_SCRATCH_BYTES inside the library, held by every GPU that loads
+ * the library until the process exits.  M is limited to
+ * floor((MIRT_NOALLOC_SCRATCH_BYTES - 256) / (8 * (J1 + ... + JD) + 16))
+ * samples (299,593 for J = 6 in 2D); larger M is rejected with
+ * MIRT_ERR_ARG.  The first call on a device looks up the array's device
+ * address, so make that first call before any stream capture.  All calls share
+ * the array, which keeps the last call's contents (every call rewrites what it
+ * reads, so nothing needs clearing): calls that overlap on the GPU, on any
+ * streams, race.
+ *   tab[d]   device FP32 tables, float2 (complex, real_tab = 0) or float
+ *            (real_tab = 1), J[d]*L[d]+1 entries
+ *   tm       device FP64 [M, D] column-major, t = omega / (2 pi / K)
+ *   ck       device float2 grid [K_D]...[K_1][ncol] (column innermost)
+ *   fm       device float2 samples [M][ncol]
+ * Asynchronous on `stream`. */
+#define MIRT_NOALLOC_SCRATCH_BYTES (32u << 20)
+int mirt_interp_gather_noalloc(int32_t D, const int32_t *K, const int32_t *J,
+	const int32_t *L, const void *const *tab, int32_t real_tab, int32_t order,
+	const double *tm, int64_t M, int32_t ncol, const void *ck, void *fm, void *stream);
+
 /* Host FP64 builders used by mirt_nufft_create, exported for callers that
  * build their own plans (st.h{d} and the 1D factors of st.sn):
  *   table: length J*L+1 complex, nufft/nufft_table_init.m:111-134

@@ -138,6 +138,11 @@ int device_ok() {
 
 }  // namespace
 
+namespace mirt {
+// Record an error for mirt_last_error() from another translation unit.
+int api_fail(int code, const std::string &msg) { return fail(code, msg); }
+}  // namespace mirt
+
 // ---------------------------------------------------------------------------
 // interpolation plan
 // ---------------------------------------------------------------------------
