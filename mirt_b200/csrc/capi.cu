@@ -1161,7 +1161,7 @@ struct mirt_nufft {
   GlueGeom gg{};
   int C = 0, nslice = 0;
   long long Mtot = 0;
-  DMem sn, grid, hx, hX;
+  DMem sn, grid, grid_cm, hx, hX;  // grid: coil innermost (interp); grid_cm: coil-major (FFT)
   cufftHandle fft = 0;
   bool fft_ok = false;
   ~mirt_nufft() {
@@ -1179,13 +1179,11 @@ namespace {
       return fail(MIRT_ERR_FFT, std::string(#call) + " failed: " + std::to_string((int)r_)); \
   } while (0)
 
+// one batched C2C execution over every slice and coil of the coil-major grid
 int nufft_fft(mirt_nufft *p, int dir, cudaStream_t st) {
   CF(cufftSetStream(p->fft, st));
-  const long long per = p->gg.ngrid * p->C;
-  for (int s = 0; s < p->nslice; s++) {
-    cufftComplex *g = reinterpret_cast<cufftComplex *>(p->grid.as<float2>() + s * per);
-    CF(cufftExecC2C(p->fft, g, g, dir));
-  }
+  cufftComplex *g = reinterpret_cast<cufftComplex *>(p->grid_cm.as<float2>());
+  CF(cufftExecC2C(p->fft, g, g, dir));
   return MIRT_OK;
 }
 
@@ -1333,12 +1331,17 @@ int mirt_nufft_create(mirt_nufft **out, int32_t D, const int32_t *Nd, const int3
   if (rc) return bail(rc);
   {
     cudaError_t e = p->grid.alloc((size_t)nslice * p->gg.ngrid * ncol * sizeof(float2));
-    if (e != cudaSuccess) return bail(fail(MIRT_ERR_ALLOC, "NUFFT grid buffer"));
+    if (e == cudaSuccess) e = p->grid_cm.alloc((size_t)nslice * p->gg.ngrid * ncol * sizeof(float2));
+    if (e != cudaSuccess) return bail(fail(MIRT_ERR_ALLOC, "NUFFT grid buffers"));
   }
+  // contiguous C2C transforms, one per (slice, coil) plane of the coil-major grid
   int n[3];
   for (int d = 0; d < D; d++) n[d] = Kd[D - 1 - d];
   if (ncol > 0) {
-    cufftResult r = cufftPlanMany(&p->fft, D, n, n, ncol, 1, n, ncol, 1, CUFFT_C2C, ncol);
+    const long long batch = (long long)nslice * ncol;
+    if (batch >= (1ll << 31)) return bail(fail(MIRT_ERR_ARG, "too many FFT planes"));
+    cufftResult r = cufftPlanMany(&p->fft, D, n, nullptr, 1, (int)p->gg.ngrid, nullptr, 1,
+                                  (int)p->gg.ngrid, CUFFT_C2C, (int)batch);
     if (r != CUFFT_SUCCESS)
       return bail(fail(MIRT_ERR_FFT, "cufftPlanMany failed: " + std::to_string((int)r)));
     p->fft_ok = true;
@@ -1355,10 +1358,12 @@ int mirt_nufft_forward(mirt_nufft *p, const void *x, void *X, void *stream) {
   if (!p) return fail(MIRT_ERR_ARG, "nufft is NULL");
   if (p->C == 0) return MIRT_OK;
   cudaStream_t st = as_stream(stream);
-  CK(launch_deapod_pad(static_cast<const float2 *>(x), p->sn.as<float2>(), p->grid.as<float2>(),
-                       p->gg, p->C, p->nslice, st));
+  CK(launch_deapod_pad_cm(static_cast<const float2 *>(x), p->sn.as<float2>(),
+                          p->grid_cm.as<float2>(), p->gg, p->C, p->nslice, st));
   int rc = nufft_fft(p, CUFFT_FORWARD, st);
   if (rc) return rc;
+  CK(launch_transpose_cols(p->grid_cm.as<float2>(), p->grid.as<float2>(), p->gg.ngrid, p->C,
+                           p->nslice, 1, st));
   CK(launch_gather(p->ip->a, p->ip->lg, p->grid.as<float2>(), static_cast<float2 *>(X), st));
   return MIRT_OK;
 }
@@ -1370,10 +1375,12 @@ int mirt_nufft_adjoint(mirt_nufft *p, const void *X, void *x, void *stream) {
   mirt_interp_plan *P = p->ip;
   CK(launch_spread(P->a, P->t, P->ls, P->bin_start.as<int>(), static_cast<const float2 *>(X),
                    p->grid.as<float2>(), st));
+  CK(launch_transpose_cols(p->grid.as<float2>(), p->grid_cm.as<float2>(), p->gg.ngrid, p->C,
+                           p->nslice, 0, st));
   int rc = nufft_fft(p, CUFFT_INVERSE, st);
   if (rc) return rc;
-  CK(launch_crop_deapod(p->grid.as<float2>(), p->sn.as<float2>(), static_cast<float2 *>(x), p->gg,
-                        p->C, p->nslice, st));
+  CK(launch_crop_deapod_cm(p->grid_cm.as<float2>(), p->sn.as<float2>(), static_cast<float2 *>(x),
+                           p->gg, p->C, p->nslice, st));
   return MIRT_OK;
 }
 

@@ -1,9 +1,12 @@
 // glue.cu -- elementwise kernels around the interpolation and the FFT.
 //
-//   deapod_pad   x .* sn, zero-padded at the end of every dimension to Kd
-//                (nufft/nufft.m:139-140, nufft/fftn_fast.m:22-26)
-//   crop_deapod  crop [Kd] -> [Nd] and multiply by conj(sn)
-//                (nufft/nufft_adj.m:63-80)
+//   deapod_pad_cm   x .* sn, zero-padded at the end of every dimension to Kd
+//                   (nufft/nufft.m:139-140, nufft/fftn_fast.m:22-26), written coil-major
+//                   for the batched FFT
+//   crop_deapod_cm  crop [Kd] -> [Nd] and multiply by conj(sn) (nufft/nufft_adj.m:63-80),
+//                   from the coil-major FFT output back to the coil-innermost image
+//   transpose_cols  coil-major <-> coil-innermost grid between the FFT and the
+//                   interpolation
 //   om_to_tm     tm = om / (2 pi / K) in FP64 and the n_shift phase
 //                exp(i om . n_shift) (nufft/nufft_table_interp.m:36-40,
 //                nufft/nufft_table_init.m:48-50)
@@ -13,56 +16,129 @@
 
 namespace mirt {
 
-__global__ void deapod_pad_kernel(const float2 *__restrict__ x, const float2 *__restrict__ sn,
-                                  float2 *__restrict__ grid, GlueGeom g, int C, int nslice) {
-  const long long total = g.ngrid * C;
-  const long long per = total;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < per * nslice;
-       i += (long long)gridDim.x * blockDim.x) {
-    const long long s = i / per;
-    const long long r = i - s * per;
-    const long long k = r / C;
-    const int c = (int)(r - k * C);
-    long long rem = k;
-    long long n = 0, nstr = 1;
-    bool inside = true;
-    for (int d = 0; d < g.D; d++) {
-      const long long kd = rem % g.K[d];
-      rem /= g.K[d];
-      if (kd >= g.N[d]) inside = false;
-      n += kd * nstr;
-      nstr *= g.N[d];
-    }
+// x[s][n][c] (coil innermost) .* sn  ->  grid[s][c][k] (coil outermost, zero-padded
+// to K at the end of every dimension), as a tiled transpose: a CTA takes 32
+// consecutive k1 of one grid row and 32 coils.
+__global__ void deapod_pad_cm_kernel(const float2 *__restrict__ x, const float2 *__restrict__ sn,
+                                     float2 *__restrict__ grid, GlueGeom g, int C) {
+  __shared__ float2 tile[32][33];
+  const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
+  const int k1_0 = blockIdx.y * 32;
+  const long long row = blockIdx.x;               // k2 + K2*k3 (+ slice)
+  const int c0 = blockIdx.z * 32;
+  const long long rows_per_slice = g.ngrid / g.K[0];
+  const long long s = row / rows_per_slice;
+  const long long r = row - s * rows_per_slice;
+  // image row of this grid row (inside the N region in every dimension > 0?)
+  long long nrow = 0, nstr = 1, rem = r;
+  bool inside = true;
+  for (int d = 1; d < g.D; d++) {
+    const long long kd = rem % g.K[d];
+    rem /= g.K[d];
+    if (kd >= g.N[d]) inside = false;
+    nrow += kd * nstr;
+    nstr *= g.N[d];
+  }
+  // load: x[s][nrow*N1 + k1][c], coil fastest
+  for (int i = ty; i < 32; i += 8) {
+    const int k1 = k1_0 + i;
+    const int c = c0 + tx;
     float2 v = make_float2(0.f, 0.f);
-    if (inside) {
+    if (inside && k1 < g.N[0] && c < C) {
+      const long long n = nrow * g.N[0] + k1;
       const float2 a = x[(s * g.npix + n) * C + c];
       const float2 b = sn[n];
       v = make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
     }
-    grid[i] = v;
+    tile[i][tx] = v;
+  }
+  __syncthreads();
+  // store: grid[s][c][r*K1 + k1], k1 fastest
+  for (int i = ty; i < 32; i += 8) {
+    const int c = c0 + i;
+    const int k1 = k1_0 + tx;
+    if (c < C && k1 < g.K[0])
+      grid[((s * C + c) * rows_per_slice + r) * g.K[0] + k1] = tile[tx][i];
   }
 }
 
-__global__ void crop_deapod_kernel(const float2 *__restrict__ grid, const float2 *__restrict__ sn,
-                                   float2 *__restrict__ x, GlueGeom g, int C, int nslice) {
-  const long long per = g.npix * C;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < per * nslice;
-       i += (long long)gridDim.x * blockDim.x) {
-    const long long s = i / per;
-    const long long r = i - s * per;
-    const long long n = r / C;
-    const int c = (int)(r - n * C);
-    long long rem = n, k = 0, kstr = 1;
-    for (int d = 0; d < g.D; d++) {
-      const long long nd = rem % g.N[d];
-      rem /= g.N[d];
-      k += nd * kstr;
-      kstr *= g.K[d];
+// grid[s][c][k] (coil outermost)  ->  crop to N, .* conj(sn)  ->  x[s][n][c]
+__global__ void crop_deapod_cm_kernel(const float2 *__restrict__ grid,
+                                      const float2 *__restrict__ sn, float2 *__restrict__ x,
+                                      GlueGeom g, int C) {
+  __shared__ float2 tile[32][33];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int n1_0 = blockIdx.y * 32;
+  const long long row = blockIdx.x;               // image row n2 + N2*n3 (+ slice)
+  const int c0 = blockIdx.z * 32;
+  const long long rows_per_slice = g.npix / g.N[0];
+  const long long s = row / rows_per_slice;
+  const long long r = row - s * rows_per_slice;
+  const long long krows = g.ngrid / g.K[0];
+  long long krow = 0, kstr = 1, rem = r;
+  for (int d = 1; d < g.D; d++) {
+    const long long nd = rem % g.N[d];
+    rem /= g.N[d];
+    krow += nd * kstr;
+    kstr *= g.K[d];
+  }
+  for (int i = ty; i < 32; i += 8) {
+    const int c = c0 + i;
+    const int n1 = n1_0 + tx;
+    float2 v = make_float2(0.f, 0.f);
+    if (c < C && n1 < g.N[0]) v = grid[((s * C + c) * krows + krow) * g.K[0] + n1];
+    tile[i][tx] = v;
+  }
+  __syncthreads();
+  for (int i = ty; i < 32; i += 8) {
+    const int n1 = n1_0 + i;
+    const int c = c0 + tx;
+    if (c < C && n1 < g.N[0]) {
+      const long long n = r * g.N[0] + n1;
+      const float2 a = tile[tx][i];
+      const float2 b = sn[n];
+      // a * conj(b)
+      x[(s * g.npix + n) * C + c] = make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
     }
-    const float2 a = grid[(s * g.ngrid + k) * C + c];
-    const float2 b = sn[n];
-    // a * conj(b)
-    x[i] = make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+  }
+}
+
+// [B][P] <-> [P][B] per slice: out[s][p][b] = in[s][b][p] (to_cl) or the reverse.
+__global__ void transpose_cols_kernel(const float2 *__restrict__ in, float2 *__restrict__ out,
+                                      long long P, int B, int to_cl) {
+  __shared__ float2 tile[32][33];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const long long p0 = (long long)blockIdx.x * 32;
+  const int b0 = blockIdx.y * 32;
+  const long long s = blockIdx.z;
+  const float2 *src = in + s * P * B;
+  float2 *dst = out + s * P * B;
+  if (to_cl) {
+    // src [B][P] -> dst [P][B]
+    for (int i = ty; i < 32; i += 8) {
+      const int b = b0 + i;
+      const long long p = p0 + tx;
+      if (b < B && p < P) tile[i][tx] = src[(long long)b * P + p];
+    }
+    __syncthreads();
+    for (int i = ty; i < 32; i += 8) {
+      const long long p = p0 + i;
+      const int b = b0 + tx;
+      if (b < B && p < P) dst[p * B + b] = tile[tx][i];
+    }
+  } else {
+    // src [P][B] -> dst [B][P]
+    for (int i = ty; i < 32; i += 8) {
+      const long long p = p0 + i;
+      const int b = b0 + tx;
+      if (b < B && p < P) tile[i][tx] = src[p * B + b];
+    }
+    __syncthreads();
+    for (int i = ty; i < 32; i += 8) {
+      const int b = b0 + i;
+      const long long p = p0 + tx;
+      if (b < B && p < P) dst[(long long)b * P + p] = tile[tx][i];
+    }
   }
 }
 
@@ -173,17 +249,27 @@ static unsigned grid_for(long long n, int thr, int maxb = 148 * 32) {
   return (unsigned)b;
 }
 
-cudaError_t launch_deapod_pad(const float2 *x, const float2 *sn, float2 *grid, const GlueGeom &g,
-                              int C, int nslice, cudaStream_t st) {
-  const long long n = g.ngrid * C * nslice;
-  deapod_pad_kernel<<<grid_for(n, 256), 256, 0, st>>>(x, sn, grid, g, C, nslice);
+cudaError_t launch_deapod_pad_cm(const float2 *x, const float2 *sn, float2 *grid,
+                                 const GlueGeom &g, int C, int nslice, cudaStream_t st) {
+  const long long rows = g.ngrid / g.K[0] * nslice;
+  dim3 grid_dim((unsigned)rows, (unsigned)((g.K[0] + 31) / 32), (unsigned)((C + 31) / 32));
+  deapod_pad_cm_kernel<<<grid_dim, dim3(32, 8), 0, st>>>(x, sn, grid, g, C);
   return cudaGetLastError();
 }
 
-cudaError_t launch_crop_deapod(const float2 *grid, const float2 *sn, float2 *x, const GlueGeom &g,
-                               int C, int nslice, cudaStream_t st) {
-  const long long n = g.npix * C * nslice;
-  crop_deapod_kernel<<<grid_for(n, 256), 256, 0, st>>>(grid, sn, x, g, C, nslice);
+cudaError_t launch_crop_deapod_cm(const float2 *grid, const float2 *sn, float2 *x,
+                                  const GlueGeom &g, int C, int nslice, cudaStream_t st) {
+  const long long rows = g.npix / g.N[0] * nslice;
+  dim3 grid_dim((unsigned)rows, (unsigned)((g.N[0] + 31) / 32), (unsigned)((C + 31) / 32));
+  crop_deapod_cm_kernel<<<grid_dim, dim3(32, 8), 0, st>>>(grid, sn, x, g, C);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_transpose_cols(const float2 *in, float2 *out, long long P, int B, int nslice,
+                                  int to_cl, cudaStream_t st) {
+  if (P == 0 || B == 0 || nslice == 0) return cudaSuccess;
+  dim3 grid_dim((unsigned)((P + 31) / 32), (unsigned)((B + 31) / 32), (unsigned)nslice);
+  transpose_cols_kernel<<<grid_dim, dim3(32, 8), 0, st>>>(in, out, P, B, to_cl);
   return cudaGetLastError();
 }
 

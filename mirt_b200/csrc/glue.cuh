@@ -13,10 +13,15 @@ struct GlueGeom {
   long long ngrid;     // prod(K)
 };
 
-cudaError_t launch_deapod_pad(const float2 *x, const float2 *sn, float2 *grid, const GlueGeom &g,
-                              int C, int nslice, cudaStream_t st);
-cudaError_t launch_crop_deapod(const float2 *grid, const float2 *sn, float2 *x, const GlueGeom &g,
-                               int C, int nslice, cudaStream_t st);
+// image x[s][n][c] -> sn-scaled, zero-padded grid[s][c][k] (coil-major)
+cudaError_t launch_deapod_pad_cm(const float2 *x, const float2 *sn, float2 *grid,
+                                 const GlueGeom &g, int C, int nslice, cudaStream_t st);
+// coil-major grid[s][c][k] -> cropped, conj(sn)-scaled image x[s][n][c]
+cudaError_t launch_crop_deapod_cm(const float2 *grid, const float2 *sn, float2 *x,
+                                  const GlueGeom &g, int C, int nslice, cudaStream_t st);
+// per slice: to_cl = 1: [B][P] -> [P][B]; to_cl = 0: [P][B] -> [B][P]
+cudaError_t launch_transpose_cols(const float2 *in, float2 *out, long long P, int B, int nslice,
+                                  int to_cl, cudaStream_t st);
 cudaError_t launch_om_to_tm(const double *om, long long M, int D, const double *gam_dev,
                             const double *nshift_dev, int want_phase, double *tm, float2 *phase,
                             cudaStream_t st);
