@@ -420,46 +420,15 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t,
     const long long end = b0 + min(b1 - b0, (long long)vr.y - vbase);
     vbase += b1 - b0;
     if (beg >= end) continue;
-    // software pipeline: while position pos is processed, the record, sample
-    // value and (fixed J) coefficients of pos + 1 and the sample index of
-    // pos + 2 are already in flight
-    constexpr int NWR = JT > 0 ? D * JT : 1;
-    auto load_f = [&](int mi, long long pi) -> float2 {
-      float2 v = make_float2(0.f, 0.f);
-      if (lane_on) {
-        v = __ldg(fm + (long long)mi * C + c0 + lc);
-        if (a.phase) v = cmulc(__ldg(a.phase + pi), v);
-      }
-      return v;
-    };
-    auto load_w = [&](long long pi, float2 *w) {
-      if constexpr (JT > 0) {
-        const float4 *W4 = reinterpret_cast<const float4 *>(a.W + pi * SJ);
-#pragma unroll
-        for (int q = 0; q < NWR / 2; q++) {
-          const float4 v = __ldg(W4 + q);
-          w[2 * q] = make_float2(v.x, v.y);
-          w[2 * q + 1] = make_float2(v.z, v.w);
-        }
-      }
-    };
+    // one position ahead: its first taps and sample index are in flight
     int4 kn = a.K0[beg];
     int mn = a.perm ? a.perm[beg] : (int)beg;
-    int mnn = (beg + 1 < end) ? (a.perm ? a.perm[beg + 1] : (int)(beg + 1)) : 0;
-    float2 fn = load_f(mn, beg);
-    float2 wn[NWR];
-    load_w(beg, wn);
     for (long long pos = beg; pos < end; pos++) {
       const int4 k = kn;
-      const float2 f = fn;
-      float2 w[NWR];
-#pragma unroll
-      for (int q = 0; q < NWR; q++) w[q] = wn[q];
+      const int m = mn;
       if (pos + 1 < end) {
         kn = a.K0[pos + 1];
-        fn = load_f(mnn, pos + 1);
-        load_w(pos + 1, wn);
-        if (pos + 2 < end) mnn = a.perm ? a.perm[pos + 2] : (int)(pos + 2);
+        mn = a.perm ? a.perm[pos + 1] : (int)(pos + 1);
       }
       const int kb = D == 1 ? k.x : (D == 2 ? k.y : k.z);
       const int l10 = k.x - lo[0];
@@ -475,12 +444,18 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t,
           const int l20 = k.y - lo[1];
           const int ja2 = D == 3 ? max(0, -l20) : 0, jb2 = D == 3 ? min(JT, ext[1] - l20) : 1;
           if (ja1 >= jb1 || jab >= jbb || ja2 >= jb2) continue;
+          float2 f = make_float2(0.f, 0.f);
+          if (lane_on) {
+            f = __ldg(fm + (long long)m * C + c0 + lc);
+            if (a.phase) f = cmulc(__ldg(a.phase + pos), f);
+          }
           float2 wr[JT], wi[JT];
           if constexpr (SUB == 1) {
 #pragma unroll
             for (int j1 = 0; j1 < JT; j1++) {
-              wr[j1] = make_float2(w[j1].x, w[j1].x);
-              wi[j1] = make_float2(w[j1].y, -w[j1].y);
+              const float2 w = __ldg(Ws + j1);
+              wr[j1] = make_float2(w.x, w.x);
+              wi[j1] = make_float2(w.y, -w.y);
             }
           }
           // lane's first column tap (class ls of SUB), then every SUB-th
@@ -498,38 +473,26 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t,
                 }
               }
             } else {
-#pragma unroll
-              for (int j1 = 0; j1 < JT; j1++) {
-                if (j1 >= j1s && j1 < jb1 && ((j1 - j1s) & (SUB - 1)) == 0) {
-                  float2 A = p[j1 * CW];
-                  A = cw_fma<REAL>(w[j1], v2, v2s, A);
-                  p[j1 * CW] = A;
-                }
+              for (int j1 = j1s; j1 < jb1; j1 += SUB) {
+                float2 A = p[j1 * CW];
+                A = cw_fma<REAL>(__ldg(Ws + j1), v2, v2s, A);
+                p[j1 * CW] = A;
               }
             }
           };
           float2 *base = acc + l10 * CW + lc;
           if constexpr (D == 2) {
-#pragma unroll
-            for (int j2 = 0; j2 < JT; j2++) {
-              if (j2 >= jab && j2 < jbb) {
-                const float2 v2 = cw_mul<REAL>(w[JT + j2], f);
-                row(base + (size_t)(lb + j2) * T0 * CW, v2);
-              }
+            for (int j2 = jab; j2 < jbb; j2++) {
+              const float2 v2 = cw_mul<REAL>(__ldg(Ws + JT + j2), f);
+              row(base + (size_t)(lb + j2) * T0 * CW, v2);
             }
           } else {
-#pragma unroll
-            for (int j3 = 0; j3 < JT; j3++) {
-              if (j3 >= jab && j3 < jbb) {
-                const float2 v3 = cw_mul<REAL>(w[2 * JT + j3], f);
-                float2 *pl = base + (size_t)(lb + j3) * T1 * T0 * CW;
-#pragma unroll
-                for (int j2 = 0; j2 < JT; j2++) {
-                  if (j2 >= ja2 && j2 < jb2) {
-                    const float2 v2 = cw_mul<REAL>(w[JT + j2], v3);
-                    row(pl + (size_t)(l20 + j2) * T0 * CW, v2);
-                  }
-                }
+            for (int j3 = jab; j3 < jbb; j3++) {
+              const float2 v3 = cw_mul<REAL>(__ldg(Ws + 2 * JT + j3), f);
+              float2 *pl = base + (size_t)(lb + j3) * T1 * T0 * CW;
+              for (int j2 = ja2; j2 < jb2; j2++) {
+                const float2 v2 = cw_mul<REAL>(__ldg(Ws + JT + j2), v3);
+                row(pl + (size_t)(l20 + j2) * T0 * CW, v2);
               }
             }
           }
@@ -539,6 +502,11 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t,
       // general path (periodic wrap inside the patch, or any J)
       const unsigned mb = tap_mask<1>(kb, Jd[BD], g.K[BD], lo[BD], band_lo, band_hi, 0);
       if (!mb) continue;
+      float2 f = make_float2(0.f, 0.f);
+      if (lane_on) {
+        f = __ldg(fm + (long long)m * C + c0 + lc);
+        if (a.phase) f = cmulc(__ldg(a.phase + pos), f);
+      }
       if constexpr (D == 1) {
         const unsigned m1 = tap_mask<SUB>(k.x, Jd[0], g.K[0], lo[0], band_lo, band_hi, ls);
         spread_row<CW, JT, REAL>(acc + lc, Ws, Jd[0], false, l10, m1, k.x, g.K[0], lo[0], ls, f);
