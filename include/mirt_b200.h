@@ -193,11 +193,22 @@ int mirt_interp_plan_adjoint(mirt_interp_plan *plan, const void *fm, void *ck, v
  * bitwise deterministic for any choice. */
 int mirt_interp_plan_autotune(mirt_interp_plan *plan, void *stream);
 
-/* Current launch configuration: up to 14 values
+/* Current launch configuration: up to 15 values
  * {T1, T2, T3, spread threads, spread heavy-first order, coil lanes,
  *  gather threads, (unused), gather CTAs, B1, B2, B3, split chunk,
- *  spread tasks}. */
+ *  spread tasks, spare tile columns}. */
 int mirt_interp_plan_config(mirt_interp_plan *plan, int32_t *out, int32_t n);
+
+/* Fix the spread's tiling instead of autotuning it: tile extents T[0..D-1]
+ * (multiples of the sort bins B of mirt_interp_plan_config, at most the grid
+ * extent rounded up to a bin), CTA size `threads` (a multiple of 32, each
+ * warp owns a band of the tile) and `padc` spare columns per tile row side in
+ * shared memory (0, or J1 - 1 = 5 for the J = 6 kernels in 2D/3D: the row
+ * update then needs no bounds tests).  Results are identical to rounding for
+ * every choice.  MIRT_ERR_ARG for out-of-range values (no reference
+ * counterpart: tuning of this implementation). */
+int mirt_interp_plan_set_spread(mirt_interp_plan *plan, const int32_t *T, int32_t threads,
+                                int32_t padc, void *stream);
 
 int mirt_interp_plan_destroy(mirt_interp_plan *plan);
 

@@ -199,6 +199,8 @@ void choose_config(mirt_interp_plan *P) {
   ls.cw = cw;
   ls.sb = 0;
   ls.grid = 0;
+  // no spare tile columns by default; the autotuner also tries J1 - 1
+  t.padc = 0;
   t.nbins = 1;
   t.ntiles = 1;
   for (int d = 0; d < MIRT_DMAX; d++) {
@@ -498,8 +500,16 @@ int set_spread_tiles(mirt_interp_plan *P, const int *T, cudaStream_t st) {
 
 struct SpreadCand {
   int T[MIRT_DMAX];
-  int threads, sb;
+  int threads, padc;
 };
+
+// spare columns the J = 6 row update can use (0 elsewhere)
+int padc_max(const InterpArgs &a) {
+  if (a.g.D < 2) return 0;
+  for (int d = 0; d < a.g.D; d++)
+    if (a.g.J[d] != 6) return 0;
+  return 5;
+}
 
 // Time `fn` (one launch) on the stream: one warm-up, then the best of 3.
 template <class F>
@@ -643,16 +653,21 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
   CK(cudaMemsetAsync(grid.p, 0, ngrid * sizeof(float2), st));
   // spread candidates: tile shape (multiples of the 8-point bins), warps
   std::vector<SpreadCand> cands;
+  const int pmax = padc_max(a);
   auto add = [&](int t0, int t1, int t2, int threads) {
-    SpreadCand c{{t0, t1, t2}, threads, 0};
-    for (int d = 0; d < D; d++) {
-      const int kr = (a.g.K[d] + P->t.B[d] - 1) / P->t.B[d] * P->t.B[d];
-      if (c.T[d] > kr) c.T[d] = kr;
-      c.T[d] = (c.T[d] + P->t.B[d] - 1) / P->t.B[d] * P->t.B[d];
+    const int npc = pmax ? 2 : 1;
+    for (int ip = 0; ip < npc; ip++) {
+      const int pc = ip ? pmax : 0;
+      SpreadCand c{{t0, t1, t2}, threads, pc};
+      for (int d = 0; d < D; d++) {
+        const int kr = (a.g.K[d] + P->t.B[d] - 1) / P->t.B[d] * P->t.B[d];
+        if (c.T[d] > kr) c.T[d] = kr;
+        c.T[d] = (c.T[d] + P->t.B[d] - 1) / P->t.B[d] * P->t.B[d];
+      }
+      size_t npts = (size_t)c.T[0] + 2 * pc;
+      for (int d = 1; d < D; d++) npts *= c.T[d];
+      if (npts * cw * 8 <= 160 * 1024) cands.push_back(c);
     }
-    size_t npts = 1;
-    for (int d = 0; d < D; d++) npts *= c.T[d];
-    if (npts * cw * 8 <= 160 * 1024) cands.push_back(c);
   };
   if (D == 1) {
     for (int t0 : {64, 128, 256, 512})
@@ -678,6 +693,7 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
     int rc = set_spread_tiles(P, c.T, st);
     if (rc) continue;
     P->ls.threads = c.threads;
+    P->t.padc = c.padc;
     float ms = 0;
     rc = time_launch([&]() {
       return launch_spread(P->a, P->t, P->ls, P->bin_start.as<int>(), samp.as<float2>(),
@@ -693,6 +709,7 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
     int rc = set_spread_tiles(P, best.T, st);
     if (rc) return rc;
     P->ls.threads = best.threads;
+    P->t.padc = best.padc;
   }
   // split size of heavy tiles (sample visits per spread task)
   {
@@ -756,10 +773,39 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
 
 int mirt_interp_plan_config(mirt_interp_plan *P, int32_t *out, int32_t n) {
   if (!P || !out) return fail(MIRT_ERR_ARG, "NULL argument");
-  const int32_t v[14] = {P->t.T[0], P->t.T[1], P->t.T[2], P->ls.threads, P->heavy_first, P->ls.cw,
+  const int32_t v[15] = {P->t.T[0], P->t.T[1], P->t.T[2], P->ls.threads, P->heavy_first, P->ls.cw,
                          P->lg.threads, P->lg.sb, P->lg.grid, P->t.B[0], P->t.B[1], P->t.B[2],
-                         P->split_chunk, P->t.ntask};
-  for (int i = 0; i < n && i < 14; i++) out[i] = v[i];
+                         P->split_chunk, P->t.ntask, P->t.padc};
+  for (int i = 0; i < n && i < 15; i++) out[i] = v[i];
+  return MIRT_OK;
+}
+
+int mirt_interp_plan_set_spread(mirt_interp_plan *P, const int32_t *T, int32_t threads,
+                                int32_t padc, void *stream) {
+  if (!P || !T) return fail(MIRT_ERR_ARG, "NULL argument");
+  const int D = P->a.g.D;
+  if (threads < 32 || threads > 1024 || threads % 32)
+    return fail(MIRT_ERR_ARG, "spread threads must be a multiple of 32 in [32, 1024]");
+  if (padc != 0 && padc != padc_max(P->a))
+    return fail(MIRT_ERR_ARG, "padc must be 0 or J1 - 1 (J = 6 kernels in 2D/3D)");
+  int Tn[MIRT_DMAX] = {1, 1, 1};
+  size_t npts = 1;
+  for (int d = 0; d < D; d++) {
+    const int B = P->t.B[d];
+    const int kr = (P->a.g.K[d] + B - 1) / B * B;
+    if (T[d] < B || T[d] % B || T[d] > kr)
+      return fail(MIRT_ERR_ARG, "tile extents must be multiples of the sort bin, at most the "
+                                "grid extent rounded up to a bin");
+    Tn[d] = T[d];
+    npts *= (size_t)(d == 0 ? T[0] + 2 * padc : T[d]);
+  }
+  if (npts * P->ls.cw * 8 > 200 * 1024) return fail(MIRT_ERR_ARG, "tile exceeds shared memory");
+  cudaStream_t st = as_stream(stream);
+  P->t.padc = padc;
+  P->ls.threads = threads;
+  int rc = set_spread_tiles(P, Tn, st);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(st));
   return MIRT_OK;
 }
 

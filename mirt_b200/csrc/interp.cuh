@@ -44,6 +44,10 @@ struct Tiling {
   int nbin[MIRT_DMAX];   // bins per dimension
   int nbins;             // prod(nbin): bins per slice
   int T[MIRT_DMAX];      // spread tile extent per dimension (multiple of B)
+  int padc;              // spread: spare columns on each side of a tile row in
+                         // shared memory (0, or J1 - 1 so that every column
+                         // tap of a visiting sample has a slot and the row
+                         // update needs no bounds tests; never written out)
   int nb[MIRT_DMAX];     // tiles per dimension
   int ntiles;            // prod(nb): tiles per slice
   int nslice;

@@ -359,6 +359,11 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t,
   int npts = 1;
 #pragma unroll
   for (int d = 0; d < D; d++) npts *= t.T[d];
+  // shared tile: rows of RS = T0 + 2 pc points, point (l1, l2, l3) at
+  // ((l3 T1 + l2) RS + pc + l1) CW + coil
+  const int pc = D > 1 ? t.padc : 0;
+  const int RS = t.T[0] + 2 * pc;
+  const int nsm = npts / t.T[0] * RS;
   float2 *acc = reinterpret_cast<float2 *>(smem);
   int Jd[MIRT_DMAX] = {1, 1, 1};
 #pragma unroll
@@ -390,7 +395,7 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t,
   const int per = (t.T[BD] + nwarp - 1) / nwarp;
   const int band_lo = min(warp * per, ext[BD]);
   const int band_hi = min(band_lo + per, ext[BD]);
-  for (int e = threadIdx.x; e < npts * CW; e += blockDim.x) acc[e] = make_float2(0.f, 0.f);
+  for (int e = threadIdx.x; e < nsm * CW; e += blockDim.x) acc[e] = make_float2(0.f, 0.f);
   __syncthreads();
 
   int ns[MIRT_DMAX] = {1, 1, 1};
@@ -460,9 +465,29 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t,
           }
           // lane's first column tap (class ls of SUB), then every SUB-th
           const int j1s = ja1 + ((ls - l10 - ja1) & (SUB - 1));
+          const bool padded = pc >= JT - 1;
+          const int j1p = (ls - l10) & (SUB - 1);
           auto row = [&](float2 *p, float2 v2) {
             const float2 v2s = make_float2(v2.y, v2.x);
-            if constexpr (SUB == 1) {
+            if (padded) {
+              // every column tap has a slot (spare columns take the ones
+              // outside the tile): no bounds tests
+              if constexpr (SUB == 1) {
+#pragma unroll
+                for (int j1 = 0; j1 < JT; j1++) {
+                  float2 A = p[j1 * CW];
+                  A = __ffma2_rn(wr[j1], v2, A);
+                  if (!REAL) A = __ffma2_rn(wi[j1], v2s, A);
+                  p[j1 * CW] = A;
+                }
+              } else {
+                for (int j1 = j1p; j1 < JT; j1 += SUB) {
+                  float2 A = p[j1 * CW];
+                  A = cw_fma<REAL>(__ldg(Ws + j1), v2, v2s, A);
+                  p[j1 * CW] = A;
+                }
+              }
+            } else if constexpr (SUB == 1) {
 #pragma unroll
               for (int j1 = 0; j1 < JT; j1++) {
                 if (j1 >= ja1 && j1 < jb1) {
@@ -480,19 +505,19 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t,
               }
             }
           };
-          float2 *base = acc + l10 * CW + lc;
+          float2 *base = acc + (pc + l10) * CW + lc;
           if constexpr (D == 2) {
             for (int j2 = jab; j2 < jbb; j2++) {
               const float2 v2 = cw_mul<REAL>(__ldg(Ws + JT + j2), f);
-              row(base + (size_t)(lb + j2) * T0 * CW, v2);
+              row(base + (size_t)(lb + j2) * RS * CW, v2);
             }
           } else {
             for (int j3 = jab; j3 < jbb; j3++) {
               const float2 v3 = cw_mul<REAL>(__ldg(Ws + 2 * JT + j3), f);
-              float2 *pl = base + (size_t)(lb + j3) * T1 * T0 * CW;
+              float2 *pl = base + (size_t)(lb + j3) * T1 * RS * CW;
               for (int j2 = ja2; j2 < jb2; j2++) {
                 const float2 v2 = cw_mul<REAL>(__ldg(Ws + JT + j2), v3);
-                row(pl + (size_t)(l20 + j2) * T0 * CW, v2);
+                row(pl + (size_t)(l20 + j2) * RS * CW, v2);
               }
             }
           }
@@ -527,7 +552,7 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t,
                 wr[j1] = make_float2(w.x, w.x);
                 wi[j1] = make_float2(w.y, -w.y);
               }
-              float2 *base = acc + l10 * CW + lc;
+              float2 *base = acc + (pc + l10) * CW + lc;
               unsigned m2 = mb;
               while (m2) {
                 const int j2 = __ffs(m2) - 1;
@@ -535,7 +560,7 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t,
                 const int l2 = tap_local(k.y, j2, g.K[1], lo[1]);
                 const float2 v2 = cw_mul<REAL>(__ldg(Ws + JT + j2), f);
                 const float2 v2s = make_float2(v2.y, v2.x);
-                float2 *p = base + (size_t)l2 * T0 * CW;
+                float2 *p = base + (size_t)l2 * RS * CW;
 #pragma unroll
                 for (int j1 = 0; j1 < JT; j1++) {
                   float2 A = p[j1 * CW];
@@ -553,8 +578,8 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t,
             m2 &= m2 - 1;
             const int l2 = tap_local(k.y, j2, g.K[1], lo[1]);
             const float2 v2 = cw_mul<REAL>(__ldg(Ws + Jd[0] + j2), f);
-            spread_row<CW, JT, REAL>(acc + (size_t)l2 * T0 * CW + lc, Ws, Jd[0], fast1, l10, m1,
-                                     k.x, g.K[0], lo[0], ls, v2);
+            spread_row<CW, JT, REAL>(acc + ((size_t)l2 * RS + pc) * CW + lc, Ws, Jd[0], fast1, l10,
+                                     m1, k.x, g.K[0], lo[0], ls, v2);
           }
         } else {
           const unsigned m2all = tap_mask<1>(k.y, Jd[1], g.K[1], lo[1], 0, ext[1], 0);
@@ -571,8 +596,8 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t,
               m2 &= m2 - 1;
               const int l2 = tap_local(k.y, j2, g.K[1], lo[1]);
               const float2 v2 = cw_mul<REAL>(__ldg(Ws + Jd[0] + j2), v3);
-              spread_row<CW, JT, REAL>(acc + ((size_t)l3 * T1 + l2) * T0 * CW + lc, Ws, Jd[0],
-                                       fast1, l10, m1, k.x, g.K[0], lo[0], ls, v2);
+              spread_row<CW, JT, REAL>(acc + (((size_t)l3 * T1 + l2) * RS + pc) * CW + lc, Ws,
+                                       Jd[0], fast1, l10, m1, k.x, g.K[0], lo[0], ls, v2);
             }
           }
         }
@@ -583,7 +608,11 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t,
   if (slot >= 0) {
     // partial tile of a split heavy tile: summed later in fixed order
     float2 *part = t.scratch + ((size_t)slot * gridDim.y + blockIdx.y) * npts * CW;
-    for (int e = threadIdx.x; e < npts * CW; e += blockDim.x) part[e] = acc[e];
+    for (int e = threadIdx.x; e < npts * CW; e += blockDim.x) {
+      const int pt = e / CW, cc = e - pt * CW;
+      const int l1 = pt % T0, r = pt / T0;
+      part[e] = acc[(r * RS + pc + l1) * CW + cc];
+    }
     return;
   }
   float2 *gout = ck + (long long)slice * a.grid_elems;
@@ -596,7 +625,7 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t,
     long long kk = lo[0] + l1;
     if (D > 1) kk += (long long)(lo[1] + l2) * g.kstride[1];
     if (D > 2) kk += (long long)(lo[2] + l3) * g.kstride[2];
-    gout[kk * C + c0 + cc] = acc[e];
+    gout[kk * C + c0 + cc] = acc[((pt / T0) * RS + pc + l1) * CW + cc];
   }
 }
 
@@ -664,8 +693,8 @@ struct Req {
 };
 
 inline size_t spread_smem_bytes(const InterpArgs &a, const Tiling &t, const Launch &l) {
-  size_t npts = 1;
-  for (int d = 0; d < a.g.D; d++) npts *= t.T[d];
+  size_t npts = a.g.D > 1 ? t.T[0] + 2 * t.padc : t.T[0];
+  for (int d = 1; d < a.g.D; d++) npts *= t.T[d];
   return npts * l.cw * 8;
 }
 

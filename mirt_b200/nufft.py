@@ -66,12 +66,12 @@ def minmax_kb_scale(N: int, J: int, K: int) -> np.ndarray:
 
 
 def _plan_config(lib, handle) -> dict:
-    v = (C.c_int32 * 14)()
-    check(lib.mirt_interp_plan_config(handle, v, 14))
+    v = (C.c_int32 * 15)()
+    check(lib.mirt_interp_plan_config(handle, v, 15))
     return {"spread_tile": [v[0], v[1], v[2]], "spread_threads": v[3], "spread_heavy_first": v[4],
             "coil_lanes": v[5], "gather_threads": v[6],
             "gather_ctas": v[8], "sort_bin": [v[9], v[10], v[11]], "split_chunk": v[12],
-            "spread_tasks": v[13]}
+            "spread_tasks": v[13], "spread_padc": v[14]}
 
 
 class InterpPlan:
@@ -150,6 +150,15 @@ class InterpPlan:
 
     def config(self):
         return _plan_config(self.lib, self.handle)
+
+    def set_spread(self, tile, threads=32, padc=0, stream=None):
+        """Fix the spread tiling (tile extents per dimension, CTA size, spare
+        tile columns 0 or J1 - 1) instead of autotuning it."""
+        T = _i32(list(tile) + [1] * (3 - len(tile)))
+        check(self.lib.mirt_interp_plan_set_spread(
+            self.handle, T.ctypes.data_as(C.POINTER(C.c_int32)), int(threads), int(padc),
+            _stream_ptr(stream)))
+        return self.config()
 
     def close(self):
         if getattr(self, "handle", None):

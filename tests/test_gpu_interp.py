@@ -213,3 +213,47 @@ def test_autotuned_plan_keeps_parity(C):
         ref = oracle.interp_for(cks, h, J, L, tm[sl], K, 0, impl=ref_impl())
         assert rel_l2(out[sl], ref) <= FWD_TOL
     plan.close()
+
+
+@pytest.mark.parametrize("C", [1, 4, 8, 32])
+def test_spread_tilings_padded_and_plain(C):
+    """Every fixed tiling -- tile shape, warps per tile, spare tile columns
+    (bounds-free row update) or none -- gives the oracle's adjoint."""
+    import torch
+    rng = np.random.default_rng(77 + C)
+    K, J, L = [96, 80], [6, 6], [1024, 1024]
+    h = [mb.minmax_kb_table(48, 6, 96, 1024), mb.minmax_kb_table(40, 6, 80, 1024)]
+    tm = rng.uniform(-100, 100, (2500, 2))
+    tm[:40] = np.round(tm[:40])
+    plan = mb.InterpPlan(K, J, L, h, tm, C)
+    fm = rng.standard_normal((len(tm), C)) + 1j * rng.standard_normal((len(tm), C))
+    fm_d = torch.from_numpy(fm.astype(np.complex64)).cuda()
+    ref = oracle.interp_adj(fm, h, J, L, tm, K, 0, impl=ref_impl())
+    for tile, threads in [((8, 8), 32), ((16, 16), 64), ((32, 8), 32), ((8, 32), 128)]:
+        for padc in (0, 5):
+            cfg = plan.set_spread(tile, threads, padc)
+            assert cfg["spread_padc"] == padc and cfg["spread_tile"][:2] == list(tile)
+            got = plan.adjoint(fm_d).cpu().numpy()[0]
+            got = np.transpose(got, (1, 0, 2)).reshape(-1, C, order="F")
+            assert rel_l2(got, ref) <= ADJ_TOL, (tile, threads, padc)
+    plan.close()
+
+
+def test_spread_tilings_3d_padded():
+    import torch
+    rng = np.random.default_rng(78)
+    K, J, L = [24, 20, 16], [6, 6, 6], [256, 256, 256]
+    h = [mb.minmax_kb_table(k // 2, 6, k, 256) for k in K]
+    tm = rng.uniform(-40, 40, (1500, 3))
+    C = 8
+    plan = mb.InterpPlan(K, J, L, h, tm, C)
+    fm = rng.standard_normal((len(tm), C)) + 1j * rng.standard_normal((len(tm), C))
+    fm_d = torch.from_numpy(fm.astype(np.complex64)).cuda()
+    ref = oracle.interp_adj(fm, h, J, L, tm, K, 0, impl=ref_impl())
+    for tile, threads in [((8, 8, 8), 32), ((16, 8, 8), 64)]:
+        for padc in (0, 5):
+            plan.set_spread(tile, threads, padc)
+            got = plan.adjoint(fm_d).cpu().numpy()[0]
+            got = np.transpose(got, (2, 1, 0, 3)).reshape(-1, C, order="F")
+            assert rel_l2(got, ref) <= ADJ_TOL, (tile, threads, padc)
+    plan.close()
