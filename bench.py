@@ -326,10 +326,12 @@ def run_gpu(args, w):
     time.sleep(0.3)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.nvtx.range_push("timed_steps")
     e0.record(stream)
     for _ in range(args.steps):
         step()
     e1.record(stream)
+    torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     clk = clocks.stop()
     t_local = e0.elapsed_time(e1) / 1000.0
@@ -351,23 +353,25 @@ def run_gpu(args, w):
     sptr = Cc.c_void_p(stream.cuda_stream)
     reps = 5
 
-    def timed(fn):
+    def timed(fn, name):
         fn()
         torch.cuda.synchronize()
         a = torch.cuda.Event(enable_timing=True)
         b = torch.cuda.Event(enable_timing=True)
+        torch.cuda.nvtx.range_push(name)
         a.record(stream)
         for _ in range(reps):
             fn()
         b.record(stream)
+        torch.cuda.nvtx.range_pop()
         torch.cuda.synchronize()
         return a.elapsed_time(b) / 1000.0 / reps
 
     from mirt_b200._lib import check
     t_gather = timed(lambda: check(plan.lib.mirt_interp_plan_forward(
-        ip, Cc.c_void_p(grid.data_ptr()), Cc.c_void_p(X.data_ptr()), sptr)))
+        ip, Cc.c_void_p(grid.data_ptr()), Cc.c_void_p(X.data_ptr()), sptr)), "roofline_gather")
     t_spread = timed(lambda: check(plan.lib.mirt_interp_plan_adjoint(
-        ip, Cc.c_void_p(X.data_ptr()), Cc.c_void_p(grid.data_ptr()), sptr)))
+        ip, Cc.c_void_p(X.data_ptr()), Cc.c_void_p(grid.data_ptr()), sptr)), "roofline_spread")
     nk = w["K"] ** D
     B = 8.0 * C * nk * plan.nslice + 8.0 * C * Mtot + 4.0 * D * Mtot
     peak, peak_kind = measured_peak()

@@ -163,6 +163,14 @@ namespace {
 // Launch shapes and tiling.  Samples are binned on 4-point bins (64 in 1D);
 // the spread runs one warp per tile (lanes = coils; the tile accumulator is
 // sized to keep several CTAs resident per SM).
+// The spread's range path serves wrapping taps when no tile can meet a
+// sample's taps both before and after their periodic wrap.
+int wrap_ok(const InterpArgs &a, const Tiling &t) {
+  for (int d = 0; d < a.g.D; d++)
+    if (a.g.K[d] < t.T[d] + a.g.J[d]) return 0;
+  return 1;
+}
+
 void choose_config(mirt_interp_plan *P) {
   InterpArgs &a = P->a;
   Tiling &t = P->t;
@@ -211,6 +219,7 @@ void choose_config(mirt_interp_plan *P) {
     t.nbins *= t.nbin[d];
     t.ntiles *= t.nb[d];
   }
+  t.wrap_ok = wrap_ok(a, t);
 }
 
 // Source bins per dimension: bins whose samples (binned by the first tap
@@ -493,6 +502,7 @@ int set_spread_tiles(mirt_interp_plan *P, const int *T, cudaStream_t st) {
     t.nb[d] = d < D ? (P->a.g.K[d] + t.T[d] - 1) / t.T[d] : 1;
     t.ntiles *= t.nb[d];
   }
+  t.wrap_ok = wrap_ok(P->a, t);
   int rc = build_sources(P, st);
   if (rc) return rc;
   return build_tasks(P, st);
@@ -673,19 +683,16 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
     for (int t0 : {64, 128, 256, 512})
       for (int th : {32, 64}) add(t0, 1, 1, th);
   } else if (D == 2) {
+    // warps per tile: each owns a band of at least 2 rows
     for (int t0 : {8, 16, 32})
-      for (int t1 : {8, 16, 32}) {
-        add(t0, t1, 1, 32);
-        if (t1 >= 16) add(t0, t1, 1, 64);
-        if (t1 >= 32) add(t0, t1, 1, 128);
-      }
+      for (int t1 : {8, 16, 32})
+        for (int th = 32; th <= 128 && th / 32 <= t1 / 2; th *= 2) add(t0, t1, 1, th);
   } else {
+    // each warp owns a band of at least 2 planes
     for (int t0 : {8, 16})
       for (int t1 : {8, 16})
-        for (int t2 : {8, 16}) {
-          add(t0, t1, t2, 32);
-          if (t2 >= 16) add(t0, t1, t2, 64);
-        }
+        for (int t2 : {8, 16})
+          for (int th = 32; th <= 128 && th / 32 <= t2 / 2; th *= 2) add(t0, t1, t2, th);
   }
   SpreadCand best{};
   float best_ms = 1e30f;

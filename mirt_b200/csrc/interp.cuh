@@ -44,6 +44,8 @@ struct Tiling {
   int nbin[MIRT_DMAX];   // bins per dimension
   int nbins;             // prod(nbin): bins per slice
   int T[MIRT_DMAX];      // spread tile extent per dimension (multiple of B)
+  int wrap_ok;           // K[d] >= T[d] + J[d] in every dimension: the spread's
+                         // range path also serves samples whose taps wrap
   int padc;              // spread: spare columns on each side of a tile row in
                          // shared memory (0, or J1 - 1 so that every column
                          // tap of a visiting sample has a slot and the row

@@ -439,14 +439,22 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t,
       const int l10 = k.x - lo[0];
       const float2 *Ws = a.W + pos * SJ;
       if constexpr (JT > 0 && D >= 2) {
-        // patch without periodic wrap: the in-tile taps of each dimension are
-        // one index range, walked with unrolled predicated loops.  A visit
-        // whose ranges are empty ends before any coefficient is loaded.
-        if (k.x + JT <= g.K[0] && k.y + JT <= g.K[1] && (D == 2 || k.z + JT <= g.K[2])) {
-          const int ja1 = max(0, -l10), jb1 = min(JT, ext[0] - l10);
-          const int lb = kb - lo[BD];
+        // The in-tile taps of each dimension are one index range, walked with
+        // unrolled loops.  With K >= T + J per dimension a tile meets a
+        // sample's taps either before or after their periodic wrap, never
+        // both, so the tile-local first tap is k0 - lo, or k0 - lo - K when
+        // the taps reach the tile only after the wrap.  A visit whose ranges
+        // are empty ends before any coefficient is loaded.
+        if (t.wrap_ok) {
+          auto rel = [&](int k0, int d) {
+            const int l = k0 - lo[d];
+            return l >= ext[d] ? l - g.K[d] : l;
+          };
+          const int f10 = rel(k.x, 0);
+          const int ja1 = max(0, -f10), jb1 = min(JT, ext[0] - f10);
+          const int lb = rel(kb, BD);
           const int jab = max(0, band_lo - lb), jbb = min(JT, band_hi - lb);
-          const int l20 = k.y - lo[1];
+          const int l20 = rel(k.y, 1);
           const int ja2 = D == 3 ? max(0, -l20) : 0, jb2 = D == 3 ? min(JT, ext[1] - l20) : 1;
           if (ja1 >= jb1 || jab >= jbb || ja2 >= jb2) continue;
           float2 f = make_float2(0.f, 0.f);
@@ -464,9 +472,9 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t,
             }
           }
           // lane's first column tap (class ls of SUB), then every SUB-th
-          const int j1s = ja1 + ((ls - l10 - ja1) & (SUB - 1));
+          const int j1s = ja1 + ((ls - f10 - ja1) & (SUB - 1));
           const bool padded = pc >= JT - 1;
-          const int j1p = (ls - l10) & (SUB - 1);
+          const int j1p = (ls - f10) & (SUB - 1);
           auto row = [&](float2 *p, float2 v2) {
             const float2 v2s = make_float2(v2.y, v2.x);
             if (padded) {
@@ -505,7 +513,7 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t,
               }
             }
           };
-          float2 *base = acc + (pc + l10) * CW + lc;
+          float2 *base = acc + (pc + f10) * CW + lc;
           if constexpr (D == 2) {
             for (int j2 = jab; j2 < jbb; j2++) {
               const float2 v2 = cw_mul<REAL>(__ldg(Ws + JT + j2), f);
