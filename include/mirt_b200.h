@@ -185,10 +185,10 @@ int mirt_interp_plan_forward(mirt_interp_plan *plan, const void *ck, void *fm, v
 /* ck = interp_adj(fm) on device buffers; overwrites all of ck. */
 int mirt_interp_plan_adjoint(mirt_interp_plan *plan, const void *fm, void *ck, void *stream);
 
-/* Autotune: time candidate spread tile shapes (multiples of the 8-point sort
- * bins), warps per spread CTA, staged batch sizes and the split size of dense
- * tiles, and gather CTA / batch sizes, on this plan's trajectory; keep the
- * fastest.  Allocates a scratch
+/* Autotune: time candidate spread tile shapes (multiples of the sort bins),
+ * warps per spread CTA (each owning a band of rows / planes), spare tile
+ * columns, the split size of dense tiles and the task order, and the gather
+ * CTA size, on this plan's trajectory; keep the fastest.  Allocates a scratch
  * grid and sample buffer for the duration of the call.  Results stay
  * bitwise deterministic for any choice. */
 int mirt_interp_plan_autotune(mirt_interp_plan *plan, void *stream);

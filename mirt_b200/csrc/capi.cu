@@ -683,16 +683,16 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
     for (int t0 : {64, 128, 256, 512})
       for (int th : {32, 64}) add(t0, 1, 1, th);
   } else if (D == 2) {
-    // warps per tile: each owns a band of at least 2 rows
+    // warps per tile: each owns a band of at least one row
     for (int t0 : {8, 16, 32})
       for (int t1 : {8, 16, 32})
-        for (int th = 32; th <= 128 && th / 32 <= t1 / 2; th *= 2) add(t0, t1, 1, th);
+        for (int th = 32; th <= 256 && th / 32 <= t1; th *= 2) add(t0, t1, 1, th);
   } else {
-    // each warp owns a band of at least 2 planes
+    // each warp owns a band of at least one plane
     for (int t0 : {8, 16})
       for (int t1 : {8, 16})
         for (int t2 : {8, 16})
-          for (int th = 32; th <= 128 && th / 32 <= t2 / 2; th *= 2) add(t0, t1, t2, th);
+          for (int th = 32; th <= 256 && th / 32 <= t2; th *= 2) add(t0, t1, t2, th);
   }
   SpreadCand best{};
   float best_ms = 1e30f;
