@@ -246,6 +246,30 @@ int mirt_nufft_autotune(mirt_nufft *p, void *stream);
 int mirt_nufft_destroy(mirt_nufft *p);
 
 /* ------------------------------------------------------------------------
+ * 3b. density compensation on a single-column NUFFT plan (ncol = 1)
+ *
+ * mirt_dcf_pipe replaces ir_mri_dcf_pipe_do (mri/ir_mri_density_comp.m:
+ * 203-281): from w = 1 (init_ones = 1) or the caller's w, repeat
+ * goal = real(P P' w), w = w ./ goal (P = the plan's table interpolator with
+ * its phase shift) until max |goal - 1| <= thresh, with at most niter + 1
+ * updates as in the reference loop; then scale so that sum(real(G' w)) =
+ * prod(N ./ fov) per slice (fov: D values, NULL for 1).  Every slice of a
+ * batched plan is its own problem and stops on its own residual.  A
+ * non-positive goal fails with "pipe bug", as the reference does.  The
+ * reference's `unitv` and `isave` options are not provided.
+ *   w       device FP64 [Mtot], sample order of the plan (in / out)
+ *   iters   host int32 [nslice] or NULL: updates done per slice
+ *   resid   host FP64 [nslice] or NULL: last max |goal - 1| per slice
+ * Interpolation in FP32; weights, ratio update, residual and scale in FP64.
+ * Returns after the result is in w.
+ *
+ * mirt_dcf_jackson replaces ir_mri_dcf_jackson (:160-180) for table plans:
+ * w = 1 ./ real(P (P' 1)). */
+int mirt_dcf_pipe(mirt_nufft *p, double *w, int32_t init_ones, int32_t niter, double thresh,
+	const double *fov, int32_t *iters, double *resid, void *stream);
+int mirt_dcf_jackson(mirt_nufft *p, double *w, void *stream);
+
+/* ------------------------------------------------------------------------
  * 4. forward gather for callers that cannot allocate device memory (no
  *    counterpart in the reference, whose mex files run on the host)
  *

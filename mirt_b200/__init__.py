@@ -4,6 +4,7 @@ interfaces.
 
 * ``mirt_b200.mex``: the six mex gateways (interp{1,2,3}_table[_adj]_mex)
 * ``mirt_b200.nufft``: device plans, nufft_init / nufft / nufft_adj
+* ``mirt_b200.dcf``: density compensation (ir_mri_density_comp 'pipe', 'jackson')
 * ``include/mirt_b200.h``: the C ABI of libmirt_b200.so underneath both
 
 All compute runs in libmirt_b200.so; importing the package does not load it,
@@ -14,6 +15,7 @@ from .mex import (MexError, interp1_table_adj_mex, interp1_table_mex, interp2_ta
                   interp2_table_mex, interp3_table_adj_mex, interp3_table_mex)
 from .nufft import (InterpPlan, NufftPlan, minmax_kb_scale, minmax_kb_table, nufft, nufft_adj,
                     nufft_init)
+from .dcf import dcf_jackson, dcf_pipe, ir_mri_density_comp
 
 __all__ = [
     "MirtError", "MexError", "load",
@@ -21,4 +23,5 @@ __all__ = [
     "interp1_table_adj_mex", "interp2_table_adj_mex", "interp3_table_adj_mex",
     "InterpPlan", "NufftPlan", "minmax_kb_table", "minmax_kb_scale",
     "nufft_init", "nufft", "nufft_adj",
+    "dcf_pipe", "dcf_jackson", "ir_mri_density_comp",
 ]

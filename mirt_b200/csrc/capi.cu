@@ -21,6 +21,7 @@
 
 #include "glue.cuh"
 #include "interp.cuh"
+#include "runtime.cuh"
 
 namespace mirt {
 bool minmax_kb_table(int N, int J, int K, int L, std::vector<std::complex<double>> &h);
@@ -48,12 +49,30 @@ int fail(int code, const std::string &msg) {
                   std::string(#call) + ": " + cudaGetErrorString(e_));                \
   } while (0)
 
+int device_ok() {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    return fail(MIRT_ERR_CUDA, "no CUDA device available");
+  }
+  return MIRT_OK;
+}
+
+}  // namespace
+
+namespace mirt {
+// Record an error for mirt_last_error() from another translation unit.
+int api_fail(int code, const std::string &msg) { return fail(code, msg); }
+
 // ---------------------------------------------------------------------------
 // caching device allocator: blocks are rounded up to a power of two and kept
 // for reuse, so repeated mex calls do not pay cudaMalloc / cudaFree.
 // ---------------------------------------------------------------------------
+namespace {
 std::mutex g_cache_mu;
 std::multimap<std::pair<int, size_t>, void *> g_free;
+}  // namespace
 
 size_t round_block(size_t b) {
   size_t r = 256;
@@ -96,67 +115,8 @@ void dfree(void *p, size_t bytes) {
   g_free.insert({{dev, round_block(bytes)}, p});
 }
 
-struct DMem {
-  void *p = nullptr;
-  size_t bytes = 0;
-  DMem() = default;
-  DMem(const DMem &) = delete;
-  DMem &operator=(const DMem &) = delete;
-  ~DMem() { release(); }
-  void release() {
-    dfree(p, bytes);
-    p = nullptr;
-    bytes = 0;
-  }
-  cudaError_t alloc(size_t b) {
-    release();
-    bytes = b;
-    return dalloc(&p, b);
-  }
-  template <class T>
-  T *as() const {
-    return static_cast<T *>(p);
-  }
-};
-
-void swap_mem(DMem &x, DMem &y) {
-  std::swap(x.p, y.p);
-  std::swap(x.bytes, y.bytes);
-}
-
-cudaStream_t as_stream(void *s) { return static_cast<cudaStream_t>(s); }
-
-int device_ok() {
-  int n = 0;
-  cudaError_t e = cudaGetDeviceCount(&n);
-  if (e != cudaSuccess || n == 0) {
-    cudaGetLastError();
-    return fail(MIRT_ERR_CUDA, "no CUDA device available");
-  }
-  return MIRT_OK;
-}
-
-}  // namespace
-
-namespace mirt {
-// Record an error for mirt_last_error() from another translation unit.
-int api_fail(int code, const std::string &msg) { return fail(code, msg); }
 }  // namespace mirt
 
-// ---------------------------------------------------------------------------
-// interpolation plan
-// ---------------------------------------------------------------------------
-struct mirt_interp_plan {
-  InterpArgs a{};
-  Tiling t{};
-  Launch lg{}, ls{};
-  DMem tm, slice, perm, bin_start, tab[MIRT_DMAX], phase, src[MIRT_DMAX], nsrc[MIRT_DMAX];
-  DMem keys, sorttmp, moff;
-  DMem task_tile, task_range, task_slot, red, scratch, wtap, k0tap;
-  int split_chunk = 1024;  // sample visits per spread task before a tile is split
-  int heavy_first = 1;     // spread task order: 1 heaviest first, 0 grid order
-  std::vector<long long> moff_host;
-};
 
 namespace {
 
@@ -1209,19 +1169,6 @@ int mirt_interp3_table_adj_mex(const double *fm_re, const double *fm_im, int64_t
 // ---------------------------------------------------------------------------
 // NUFFT
 // ---------------------------------------------------------------------------
-struct mirt_nufft {
-  mirt_interp_plan *ip = nullptr;
-  GlueGeom gg{};
-  int C = 0, nslice = 0;
-  long long Mtot = 0;
-  DMem sn, grid, grid_cm, hx, hX;  // grid: coil innermost (interp); grid_cm: coil-major (FFT)
-  cufftHandle fft = 0;
-  bool fft_ok = false;
-  ~mirt_nufft() {
-    if (fft_ok) cufftDestroy(fft);
-    delete ip;
-  }
-};
 
 namespace {
 

@@ -1,0 +1,84 @@
+// runtime.cuh -- host-side state shared by the translation units of the C ABI:
+// the caching device allocator, device buffers, and the interpolation and
+// NUFFT plan objects behind the opaque handles of include/mirt_b200.h.
+#pragma once
+
+#include <cufft.h>
+
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "glue.cuh"
+#include "interp.cuh"
+
+namespace mirt {
+
+// Record an error for mirt_last_error(); returns `code`.
+int api_fail(int code, const std::string &msg);
+
+// Caching device allocator: blocks are rounded up to a power of two and kept
+// for reuse, so repeated calls do not pay cudaMalloc / cudaFree.
+cudaError_t dalloc(void **p, size_t bytes);
+void dfree(void *p, size_t bytes);
+
+struct DMem {
+  void *p = nullptr;
+  size_t bytes = 0;
+  DMem() = default;
+  DMem(const DMem &) = delete;
+  DMem &operator=(const DMem &) = delete;
+  ~DMem() { release(); }
+  void release() {
+    dfree(p, bytes);
+    p = nullptr;
+    bytes = 0;
+  }
+  cudaError_t alloc(size_t b) {
+    release();
+    bytes = b;
+    return dalloc(&p, b);
+  }
+  template <class T>
+  T *as() const {
+    return static_cast<T *>(p);
+  }
+};
+
+inline void swap_mem(DMem &x, DMem &y) {
+  std::swap(x.p, y.p);
+  std::swap(x.bytes, y.bytes);
+}
+
+inline cudaStream_t as_stream(void *s) { return static_cast<cudaStream_t>(s); }
+
+}  // namespace mirt
+
+// Interpolation plan: geometry, tables, sorted trajectory, tap records, spread
+// tiling and work list, launch shapes.
+struct mirt_interp_plan {
+  mirt::InterpArgs a{};
+  mirt::Tiling t{};
+  mirt::Launch lg{}, ls{};
+  mirt::DMem tm, slice, perm, bin_start, tab[MIRT_DMAX], phase, src[MIRT_DMAX], nsrc[MIRT_DMAX];
+  mirt::DMem keys, sorttmp, moff;
+  mirt::DMem task_tile, task_range, task_slot, red, scratch, wtap, k0tap;
+  int split_chunk = 1024;  // sample visits per spread task before a tile is split
+  int heavy_first = 1;     // spread task order: 1 heaviest first, 0 grid order
+  std::vector<long long> moff_host;
+};
+
+// NUFFT plan: an interpolation plan plus scaling factors, grids and the FFT.
+struct mirt_nufft {
+  mirt_interp_plan *ip = nullptr;
+  mirt::GlueGeom gg{};
+  int C = 0, nslice = 0;
+  long long Mtot = 0;
+  mirt::DMem sn, grid, grid_cm, hx, hX;  // grid: coil innermost (interp); grid_cm: coil-major (FFT)
+  cufftHandle fft = 0;
+  bool fft_ok = false;
+  ~mirt_nufft() {
+    if (fft_ok) cufftDestroy(fft);
+    delete ip;
+  }
+};

@@ -9,6 +9,8 @@ the shapes and value distributions the configurations name.
   mri/ir_mri_kspace_ga_radial.m:34-53), scaled to radians
 * 3D kooshball: spokes through the centre along directions on a Fibonacci
   sphere
+* variable-density spirals and random variable-density point sets (the
+  training trajectories of the learned density compensation)
 * phantoms: random ellipses / ellipsoids with amplitude U[0,1] and phase
   U[-pi, pi)
 * coil maps: smooth complex Gaussian bumps with seeded centres and widths
@@ -34,6 +36,31 @@ def ga_radial(nspoke: int, nro: int, start: float = np.pi / 2) -> np.ndarray:
     kx = np.outer(rho, np.cos(phi))
     ky = np.outer(rho, np.sin(-phi))
     return 2 * np.pi * np.stack([kx.ravel(order="F"), ky.ravel(order="F")], 1)
+
+
+def vd_spiral(ninterleave: int, nsamp: int, N: int, alpha: float = 1.5) -> np.ndarray:
+    """[ninterleave*nsamp, 2] radians: variable-density spiral interleaves.
+
+    Radius pi * t**alpha and angle 2 pi * turns * t for t in [0, 1], with
+    turns = N / (2 ninterleave) (Nyquist-spaced turns at the edge for
+    alpha = 1); alpha > 1 samples the centre more densely.  Interleave i is
+    rotated by 2 pi i / ninterleave; samples of one interleave are contiguous.
+    """
+    t = np.linspace(0, 1, nsamp)
+    turns = N / (2.0 * ninterleave)
+    r = np.pi * t ** alpha
+    th = 2 * np.pi * turns * t
+    rot = 2 * np.pi * np.arange(ninterleave) / ninterleave
+    a = th[None, :] + rot[:, None]
+    return np.stack([(r * np.cos(a)).ravel(), (r * np.sin(a)).ravel()], 1)
+
+
+def vd_random(M: int, rng: np.random.Generator, gamma: float = 1.6) -> np.ndarray:
+    """[M, 2] radians: random variable-density points, radius pi * u**gamma
+    (u ~ U[0, 1]), angle ~ U[0, 2 pi); gamma > 1 concentrates the centre."""
+    r = np.pi * rng.uniform(0, 1, M) ** gamma
+    a = rng.uniform(0, 2 * np.pi, M)
+    return np.stack([r * np.cos(a), r * np.sin(a)], 1)
 
 
 def kooshball(nspoke: int, nro: int) -> np.ndarray:
