@@ -269,6 +269,51 @@ int mirt_dcf_pipe(mirt_nufft *p, double *w, int32_t init_ones, int32_t niter, do
 	const double *fov, int32_t *iters, double *resid, void *stream);
 int mirt_dcf_jackson(mirt_nufft *p, double *w, void *stream);
 
+/* The final step of mirt_dcf_pipe on its own: scale w (device FP64 [Mtot])
+ * so that sum(real(G' w)) = prod(N ./ fov) per slice (fov: D values or NULL
+ * for 1), as mri/ir_mri_density_comp.m:258-261 does; for weights from
+ * elsewhere (e.g. the learned regressor below).  Synchronous. */
+int mirt_dcf_scale(mirt_nufft *p, double *w, const double *fov, void *stream);
+
+/* ------------------------------------------------------------------------
+ * 3c. learned density compensation (no counterpart in the reference)
+ *
+ * Features of each 2D sample (MIRT_DCF_NFEAT floats, row per sample, sample
+ * order of om): |omega| / pi, atan2(omega_2, omega_1) / pi, and log1p of the
+ * counts of other samples of the same trajectory (slice) at distance
+ * [b/8, (b+1)/8) grid cells, b < 16, of the oversampled grid
+ * (t = omega / (2 pi / K), no periodic wrap).  Counts are exact (FP64
+ * distances).  om: device FP64 [M, 2] column-major; feat: device FP32.
+ * Synchronous. */
+#define MIRT_DCF_NFEAT 18
+int mirt_dcf_features(const double *om, int64_t M, const int64_t *slice_moff, int32_t nslice,
+	const int32_t *K, float *feat, void *stream);
+
+/* Regressor 18 -> 64 -> 64 -> 64 -> 1 (ReLU) with BF16 weights and FP32
+ * accumulation.  Parameters: one FP32 vector of MIRT_MLP_NPARAM values,
+ * W1[64][18] b1[64] W2[64][64] b2[64] W3[64][64] b3[64] W4[64] b4 (row =
+ * output unit); the kernels use their BF16 rounding.
+ *   create   copies the initial parameters (host) to the device
+ *   params   copies the FP32 master parameters back to the host
+ *   grad     gradient (host, MIRT_MLP_NPARAM) and loss of the mean squared
+ *            error over the n rows of x (device [n][18]) against y (device [n])
+ *   train    `steps` Adam steps (lr, beta 0.9 / 0.999, eps 1e-8) on batches of
+ *            `batch` rows drawn by a counter-based hash of (seed, step, row);
+ *            loss_hist (host, `steps` floats, or NULL) gets each step's loss
+ *   infer    yhat = network output (device FP32 [n], or NULL) and / or
+ *            w = exp(sigma * yhat + mu) (device FP64 [n], or NULL); async */
+#define MIRT_MLP_NPARAM 9601
+typedef struct mirt_mlp mirt_mlp;
+int mirt_mlp_create(mirt_mlp **out, const float *params);
+int mirt_mlp_params(mirt_mlp *m, float *params);
+int mirt_mlp_grad(mirt_mlp *m, const float *x, const float *y, int64_t n, float *grad,
+	float *loss, void *stream);
+int mirt_mlp_train(mirt_mlp *m, const float *x, const float *y, int64_t n, int32_t batch,
+	int32_t steps, float lr, uint64_t seed, float *loss_hist, void *stream);
+int mirt_mlp_infer(mirt_mlp *m, const float *x, int64_t n, float mu, float sigma, float *yhat,
+	double *w, void *stream);
+int mirt_mlp_destroy(mirt_mlp *m);
+
 /* ------------------------------------------------------------------------
  * 4. forward gather for callers that cannot allocate device memory (no
  *    counterpart in the reference, whose mex files run on the host)

@@ -5,6 +5,7 @@ interfaces.
 * ``mirt_b200.mex``: the six mex gateways (interp{1,2,3}_table[_adj]_mex)
 * ``mirt_b200.nufft``: device plans, nufft_init / nufft / nufft_adj
 * ``mirt_b200.dcf``: density compensation (ir_mri_density_comp 'pipe', 'jackson')
+* ``mirt_b200.learned_dcf``: the learned density compensation (features, MLP)
 * ``include/mirt_b200.h``: the C ABI of libmirt_b200.so underneath both
 
 All compute runs in libmirt_b200.so; importing the package does not load it,
@@ -16,6 +17,7 @@ from .mex import (MexError, interp1_table_adj_mex, interp1_table_mex, interp2_ta
 from .nufft import (InterpPlan, NufftPlan, minmax_kb_scale, minmax_kb_table, nufft, nufft_adj,
                     nufft_init)
 from .dcf import dcf_jackson, dcf_pipe, ir_mri_density_comp
+from .learned_dcf import DcfMLP, LearnedDCF, dcf_features
 
 __all__ = [
     "MirtError", "MexError", "load",
@@ -24,4 +26,5 @@ __all__ = [
     "InterpPlan", "NufftPlan", "minmax_kb_table", "minmax_kb_scale",
     "nufft_init", "nufft", "nufft_adj",
     "dcf_pipe", "dcf_jackson", "ir_mri_density_comp",
+    "dcf_features", "DcfMLP", "LearnedDCF",
 ]

@@ -62,6 +62,16 @@ _SIGS = {
     "mirt_interp_plan_set_spread": ([_vp, _i32p, _i32, _i32, _vp], C.c_int),
     "mirt_dcf_pipe": ([_vp, _vp, _i32, _i32, C.c_double, _dp, _i32p, _dp, _vp], C.c_int),
     "mirt_dcf_jackson": ([_vp, _vp, _vp], C.c_int),
+    "mirt_dcf_scale": ([_vp, _vp, _dp, _vp], C.c_int),
+    "mirt_dcf_features": ([_vp, _i64, _i64p, _i32, _i32p, _vp, _vp], C.c_int),
+    "mirt_mlp_create": ([C.POINTER(_vp), C.POINTER(C.c_float)], C.c_int),
+    "mirt_mlp_params": ([_vp, C.POINTER(C.c_float)], C.c_int),
+    "mirt_mlp_grad": ([_vp, _vp, _vp, _i64, C.POINTER(C.c_float), C.POINTER(C.c_float), _vp],
+                      C.c_int),
+    "mirt_mlp_train": ([_vp, _vp, _vp, _i64, _i32, _i32, C.c_float, C.c_uint64,
+                        C.POINTER(C.c_float), _vp], C.c_int),
+    "mirt_mlp_infer": ([_vp, _vp, _i64, C.c_float, C.c_float, _vp, _vp, _vp], C.c_int),
+    "mirt_mlp_destroy": ([_vp], C.c_int),
     "mirt_interp_plan_destroy": ([_vp], C.c_int),
     "mirt_nufft_create": ([C.POINTER(_vp), _i32, _i32p, _i32p, _i32p, _i32p, _dp, _dp, _i64,
                            _i64p, _i32, _i32, _vp], C.c_int),

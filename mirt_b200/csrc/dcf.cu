@@ -170,6 +170,31 @@ int ppt(mirt_nufft *p, const float2 *f, float2 *g, cudaStream_t st) {
   return MIRT_OK;
 }
 
+// scale: sum(real(G' w)) = prod(N ./ fov) per slice (mri/ir_mri_density_comp.m:258-261)
+int scale_to_psf(mirt_nufft *p, double *w, const double *fov, DcfBuffers &b, cudaStream_t st) {
+  const long long M = p->Mtot;
+  const int S = p->nslice;
+  double target = 1.0;
+  for (int d = 0; d < p->gg.D; d++) {
+    const double fv = fov ? fov[d] : 1.0;
+    if (!(fv > 0.0)) return api_fail(MIRT_ERR_ARG, "fov must be positive");
+    target *= p->gg.N[d] / fv;
+  }
+  DMem x, sums;
+  DCK(x.alloc((size_t)S * p->gg.npix * sizeof(float2)));
+  DCK(sums.alloc(S * sizeof(double)));
+  w_to_c64_kernel<<<grid_for(M, 256), 256, 0, st>>>(w, M, b.f.as<float2>());
+  DCK(cudaGetLastError());
+  int rc = mirt_nufft_adjoint(p, b.f.p, x.p, st);
+  if (rc) return rc;
+  psf_sum_kernel<<<S, 256, 0, st>>>(x.as<float2>(), p->gg.npix, sums.as<double>());
+  DCK(cudaGetLastError());
+  const int *slice_of = S > 1 ? b.slice_of.as<int>() : nullptr;
+  dcf_scale_kernel<<<grid_for(M, 256), 256, 0, st>>>(w, slice_of, M, sums.as<double>(), target);
+  DCK(cudaGetLastError());
+  return MIRT_OK;
+}
+
 int check_plan(mirt_nufft *p, const double *w) {
   if (!p) return api_fail(MIRT_ERR_ARG, "nufft is NULL");
   if (!w) return api_fail(MIRT_ERR_ARG, "w is NULL");
@@ -195,7 +220,7 @@ int mirt_dcf_pipe(mirt_nufft *p, double *w, int32_t init_ones, int32_t niter, do
   DcfBuffers b;
   rc = b.alloc(p, st);
   if (rc) return rc;
-  DMem active, rbits, rdev, idev, flags, x, sums;
+  DMem active, rbits, rdev, idev, flags;
   DCK(active.alloc(S * sizeof(int)));
   DCK(rbits.alloc(S * sizeof(unsigned long long)));
   DCK(rdev.alloc(S * sizeof(double)));
@@ -242,25 +267,23 @@ int mirt_dcf_pipe(mirt_nufft *p, double *w, int32_t init_ones, int32_t niter, do
     DCK(cudaStreamSynchronize(st));
     if (h[0]) return api_fail(MIRT_ERR_ARG, "pipe bug: non-positive P P' w");
   }
-  // scale: sum(real(G' w)) = prod(N ./ fov) per slice
-  double target = 1.0;
-  for (int d = 0; d < D; d++) {
-    const double fv = fov ? fov[d] : 1.0;
-    if (!(fv > 0.0)) return api_fail(MIRT_ERR_ARG, "fov must be positive");
-    target *= p->gg.N[d] / fv;
-  }
-  DCK(x.alloc((size_t)S * p->gg.npix * sizeof(float2)));
-  DCK(sums.alloc(S * sizeof(double)));
-  w_to_c64_kernel<<<grid_for(M, 256), 256, 0, st>>>(w, M, b.f.as<float2>());
-  DCK(cudaGetLastError());
-  rc = mirt_nufft_adjoint(p, b.f.p, x.p, stream);
+  rc = scale_to_psf(p, w, fov, b, st);
   if (rc) return rc;
-  psf_sum_kernel<<<S, 256, 0, st>>>(x.as<float2>(), p->gg.npix, sums.as<double>());
-  DCK(cudaGetLastError());
-  dcf_scale_kernel<<<grid_for(M, 256), 256, 0, st>>>(w, slice_of, M, sums.as<double>(), target);
-  DCK(cudaGetLastError());
   if (iters) DCK(cudaMemcpyAsync(iters, idev.p, S * sizeof(int), cudaMemcpyDeviceToHost, st));
   if (resid) DCK(cudaMemcpyAsync(resid, rdev.p, S * sizeof(double), cudaMemcpyDeviceToHost, st));
+  DCK(cudaStreamSynchronize(st));
+  return MIRT_OK;
+}
+
+int mirt_dcf_scale(mirt_nufft *p, double *w, const double *fov, void *stream) {
+  int rc = check_plan(p, w);
+  if (rc) return rc;
+  cudaStream_t st = as_stream(stream);
+  DcfBuffers b;
+  rc = b.alloc(p, st);
+  if (rc) return rc;
+  rc = scale_to_psf(p, w, fov, b, st);
+  if (rc) return rc;
   DCK(cudaStreamSynchronize(st));
   return MIRT_OK;
 }
