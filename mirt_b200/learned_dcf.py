@@ -235,6 +235,14 @@ class LearnedDCF:
         np.savez(path, params=self.mlp.params(), mu=self.mu, sigma=self.sigma, N=self.N, K=self.K)
 
     @staticmethod
+    def pretrained(N: int = 256, K: int = 512):
+        """The regressor trained by ``python -m mirt_b200.learned_dcf --ntraj 10000
+        --steps 20000 --batch 16384`` (seed 0), shipped in mirt_b200/data."""
+        import os
+        path = os.path.join(os.path.dirname(__file__), "data", f"learned_dcf_n{N}_k{K}.npz")
+        return LearnedDCF.load(path)
+
+    @staticmethod
     def load(path):
         z = np.load(path)
         return LearnedDCF(DcfMLP(z["params"]), float(z["mu"]), float(z["sigma"]), int(z["N"]),
