@@ -276,6 +276,40 @@ int mirt_dcf_jackson(mirt_nufft *p, double *w, void *stream);
 int mirt_dcf_scale(mirt_nufft *p, double *w, const double *fov, void *stream);
 
 /* ------------------------------------------------------------------------
+ * 3d. batched CG-SENSE on a 2D NUFFT plan (one problem per slice, ncol = coils)
+ *
+ * A = Asense(G, sens) (systems/Asense.m:53-56), R = C'C of Reg1's quadratic
+ * first-order penalty with its defaults (penalty/Reg1.m, offsets
+ * [1 nx nx+1 nx-1] of penalty/penalty_offsets.m, 'tight' edges and
+ * w = beta / |offset| of penalty/Rweights.m), beta per problem.
+ *   sens  device complex64 [S][N2][N1][C] (copied)
+ *   x     device complex64 [S][N2][N1];  y: device complex64 [Mtot][C]
+ * forward y = A x, adjoint x = A' y, reg rx = R x (all asynchronous).
+ * mirt_sense_cg runs `niter` iterations of wls/qpwls_pcg1.m:94-189 (precon 1,
+ * Fletcher-Reeves, real step, FP64 inner products per problem) from the x
+ * given, in place, with data weights W (device FP32 [Mtot], all coils) or
+ * NULL for W = 1.  With xref (device, layout of x) and nrmse (host FP64
+ * [(niter + 1) * S]), nrmse[it * S + s] = ||x_it - xref|| / ||xref|| of
+ * problem s; ms (host FP32 [niter] or NULL) gets the device time from the
+ * start of the call to the end of each iteration.  Returns after the last
+ * iteration.  S <= 1024. */
+typedef struct mirt_sense mirt_sense;
+int mirt_sense_create(mirt_sense **out, mirt_nufft *G, const void *sens, const double *beta,
+	void *stream);
+int mirt_sense_forward(mirt_sense *op, const void *x, void *y, void *stream);
+int mirt_sense_adjoint(mirt_sense *op, const void *y, void *x, void *stream);
+int mirt_sense_reg(mirt_sense *op, const void *x, void *rx, void *stream);
+int mirt_sense_cg(mirt_sense *op, void *x, const void *y, const float *W, int32_t niter,
+	const void *xref, double *nrmse, float *ms, void *stream);
+/* Warm start for mirt_sense_cg: x = a A'(W y) per problem, the density-
+ * compensated conjugate-phase image (the initial estimate of
+ * example/mri_example.m:125 and :148) with a = Re<A x, y> / ||A x||^2, the
+ * least-squares scale.  W: device FP32 [Mtot] weights (a density
+ * compensation) or NULL.  Synchronous. */
+int mirt_sense_warm_start(mirt_sense *op, void *x, const void *y, const float *W, void *stream);
+int mirt_sense_destroy(mirt_sense *op);
+
+/* ------------------------------------------------------------------------
  * 3c. learned density compensation (no counterpart in the reference)
  *
  * Features of each 2D sample (MIRT_DCF_NFEAT floats, row per sample, sample

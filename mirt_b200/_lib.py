@@ -63,6 +63,13 @@ _SIGS = {
     "mirt_dcf_pipe": ([_vp, _vp, _i32, _i32, C.c_double, _dp, _i32p, _dp, _vp], C.c_int),
     "mirt_dcf_jackson": ([_vp, _vp, _vp], C.c_int),
     "mirt_dcf_scale": ([_vp, _vp, _dp, _vp], C.c_int),
+    "mirt_sense_create": ([C.POINTER(_vp), _vp, _vp, _dp, _vp], C.c_int),
+    "mirt_sense_forward": ([_vp, _vp, _vp, _vp], C.c_int),
+    "mirt_sense_adjoint": ([_vp, _vp, _vp, _vp], C.c_int),
+    "mirt_sense_reg": ([_vp, _vp, _vp, _vp], C.c_int),
+    "mirt_sense_cg": ([_vp, _vp, _vp, _vp, _i32, _vp, _dp, C.POINTER(C.c_float), _vp], C.c_int),
+    "mirt_sense_warm_start": ([_vp, _vp, _vp, _vp, _vp], C.c_int),
+    "mirt_sense_destroy": ([_vp], C.c_int),
     "mirt_dcf_features": ([_vp, _i64, _i64p, _i32, _i32p, _vp, _vp], C.c_int),
     "mirt_mlp_create": ([C.POINTER(_vp), C.POINTER(C.c_float)], C.c_int),
     "mirt_mlp_params": ([_vp, C.POINTER(C.c_float)], C.c_int),
