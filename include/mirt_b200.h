@@ -193,10 +193,10 @@ int mirt_interp_plan_adjoint(mirt_interp_plan *plan, const void *fm, void *ck, v
  * bitwise deterministic for any choice. */
 int mirt_interp_plan_autotune(mirt_interp_plan *plan, void *stream);
 
-/* Current launch configuration: up to 15 values
+/* Current launch configuration: up to 16 values
  * {T1, T2, T3, spread threads, spread heavy-first order, coil lanes,
  *  gather threads, (unused), gather CTAs, B1, B2, B3, split chunk,
- *  spread tasks, spare tile columns}. */
+ *  spread tasks, spare tile columns, partial-tile reductions}. */
 int mirt_interp_plan_config(mirt_interp_plan *plan, int32_t *out, int32_t n);
 
 /* Fix the spread's tiling instead of autotuning it: tile extents T[0..D-1]
@@ -301,6 +301,25 @@ int mirt_sense_adjoint(mirt_sense *op, const void *y, void *x, void *stream);
 int mirt_sense_reg(mirt_sense *op, const void *x, void *rx, void *stream);
 int mirt_sense_cg(mirt_sense *op, void *x, const void *y, const float *W, int32_t niter,
 	const void *xref, double *nrmse, float *ms, void *stream);
+/* Attach the Toeplitz Gram operator of the plan's NUFFT (no data weights;
+ * see mirt_toeplitz_create) and the circulant preconditioner built from it
+ * (spectrum 1 / max(lam Re H + r, 1e-3 max), lam the problem's mean coil
+ * power, r the spectrum of the Reg1 penalty).  om: the plan's host FP64
+ * [Mtot, 2] column-major trajectory.  Synchronous. */
+int mirt_sense_toeplitz(mirt_sense *op, const double *om, void *stream);
+
+/* mirt_sense_cg with options (flags, OR of):
+ *   MIRT_PCG_CIRCULANT  precondition with the attached circulant
+ *                       preconditioner (qpwls_pcg1's `precon`)
+ *   MIRT_PCG_TOEPLITZ   iterate on the normal equations with the attached
+ *                       Toeplitz Gram operator, b = A'y, as
+ *                       wls/qpwls_pcg2.m does (W must be NULL)
+ * Both need mirt_sense_toeplitz first. */
+#define MIRT_PCG_CIRCULANT 1
+#define MIRT_PCG_TOEPLITZ 2
+int mirt_sense_pcg(mirt_sense *op, void *x, const void *y, const float *W, int32_t niter,
+	int32_t flags, const void *xref, double *nrmse, float *ms, void *stream);
+
 /* Warm start for mirt_sense_cg: x = a A'(W y) per problem, the density-
  * compensated conjugate-phase image (the initial estimate of
  * example/mri_example.m:125 and :148) with a = Re<A x, y> / ||A x||^2, the
@@ -308,6 +327,23 @@ int mirt_sense_cg(mirt_sense *op, void *x, const void *y, const float *W, int32_
  * compensation) or NULL.  Synchronous. */
 int mirt_sense_warm_start(mirt_sense *op, void *x, const void *y, const float *W, void *stream);
 int mirt_sense_destroy(mirt_sense *op);
+
+/* ------------------------------------------------------------------------
+ * 3e. Toeplitz Gram operator T = G'WG of a batched 2D NUFFT
+ *     (systems/Gnufft_gram.m; kernel as Gnufft_gram_init2, :183-198)
+ *
+ * Built from two adjoint NUFFTs of the weights (FP32 tables and FFTs, one
+ * slice per problem), embedded in a 2N1 x 2N2 circulant per slice and made
+ * Hermitian (systems/private/dsft_gram_hermitify.m).  om: host FP64 [M, 2]
+ * column-major; w: device FP64 [M] or NULL for W = 1; ncol: columns per
+ * image for apply.  apply: y = T x for x, y device complex64
+ * [S][N2][N1][ncol] (asynchronous). */
+typedef struct mirt_toeplitz mirt_toeplitz;
+int mirt_toeplitz_create(mirt_toeplitz **out, const double *om, int64_t M,
+	const int64_t *slice_moff, int32_t nslice, const int32_t *Nd, const int32_t *Kd,
+	const int32_t *Jd, const int32_t *Ld, const double *w, int32_t ncol, void *stream);
+int mirt_toeplitz_apply(mirt_toeplitz *T, const void *x, void *y, void *stream);
+int mirt_toeplitz_destroy(mirt_toeplitz *T);
 
 /* ------------------------------------------------------------------------
  * 3c. learned density compensation (no counterpart in the reference)

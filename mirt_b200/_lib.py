@@ -70,6 +70,13 @@ _SIGS = {
     "mirt_sense_cg": ([_vp, _vp, _vp, _vp, _i32, _vp, _dp, C.POINTER(C.c_float), _vp], C.c_int),
     "mirt_sense_warm_start": ([_vp, _vp, _vp, _vp, _vp], C.c_int),
     "mirt_sense_destroy": ([_vp], C.c_int),
+    "mirt_sense_toeplitz": ([_vp, _dp, _vp], C.c_int),
+    "mirt_sense_pcg": ([_vp, _vp, _vp, _vp, _i32, _i32, _vp, _dp, C.POINTER(C.c_float), _vp],
+                       C.c_int),
+    "mirt_toeplitz_create": ([C.POINTER(_vp), _dp, _i64, _i64p, _i32, _i32p, _i32p, _i32p,
+                              _i32p, _vp, _i32, _vp], C.c_int),
+    "mirt_toeplitz_apply": ([_vp, _vp, _vp, _vp], C.c_int),
+    "mirt_toeplitz_destroy": ([_vp], C.c_int),
     "mirt_dcf_features": ([_vp, _i64, _i64p, _i32, _i32p, _vp, _vp], C.c_int),
     "mirt_mlp_create": ([C.POINTER(_vp), C.POINTER(C.c_float)], C.c_int),
     "mirt_mlp_params": ([_vp, C.POINTER(C.c_float)], C.c_int),

@@ -740,10 +740,10 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
 
 int mirt_interp_plan_config(mirt_interp_plan *P, int32_t *out, int32_t n) {
   if (!P || !out) return fail(MIRT_ERR_ARG, "NULL argument");
-  const int32_t v[15] = {P->t.T[0], P->t.T[1], P->t.T[2], P->ls.threads, P->heavy_first, P->ls.cw,
+  const int32_t v[16] = {P->t.T[0], P->t.T[1], P->t.T[2], P->ls.threads, P->heavy_first, P->ls.cw,
                          P->lg.threads, P->lg.sb, P->lg.grid, P->t.B[0], P->t.B[1], P->t.B[2],
-                         P->split_chunk, P->t.ntask, P->t.padc};
-  for (int i = 0; i < n && i < 15; i++) out[i] = v[i];
+                         P->split_chunk, P->t.ntask, P->t.padc, P->t.nred};
+  for (int i = 0; i < n && i < 16; i++) out[i] = v[i];
   return MIRT_OK;
 }
 

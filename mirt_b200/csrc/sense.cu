@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "runtime.cuh"
+#include "toeplitz.cuh"
 
 using namespace mirt;
 
@@ -145,8 +146,16 @@ __global__ void k_segdot(const float2 *__restrict__ a, const float2 *__restrict_
   if (threadIdx.x == 0) out[s * stride] = part[0];
 }
 
+// out = b - u - v (the negative gradient of the Gram form)
+__global__ void k_sub2(const float2 *__restrict__ b, const float2 *__restrict__ u,
+                       const float2 *__restrict__ v, float2 *__restrict__ out, long long n) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+       e += (long long)gridDim.x * blockDim.x)
+    out[e] = make_float2(b[e].x - u[e].x - v[e].x, b[e].y - u[e].y - v[e].y);
+}
+
 // Fletcher-Reeves: gamma = new / old (0 on the first iteration or old = 0);
-// ddir = ngrad + gamma ddir; old = new
+// ddir = pregrad + gamma ddir; old = new
 __global__ void k_dir(const float2 *__restrict__ ngrad, float2 *__restrict__ ddir,
                       const double *__restrict__ sc, long long np, int S, int first) {
   const long long n = (long long)S * np;
@@ -220,6 +229,9 @@ struct mirt_sense {
   int S = 0, C = 0, N1 = 0, N2 = 0;
   long long np = 0, M = 0;
   DMem sens, beta, z, ioff, soff, slice_of;
+  std::vector<double> beta_host;
+  mirt_toeplitz *T = nullptr;  // Gram operator and preconditioner (mirt_sense_toeplitz)
+  ~mirt_sense() { delete T; }
 };
 
 namespace {
@@ -285,6 +297,7 @@ int mirt_sense_create(mirt_sense **out, mirt_nufft *G, const void *sens, const d
   }
   cudaError_t e = cudaMemcpyAsync(op->sens.p, sens, nimg * op->C * sizeof(float2),
                                   cudaMemcpyDeviceToDevice, st);
+  op->beta_host.assign(beta, beta + op->S);
   if (!e) e = cudaMemcpyAsync(op->beta.p, beta, op->S * sizeof(double), cudaMemcpyHostToDevice, st);
   if (!e) e = cudaMemcpyAsync(op->ioff.p, io.data(), io.size() * sizeof(long long),
                               cudaMemcpyHostToDevice, st);
@@ -316,23 +329,35 @@ int mirt_sense_reg(mirt_sense *op, const void *x, void *rx, void *stream) {
   return sense_R(op, static_cast<const float2 *>(x), static_cast<float2 *>(rx), as_stream(stream));
 }
 
-int mirt_sense_cg(mirt_sense *op, void *x_, const void *y_, const float *W, int32_t niter,
-                  const void *xref_, double *nrmse, float *ms, void *stream) {
+int mirt_sense_pcg(mirt_sense *op, void *x_, const void *y_, const float *W, int32_t niter,
+                   int32_t flags, const void *xref_, double *nrmse, float *ms, void *stream) {
   if (!op || !x_ || !y_) return api_fail(MIRT_ERR_ARG, "NULL argument");
   if (niter < 0) return api_fail(MIRT_ERR_ARG, "niter must be >= 0");
+  const bool precon = flags & MIRT_PCG_CIRCULANT, gram = flags & MIRT_PCG_TOEPLITZ;
+  if ((precon || gram) && !op->T)
+    return api_fail(MIRT_ERR_ARG, "attach the Toeplitz operator first (mirt_sense_toeplitz)");
+  if (gram && W) return api_fail(MIRT_ERR_ARG, "the Toeplitz Gram form takes no data weights");
   cudaStream_t st = as_stream(stream);
   const int S = op->S, C = op->C;
   const long long ni = (long long)S * op->np, ns = op->M * C;
   float2 *x = static_cast<float2 *>(x_);
   const float2 *y = static_cast<const float2 *>(y_);
   const float2 *xref = static_cast<const float2 *>(xref_);
-  DMem Ax, Adir, r, Rx, Rdir, ngrad, ddir, sc, err, refn;
-  SCK(Ax.alloc(std::max<long long>(ns, 1) * sizeof(float2)));
-  SCK(Adir.alloc(std::max<long long>(ns, 1) * sizeof(float2)));
-  SCK(r.alloc(std::max<long long>(ns, 1) * sizeof(float2)));
+  // data-side vectors: Ax, Adir, residual (form 1) or A'y, Gx, Gdir (Gram form)
+  DMem Ax, Adir, r, Rx, Rdir, ngrad, pgrad, ddir, sc, err, refn;
+  if (gram) {
+    SCK(Ax.alloc(ni * sizeof(float2)));    // G x
+    SCK(Adir.alloc(ni * sizeof(float2)));  // G ddir
+    SCK(r.alloc(ni * sizeof(float2)));     // b = A'y
+  } else {
+    SCK(Ax.alloc(std::max<long long>(ns, 1) * sizeof(float2)));
+    SCK(Adir.alloc(std::max<long long>(ns, 1) * sizeof(float2)));
+    SCK(r.alloc(std::max<long long>(ns, 1) * sizeof(float2)));
+  }
   SCK(Rx.alloc(ni * sizeof(float2)));
   SCK(Rdir.alloc(ni * sizeof(float2)));
   SCK(ngrad.alloc(ni * sizeof(float2)));
+  if (precon) SCK(pgrad.alloc(ni * sizeof(float2)));
   SCK(ddir.alloc(ni * sizeof(float2)));
   SCK(sc.alloc(S * SC_N * sizeof(double)));
   SCK(cudaMemsetAsync(sc.p, 0, S * SC_N * sizeof(double), st));
@@ -356,35 +381,66 @@ int mirt_sense_cg(mirt_sense *op, void *x_, const void *y_, const float *W, int3
   auto cleanup = [&]() {
     for (auto &e : ev) cudaEventDestroy(e);
   };
-  // Ax, R x of the initial estimate
-  int rc = sense_A(op, x, Ax.as<float2>(), st);
+  auto gram_apply = [&](const float2 *v, float2 *out) {
+    return toep_gram_sense(op->T, v, op->sens.as<float2>(), out, st);
+  };
+  // data term and penalty of the initial estimate
+  int rc = MIRT_OK;
+  if (gram) {
+    rc = sense_At(op, y, r.as<float2>(), nullptr, st);  // b = A'y
+    if (!rc) rc = gram_apply(x, Ax.as<float2>());
+  } else {
+    rc = sense_A(op, x, Ax.as<float2>(), st);
+  }
   if (!rc) rc = sense_R(op, x, Rx.as<float2>(), st);
   const long long *ioff = op->ioff.as<long long>(), *soff = op->soff.as<long long>();
   double *scp = sc.as<double>();
   for (int it = 1; it <= niter && !rc; it++) {
     const int first = it == 1;
-    // negative gradient A'(W (y - Ax)) - R x
-    k_resid<<<nblocks(ns), 256, 0, st>>>(y, Ax.as<float2>(), W, r.as<float2>(), ns, C);
-    rc = sense_At(op, r.as<float2>(), ngrad.as<float2>(), Rx.as<float2>(), st);
-    if (rc) break;
-    k_segdot<<<S, 256, 0, st>>>(ngrad.as<float2>(), ngrad.as<float2>(), ioff, nullptr, 1,
-                                scp + SC_NEW, SC_N);
-    k_dir<<<nblocks(ni), 256, 0, st>>>(ngrad.as<float2>(), ddir.as<float2>(), scp, op->np, S,
-                                       first);
+    // negative gradient
+    if (gram) {
+      k_sub2<<<nblocks(ni), 256, 0, st>>>(r.as<float2>(), Ax.as<float2>(), Rx.as<float2>(),
+                                          ngrad.as<float2>(), ni);
+    } else {
+      k_resid<<<nblocks(ns), 256, 0, st>>>(y, Ax.as<float2>(), W, r.as<float2>(), ns, C);
+      rc = sense_At(op, r.as<float2>(), ngrad.as<float2>(), Rx.as<float2>(), st);
+      if (rc) break;
+    }
+    // preconditioned gradient and the Fletcher-Reeves direction
+    const float2 *pg = ngrad.as<float2>();
+    if (precon) {
+      rc = toep_precon_apply(op->T, ngrad.as<float2>(), pgrad.as<float2>(), st);
+      if (rc) break;
+      pg = pgrad.as<float2>();
+    }
+    k_segdot<<<S, 256, 0, st>>>(ngrad.as<float2>(), pg, ioff, nullptr, 1, scp + SC_NEW, SC_N);
+    k_dir<<<nblocks(ni), 256, 0, st>>>(pg, ddir.as<float2>(), scp, op->np, S, first);
     k_scal_dir<<<1, 64 * ((S + 63) / 64), 0, st>>>(scp, S, first);
-    // step: (ddir' ngrad) / (Adir' W Adir + ddir' R ddir)
-    rc = sense_A(op, ddir.as<float2>(), Adir.as<float2>(), st);
+    // step: (ddir' ngrad) / (data curvature + ddir' R ddir)
+    if (gram) {
+      rc = gram_apply(ddir.as<float2>(), Adir.as<float2>());
+    } else {
+      rc = sense_A(op, ddir.as<float2>(), Adir.as<float2>(), st);
+    }
     if (!rc) rc = sense_R(op, ddir.as<float2>(), Rdir.as<float2>(), st);
     if (rc) break;
-    k_segdot<<<S, 256, 0, st>>>(Adir.as<float2>(), Adir.as<float2>(), soff, W, C, scp + SC_DEN,
-                                SC_N);
+    if (gram)
+      k_segdot<<<S, 256, 0, st>>>(ddir.as<float2>(), Adir.as<float2>(), ioff, nullptr, 1,
+                                  scp + SC_DEN, SC_N);
+    else
+      k_segdot<<<S, 256, 0, st>>>(Adir.as<float2>(), Adir.as<float2>(), soff, W, C, scp + SC_DEN,
+                                  SC_N);
     k_segdot<<<S, 256, 0, st>>>(ddir.as<float2>(), Rdir.as<float2>(), ioff, nullptr, 1,
                                 scp + SC_DENR, SC_N);
     k_segdot<<<S, 256, 0, st>>>(ddir.as<float2>(), ngrad.as<float2>(), ioff, nullptr, 1,
                                 scp + SC_NUM, SC_N);
     k_scal_step<<<1, 64 * ((S + 63) / 64), 0, st>>>(scp, S);
-    k_axpy<<<nblocks(ns), 256, 0, st>>>(Ax.as<float2>(), Adir.as<float2>(), scp, ns, 0,
-                                        op->slice_of.as<int>(), C);
+    if (gram)
+      k_axpy<<<nblocks(ni), 256, 0, st>>>(Ax.as<float2>(), Adir.as<float2>(), scp, ni, op->np,
+                                          nullptr, 1);
+    else
+      k_axpy<<<nblocks(ns), 256, 0, st>>>(Ax.as<float2>(), Adir.as<float2>(), scp, ns, 0,
+                                          op->slice_of.as<int>(), C);
     k_axpy<<<nblocks(ni), 256, 0, st>>>(Rx.as<float2>(), Rdir.as<float2>(), scp, ni, op->np,
                                         nullptr, 1);
     k_axpy<<<nblocks(ni), 256, 0, st>>>(x, ddir.as<float2>(), scp, ni, op->np, nullptr, 1);
@@ -414,6 +470,53 @@ int mirt_sense_cg(mirt_sense *op, void *x_, const void *y_, const float *W, int3
       nrmse[i] = d > 0 ? std::sqrt(h[i] / d) : std::sqrt(h[i]);
     }
   }
+  return MIRT_OK;
+}
+
+int mirt_sense_cg(mirt_sense *op, void *x, const void *y, const float *W, int32_t niter,
+                  const void *xref, double *nrmse, float *ms, void *stream) {
+  return mirt_sense_pcg(op, x, y, W, niter, 0, xref, nrmse, ms, stream);
+}
+
+int mirt_sense_toeplitz(mirt_sense *op, const double *om, void *stream) {
+  if (!op || !om) return api_fail(MIRT_ERR_ARG, "NULL argument");
+  cudaStream_t st = as_stream(stream);
+  mirt_interp_plan *P = op->G->ip;
+  const int Nd[2] = {op->N1, op->N2}, Kd[2] = {P->a.g.K[0], P->a.g.K[1]};
+  const int Jd[2] = {P->a.g.J[0], P->a.g.J[1]}, Ld[2] = {P->a.g.L[0], P->a.g.L[1]};
+  mirt_toeplitz *T = nullptr;
+  int rc = toep_create(&T, om, op->M, P->moff_host.data(), op->S, Nd, Kd, Jd, Ld, nullptr, op->C,
+                       st);
+  if (rc) return rc;
+  // mean coil power per problem, for the preconditioner
+  std::vector<long long> off(op->S + 1);
+  for (int s = 0; s <= op->S; s++) off[s] = (long long)s * op->np * op->C;
+  DMem doff, pw;
+  cudaError_t e = doff.alloc((op->S + 1) * sizeof(long long));
+  if (!e) e = pw.alloc(op->S * sizeof(double));
+  if (!e) e = cudaMemcpyAsync(doff.p, off.data(), off.size() * sizeof(long long),
+                              cudaMemcpyHostToDevice, st);
+  if (e) {
+    delete T;
+    return api_fail(MIRT_ERR_CUDA, cudaGetErrorString(e));
+  }
+  k_segdot<<<op->S, 256, 0, st>>>(op->sens.as<float2>(), op->sens.as<float2>(),
+                                  doff.as<long long>(), nullptr, 1, pw.as<double>(), 1);
+  std::vector<double> lam(op->S);
+  e = cudaMemcpyAsync(lam.data(), pw.p, op->S * sizeof(double), cudaMemcpyDeviceToHost, st);
+  if (!e) e = cudaStreamSynchronize(st);
+  if (e) {
+    delete T;
+    return api_fail(MIRT_ERR_CUDA, cudaGetErrorString(e));
+  }
+  for (auto &v : lam) v /= (double)op->np;
+  rc = toep_precon_build(T, lam.data(), op->beta_host.data(), st);
+  if (rc) {
+    delete T;
+    return rc;
+  }
+  delete op->T;
+  op->T = T;
   return MIRT_OK;
 }
 

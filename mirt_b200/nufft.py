@@ -66,12 +66,12 @@ def minmax_kb_scale(N: int, J: int, K: int) -> np.ndarray:
 
 
 def _plan_config(lib, handle) -> dict:
-    v = (C.c_int32 * 15)()
-    check(lib.mirt_interp_plan_config(handle, v, 15))
+    v = (C.c_int32 * 16)()
+    check(lib.mirt_interp_plan_config(handle, v, 16))
     return {"spread_tile": [v[0], v[1], v[2]], "spread_threads": v[3], "spread_heavy_first": v[4],
             "coil_lanes": v[5], "gather_threads": v[6],
             "gather_ctas": v[8], "sort_bin": [v[9], v[10], v[11]], "split_chunk": v[12],
-            "spread_tasks": v[13], "spread_padc": v[14]}
+            "spread_tasks": v[13], "spread_padc": v[14], "spread_reductions": v[15]}
 
 
 class InterpPlan:
@@ -204,6 +204,8 @@ class NufftPlan:
             None if mo is None else mo.ctypes.data_as(_i64p), self.nslice, self.ncol,
             _stream_ptr(stream)))
         self.handle = h
+        self.om_f = omf                      # trajectory, column-major FP64 (Toeplitz set-up)
+        self.slice_moff = mo
         self.image_shape = (self.nslice,) + tuple(int(n) for n in self.Nd[::-1]) + (self.ncol,)
         self.sample_shape = (self.Mtot, self.ncol)
 

@@ -67,6 +67,33 @@ class SenseSystem:
         check(self.lib.mirt_sense_reg(self.handle, _ptr(x.contiguous()), _ptr(out), _stream_ptr(stream)))
         return out
 
+    def toeplitz(self, stream=None):
+        """Attach the Toeplitz Gram operator (Gnufft_gram) and the circulant
+        preconditioner built from it; needed by pcg(precon=True / gram=True)."""
+        check(self.lib.mirt_sense_toeplitz(self.handle, self.G.om_f.ctypes.data_as(_dp),
+                                           _stream_ptr(stream)))
+        self.has_toeplitz = True
+        return self
+
+    def pcg(self, x, y, niter, W=None, precon=False, gram=False, xref=None, timing=False,
+            stream=None):
+        """niter iterations of qpwls_pcg1 (NUFFT pair each iteration) or, with
+        gram=True, of qpwls_pcg2 on the Toeplitz normal equations; precon=True
+        uses the circulant preconditioner.  In place on x; returns (nrmse, ms)
+        as cg() does."""
+        torch = _torch()
+        Wf = None if W is None else W.to(torch.float32).contiguous()
+        flags = (1 if precon else 0) | (2 if gram else 0)
+        nr = np.zeros((niter + 1, self.S)) if xref is not None else None
+        ms = np.zeros(max(niter, 1), dtype=np.float32) if timing else None
+        check(self.lib.mirt_sense_pcg(self.handle, _ptr(x), _ptr(y.contiguous()), _ptr(Wf),
+                                      int(niter), flags,
+                                      _ptr(None if xref is None else xref.contiguous()),
+                                      None if nr is None else nr.ctypes.data_as(_dp),
+                                      None if ms is None else ms.ctypes.data_as(_fp),
+                                      _stream_ptr(stream)))
+        return nr, (ms[:niter] if timing else None)
+
     def warm_start(self, y, W=None, stream=None):
         """x0 = a A'(W y) per problem with the least-squares scale a."""
         torch = _torch()
@@ -100,6 +127,50 @@ class SenseSystem:
             self.close()
         except Exception:
             pass
+
+
+class Gram:
+    """T = Gnufft_gram(G, W): the Toeplitz-embedded Gram operator G'WG of a 2D
+    plan's trajectory (systems/Gnufft_gram.m), applied by two FFTs of the
+    2N-padded image per column.  W: device FP64 [Mtot] weights or None;
+    ncol: columns of the images it is applied to ([S, N2, N1, ncol])."""
+
+    def __init__(self, G: NufftPlan, W=None, ncol=1, stream=None):
+        self.lib = G.lib
+        self.S, self.ncol = G.nslice, int(ncol)
+        self.shape = (G.nslice, int(G.Nd[1]), int(G.Nd[0]), self.ncol)
+        mo = G.slice_moff
+        h = C.c_void_p()
+        check(self.lib.mirt_toeplitz_create(
+            C.byref(h), G.om_f.ctypes.data_as(_dp), G.Mtot,
+            None if mo is None else mo.ctypes.data_as(C.POINTER(C.c_int64)), G.nslice,
+            G.Nd.ctypes.data_as(C.POINTER(C.c_int32)), G.Kd.ctypes.data_as(C.POINTER(C.c_int32)),
+            G.Jd.ctypes.data_as(C.POINTER(C.c_int32)), G.Ld.ctypes.data_as(C.POINTER(C.c_int32)),
+            _ptr(None if W is None else W.contiguous()), self.ncol, _stream_ptr(stream)))
+        self.handle = h
+
+    def apply(self, x, out=None, stream=None):
+        torch = _torch()
+        out = torch.empty(self.shape, dtype=torch.complex64, device="cuda") if out is None else out
+        check(self.lib.mirt_toeplitz_apply(self.handle, _ptr(x.contiguous()), _ptr(out),
+                                           _stream_ptr(stream)))
+        return out
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.mirt_toeplitz_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def Gnufft_gram(G: NufftPlan, W=None, ncol=1):
+    """[T, reuse] = Gnufft_gram(A, W) (systems/Gnufft_gram.m) for a table plan."""
+    return Gram(G, W, ncol)
 
 
 def Asense(G: NufftPlan, sens, beta=0.0):

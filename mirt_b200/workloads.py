@@ -126,3 +126,23 @@ def batch_ga_radial(nslice: int, spoke_lo: int, spoke_hi: int, nro: int,
     oms = [ga_radial(int(s), nro, start=np.pi / 2 + rng.uniform(0, np.pi)) for s in spokes]
     moff = np.concatenate([[0], np.cumsum([len(o) for o in oms])]).astype(np.int64)
     return np.concatenate(oms), moff, spokes
+
+
+def cgsense_problems(nprob: int, rng: np.random.Generator, Ns=(128, 192, 256),
+                     coils=(8, 16, 24, 32), R: int = 4, snr_db: float = 30.0):
+    """Seeded CG-SENSE problems: image size N ~ U(Ns), coils C ~ U(coils),
+    golden-angle radial at undersampling R (readout 2N, ceil(pi N / 2 / R)
+    spokes), smooth coil maps, an ellipse phantom; the data and its noise
+    level (snr_db) are formed by the caller's forward operator.
+    Returns dicts with N, C, om [M, 2], sens [N2, N1, C], xtrue [N2, N1], snr_db."""
+    out = []
+    for _ in range(nprob):
+        N = int(rng.choice(Ns))
+        C = int(rng.choice(coils))
+        nspoke = int(np.ceil(np.pi * N / 2 / R))
+        om = ga_radial(nspoke, 2 * N, start=rng.uniform(0, np.pi))
+        sens = coil_maps((N, N), C, rng).transpose(1, 0, 2)
+        xt = ellipses(N, 10, rng).T.astype(np.complex64)
+        out.append(dict(N=N, C=C, om=om, sens=np.ascontiguousarray(sens), xtrue=xt,
+                        snr_db=snr_db))
+    return out
