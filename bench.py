@@ -423,7 +423,11 @@ def run_gpu(args, w):
                "sample": f"{ns} of {plan.nslice} slices, forward + adjoint, {C} coils "
                          f"({u:.3g} sample-coils in {tc:.1f} s)"}
 
-    launches_per_step = 4  # deapod_pad, gather, spread, crop_deapod (cuFFT not counted)
+    # deapod_pad, 2 transposes, gather, spread, [spread_reduce], crop_deapod (cuFFT not counted)
+    launches_per_step = 6 + (1 if tuned.get("spread_reductions", 0) > 0 else 0)
+    cg = None
+    if rank == 0 and world == 1 and not args.no_cg and w["D"] == 2:
+        cg = run_cgsense(args)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
@@ -437,6 +441,7 @@ def run_gpu(args, w):
                        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": launches_per_step * args.steps, "clocks": clk,
+            "cg_sense": cg,
         }
         print(json.dumps(line), flush=True)
     plan.close()
@@ -444,6 +449,132 @@ def run_gpu(args, w):
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+# ---------------------------------------------------------------------------
+# batched CG-SENSE: time to NRMSE 1e-3, learned density compensation vs plain
+# ---------------------------------------------------------------------------
+def _first_below(nr, ms, tol):
+    """(device ms, iterations) until every problem of the group has NRMSE <=
+    tol, or (None, None); nr [it + 1, S], ms [it]."""
+    ok = np.all(nr <= tol, axis=1)
+    if ok[0]:
+        return 0.0, 0
+    hit = np.nonzero(ok)[0]
+    if len(hit) == 0:
+        return None, None
+    i = int(hit[0])
+    return float(ms[i - 1]), i
+
+
+def run_cgsense(args):
+    """64 uneven 2D problems (N in {128, 192, 256}, 8-32 coils, golden-angle
+    radial at R = 4, 30 dB noise, quadratic Reg1 with beta = 2^-8 trace
+    scale), grouped by (N, coils) into batched plans.  Per group: a reference
+    solution, then five ways to it, each timed with CUDA events until every
+    problem has NRMSE <= 1e-3 (density-compensation and warm-start time
+    included; plan and Toeplitz set-up reported apart):
+      plain             qpwls_pcg1 from zero (precon = 1), NUFFT pair per iteration
+      precon_only       the same with the circulant preconditioner
+      learned           learned DCF (features + MLP + PSF scale) warm start + preconditioner
+      learned_toeplitz  the same on the Toeplitz normal equations (qpwls_pcg2)
+      pipe              Pipe-Menon DCF (30 updates) warm start + preconditioner"""
+    import torch
+
+    import mirt_b200 as mb
+    from mirt_b200 import learned_dcf as ld
+    from mirt_b200 import sense as ms
+    from mirt_b200 import workloads as wl
+
+    tol = 1e-3
+    modes = ("plain", "precon_only", "learned", "learned_toeplitz", "pipe")
+    rng = np.random.default_rng(5)
+    probs = wl.cgsense_problems(args.cg_problems, rng)
+    groups = {}
+    for i, p in enumerate(probs):
+        groups.setdefault((p["N"], p["C"]), []).append(i)
+    model = ld.LearnedDCF.pretrained()
+    model.predict(wl.ga_radial(8, 64))   # first-call set-up (kernel attributes) outside the timing
+    torch.cuda.synchronize()
+    st = torch.cuda.current_stream()
+
+    def ev():
+        e = torch.cuda.Event(enable_timing=True)
+        e.record(st)
+        return e
+
+    tot = {k: 0.0 for k in modes}
+    reached = {k: True for k in modes}
+    per = []
+    setup_s = 0.0
+    for (N, C), idx in sorted(groups.items()):
+        oms = [probs[i]["om"] for i in idx]
+        moff = np.concatenate([[0], np.cumsum([len(o) for o in oms])]).astype(np.int64)
+        om = np.concatenate(oms)
+        K = 2 * N
+        t0 = time.perf_counter()
+        G = mb.NufftPlan(om, (N, N), (6, 6), (K, K), n_shift=(N / 2, N / 2), Ld=1024, ncol=C,
+                         slice_moff=moff)
+        G1 = mb.NufftPlan(om, (N, N), (6, 6), (K, K), n_shift=(N / 2, N / 2), Ld=1024, ncol=1,
+                          slice_moff=moff)
+        sens = torch.from_numpy(np.stack([probs[i]["sens"] for i in idx])).cuda()
+        A = ms.SenseSystem(G, sens, ms.trace_beta(np.diff(moff), sens)).toeplitz()
+        torch.cuda.synchronize()
+        setup_s += time.perf_counter() - t0
+        xt = torch.from_numpy(np.stack([probs[i]["xtrue"] for i in idx])).cuda()
+        y = A.forward(xt)
+        g = torch.Generator(device="cuda").manual_seed(N * 100 + C)
+        noise = torch.randn(y.shape, dtype=torch.complex64, device="cuda", generator=g)
+        for s in range(len(idx)):
+            a, b = int(moff[s]), int(moff[s + 1])
+            noise[a:b] *= y[a:b].norm() / noise[a:b].norm() * 10 ** (-30 / 20)
+        y = (y + noise).contiguous()
+        sid = torch.repeat_interleave(torch.arange(len(idx), device="cuda"),
+                                      torch.from_numpy(np.diff(moff)).cuda())
+        om_d = torch.from_numpy(om).cuda()
+        xref = torch.zeros(A.image_shape, dtype=torch.complex64, device="cuda")
+        A.pcg(xref, y, args.cg_ref, precon=True)
+        res = {"N": N, "coils": C, "problems": len(idx)}
+        for mode in modes:
+            e0 = ev()
+            if mode in ("plain", "precon_only"):
+                x = torch.zeros_like(xref)
+            else:
+                if mode == "pipe":
+                    w = mb.dcf_pipe(G1, niter=29, thresh=0.0)
+                else:
+                    w = model.predict(om_d, G1, moff)
+                cnt = torch.from_numpy(np.diff(moff)).cuda()
+                sums = torch.zeros(len(idx), dtype=torch.float64, device="cuda").index_add_(0, sid, w)
+                wn = (w / (sums / cnt)[sid]).to(torch.float32)
+                x = A.warm_start(y, W=wn)
+            e1 = ev()
+            nr, tms = A.pcg(x, y, args.cg_iters, precon=(mode != "plain"),
+                            gram=(mode == "learned_toeplitz"), xref=xref, timing=True)
+            torch.cuda.synchronize()
+            pre = e0.elapsed_time(e1)
+            t, it = _first_below(nr, tms, tol)
+            res[mode] = {"s": None if t is None else (pre + t) / 1e3, "setup_s": pre / 1e3,
+                         "iters": it, "ms_per_iter": float(tms[-1] / len(tms)),
+                         "nrmse_start": float(nr[0].max()), "nrmse_end": float(nr[-1].max())}
+        for k in modes:
+            if res[k]["s"] is None:
+                reached[k] = False
+            else:
+                tot[k] += res[k]["s"]
+        per.append(res)
+        A.close()
+        del G, G1
+    out = {"metric": "CG-SENSE s to NRMSE 1e-3 (every problem of the batch)",
+           "problems": args.cg_problems, "groups": len(per), "max_iters": args.cg_iters}
+    for k in modes:
+        out[f"{k}_s"] = tot[k] if reached[k] else None
+    out.update({
+        "plan_and_toeplitz_setup_s": setup_s,
+        "reference": f"{args.cg_ref} preconditioned CG iterations from zero (FP32 operators, "
+                     "FP64 inner products; within 1e-4 of the FP64 solution on the parity cases)",
+        "per_group": per})
+    return out
 
 
 def main():
@@ -457,6 +588,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cg", action="store_true", help="skip the CG-SENSE comparison")
+    ap.add_argument("--cg-problems", type=int, default=64)
+    ap.add_argument("--cg-iters", type=int, default=60)
+    ap.add_argument("--cg-ref", type=int, default=300)
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
     if args.impl == "reference":
