@@ -276,6 +276,28 @@ def run_reference(args, w):
 # ---------------------------------------------------------------------------
 # GPU path
 # ---------------------------------------------------------------------------
+def combine_over_ranks(t_local, units_local, world, dev):
+    """Whole-job (time, units): the slowest rank's time (every rank's batch is
+    independent, so the job ends when the last rank does) and the units all
+    ranks processed.  One all-reduce each, outside the timed region."""
+    if world <= 1:
+        return t_local, units_local
+    import torch
+    import torch.distributed as dist
+    tt = torch.tensor([t_local], device=dev, dtype=torch.float64)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    uu = torch.tensor([units_local], device=dev, dtype=torch.float64)
+    dist.all_reduce(uu, op=dist.ReduceOp.SUM)
+    return float(tt.item()), float(uu.item())
+
+
+def rank_batch(w, rank):
+    """The independent batch of slices of one rank (weak scaling): its own
+    seeded trajectories; no sample is shared between ranks."""
+    rng = np.random.default_rng(1234 + rank)
+    return make_trajectory(w, rng)
+
+
 def run_gpu(args, w):
     import torch
     import torch.distributed as dist
@@ -291,8 +313,7 @@ def run_gpu(args, w):
         dist.init_process_group("nccl", timeout=timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
     dev = torch.device("cuda", local)
-    rng = np.random.default_rng(1234 + rank)
-    om, moff = make_trajectory(w, rng)
+    om, moff = rank_batch(w, rank)
     Mtot = len(om)
     C = w["ncoil"]
     D = w["D"]
@@ -336,14 +357,7 @@ def run_gpu(args, w):
     clk = clocks.stop()
     t_local = e0.elapsed_time(e1) / 1000.0
     units_local = 2.0 * Mtot * C * args.steps
-    if world > 1:
-        tt = torch.tensor([t_local], device=dev, dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        uu = torch.tensor([units_local], device=dev, dtype=torch.float64)
-        dist.all_reduce(uu, op=dist.ReduceOp.SUM)
-        t, units = float(tt.item()), float(uu.item())
-    else:
-        t, units = t_local, units_local
+    t, units = combine_over_ranks(t_local, units_local, world, dev)
     value = units / t / 1e6
 
     # --- roofline of the interpolation kernels (device buffers, same plan) ---
