@@ -118,11 +118,28 @@ void dfree(void *p, size_t bytes) {
 }  // namespace mirt
 
 
+namespace mirt_plan_kernels {
+// records of position gorder[i] to slot i (the gather's order)
+__global__ void gather_records_kernel(const int *__restrict__ gorder, long long M, int SJ,
+                                      const float2 *__restrict__ W, const int4 *__restrict__ K0,
+                                      const int *__restrict__ perm, const float2 *__restrict__ ph,
+                                      float2 *__restrict__ Wg, int4 *__restrict__ K0g,
+                                      int *__restrict__ permg, float2 *__restrict__ phg) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= M) return;
+  const long long p = gorder[i];
+  K0g[i] = K0[p];
+  permg[i] = perm ? perm[p] : (int)p;
+  if (ph) phg[i] = ph[p];
+  for (int j = 0; j < SJ; j++) Wg[i * SJ + j] = W[p * SJ + j];
+}
+}  // namespace mirt_plan_kernels
+
 namespace {
 
-// Launch shapes and tiling.  Samples are binned on 4-point bins (64 in 1D);
-// the spread runs one warp per tile (lanes = coils; the tile accumulator is
-// sized to keep several CTAs resident per SM).
+// Launch shapes and tiling.  Samples are binned on one-point bins of their
+// first tap; the spread runs one warp per tile by default (lanes = coils; the
+// tile accumulator is sized to keep several CTAs resident per SM).
 // The spread's range path serves wrapping taps when no tile can meet a
 // sample's taps both before and after their periodic wrap.
 int wrap_ok(const InterpArgs &a, const Tiling &t) {
@@ -143,16 +160,15 @@ void choose_config(mirt_interp_plan *P) {
   lg.sb = 0;
   lg.grid = 0;
 
+  // one-point sort bins: a tile's source samples in one row of bins are one
+  // contiguous range, and every visit has taps in the tile
   int B[MIRT_DMAX] = {1, 1, 1}, T[MIRT_DMAX] = {1, 1, 1};
   if (D == 1) {
-    B[0] = 64;
     T[0] = cw == 32 ? 64 : 256;
   } else if (D == 2) {
-    B[0] = B[1] = 4;
     const int e = cw == 32 ? 8 : cw == 8 ? 16 : 32;
     T[0] = T[1] = e;
   } else {
-    B[0] = B[1] = B[2] = 4;
     T[0] = T[1] = T[2] = 8;
     if (cw <= 4) T[0] = 16;
   }
@@ -188,6 +204,7 @@ int build_sources(mirt_interp_plan *P, cudaStream_t st) {
   const InterpArgs &a = P->a;
   Tiling &t = P->t;
   std::vector<int> src[MIRT_DMAX], nsrc[MIRT_DMAX];
+  std::vector<int4> run0(t.nb[0], make_int4(0, 1, 0, 0));
   for (int d = 0; d < MIRT_DMAX; d++) {
     const int nb = t.nb[d];
     src[d].assign((size_t)nb * MIRT_SRCMAX, 0);
@@ -211,12 +228,32 @@ int build_sources(mirt_interp_plan *P, cudaStream_t st) {
           }
         }
       }
+      if (d == 0) {
+        // consecutive bins in order, split where the periodic wrap restarts at 0
+        int4 r = make_int4(list[0], 1, 0, 0);
+        size_t i = 1;
+        for (; i < list.size() && list[i] == list[i - 1] + 1; i++) r.y++;
+        if (i < list.size()) {
+          r.z = list[i];
+          r.w = 1;
+          for (i++; i < list.size(); i++) {
+            if (list[i] != list[i - 1] + 1) return fail(MIRT_ERR_ARG, "spread source runs");
+            r.w++;
+          }
+        }
+        run0[b] = r;
+        continue;
+      }
       if ((int)list.size() > MIRT_SRCMAX)
         return fail(MIRT_ERR_ARG, "spread tile spans too many sort bins");
       nsrc[d][b] = (int)list.size();
       for (size_t i = 0; i < list.size(); i++) src[d][(size_t)b * MIRT_SRCMAX + i] = list[i];
     }
   }
+  CK(P->run0.alloc(run0.size() * sizeof(int4)));
+  CK(cudaMemcpyAsync(P->run0.p, run0.data(), run0.size() * sizeof(int4), cudaMemcpyHostToDevice,
+                     st));
+  t.run0 = P->run0.as<int4>();
   for (int d = 0; d < MIRT_DMAX; d++) {
     CK(P->src[d].alloc(src[d].size() * sizeof(int)));
     CK(P->nsrc[d].alloc(nsrc[d].size() * sizeof(int)));
@@ -304,6 +341,8 @@ int build_tasks(mirt_interp_plan *P, cudaStream_t st) {
     CK(cudaMemcpyAsync(nsrc[d].data(), t.nsrc[d], nsrc[d].size() * sizeof(int),
                        cudaMemcpyDeviceToHost, st));
   }
+  std::vector<int4> run0(t.nb[0]);
+  CK(cudaMemcpyAsync(run0.data(), t.run0, run0.size() * sizeof(int4), cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
   const long long chunk = std::max(32, P->split_chunk);
   struct Task {
@@ -322,15 +361,18 @@ int build_tasks(mirt_interp_plan *P, cudaStream_t st) {
       r /= t.nb[d];
     }
     long long w = 0;
-    const int n0 = nsrc[0][b[0]], n1 = D > 1 ? nsrc[1][b[1]] : 1, n2 = D > 2 ? nsrc[2][b[2]] : 1;
+    const int n1 = D > 1 ? nsrc[1][b[1]] : 1, n2 = D > 2 ? nsrc[2][b[2]] : 1;
+    const int4 rr = run0[b[0]];
     for (int i2 = 0; i2 < n2; i2++)
       for (int i1 = 0; i1 < n1; i1++)
-        for (int i0 = 0; i0 < n0; i0++) {
-          long long st_ = src[0][b[0] * MIRT_SRCMAX + i0];
-          if (D > 1) st_ += (long long)src[1][b[1] * MIRT_SRCMAX + i1] * t.nbin[0];
-          if (D > 2) st_ += (long long)src[2][b[2] * MIRT_SRCMAX + i2] * t.nbin[0] * t.nbin[1];
-          const long long bin = slice * t.nbins + st_;
-          w += bs[bin + 1] - bs[bin];
+        for (int k = 0; k < 2; k++) {
+          const int rs = k ? rr.z : rr.x, rl = k ? rr.w : rr.y;
+          if (rl == 0) continue;
+          long long row = 0;
+          if (D > 1) row += (long long)src[1][b[1] * MIRT_SRCMAX + i1] * t.nbin[0];
+          if (D > 2) row += (long long)src[2][b[2] * MIRT_SRCMAX + i2] * t.nbin[0] * t.nbin[1];
+          const long long bin = slice * t.nbins + row + rs;
+          w += bs[bin + rl] - bs[bin];
         }
     if (w >= (1ll << 31)) return fail(MIRT_ERR_ARG, "too many samples in one tile");
     if (w <= chunk) {
@@ -445,6 +487,43 @@ int plan_finish(mirt_interp_plan *P, long long Mtot, const long long *moff, int 
   CK(launch_prep_taps(a, P->wtap.as<float2>(), P->k0tap.as<int4>(), st));
   a.W = P->wtap.as<float2>();
   a.K0 = P->k0tap.as<int4>();
+  // gather order: the sorted positions re-sorted (stably) by 4-point blocks
+  // of their first taps, so that a CTA's consecutive samples share grid rows
+  // in every dimension; the gather gets its own copy of the records in that
+  // order, read sequentially
+  P->ag = a;
+  if (a.g.D > 1 && Mtot > 0) {
+    Tiling t4 = P->t;
+    t4.nbins = 1;
+    for (int d = 0; d < MIRT_DMAX; d++) {
+      t4.B[d] = d < a.g.D ? std::min(4, a.g.K[d]) : 1;
+      t4.nbin[d] = d < a.g.D ? (a.g.K[d] + t4.B[d] - 1) / t4.B[d] : 1;
+      t4.nbins *= t4.nbin[d];
+    }
+    const long long nb4 = (long long)t4.nbins * nslice;
+    DMem keys4, bs4, tmp4;
+    CK(keys4.alloc(Mtot * sizeof(uint32_t)));
+    CK(bs4.alloc((nb4 + 1) * sizeof(int)));
+    CK(tmp4.alloc(radix_sort_tmp_bytes(Mtot)));
+    DMem gorder;
+    CK(gorder.alloc(Mtot * sizeof(int)));
+    CK(launch_bin_keys(a, t4, keys4.as<uint32_t>(), st));  // a.tm, a.slice_id already sorted
+    CK(radix_sort_bins(keys4.as<uint32_t>(), Mtot, (int)nb4, tmp4.p, gorder.as<int>(),
+                       bs4.as<int>(), st));
+    CK(P->wtap_g.alloc(Mtot * a.SJ * sizeof(float2)));
+    CK(P->k0tap_g.alloc(Mtot * sizeof(int4)));
+    CK(P->perm_g.alloc(Mtot * sizeof(int)));
+    if (a.phase) CK(P->phase_g.alloc(Mtot * sizeof(float2)));
+    mirt_plan_kernels::gather_records_kernel<<<(unsigned)((Mtot + 255) / 256), 256, 0, st>>>(
+        gorder.as<int>(), Mtot, a.SJ, a.W, a.K0, a.perm, a.phase, P->wtap_g.as<float2>(),
+        P->k0tap_g.as<int4>(), P->perm_g.as<int>(), P->phase_g.as<float2>());
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(st));
+    P->ag.W = P->wtap_g.as<float2>();
+    P->ag.K0 = P->k0tap_g.as<int4>();
+    P->ag.perm = P->perm_g.as<int>();
+    P->ag.phase = a.phase ? P->phase_g.as<float2>() : nullptr;
+  }
   int rc2 = build_tasks(P, st);
   if (rc2) return rc2;
   CK(query_gather_grid(a, P->lg));
@@ -596,7 +675,7 @@ int mirt_interp_plan_create(mirt_interp_plan **plan, int32_t D, const int32_t *K
 
 int mirt_interp_plan_forward(mirt_interp_plan *P, const void *ck, void *fm, void *stream) {
   if (!P) return fail(MIRT_ERR_ARG, "plan is NULL");
-  CK(launch_gather(P->a, P->lg, static_cast<const float2 *>(ck), static_cast<float2 *>(fm),
+  CK(launch_gather(P->ag, P->lg, static_cast<const float2 *>(ck), static_cast<float2 *>(fm),
                    as_stream(stream)));
   return MIRT_OK;
 }
@@ -621,7 +700,7 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
   CK(samp.alloc(nsamp * sizeof(float2)));
   CK(cudaMemsetAsync(samp.p, 0, nsamp * sizeof(float2), st));
   CK(cudaMemsetAsync(grid.p, 0, ngrid * sizeof(float2), st));
-  // spread candidates: tile shape (multiples of the 8-point bins), warps
+  // spread candidates: tile shape (multiples of the sort bins), warps
   std::vector<SpreadCand> cands;
   const int pmax = padc_max(a);
   auto add = [&](int t0, int t1, int t2, int threads) {
@@ -725,7 +804,7 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
     CK(query_gather_grid(P->a, l));
     float ms = 0;
     int rc = time_launch([&]() {
-      return launch_gather(P->a, l, grid.as<float2>(), samp.as<float2>(), st);
+      return launch_gather(P->ag, l, grid.as<float2>(), samp.as<float2>(), st);
     }, st, &ms);
     if (rc) return rc;
     if (ms < bestg_ms) {
@@ -894,7 +973,7 @@ int mex_run(MexCall &c) {
     CK(launch_spread(P.a, P.t, P.ls, P.bin_start.as<int>(), in_il.as<float2>(),
                      out_il.as<float2>(), st));
   else
-    CK(launch_gather(P.a, P.lg, in_il.as<float2>(), out_il.as<float2>(), st));
+    CK(launch_gather(P.ag, P.lg, in_il.as<float2>(), out_il.as<float2>(), st));
   CK(launch_il_to_split(out_il.as<float2>(), nout, N, orr, oi, st));
   if (nout * N) {
     CK(cudaMemcpyAsync(c.out_re, orr, nout * N * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -1364,7 +1443,7 @@ int mirt_nufft_forward(mirt_nufft *p, const void *x, void *X, void *stream) {
   if (rc) return rc;
   CK(launch_transpose_cols(p->grid_cm.as<float2>(), p->grid.as<float2>(), p->gg.ngrid, p->C,
                            p->nslice, 1, st));
-  CK(launch_gather(p->ip->a, p->ip->lg, p->grid.as<float2>(), static_cast<float2 *>(X), st));
+  CK(launch_gather(p->ip->ag, p->ip->lg, p->grid.as<float2>(), static_cast<float2 *>(X), st));
   return MIRT_OK;
 }
 

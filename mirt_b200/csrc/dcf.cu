@@ -166,7 +166,7 @@ struct DcfBuffers {
 int ppt(mirt_nufft *p, const float2 *f, float2 *g, cudaStream_t st) {
   mirt_interp_plan *P = p->ip;
   DCK(launch_spread(P->a, P->t, P->ls, P->bin_start.as<int>(), f, p->grid.as<float2>(), st));
-  DCK(launch_gather(P->a, P->lg, p->grid.as<float2>(), g, st));
+  DCK(launch_gather(P->ag, P->lg, p->grid.as<float2>(), g, st));
   return MIRT_OK;
 }
 

@@ -53,11 +53,17 @@ struct Tiling {
   int nb[MIRT_DMAX];     // tiles per dimension
   int ntiles;            // prod(nb): tiles per slice
   int nslice;
-  // source-bin lists per dimension: for tile index b of dimension d,
+  // source bins per dimension: for tile index b of dimension d >= 1,
   // src[d][b*MIRT_SRCMAX + i], i < nsrc[d][b], are the bins whose samples
-  // (binned by their first tap) can have a tap in tile b.
+  // (binned by their first tap) can have a tap in tile b; in dimension 0 the
+  // source bins are at most two runs of consecutive bins (two when the
+  // periodic wrap splits them), run0[b] = (first, count, first, count), so
+  // that for each source row the samples of a run are one contiguous range
+  // of the sort order.  Visit order: rows (dimension 1 sources inner), then
+  // the two runs.
   const int *src[MIRT_DMAX];
   const int *nsrc[MIRT_DMAX];
+  const int4 *run0;
   // Spread work list, heaviest first.  Task i covers the sample visits
   // [task_range[i].x, task_range[i].y) of tile task_tile[i] (= slice * ntiles
   // + tile; a tile's visits are its source bins' samples in fixed order).  A
@@ -73,7 +79,7 @@ struct Tiling {
   const int4 *red;
   float2 *scratch;       // [slots][coil chunks][prod(T)][cw]
 };
-#define MIRT_SRCMAX 16
+#define MIRT_SRCMAX 48
 
 // Launch tuning chosen by the host (autotuned per geometry).
 struct Launch {

@@ -398,10 +398,10 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t,
   for (int e = threadIdx.x; e < nsm * CW; e += blockDim.x) acc[e] = make_float2(0.f, 0.f);
   __syncthreads();
 
-  int ns[MIRT_DMAX] = {1, 1, 1};
-#pragma unroll
-  for (int d = 0; d < D; d++) ns[d] = t.nsrc[d][b[d]];
-  const int nsrc_tot = ns[0] * ns[1] * ns[2];
+  // source rows (dimensions >= 1) x the two dimension-0 runs
+  const int ns1 = D > 1 ? t.nsrc[1][b[1]] : 1, ns2 = D > 2 ? t.nsrc[2][b[2]] : 1;
+  const int4 run = t.run0[b[0]];
+  const int nsrc_tot = ns1 * ns2 * 2;
   const int C = a.C;
   const int T0 = t.T[0];
   const int T1 = D > 1 ? t.T[1] : 1;
@@ -410,16 +410,14 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t,
 
   long long vbase = 0;
   for (int si = 0; si < nsrc_tot && vbase < vr.y && band_lo < band_hi; si++) {
-    int r = si, stile = 0, mul = 1;
-#pragma unroll
-    for (int d = 0; d < D; d++) {
-      const int i = r % ns[d];
-      r /= ns[d];
-      stile += t.src[d][b[d] * MIRT_SRCMAX + i] * mul;
-      mul *= t.nbin[d];
-    }
-    const int bin = slice * t.nbins + stile;
-    const long long b0 = bin_start[bin], b1 = bin_start[bin + 1];
+    const int kr = si & 1, rest = si >> 1;
+    const int rs = kr ? run.z : run.x, rl = kr ? run.w : run.y;
+    if (rl == 0) continue;
+    int row = 0;
+    if (D > 1) row += t.src[1][b[1] * MIRT_SRCMAX + rest % ns1] * t.nbin[0];
+    if (D > 2) row += t.src[2][b[2] * MIRT_SRCMAX + rest / ns1] * t.nbin[0] * t.nbin[1];
+    const int bin = slice * t.nbins + row + rs;
+    const long long b0 = bin_start[bin], b1 = bin_start[bin + rl];
     // this task's share of the tile's visit sequence
     const long long beg = b0 + max(0ll, (long long)vr.x - vbase);
     const long long end = b0 + min(b1 - b0, (long long)vr.y - vbase);

@@ -62,7 +62,11 @@ struct mirt_interp_plan {
   mirt::Launch lg{}, ls{};
   mirt::DMem tm, slice, perm, bin_start, tab[MIRT_DMAX], phase, src[MIRT_DMAX], nsrc[MIRT_DMAX];
   mirt::DMem keys, sorttmp, moff;
-  mirt::DMem task_tile, task_range, task_slot, red, scratch, wtap, k0tap;
+  mirt::DMem task_tile, task_range, task_slot, red, scratch, wtap, k0tap, run0;
+  // the gather's copy of the per-position records, in its own order (4-point
+  // blocks of the first tap); ag is `a` with these arrays
+  mirt::InterpArgs ag{};
+  mirt::DMem wtap_g, k0tap_g, perm_g, phase_g;
   int split_chunk = 1024;  // sample visits per spread task before a tile is split
   int heavy_first = 1;     // spread task order: 1 heaviest first, 0 grid order
   std::vector<long long> moff_host;
