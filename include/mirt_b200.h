@@ -245,6 +245,17 @@ int mirt_nufft_autotune(mirt_nufft *p, void *stream);
 
 int mirt_nufft_destroy(mirt_nufft *p);
 
+/* Capture one batched step of the plan -- forward x -> X when x is given,
+ * then adjoint X -> xa when xa is given -- into a CUDA graph (on an internal
+ * capture stream) and return it instantiated; mirt_graph_launch replays it
+ * on `stream` with the same buffers.  The plan's calls allocate nothing per
+ * call, so the whole step (deapodise/pad, FFTs, transposes, gather, spread,
+ * crop) is one graph launch.  The plan and buffers must outlive the graph. */
+typedef struct mirt_graph mirt_graph;
+int mirt_nufft_capture(mirt_nufft *p, const void *x, void *X, void *xa, mirt_graph **out);
+int mirt_graph_launch(mirt_graph *g, void *stream);
+int mirt_graph_destroy(mirt_graph *g);
+
 /* ------------------------------------------------------------------------
  * 3b. density compensation on a single-column NUFFT plan (ncol = 1)
  *

@@ -63,6 +63,9 @@ _SIGS = {
     "mirt_dcf_pipe": ([_vp, _vp, _i32, _i32, C.c_double, _dp, _i32p, _dp, _vp], C.c_int),
     "mirt_dcf_jackson": ([_vp, _vp, _vp], C.c_int),
     "mirt_dcf_scale": ([_vp, _vp, _dp, _vp], C.c_int),
+    "mirt_nufft_capture": ([_vp, _vp, _vp, _vp, C.POINTER(_vp)], C.c_int),
+    "mirt_graph_launch": ([_vp, _vp], C.c_int),
+    "mirt_graph_destroy": ([_vp], C.c_int),
     "mirt_sense_create": ([C.POINTER(_vp), _vp, _vp, _dp, _vp], C.c_int),
     "mirt_sense_forward": ([_vp, _vp, _vp, _vp], C.c_int),
     "mirt_sense_adjoint": ([_vp, _vp, _vp, _vp], C.c_int),

@@ -1495,6 +1495,55 @@ int mirt_nufft_adjoint_host(mirt_nufft *p, const float *X, float *x, void *strea
 
 mirt_interp_plan *mirt_nufft_interp_plan(mirt_nufft *p) { return p ? p->ip : nullptr; }
 
+}  // extern "C"
+
+struct mirt_graph {
+  cudaGraphExec_t exec = nullptr;
+  ~mirt_graph() {
+    if (exec) cudaGraphExecDestroy(exec);
+  }
+};
+
+extern "C" {
+
+int mirt_nufft_capture(mirt_nufft *p, const void *x, void *X, void *xa, mirt_graph **out) {
+  if (!p || !out || !X || (!x && !xa)) return fail(MIRT_ERR_ARG, "NULL argument");
+  *out = nullptr;
+  cudaStream_t cs;
+  CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+  cudaGraph_t graph = nullptr;
+  cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+  int rc = MIRT_OK;
+  if (e == cudaSuccess) {
+    if (x) rc = mirt_nufft_forward(p, x, X, cs);
+    if (!rc && xa) rc = mirt_nufft_adjoint(p, X, xa, cs);
+    const cudaError_t e2 = cudaStreamEndCapture(cs, &graph);
+    if (!rc && e2 != cudaSuccess) e = e2;
+  }
+  cudaGraphExec_t exec = nullptr;
+  if (!rc && e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+  if (graph) cudaGraphDestroy(graph);
+  cudaStreamDestroy(cs);
+  if (rc) return rc;
+  if (e != cudaSuccess)
+    return fail(MIRT_ERR_CUDA, std::string("NUFFT graph capture: ") + cudaGetErrorString(e));
+  auto *g = new mirt_graph();
+  g->exec = exec;
+  *out = g;
+  return MIRT_OK;
+}
+
+int mirt_graph_launch(mirt_graph *g, void *stream) {
+  if (!g) return fail(MIRT_ERR_ARG, "graph is NULL");
+  CK(cudaGraphLaunch(g->exec, as_stream(stream)));
+  return MIRT_OK;
+}
+
+int mirt_graph_destroy(mirt_graph *g) {
+  delete g;
+  return MIRT_OK;
+}
+
 int mirt_nufft_autotune(mirt_nufft *p, void *stream) {
   if (!p) return fail(MIRT_ERR_ARG, "nufft is NULL");
   return mirt_interp_plan_autotune(p->ip, stream);

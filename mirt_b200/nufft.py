@@ -232,6 +232,11 @@ class NufftPlan:
         check(self.lib.mirt_nufft_autotune(self.handle, _stream_ptr(stream)))
         return self.config()
 
+    def capture(self, x=None, X=None, xa=None):
+        """CUDA graph of forward x -> X (if x) then adjoint X -> xa (if xa) on
+        these buffers; replay with .launch(stream)."""
+        return NufftGraph(self, x, X, xa)
+
     def config(self):
         return _plan_config(self.lib, self.lib.mirt_nufft_interp_plan(self.handle))
 
@@ -308,3 +313,29 @@ def nufft_adj(X, st: NufftPlan):
     Xd = torch.from_numpy(np.asarray(X, dtype=np.complex64).reshape(-1, 1).copy()).cuda()
     x = st.adjoint(Xd).cpu().numpy()[0, ..., 0]
     return np.transpose(x, tuple(range(st.D - 1, -1, -1))).astype(np.complex128)
+
+
+class NufftGraph:
+    """One captured batched NUFFT step (mirt_nufft_capture); keeps its plan and
+    buffers alive."""
+
+    def __init__(self, plan, x, X, xa):
+        self.plan, self.bufs, self.lib = plan, (x, X, xa), plan.lib
+        h = C.c_void_p()
+        ptr = lambda t: None if t is None else C.c_void_p(t.data_ptr())
+        check(self.lib.mirt_nufft_capture(plan.handle, ptr(x), ptr(X), ptr(xa), C.byref(h)))
+        self.handle = h
+
+    def launch(self, stream=None):
+        check(self.lib.mirt_graph_launch(self.handle, _stream_ptr(stream)))
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.mirt_graph_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
