@@ -321,6 +321,8 @@ def run_gpu(args, w):
     plan = mb.NufftPlan(om, (w["N"],) * D, (w["J"],) * D, (w["K"],) * D, n_shift=n_shift,
                         Ld=w["L"], ncol=C, slice_moff=moff)
     t0 = time.perf_counter()
+    if args.nondeterministic:
+        plan.set_deterministic(False)
     tuned = plan.autotune() if not args.no_autotune else plan.config()
     t_tune = time.perf_counter() - t0
     img_np = make_images(w, np.random.default_rng(99 + rank))
@@ -469,6 +471,9 @@ def run_gpu(args, w):
                        "l2": "inputs larger than L2; no flush",
                        "launch": tuned, "autotune_s": round(t_tune, 2),
                        "step": "one CUDA graph launch (forward + adjoint of the batch)",
+                       "adjoint_order": ("shared-memory atomics (not bitwise reproducible)"
+                                         if tuned.get("spread_atomic") else
+                                         "fixed (bitwise reproducible)"),
                        "eager_ms_per_step": eager_ms,
                        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
@@ -620,6 +625,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--nondeterministic", action="store_true",
+                    help="let the spread add with shared-memory atomics (not bitwise reproducible)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cg", action="store_true", help="skip the CG-SENSE comparison")
     ap.add_argument("--cg-problems", type=int, default=64)

@@ -193,11 +193,21 @@ int mirt_interp_plan_adjoint(mirt_interp_plan *plan, const void *fm, void *ck, v
  * bitwise deterministic for any choice. */
 int mirt_interp_plan_autotune(mirt_interp_plan *plan, void *stream);
 
-/* Current launch configuration: up to 16 values
+/* Current launch configuration: up to 17 values
  * {T1, T2, T3, spread threads, spread heavy-first order, coil lanes,
  *  gather threads, (unused), gather CTAs, B1, B2, B3, split chunk,
- *  spread tasks, spare tile columns, partial-tile reductions}. */
+ *  spread tasks, spare tile columns, partial-tile reductions,
+ *  spread shared-tile atomics}. */
 int mirt_interp_plan_config(mirt_interp_plan *plan, int32_t *out, int32_t n);
+
+/* Adjoint accumulation order.  deterministic = 1 (the default): every
+ * shared-memory accumulator of a spread tile has one owner warp and samples
+ * are added in a fixed order, so the adjoint is bitwise reproducible.
+ * deterministic = 0: all warps of a tile take whole samples and add with
+ * shared-memory atomics (more warps per tile, no band tests; the same FP32
+ * arithmetic, summed in a run-dependent order); the autotuner then also
+ * tries this variant.  No reference counterpart (the reference is serial). */
+int mirt_interp_plan_set_deterministic(mirt_interp_plan *plan, int32_t deterministic);
 
 /* Fix the spread's tiling instead of autotuning it: tile extents T[0..D-1]
  * (multiples of the sort bins B of mirt_interp_plan_config, at most the grid

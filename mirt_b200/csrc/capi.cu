@@ -178,11 +178,13 @@ void choose_config(mirt_interp_plan *P) {
     if (T[d] > kr) T[d] = kr;
     T[d] = (T[d] + B[d] - 1) / B[d] * B[d];
   }
+  lg.atomic = 0;
   Launch &ls = P->ls;
   ls.threads = 32;
   ls.cw = cw;
   ls.sb = 0;
   ls.grid = 0;
+  ls.atomic = 0;
   // no spare tile columns by default; the autotuner also tries J1 - 1
   t.padc = 0;
   t.nbins = 1;
@@ -549,7 +551,7 @@ int set_spread_tiles(mirt_interp_plan *P, const int *T, cudaStream_t st) {
 
 struct SpreadCand {
   int T[MIRT_DMAX];
-  int threads, padc;
+  int threads, padc, atomic;
 };
 
 // spare columns the J = 6 row update can use (0 elsewhere)
@@ -707,7 +709,7 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
     const int npc = pmax ? 2 : 1;
     for (int ip = 0; ip < npc; ip++) {
       const int pc = ip ? pmax : 0;
-      SpreadCand c{{t0, t1, t2}, threads, pc};
+      SpreadCand c{{t0, t1, t2}, threads, pc, 0};
       for (int d = 0; d < D; d++) {
         const int kr = (a.g.K[d] + P->t.B[d] - 1) / P->t.B[d] * P->t.B[d];
         if (c.T[d] > kr) c.T[d] = kr;
@@ -715,7 +717,17 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
       }
       size_t npts = (size_t)c.T[0] + 2 * pc;
       for (int d = 1; d < D; d++) npts *= c.T[d];
-      if (npts * cw * 8 <= 160 * 1024) cands.push_back(c);
+      if (npts * cw * 8 <= 160 * 1024) {
+        cands.push_back(c);
+        // shared-tile variant: every warp takes whole visits, atomic adds
+        if (!P->deterministic)
+          for (int th : {128, 256}) {
+            SpreadCand ca = c;
+            ca.threads = th;
+            ca.atomic = 1;
+            cands.push_back(ca);
+          }
+      }
     }
   };
   if (D == 1) {
@@ -740,6 +752,7 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
     if (rc) continue;
     P->ls.threads = c.threads;
     P->t.padc = c.padc;
+    P->ls.atomic = c.atomic;
     float ms = 0;
     rc = time_launch([&]() {
       return launch_spread(P->a, P->t, P->ls, P->bin_start.as<int>(), samp.as<float2>(),
@@ -756,6 +769,7 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
     if (rc) return rc;
     P->ls.threads = best.threads;
     P->t.padc = best.padc;
+    P->ls.atomic = best.atomic;
   }
   // split size of heavy tiles (sample visits per spread task)
   {
@@ -819,10 +833,23 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
 
 int mirt_interp_plan_config(mirt_interp_plan *P, int32_t *out, int32_t n) {
   if (!P || !out) return fail(MIRT_ERR_ARG, "NULL argument");
-  const int32_t v[16] = {P->t.T[0], P->t.T[1], P->t.T[2], P->ls.threads, P->heavy_first, P->ls.cw,
+  const int32_t v[17] = {P->t.T[0], P->t.T[1], P->t.T[2], P->ls.threads, P->heavy_first, P->ls.cw,
                          P->lg.threads, P->lg.sb, P->lg.grid, P->t.B[0], P->t.B[1], P->t.B[2],
-                         P->split_chunk, P->t.ntask, P->t.padc, P->t.nred};
-  for (int i = 0; i < n && i < 16; i++) out[i] = v[i];
+                         P->split_chunk, P->t.ntask, P->t.padc, P->t.nred, P->ls.atomic};
+  for (int i = 0; i < n && i < 17; i++) out[i] = v[i];
+  return MIRT_OK;
+}
+
+int mirt_interp_plan_set_deterministic(mirt_interp_plan *P, int32_t deterministic) {
+  if (!P) return fail(MIRT_ERR_ARG, "plan is NULL");
+  P->deterministic = deterministic ? 1 : 0;
+  if (deterministic) {
+    P->ls.atomic = 0;
+    if (P->ls.threads > 32 * P->t.T[P->a.g.D - 1]) P->ls.threads = 32;
+  } else {
+    P->ls.atomic = 1;
+    P->ls.threads = 256;
+  }
   return MIRT_OK;
 }
 

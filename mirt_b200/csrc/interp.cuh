@@ -87,6 +87,8 @@ struct Launch {
   int cw;        // coil lanes per sample group
   int sb;        // samples per staged batch (even)
   int grid;      // CTAs for the persistent gather (0: size from occupancy)
+  int atomic;    // spread: warps share the tile and add with shared-memory
+                 // atomics (not bitwise reproducible); 0: one owner per point
 };
 
 // Compute the sort key of every sample: slice * nbins + bin of its first tap.

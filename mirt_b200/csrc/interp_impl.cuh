@@ -116,6 +116,29 @@ __device__ __forceinline__ float2 cw_fma(float2 w, float2 v, float2 vs, float2 A
   return A;
 }
 
+// *p += (wr, wr) v2 + (wi, -wi) v2s: a read-modify-write by the point's one
+// owner, or (ATOMIC) two shared-memory atomic adds when warps share the tile
+template <bool ATOMIC, bool REAL>
+__device__ __forceinline__ void acc_pair(float2 *p, float2 wr, float2 wi, float2 v2, float2 v2s) {
+  if constexpr (ATOMIC) {
+    float2 c = __fmul2_rn(wr, v2);
+    if (!REAL) c = __ffma2_rn(wi, v2s, c);
+    atomicAdd(&p->x, c.x);
+    atomicAdd(&p->y, c.y);
+  } else {
+    float2 A = *p;
+    A = __ffma2_rn(wr, v2, A);
+    if (!REAL) A = __ffma2_rn(wi, v2s, A);
+    *p = A;
+  }
+}
+
+// *p += conj(w) v (vs = (vi, vr))
+template <bool ATOMIC, bool REAL>
+__device__ __forceinline__ void acc_cw(float2 *p, float2 w, float2 v, float2 vs) {
+  acc_pair<ATOMIC, REAL>(p, make_float2(w.x, w.x), make_float2(w.y, -w.y), v, vs);
+}
+
 // ------------------------------------------------------------------------
 // forward gather
 // ------------------------------------------------------------------------
@@ -321,7 +344,7 @@ __host__ __device__ __forceinline__ int tap_local(int k0w, int j, int K, int lo_
 
 // One grid row of the tile for one sample: acc[l1][lane coil] += conj(w1) v2
 // for the lane's taps.  Fast path when all J1 taps lie inside the tile.
-template <int CW, int JT, bool REAL>
+template <int CW, int JT, bool REAL, bool ATOMIC>
 __device__ __forceinline__ void spread_row(float2 *row, const float2 *Ws, int J1, bool fast1,
                                            int l10, unsigned m1, int k10, int K1, int lo1,
                                            int ls, float2 v2) {
@@ -330,9 +353,7 @@ __device__ __forceinline__ void spread_row(float2 *row, const float2 *Ws, int J1
   if (fast1) {
     for (int j1 = (ls - l10) & (SUB - 1); j1 < J1; j1 += SUB) {
       float2 *p = row + (l10 + j1) * CW;
-      float2 A = *p;
-      A = cw_fma<REAL>(__ldg(Ws + j1), v2, v2s, A);
-      *p = A;
+      acc_cw<ATOMIC, REAL>(p, __ldg(Ws + j1), v2, v2s);
     }
   } else {
     unsigned mm = m1;
@@ -340,14 +361,12 @@ __device__ __forceinline__ void spread_row(float2 *row, const float2 *Ws, int J1
       const int j1 = __ffs(mm) - 1;
       mm &= mm - 1;
       float2 *p = row + tap_local(k10, j1, K1, lo1) * CW;
-      float2 A = *p;
-      A = cw_fma<REAL>(__ldg(Ws + j1), v2, v2s, A);
-      *p = A;
+      acc_cw<ATOMIC, REAL>(p, __ldg(Ws + j1), v2, v2s);
     }
   }
 }
 
-template <int D, int CW, int JT, bool REAL>
+template <int D, int CW, int JT, bool REAL, bool ATOMIC>
 __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t,
                                                      const int *__restrict__ bin_start,
                                                      const float2 *__restrict__ fm,
@@ -392,9 +411,12 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t,
   const int ls = lane / CW;   // column class
   const int lc = lane % CW;   // coil within the chunk
   constexpr int BD = D - 1;   // band dimension
-  const int per = (t.T[BD] + nwarp - 1) / nwarp;
-  const int band_lo = min(warp * per, ext[BD]);
-  const int band_hi = min(band_lo + per, ext[BD]);
+  // deterministic: warp w owns a band of the slowest tiled dimension and walks
+  // every visit; ATOMIC: every warp owns the whole tile and takes every
+  // nwarp-th visit
+  const int per = ATOMIC ? t.T[BD] : (t.T[BD] + nwarp - 1) / nwarp;
+  const int band_lo = ATOMIC ? 0 : min(warp * per, ext[BD]);
+  const int band_hi = ATOMIC ? ext[BD] : min(band_lo + per, ext[BD]);
   for (int e = threadIdx.x; e < nsm * CW; e += blockDim.x) acc[e] = make_float2(0.f, 0.f);
   __syncthreads();
 
@@ -408,7 +430,7 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t,
   const int jb0 = D == 1 ? 0 : (D == 2 ? Jd[0] : Jd[0] + Jd[1]);  // first tap of dim BD
   const bool lane_on = c0 + lc < C;
 
-  long long vbase = 0;
+  long long vbase = 0, vcta = 0;
   for (int si = 0; si < nsrc_tot && vbase < vr.y && band_lo < band_hi; si++) {
     const int kr = si & 1, rest = si >> 1;
     const int rs = kr ? run.z : run.x, rl = kr ? run.w : run.y;
@@ -423,15 +445,23 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t,
     const long long end = b0 + min(b1 - b0, (long long)vr.y - vbase);
     vbase += b1 - b0;
     if (beg >= end) continue;
+    // ATOMIC: warp w takes the task's visits w, w + nwarp, ...
+    const int stp = ATOMIC ? nwarp : 1;
+    long long first = beg;
+    if (ATOMIC) {
+      first = beg + ((warp - (int)(vcta % nwarp)) % nwarp + nwarp) % nwarp;
+      vcta += end - beg;
+    }
+    if (first >= end) continue;
     // one position ahead: its first taps and sample index are in flight
-    int4 kn = a.K0[beg];
-    int mn = a.perm ? a.perm[beg] : (int)beg;
-    for (long long pos = beg; pos < end; pos++) {
+    int4 kn = a.K0[first];
+    int mn = a.perm ? a.perm[first] : (int)first;
+    for (long long pos = first; pos < end; pos += stp) {
       const int4 k = kn;
       const int m = mn;
-      if (pos + 1 < end) {
-        kn = a.K0[pos + 1];
-        mn = a.perm ? a.perm[pos + 1] : (int)(pos + 1);
+      if (pos + stp < end) {
+        kn = a.K0[pos + stp];
+        mn = a.perm ? a.perm[pos + stp] : (int)(pos + stp);
       }
       const int kb = D == 1 ? k.x : (D == 2 ? k.y : k.z);
       const int l10 = k.x - lo[0];
@@ -481,33 +511,23 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t,
               if constexpr (SUB == 1) {
 #pragma unroll
                 for (int j1 = 0; j1 < JT; j1++) {
-                  float2 A = p[j1 * CW];
-                  A = __ffma2_rn(wr[j1], v2, A);
-                  if (!REAL) A = __ffma2_rn(wi[j1], v2s, A);
-                  p[j1 * CW] = A;
+                  acc_pair<ATOMIC, REAL>(p + j1 * CW, wr[j1], wi[j1], v2, v2s);
                 }
               } else {
                 for (int j1 = j1p; j1 < JT; j1 += SUB) {
-                  float2 A = p[j1 * CW];
-                  A = cw_fma<REAL>(__ldg(Ws + j1), v2, v2s, A);
-                  p[j1 * CW] = A;
+                  acc_cw<ATOMIC, REAL>(p + j1 * CW, __ldg(Ws + j1), v2, v2s);
                 }
               }
             } else if constexpr (SUB == 1) {
 #pragma unroll
               for (int j1 = 0; j1 < JT; j1++) {
                 if (j1 >= ja1 && j1 < jb1) {
-                  float2 A = p[j1 * CW];
-                  A = __ffma2_rn(wr[j1], v2, A);
-                  if (!REAL) A = __ffma2_rn(wi[j1], v2s, A);
-                  p[j1 * CW] = A;
+                  acc_pair<ATOMIC, REAL>(p + j1 * CW, wr[j1], wi[j1], v2, v2s);
                 }
               }
             } else {
               for (int j1 = j1s; j1 < jb1; j1 += SUB) {
-                float2 A = p[j1 * CW];
-                A = cw_fma<REAL>(__ldg(Ws + j1), v2, v2s, A);
-                p[j1 * CW] = A;
+                acc_cw<ATOMIC, REAL>(p + j1 * CW, __ldg(Ws + j1), v2, v2s);
               }
             }
           };
@@ -540,7 +560,7 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t,
       }
       if constexpr (D == 1) {
         const unsigned m1 = tap_mask<SUB>(k.x, Jd[0], g.K[0], lo[0], band_lo, band_hi, ls);
-        spread_row<CW, JT, REAL>(acc + lc, Ws, Jd[0], false, l10, m1, k.x, g.K[0], lo[0], ls, f);
+        spread_row<CW, JT, REAL, ATOMIC>(acc + lc, Ws, Jd[0], false, l10, m1, k.x, g.K[0], lo[0], ls, f);
       } else {
         // lane's columns: fast when the J1 taps do not leave the tile
         const bool fast1 = l10 >= 0 && l10 + Jd[0] <= ext[0];
@@ -569,10 +589,7 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t,
                 float2 *p = base + (size_t)l2 * RS * CW;
 #pragma unroll
                 for (int j1 = 0; j1 < JT; j1++) {
-                  float2 A = p[j1 * CW];
-                  A = __ffma2_rn(wr[j1], v2, A);
-                  if (!REAL) A = __ffma2_rn(wi[j1], v2s, A);
-                  p[j1 * CW] = A;
+                  acc_pair<ATOMIC, REAL>(p + j1 * CW, wr[j1], wi[j1], v2, v2s);
                 }
               }
               continue;
@@ -584,7 +601,7 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t,
             m2 &= m2 - 1;
             const int l2 = tap_local(k.y, j2, g.K[1], lo[1]);
             const float2 v2 = cw_mul<REAL>(__ldg(Ws + Jd[0] + j2), f);
-            spread_row<CW, JT, REAL>(acc + ((size_t)l2 * RS + pc) * CW + lc, Ws, Jd[0], fast1, l10,
+            spread_row<CW, JT, REAL, ATOMIC>(acc + ((size_t)l2 * RS + pc) * CW + lc, Ws, Jd[0], fast1, l10,
                                      m1, k.x, g.K[0], lo[0], ls, v2);
           }
         } else {
@@ -602,7 +619,7 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t,
               m2 &= m2 - 1;
               const int l2 = tap_local(k.y, j2, g.K[1], lo[1]);
               const float2 v2 = cw_mul<REAL>(__ldg(Ws + Jd[0] + j2), v3);
-              spread_row<CW, JT, REAL>(acc + (((size_t)l3 * T1 + l2) * RS + pc) * CW + lc, Ws,
+              spread_row<CW, JT, REAL, ATOMIC>(acc + (((size_t)l3 * T1 + l2) * RS + pc) * CW + lc, Ws,
                                        Jd[0], fast1, l10, m1, k.x, g.K[0], lo[0], ls, v2);
             }
           }
@@ -731,7 +748,7 @@ cudaError_t run(Req &r) {
   } else {
     const Tiling &t = *r.t;
     const size_t sm = spread_smem_bytes(a, t, l);
-    auto kern = spread_kernel<D, CW, JT, REAL>;
+    auto kern = l.atomic ? spread_kernel<D, CW, JT, REAL, true> : spread_kernel<D, CW, JT, REAL, false>;
     cudaError_t e =
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;

@@ -69,6 +69,7 @@ struct mirt_interp_plan {
   mirt::DMem wtap_g, k0tap_g, perm_g, phase_g;
   int split_chunk = 1024;  // sample visits per spread task before a tile is split
   int heavy_first = 1;     // spread task order: 1 heaviest first, 0 grid order
+  int deterministic = 1;   // 0: the spread may use shared-memory atomics
   std::vector<long long> moff_host;
 };
 

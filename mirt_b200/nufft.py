@@ -66,12 +66,13 @@ def minmax_kb_scale(N: int, J: int, K: int) -> np.ndarray:
 
 
 def _plan_config(lib, handle) -> dict:
-    v = (C.c_int32 * 16)()
-    check(lib.mirt_interp_plan_config(handle, v, 16))
+    v = (C.c_int32 * 17)()
+    check(lib.mirt_interp_plan_config(handle, v, 17))
     return {"spread_tile": [v[0], v[1], v[2]], "spread_threads": v[3], "spread_heavy_first": v[4],
             "coil_lanes": v[5], "gather_threads": v[6],
             "gather_ctas": v[8], "sort_bin": [v[9], v[10], v[11]], "split_chunk": v[12],
-            "spread_tasks": v[13], "spread_padc": v[14], "spread_reductions": v[15]}
+            "spread_tasks": v[13], "spread_padc": v[14], "spread_reductions": v[15],
+            "spread_atomic": v[16]}
 
 
 class InterpPlan:
@@ -150,6 +151,12 @@ class InterpPlan:
 
     def config(self):
         return _plan_config(self.lib, self.handle)
+
+    def set_deterministic(self, deterministic=True):
+        """False: the spread may add with shared-memory atomics (faster, not
+        bitwise reproducible); the autotuner then also tries that variant."""
+        check(self.lib.mirt_interp_plan_set_deterministic(self.handle, int(bool(deterministic))))
+        return self.config()
 
     def set_spread(self, tile, threads=32, padc=0, stream=None):
         """Fix the spread tiling (tile extents per dimension, CTA size, spare
@@ -230,6 +237,12 @@ class NufftPlan:
     def autotune(self, stream=None):
         """Pick the fastest gather / spread launch shapes for this trajectory."""
         check(self.lib.mirt_nufft_autotune(self.handle, _stream_ptr(stream)))
+        return self.config()
+
+    def set_deterministic(self, deterministic=True):
+        """See InterpPlan.set_deterministic."""
+        check(self.lib.mirt_interp_plan_set_deterministic(
+            self.lib.mirt_nufft_interp_plan(self.handle), int(bool(deterministic))))
         return self.config()
 
     def capture(self, x=None, X=None, xa=None):

@@ -257,3 +257,56 @@ def test_spread_tilings_3d_padded():
             got = np.transpose(got, (2, 1, 0, 3)).reshape(-1, C, order="F")
             assert rel_l2(got, ref) <= ADJ_TOL, (tile, threads, padc)
     plan.close()
+
+
+@pytest.mark.parametrize("C", [1, 8, 32])
+def test_atomic_spread_matches_oracle(C):
+    """Non-deterministic mode: all warps of a tile take whole samples and add
+    with shared-memory atomics; the result is the oracle's adjoint to the same
+    tolerance, for several tilings, and the autotuner may pick it."""
+    import torch
+    rng = np.random.default_rng(91 + C)
+    K, J, L = [96, 80], [6, 6], [1024, 1024]
+    h = [mb.minmax_kb_table(48, 6, 96, 1024), mb.minmax_kb_table(40, 6, 80, 1024)]
+    counts = [2000, 1500]
+    moff = np.concatenate([[0], np.cumsum(counts)])
+    tm = np.concatenate([rng.uniform(-100, 100, (c, 2)) for c in counts])
+    plan = mb.InterpPlan(K, J, L, h, tm, C, slice_moff=moff)
+    cfg = plan.set_deterministic(False)
+    assert cfg["spread_atomic"] == 1
+    fm = rng.standard_normal((len(tm), C)) + 1j * rng.standard_normal((len(tm), C))
+    fm_d = torch.from_numpy(fm.astype(np.complex64)).cuda()
+    refs = [oracle.interp_adj(fm[moff[s]:moff[s + 1]], h, J, L, tm[moff[s]:moff[s + 1]], K, 0,
+                              impl=ref_impl()) for s in range(2)]
+
+    def check():
+        out = plan.adjoint(fm_d).cpu().numpy()
+        for s in range(2):
+            got = np.transpose(out[s], (1, 0, 2)).reshape(-1, C, order="F")
+            assert rel_l2(got, refs[s]) <= ADJ_TOL
+
+    check()
+    for tile, threads in [((8, 8), 128), ((16, 16), 256), ((32, 8), 256)]:
+        plan.set_spread(tile, threads, 0)
+        assert plan.config()["spread_atomic"] == 1
+        check()
+    plan.autotune()
+    check()
+    plan.close()
+
+
+def test_atomic_spread_3d():
+    import torch
+    rng = np.random.default_rng(92)
+    K, J, L = [24, 20, 16], [6, 6, 6], [256, 256, 256]
+    h = [mb.minmax_kb_table(k // 2, 6, k, 256) for k in K]
+    tm = rng.uniform(-40, 40, (1500, 3))
+    C = 8
+    plan = mb.InterpPlan(K, J, L, h, tm, C)
+    plan.set_deterministic(False)
+    fm = rng.standard_normal((len(tm), C)) + 1j * rng.standard_normal((len(tm), C))
+    got = plan.adjoint(torch.from_numpy(fm.astype(np.complex64)).cuda()).cpu().numpy()[0]
+    got = np.transpose(got, (2, 1, 0, 3)).reshape(-1, C, order="F")
+    ref = oracle.interp_adj(fm, h, J, L, tm, K, 0, impl=ref_impl())
+    assert rel_l2(got, ref) <= ADJ_TOL
+    plan.close()
