@@ -8,7 +8,8 @@ TEST INFRASTRUCTURE ONLY (the checker of mirt_sense_*).
   (penalty/penalty_offsets.m), first-order differences, 'tight' edges
   (penalty/Rweights.m:290-300: only pairs with both pixels inside the image)
   and weights beta / |offset| (distance_power 1);
-* qpwls_pcg1 (wls/qpwls_pcg1.m:94-189) with precon = 1.
+* qpwls_pcg1 (wls/qpwls_pcg1.m:94-189), with precon = 1 or the circulant
+  preconditioner of the device solver.
 Images are numpy [N2, N1] (n1 fastest, the device layout); data [M, C].
 """
 from __future__ import annotations
@@ -72,9 +73,34 @@ class Sense64:
         return out
 
 
-def qpwls_pcg1(x, A: Sense64, W, yi, niter):
-    """Iterates of wls/qpwls_pcg1.m:94-189 (precon = 1) in FP64; returns the
-    list [x_0, x_1, ..., x_niter]."""
+def circulant_precon(A: Sense64):
+    """The circulant preconditioner of the device solver, in FP64: spectrum
+    1 / max(lam Re H1 + r, 1e-3 max(lam Re H1)) on the 2N grid, H1 the FFT of
+    the Toeplitz embedding of G'G (oracle.toeplitz_ref), lam the mean coil
+    power, r the spectrum of the Reg1 penalty; applied as crop(ifft2(Hp
+    fft2(pad(x)))).  Returns a function of an image [N2, N1]."""
+    from oracle import toeplitz_ref as tr
+    st = A.st
+    N = A.N
+    H = tr.gram_kernel(st["om"], (N, N), st["Kd"], st["Jd"], st["Ld"]).real    # [q1, q2]
+    lam = np.mean(np.sum(np.abs(A.sens) ** 2, axis=-1))
+    a = np.pi * np.arange(2 * N) / N
+    A1, A2 = np.meshgrid(a, a, indexing="ij")
+    r = A.beta * ((2 - 2 * np.cos(A1)) + (2 - 2 * np.cos(A2))
+                  + ((2 - 2 * np.cos(A1 + A2)) + (2 - 2 * np.cos(A2 - A1))) / np.sqrt(2))
+    v = lam * H + r
+    Hp = 1.0 / np.maximum(v, 1e-3 * np.max(lam * H))
+
+    def apply(g):
+        X = np.zeros((2 * N, 2 * N), np.complex128)
+        X[:N, :N] = g.T                                       # [n1, n2]
+        return np.fft.ifft2(Hp * np.fft.fft2(X))[:N, :N].T
+    return apply
+
+
+def qpwls_pcg1(x, A: Sense64, W, yi, niter, precon=None):
+    """Iterates of wls/qpwls_pcg1.m:94-189 in FP64 (precon: a function of the
+    gradient image, or None for 1); returns the list [x_0, x_1, ..., x_niter]."""
     x = np.asarray(x, np.complex128).copy()
     W = 1.0 if W is None else np.asarray(W, np.float64)[:, None]
     Ax = A.forward(x)
@@ -84,12 +110,13 @@ def qpwls_pcg1(x, A: Sense64, W, yi, niter):
     ddir = None
     for it in range(1, niter + 1):
         ngrad = A.adjoint(W * (yi - Ax)) - Rx
-        newinprod = np.real(np.vdot(ngrad, ngrad))
+        pregrad = ngrad if precon is None else precon(ngrad)
+        newinprod = np.real(np.vdot(ngrad, pregrad))
         if it == 1:
-            ddir = ngrad
+            ddir = pregrad
         else:
             gamma = 0.0 if oldinprod == 0 else newinprod / oldinprod
-            ddir = ngrad + gamma * ddir
+            ddir = pregrad + gamma * ddir
         oldinprod = newinprod
         Adir = A.forward(ddir)
         Rdir = A.reg(ddir)

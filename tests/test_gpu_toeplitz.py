@@ -87,3 +87,30 @@ def test_gram_form_solution_matches_nufft_form():
     A.pcg(x2, y, 150, precon=True, gram=True)
     for s in range(A.S):
         assert rel_l2(x2[s].cpu().numpy(), x1[s].cpu().numpy()) <= 1e-3
+
+
+def test_c5_size_problem_reaches_fp64_solution():
+    """One problem at a C5 size (N = 128, 8 coils, golden-angle radial at
+    R = 4, 30 dB noise, beta = 2^-8 trace scale): the device solver (FP32
+    operators, FP64 inner products, circulant preconditioner) lands within
+    1e-4 of the converged FP64 solution (the FP64 oracle with the same
+    preconditioner), one order below the 1e-3 of the solver benchmark."""
+    import torch
+    from oracle.sense_ref import circulant_precon
+    rng = np.random.default_rng(21)
+    N, K, C = 128, 256, 8
+    om = wl.ga_radial(int(np.ceil(np.pi * N / 8)), 2 * N, start=0.4)
+    sens = wl.coil_maps((N, N), C, rng).transpose(1, 0, 2)
+    beta = 2.0 ** -8 * len(om) * np.mean(np.sum(np.abs(sens) ** 2, -1))
+    R = Sense64(om, N, K, sens, beta)
+    xt = wl.ellipses(N, 10, rng).T
+    y = R.forward(xt)
+    noise = rng.standard_normal(y.shape) + 1j * rng.standard_normal(y.shape)
+    y = y + noise * np.linalg.norm(y) / np.linalg.norm(noise) * 10 ** (-30 / 20)
+    ref = qpwls_pcg1(np.zeros((N, N), complex), R, None, y, 120, precon=circulant_precon(R))[-1]
+    G = mb.NufftPlan(om, (N, N), (6, 6), (K, K), n_shift=(N / 2, N / 2), Ld=1024, ncol=C)
+    sens_d = torch.from_numpy(sens[None].astype(np.complex64)).cuda()
+    A = ms.SenseSystem(G, sens_d, [beta]).toeplitz()
+    x = torch.zeros(A.image_shape, dtype=torch.complex64, device="cuda")
+    A.pcg(x, torch.from_numpy(y.astype(np.complex64)).cuda(), 120, precon=True)
+    assert rel_l2(x[0].cpu().numpy(), ref) <= 1e-4
