@@ -193,11 +193,11 @@ int mirt_interp_plan_adjoint(mirt_interp_plan *plan, const void *fm, void *ck, v
  * bitwise deterministic for any choice. */
 int mirt_interp_plan_autotune(mirt_interp_plan *plan, void *stream);
 
-/* Current launch configuration: up to 17 values
+/* Current launch configuration: up to 18 values
  * {T1, T2, T3, spread threads, spread heavy-first order, coil lanes,
  *  gather threads, (unused), gather CTAs, B1, B2, B3, split chunk,
  *  spread tasks, spare tile columns, partial-tile reductions,
- *  spread shared-tile atomics}. */
+ *  spread shared-tile atomics, ownership spread}. */
 int mirt_interp_plan_config(mirt_interp_plan *plan, int32_t *out, int32_t n);
 
 /* Adjoint accumulation order.  deterministic = 1 (the default): every
@@ -208,6 +208,15 @@ int mirt_interp_plan_config(mirt_interp_plan *plan, int32_t *out, int32_t n);
  * arithmetic, summed in a run-dependent order); the autotuner then also
  * tries this variant.  No reference counterpart (the reference is serial). */
 int mirt_interp_plan_set_deterministic(mirt_interp_plan *plan, int32_t deterministic);
+
+/* Ownership spread (2D, J = 6): the tile holding a sample's first tap adds
+ * all 36 taps into a shared tile padded by J - 1 points; tiles run in four
+ * launches by the parities of their indices (no two padded tiles of one
+ * launch overlap) and add their padded tiles into the cleared grid.
+ * Deterministic.  Needs tiles of >= 5 points and an even number of tiles
+ * (the last >= 5 points) per dimension; else MIRT_ERR_ARG.  The autotuner
+ * tries it where it applies.  No reference counterpart. */
+int mirt_interp_plan_set_ownership(mirt_interp_plan *plan, int32_t own, void *stream);
 
 /* Fix the spread's tiling instead of autotuning it: tile extents T[0..D-1]
  * (multiples of the sort bins B of mirt_interp_plan_config, at most the grid

@@ -142,6 +142,21 @@ namespace {
 // tile accumulator is sized to keep several CTAs resident per SM).
 // The spread's range path serves wrapping taps when no tile can meet a
 // sample's taps both before and after their periodic wrap.
+// The ownership spread needs: 2D, J = 6, one-point bins, tiles of at least
+// J - 1 points, an even number (>= 2) of tiles per dimension and a last tile
+// of at least J - 1 points, so that a padded tile reaches only the next tile
+// and tiles of one colour (index parities) never overlap, wrap included.
+int own_ok(const InterpArgs &a, const Tiling &t) {
+  if (a.g.D != 2) return 0;
+  for (int d = 0; d < 2; d++) {
+    const int K = a.g.K[d], T = t.T[d];
+    if (a.g.J[d] != 6 || t.B[d] != 1 || T < 5 || K < T + 5) return 0;
+    const int nb = (K + T - 1) / T;
+    if (nb < 2 || nb % 2 || K - (nb - 1) * T < 5) return 0;
+  }
+  return 1;
+}
+
 int wrap_ok(const InterpArgs &a, const Tiling &t) {
   for (int d = 0; d < a.g.D; d++)
     if (a.g.K[d] < t.T[d] + a.g.J[d]) return 0;
@@ -187,6 +202,7 @@ void choose_config(mirt_interp_plan *P) {
   ls.atomic = 0;
   // no spare tile columns by default; the autotuner also tries J1 - 1
   t.padc = 0;
+  t.own = 0;
   t.nbins = 1;
   t.ntiles = 1;
   for (int d = 0; d < MIRT_DMAX; d++) {
@@ -349,8 +365,9 @@ int build_tasks(mirt_interp_plan *P, cudaStream_t st) {
   const long long chunk = std::max(32, P->split_chunk);
   struct Task {
     long long work;
-    int tile, v0, v1, slot;
+    int tile, v0, v1, slot, color;
   };
+  std::vector<int> red_color;
   std::vector<Task> tasks;
   std::vector<int4> red;
   int nslot = 0;
@@ -363,6 +380,18 @@ int build_tasks(mirt_interp_plan *P, cudaStream_t st) {
       r /= t.nb[d];
     }
     long long w = 0;
+    int color = 0;
+    if (t.own) {
+      // the tile's own samples: first tap inside the tile, one range per row
+      const int lo0 = b[0] * t.T[0], lo1 = b[1] * t.T[1];
+      const int ext0 = std::min(t.T[0], P->a.g.K[0] - lo0);
+      const int ext1 = std::min(t.T[1], P->a.g.K[1] - lo1);
+      for (int i1 = 0; i1 < ext1; i1++) {
+        const long long key = slice * t.nbins + (long long)(lo1 + i1) * t.nbin[0] + lo0;
+        w += bs[key + ext0] - bs[key];
+      }
+      color = (b[0] & 1) | ((b[1] & 1) << 1);
+    } else {
     const int n1 = D > 1 ? nsrc[1][b[1]] : 1, n2 = D > 2 ? nsrc[2][b[2]] : 1;
     const int4 rr = run0[b[0]];
     for (int i2 = 0; i2 < n2; i2++)
@@ -376,15 +405,17 @@ int build_tasks(mirt_interp_plan *P, cudaStream_t st) {
           const long long bin = slice * t.nbins + row + rs;
           w += bs[bin + rl] - bs[bin];
         }
+    }
     if (w >= (1ll << 31)) return fail(MIRT_ERR_ARG, "too many samples in one tile");
     if (w <= chunk) {
-      tasks.push_back({w, (int)task, 0, (int)w, -1});
+      tasks.push_back({w, (int)task, 0, (int)w, -1, color});
     } else {
       const int np = (int)((w + chunk - 1) / chunk);
       red.push_back(make_int4((int)task, nslot, np, 0));
+      red_color.push_back(color);
       for (int i = 0; i < np; i++) {
         const long long v0 = i * chunk, v1 = std::min(w, v0 + chunk);
-        tasks.push_back({v1 - v0, (int)task, (int)v0, (int)v1, nslot + i});
+        tasks.push_back({v1 - v0, (int)task, (int)v0, (int)v1, nslot + i, color});
       }
       nslot += np;
     }
@@ -392,6 +423,25 @@ int build_tasks(mirt_interp_plan *P, cudaStream_t st) {
   if (P->heavy_first)
     std::stable_sort(tasks.begin(), tasks.end(),
                      [](const Task &x, const Task &y) { return x.work > y.work; });
+  for (int c = 0; c < 9; c++) t.color_beg[c] = t.red_beg[c] = 0;
+  if (t.own) {
+    // colour-major (each colour one launch), the order above within a colour
+    std::stable_sort(tasks.begin(), tasks.end(),
+                     [](const Task &x, const Task &y) { return x.color < y.color; });
+    std::vector<int> idx(red.size());
+    for (size_t i = 0; i < idx.size(); i++) idx[i] = (int)i;
+    std::stable_sort(idx.begin(), idx.end(),
+                     [&](int x, int y) { return red_color[x] < red_color[y]; });
+    std::vector<int4> red2(red.size());
+    for (size_t i = 0; i < idx.size(); i++) red2[i] = red[idx[i]];
+    red.swap(red2);
+    for (int c = 0; c < 4; c++) {
+      t.color_beg[c + 1] = t.color_beg[c];
+      for (const Task &k : tasks) t.color_beg[c + 1] += k.color == c;
+      t.red_beg[c + 1] = t.red_beg[c];
+      for (int rc : red_color) t.red_beg[c + 1] += rc == c;
+    }
+  }
   const size_t nt = tasks.size();
   std::vector<int> tt(nt), ts(nt);
   std::vector<int2> tr(nt);
@@ -414,6 +464,7 @@ int build_tasks(mirt_interp_plan *P, cudaStream_t st) {
                        st));
   size_t npts = 1;
   for (int d = 0; d < D; d++) npts *= t.T[d];
+  if (t.own) npts = (size_t)(t.T[0] + 5) * (t.T[1] + 5);
   const int cw = P->ls.cw;
   const size_t nchunk = (P->a.C + cw - 1) / cw;
   const size_t sbytes = (size_t)nslot * nchunk * npts * cw * sizeof(float2);
@@ -544,6 +595,7 @@ int set_spread_tiles(mirt_interp_plan *P, const int *T, cudaStream_t st) {
     t.ntiles *= t.nb[d];
   }
   t.wrap_ok = wrap_ok(P->a, t);
+  if (t.own && !own_ok(P->a, t)) t.own = 0;
   int rc = build_sources(P, st);
   if (rc) return rc;
   return build_tasks(P, st);
@@ -551,7 +603,7 @@ int set_spread_tiles(mirt_interp_plan *P, const int *T, cudaStream_t st) {
 
 struct SpreadCand {
   int T[MIRT_DMAX];
-  int threads, padc, atomic;
+  int threads, padc, atomic, own;
 };
 
 // spare columns the J = 6 row update can use (0 elsewhere)
@@ -709,7 +761,7 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
     const int npc = pmax ? 2 : 1;
     for (int ip = 0; ip < npc; ip++) {
       const int pc = ip ? pmax : 0;
-      SpreadCand c{{t0, t1, t2}, threads, pc, 0};
+      SpreadCand c{{t0, t1, t2}, threads, pc, 0, 0};
       for (int d = 0; d < D; d++) {
         const int kr = (a.g.K[d] + P->t.B[d] - 1) / P->t.B[d] * P->t.B[d];
         if (c.T[d] > kr) c.T[d] = kr;
@@ -728,6 +780,16 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
             cands.push_back(ca);
           }
       }
+    }
+    // ownership spread (2D, J = 6): padded tile, warps on bands of its rows
+    if (D == 2 && pmax) {
+      Tiling tt = P->t;
+      tt.T[0] = t0;
+      tt.T[1] = t1;
+      const size_t pts = (size_t)(t0 + 5) * (t1 + 5);
+      if (own_ok(a, tt) && pts * cw * 8 <= 160 * 1024 && threads == 32)
+        for (int th = 32; th <= 256 && th / 32 <= t1 + 5; th *= 2)
+          cands.push_back(SpreadCand{{t0, t1, 1}, th, 0, 0, 1});
     }
   };
   if (D == 1) {
@@ -748,6 +810,7 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
   SpreadCand best{};
   float best_ms = 1e30f;
   for (const SpreadCand &c : cands) {
+    P->t.own = c.own;
     int rc = set_spread_tiles(P, c.T, st);
     if (rc) continue;
     P->ls.threads = c.threads;
@@ -765,6 +828,7 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
     }
   }
   if (best_ms < 1e30f) {
+    P->t.own = best.own;
     int rc = set_spread_tiles(P, best.T, st);
     if (rc) return rc;
     P->ls.threads = best.threads;
@@ -833,10 +897,25 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
 
 int mirt_interp_plan_config(mirt_interp_plan *P, int32_t *out, int32_t n) {
   if (!P || !out) return fail(MIRT_ERR_ARG, "NULL argument");
-  const int32_t v[17] = {P->t.T[0], P->t.T[1], P->t.T[2], P->ls.threads, P->heavy_first, P->ls.cw,
+  const int32_t v[18] = {P->t.T[0], P->t.T[1], P->t.T[2], P->ls.threads, P->heavy_first, P->ls.cw,
                          P->lg.threads, P->lg.sb, P->lg.grid, P->t.B[0], P->t.B[1], P->t.B[2],
-                         P->split_chunk, P->t.ntask, P->t.padc, P->t.nred, P->ls.atomic};
-  for (int i = 0; i < n && i < 17; i++) out[i] = v[i];
+                         P->split_chunk, P->t.ntask, P->t.padc, P->t.nred, P->ls.atomic,
+                         P->t.own};
+  for (int i = 0; i < n && i < 18; i++) out[i] = v[i];
+  return MIRT_OK;
+}
+
+int mirt_interp_plan_set_ownership(mirt_interp_plan *P, int32_t own, void *stream) {
+  if (!P) return fail(MIRT_ERR_ARG, "plan is NULL");
+  if (own && !own_ok(P->a, P->t))
+    return fail(MIRT_ERR_ARG, "ownership spread needs 2D, J = 6, tiles of >= 5 points and an "
+                              "even number of tiles (last one >= 5 points) per dimension");
+  P->t.own = own ? 1 : 0;
+  if (own) P->ls.atomic = 0;
+  int T[MIRT_DMAX] = {P->t.T[0], P->t.T[1], P->t.T[2]};
+  int rc = set_spread_tiles(P, T, as_stream(stream));
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(as_stream(stream)));
   return MIRT_OK;
 }
 

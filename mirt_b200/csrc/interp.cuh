@@ -46,6 +46,15 @@ struct Tiling {
   int T[MIRT_DMAX];      // spread tile extent per dimension (multiple of B)
   int wrap_ok;           // K[d] >= T[d] + J[d] in every dimension: the spread's
                          // range path also serves samples whose taps wrap
+  // Ownership spread (2D, J = 6): the tile holding a sample's wrapped first
+  // tap owns it and accumulates all its taps in a shared tile padded by J - 1
+  // points; tiles are processed by colour (tile index parities), one launch
+  // per colour, adding their padded tiles into the cleared grid.  Tasks are
+  // sorted by colour: colour c is tasks [color_beg[c], color_beg[c+1]) and
+  // reductions [red_beg[c], red_beg[c+1]).
+  int own;
+  int color_beg[9];
+  int red_beg[9];
   int padc;              // spread: spare columns on each side of a tile row in
                          // shared memory (0, or J1 - 1 so that every column
                          // tap of a visiting sample has a slot and the row

@@ -700,6 +700,176 @@ __global__ void __launch_bounds__(256) spread_reduce_kernel(InterpArgs a, Tiling
 }
 
 // ------------------------------------------------------------------------
+// ownership spread (2D, J = 6)
+// ------------------------------------------------------------------------
+// A CTA takes the samples whose wrapped first tap lies in its tile (rows of
+// the tile: one contiguous range of the one-point sort each) and adds all 36
+// taps into a shared tile of (T0 + 5) x (T1 + 5) points -- no bounds tests,
+// no wrap tests.  Warps own bands of padded rows (a sample is skipped by the
+// warps whose band its six rows miss).  The padded tile is then added into
+// the grid (periodic wrap) or, for a split heavy tile, written as a partial.
+// Within one launch (one colour) no two padded tiles overlap, so the adds
+// need no atomics; colours run in a fixed order: deterministic.
+template <int CW, bool REAL>
+__global__ void __launch_bounds__(256) spread_own_kernel(InterpArgs a, Tiling t,
+                                                         const int *__restrict__ bin_start,
+                                                         const float2 *__restrict__ fm,
+                                                         float2 *__restrict__ ck, int task0) {
+  constexpr int SUB = 32 / CW, JT = 6;
+  extern __shared__ __align__(16) unsigned char smem[];
+  float2 *acc = reinterpret_cast<float2 *>(smem);
+  const Geom &g = a.g;
+  const int T0 = t.T[0], T1 = t.T[1];
+  const int P0 = T0 + JT - 1, P1 = T1 + JT - 1;
+  const int ti = task0 + blockIdx.x;
+  const int task = t.task_tile[ti];
+  const int2 vr = t.task_range[ti];
+  const int slot = t.task_slot[ti];
+  const int tile = task % t.ntiles, slice = task / t.ntiles;
+  const int bx = tile % t.nb[0], by = tile / t.nb[0];
+  const int lo0 = bx * T0, lo1 = by * T1;
+  const int ext0 = min(T0, g.K[0] - lo0), ext1 = min(T1, g.K[1] - lo1);
+  const int c0 = blockIdx.y * CW;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nwarp = blockDim.x >> 5;
+  const int ls = lane / CW, lc = lane % CW;
+  const int per = (P1 + nwarp - 1) / nwarp;
+  const int band_lo = min(warp * per, P1), band_hi = min(band_lo + per, P1);
+  for (int e = threadIdx.x; e < P0 * P1 * CW; e += blockDim.x) acc[e] = make_float2(0.f, 0.f);
+  __syncthreads();
+  const int C = a.C;
+  const bool lane_on = c0 + lc < C;
+  const int SJ = a.SJ;
+  long long vbase = 0;
+  for (int i1 = 0; i1 < ext1 && vbase < vr.y && band_lo < band_hi; i1++) {
+    const int key = slice * t.nbins + (lo1 + i1) * t.nbin[0] + lo0;
+    const long long b0 = bin_start[key], b1 = bin_start[key + ext0];
+    const long long beg = b0 + max(0ll, (long long)vr.x - vbase);
+    const long long end = b0 + min(b1 - b0, (long long)vr.y - vbase);
+    vbase += b1 - b0;
+    // every sample of this row has l2 = i1: rows l2 .. l2 + 5 of the padded tile
+    const int jab = max(0, band_lo - i1), jbb = min(JT, band_hi - i1);
+    if (beg >= end || jab >= jbb) continue;
+    int4 kn = a.K0[beg];
+    int mn = a.perm ? a.perm[beg] : (int)beg;
+    for (long long pos = beg; pos < end; pos++) {
+      const int4 k = kn;
+      const int m = mn;
+      if (pos + 1 < end) {
+        kn = a.K0[pos + 1];
+        mn = a.perm ? a.perm[pos + 1] : (int)(pos + 1);
+      }
+      const int l1 = k.x - lo0;
+      const float2 *Ws = a.W + pos * SJ;
+      float2 f = make_float2(0.f, 0.f);
+      if (lane_on) {
+        f = __ldg(fm + (long long)m * C + c0 + lc);
+        if (a.phase) f = cmulc(__ldg(a.phase + pos), f);
+      }
+      float2 *base = acc + ((size_t)i1 * P0 + l1) * CW + lc;
+      if constexpr (SUB == 1) {
+        float2 wr[JT], wi[JT];
+#pragma unroll
+        for (int j1 = 0; j1 < JT; j1++) {
+          const float2 w = __ldg(Ws + j1);
+          wr[j1] = make_float2(w.x, w.x);
+          wi[j1] = make_float2(w.y, -w.y);
+        }
+        for (int j2 = jab; j2 < jbb; j2++) {
+          const float2 v2 = cw_mul<REAL>(__ldg(Ws + JT + j2), f);
+          const float2 v2s = make_float2(v2.y, v2.x);
+          float2 *p = base + (size_t)j2 * P0 * CW;
+#pragma unroll
+          for (int j1 = 0; j1 < JT; j1++) {
+            float2 A = p[j1 * CW];
+            A = __ffma2_rn(wr[j1], v2, A);
+            if (!REAL) A = __ffma2_rn(wi[j1], v2s, A);
+            p[j1 * CW] = A;
+          }
+        }
+      } else {
+        // lane class ls takes the padded columns l1 + j1 = ls (mod SUB)
+        const int j1s = (ls - l1) & (SUB - 1);
+        for (int j2 = jab; j2 < jbb; j2++) {
+          const float2 v2 = cw_mul<REAL>(__ldg(Ws + JT + j2), f);
+          const float2 v2s = make_float2(v2.y, v2.x);
+          float2 *p = base + (size_t)j2 * P0 * CW;
+          for (int j1 = j1s; j1 < JT; j1 += SUB) {
+            float2 A = p[j1 * CW];
+            A = cw_fma<REAL>(__ldg(Ws + j1), v2, v2s, A);
+            p[j1 * CW] = A;
+          }
+        }
+      }
+    }
+  }
+  __syncthreads();
+  if (slot >= 0) {
+    float2 *part = t.scratch + ((size_t)slot * gridDim.y + blockIdx.y) * P0 * P1 * CW;
+    for (int e = threadIdx.x; e < P0 * P1 * CW; e += blockDim.x) part[e] = acc[e];
+    return;
+  }
+  float2 *gout = ck + (long long)slice * a.grid_elems;
+  const int q0 = ext0 + JT - 1, q1 = ext1 + JT - 1;
+  for (int e = threadIdx.x; e < q0 * q1 * CW; e += blockDim.x) {
+    const int cc = e % CW, pt = e / CW;
+    const int p0 = pt % q0, p1 = pt / q0;
+    if (c0 + cc >= C) continue;
+    int g0 = lo0 + p0, g1 = lo1 + p1;
+    if (g0 >= g.K[0]) g0 -= g.K[0];
+    if (g1 >= g.K[1]) g1 -= g.K[1];
+    float2 *q = gout + ((long long)g1 * g.K[0] + g0) * C + c0 + cc;
+    const float2 v = acc[((size_t)p1 * P0 + p0) * CW + cc];
+    float2 o = *q;
+    o.x += v.x;
+    o.y += v.y;
+    *q = o;
+  }
+}
+
+// Sum the partial padded tiles of each split tile of one colour, in slot
+// order, into the grid.
+template <int CW>
+__global__ void __launch_bounds__(256) spread_own_reduce_kernel(InterpArgs a, Tiling t,
+                                                                float2 *__restrict__ ck,
+                                                                int red0) {
+  constexpr int JT = 6;
+  const int4 it = t.red[red0 + blockIdx.x];
+  const int task = it.x, first = it.y, nparts = it.z;
+  const int tile = task % t.ntiles, slice = task / t.ntiles;
+  const Geom &g = a.g;
+  const int T0 = t.T[0], T1 = t.T[1];
+  const int P0 = T0 + JT - 1, P1 = T1 + JT - 1;
+  const int lo0 = (tile % t.nb[0]) * T0, lo1 = (tile / t.nb[0]) * T1;
+  const int ext0 = min(T0, g.K[0] - lo0), ext1 = min(T1, g.K[1] - lo1);
+  const int c0 = blockIdx.y * CW;
+  const size_t stride = (size_t)gridDim.y * P0 * P1 * CW;
+  const float2 *part = t.scratch + ((size_t)first * gridDim.y + blockIdx.y) * P0 * P1 * CW;
+  float2 *gout = ck + (long long)slice * a.grid_elems;
+  const int q0 = ext0 + JT - 1, q1 = ext1 + JT - 1;
+  for (int e = threadIdx.x; e < q0 * q1 * CW; e += blockDim.x) {
+    const int cc = e % CW, pt = e / CW;
+    const int p0 = pt % q0, p1 = pt / q0;
+    if (c0 + cc >= a.C) continue;
+    const size_t pe = ((size_t)p1 * P0 + p0) * CW + cc;
+    float2 v = part[pe];
+    for (int p = 1; p < nparts; p++) {
+      const float2 w = part[p * stride + pe];
+      v.x += w.x;
+      v.y += w.y;
+    }
+    int g0 = lo0 + p0, g1 = lo1 + p1;
+    if (g0 >= g.K[0]) g0 -= g.K[0];
+    if (g1 >= g.K[1]) g1 -= g.K[1];
+    float2 *q = gout + ((long long)g1 * g.K[0] + g0) * a.C + c0 + cc;
+    float2 o = *q;
+    o.x += v.x;
+    o.y += v.y;
+    *q = o;
+  }
+}
+
+// ------------------------------------------------------------------------
 // launch dispatch
 // ------------------------------------------------------------------------
 enum What { GATHER = 0, GATHER_GRID = 1, SPREAD = 2 };
@@ -716,6 +886,7 @@ struct Req {
 };
 
 inline size_t spread_smem_bytes(const InterpArgs &a, const Tiling &t, const Launch &l) {
+  if (t.own) return (size_t)(t.T[0] + 5) * (t.T[1] + 5) * l.cw * 8;
   size_t npts = a.g.D > 1 ? t.T[0] + 2 * t.padc : t.T[0];
   for (int d = 1; d < a.g.D; d++) npts *= t.T[d];
   return npts * l.cw * 8;
@@ -748,6 +919,35 @@ cudaError_t run(Req &r) {
   } else {
     const Tiling &t = *r.t;
     const size_t sm = spread_smem_bytes(a, t, l);
+    if constexpr (D == 2 && JT == 6) {
+      if (t.own) {
+        // cleared grid, then one launch (and one reduction) per colour
+        auto kern = spread_own_kernel<CW, REAL>;
+        cudaError_t e =
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        if (e != cudaSuccess) return e;
+        e = cudaMemsetAsync(r.out, 0, (size_t)t.nslice * a.grid_elems * sizeof(float2), r.st);
+        if (e != cudaSuccess) return e;
+        const unsigned nchunk = (unsigned)((a.C + CW - 1) / CW);
+        for (int c = 0; c < 4; c++) {
+          const int n = t.color_beg[c + 1] - t.color_beg[c];
+          if (n > 0) {
+            kern<<<dim3((unsigned)n, nchunk), l.threads, sm, r.st>>>(a, t, r.bin_start, r.in, r.out,
+                                                                    t.color_beg[c]);
+            e = cudaGetLastError();
+            if (e != cudaSuccess) return e;
+          }
+          const int nr = t.red_beg[c + 1] - t.red_beg[c];
+          if (nr > 0) {
+            spread_own_reduce_kernel<CW><<<dim3((unsigned)nr, nchunk), 256, 0, r.st>>>(
+                a, t, r.out, t.red_beg[c]);
+            e = cudaGetLastError();
+            if (e != cudaSuccess) return e;
+          }
+        }
+        return cudaSuccess;
+      }
+    }
     auto kern = l.atomic ? spread_kernel<D, CW, JT, REAL, true> : spread_kernel<D, CW, JT, REAL, false>;
     cudaError_t e =
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);

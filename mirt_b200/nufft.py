@@ -66,13 +66,13 @@ def minmax_kb_scale(N: int, J: int, K: int) -> np.ndarray:
 
 
 def _plan_config(lib, handle) -> dict:
-    v = (C.c_int32 * 17)()
-    check(lib.mirt_interp_plan_config(handle, v, 17))
+    v = (C.c_int32 * 18)()
+    check(lib.mirt_interp_plan_config(handle, v, 18))
     return {"spread_tile": [v[0], v[1], v[2]], "spread_threads": v[3], "spread_heavy_first": v[4],
             "coil_lanes": v[5], "gather_threads": v[6],
             "gather_ctas": v[8], "sort_bin": [v[9], v[10], v[11]], "split_chunk": v[12],
             "spread_tasks": v[13], "spread_padc": v[14], "spread_reductions": v[15],
-            "spread_atomic": v[16]}
+            "spread_atomic": v[16], "spread_own": v[17]}
 
 
 class InterpPlan:
@@ -156,6 +156,12 @@ class InterpPlan:
         """False: the spread may add with shared-memory atomics (faster, not
         bitwise reproducible); the autotuner then also tries that variant."""
         check(self.lib.mirt_interp_plan_set_deterministic(self.handle, int(bool(deterministic))))
+        return self.config()
+
+    def set_ownership(self, own=True, stream=None):
+        """Ownership spread (2D, J = 6; see mirt_interp_plan_set_ownership)."""
+        check(self.lib.mirt_interp_plan_set_ownership(self.handle, int(bool(own)),
+                                                      _stream_ptr(stream)))
         return self.config()
 
     def set_spread(self, tile, threads=32, padc=0, stream=None):

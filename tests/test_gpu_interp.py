@@ -310,3 +310,44 @@ def test_atomic_spread_3d():
     ref = oracle.interp_adj(fm, h, J, L, tm, K, 0, impl=ref_impl())
     assert rel_l2(got, ref) <= ADJ_TOL
     plan.close()
+
+
+@pytest.mark.parametrize("C", [1, 8, 32])
+def test_ownership_spread_matches_oracle(C):
+    """Ownership spread (2D, J = 6): padded tiles in four colour launches.  A
+    dense slice forces split tiles (partial tiles summed by the reduction);
+    every tiling gives the oracle's adjoint, bitwise reproducibly."""
+    import torch
+    rng = np.random.default_rng(71 + C)
+    K, J, L = [96, 96], [6, 6], [1024, 1024]
+    h = [mb.minmax_kb_table(48, 6, 96, 1024)] * 2
+    tms = [rng.uniform(-60, 60, (1500, 2)), rng.uniform(-3, 3, (5000, 2)),
+           rng.uniform(-48, 48, (800, 2))]
+    moff = np.concatenate([[0], np.cumsum([len(t) for t in tms])])
+    tm = np.concatenate(tms)
+    plan = mb.InterpPlan(K, J, L, h, tm, C, slice_moff=moff)
+    fm = rng.standard_normal((len(tm), C)) + 1j * rng.standard_normal((len(tm), C))
+    fm_d = torch.from_numpy(fm.astype(np.complex64)).cuda()
+    refs = [oracle.interp_adj(fm[moff[s]:moff[s + 1]], h, J, L, tms[s], K, 0, impl=ref_impl())
+            for s in range(3)]
+    for tile, threads in [((8, 8), 32), ((16, 8), 64), ((16, 16), 128)]:
+        plan.set_spread(tile, threads, 0)
+        cfg = plan.set_ownership(True)
+        assert cfg["spread_own"] == 1 and cfg["spread_reductions"] > 0
+        out = plan.adjoint(fm_d).cpu().numpy()
+        for s in range(3):
+            got = np.transpose(out[s], (1, 0, 2)).reshape(-1, C, order="F")
+            assert rel_l2(got, refs[s]) <= ADJ_TOL, (tile, s)
+        assert np.array_equal(out, plan.adjoint(fm_d).cpu().numpy())
+    plan.close()
+
+
+def test_ownership_spread_refused_where_colours_would_overlap():
+    K, J, L = [80, 96], [6, 6], [256, 256]
+    h = [mb.minmax_kb_table(40, 6, 80, 256), mb.minmax_kb_table(48, 6, 96, 256)]
+    tm = np.random.default_rng(0).uniform(-40, 40, (300, 2))
+    plan = mb.InterpPlan(K, J, L, h, tm, 4)
+    plan.set_spread((16, 16), 32, 0)         # 5 tiles along K1 = 80: odd
+    with pytest.raises(mb.MirtError, match="even number of tiles"):
+        plan.set_ownership(True)
+    plan.close()
