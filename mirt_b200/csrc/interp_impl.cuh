@@ -710,6 +710,49 @@ __global__ void __launch_bounds__(256) spread_reduce_kernel(InterpArgs a, Tiling
 // the grid (periodic wrap) or, for a split heavy tile, written as a partial.
 // Within one launch (one colour) no two padded tiles overlap, so the adds
 // need no atomics; colours run in a fixed order: deterministic.
+// grid[(lo + p) mod K] += sum over parts of src[part][p] for the q0 x q1
+// points p of a padded tile (src: [P1][P0][CW], parts `pstride` apart);
+// U grid values are loaded before any is written back, so a thread keeps U
+// independent loads in flight.
+template <int CW, int U>
+__device__ __forceinline__ void own_add_tile(const float2 *src, int P0, int q0, int q1, int lo0,
+                                             int lo1, int c0, int C, int K0, int K1,
+                                             float2 *gout, int nparts, size_t pstride) {
+  const int n = q0 * q1 * CW;
+  for (int e0 = threadIdx.x; e0 < n; e0 += U * blockDim.x) {
+    float2 o[U];
+    float2 *q[U];
+    size_t pe[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int e = e0 + u * blockDim.x;
+      q[u] = nullptr;
+      if (e < n) {
+        const int cc = e % CW, pt = e / CW;
+        const int p0 = pt % q0, p1 = pt / q0;
+        if (c0 + cc < C) {
+          int g0 = lo0 + p0, g1 = lo1 + p1;
+          if (g0 >= K0) g0 -= K0;
+          if (g1 >= K1) g1 -= K1;
+          q[u] = gout + ((long long)g1 * K0 + g0) * C + c0 + cc;
+          pe[u] = ((size_t)p1 * P0 + p0) * CW + cc;
+          o[u] = *q[u];
+        }
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      if (!q[u]) continue;
+      for (int p = 0; p < nparts; p++) {
+        const float2 v = src[p * pstride + pe[u]];
+        o[u].x += v.x;
+        o[u].y += v.y;
+      }
+      *q[u] = o[u];
+    }
+  }
+}
+
 template <int CW, bool REAL>
 __global__ void __launch_bounds__(256) spread_own_kernel(InterpArgs a, Tiling t,
                                                          const int *__restrict__ bin_start,
@@ -811,20 +854,7 @@ __global__ void __launch_bounds__(256) spread_own_kernel(InterpArgs a, Tiling t,
   }
   float2 *gout = ck + (long long)slice * a.grid_elems;
   const int q0 = ext0 + JT - 1, q1 = ext1 + JT - 1;
-  for (int e = threadIdx.x; e < q0 * q1 * CW; e += blockDim.x) {
-    const int cc = e % CW, pt = e / CW;
-    const int p0 = pt % q0, p1 = pt / q0;
-    if (c0 + cc >= C) continue;
-    int g0 = lo0 + p0, g1 = lo1 + p1;
-    if (g0 >= g.K[0]) g0 -= g.K[0];
-    if (g1 >= g.K[1]) g1 -= g.K[1];
-    float2 *q = gout + ((long long)g1 * g.K[0] + g0) * C + c0 + cc;
-    const float2 v = acc[((size_t)p1 * P0 + p0) * CW + cc];
-    float2 o = *q;
-    o.x += v.x;
-    o.y += v.y;
-    *q = o;
-  }
+  own_add_tile<CW, 8>(acc, P0, q0, q1, lo0, lo1, c0, C, g.K[0], g.K[1], gout, 1, 0);
 }
 
 // Sum the partial padded tiles of each split tile of one colour, in slot
@@ -847,26 +877,7 @@ __global__ void __launch_bounds__(256) spread_own_reduce_kernel(InterpArgs a, Ti
   const float2 *part = t.scratch + ((size_t)first * gridDim.y + blockIdx.y) * P0 * P1 * CW;
   float2 *gout = ck + (long long)slice * a.grid_elems;
   const int q0 = ext0 + JT - 1, q1 = ext1 + JT - 1;
-  for (int e = threadIdx.x; e < q0 * q1 * CW; e += blockDim.x) {
-    const int cc = e % CW, pt = e / CW;
-    const int p0 = pt % q0, p1 = pt / q0;
-    if (c0 + cc >= a.C) continue;
-    const size_t pe = ((size_t)p1 * P0 + p0) * CW + cc;
-    float2 v = part[pe];
-    for (int p = 1; p < nparts; p++) {
-      const float2 w = part[p * stride + pe];
-      v.x += w.x;
-      v.y += w.y;
-    }
-    int g0 = lo0 + p0, g1 = lo1 + p1;
-    if (g0 >= g.K[0]) g0 -= g.K[0];
-    if (g1 >= g.K[1]) g1 -= g.K[1];
-    float2 *q = gout + ((long long)g1 * g.K[0] + g0) * a.C + c0 + cc;
-    float2 o = *q;
-    o.x += v.x;
-    o.y += v.y;
-    *q = o;
-  }
+  own_add_tile<CW, 4>(part, P0, q0, q1, lo0, lo1, c0, a.C, g.K[0], g.K[1], gout, nparts, stride);
 }
 
 // ------------------------------------------------------------------------
