@@ -264,6 +264,43 @@ int mirt_nufft_autotune(mirt_nufft *p, void *stream);
 
 int mirt_nufft_destroy(mirt_nufft *p);
 
+/* ------------------------------------------------------------------------
+ * 3a. newfft in table mode: st = newfft(om, Nd, 'Jd', Jd, 'Kd', Kd,
+ *     'n_shift', n_shift, 'mode', 'table0' | 'table1', 'oversample', Ld,
+ *     'phasing', 'real' | 'complex', ...)
+ *     set-up    nufft/newfft.m:146-176, nufft/private/newfft_table_init.m:40-52,130-137
+ *     forward   st.fft  = nufft/private/newfft_approx_for.m:15-63
+ *     adjoint   st.adj  = nufft/private/newfft_approx_adj.m:30-82
+ *
+ * The caller gives the tables h{d} (J_d L_d + 1 values each; h_im NULL or
+ * h_im[0] NULL for real tables), the interpolation order (0 or 1; 1 only
+ * with real tables, as the table mex files require), the scaling factors
+ * st.sn [prod Nd] (sn_im may be NULL) and Nmid (NULL: no phases, as
+ * phasing 'complex').  The plan applies, inside its existing passes:
+ *   phase_before[k] = prod_d exp(i 2 pi k_d Nmid_d / K_d)   (nufft/newfft.m:511-520)
+ *       on the grid after the FFT (conjugate before the inverse FFT), and
+ *   phase_after[m] = exp(i om_m . (n_shift - Nmid))           (nufft/newfft.m:522-527)
+ *       on the samples after interpolation (conjugate before spreading).
+ * Everything else (layouts, forward/adjoint/host/autotune/capture/destroy)
+ * is that of mirt_nufft above.
+ * ---------------------------------------------------------------------- */
+int mirt_newfft_create(mirt_nufft **out, int32_t D, const int32_t *Nd, const int32_t *Kd,
+	const int32_t *Jd, const int32_t *Ld, const double *const *h_re,
+	const double *const *h_im, int32_t order, const double *sn_re, const double *sn_im,
+	const double *nmid, const double *n_shift, const double *om, int64_t Mtot,
+	const int64_t *slice_moff, int32_t nslice, int32_t ncol, void *stream);
+
+/* newfft's default interpolator, ktype 'kb:minmax' with phasing 'real'
+ * (host FP64):
+ *   table: J*L+1 real values, the KB kernel (alpha = 2.34 J, kb_m = 0)
+ *          at t = -J/2 + i/L  (nufft/private/newfft_table_init.m:140-184,
+ *          nufft/kaiser_bessel.m:106-117)
+ *   scale: N real values 1 / KB-FT((n - nmid) / K)  (nufft/newfft.m:352-356,
+ *          nufft/kaiser_bessel_ft.m); st.sn is their outer product and
+ *          nmid = floor(N/2) for phasing 'real' (nufft/newfft.m:146-151). */
+int mirt_newfft_kb_table(int32_t J, int32_t L, double *h);
+int mirt_newfft_kb_scale(int32_t N, int32_t J, int32_t K, double nmid, double *sn);
+
 /* Capture one batched step of the plan -- forward x -> X when x is given,
  * then adjoint X -> xa when xa is given -- into a CUDA graph (on an internal
  * capture stream) and return it instantiated; mirt_graph_launch replays it

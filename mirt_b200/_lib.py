@@ -105,6 +105,11 @@ _SIGS = {
                                     _i64, _i32, _vp, _vp, _vp], C.c_int),
     "mirt_minmax_kb_table": ([_i32, _i32, _i32, _i32, _dp, _dp], C.c_int),
     "mirt_minmax_kb_scale": ([_i32, _i32, _i32, _dp, _dp], C.c_int),
+    "mirt_newfft_create": ([C.POINTER(_vp), _i32, _i32p, _i32p, _i32p, _i32p, C.POINTER(_dp),
+                            C.POINTER(_dp), _i32, _dp, _dp, _dp, _dp, _dp, _i64, _i64p, _i32,
+                            _i32, _vp], C.c_int),
+    "mirt_newfft_kb_table": ([_i32, _i32, _dp], C.c_int),
+    "mirt_newfft_kb_scale": ([_i32, _i32, _i32, C.c_double, _dp], C.c_int),
 }
 
 _lib: C.CDLL | None = None

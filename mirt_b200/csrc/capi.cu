@@ -28,6 +28,8 @@ bool minmax_kb_table(int N, int J, int K, int L, std::vector<std::complex<double
 void alpha_kb_fit(int N, int J, int K, std::vector<double> &alphas, double &beta);
 std::vector<std::complex<double>> scale1(int N, int K, const std::vector<double> &alpha,
                                          double beta);
+void kb_table(int J, int L, std::vector<double> &h);
+std::vector<double> kb_scale(int N, int J, int K, double nmid);
 }  // namespace mirt
 
 using namespace mirt;
@@ -1400,20 +1402,22 @@ int mirt_minmax_kb_scale(int32_t N, int32_t J, int32_t K, double *sn_re, double 
   return MIRT_OK;
 }
 
-int mirt_nufft_create(mirt_nufft **out, int32_t D, const int32_t *Nd, const int32_t *Kd,
-                      const int32_t *Jd, const int32_t *Ld, const double *n_shift,
-                      const double *om, int64_t Mtot, const int64_t *slice_moff, int32_t nslice,
-                      int32_t ncol, void *stream) {
-  if (!out) return fail(MIRT_ERR_ARG, "output pointer is NULL");
-  *out = nullptr;
+}  // extern "C"
+
+namespace {
+
+// Geometry checks shared by the NUFFT constructors; fills the slice offsets.
+int nufft_check(int D, const int32_t *Nd, const int32_t *Kd, const int32_t *Jd, const int32_t *Ld,
+                int order, bool cplx, int64_t Mtot, const int64_t *slice_moff, int nslice,
+                int ncol, std::vector<long long> &moff) {
   int rc = device_ok();
   if (rc) return rc;
   if (nslice < 1) return fail(MIRT_ERR_ARG, "nslice must be >= 1");
-  rc = validate_geometry(D, Kd, Jd, Ld, 0, true, Mtot, ncol);
+  rc = validate_geometry(D, Kd, Jd, Ld, order, cplx, Mtot, ncol);
   if (rc) return rc;
   for (int d = 0; d < D; d++)
     if (Nd[d] < 1 || Nd[d] > Kd[d]) return fail(MIRT_ERR_ARG, "need 1 <= N <= K per dimension");
-  std::vector<long long> moff(nslice + 1);
+  moff.assign(nslice + 1, 0);
   if (slice_moff) {
     for (int s = 0; s <= nslice; s++) moff[s] = slice_moff[s];
     if (moff[0] != 0 || moff[nslice] != Mtot)
@@ -1425,8 +1429,18 @@ int mirt_nufft_create(mirt_nufft **out, int32_t D, const int32_t *Nd, const int3
     moff[0] = 0;
     moff[1] = Mtot;
   }
-  cudaStream_t st = as_stream(stream);
-  auto *p = new mirt_nufft();
+  return MIRT_OK;
+}
+
+// The plan once its tables and scaling factors are known: device tables,
+// sn, tm = om / (2 pi / K) with the per-sample phase exp(i om . ns), the
+// grid phase prod_d exp(i 2 pi k_d nmid_d / K_d) when nmid is given, the
+// sorted interpolation plan, the grids and the batched FFT.
+int nufft_finish(mirt_nufft *p, int D, const int32_t *Nd, const int32_t *Kd, const int32_t *Jd,
+                 const int32_t *Ld, const double *const *hr, const double *const *hi, int order,
+                 const std::vector<std::complex<double>> &sn, const double *ns_in,
+                 const double *nmid, const double *om, int64_t Mtot,
+                 const std::vector<long long> &moff, int nslice, int ncol, cudaStream_t st) {
   p->C = ncol;
   p->nslice = nslice;
   p->Mtot = Mtot;
@@ -1439,17 +1453,116 @@ int mirt_nufft_create(mirt_nufft **out, int32_t D, const int32_t *Nd, const int3
     p->gg.npix *= p->gg.N[d];
     p->gg.ngrid *= p->gg.K[d];
   }
-  auto bail = [&](int code) {
-    delete p;
-    return code;
-  };
+  p->ip = new mirt_interp_plan();
+  mirt_interp_plan *P = p->ip;
+  int rc = plan_geometry(P, D, Kd, Jd, Ld, hr, hi, order, ncol, st);
+  if (rc) return rc;
+  {
+    std::vector<float2> snf(sn.size());
+    for (size_t i = 0; i < sn.size(); i++)
+      snf[i] = make_float2((float)sn[i].real(), (float)sn[i].imag());
+    cudaError_t e = p->sn.alloc(snf.size() * sizeof(float2));
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(p->sn.p, snf.data(), snf.size() * sizeof(float2),
+                          cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return fail(MIRT_ERR_CUDA, cudaGetErrorString(e));
+  }
+  bool any_mid = false;
+  for (int d = 0; d < D; d++)
+    if (nmid && nmid[d] != 0) any_mid = true;
+  if (any_mid) {
+    // phase_before per dimension in FP64: angle 2 pi frac(k nmid / K)
+    std::vector<float2> ph;
+    for (int d = 0; d < D; d++)
+      for (int k = 0; k < Kd[d]; k++) {
+        const double f = std::fmod((double)k * nmid[d], (double)Kd[d]) / Kd[d];
+        ph.push_back(make_float2((float)std::cos(2 * M_PI * f), (float)std::sin(2 * M_PI * f)));
+      }
+    cudaError_t e = p->phtab.alloc(ph.size() * sizeof(float2));
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(p->phtab.p, ph.data(), ph.size() * sizeof(float2),
+                          cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return fail(MIRT_ERR_CUDA, cudaGetErrorString(e));
+    p->gp.D = D;
+    long long off = 0;
+    for (int d = 0; d < 3; d++) {
+      p->gp.K[d] = d < D ? Kd[d] : 1;
+      p->gp.tab[d] = d < D ? p->phtab.as<float2>() + off : nullptr;
+      if (d < D) off += Kd[d];
+    }
+  }
+  // om -> tm (FP64, om / (2 pi / K)) and the per-sample phase on the device
+  bool any_shift = false;
+  double gam[3] = {1, 1, 1}, ns[3] = {0, 0, 0};
+  for (int d = 0; d < D; d++) {
+    gam[d] = 2 * M_PI / Kd[d];
+    ns[d] = ns_in ? ns_in[d] : 0.0;
+    if (ns[d] != 0) any_shift = true;
+  }
+  {
+    DMem om_d, par;
+    cudaError_t e = om_d.alloc(std::max<long long>(Mtot, 1) * D * sizeof(double));
+    if (e == cudaSuccess) e = par.alloc(6 * sizeof(double));
+    if (e == cudaSuccess) e = P->tm.alloc(std::max<long long>(Mtot, 1) * D * sizeof(double));
+    if (e == cudaSuccess && any_shift) e = P->phase.alloc(std::max<long long>(Mtot, 1) * sizeof(float2));
+    double hp[6] = {gam[0], gam[1], gam[2], ns[0], ns[1], ns[2]};
+    if (e == cudaSuccess && Mtot)
+      e = cudaMemcpyAsync(om_d.p, om, Mtot * D * sizeof(double), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(par.p, hp, sizeof hp, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+      e = launch_om_to_tm(om_d.as<double>(), Mtot, D, par.as<double>(), par.as<double>() + 3,
+                          any_shift ? 1 : 0, P->tm.as<double>(), P->phase.as<float2>(), st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return fail(MIRT_ERR_CUDA, cudaGetErrorString(e));
+    P->a.phase = any_shift ? P->phase.as<float2>() : nullptr;
+  }
+  rc = plan_finish(P, Mtot, moff.data(), nslice, st);
+  if (rc) return rc;
+  {
+    cudaError_t e = p->grid.alloc((size_t)nslice * p->gg.ngrid * ncol * sizeof(float2));
+    if (e == cudaSuccess) e = p->grid_cm.alloc((size_t)nslice * p->gg.ngrid * ncol * sizeof(float2));
+    if (e != cudaSuccess) return fail(MIRT_ERR_ALLOC, "NUFFT grid buffers");
+  }
+  // contiguous C2C transforms, one per (slice, coil) plane of the coil-major grid
+  int n[3];
+  for (int d = 0; d < D; d++) n[d] = Kd[D - 1 - d];
+  if (ncol > 0) {
+    const long long batch = (long long)nslice * ncol;
+    if (batch >= (1ll << 31)) return fail(MIRT_ERR_ARG, "too many FFT planes");
+    cufftResult r = cufftPlanMany(&p->fft, D, n, nullptr, 1, (int)p->gg.ngrid, nullptr, 1,
+                                  (int)p->gg.ngrid, CUFFT_C2C, (int)batch);
+    if (r != CUFFT_SUCCESS)
+      return fail(MIRT_ERR_FFT, "cufftPlanMany failed: " + std::to_string((int)r));
+    p->fft_ok = true;
+  }
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return fail(MIRT_ERR_CUDA, cudaGetErrorString(e));
+  return MIRT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mirt_nufft_create(mirt_nufft **out, int32_t D, const int32_t *Nd, const int32_t *Kd,
+                      const int32_t *Jd, const int32_t *Ld, const double *n_shift,
+                      const double *om, int64_t Mtot, const int64_t *slice_moff, int32_t nslice,
+                      int32_t ncol, void *stream) {
+  if (!out) return fail(MIRT_ERR_ARG, "output pointer is NULL");
+  *out = nullptr;
+  std::vector<long long> moff;
+  int rc = nufft_check(D, Nd, Kd, Jd, Ld, 0, true, Mtot, slice_moff, nslice, ncol, moff);
+  if (rc) return rc;
   // tables (FP64 host), scaling factors as the outer product of conj(1D factors)
   std::vector<std::vector<double>> hre(D), him(D);
   std::vector<std::complex<double>> sn(1, 1.0);
   for (int d = 0; d < D; d++) {
     std::vector<std::complex<double>> h;
     if (!minmax_kb_table(Nd[d], Jd[d], Kd[d], Ld[d], h))
-      return bail(fail(MIRT_ERR_ARG, "singular min-max system"));
+      return fail(MIRT_ERR_ARG, "singular min-max system");
     hre[d].resize(h.size());
     him[d].resize(h.size());
     for (size_t i = 0; i < h.size(); i++) {
@@ -1471,71 +1584,67 @@ int mirt_nufft_create(mirt_nufft **out, int32_t D, const int32_t *Nd, const int3
     hr[d] = hre[d].data();
     hi[d] = him[d].data();
   }
-  p->ip = new mirt_interp_plan();
-  mirt_interp_plan *P = p->ip;
-  rc = plan_geometry(P, D, Kd, Jd, Ld, hr, hi, 0, ncol, st);
-  if (rc) return bail(rc);
-  {
-    std::vector<float2> snf(sn.size());
-    for (size_t i = 0; i < sn.size(); i++)
-      snf[i] = make_float2((float)sn[i].real(), (float)sn[i].imag());
-    cudaError_t e = p->sn.alloc(snf.size() * sizeof(float2));
-    if (e == cudaSuccess)
-      e = cudaMemcpyAsync(p->sn.p, snf.data(), snf.size() * sizeof(float2),
-                          cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) return bail(fail(MIRT_ERR_CUDA, cudaGetErrorString(e)));
-  }
-  // om -> tm (FP64, om / (2 pi / K)) and the n_shift phase on the device
-  bool any_shift = false;
-  double gam[3] = {1, 1, 1}, ns[3] = {0, 0, 0};
-  for (int d = 0; d < D; d++) {
-    gam[d] = 2 * M_PI / Kd[d];
-    ns[d] = n_shift ? n_shift[d] : 0.0;
-    if (ns[d] != 0) any_shift = true;
-  }
-  {
-    DMem om_d, par;
-    cudaError_t e = om_d.alloc(std::max<long long>(Mtot, 1) * D * sizeof(double));
-    if (e == cudaSuccess) e = par.alloc(6 * sizeof(double));
-    if (e == cudaSuccess) e = P->tm.alloc(std::max<long long>(Mtot, 1) * D * sizeof(double));
-    if (e == cudaSuccess && any_shift) e = P->phase.alloc(std::max<long long>(Mtot, 1) * sizeof(float2));
-    double hp[6] = {gam[0], gam[1], gam[2], ns[0], ns[1], ns[2]};
-    if (e == cudaSuccess && Mtot)
-      e = cudaMemcpyAsync(om_d.p, om, Mtot * D * sizeof(double), cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess)
-      e = cudaMemcpyAsync(par.p, hp, sizeof hp, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess)
-      e = launch_om_to_tm(om_d.as<double>(), Mtot, D, par.as<double>(), par.as<double>() + 3,
-                          any_shift ? 1 : 0, P->tm.as<double>(), P->phase.as<float2>(), st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) return bail(fail(MIRT_ERR_CUDA, cudaGetErrorString(e)));
-    P->a.phase = any_shift ? P->phase.as<float2>() : nullptr;
-  }
-  rc = plan_finish(P, Mtot, moff.data(), nslice, st);
-  if (rc) return bail(rc);
-  {
-    cudaError_t e = p->grid.alloc((size_t)nslice * p->gg.ngrid * ncol * sizeof(float2));
-    if (e == cudaSuccess) e = p->grid_cm.alloc((size_t)nslice * p->gg.ngrid * ncol * sizeof(float2));
-    if (e != cudaSuccess) return bail(fail(MIRT_ERR_ALLOC, "NUFFT grid buffers"));
-  }
-  // contiguous C2C transforms, one per (slice, coil) plane of the coil-major grid
-  int n[3];
-  for (int d = 0; d < D; d++) n[d] = Kd[D - 1 - d];
-  if (ncol > 0) {
-    const long long batch = (long long)nslice * ncol;
-    if (batch >= (1ll << 31)) return bail(fail(MIRT_ERR_ARG, "too many FFT planes"));
-    cufftResult r = cufftPlanMany(&p->fft, D, n, nullptr, 1, (int)p->gg.ngrid, nullptr, 1,
-                                  (int)p->gg.ngrid, CUFFT_C2C, (int)batch);
-    if (r != CUFFT_SUCCESS)
-      return bail(fail(MIRT_ERR_FFT, "cufftPlanMany failed: " + std::to_string((int)r)));
-    p->fft_ok = true;
-  }
-  {
-    cudaError_t e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) return bail(fail(MIRT_ERR_CUDA, cudaGetErrorString(e)));
+  auto *p = new mirt_nufft();
+  rc = nufft_finish(p, D, Nd, Kd, Jd, Ld, hr, hi, 0, sn, n_shift, nullptr, om, Mtot, moff,
+                    nslice, ncol, as_stream(stream));
+  if (rc) {
+    delete p;
+    return rc;
   }
   *out = p;
+  return MIRT_OK;
+}
+
+int mirt_newfft_create(mirt_nufft **out, int32_t D, const int32_t *Nd, const int32_t *Kd,
+                       const int32_t *Jd, const int32_t *Ld, const double *const *h_re,
+                       const double *const *h_im, int32_t order, const double *sn_re,
+                       const double *sn_im, const double *nmid, const double *n_shift,
+                       const double *om, int64_t Mtot, const int64_t *slice_moff, int32_t nslice,
+                       int32_t ncol, void *stream) {
+  if (!out) return fail(MIRT_ERR_ARG, "output pointer is NULL");
+  *out = nullptr;
+  if (!h_re || !sn_re) return fail(MIRT_ERR_ARG, "tables and scaling factors are required");
+  const bool cplx = h_im != nullptr && h_im[0] != nullptr;
+  std::vector<long long> moff;
+  int rc = nufft_check(D, Nd, Kd, Jd, Ld, order, cplx, Mtot, slice_moff, nslice, ncol, moff);
+  if (rc) return rc;
+  for (int d = 0; d < D; d++) {
+    if (!h_re[d]) return fail(MIRT_ERR_ARG, "table of a dimension is NULL");
+    if (cplx && !h_im[d]) return fail(MIRT_ERR_ARG, "complex tables need every imaginary part");
+  }
+  long long npix = 1;
+  for (int d = 0; d < D; d++) npix *= Nd[d];
+  std::vector<std::complex<double>> sn(npix);
+  for (long long i = 0; i < npix; i++) sn[i] = {sn_re[i], sn_im ? sn_im[i] : 0.0};
+  // phase_after = exp(i om . (n_shift - nmid)) per sample
+  double ns[3] = {0, 0, 0};
+  for (int d = 0; d < D; d++) ns[d] = (n_shift ? n_shift[d] : 0.0) - (nmid ? nmid[d] : 0.0);
+  auto *p = new mirt_nufft();
+  rc = nufft_finish(p, D, Nd, Kd, Jd, Ld, h_re, cplx ? h_im : nullptr, order, sn, ns, nmid, om,
+                    Mtot, moff, nslice, ncol, as_stream(stream));
+  if (rc) {
+    delete p;
+    return rc;
+  }
+  *out = p;
+  return MIRT_OK;
+}
+
+int mirt_newfft_kb_table(int32_t J, int32_t L, double *h) {
+  if (J < 1 || J > MIRT_JMAX || L < 1) return fail(MIRT_ERR_ARG, "J must be in 1..16, L positive");
+  if (!h) return fail(MIRT_ERR_ARG, "output pointer is NULL");
+  std::vector<double> t;
+  kb_table(J, L, t);
+  std::copy(t.begin(), t.end(), h);
+  return MIRT_OK;
+}
+
+int mirt_newfft_kb_scale(int32_t N, int32_t J, int32_t K, double nmid, double *sn) {
+  if (N < 1 || J < 1 || J > MIRT_JMAX || K < 1)
+    return fail(MIRT_ERR_ARG, "N, K must be positive, J in 1..16");
+  if (!sn) return fail(MIRT_ERR_ARG, "output pointer is NULL");
+  std::vector<double> s = kb_scale(N, J, K, nmid);
+  std::copy(s.begin(), s.end(), sn);
   return MIRT_OK;
 }
 
@@ -1548,7 +1657,7 @@ int mirt_nufft_forward(mirt_nufft *p, const void *x, void *X, void *stream) {
   int rc = nufft_fft(p, CUFFT_FORWARD, st);
   if (rc) return rc;
   CK(launch_transpose_cols(p->grid_cm.as<float2>(), p->grid.as<float2>(), p->gg.ngrid, p->C,
-                           p->nslice, 1, st));
+                           p->nslice, 1, st, &p->gp));
   CK(launch_gather(p->ip->ag, p->ip->lg, p->grid.as<float2>(), static_cast<float2 *>(X), st));
   return MIRT_OK;
 }
@@ -1561,7 +1670,7 @@ int mirt_nufft_adjoint(mirt_nufft *p, const void *X, void *x, void *stream) {
   CK(launch_spread(P->a, P->t, P->ls, P->bin_start.as<int>(), static_cast<const float2 *>(X),
                    p->grid.as<float2>(), st));
   CK(launch_transpose_cols(p->grid.as<float2>(), p->grid_cm.as<float2>(), p->gg.ngrid, p->C,
-                           p->nslice, 0, st));
+                           p->nslice, 0, st, &p->gp));
   int rc = nufft_fft(p, CUFFT_INVERSE, st);
   if (rc) return rc;
   CK(launch_crop_deapod_cm(p->grid_cm.as<float2>(), p->sn.as<float2>(), static_cast<float2 *>(x),

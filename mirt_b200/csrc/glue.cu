@@ -6,7 +6,9 @@
 //   crop_deapod_cm  crop [Kd] -> [Nd] and multiply by conj(sn) (nufft/nufft_adj.m:63-80),
 //                   from the coil-major FFT output back to the coil-innermost image
 //   transpose_cols  coil-major <-> coil-innermost grid between the FFT and the
-//                   interpolation
+//                   interpolation, optionally times newfft's phase_before over the
+//                   grid or its conjugate (nufft/newfft.m:511-520,
+//                   nufft/private/newfft_approx_for.m:32-34, newfft_approx_adj.m:56-58)
 //   om_to_tm     tm = om / (2 pi / K) in FP64 and the n_shift phase
 //                exp(i om . n_shift) (nufft/nufft_table_interp.m:36-40,
 //                nufft/nufft_table_init.m:48-50)
@@ -103,9 +105,24 @@ __global__ void crop_deapod_cm_kernel(const float2 *__restrict__ grid,
   }
 }
 
-// [B][P] <-> [P][B] per slice: out[s][p][b] = in[s][b][p] (to_cl) or the reverse.
+// grid phase prod_d tab[d][k_d] of grid point p (k1 fastest)
+__device__ __forceinline__ float2 grid_phase(const GridPhase &ph, long long p) {
+  float2 v = make_float2(1.f, 0.f);
+  long long r = p;
+  for (int d = 0; d < ph.D; d++) {
+    const int k = (int)(r % ph.K[d]);
+    r /= ph.K[d];
+    const float2 t = ph.tab[d][k];
+    v = make_float2(v.x * t.x - v.y * t.y, v.x * t.y + v.y * t.x);
+  }
+  return v;
+}
+
+// [B][P] <-> [P][B] per slice: out[s][p][b] = in[s][b][p] (to_cl) or the reverse;
+// PH: times the grid phase of p (to_cl) or its conjugate (the reverse).
+template <bool PH>
 __global__ void transpose_cols_kernel(const float2 *__restrict__ in, float2 *__restrict__ out,
-                                      long long P, int B, int to_cl) {
+                                      long long P, int B, int to_cl, GridPhase ph) {
   __shared__ float2 tile[32][33];
   const int tx = threadIdx.x, ty = threadIdx.y;
   const long long p0 = (long long)blockIdx.x * 32;
@@ -124,7 +141,14 @@ __global__ void transpose_cols_kernel(const float2 *__restrict__ in, float2 *__r
     for (int i = ty; i < 32; i += 8) {
       const long long p = p0 + i;
       const int b = b0 + tx;
-      if (b < B && p < P) dst[p * B + b] = tile[tx][i];
+      if (b < B && p < P) {
+        float2 v = tile[tx][i];
+        if (PH) {
+          const float2 q = grid_phase(ph, p);
+          v = make_float2(v.x * q.x - v.y * q.y, v.x * q.y + v.y * q.x);
+        }
+        dst[p * B + b] = v;
+      }
     }
   } else {
     // src [P][B] -> dst [B][P]
@@ -137,7 +161,14 @@ __global__ void transpose_cols_kernel(const float2 *__restrict__ in, float2 *__r
     for (int i = ty; i < 32; i += 8) {
       const int b = b0 + i;
       const long long p = p0 + tx;
-      if (b < B && p < P) dst[(long long)b * P + p] = tile[tx][i];
+      if (b < B && p < P) {
+        float2 v = tile[tx][i];
+        if (PH) {
+          const float2 q = grid_phase(ph, p);  // v * conj(q)
+          v = make_float2(v.x * q.x + v.y * q.y, v.y * q.x - v.x * q.y);
+        }
+        dst[(long long)b * P + p] = v;
+      }
     }
   }
 }
@@ -266,10 +297,14 @@ cudaError_t launch_crop_deapod_cm(const float2 *grid, const float2 *sn, float2 *
 }
 
 cudaError_t launch_transpose_cols(const float2 *in, float2 *out, long long P, int B, int nslice,
-                                  int to_cl, cudaStream_t st) {
+                                  int to_cl, cudaStream_t st, const GridPhase *ph) {
   if (P == 0 || B == 0 || nslice == 0) return cudaSuccess;
   dim3 grid_dim((unsigned)((P + 31) / 32), (unsigned)((B + 31) / 32), (unsigned)nslice);
-  transpose_cols_kernel<<<grid_dim, dim3(32, 8), 0, st>>>(in, out, P, B, to_cl);
+  if (ph && ph->tab[0])
+    transpose_cols_kernel<true><<<grid_dim, dim3(32, 8), 0, st>>>(in, out, P, B, to_cl, *ph);
+  else
+    transpose_cols_kernel<false><<<grid_dim, dim3(32, 8), 0, st>>>(in, out, P, B, to_cl,
+                                                                   GridPhase{});
   return cudaGetLastError();
 }
 

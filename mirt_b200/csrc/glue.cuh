@@ -5,6 +5,15 @@
 
 namespace mirt {
 
+// Separable phase on the oversampled grid, prod_d tab[d][k_d] (k1 fastest):
+// newfft's phase_before = exp(i 2 pi sum_d k_d Nmid_d / K_d) as one table
+// of K_d values per dimension.
+struct GridPhase {
+  int D;
+  int K[3];
+  const float2 *tab[3];
+};
+
 struct GlueGeom {
   int D;
   int N[3];            // image size per dimension (N1 fastest)
@@ -19,9 +28,10 @@ cudaError_t launch_deapod_pad_cm(const float2 *x, const float2 *sn, float2 *grid
 // coil-major grid[s][c][k] -> cropped, conj(sn)-scaled image x[s][n][c]
 cudaError_t launch_crop_deapod_cm(const float2 *grid, const float2 *sn, float2 *x,
                                   const GlueGeom &g, int C, int nslice, cudaStream_t st);
-// per slice: to_cl = 1: [B][P] -> [P][B]; to_cl = 0: [P][B] -> [B][P]
+// per slice: to_cl = 1: [B][P] -> [P][B]; to_cl = 0: [P][B] -> [B][P]; with ph,
+// times the grid phase (to_cl = 1) or its conjugate (to_cl = 0)
 cudaError_t launch_transpose_cols(const float2 *in, float2 *out, long long P, int B, int nslice,
-                                  int to_cl, cudaStream_t st);
+                                  int to_cl, cudaStream_t st, const GridPhase *ph = nullptr);
 cudaError_t launch_om_to_tm(const double *om, long long M, int D, const double *gam_dev,
                             const double *nshift_dev, int want_phase, double *tm, float2 *phase,
                             cudaStream_t st);

@@ -80,6 +80,8 @@ struct mirt_nufft {
   int C = 0, nslice = 0;
   long long Mtot = 0;
   mirt::DMem sn, grid, grid_cm, hx, hX;  // grid: coil innermost (interp); grid_cm: coil-major (FFT)
+  mirt::DMem phtab;                      // newfft phase_before per dimension, float2 [sum K_d]
+  mirt::GridPhase gp{};                  // tables into phtab (tab[0] null: no grid phase)
   cufftHandle fft = 0;
   bool fft_ok = false;
   ~mirt_nufft() {

@@ -10,6 +10,9 @@
 //   T, r, offset       nufft/private/nufft_T.m:45-75, nufft_r.m:32-50, nufft_offset.m:18-19
 //   sinc "diric"       nufft/nufft_diric.m:38-40, nufft/nufft_sinc.m
 //   1D table           nufft/nufft_table_init.m:111-134 with nufft/nufft_init.m:234-263,287-288
+//   newfft kb:minmax   real table nufft/private/newfft_table_init.m:140-184 ('ratio'),
+//                      kernel nufft/kaiser_bessel.m:68-69,106-117 (alpha = 2.34 J, kb_m = 0),
+//                      sn nufft/newfft.m:340-375 with Nmid (nufft/newfft.m:146-151)
 //
 // MATLAB built-ins are replaced: mldivide by a Householder QR least-squares
 // solve, inv by Gauss-Jordan with partial pivoting, besseli(0, .) by its power
@@ -233,6 +236,35 @@ bool minmax_kb_table(int N, int J, int K, int L, std::vector<cd> &h) {
     for (int l = 0; l < L; l++) h[(size_t)blk * L + l] = p[(size_t)l + (size_t)jj * L];
   h[(size_t)J * L] = 0;
   return true;
+}
+
+// Real table of newfft's default 'table0' / 'table1' modes (ktype
+// 'kb:minmax', phasing 'real'): the KB kernel sampled at t = -J/2 + i / L,
+// i = 0 .. J*L.  The 'ratio' construction reads the sparse interpolator of a
+// fake N = J problem column by column; for a kernel that depends only on the
+// offset t that is the kernel itself, symmetric, zero at |t| = J/2.  The
+// inline kernel carries alpha printed with %g.
+void kb_table(int J, int L, std::vector<double> &h) {
+  char buf[64];
+  std::snprintf(buf, sizeof buf, "%g", 2.34 * J);
+  const double alpha = std::atof(buf);
+  const double i0a = bessel_i0(alpha);
+  h.assign((size_t)J * L + 1, 0.0);
+  for (size_t i = 0; i < h.size(); i++) {
+    const double t = -J / 2.0 + (double)i / L;
+    if (std::fabs(t) < J / 2.0) {
+      const double f = std::sqrt(1 - (t / (J / 2.0)) * (t / (J / 2.0)));
+      h[i] = bessel_i0(alpha * f) / i0a;
+    }
+  }
+}
+
+// 1D scaling factors of newfft with ktype 'kb:minmax': 1 / KB-FT((n - Nmid) / K)
+// (alpha = 2.34 J as a number, no %g round trip here).
+std::vector<double> kb_scale(int N, int J, int K, double nmid) {
+  std::vector<double> s(N);
+  for (int n = 0; n < N; n++) s[n] = 1.0 / kb_ft((n - nmid) / K, J, 2.34 * J);
+  return s;
 }
 
 }  // namespace mirt

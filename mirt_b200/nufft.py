@@ -209,18 +209,21 @@ class NufftPlan:
         self.ncol = int(ncol)
         mo, self.nslice = _moff(slice_moff, self.Mtot)
         omf = np.ascontiguousarray(om.ravel(order="F"))
-        h = C.c_void_p()
-        check(self.lib.mirt_nufft_create(
-            C.byref(h), D, self.Nd.ctypes.data_as(_i32p), self.Kd.ctypes.data_as(_i32p),
-            self.Jd.ctypes.data_as(_i32p), self.Ld.ctypes.data_as(_i32p),
-            self.n_shift.ctypes.data_as(_dp), omf.ctypes.data_as(_dp), self.Mtot,
-            None if mo is None else mo.ctypes.data_as(_i64p), self.nslice, self.ncol,
-            _stream_ptr(stream)))
-        self.handle = h
+        self.handle = self._create(omf, mo, stream)
         self.om_f = omf                      # trajectory, column-major FP64 (Toeplitz set-up)
         self.slice_moff = mo
         self.image_shape = (self.nslice,) + tuple(int(n) for n in self.Nd[::-1]) + (self.ncol,)
         self.sample_shape = (self.Mtot, self.ncol)
+
+    def _create(self, omf, mo, stream):
+        h = C.c_void_p()
+        check(self.lib.mirt_nufft_create(
+            C.byref(h), self.D, self.Nd.ctypes.data_as(_i32p), self.Kd.ctypes.data_as(_i32p),
+            self.Jd.ctypes.data_as(_i32p), self.Ld.ctypes.data_as(_i32p),
+            self.n_shift.ctypes.data_as(_dp), omf.ctypes.data_as(_dp), self.Mtot,
+            None if mo is None else mo.ctypes.data_as(_i64p), self.nslice, self.ncol,
+            _stream_ptr(stream)))
+        return h
 
     def forward(self, x, out=None, stream=None):
         torch = _torch()
@@ -286,6 +289,112 @@ class NufftPlan:
             self.close()
         except Exception:
             pass
+
+
+def newfft_kb_table(J: int, L: int) -> np.ndarray:
+    """Real table of newfft's default 'kb:minmax' interpolator, [J*L+1]."""
+    h = np.empty(int(J) * int(L) + 1)
+    check(load().mirt_newfft_kb_table(int(J), int(L), h.ctypes.data_as(_dp)))
+    return h
+
+
+def newfft_kb_scale(N: int, J: int, K: int, nmid: float) -> np.ndarray:
+    """1D scaling factors of newfft's 'kb:minmax' interpolator, [N]."""
+    s = np.empty(int(N))
+    check(load().mirt_newfft_kb_scale(int(N), int(J), int(K), float(nmid),
+                                      s.ctypes.data_as(_dp)))
+    return s
+
+
+class NewfftPlan(NufftPlan):
+    """st = newfft(om, Nd, 'Jd', Jd, 'Kd', Kd, 'n_shift', n_shift, 'mode',
+    'table0' | 'table1', 'oversample', Ld, 'phasing', phasing) on the device
+    (nufft/newfft.m, nufft/private/newfft_table_init.m).
+
+    phasing 'real' (the reference's default) with ``tables=None`` builds the
+    'kb:minmax' real tables and scaling factors in the library; any other
+    interpolator is given as ``tables`` (one 1D table per dimension, real or
+    complex, J*L+1 values) and ``sn`` ([(Nd)], first index fastest).
+    phasing 'real' applies phase_before / phase_after with Nmid = floor(N/2);
+    'complex' applies only exp(i om . n_shift) per sample.  Layouts and
+    methods are those of NufftPlan.
+    """
+
+    def __init__(self, om, Nd, Jd=None, Kd=None, n_shift=None, mode="table1", Ld=None,
+                 phasing="real", tables=None, sn=None, ncol=1, slice_moff=None, stream=None):
+        om = np.asarray(om, dtype=np.float64)
+        D = 1 if om.ndim == 1 else om.shape[1]
+        Nd = _i32(Nd)
+        Jd = _i32([6] * D if Jd is None else Jd)
+        Kd = _i32(2 * Nd if Kd is None else Kd)
+        if mode not in ("table0", "table1"):
+            raise ValueError("mode must be 'table0' or 'table1'")
+        if phasing not in ("real", "complex"):
+            raise ValueError("phasing must be 'real' or 'complex'")
+        self.order = 0 if mode == "table0" else 1
+        if Ld is None:
+            Ld = 2 ** 11 if self.order == 0 else 2 ** 9
+        Ld = _i32(Ld if np.ndim(Ld) else [Ld] * D)
+        self.phasing = phasing
+        self.Nmid = (np.floor(Nd / 2) if phasing == "real" else (Nd - 1) / 2).astype(np.float64)
+        if tables is None:
+            if phasing != "real":
+                raise ValueError("built-in tables are the 'kb:minmax' real ones; pass tables "
+                                 "and sn for other phasings")
+            tables = [newfft_kb_table(Jd[d], Ld[d]) for d in range(D)]
+            s = np.ones(1)
+            for d in range(D):
+                s = np.outer(s.ravel(order="F"), newfft_kb_scale(Nd[d], Jd[d], Kd[d],
+                                                                 self.Nmid[d]))
+            sn = s.ravel(order="F")
+        if sn is None:
+            raise ValueError("sn is required with caller tables")
+        self._tab = [np.ascontiguousarray(t) for t in tables]
+        self._sn = np.asarray(sn).ravel(order="F")
+        super().__init__(om, Nd, Jd, Kd, n_shift=n_shift, Ld=Ld, ncol=ncol,
+                         slice_moff=slice_moff, stream=stream)
+
+    def _create(self, omf, mo, stream):
+        D = self.D
+        cx = any(np.iscomplexobj(t) for t in self._tab)
+        hr = [np.ascontiguousarray(np.real(t), dtype=np.float64) for t in self._tab]
+        hi = [np.ascontiguousarray(np.imag(t), dtype=np.float64) for t in self._tab]
+        for d in range(D):
+            if hr[d].size != int(self.Jd[d]) * int(self.Ld[d]) + 1:
+                raise ValueError(f"table {d} must have J*L+1 values")
+        if self._sn.size != int(np.prod(self.Nd)):
+            raise ValueError("sn must have prod(Nd) values")
+        hr_p = (_dp * D)(*[t.ctypes.data_as(_dp) for t in hr])
+        hi_p = (_dp * D)(*[t.ctypes.data_as(_dp) for t in hi]) if cx else None
+        snr = np.ascontiguousarray(self._sn.real, dtype=np.float64)
+        sni = np.ascontiguousarray(self._sn.imag, dtype=np.float64)
+        nmid = np.ascontiguousarray(self.Nmid)
+        h = C.c_void_p()
+        check(self.lib.mirt_newfft_create(
+            C.byref(h), D, self.Nd.ctypes.data_as(_i32p), self.Kd.ctypes.data_as(_i32p),
+            self.Jd.ctypes.data_as(_i32p), self.Ld.ctypes.data_as(_i32p), hr_p, hi_p,
+            self.order, snr.ctypes.data_as(_dp), sni.ctypes.data_as(_dp),
+            nmid.ctypes.data_as(_dp) if self.phasing == "real" else None,
+            self.n_shift.ctypes.data_as(_dp), omf.ctypes.data_as(_dp), self.Mtot,
+            None if mo is None else mo.ctypes.data_as(_i64p), self.nslice, self.ncol,
+            _stream_ptr(stream)))
+        return h
+
+    def fft(self, x):
+        """X = st.fft(x) for a numpy image x[n1, n2, ...] (one column)."""
+        return nufft(x, self)
+
+    def adj(self, X):
+        """x = st.adj(X) for numpy samples X[M] (one column)."""
+        return nufft_adj(X, self)
+
+
+def newfft(om, Nd, **kw) -> NewfftPlan:
+    """st = newfft(om, Nd, 'Jd', ..., 'Kd', ..., 'n_shift', ..., 'mode', ...,
+    'oversample', ..., 'phasing', ...) in table mode; see NewfftPlan."""
+    if "oversample" in kw:
+        kw["Ld"] = kw.pop("oversample")
+    return NewfftPlan(om, Nd, **kw)
 
 
 # ---------------------------------------------------------------------------

@@ -1,0 +1,134 @@
+"""FP64 numpy restatement of MIRT's newfft in table mode (real KB kernel).
+
+TEST INFRASTRUCTURE ONLY.  Only tests/ and ``__graft_entry__.smoke()`` import
+this module, as the checker.  The product (mirt_b200) builds its own tables in
+C++ and never calls into oracle/.
+
+What is restated, with the reference lines followed:
+
+* ``Nmid``               nufft/newfft.m:146-151 (floor(N/2) for phasing 'real',
+  (N-1)/2 otherwise)
+* ``kb_table``           the 'ratio' table of nufft/private/newfft_table_init.m:
+  140-184 for ktype 'kb:minmax' (kernel nufft/kaiser_bessel.m:68-69,106-117 with
+  alpha = 2.34 J, kb_m = 0; the inline kernel string prints alpha with %g,
+  nufft/kaiser_bessel.m:80-82).  The table reads the sparse interpolator of a
+  fake N = J problem column by column (J:-1:1), which for a kernel of the
+  offset alone is the kernel sampled at t = -J/2 + i/L; the last entry
+  repeats the first (0 at |t| = J/2).
+* ``kb_scale``           1 / kaiser_bessel_ft((n - Nmid) / K, J, alpha, 0, 1),
+  nufft/newfft.m:352-356, outer product nufft/newfft.m:366-375
+* ``phase_before``       nufft/newfft.m:511-520
+* ``phase_after``        nufft/newfft.m:522-527
+* ``newfft_for/adj``     nufft/private/newfft_approx_for.m:15-63,
+  nufft/private/newfft_approx_adj.m:30-82, the interpolation through the
+  table kernels of oracle/interp_table.c (st.order from
+  nufft/private/newfft_table_init.m:40-49: 0 for 'table0' with L = 2^11,
+  1 for 'table1' with L = 2^9; phase_shift empty, :34).
+
+scipy.special.iv stands in for MATLAB's besseli.
+"""
+from __future__ import annotations
+
+import numpy as np
+from scipy import special
+
+import oracle
+from oracle import nufft_ref as nr
+
+
+def nmid_of(Nd, phasing="real"):
+    Nd = np.asarray(Nd, dtype=np.float64)
+    return np.floor(Nd / 2) if phasing == "real" else (Nd - 1) / 2
+
+
+def kb_alpha(J):
+    return 2.34 * J
+
+
+def kb_table(J: int, L: int) -> np.ndarray:
+    """Real [J*L+1] table of the 'kb:minmax' kernel (alpha printed with %g)."""
+    alpha = float(f"{kb_alpha(J):g}")
+    t = (np.arange(J * L + 1) - J * L / 2) / L
+    h = np.zeros(J * L + 1)
+    inside = np.abs(t) < J / 2
+    f = np.sqrt(1 - (t[inside] / (J / 2)) ** 2)
+    h[inside] = special.iv(0, alpha * f) / special.iv(0, alpha)
+    return h
+
+
+def kb_scale(N: int, J: int, K: int, Nmid: float) -> np.ndarray:
+    nc = np.arange(N) - Nmid
+    return 1.0 / nr.kaiser_bessel_ft(nc / K, J, kb_alpha(J), 0.0, 1)
+
+
+def phase_before(Kd, Nmid) -> np.ndarray:
+    """exp(i 2 pi sum_d k_d / K_d Nmid_d) over the grid [(Kd)]."""
+    ph = np.zeros(())
+    for K, m in zip(Kd, Nmid):
+        tmp = 2 * np.pi * np.arange(K) / K * m
+        ph = np.add.outer(ph, tmp) if ph.ndim else tmp
+    return np.exp(1j * ph)
+
+
+def newfft_init(om, Nd, Jd=None, Kd=None, n_shift=None, mode="table1", Ld=None,
+                phasing="real", h=None, sn=None) -> dict:
+    """st of newfft(om, Nd, 'Jd', Jd, 'Kd', Kd, 'n_shift', n_shift, 'mode', mode,
+    'oversample', Ld, 'phasing', phasing) with ktype 'kb:minmax' (or the
+    caller's tables h and scaling factors sn)."""
+    om = np.asarray(om, dtype=np.float64)
+    if om.ndim == 1:
+        om = om[:, None]
+    dd = len(Nd)
+    Jd = tuple([6] * dd if Jd is None else Jd)
+    Kd = tuple(2 * np.asarray(Nd) if Kd is None else Kd)
+    n_shift = np.zeros(dd) if n_shift is None else np.asarray(n_shift, dtype=np.float64)
+    order = {"table0": 0, "table1": 1}[mode]
+    if Ld is None:
+        Ld = 2 ** 11 if order == 0 else 2 ** 9
+    Ld = tuple(Ld if np.ndim(Ld) else [int(Ld)] * dd)
+    Nmid = nmid_of(Nd, phasing)
+    if h is None:
+        h = [kb_table(Jd[d], Ld[d]) for d in range(dd)]
+    if sn is None:
+        s = np.ones(1)
+        for d in range(dd):
+            s = np.outer(s.ravel(order="F"), kb_scale(Nd[d], Jd[d], Kd[d], Nmid[d]))
+        sn = s.reshape(tuple(Nd), order="F")
+    st = dict(om=om, Nd=tuple(Nd), Jd=Jd, Kd=Kd, Ld=Ld, order=order, Nmid=Nmid,
+              n_shift=n_shift, h=h, sn=np.asarray(sn).reshape(tuple(Nd), order="F"),
+              tm=np.stack([om[:, d] / (2 * np.pi / Kd[d]) for d in range(dd)], axis=1))
+    if phasing in ("real", "flipreal"):
+        st["phase_before"] = phase_before(Kd, Nmid)
+        st["phase_after"] = np.exp(1j * (om @ (n_shift - Nmid)))
+    else:
+        st["phase_before"] = None
+        st["phase_after"] = None
+    return st
+
+
+def newfft_for(x, st):
+    """X = st.fft(x) for one image x [(Nd)]."""
+    Nd, Kd = st["Nd"], st["Kd"]
+    x = np.asarray(x, dtype=np.complex128).reshape(Nd, order="F") * st["sn"]
+    Xk = np.fft.fftn(x, s=Kd, axes=tuple(range(len(Kd))))
+    if st["phase_before"] is not None:
+        Xk = Xk * st["phase_before"]
+    X = oracle.interp_for(Xk.ravel(order="F"), st["h"], st["Jd"], st["Ld"], st["tm"], Kd,
+                          st["order"])[:, 0]
+    if st["phase_after"] is not None:
+        X = X * st["phase_after"]
+    return X
+
+
+def newfft_adj(X, st):
+    """x = st.adj(X) for one column X [M]."""
+    Nd, Kd = st["Nd"], st["Kd"]
+    X = np.asarray(X, dtype=np.complex128)
+    if st["phase_after"] is not None:
+        X = X * np.conj(st["phase_after"])
+    Xk = oracle.interp_adj(X, st["h"], st["Jd"], st["Ld"], st["tm"], Kd,
+                           st["order"])[:, 0].reshape(Kd, order="F")
+    if st["phase_before"] is not None:
+        Xk = Xk * np.conj(st["phase_before"])
+    x = np.fft.ifftn(Xk, norm="forward")[tuple(slice(0, n) for n in Nd)]
+    return x * np.conj(st["sn"])

@@ -1,0 +1,133 @@
+"""GPU: newfft in table mode (mirt_newfft_create) against the FP64 oracle of
+newfft_approx_for / newfft_approx_adj (oracle/newfft_ref.py), and against the
+exact DTFT.
+
+Tolerances: forward and adjoint relative L2 <= 1e-5 against the oracle (FP32
+grid and accumulation, FP32 phase tables); the error against the exact DTFT
+stays within the oracle's own bounds (max percent difference, table0 0.12 %,
+table1 0.01 %), which the FP32 path must not widen.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import mirt_b200 as mb
+from mirt_b200 import workloads as wl
+from conftest import rel_l2
+from oracle import newfft_ref as nf
+from oracle import nufft_ref as nr
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5
+BOUND = {"table0": 0.12, "table1": 0.01}
+
+
+def _mpd(exact, approx):
+    return 100 * np.max(np.abs(approx - exact)) / np.max(np.abs(exact))
+
+
+@pytest.mark.parametrize("Nd", [(21,), (20,), (20, 10), (20, 10, 8)])
+@pytest.mark.parametrize("mode", ["table0", "table1"])
+def test_reference_selftest_setups(Nd, mode):
+    """The reference's self-test shapes: 100 samples with |om| up to 3 pi."""
+    rng = np.random.default_rng(0)
+    om = 3 * 2 * np.pi * (rng.random((100, len(Nd))) - 0.5)
+    x0 = rng.random(Nd)
+    st = mb.newfft(om, Nd, mode=mode)
+    so = nf.newfft_init(om, Nd, mode=mode)
+    X = st.fft(x0)
+    Xo = nf.newfft_for(x0, so)
+    assert rel_l2(X, Xo) <= TOL
+    xa = st.adj(Xo)
+    assert rel_l2(xa, nf.newfft_adj(Xo, so)) <= TOL
+    ns = np.zeros(len(Nd))
+    Xe = nr.dtft(x0, om, ns)
+    assert _mpd(Xe, X) < BOUND[mode]
+    assert _mpd(nr.dtft_adj(Xe, om, Nd, ns), st.adj(Xe)) < BOUND[mode]
+
+
+def test_batched_slices_coils_and_shift():
+    """Three trajectories of uneven length, 3 columns, centred image (n_shift =
+    N/2), table1: every slice and column against the oracle."""
+    import torch
+    rng = np.random.default_rng(5)
+    oms = [wl.ga_radial(30, 128), wl.vd_spiral(8, 300, 64, alpha=1.3), wl.vd_random(5000, rng)]
+    moff = np.concatenate([[0], np.cumsum([len(o) for o in oms])])
+    N, C = 64, 3
+    st = mb.newfft(np.concatenate(oms), (N, N), n_shift=(N / 2, N / 2), ncol=C,
+                   slice_moff=moff)
+    x = (rng.standard_normal(st.image_shape) + 1j * rng.standard_normal(st.image_shape))
+    Xd = st.forward(torch.from_numpy(x.astype(np.complex64)).cuda()).cpu().numpy()
+    Y = rng.standard_normal(st.sample_shape) + 1j * rng.standard_normal(st.sample_shape)
+    xd = st.adjoint(torch.from_numpy(Y.astype(np.complex64)).cuda()).cpu().numpy()
+    for s, om in enumerate(oms):
+        so = nf.newfft_init(om, (N, N), n_shift=(N / 2, N / 2))
+        for c in range(C):
+            Xo = nf.newfft_for(x[s, :, :, c].T, so)
+            assert rel_l2(Xd[moff[s]:moff[s + 1], c], Xo) <= TOL, (s, c)
+            xo = nf.newfft_adj(Y[moff[s]:moff[s + 1], c], so)
+            assert rel_l2(xd[s, :, :, c].T, xo) <= TOL, (s, c)
+
+
+def test_accuracy_128_against_exact():
+    """128 x 128 image, 8192 variable-density samples, n_shift = N/2: the
+    device result is as close to the exact DTFT as the FP64 table NUFFT."""
+    rng = np.random.default_rng(7)
+    N = 128
+    om = wl.vd_random(8192, rng)
+    x = wl.ellipses(N, 8, rng)
+    ns = np.array([N / 2, N / 2])
+    st = mb.newfft(om, (N, N), n_shift=ns)
+    Xe = nr.dtft(x, om, ns)
+    assert _mpd(Xe, st.fft(x)) < BOUND["table1"]
+
+
+def test_complex_tables_equal_nufft():
+    """phasing 'complex' with the min-max:KB tables and sn of nufft_init is the
+    NUFFT of mirt_nufft_create (no grid phase, exp(i om . n_shift) per sample)."""
+    import torch
+    rng = np.random.default_rng(2)
+    om = wl.ga_radial(40, 64)
+    Nd, Jd, Kd, Ld = (32, 32), (6, 6), (64, 64), (1024, 1024)
+    ns = (16, 16)
+    tabs = [mb.minmax_kb_table(Nd[d], Jd[d], Kd[d], Ld[d]) for d in range(2)]
+    s1 = [np.conj(mb.minmax_kb_scale(Nd[d], Jd[d], Kd[d])) for d in range(2)]
+    sn = np.outer(s1[0], s1[1]).ravel(order="F")
+    A = mb.newfft(om, Nd, Jd=Jd, Kd=Kd, n_shift=ns, mode="table0", Ld=Ld, phasing="complex",
+                  tables=tabs, sn=sn, ncol=2)
+    B = mb.NufftPlan(om, Nd, Jd, Kd, n_shift=ns, Ld=1024, ncol=2)
+    x = torch.randn(A.image_shape, dtype=torch.complex64, device="cuda")
+    Xa, Xb = A.forward(x), B.forward(x)
+    assert rel_l2(Xa.cpu().numpy(), Xb.cpu().numpy()) <= 1e-6
+    assert rel_l2(A.adjoint(Xb).cpu().numpy(), B.adjoint(Xb).cpu().numpy()) <= 1e-6
+
+
+def test_graph_capture_with_phases():
+    import torch
+    rng = np.random.default_rng(3)
+    om = wl.vd_random(3000, rng)
+    st = mb.newfft(om, (48, 48), n_shift=(24, 24), ncol=4)
+    x = torch.randn(st.image_shape, dtype=torch.complex64, device="cuda")
+    X = torch.empty(st.sample_shape, dtype=torch.complex64, device="cuda")
+    xa = torch.empty(st.image_shape, dtype=torch.complex64, device="cuda")
+    Xe = st.forward(x)
+    xe = st.adjoint(Xe)
+    g = st.capture(x, X, xa)
+    g.launch()
+    torch.cuda.synchronize()
+    assert torch.equal(X, Xe) and torch.equal(xa, xe)
+    g.close()
+
+
+def test_argument_errors():
+    om = wl.ga_radial(4, 32)
+    tabs = [mb.minmax_kb_table(16, 6, 32, 64)] * 2
+    with pytest.raises(mb.MirtError, match="only 0th order"):
+        mb.newfft(om, (16, 16), mode="table1", Ld=64, phasing="complex", tables=tabs,
+                  sn=np.ones(256))
+    with pytest.raises(ValueError, match="sn is required"):
+        mb.newfft(om, (16, 16), tables=[np.ones(6 * 512 + 1)] * 2)
+    with pytest.raises(ValueError, match="J\\*L\\+1"):
+        mb.newfft(om, (16, 16), tables=[np.ones(10)] * 2, sn=np.ones(256))

@@ -1,0 +1,79 @@
+"""newfft in table mode on the CPU: the oracle pinned against the exact DTFT
+on the reference's own self-test set-up (nufft/newfft.m:589-668: Nd = 21,
+20, [20 10], [20 10 8]; om = 3 * 2 pi (rand - 1/2), 100 samples; x0 = rand),
+and the library's host table builders against the oracle.
+
+The reference prints max_percent_diff against 'exact' without a threshold;
+the bounds here are about 3x the measured errors of the 'kb:minmax' tables
+(table0 L = 2^11: <= 0.04 %, table1 L = 2^9: <= 0.003 %).  A wrong phase
+convention or sign gives errors of order 100 %.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import mirt_b200 as mb
+from oracle import newfft_ref as nf
+from oracle import nufft_ref as nr
+
+ND_LIST = [(21,), (20,), (20, 10), (20, 10, 8)]
+BOUND = {"table0": 0.12, "table1": 0.01}       # percent of max |exact|
+
+
+def _mpd(exact, approx):
+    return 100 * np.max(np.abs(approx - exact)) / np.max(np.abs(exact))
+
+
+def _case(Nd, seed=0):
+    rng = np.random.default_rng(seed)
+    om = 3 * 2 * np.pi * (rng.random((100, len(Nd))) - 0.5)
+    return om, rng.random(Nd)
+
+
+@pytest.mark.parametrize("Nd", ND_LIST)
+@pytest.mark.parametrize("mode", ["table0", "table1"])
+def test_oracle_matches_exact_dtft(Nd, mode):
+    om, x0 = _case(Nd)
+    ns = np.zeros(len(Nd))
+    Xe = nr.dtft(x0, om, ns)
+    xe = nr.dtft_adj(Xe, om, Nd, ns)
+    st = nf.newfft_init(om, Nd, mode=mode)
+    assert _mpd(Xe, nf.newfft_for(x0, st)) < BOUND[mode]
+    assert _mpd(xe, nf.newfft_adj(Xe, st)) < BOUND[mode]
+
+
+def test_oracle_n_shift_and_phasing():
+    """n_shift = Nd/2 (centred image) with 'real' phasing (Nmid = floor(N/2)),
+    and odd N where Nmid differs from (N-1)/2 only for even N."""
+    for Nd in [(20, 10), (21, 9)]:
+        om, x0 = _case(Nd, 1)
+        ns = np.asarray(Nd) / 2
+        st = nf.newfft_init(om, Nd, n_shift=ns)
+        assert _mpd(nr.dtft(x0, om, ns), nf.newfft_for(x0, st)) < BOUND["table1"]
+    assert list(nf.nmid_of((20, 21))) == [10, 10]
+    assert list(nf.nmid_of((20, 21), "complex")) == [9.5, 10]
+
+
+@pytest.mark.parametrize("J,L", [(6, 512), (6, 2048), (5, 7), (8, 64), (2, 1)])
+def test_kb_table_builder(J, L):
+    h = mb.newfft_kb_table(J, L)
+    ref = nf.kb_table(J, L)
+    assert h.shape == (J * L + 1,)
+    assert np.max(np.abs(h - ref)) <= 1e-13
+    assert h[0] == 0 and h[-1] == 0 and np.allclose(h, h[::-1], atol=1e-15)
+
+
+@pytest.mark.parametrize("N,J,K,nmid", [(20, 6, 40, 10), (21, 6, 42, 10), (64, 6, 128, 32),
+                                        (10, 4, 17, 4.5)])
+def test_kb_scale_builder(N, J, K, nmid):
+    s = mb.newfft_kb_scale(N, J, K, nmid)
+    ref = nf.kb_scale(N, J, K, nmid)
+    assert np.max(np.abs(s - ref) / np.abs(ref)) <= 1e-12
+
+
+def test_builder_argument_errors():
+    with pytest.raises(mb.MirtError, match="J must be"):
+        mb.newfft_kb_table(0, 16)
+    with pytest.raises(mb.MirtError, match="positive"):
+        mb.newfft_kb_scale(0, 6, 12, 0.0)
