@@ -455,8 +455,13 @@ def run_gpu(args, w):
                "sample": f"{ns} of {plan.nslice} slices, forward + adjoint, {C} coils "
                          f"({u:.3g} sample-coils in {tc:.1f} s)"}
 
-    # deapod_pad, 2 transposes, gather, spread, [spread_reduce], crop_deapod (cuFFT not counted)
-    launches_per_step = 6 + (1 if tuned.get("spread_reductions", 0) > 0 else 0)
+    # deapod_pad, 2 transposes, gather, crop_deapod (cuFFT not counted), and the spread:
+    # row sweep = sample ordering + sweep; tiled = spread [+ reductions]
+    if tuned.get("spread_sweep", 0) > 0:
+        spread_launches = 2
+    else:
+        spread_launches = 1 + (1 if tuned.get("spread_reductions", 0) > 0 else 0)
+    launches_per_step = 5 + spread_launches
     cg = None
     if rank == 0 and world == 1 and not args.no_cg and w["D"] == 2:
         cg = run_cgsense(args)

@@ -193,11 +193,12 @@ int mirt_interp_plan_adjoint(mirt_interp_plan *plan, const void *fm, void *ck, v
  * bitwise deterministic for any choice. */
 int mirt_interp_plan_autotune(mirt_interp_plan *plan, void *stream);
 
-/* Current launch configuration: up to 18 values
+/* Current launch configuration: up to 20 values
  * {T1, T2, T3, spread threads, spread heavy-first order, coil lanes,
  *  gather threads, (unused), gather CTAs, B1, B2, B3, split chunk,
  *  spread tasks, spare tile columns, partial-tile reductions,
- *  spread shared-tile atomics, ownership spread}. */
+ *  spread shared-tile atomics, ownership spread, row-sweep segments (0: off),
+ *  row-sweep rows per band}. */
 int mirt_interp_plan_config(mirt_interp_plan *plan, int32_t *out, int32_t n);
 
 /* Adjoint accumulation order.  deterministic = 1 (the default): every
@@ -217,6 +218,18 @@ int mirt_interp_plan_set_deterministic(mirt_interp_plan *plan, int32_t determini
  * (the last >= 5 points) per dimension; else MIRT_ERR_ARG.  The autotuner
  * tries it where it applies.  No reference counterpart. */
 int mirt_interp_plan_set_ownership(mirt_interp_plan *plan, int32_t own, void *stream);
+
+/* Row-sweep spread (2D, J = 6, K >= 6 per dimension): lanes of one coil
+ * chunk own a band of `rows` grid rows (1, 2 or 4) and one of `segments`
+ * segments of their columns, and sweep the bin columns of the rows + 5 bin
+ * rows whose samples reach the band, with six grid columns of accumulators
+ * per row in registers; each grid point is written once, summed in a fixed
+ * order that does not depend on rows or segments (deterministic), with no
+ * tiles, shared memory or reduction launches.  segments: 1..K1 (more
+ * segments, more parallel teams, five warm-up columns each); 0 returns to
+ * the tiled spread.  MIRT_ERR_ARG where it does not apply.  The autotuner
+ * tries it where it applies.  No reference counterpart. */
+int mirt_interp_plan_set_sweep(mirt_interp_plan *plan, int32_t segments, int32_t rows);
 
 /* Fix the spread's tiling instead of autotuning it: tile extents T[0..D-1]
  * (multiples of the sort bins B of mirt_interp_plan_config, at most the grid

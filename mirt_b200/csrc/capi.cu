@@ -159,6 +159,25 @@ int own_ok(const InterpArgs &a, const Tiling &t) {
   return 1;
 }
 
+// The row-sweep spread needs: 2D, J = 6, one-point bins, K >= J per dimension
+// (each bin row and column reaches a grid row or column through one tap).
+int sweep_ok(const InterpArgs &a, const Tiling &t) {
+  if (a.g.D != 2) return 0;
+  for (int d = 0; d < 2; d++)
+    if (a.g.J[d] != 6 || t.B[d] != 1 || a.g.K[d] < 6) return 0;
+  return 1;
+}
+
+// The row sweep's copy of the samples in plan order (allocated when the sweep
+// is first selected, outside any launch).
+int sweep_buffer(mirt_interp_plan *P) {
+  const size_t bytes = (size_t)std::max<long long>(P->a.Mtot, 1) * std::max(P->a.C, 1) *
+                       sizeof(float2);
+  if (P->swept.bytes < bytes) CK(P->swept.alloc(bytes));
+  P->t.sorted = P->swept.as<float2>();
+  return MIRT_OK;
+}
+
 int wrap_ok(const InterpArgs &a, const Tiling &t) {
   for (int d = 0; d < a.g.D; d++)
     if (a.g.K[d] < t.T[d] + a.g.J[d]) return 0;
@@ -205,6 +224,9 @@ void choose_config(mirt_interp_plan *P) {
   // no spare tile columns by default; the autotuner also tries J1 - 1
   t.padc = 0;
   t.own = 0;
+  t.sweep = 0;
+  t.sweep_rows = 1;
+  t.sorted = nullptr;
   t.nbins = 1;
   t.ntiles = 1;
   for (int d = 0; d < MIRT_DMAX; d++) {
@@ -582,6 +604,17 @@ int plan_finish(mirt_interp_plan *P, long long Mtot, const long long *moff, int 
   int rc2 = build_tasks(P, st);
   if (rc2) return rc2;
   CK(query_gather_grid(a, P->lg));
+  // 2D, J = 6, 32-coil chunks: the row sweep by default, two rows per band,
+  // rows split into segments (of at least 32 columns) until about 32k teams
+  if (sweep_ok(a, P->t) && P->ls.cw == 32) {
+    int nseg = 1;
+    const long long bands = (long long)nslice * ((a.g.K[1] + 1) / 2);
+    while (bands * nseg < 32768 && a.g.K[0] / (2 * nseg) >= 32) nseg *= 2;
+    int rc3 = sweep_buffer(P);
+    if (rc3) return rc3;
+    P->t.sweep = nseg;
+    P->t.sweep_rows = 2;
+  }
   return MIRT_OK;
 }
 
@@ -605,7 +638,7 @@ int set_spread_tiles(mirt_interp_plan *P, const int *T, cudaStream_t st) {
 
 struct SpreadCand {
   int T[MIRT_DMAX];
-  int threads, padc, atomic, own;
+  int threads, padc, atomic, own, sweep, sweep_rows;
 };
 
 // spare columns the J = 6 row update can use (0 elsewhere)
@@ -763,7 +796,7 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
     const int npc = pmax ? 2 : 1;
     for (int ip = 0; ip < npc; ip++) {
       const int pc = ip ? pmax : 0;
-      SpreadCand c{{t0, t1, t2}, threads, pc, 0, 0};
+      SpreadCand c{{t0, t1, t2}, threads, pc, 0, 0, 0, 1};
       for (int d = 0; d < D; d++) {
         const int kr = (a.g.K[d] + P->t.B[d] - 1) / P->t.B[d] * P->t.B[d];
         if (c.T[d] > kr) c.T[d] = kr;
@@ -791,7 +824,7 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
       const size_t pts = (size_t)(t0 + 5) * (t1 + 5);
       if (own_ok(a, tt) && pts * cw * 8 <= 160 * 1024 && threads == 32)
         for (int th = 32; th <= 256 && th / 32 <= t1 + 5; th *= 2)
-          cands.push_back(SpreadCand{{t0, t1, 1}, th, 0, 0, 1});
+          cands.push_back(SpreadCand{{t0, t1, 1}, th, 0, 0, 1, 0, 1});
     }
   };
   if (D == 1) {
@@ -809,10 +842,19 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
         for (int t2 : {8, 16})
           for (int th = 32; th <= 256 && th / 32 <= t2; th *= 2) add(t0, t1, t2, th);
   }
+  // row sweep (no tiles): bands of 1, 2 or 4 rows, whole rows or segments of
+  // at least 32 columns
+  if (sweep_ok(a, P->t) && sweep_buffer(P) == MIRT_OK)
+    for (int rows : {1, 2, 4})
+      for (int nseg = 1; nseg <= 16 && (nseg == 1 || a.g.K[0] / nseg >= 32); nseg *= 2)
+        cands.push_back(SpreadCand{{P->t.T[0], P->t.T[1], P->t.T[2]}, P->ls.threads, 0, 0, 0,
+                                   nseg, rows});
   SpreadCand best{};
   float best_ms = 1e30f;
   for (const SpreadCand &c : cands) {
     P->t.own = c.own;
+    P->t.sweep = c.sweep;
+    P->t.sweep_rows = c.sweep_rows;
     int rc = set_spread_tiles(P, c.T, st);
     if (rc) continue;
     P->ls.threads = c.threads;
@@ -831,6 +873,8 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
   }
   if (best_ms < 1e30f) {
     P->t.own = best.own;
+    P->t.sweep = best.sweep;
+    P->t.sweep_rows = best.sweep_rows;
     int rc = set_spread_tiles(P, best.T, st);
     if (rc) return rc;
     P->ls.threads = best.threads;
@@ -838,7 +882,7 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
     P->ls.atomic = best.atomic;
   }
   // split size of heavy tiles (sample visits per spread task)
-  {
+  if (!P->t.sweep) {
     int best_chunk = P->split_chunk;
     float bc_ms = 1e30f;
     for (int chunk : {256, 512, 1024, 2048, 4096, 16384}) {
@@ -899,11 +943,32 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
 
 int mirt_interp_plan_config(mirt_interp_plan *P, int32_t *out, int32_t n) {
   if (!P || !out) return fail(MIRT_ERR_ARG, "NULL argument");
-  const int32_t v[18] = {P->t.T[0], P->t.T[1], P->t.T[2], P->ls.threads, P->heavy_first, P->ls.cw,
+  const int32_t v[20] = {P->t.T[0], P->t.T[1], P->t.T[2], P->ls.threads, P->heavy_first, P->ls.cw,
                          P->lg.threads, P->lg.sb, P->lg.grid, P->t.B[0], P->t.B[1], P->t.B[2],
                          P->split_chunk, P->t.ntask, P->t.padc, P->t.nred, P->ls.atomic,
-                         P->t.own};
-  for (int i = 0; i < n && i < 18; i++) out[i] = v[i];
+                         P->t.own, P->t.sweep, P->t.sweep_rows};
+  for (int i = 0; i < n && i < 20; i++) out[i] = v[i];
+  return MIRT_OK;
+}
+
+int mirt_interp_plan_set_sweep(mirt_interp_plan *P, int32_t segments, int32_t rows) {
+  if (!P) return fail(MIRT_ERR_ARG, "plan is NULL");
+  if (segments && !sweep_ok(P->a, P->t))
+    return fail(MIRT_ERR_ARG, "row-sweep spread needs 2D, J = 6 and K >= 6 per dimension");
+  if (segments < 0 || (segments > 0 && segments > P->a.g.K[0]))
+    return fail(MIRT_ERR_ARG, "row-sweep segments must be in 1..K1 (0: off)");
+  if (segments && rows != 1 && rows != 2 && rows != 4)
+    return fail(MIRT_ERR_ARG, "row-sweep rows per band must be 1, 2 or 4");
+  if (segments) {
+    int rc = sweep_buffer(P);
+    if (rc) return rc;
+  }
+  P->t.sweep = segments;
+  if (segments) P->t.sweep_rows = rows;
+  if (segments) {
+    P->t.own = 0;
+    P->ls.atomic = 0;
+  }
   return MIRT_OK;
 }
 
@@ -913,7 +978,10 @@ int mirt_interp_plan_set_ownership(mirt_interp_plan *P, int32_t own, void *strea
     return fail(MIRT_ERR_ARG, "ownership spread needs 2D, J = 6, tiles of >= 5 points and an "
                               "even number of tiles (last one >= 5 points) per dimension");
   P->t.own = own ? 1 : 0;
-  if (own) P->ls.atomic = 0;
+  if (own) {
+    P->ls.atomic = 0;
+    P->t.sweep = 0;
+  }
   int T[MIRT_DMAX] = {P->t.T[0], P->t.T[1], P->t.T[2]};
   int rc = set_spread_tiles(P, T, as_stream(stream));
   if (rc) return rc;
@@ -957,6 +1025,7 @@ int mirt_interp_plan_set_spread(mirt_interp_plan *P, const int32_t *T, int32_t t
   cudaStream_t st = as_stream(stream);
   P->t.padc = padc;
   P->ls.threads = threads;
+  P->t.sweep = 0;
   int rc = set_spread_tiles(P, Tn, st);
   if (rc) return rc;
   CK(cudaStreamSynchronize(st));

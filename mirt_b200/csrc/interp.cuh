@@ -53,6 +53,16 @@ struct Tiling {
   // sorted by colour: colour c is tasks [color_beg[c], color_beg[c+1]) and
   // reductions [red_beg[c], red_beg[c+1]).
   int own;
+  // Row-sweep spread (2D, J = 6, one-point bins, K1, K2 >= 6): a team of
+  // lanes owns a band of sweep_rows grid rows (1, 2 or 4) and one of `sweep`
+  // segments of their columns, and sweeps the bin columns of the bin rows
+  // that reach the band, with six grid columns of accumulators per row in
+  // registers; every grid point is written once, in a fixed summation order.
+  // No tiles, shared memory or reductions (the tiling fields are unused).
+  // sweep = 0: the tiled spread.
+  int sweep;
+  int sweep_rows;
+  float2 *sorted;        // row sweep: [Mtot][C] samples in plan order times conj(phase)
   int color_beg[9];
   int red_beg[9];
   int padc;              // spread: spare columns on each side of a tile row in

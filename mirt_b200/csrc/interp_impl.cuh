@@ -652,6 +652,125 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t,
   }
 }
 
+// Row-sweep spread (2D, J = 6 in both dimensions, one-point bins, K1, K2 >= 6).
+// A team of CW lanes (lane = coil) owns a band of R grid rows y0 .. y0 + R - 1
+// (rows past K2 - 1 in the last band are computed and dropped) and a segment
+// [x0, x1) of their columns, of one slice and coil chunk.  The samples with a
+// tap in the band are those binned (by their wrapped first tap) in bin rows
+// y0 - 5 + q, q = 0 .. R + 4 (modulo K2); bin row q reaches band row r through
+// tap row j2 = r - q + 5 when 0 <= j2 < 6, a static set per q.  The team sweeps
+// bin columns xb = x0 - 5 .. x1 - 1 (modulo K1: five warm-up columns, wrapped
+// when x0 < 5) and keeps the accumulators of grid columns xb .. xb + 5 of its R
+// rows in registers; after bin column xb, column xb has all its contributions
+// and is stored if it lies in the segment.  Summation order per grid point:
+// bin columns ascending, bin rows ascending, samples in the stable sort order
+// -- fixed, and the same for every R and segmentation, so the result is
+// bitwise reproducible and independent of both.
+// sorted[p][c] = conj(phase[p]) fm[perm[p]][c]: the samples in plan order, so
+// that the sweep reads each bin's samples as one contiguous block.
+template <int CW>
+__global__ void __launch_bounds__(256) sweep_order_kernel(InterpArgs a, const float2 *__restrict__ fm,
+                                                          float2 *__restrict__ sorted) {
+  const long long n = a.Mtot * (long long)a.C;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long p = e / a.C;
+    const int c = (int)(e - p * a.C);
+    const int m = a.perm ? __ldg(a.perm + p) : (int)p;
+    float2 v = __ldg(fm + (long long)m * a.C + c);
+    if (a.phase) v = cmulc(__ldg(a.phase + p), v);
+    sorted[e] = v;
+  }
+}
+
+template <int CW, int R, bool REAL>
+__global__ void __launch_bounds__(256) spread_sweep_kernel(InterpArgs a, Tiling t,
+                                                           const int *__restrict__ bin_start,
+                                                           const float2 *__restrict__ fs,
+                                                           float2 *__restrict__ ck) {
+  constexpr int NQ = R + 5;  // bin rows reaching the band
+  const int K1 = a.g.K[0], K2 = a.g.K[1];
+  const int nseg = t.sweep;
+  const int nband = (K2 + R - 1) / R;
+  const long long team = ((long long)blockIdx.x * blockDim.x + threadIdx.x) / CW;
+  if (team >= (long long)t.nslice * nband * nseg) return;  // the team's lanes leave together
+  const int seg = (int)(team % nseg);
+  const long long bandid = team / nseg;
+  const int slice = (int)(bandid / nband);
+  const int y0 = (int)(bandid - (long long)slice * nband) * R;
+  const int sw = (K1 + nseg - 1) / nseg;
+  const int x0 = seg * sw, x1 = min(K1, x0 + sw);
+  if (x0 >= x1) return;
+  const int C = a.C;
+  const int c = blockIdx.y * CW + (int)(threadIdx.x % CW);
+  const bool on = c < C;
+  const int *bs = bin_start + (long long)slice * t.nbins;
+  int row[NQ];
+#pragma unroll
+  for (int q = 0; q < NQ; q++) {
+    int b = (y0 - 5 + q) % K2;
+    if (b < 0) b += K2;
+    row[q] = b * K1;  // one-point bins: K1 bins per row
+  }
+  const int xs = x0 - 5;
+  int beg[NQ];
+#pragma unroll
+  for (int q = 0; q < NQ; q++) beg[q] = __ldg(bs + row[q] + (xs < 0 ? xs + K1 : xs));
+  float2 acc[R][6];
+#pragma unroll
+  for (int r = 0; r < R; r++)
+#pragma unroll
+    for (int j = 0; j < 6; j++) acc[r][j] = make_float2(0.f, 0.f);
+  float2 *out = ck + (long long)slice * a.grid_elems + (long long)y0 * K1 * C + c;
+  for (int xb = xs; xb < x1; xb++) {
+    const int xw = xb < 0 ? xb + K1 : xb;
+    if (xb == 0 && xs < 0) {
+#pragma unroll
+      for (int q = 0; q < NQ; q++) beg[q] = __ldg(bs + row[q]);
+    }
+    int end[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; q++) end[q] = __ldg(bs + row[q] + xw + 1);
+#pragma unroll
+    for (int q = 0; q < NQ; q++) {
+      for (int p = beg[q]; p < end[q]; p++) {
+        const float2 f = on ? __ldg(fs + (long long)p * C + c) : make_float2(0.f, 0.f);
+        const float2 *Ws = a.W + (long long)p * 12;
+        const float4 *W4 = reinterpret_cast<const float4 *>(Ws);
+        float4 w1[3];
+#pragma unroll
+        for (int h = 0; h < 3; h++) w1[h] = __ldg(W4 + h);
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+          const int j2 = r - q + 5;  // compile-time after unrolling
+          if (j2 >= 0 && j2 < 6) {
+            const float2 v = cw_mul<REAL>(__ldg(Ws + 6 + j2), f);
+            const float2 vs = make_float2(v.y, v.x);
+#pragma unroll
+            for (int h = 0; h < 3; h++) {
+              acc[r][2 * h] = cw_fma<REAL>(make_float2(w1[h].x, w1[h].y), v, vs, acc[r][2 * h]);
+              acc[r][2 * h + 1] =
+                  cw_fma<REAL>(make_float2(w1[h].z, w1[h].w), v, vs, acc[r][2 * h + 1]);
+            }
+          }
+        }
+      }
+      beg[q] = end[q];
+    }
+    if (xb >= x0 && on) {
+#pragma unroll
+      for (int r = 0; r < R; r++)
+        if (y0 + r < K2) out[((long long)r * K1 + xb) * C] = acc[r][0];
+    }
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+#pragma unroll
+      for (int j = 0; j < 5; j++) acc[r][j] = acc[r][j + 1];
+      acc[r][5] = make_float2(0.f, 0.f);
+    }
+  }
+}
+
 // Sum the partial tiles of each split heavy tile, in slot order, into the grid.
 template <int D, int CW>
 __global__ void __launch_bounds__(256) spread_reduce_kernel(InterpArgs a, Tiling t,
@@ -931,6 +1050,38 @@ cudaError_t run(Req &r) {
     const Tiling &t = *r.t;
     const size_t sm = spread_smem_bytes(a, t, l);
     if constexpr (D == 2 && JT == 6) {
+      if (t.sweep > 0) {
+        const long long nband = (a.g.K[1] + t.sweep_rows - 1) / max(t.sweep_rows, 1);
+        const long long teams = (long long)t.nslice * nband * t.sweep;
+        const long long thr = teams * CW;
+        const unsigned nchunk = (unsigned)((a.C + CW - 1) / CW);
+        if (thr == 0) return cudaSuccess;
+        if (!t.sorted) return cudaErrorInvalidValue;
+        {
+          const long long n = a.Mtot * (long long)a.C;
+          long long nb = (n + 255) / 256;
+          if (nb > 148 * 16) nb = 148 * 16;
+          if (n > 0) sweep_order_kernel<CW><<<(unsigned)nb, 256, 0, r.st>>>(a, r.in, t.sorted);
+          cudaError_t e = cudaGetLastError();
+          if (e != cudaSuccess) return e;
+        }
+        const dim3 grid((unsigned)((thr + 255) / 256), nchunk);
+        const float2 *fs = t.sorted;
+        switch (t.sweep_rows) {
+          case 1:
+            spread_sweep_kernel<CW, 1, REAL><<<grid, 256, 0, r.st>>>(a, t, r.bin_start, fs, r.out);
+            break;
+          case 2:
+            spread_sweep_kernel<CW, 2, REAL><<<grid, 256, 0, r.st>>>(a, t, r.bin_start, fs, r.out);
+            break;
+          case 4:
+            spread_sweep_kernel<CW, 4, REAL><<<grid, 256, 0, r.st>>>(a, t, r.bin_start, fs, r.out);
+            break;
+          default:
+            return cudaErrorInvalidValue;
+        }
+        return cudaGetLastError();
+      }
       if (t.own) {
         // cleared grid, then one launch (and one reduction) per colour
         auto kern = spread_own_kernel<CW, REAL>;

@@ -66,13 +66,14 @@ def minmax_kb_scale(N: int, J: int, K: int) -> np.ndarray:
 
 
 def _plan_config(lib, handle) -> dict:
-    v = (C.c_int32 * 18)()
-    check(lib.mirt_interp_plan_config(handle, v, 18))
+    v = (C.c_int32 * 20)()
+    check(lib.mirt_interp_plan_config(handle, v, 20))
     return {"spread_tile": [v[0], v[1], v[2]], "spread_threads": v[3], "spread_heavy_first": v[4],
             "coil_lanes": v[5], "gather_threads": v[6],
             "gather_ctas": v[8], "sort_bin": [v[9], v[10], v[11]], "split_chunk": v[12],
             "spread_tasks": v[13], "spread_padc": v[14], "spread_reductions": v[15],
-            "spread_atomic": v[16], "spread_own": v[17]}
+            "spread_atomic": v[16], "spread_own": v[17], "spread_sweep": v[18],
+            "spread_sweep_rows": v[19]}
 
 
 class InterpPlan:
@@ -164,6 +165,13 @@ class InterpPlan:
                                                       _stream_ptr(stream)))
         return self.config()
 
+    def set_sweep(self, segments=1, rows=4):
+        """Row-sweep spread (2D, J = 6; see mirt_interp_plan_set_sweep):
+        segments per grid row (True = 1; 0 / False = tiled spread) and grid
+        rows per band (1, 2 or 4)."""
+        check(self.lib.mirt_interp_plan_set_sweep(self.handle, int(segments), int(rows)))
+        return self.config()
+
     def set_spread(self, tile, threads=32, padc=0, stream=None):
         """Fix the spread tiling (tile extents per dimension, CTA size, spare
         tile columns 0 or J1 - 1) instead of autotuning it."""
@@ -252,6 +260,12 @@ class NufftPlan:
         """See InterpPlan.set_deterministic."""
         check(self.lib.mirt_interp_plan_set_deterministic(
             self.lib.mirt_nufft_interp_plan(self.handle), int(bool(deterministic))))
+        return self.config()
+
+    def set_sweep(self, segments=1, rows=4):
+        """See InterpPlan.set_sweep."""
+        check(self.lib.mirt_interp_plan_set_sweep(
+            self.lib.mirt_nufft_interp_plan(self.handle), int(segments), int(rows)))
         return self.config()
 
     def capture(self, x=None, X=None, xa=None):

@@ -351,3 +351,80 @@ def test_ownership_spread_refused_where_colours_would_overlap():
     with pytest.raises(mb.MirtError, match="even number of tiles"):
         plan.set_ownership(True)
     plan.close()
+
+
+@pytest.mark.parametrize("C", [1, 3, 8, 32, 40])
+def test_sweep_spread_matches_oracle(C):
+    """Row-sweep spread (2D, J = 6): three slices (one dense, one with
+    coordinates far outside the grid, wrapping several times), a partial
+    coil chunk at C = 3 and 40, bands of 1, 2 and 4 rows, whole rows and row
+    segments down to one column (K1 = 96 in 5 segments: a shorter last one); the oracle's adjoint, bitwise reproducible and
+    independent of bands and segments, and the tiled spread's result to FP32
+    rounding (another summation order)."""
+    import torch
+    rng = np.random.default_rng(171 + C)
+    K, J, L = [96, 64], [6, 6], [1024, 1024]
+    h = [mb.minmax_kb_table(48, 6, 96, 1024), mb.minmax_kb_table(32, 6, 64, 1024)]
+    tms = [rng.uniform(-60, 60, (1500, 2)), rng.uniform(-3, 3, (5000, 2)),
+           rng.uniform(-300, 300, (800, 2))]
+    moff = np.concatenate([[0], np.cumsum([len(t) for t in tms])])
+    tm = np.concatenate(tms)
+    plan = mb.InterpPlan(K, J, L, h, tm, C, slice_moff=moff)
+    fm = rng.standard_normal((len(tm), C)) + 1j * rng.standard_normal((len(tm), C))
+    fm_d = torch.from_numpy(fm.astype(np.complex64)).cuda()
+    assert plan.config()["spread_sweep"] == (2 if C >= 32 else 0)   # the default for 32 coils
+    plan.set_sweep(0)
+    tiled = plan.adjoint(fm_d).cpu().numpy()
+    refs = [oracle.interp_adj(fm[moff[s]:moff[s + 1]], h, J, L, tms[s], K, 0, impl=ref_impl())
+            for s in range(3)]
+    first = None
+    for nseg, rows in [(1, 1), (3, 2), (16, 4), (96, 4), (1, 4), (5, 2)]:   # segments of 96 .. 1 columns
+        cfg = plan.set_sweep(nseg, rows)
+        assert cfg["spread_sweep"] == nseg and cfg["spread_sweep_rows"] == rows
+        out = plan.adjoint(fm_d).cpu().numpy()
+        for s in range(3):
+            got = np.transpose(out[s], (1, 0, 2)).reshape(-1, C, order="F")
+            assert rel_l2(got, refs[s]) <= ADJ_TOL, (nseg, rows, s)
+        assert np.array_equal(out, plan.adjoint(fm_d).cpu().numpy())
+        assert rel_l2(out, tiled) <= 5e-6      # two FP32 summation orders
+        if first is None:
+            first = out
+        assert np.array_equal(out, first)      # neither segments nor bands change the sums
+    with pytest.raises(mb.MirtError, match="segments"):
+        plan.set_sweep(97)
+    with pytest.raises(mb.MirtError, match="rows per band"):
+        plan.set_sweep(1, 3)
+    plan.set_sweep(False)
+    assert np.array_equal(plan.adjoint(fm_d).cpu().numpy(), tiled)
+    plan.close()
+
+
+@pytest.mark.parametrize("order", [0, 1])
+def test_sweep_spread_real_tables_phase_small_grid(order):
+    """Real tables (order 0 and 1) with a per-sample phase, on grids down to
+    K = 6 x 7 where every tap row and column wraps; bands of 2 and 4 rows
+    with a partial last band (K2 = 7, 9)."""
+    import torch
+    rng = np.random.default_rng(5 + order)
+    for K in ([6, 7], [12, 9], [40, 24]):
+        J, L = [6, 6], [64, 64]
+        h = [np.cos(np.linspace(-1.2, 1.2, 6 * 64 + 1)), np.exp(-np.linspace(-2, 2, 6 * 64 + 1) ** 2)]
+        tm = rng.uniform(-20, 20, (700, 2))
+        ph = np.exp(1j * rng.uniform(-np.pi, np.pi, len(tm)))
+        C = 4
+        plan = mb.InterpPlan(K, J, L, h, tm, C, order=order, phase=ph)
+        plan.set_sweep(1, 4 if K[1] > 7 else 2)
+        fm = rng.standard_normal((len(tm), C)) + 1j * rng.standard_normal((len(tm), C))
+        got = plan.adjoint(torch.from_numpy(fm.astype(np.complex64)).cuda()).cpu().numpy()[0]
+        got = np.transpose(got, (1, 0, 2)).reshape(-1, C, order="F")
+        ref = oracle.interp_adj(fm * np.conj(ph)[:, None], h, J, L, tm, K, order, impl=ref_impl())
+        assert rel_l2(got, ref) <= ADJ_TOL, K
+        plan.close()
+
+
+def test_sweep_spread_refused_where_it_does_not_apply():
+    h = [mb.minmax_kb_table(8, 4, 16, 64)] * 2
+    plan = mb.InterpPlan([16, 16], [4, 4], [64, 64], h, np.zeros((10, 2)), 2)
+    with pytest.raises(mb.MirtError, match="row-sweep"):
+        plan.set_sweep(True)
+    plan.close()
