@@ -155,12 +155,13 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def traffic_from_profiles(kernel, workload):
-    """dram bytes per launch recorded from an ncu capture (profiles/traffic.json)."""
+def traffic_from_profiles(call, workload, variant):
+    """DRAM bytes of one gather or spread call (the sum over its kernels) recorded
+    from an ncu capture (profiles/traffic.json), for the plan's spread variant."""
     try:
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
             t = json.load(f)
-        return t.get(workload, {}).get(kernel)
+        return t.get(workload, {}).get(call if call == "gather" else f"spread_{variant}")
     except (OSError, ValueError):
         return None
 
@@ -409,9 +410,13 @@ def run_gpu(args, w):
     peak, peak_kind = measured_peak()
     dom, tdom = ("spread", t_spread) if t_spread >= t_gather else ("gather", t_gather)
     achieved = B / tdom / 1e9
-    roof = {"bound": "hbm", "kernel": f"{dom}_kernel", "achieved": achieved, "peak": peak,
+    variant = "sweep" if tuned.get("spread_sweep", 0) > 0 else "tiled"
+    kernels = {"gather": "gather_kernel",
+               "spread": ("sweep_order_kernel + spread_sweep_kernel" if variant == "sweep"
+                          else "spread_kernel (+ spread_reduce_kernel)")}
+    roof = {"bound": "hbm", "kernel": kernels[dom], "achieved": achieved, "peak": peak,
             "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
-            "traffic": traffic_from_profiles(f"{dom}_kernel", args.workload),
+            "traffic": traffic_from_profiles(dom, args.workload, variant),
             "algorithmic_bytes": B,
             "gather": {"ms": 1e3 * t_gather, "GBps": B / t_gather / 1e9,
                        "frac": B / t_gather / 1e9 / peak},
@@ -455,13 +460,14 @@ def run_gpu(args, w):
                "sample": f"{ns} of {plan.nslice} slices, forward + adjoint, {C} coils "
                          f"({u:.3g} sample-coils in {tc:.1f} s)"}
 
-    # deapod_pad, 2 transposes, gather, crop_deapod (cuFFT not counted), and the spread:
-    # row sweep = sample ordering + sweep; tiled = spread [+ reductions]
+    # deapodise, forward transpose, gather, crop (cuFFT not counted), and the spread:
+    # row sweep = sample ordering + sweep into the coil-major grid; tiled = spread
+    # [+ reductions] + the adjoint transpose
     if tuned.get("spread_sweep", 0) > 0:
         spread_launches = 2
     else:
-        spread_launches = 1 + (1 if tuned.get("spread_reductions", 0) > 0 else 0)
-    launches_per_step = 5 + spread_launches
+        spread_launches = 2 + (1 if tuned.get("spread_reductions", 0) > 0 else 0)
+    launches_per_step = 4 + spread_launches
     cg = None
     if rank == 0 and world == 1 and not args.no_cg and w["D"] == 2:
         cg = run_cgsense(args)

@@ -227,6 +227,9 @@ void choose_config(mirt_interp_plan *P) {
   t.sweep = 0;
   t.sweep_rows = 1;
   t.sorted = nullptr;
+  t.slice0 = 0;
+  t.pos0 = 0;
+  t.npos = -1;
   t.nbins = 1;
   t.ntiles = 1;
   for (int d = 0; d < MIRT_DMAX; d++) {
@@ -1435,11 +1438,13 @@ namespace {
       return fail(MIRT_ERR_FFT, std::string(#call) + " failed: " + std::to_string((int)r_)); \
   } while (0)
 
-// one batched C2C execution over every slice and coil of the coil-major grid
+// one batched C2C execution over every slice and coil of the coil-major grid:
+// forward out of place from the zero-padded input, inverse in place
 int nufft_fft(mirt_nufft *p, int dir, cudaStream_t st) {
   CF(cufftSetStream(p->fft, st));
   cufftComplex *g = reinterpret_cast<cufftComplex *>(p->grid_cm.as<float2>());
-  CF(cufftExecC2C(p->fft, g, g, dir));
+  cufftComplex *src = dir == CUFFT_FORWARD ? reinterpret_cast<cufftComplex *>(p->pad.as<float2>()) : g;
+  CF(cufftExecC2C(p->fft, src, g, dir));
   return MIRT_OK;
 }
 
@@ -1593,6 +1598,9 @@ int nufft_finish(mirt_nufft *p, int D, const int32_t *Nd, const int32_t *Kd, con
   {
     cudaError_t e = p->grid.alloc((size_t)nslice * p->gg.ngrid * ncol * sizeof(float2));
     if (e == cudaSuccess) e = p->grid_cm.alloc((size_t)nslice * p->gg.ngrid * ncol * sizeof(float2));
+    if (e == cudaSuccess) e = p->pad.alloc((size_t)nslice * p->gg.ngrid * ncol * sizeof(float2));
+    if (e == cudaSuccess)
+      e = cudaMemsetAsync(p->pad.p, 0, (size_t)nslice * p->gg.ngrid * ncol * sizeof(float2), st);
     if (e != cudaSuccess) return fail(MIRT_ERR_ALLOC, "NUFFT grid buffers");
   }
   // contiguous C2C transforms, one per (slice, coil) plane of the coil-major grid
@@ -1721,8 +1729,8 @@ int mirt_nufft_forward(mirt_nufft *p, const void *x, void *X, void *stream) {
   if (!p) return fail(MIRT_ERR_ARG, "nufft is NULL");
   if (p->C == 0) return MIRT_OK;
   cudaStream_t st = as_stream(stream);
-  CK(launch_deapod_pad_cm(static_cast<const float2 *>(x), p->sn.as<float2>(),
-                          p->grid_cm.as<float2>(), p->gg, p->C, p->nslice, st));
+  CK(launch_deapod_image_cm(static_cast<const float2 *>(x), p->sn.as<float2>(),
+                            p->pad.as<float2>(), p->gg, p->C, p->nslice, st));
   int rc = nufft_fft(p, CUFFT_FORWARD, st);
   if (rc) return rc;
   CK(launch_transpose_cols(p->grid_cm.as<float2>(), p->grid.as<float2>(), p->gg.ngrid, p->C,
@@ -1747,6 +1755,146 @@ int mirt_nufft_adjoint(mirt_nufft *p, const void *X, void *x, void *stream) {
   return MIRT_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// Slices [s0, s1) of the forward NUFFT on the plan's full-size buffers (x, X:
+// the whole batch's device image and samples), with `fft` made for s1 - s0
+// slices.
+int nufft_forward_range(mirt_nufft *p, int s0, int s1, const float2 *x, float2 *X,
+                        cufftHandle fft, cudaStream_t st) {
+  const int ns = s1 - s0, C = p->C;
+  const long long gi = p->gg.ngrid * C, xi = p->gg.npix * C;
+  float2 *pad = p->pad.as<float2>() + s0 * gi;
+  float2 *gcm = p->grid_cm.as<float2>() + s0 * gi;
+  CK(launch_deapod_image_cm(x + s0 * xi, p->sn.as<float2>(), pad, p->gg, C, ns, st));
+  CF(cufftSetStream(fft, st));
+  CF(cufftExecC2C(fft, reinterpret_cast<cufftComplex *>(pad), reinterpret_cast<cufftComplex *>(gcm),
+                  CUFFT_FORWARD));
+  CK(launch_transpose_cols(gcm, p->grid.as<float2>() + s0 * gi, p->gg.ngrid, C, ns, 1, st,
+                           &p->gp));
+  // the gather over the chunk's positions (slice-major in the gather order)
+  mirt_interp_plan *P = p->ip;
+  const long long q0 = P->moff_host[s0], nq = P->moff_host[s1] - q0;
+  InterpArgs ag = P->ag;
+  ag.Mtot = nq;
+  ag.W += q0 * ag.SJ;
+  ag.K0 += q0;
+  if (ag.perm) ag.perm += q0;
+  if (ag.phase) ag.phase += q0;
+  CK(launch_gather(ag, P->lg, p->grid.as<float2>(), X, st));
+  return MIRT_OK;
+}
+
+// Slices [s0, s1) of the adjoint NUFFT (row-sweep spread) on the full-size
+// buffers.
+int nufft_adjoint_range(mirt_nufft *p, int s0, int s1, const float2 *X, float2 *x,
+                        cufftHandle fft, cudaStream_t st) {
+  const int ns = s1 - s0, C = p->C;
+  const long long gi = p->gg.ngrid * C, xi = p->gg.npix * C;
+  mirt_interp_plan *P = p->ip;
+  Tiling t = P->t;
+  t.slice0 = s0;
+  t.nslice = ns;
+  t.pos0 = P->moff_host[s0];
+  t.npos = P->moff_host[s1] - t.pos0;
+  CK(launch_spread(P->a, t, P->ls, P->bin_start.as<int>(), X, p->grid.as<float2>(), st));
+  float2 *gcm = p->grid_cm.as<float2>() + s0 * gi;
+  CK(launch_transpose_cols(p->grid.as<float2>() + s0 * gi, gcm, p->gg.ngrid, C, ns, 0, st,
+                           &p->gp));
+  CF(cufftSetStream(fft, st));
+  CF(cufftExecC2C(fft, reinterpret_cast<cufftComplex *>(gcm), reinterpret_cast<cufftComplex *>(gcm),
+                  CUFFT_INVERSE));
+  CK(launch_crop_deapod_cm(gcm, p->sn.as<float2>(), x + s0 * xi, p->gg, C, ns, st));
+  return MIRT_OK;
+}
+
+// Chunks of a host-buffer call: up to 8, of ch slices (the last may be smaller).
+int host_chunks(const mirt_nufft *p, int *ch) {
+  const int nch = std::min(p->nslice, 8);
+  *ch = (p->nslice + nch - 1) / nch;
+  return (p->nslice + *ch - 1) / *ch;
+}
+
+// Streams, events and the chunk-size FFT plans for the pipelined host calls.
+int host_pipeline_setup(mirt_nufft *p) {
+  if (!p->cs_in) CK(cudaStreamCreateWithFlags(&p->cs_in, cudaStreamNonBlocking));
+  if (!p->cs_out) CK(cudaStreamCreateWithFlags(&p->cs_out, cudaStreamNonBlocking));
+  int ch = 0;
+  const int nch = host_chunks(p, &ch);
+  while ((int)p->ev.size() < 2 * nch + 1) {
+    cudaEvent_t e;
+    CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    p->ev.push_back(e);
+  }
+  const int sizes[2] = {ch, p->nslice - (nch - 1) * ch};
+  int n[3];
+  for (int d = 0; d < p->gg.D; d++) n[d] = p->gg.K[p->gg.D - 1 - d];
+  for (int i = 0; i < 2; i++) {
+    if (p->ch_n[i] == sizes[i]) continue;
+    if (p->ch_n[i]) cufftDestroy(p->fft_ch[i]);
+    p->ch_n[i] = 0;
+    cufftResult r = cufftPlanMany(&p->fft_ch[i], p->gg.D, n, nullptr, 1, (int)p->gg.ngrid, nullptr,
+                                  1, (int)p->gg.ngrid, CUFFT_C2C, sizes[i] * p->C);
+    if (r != CUFFT_SUCCESS)
+      return fail(MIRT_ERR_FFT, "cufftPlanMany failed: " + std::to_string((int)r));
+    p->ch_n[i] = sizes[i];
+  }
+  return MIRT_OK;
+}
+
+// Host-buffer call pipelined over slice chunks: the copy in of chunk i + 1 and
+// the copy out of chunk i - 1 overlap the compute of chunk i (copy streams
+// cs_in / cs_out, compute on the caller's stream, ordered by events).
+template <bool FWD>
+int host_pipelined(mirt_nufft *p, const float *in, float *out, cudaStream_t st) {
+  int rc = host_pipeline_setup(p);
+  if (rc) return rc;
+  int ch = 0;
+  const int nch = host_chunks(p, &ch);
+  const long long C = p->C, xi = p->gg.npix * C;
+  const std::vector<long long> &mo = p->ip->moff_host;
+  const float2 *hin = reinterpret_cast<const float2 *>(in);
+  float2 *hout = reinterpret_cast<float2 *>(out);
+  float2 *din = FWD ? p->hx.as<float2>() : p->hX.as<float2>();
+  float2 *dout = FWD ? p->hX.as<float2>() : p->hx.as<float2>();
+  // earlier work on the caller's stream comes first
+  CK(cudaEventRecord(p->ev[2 * nch], st));
+  CK(cudaStreamWaitEvent(p->cs_in, p->ev[2 * nch], 0));
+  for (int i = 0; i < nch; i++) {
+    const int s0 = i * ch, s1 = std::min(p->nslice, s0 + ch);
+    const long long i0 = FWD ? s0 * xi : mo[s0] * C, i1 = FWD ? s1 * xi : mo[s1] * C;
+    const long long o0 = FWD ? mo[s0] * C : s0 * xi, o1 = FWD ? mo[s1] * C : s1 * xi;
+    if (i1 > i0)
+      CK(cudaMemcpyAsync(din + i0, hin + i0, (i1 - i0) * sizeof(float2), cudaMemcpyHostToDevice,
+                         p->cs_in));
+    CK(cudaEventRecord(p->ev[2 * i], p->cs_in));
+    CK(cudaStreamWaitEvent(st, p->ev[2 * i], 0));
+    cufftHandle f = p->fft_ch[(s1 - s0) == p->ch_n[0] ? 0 : 1];
+    rc = FWD ? nufft_forward_range(p, s0, s1, din, dout, f, st)
+             : nufft_adjoint_range(p, s0, s1, din, dout, f, st);
+    if (rc) return rc;
+    CK(cudaEventRecord(p->ev[2 * i + 1], st));
+    CK(cudaStreamWaitEvent(p->cs_out, p->ev[2 * i + 1], 0));
+    if (o1 > o0)
+      CK(cudaMemcpyAsync(hout + o0, dout + o0, (o1 - o0) * sizeof(float2), cudaMemcpyDeviceToHost,
+                         p->cs_out));
+  }
+  CK(cudaStreamSynchronize(p->cs_out));
+  CK(cudaStreamSynchronize(st));
+  return MIRT_OK;
+}
+
+// the chunked path needs several slices and, for the adjoint, the row sweep
+bool host_pipeline_ok(const mirt_nufft *p, bool fwd) {
+  return p->nslice > 1 && p->C > 0 && (fwd || p->ip->t.sweep > 0);
+}
+
+}  // namespace
+
+extern "C" {
+
 int mirt_nufft_forward_host(mirt_nufft *p, const float *x, float *X, void *stream) {
   if (!p) return fail(MIRT_ERR_ARG, "nufft is NULL");
   cudaStream_t st = as_stream(stream);
@@ -1754,6 +1902,7 @@ int mirt_nufft_forward_host(mirt_nufft *p, const float *x, float *X, void *strea
   const size_t bX = (size_t)p->Mtot * p->C * sizeof(float2);
   if (p->hx.bytes < bx) CK(p->hx.alloc(bx));
   if (p->hX.bytes < bX) CK(p->hX.alloc(bX));
+  if (host_pipeline_ok(p, true)) return host_pipelined<true>(p, x, X, st);
   CK(cudaMemcpyAsync(p->hx.p, x, bx, cudaMemcpyHostToDevice, st));
   int rc = mirt_nufft_forward(p, p->hx.p, p->hX.p, stream);
   if (rc) return rc;
@@ -1769,6 +1918,7 @@ int mirt_nufft_adjoint_host(mirt_nufft *p, const float *X, float *x, void *strea
   const size_t bX = (size_t)p->Mtot * p->C * sizeof(float2);
   if (p->hx.bytes < bx) CK(p->hx.alloc(bx));
   if (p->hX.bytes < bX) CK(p->hX.alloc(bX));
+  if (host_pipeline_ok(p, false)) return host_pipelined<false>(p, X, x, st);
   CK(cudaMemcpyAsync(p->hX.p, X, bX, cudaMemcpyHostToDevice, st));
   int rc = mirt_nufft_adjoint(p, p->hX.p, p->hx.p, stream);
   if (rc) return rc;

@@ -1,8 +1,8 @@
 // glue.cu -- elementwise kernels around the interpolation and the FFT.
 //
-//   deapod_pad_cm   x .* sn, zero-padded at the end of every dimension to Kd
-//                   (nufft/nufft.m:139-140, nufft/fftn_fast.m:22-26), written coil-major
-//                   for the batched FFT
+//   deapod_image_cm x .* sn into the coil-major FFT input, zero-padded at the end of
+//                   every dimension to Kd (nufft/nufft.m:139-140, nufft/fftn_fast.m:22-26);
+//                   the padding is written once, this kernel writes the image region
 //   crop_deapod_cm  crop [Kd] -> [Nd] and multiply by conj(sn) (nufft/nufft_adj.m:63-80),
 //                   from the coil-major FFT output back to the coil-innermost image
 //   transpose_cols  coil-major <-> coil-innermost grid between the FFT and the
@@ -18,89 +18,90 @@
 
 namespace mirt {
 
-// x[s][n][c] (coil innermost) .* sn  ->  grid[s][c][k] (coil outermost, zero-padded
-// to K at the end of every dimension), as a tiled transpose: a CTA takes 32
-// consecutive k1 of one grid row and 32 coils.
-__global__ void deapod_pad_cm_kernel(const float2 *__restrict__ x, const float2 *__restrict__ sn,
-                                     float2 *__restrict__ grid, GlueGeom g, int C) {
-  __shared__ float2 tile[32][33];
-  const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
-  const int k1_0 = blockIdx.y * 32;
-  const long long row = blockIdx.x;               // k2 + K2*k3 (+ slice)
-  const int c0 = blockIdx.z * 32;
-  const long long rows_per_slice = g.ngrid / g.K[0];
-  const long long s = row / rows_per_slice;
-  const long long r = row - s * rows_per_slice;
-  // image row of this grid row (inside the N region in every dimension > 0?)
-  long long nrow = 0, nstr = 1, rem = r;
-  bool inside = true;
+// Image tiles of 32 n1 x 32 coils of one image row (n2 + N2 n3) of one slice:
+// blockIdx.x = image row (slices outer), y = n1 block, z = coil block.  The
+// grid row of an image row is its own index in the K grid (the image sits at
+// the start of every dimension).
+struct ImageTile {
+  long long s, r, krow;
+  int n1_0, c0;
+};
+
+__device__ __forceinline__ ImageTile image_tile(const GlueGeom &g) {
+  ImageTile t;
+  const long long row = blockIdx.x;
+  const long long rows_per_slice = g.npix / g.N[0];
+  t.s = row / rows_per_slice;
+  t.r = row - t.s * rows_per_slice;
+  t.n1_0 = blockIdx.y * 32;
+  t.c0 = blockIdx.z * 32;
+  long long kstr = 1, rem = t.r;
+  t.krow = 0;
   for (int d = 1; d < g.D; d++) {
-    const long long kd = rem % g.K[d];
-    rem /= g.K[d];
-    if (kd >= g.N[d]) inside = false;
-    nrow += kd * nstr;
-    nstr *= g.N[d];
+    const long long nd = rem % g.N[d];
+    rem /= g.N[d];
+    t.krow += nd * kstr;
+    kstr *= g.K[d];
   }
-  // load: x[s][nrow*N1 + k1][c], coil fastest
+  return t;
+}
+
+// x[s][n][c] (coil innermost) .* sn  ->  pad[s][c][k] on the image region only;
+// the rest of pad is the zero padding, written once when the plan is made.
+__global__ void __launch_bounds__(256) deapod_image_cm_kernel(const float2 *__restrict__ x,
+                                                              const float2 *__restrict__ sn,
+                                                              float2 *__restrict__ pad,
+                                                              GlueGeom g, int C) {
+  __shared__ float2 tile[32][33];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const long long krows = g.ngrid / g.K[0];
+  const ImageTile t = image_tile(g);
   for (int i = ty; i < 32; i += 8) {
-    const int k1 = k1_0 + i;
-    const int c = c0 + tx;
+    const int n1 = t.n1_0 + i;
+    const int c = t.c0 + tx;
     float2 v = make_float2(0.f, 0.f);
-    if (inside && k1 < g.N[0] && c < C) {
-      const long long n = nrow * g.N[0] + k1;
-      const float2 a = x[(s * g.npix + n) * C + c];
+    if (c < C && n1 < g.N[0]) {
+      const long long n = t.r * g.N[0] + n1;
+      const float2 a = x[(t.s * g.npix + n) * C + c];
       const float2 b = sn[n];
       v = make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
     }
     tile[i][tx] = v;
   }
   __syncthreads();
-  // store: grid[s][c][r*K1 + k1], k1 fastest
   for (int i = ty; i < 32; i += 8) {
-    const int c = c0 + i;
-    const int k1 = k1_0 + tx;
-    if (c < C && k1 < g.K[0])
-      grid[((s * C + c) * rows_per_slice + r) * g.K[0] + k1] = tile[tx][i];
+    const int c = t.c0 + i;
+    const int n1 = t.n1_0 + tx;
+    if (c < C && n1 < g.N[0]) pad[((t.s * C + c) * krows + t.krow) * g.K[0] + n1] = tile[tx][i];
   }
 }
 
 // grid[s][c][k] (coil outermost)  ->  crop to N, .* conj(sn)  ->  x[s][n][c]
-__global__ void crop_deapod_cm_kernel(const float2 *__restrict__ grid,
-                                      const float2 *__restrict__ sn, float2 *__restrict__ x,
-                                      GlueGeom g, int C) {
+__global__ void __launch_bounds__(256) crop_deapod_cm_kernel(const float2 *__restrict__ grid,
+                                                             const float2 *__restrict__ sn,
+                                                             float2 *__restrict__ x, GlueGeom g,
+                                                             int C) {
   __shared__ float2 tile[32][33];
   const int tx = threadIdx.x, ty = threadIdx.y;
-  const int n1_0 = blockIdx.y * 32;
-  const long long row = blockIdx.x;               // image row n2 + N2*n3 (+ slice)
-  const int c0 = blockIdx.z * 32;
-  const long long rows_per_slice = g.npix / g.N[0];
-  const long long s = row / rows_per_slice;
-  const long long r = row - s * rows_per_slice;
   const long long krows = g.ngrid / g.K[0];
-  long long krow = 0, kstr = 1, rem = r;
-  for (int d = 1; d < g.D; d++) {
-    const long long nd = rem % g.N[d];
-    rem /= g.N[d];
-    krow += nd * kstr;
-    kstr *= g.K[d];
-  }
+  const ImageTile t = image_tile(g);
   for (int i = ty; i < 32; i += 8) {
-    const int c = c0 + i;
-    const int n1 = n1_0 + tx;
+    const int c = t.c0 + i;
+    const int n1 = t.n1_0 + tx;
     float2 v = make_float2(0.f, 0.f);
-    if (c < C && n1 < g.N[0]) v = grid[((s * C + c) * krows + krow) * g.K[0] + n1];
+    if (c < C && n1 < g.N[0]) v = grid[((t.s * C + c) * krows + t.krow) * g.K[0] + n1];
     tile[i][tx] = v;
   }
   __syncthreads();
   for (int i = ty; i < 32; i += 8) {
-    const int n1 = n1_0 + i;
-    const int c = c0 + tx;
+    const int n1 = t.n1_0 + i;
+    const int c = t.c0 + tx;
     if (c < C && n1 < g.N[0]) {
-      const long long n = r * g.N[0] + n1;
+      const long long n = t.r * g.N[0] + n1;
       const float2 a = tile[tx][i];
       const float2 b = sn[n];
       // a * conj(b)
-      x[(s * g.npix + n) * C + c] = make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+      x[(t.s * g.npix + n) * C + c] = make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
     }
   }
 }
@@ -280,19 +281,24 @@ static unsigned grid_for(long long n, int thr, int maxb = 148 * 32) {
   return (unsigned)b;
 }
 
-cudaError_t launch_deapod_pad_cm(const float2 *x, const float2 *sn, float2 *grid,
-                                 const GlueGeom &g, int C, int nslice, cudaStream_t st) {
-  const long long rows = g.ngrid / g.K[0] * nslice;
-  dim3 grid_dim((unsigned)rows, (unsigned)((g.K[0] + 31) / 32), (unsigned)((C + 31) / 32));
-  deapod_pad_cm_kernel<<<grid_dim, dim3(32, 8), 0, st>>>(x, sn, grid, g, C);
+namespace {
+dim3 image_grid(const GlueGeom &g, int C, int nslice) {
+  return dim3((unsigned)(g.npix / g.N[0] * nslice), (unsigned)((g.N[0] + 31) / 32),
+              (unsigned)((C + 31) / 32));
+}
+}  // namespace
+
+cudaError_t launch_deapod_image_cm(const float2 *x, const float2 *sn, float2 *pad,
+                                   const GlueGeom &g, int C, int nslice, cudaStream_t st) {
+  if (nslice == 0 || C == 0) return cudaSuccess;
+  deapod_image_cm_kernel<<<image_grid(g, C, nslice), dim3(32, 8), 0, st>>>(x, sn, pad, g, C);
   return cudaGetLastError();
 }
 
 cudaError_t launch_crop_deapod_cm(const float2 *grid, const float2 *sn, float2 *x,
                                   const GlueGeom &g, int C, int nslice, cudaStream_t st) {
-  const long long rows = g.npix / g.N[0] * nslice;
-  dim3 grid_dim((unsigned)rows, (unsigned)((g.N[0] + 31) / 32), (unsigned)((C + 31) / 32));
-  crop_deapod_cm_kernel<<<grid_dim, dim3(32, 8), 0, st>>>(grid, sn, x, g, C);
+  if (nslice == 0 || C == 0) return cudaSuccess;
+  crop_deapod_cm_kernel<<<image_grid(g, C, nslice), dim3(32, 8), 0, st>>>(grid, sn, x, g, C);
   return cudaGetLastError();
 }
 

@@ -22,9 +22,10 @@ struct GlueGeom {
   long long ngrid;     // prod(K)
 };
 
-// image x[s][n][c] -> sn-scaled, zero-padded grid[s][c][k] (coil-major)
-cudaError_t launch_deapod_pad_cm(const float2 *x, const float2 *sn, float2 *grid,
-                                 const GlueGeom &g, int C, int nslice, cudaStream_t st);
+// image x[s][n][c] .* sn -> the image region of the coil-major zero-padded grid
+// pad[s][c][k] (its padding is zero already and stays so)
+cudaError_t launch_deapod_image_cm(const float2 *x, const float2 *sn, float2 *pad,
+                                   const GlueGeom &g, int C, int nslice, cudaStream_t st);
 // coil-major grid[s][c][k] -> cropped, conj(sn)-scaled image x[s][n][c]
 cudaError_t launch_crop_deapod_cm(const float2 *grid, const float2 *sn, float2 *x,
                                   const GlueGeom &g, int C, int nslice, cudaStream_t st);

@@ -63,6 +63,10 @@ struct Tiling {
   int sweep;
   int sweep_rows;
   float2 *sorted;        // row sweep: [Mtot][C] samples in plan order times conj(phase)
+  // Row sweep over part of the batch: slices [slice0, slice0 + nslice), whose
+  // samples are positions [pos0, pos0 + npos) (npos < 0: the whole batch).
+  int slice0;
+  long long pos0, npos;
   int color_beg[9];
   int red_beg[9];
   int padc;              // spread: spare columns on each side of a tile row in

@@ -670,10 +670,12 @@ __global__ void __launch_bounds__(256) spread_kernel(InterpArgs a, Tiling t,
 // that the sweep reads each bin's samples as one contiguous block.
 template <int CW>
 __global__ void __launch_bounds__(256) sweep_order_kernel(InterpArgs a, const float2 *__restrict__ fm,
-                                                          float2 *__restrict__ sorted) {
-  const long long n = a.Mtot * (long long)a.C;
-  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n;
-       e += (long long)gridDim.x * blockDim.x) {
+                                                          float2 *__restrict__ sorted,
+                                                          long long pos0, long long npos) {
+  const long long e0 = pos0 * a.C, n = npos * (long long)a.C;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long e = e0 + i;
     const long long p = e / a.C;
     const int c = (int)(e - p * a.C);
     const int m = a.perm ? __ldg(a.perm + p) : (int)p;
@@ -696,8 +698,9 @@ __global__ void __launch_bounds__(256) spread_sweep_kernel(InterpArgs a, Tiling 
   if (team >= (long long)t.nslice * nband * nseg) return;  // the team's lanes leave together
   const int seg = (int)(team % nseg);
   const long long bandid = team / nseg;
-  const int slice = (int)(bandid / nband);
-  const int y0 = (int)(bandid - (long long)slice * nband) * R;
+  const int sl = (int)(bandid / nband);
+  const int y0 = (int)(bandid - (long long)sl * nband) * R;
+  const int slice = t.slice0 + sl;
   const int sw = (K1 + nseg - 1) / nseg;
   const int x0 = seg * sw, x1 = min(K1, x0 + sw);
   if (x0 >= x1) return;
@@ -1058,10 +1061,13 @@ cudaError_t run(Req &r) {
         if (thr == 0) return cudaSuccess;
         if (!t.sorted) return cudaErrorInvalidValue;
         {
-          const long long n = a.Mtot * (long long)a.C;
+          const long long p0 = t.npos < 0 ? 0 : t.pos0;
+          const long long np = t.npos < 0 ? a.Mtot : t.npos;
+          const long long n = np * (long long)a.C;
           long long nb = (n + 255) / 256;
           if (nb > 148 * 16) nb = 148 * 16;
-          if (n > 0) sweep_order_kernel<CW><<<(unsigned)nb, 256, 0, r.st>>>(a, r.in, t.sorted);
+          if (n > 0)
+            sweep_order_kernel<CW><<<(unsigned)nb, 256, 0, r.st>>>(a, r.in, t.sorted, p0, np);
           cudaError_t e = cudaGetLastError();
           if (e != cudaSuccess) return e;
         }
@@ -1131,7 +1137,8 @@ cudaError_t run(Req &r) {
 
 template <int D, int CW, int JT, bool REAL>
 cudaError_t by_cx(Req &r) {
-  if (r.what != SPREAD && JT > 0 && r.a->C == CW) return run<D, CW, JT, REAL, true>(r);
+  if ((r.what == GATHER || r.what == GATHER_GRID) && JT > 0 && r.a->C == CW)
+    return run<D, CW, JT, REAL, true>(r);
   return run<D, CW, JT, REAL, false>(r);
 }
 

@@ -81,12 +81,25 @@ struct mirt_nufft {
   int C = 0, nslice = 0;
   long long Mtot = 0;
   mirt::DMem sn, grid, grid_cm, hx, hX;  // grid: coil innermost (interp); grid_cm: coil-major (FFT)
+  mirt::DMem pad;                        // coil-major FFT input: image region rewritten per
+                                         // call, zero padding written once
   mirt::DMem phtab;                      // newfft phase_before per dimension, float2 [sum K_d]
   mirt::GridPhase gp{};                  // tables into phtab (tab[0] null: no grid phase)
   cufftHandle fft = 0;
   bool fft_ok = false;
+  // host-buffer calls, pipelined by slice chunks: copy streams, per-chunk
+  // events and the FFT plans of the chunk sizes (made at the first such call)
+  cudaStream_t cs_in = nullptr, cs_out = nullptr;
+  std::vector<cudaEvent_t> ev;
+  cufftHandle fft_ch[2] = {0, 0};
+  int ch_n[2] = {0, 0};  // slices per chunk of fft_ch[i] (0: not made)
   ~mirt_nufft() {
     if (fft_ok) cufftDestroy(fft);
+    for (int i = 0; i < 2; i++)
+      if (ch_n[i]) cufftDestroy(fft_ch[i]);
+    for (cudaEvent_t e : ev) cudaEventDestroy(e);
+    if (cs_in) cudaStreamDestroy(cs_in);
+    if (cs_out) cudaStreamDestroy(cs_out);
     delete ip;
   }
 };

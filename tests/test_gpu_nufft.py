@@ -127,3 +127,82 @@ def test_3d_nufft_vs_oracle():
     y = rng.standard_normal(M) + 1j * rng.standard_normal(M)
     assert rel_l2(mb.nufft_adj(y, st), nr.nufft_adj(y, st_o, ad)) <= ADJ_TOL
     st.close()
+
+
+@pytest.mark.parametrize("C,K1", [(32, 80), (40, 82)])
+def test_32coil_row_sweep_adjoint_vs_oracle(C, K1):
+    """32-coil chunks: the plan's default spread is the row sweep.  The NUFFT
+    adjoint against the oracle for several band / segment choices (K1 = 80
+    and 82, segment edges anywhere), bitwise the same for all of them, and
+    against the tiled spread to FP32 rounding; a newfft plan of the same
+    batch (grid phase on the transpose) against its oracle."""
+    import torch
+    from oracle import newfft_ref as nf
+    rng = np.random.default_rng(40 + C)
+    N, K = (40, 48), (K1, 96)
+    counts = [1200, 2500, 700]
+    moff = np.concatenate([[0], np.cumsum(counts)])
+    om = np.concatenate([rng.uniform(-np.pi, np.pi, (c, 2)) for c in counts])
+    ns = (20, 24)
+    plan = mb.NufftPlan(om, N, (6, 6), K, n_shift=ns, Ld=1024, ncol=C, slice_moff=moff)
+    assert plan.config()["spread_sweep"] > 0
+    X = rng.standard_normal((len(om), C)) + 1j * rng.standard_normal((len(om), C))
+    Xd = torch.from_numpy(X.astype(np.complex64)).cuda()
+    out = plan.adjoint(Xd).cpu().numpy()
+    refs = []
+    for s in range(len(counts)):
+        sl = slice(moff[s], moff[s + 1])
+        st_o = nr.nufft_init_table(om[sl], N, (6, 6), K, ns, 1024)
+        _, ad = _oracle_pair(st_o)
+        refs.append({c: nr.nufft_adj(X[sl, c], st_o, ad) for c in (0, 17, C - 1)})
+    for seg, rows in [(None, None), (3, 2), (5, 1), (1, 4)]:
+        if seg is not None:
+            plan.set_sweep(seg, rows)
+        o = plan.adjoint(Xd).cpu().numpy()
+        for s in range(len(counts)):
+            for c, ref in refs[s].items():
+                assert rel_l2(o[s, :, :, c].T, ref) <= ADJ_TOL, (seg, rows, s, c)
+        assert np.array_equal(o, out)          # same sums for every band / segment choice
+    assert np.array_equal(out, plan.adjoint(Xd).cpu().numpy())
+    plan.set_sweep(0)
+    assert rel_l2(plan.adjoint(Xd).cpu().numpy(), out) <= 5e-6
+    plan.close()
+    nplan = mb.newfft(om, N, Kd=K, n_shift=ns, ncol=C, slice_moff=moff)
+    outn = nplan.adjoint(Xd).cpu().numpy()
+    for s in range(len(counts)):
+        sl = slice(moff[s], moff[s + 1])
+        so = nf.newfft_init(om[sl], N, Kd=K, n_shift=ns)
+        assert rel_l2(outn[s, :, :, C - 1].T, nf.newfft_adj(X[sl, C - 1], so)) <= ADJ_TOL, s
+    nplan.close()
+
+
+@pytest.mark.parametrize("C,nslice", [(32, 5), (32, 11), (8, 11)])
+def test_host_calls_pipelined_by_slice_chunks(C, nslice):
+    """Host-buffer calls of a multi-slice plan run in slice chunks (copies on
+    their own streams overlapping the compute; 11 slices: five chunks of two
+    and one of one).  Their results are the device calls' to FP32 rounding
+    (the chunk FFT plans have other batch counts); the adjoint is chunked
+    where the spread is the row sweep (32 coils), whole-batch otherwise."""
+    import torch
+    rng = np.random.default_rng(60 + nslice + C)
+    N, K = (32, 40), (64, 80)
+    counts = rng.integers(300, 1200, nslice)
+    moff = np.concatenate([[0], np.cumsum(counts)])
+    om = rng.uniform(-np.pi, np.pi, (int(moff[-1]), 2))
+    plan = mb.NufftPlan(om, N, (6, 6), K, n_shift=(16, 20), Ld=1024, ncol=C, slice_moff=moff)
+    x = (rng.standard_normal(plan.image_shape) + 1j * rng.standard_normal(plan.image_shape))
+    x = x.astype(np.complex64)
+    for _ in range(2):                          # the second call reuses streams and plans
+        a = plan.forward_host(x)
+        b = plan.forward(torch.from_numpy(x).cuda()).cpu().numpy()
+        assert rel_l2(a, b) <= 1e-6
+        y = plan.adjoint_host(b)
+        z = plan.adjoint(torch.from_numpy(b).cuda()).cpu().numpy()
+        assert rel_l2(y, z) <= 1e-6
+    for s in (0, nslice - 1):                   # first and last chunk against the oracle
+        sl = slice(moff[s], moff[s + 1])
+        st_o = nr.nufft_init_table(om[sl], N, (6, 6), K, (16, 20), 1024)
+        fw, ad = _oracle_pair(st_o)
+        assert rel_l2(a[sl, C - 1], nr.nufft(x[s, :, :, C - 1].T, st_o, fw)) <= FWD_TOL
+        assert rel_l2(y[s, :, :, 0].T, nr.nufft_adj(b[sl, 0], st_o, ad)) <= ADJ_TOL
+    plan.close()
