@@ -325,6 +325,16 @@ def run_gpu(args, w):
     if args.nondeterministic:
         plan.set_deterministic(False)
     tuned = plan.autotune() if not args.no_autotune else plan.config()
+    if args.spread == "sweep" and tuned.get("spread_sweep", 0) == 0:
+        # the plan's own default: one grid row per team, rows split into
+        # segments (of at least 32 columns) until about 64k teams
+        K1, K2 = w["K"], w["K"]
+        bands, nseg = plan.nslice * K2, 1
+        while bands * nseg < 65536 and K1 // (2 * nseg) >= 32:
+            nseg *= 2
+        tuned = plan.set_sweep(nseg, 1)
+    elif args.spread == "tiled" and tuned.get("spread_sweep", 0) > 0:
+        tuned = plan.set_sweep(0)
     t_tune = time.perf_counter() - t0
     img_np = make_images(w, np.random.default_rng(99 + rank))
     if img_np.shape[0] != plan.nslice:
@@ -642,6 +652,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--spread", default="auto", choices=["auto", "sweep", "tiled"],
+                    help="spread variant: the autotuner's choice, or the row sweep / tiled spread")
     ap.add_argument("--nondeterministic", action="store_true",
                     help="let the spread add with shared-memory atomics (not bitwise reproducible)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)

@@ -607,16 +607,17 @@ int plan_finish(mirt_interp_plan *P, long long Mtot, const long long *moff, int 
   int rc2 = build_tasks(P, st);
   if (rc2) return rc2;
   CK(query_gather_grid(a, P->lg));
-  // 2D, J = 6, 32-coil chunks: the row sweep by default, two rows per band,
-  // rows split into segments (of at least 32 columns) until about 32k teams
+  // 2D, J = 6, 32-coil chunks: the row sweep by default, one grid row per
+  // team, rows split into segments (of at least 32 columns) until about 64k
+  // teams
   if (sweep_ok(a, P->t) && P->ls.cw == 32) {
     int nseg = 1;
-    const long long bands = (long long)nslice * ((a.g.K[1] + 1) / 2);
-    while (bands * nseg < 32768 && a.g.K[0] / (2 * nseg) >= 32) nseg *= 2;
+    const long long bands = (long long)nslice * a.g.K[1];
+    while (bands * nseg < 65536 && a.g.K[0] / (2 * nseg) >= 32) nseg *= 2;
     int rc3 = sweep_buffer(P);
     if (rc3) return rc3;
     P->t.sweep = nseg;
-    P->t.sweep_rows = 2;
+    P->t.sweep_rows = 1;
   }
   return MIRT_OK;
 }

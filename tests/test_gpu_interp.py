@@ -372,7 +372,8 @@ def test_sweep_spread_matches_oracle(C):
     plan = mb.InterpPlan(K, J, L, h, tm, C, slice_moff=moff)
     fm = rng.standard_normal((len(tm), C)) + 1j * rng.standard_normal((len(tm), C))
     fm_d = torch.from_numpy(fm.astype(np.complex64)).cuda()
-    assert plan.config()["spread_sweep"] == (2 if C >= 32 else 0)   # the default for 32 coils
+    cfg = plan.config()                        # the default for 32-coil chunks
+    assert (cfg["spread_sweep"], cfg["spread_sweep_rows"]) == ((2, 1) if C >= 32 else (0, 1))
     plan.set_sweep(0)
     tiled = plan.adjoint(fm_d).cpu().numpy()
     refs = [oracle.interp_adj(fm[moff[s]:moff[s + 1]], h, J, L, tms[s], K, 0, impl=ref_impl())
