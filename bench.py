@@ -326,14 +326,8 @@ def run_gpu(args, w):
         plan.set_deterministic(False)
     tuned = plan.autotune() if not args.no_autotune else plan.config()
     if args.spread == "sweep" and tuned.get("spread_sweep", 0) == 0:
-        # the plan's own default: one grid row per team, rows split into
-        # segments (of at least 32 columns) until about 64k teams
-        K1, K2 = w["K"], w["K"]
-        bands, nseg = plan.nslice * K2, 1
-        while bands * nseg < 65536 and K1 // (2 * nseg) >= 32:
-            nseg *= 2
-        tuned = plan.set_sweep(nseg, 1)
-    elif args.spread == "tiled" and tuned.get("spread_sweep", 0) > 0:
+        tuned = plan.set_sweep(-1, 1)        # the plan's default: balanced teams of one row
+    elif args.spread == "tiled" and tuned.get("spread_sweep", 0) != 0:
         tuned = plan.set_sweep(0)
     t_tune = time.perf_counter() - t0
     img_np = make_images(w, np.random.default_rng(99 + rank))
@@ -420,7 +414,7 @@ def run_gpu(args, w):
     peak, peak_kind = measured_peak()
     dom, tdom = ("spread", t_spread) if t_spread >= t_gather else ("gather", t_gather)
     achieved = B / tdom / 1e9
-    variant = "sweep" if tuned.get("spread_sweep", 0) > 0 else "tiled"
+    variant = "sweep" if tuned.get("spread_sweep", 0) != 0 else "tiled"
     kernels = {"gather": "gather_kernel",
                "spread": ("sweep_order_kernel + spread_sweep_kernel" if variant == "sweep"
                           else "spread_kernel (+ spread_reduce_kernel)")}
@@ -473,7 +467,7 @@ def run_gpu(args, w):
     # deapodise, forward transpose, gather, crop (cuFFT not counted), and the spread:
     # row sweep = sample ordering + sweep into the coil-major grid; tiled = spread
     # [+ reductions] + the adjoint transpose
-    if tuned.get("spread_sweep", 0) > 0:
+    if tuned.get("spread_sweep", 0) != 0:
         spread_launches = 2
     else:
         spread_launches = 2 + (1 if tuned.get("spread_reductions", 0) > 0 else 0)

@@ -197,8 +197,8 @@ int mirt_interp_plan_autotune(mirt_interp_plan *plan, void *stream);
  * {T1, T2, T3, spread threads, spread heavy-first order, coil lanes,
  *  gather threads, (unused), gather CTAs, B1, B2, B3, split chunk,
  *  spread tasks, spare tile columns, partial-tile reductions,
- *  spread shared-tile atomics, ownership spread, row-sweep segments (0: off),
- *  row-sweep rows per band}. */
+ *  spread shared-tile atomics, ownership spread, row-sweep segments (0: off,
+ *  -1: balanced team list), row-sweep rows per band}. */
 int mirt_interp_plan_config(mirt_interp_plan *plan, int32_t *out, int32_t n);
 
 /* Adjoint accumulation order.  deterministic = 1 (the default): every
@@ -225,10 +225,13 @@ int mirt_interp_plan_set_ownership(mirt_interp_plan *plan, int32_t own, void *st
  * rows whose samples reach the band, with six grid columns of accumulators
  * per row in registers; each grid point is written once, summed in a fixed
  * order that does not depend on rows or segments (deterministic), with no
- * tiles, shared memory or reduction launches.  segments: 1..K1 (more
- * segments, more parallel teams, five warm-up columns each); 0 returns to
- * the tiled spread.  MIRT_ERR_ARG where it does not apply.  The autotuner
- * tries it where it applies.  No reference counterpart. */
+ * tiles, shared memory or reduction launches.  segments: 1..K1 uniform
+ * segments per row (more segments, more parallel teams, five warm-up columns
+ * each); -1 a balanced team list built from the sort's bins (rows cut into
+ * segments of about equal visit counts, about 64k teams: the default for
+ * 32-coil plans); 0 returns to the tiled spread.  MIRT_ERR_ARG
+ * where it does not apply.  The autotuner tries it where it applies.  No
+ * reference counterpart. */
 int mirt_interp_plan_set_sweep(mirt_interp_plan *plan, int32_t segments, int32_t rows);
 
 /* Fix the spread's tiling instead of autotuning it: tile extents T[0..D-1]

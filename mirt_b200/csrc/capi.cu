@@ -178,6 +178,82 @@ int sweep_buffer(mirt_interp_plan *P) {
   return MIRT_OK;
 }
 
+// Balanced row-sweep teams: each band of `rows` grid rows of each slice is
+// cut into column segments of about equal cost, cost = visits (samples of the
+// rows + 5 bin rows in the segment's columns and its five warm-up columns)
+// + 2 per column step; segments of at least 8 columns, about `target` teams
+// in all, in grid order (neighbouring bands read the same samples, so they
+// run together; heaviest-first order measured slower at full size).  Teams
+// write disjoint points, each summed in the same fixed order.
+int build_sweep_teams(mirt_interp_plan *P, int rows, long long target, cudaStream_t st) {
+  const InterpArgs &a = P->a;
+  Tiling &t = P->t;
+  const int K1 = a.g.K[0], K2 = a.g.K[1], S = t.nslice, NQ = rows + 5;
+  const long long nb = (long long)t.nbins * S;
+  std::vector<int> bs(nb + 1);
+  CK(cudaMemcpyAsync(bs.data(), P->bin_start.p, (nb + 1) * sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  const double alpha = 2.0;
+  const int nband = (K2 + rows - 1) / rows;
+  // visits per bin column of every band: v[x] = sum over its NQ bin rows
+  std::vector<std::vector<float>> vb((size_t)S * nband);
+  double total = 0;
+  for (int s = 0; s < S; s++) {
+    const int *b = bs.data() + (size_t)s * t.nbins;
+    for (int bi = 0; bi < nband; bi++) {
+      std::vector<float> &v = vb[(size_t)s * nband + bi];
+      v.assign(K1, 0.f);
+      for (int q = 0; q < NQ; q++) {
+        int r = (bi * rows - 5 + q) % K2;
+        if (r < 0) r += K2;
+        const int *br = b + (size_t)r * K1;
+        for (int x = 0; x < K1; x++) v[x] += (float)(br[x + 1] - br[x]);
+      }
+      for (int x = 0; x < K1; x++) total += v[x] + alpha;
+    }
+  }
+  const double T = std::max(1.0, total / (double)std::max<long long>(target, 1));
+  struct Team {
+    double cost;  // kept for inspection; the list is in grid order
+    int4 k;
+  };
+  std::vector<Team> teams;
+  for (int s = 0; s < S; s++)
+    for (int bi = 0; bi < nband; bi++) {
+      const std::vector<float> &v = vb[(size_t)s * nband + bi];
+      auto vx = [&](int x) { return (double)v[(x % K1 + K1) % K1]; };
+      int x0 = 0;
+      while (x0 < K1) {
+        double c = 5 * alpha;
+        for (int x = x0 - 5; x < x0; x++) c += vx(x);
+        int x1 = x0;
+        while (x1 < K1) {
+          const double add = vx(x1) + alpha;
+          if (x1 - x0 >= 8 && c + add > T) break;
+          c += add;
+          x1++;
+        }
+        if (K1 - x1 < 8) {  // a short tail joins this segment
+          for (int x = x1; x < K1; x++) c += vx(x) + alpha;
+          x1 = K1;
+        }
+        teams.push_back(Team{c, make_int4(s, bi * rows, x0, x1)});
+        x0 = x1;
+      }
+    }
+  std::vector<int4> tk(teams.size());
+  for (size_t i = 0; i < teams.size(); i++) tk[i] = teams[i].k;
+  if (P->sweep_teams.bytes < tk.size() * sizeof(int4)) CK(P->sweep_teams.alloc(tk.size() * sizeof(int4)));
+  CK(cudaMemcpyAsync(P->sweep_teams.p, tk.data(), tk.size() * sizeof(int4), cudaMemcpyHostToDevice,
+                     st));
+  CK(cudaStreamSynchronize(st));
+  t.sweep_team = P->sweep_teams.as<int4>();
+  t.nteams = (int)tk.size();
+  t.sweep = -1;
+  t.sweep_rows = rows;
+  return MIRT_OK;
+}
+
 int wrap_ok(const InterpArgs &a, const Tiling &t) {
   for (int d = 0; d < a.g.D; d++)
     if (a.g.K[d] < t.T[d] + a.g.J[d]) return 0;
@@ -230,6 +306,8 @@ void choose_config(mirt_interp_plan *P) {
   t.slice0 = 0;
   t.pos0 = 0;
   t.npos = -1;
+  t.sweep_team = nullptr;
+  t.nteams = 0;
   t.nbins = 1;
   t.ntiles = 1;
   for (int d = 0; d < MIRT_DMAX; d++) {
@@ -608,16 +686,12 @@ int plan_finish(mirt_interp_plan *P, long long Mtot, const long long *moff, int 
   if (rc2) return rc2;
   CK(query_gather_grid(a, P->lg));
   // 2D, J = 6, 32-coil chunks: the row sweep by default, one grid row per
-  // team, rows split into segments (of at least 32 columns) until about 64k
-  // teams
+  // team, balanced segments (about 64k teams, heaviest first)
   if (sweep_ok(a, P->t) && P->ls.cw == 32) {
-    int nseg = 1;
-    const long long bands = (long long)nslice * a.g.K[1];
-    while (bands * nseg < 65536 && a.g.K[0] / (2 * nseg) >= 32) nseg *= 2;
     int rc3 = sweep_buffer(P);
     if (rc3) return rc3;
-    P->t.sweep = nseg;
-    P->t.sweep_rows = 1;
+    rc3 = build_sweep_teams(P, 1, 65536, st);
+    if (rc3) return rc3;
   }
   return MIRT_OK;
 }
@@ -846,11 +920,12 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
         for (int t2 : {8, 16})
           for (int th = 32; th <= 256 && th / 32 <= t2; th *= 2) add(t0, t1, t2, th);
   }
-  // row sweep (no tiles): bands of 1, 2 or 4 rows, whole rows or segments of
-  // at least 32 columns
+  // row sweep (no tiles): bands of 1, 2 or 4 rows, whole rows or uniform
+  // segments of at least 32 columns, or balanced teams (sweep = -1)
   if (sweep_ok(a, P->t) && sweep_buffer(P) == MIRT_OK)
     for (int rows : {1, 2, 4})
-      for (int nseg = 1; nseg <= 16 && (nseg == 1 || a.g.K[0] / nseg >= 32); nseg *= 2)
+      for (int nseg = (rows < 4 ? -1 : 1); nseg <= 16 && (nseg <= 1 || a.g.K[0] / nseg >= 32);
+           nseg = nseg < 0 ? 1 : nseg * 2)
         cands.push_back(SpreadCand{{P->t.T[0], P->t.T[1], P->t.T[2]}, P->ls.threads, 0, 0, 0,
                                    nseg, rows});
   SpreadCand best{};
@@ -859,6 +934,10 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
     P->t.own = c.own;
     P->t.sweep = c.sweep;
     P->t.sweep_rows = c.sweep_rows;
+    if (c.sweep < 0) {
+      int rc = build_sweep_teams(P, c.sweep_rows, 65536, st);
+      if (rc) return rc;
+    }
     int rc = set_spread_tiles(P, c.T, st);
     if (rc) continue;
     P->ls.threads = c.threads;
@@ -879,6 +958,10 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
     P->t.own = best.own;
     P->t.sweep = best.sweep;
     P->t.sweep_rows = best.sweep_rows;
+    if (best.sweep < 0) {
+      int rc = build_sweep_teams(P, best.sweep_rows, 65536, st);
+      if (rc) return rc;
+    }
     int rc = set_spread_tiles(P, best.T, st);
     if (rc) return rc;
     P->ls.threads = best.threads;
@@ -959,12 +1042,16 @@ int mirt_interp_plan_set_sweep(mirt_interp_plan *P, int32_t segments, int32_t ro
   if (!P) return fail(MIRT_ERR_ARG, "plan is NULL");
   if (segments && !sweep_ok(P->a, P->t))
     return fail(MIRT_ERR_ARG, "row-sweep spread needs 2D, J = 6 and K >= 6 per dimension");
-  if (segments < 0 || (segments > 0 && segments > P->a.g.K[0]))
-    return fail(MIRT_ERR_ARG, "row-sweep segments must be in 1..K1 (0: off)");
+  if (segments < -1 || (segments > 0 && segments > P->a.g.K[0]))
+    return fail(MIRT_ERR_ARG, "row-sweep segments must be in 1..K1 (0: off, -1: balanced)");
   if (segments && rows != 1 && rows != 2 && rows != 4)
     return fail(MIRT_ERR_ARG, "row-sweep rows per band must be 1, 2 or 4");
   if (segments) {
     int rc = sweep_buffer(P);
+    if (rc) return rc;
+  }
+  if (segments < 0) {
+    int rc = build_sweep_teams(P, rows, 65536, as_stream(nullptr));
     if (rc) return rc;
   }
   P->t.sweep = segments;
@@ -1796,6 +1883,7 @@ int nufft_adjoint_range(mirt_nufft *p, int s0, int s1, const float2 *X, float2 *
   const long long gi = p->gg.ngrid * C, xi = p->gg.npix * C;
   mirt_interp_plan *P = p->ip;
   Tiling t = P->t;
+  if (t.sweep < 0) t.sweep = 2;  // a chunk: uniform halves of rows (same sums)
   t.slice0 = s0;
   t.nslice = ns;
   t.pos0 = P->moff_host[s0];
@@ -1889,7 +1977,7 @@ int host_pipelined(mirt_nufft *p, const float *in, float *out, cudaStream_t st) 
 
 // the chunked path needs several slices and, for the adjoint, the row sweep
 bool host_pipeline_ok(const mirt_nufft *p, bool fwd) {
-  return p->nslice > 1 && p->C > 0 && (fwd || p->ip->t.sweep > 0);
+  return p->nslice > 1 && p->C > 0 && (fwd || p->ip->t.sweep != 0);
 }
 
 }  // namespace

@@ -59,7 +59,7 @@ struct Tiling {
   // that reach the band, with six grid columns of accumulators per row in
   // registers; every grid point is written once, in a fixed summation order.
   // No tiles, shared memory or reductions (the tiling fields are unused).
-  // sweep = 0: the tiled spread.
+  // sweep = 0: the tiled spread; -1: the team list below.
   int sweep;
   int sweep_rows;
   float2 *sorted;        // row sweep: [Mtot][C] samples in plan order times conj(phase)
@@ -67,6 +67,11 @@ struct Tiling {
   // samples are positions [pos0, pos0 + npos) (npos < 0: the whole batch).
   int slice0;
   long long pos0, npos;
+  // Row sweep with a team list (sweep = -1): team i covers band rows from
+  // sweep_team[i].y of slice .x, columns [.z, .w); nteams entries, heaviest
+  // first (segments of about equal visit counts, from the sort's bins).
+  const int4 *sweep_team;
+  int nteams;
   int color_beg[9];
   int red_beg[9];
   int padc;              // spread: spare columns on each side of a tile row in

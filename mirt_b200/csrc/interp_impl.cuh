@@ -692,17 +692,28 @@ __global__ void __launch_bounds__(256) spread_sweep_kernel(InterpArgs a, Tiling 
                                                            float2 *__restrict__ ck) {
   constexpr int NQ = R + 5;  // bin rows reaching the band
   const int K1 = a.g.K[0], K2 = a.g.K[1];
-  const int nseg = t.sweep;
-  const int nband = (K2 + R - 1) / R;
   const long long team = ((long long)blockIdx.x * blockDim.x + threadIdx.x) / CW;
-  if (team >= (long long)t.nslice * nband * nseg) return;  // the team's lanes leave together
-  const int seg = (int)(team % nseg);
-  const long long bandid = team / nseg;
-  const int sl = (int)(bandid / nband);
-  const int y0 = (int)(bandid - (long long)sl * nband) * R;
-  const int slice = t.slice0 + sl;
-  const int sw = (K1 + nseg - 1) / nseg;
-  const int x0 = seg * sw, x1 = min(K1, x0 + sw);
+  int slice, y0, x0, x1;
+  if (t.sweep < 0) {
+    if (team >= t.nteams) return;  // the team's lanes leave together
+    const int4 tk = t.sweep_team[team];
+    slice = tk.x;
+    y0 = tk.y;
+    x0 = tk.z;
+    x1 = tk.w;
+  } else {
+    const int nseg = t.sweep;
+    const int nband = (K2 + R - 1) / R;
+    if (team >= (long long)t.nslice * nband * nseg) return;
+    const int seg = (int)(team % nseg);
+    const long long bandid = team / nseg;
+    const int sl = (int)(bandid / nband);
+    y0 = (int)(bandid - (long long)sl * nband) * R;
+    slice = t.slice0 + sl;
+    const int sw = (K1 + nseg - 1) / nseg;
+    x0 = seg * sw;
+    x1 = min(K1, x0 + sw);
+  }
   if (x0 >= x1) return;
   const int C = a.C;
   const int c = blockIdx.y * CW + (int)(threadIdx.x % CW);
@@ -1053,9 +1064,10 @@ cudaError_t run(Req &r) {
     const Tiling &t = *r.t;
     const size_t sm = spread_smem_bytes(a, t, l);
     if constexpr (D == 2 && JT == 6) {
-      if (t.sweep > 0) {
+      if (t.sweep != 0) {
         const long long nband = (a.g.K[1] + t.sweep_rows - 1) / max(t.sweep_rows, 1);
-        const long long teams = (long long)t.nslice * nband * t.sweep;
+        const long long teams =
+            t.sweep < 0 ? t.nteams : (long long)t.nslice * nband * t.sweep;
         const long long thr = teams * CW;
         const unsigned nchunk = (unsigned)((a.C + CW - 1) / CW);
         if (thr == 0) return cudaSuccess;

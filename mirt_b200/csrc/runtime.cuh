@@ -68,6 +68,7 @@ struct mirt_interp_plan {
   mirt::InterpArgs ag{};
   mirt::DMem wtap_g, k0tap_g, perm_g, phase_g;
   mirt::DMem swept;        // row-sweep spread: the samples in plan order, [Mtot][C]
+  mirt::DMem sweep_teams;  // row-sweep spread: balanced team list (int4 per team)
   int split_chunk = 1024;  // sample visits per spread task before a tile is split
   int heavy_first = 1;     // spread task order: 1 heaviest first, 0 grid order
   int deterministic = 1;   // 0: the spread may use shared-memory atomics

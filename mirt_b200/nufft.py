@@ -167,8 +167,8 @@ class InterpPlan:
 
     def set_sweep(self, segments=1, rows=4):
         """Row-sweep spread (2D, J = 6; see mirt_interp_plan_set_sweep):
-        segments per grid row (True = 1; 0 / False = tiled spread) and grid
-        rows per band (1, 2 or 4)."""
+        uniform segments per grid row (True = 1; 0 / False = tiled spread;
+        -1 = balanced team list) and grid rows per band (1, 2 or 4)."""
         check(self.lib.mirt_interp_plan_set_sweep(self.handle, int(segments), int(rows)))
         return self.config()
 

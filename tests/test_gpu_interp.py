@@ -357,8 +357,9 @@ def test_ownership_spread_refused_where_colours_would_overlap():
 def test_sweep_spread_matches_oracle(C):
     """Row-sweep spread (2D, J = 6): three slices (one dense, one with
     coordinates far outside the grid, wrapping several times), a partial
-    coil chunk at C = 3 and 40, bands of 1, 2 and 4 rows, whole rows and row
-    segments down to one column (K1 = 96 in 5 segments: a shorter last one); the oracle's adjoint, bitwise reproducible and
+    coil chunk at C = 3 and 40, bands of 1, 2 and 4 rows, whole rows, uniform
+    row segments down to one column (K1 = 96 in 5 segments: a shorter last
+    one) and balanced team lists (segments cut at equal visit counts); the oracle's adjoint, bitwise reproducible and
     independent of bands and segments, and the tiled spread's result to FP32
     rounding (another summation order)."""
     import torch
@@ -372,14 +373,14 @@ def test_sweep_spread_matches_oracle(C):
     plan = mb.InterpPlan(K, J, L, h, tm, C, slice_moff=moff)
     fm = rng.standard_normal((len(tm), C)) + 1j * rng.standard_normal((len(tm), C))
     fm_d = torch.from_numpy(fm.astype(np.complex64)).cuda()
-    cfg = plan.config()                        # the default for 32-coil chunks
-    assert (cfg["spread_sweep"], cfg["spread_sweep_rows"]) == ((2, 1) if C >= 32 else (0, 1))
+    cfg = plan.config()                        # the default for 32-coil chunks: balanced teams
+    assert (cfg["spread_sweep"], cfg["spread_sweep_rows"]) == ((-1, 1) if C >= 32 else (0, 1))
     plan.set_sweep(0)
     tiled = plan.adjoint(fm_d).cpu().numpy()
     refs = [oracle.interp_adj(fm[moff[s]:moff[s + 1]], h, J, L, tms[s], K, 0, impl=ref_impl())
             for s in range(3)]
     first = None
-    for nseg, rows in [(1, 1), (3, 2), (16, 4), (96, 4), (1, 4), (5, 2)]:   # segments of 96 .. 1 columns
+    for nseg, rows in [(1, 1), (3, 2), (16, 4), (96, 4), (1, 4), (5, 2), (-1, 1), (-1, 2)]:
         cfg = plan.set_sweep(nseg, rows)
         assert cfg["spread_sweep"] == nseg and cfg["spread_sweep_rows"] == rows
         out = plan.adjoint(fm_d).cpu().numpy()

@@ -145,7 +145,7 @@ def test_32coil_row_sweep_adjoint_vs_oracle(C, K1):
     om = np.concatenate([rng.uniform(-np.pi, np.pi, (c, 2)) for c in counts])
     ns = (20, 24)
     plan = mb.NufftPlan(om, N, (6, 6), K, n_shift=ns, Ld=1024, ncol=C, slice_moff=moff)
-    assert plan.config()["spread_sweep"] > 0
+    assert plan.config()["spread_sweep"] == -1     # balanced teams by default
     X = rng.standard_normal((len(om), C)) + 1j * rng.standard_normal((len(om), C))
     Xd = torch.from_numpy(X.astype(np.complex64)).cuda()
     out = plan.adjoint(Xd).cpu().numpy()
@@ -155,7 +155,7 @@ def test_32coil_row_sweep_adjoint_vs_oracle(C, K1):
         st_o = nr.nufft_init_table(om[sl], N, (6, 6), K, ns, 1024)
         _, ad = _oracle_pair(st_o)
         refs.append({c: nr.nufft_adj(X[sl, c], st_o, ad) for c in (0, 17, C - 1)})
-    for seg, rows in [(None, None), (3, 2), (5, 1), (1, 4)]:
+    for seg, rows in [(None, None), (3, 2), (5, 1), (1, 4), (-1, 2)]:
         if seg is not None:
             plan.set_sweep(seg, rows)
         o = plan.adjoint(Xd).cpu().numpy()
