@@ -193,12 +193,12 @@ int mirt_interp_plan_adjoint(mirt_interp_plan *plan, const void *fm, void *ck, v
  * bitwise deterministic for any choice. */
 int mirt_interp_plan_autotune(mirt_interp_plan *plan, void *stream);
 
-/* Current launch configuration: up to 20 values
+/* Current launch configuration: up to 21 values
  * {T1, T2, T3, spread threads, spread heavy-first order, coil lanes,
  *  gather threads, (unused), gather CTAs, B1, B2, B3, split chunk,
  *  spread tasks, spare tile columns, partial-tile reductions,
  *  spread shared-tile atomics, ownership spread, row-sweep segments (0: off,
- *  -1: balanced team list), row-sweep rows per band}. */
+ *  -1: balanced team list), row-sweep rows per band, TMA gather}. */
 int mirt_interp_plan_config(mirt_interp_plan *plan, int32_t *out, int32_t n);
 
 /* Adjoint accumulation order.  deterministic = 1 (the default): every
@@ -233,6 +233,24 @@ int mirt_interp_plan_set_ownership(mirt_interp_plan *plan, int32_t own, void *st
  * where it does not apply.  The autotuner tries it where it applies.  No
  * reference counterpart. */
 int mirt_interp_plan_set_sweep(mirt_interp_plan *plan, int32_t segments, int32_t rows);
+
+/* Gather over TMA-staged tiles and records (2D, J = 6, an even C >= 32,
+ * K >= 13; the default there, and the autotuner times it against the plain
+ * gather): the gather order groups samples by 8 x 8 blocks of first taps; for
+ * each work item (up to 96 samples of one block) a CTA loads the block's
+ * 13 x 13 x 32-coil grid tile (cp.async.bulk.tensor) and the item's tap
+ * coefficients and first taps (1-D bulk copies) into shared memory, two
+ * stages deep, and reads all taps and records from there; blocks whose taps
+ * wrap past K read the grid directly.  Same arithmetic and summation order
+ * as the plain gather: identical results.  tma = 0 selects the plain gather;
+ * MIRT_ERR_ARG where the plan has no TMA blocks.  No reference counterpart. */
+int mirt_interp_plan_set_gather(mirt_interp_plan *plan, int32_t tma);
+
+/* Fault flag of the plan's bounded in-kernel waits (TMA stage arrivals):
+ * synchronises the device, stores 1 in *fault if a wait ran out since the
+ * last call (the affected samples were not computed), else 0, and clears it.
+ * No reference counterpart. */
+int mirt_interp_plan_fault(mirt_interp_plan *plan, int32_t *fault);
 
 /* Fix the spread's tiling instead of autotuning it: tile extents T[0..D-1]
  * (multiples of the sort bins B of mirt_interp_plan_config, at most the grid

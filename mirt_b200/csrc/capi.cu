@@ -254,6 +254,28 @@ int build_sweep_teams(mirt_interp_plan *P, int rows, long long target, cudaStrea
   return MIRT_OK;
 }
 
+// The plan's gather over slices [s0, s1) (all: s1 < 0): the TMA-staged tiles
+// when the plan has them, else the plain gather over the slices' positions.
+cudaError_t plan_gather(mirt_interp_plan *P, const float2 *ck, float2 *fm, cudaStream_t st,
+                        int s0 = 0, int s1 = -1) {
+  const int S = P->t.nslice;
+  if (s1 < 0) s1 = S;
+  if (P->gtma) {
+    const long long i0 = P->gitem_slice[s0], i1 = P->gitem_slice[s1];
+    return launch_gather_tma(P->ag, P->gbk, S, i0, i1 - i0, ck, fm, P->gfault.as<int>(), st);
+  }
+  InterpArgs ag = P->ag;
+  if (s0 > 0 || s1 < S) {
+    const long long q0 = P->moff_host[s0], nq = P->moff_host[s1] - q0;
+    ag.Mtot = nq;
+    ag.W += q0 * ag.SJ;
+    ag.K0 += q0;
+    if (ag.perm) ag.perm += q0;
+    if (ag.phase) ag.phase += q0;
+  }
+  return launch_gather(ag, P->lg, ck, fm, st);
+}
+
 int wrap_ok(const InterpArgs &a, const Tiling &t) {
   for (int d = 0; d < a.g.D; d++)
     if (a.g.K[d] < t.T[d] + a.g.J[d]) return 0;
@@ -650,16 +672,21 @@ int plan_finish(mirt_interp_plan *P, long long Mtot, const long long *moff, int 
   // in every dimension; the gather gets its own copy of the records in that
   // order, read sequentially
   P->ag = a;
+  P->gtma = 0;
   if (a.g.D > 1 && Mtot > 0) {
+    // 8-point blocks where the gather runs on TMA-staged tiles (2D, J = 6,
+    // 32-coil chunks), 4-point blocks otherwise
+    const int gbs = (gather_tma_ok(a) && P->lg.cw == 32) ? gather_tma_block() : 4;
     Tiling t4 = P->t;
     t4.nbins = 1;
     for (int d = 0; d < MIRT_DMAX; d++) {
-      t4.B[d] = d < a.g.D ? std::min(4, a.g.K[d]) : 1;
+      t4.B[d] = d < a.g.D ? std::min(gbs, a.g.K[d]) : 1;
       t4.nbin[d] = d < a.g.D ? (a.g.K[d] + t4.B[d] - 1) / t4.B[d] : 1;
       t4.nbins *= t4.nbin[d];
     }
     const long long nb4 = (long long)t4.nbins * nslice;
-    DMem keys4, bs4, tmp4;
+    DMem keys4, tmp4;
+    DMem &bs4 = P->gblk;
     CK(keys4.alloc(Mtot * sizeof(uint32_t)));
     CK(bs4.alloc((nb4 + 1) * sizeof(int)));
     CK(tmp4.alloc(radix_sort_tmp_bytes(Mtot)));
@@ -681,6 +708,27 @@ int plan_finish(mirt_interp_plan *P, long long Mtot, const long long *moff, int 
     P->ag.K0 = P->k0tap_g.as<int4>();
     P->ag.perm = P->perm_g.as<int>();
     P->ag.phase = a.phase ? P->phase_g.as<float2>() : nullptr;
+    if (gbs == gather_tma_block() && a.g.D == 2) {
+      // work items: up to gather_tma_item() samples of one non-empty block
+      std::vector<int> hb(nb4 + 1);
+      CK(cudaMemcpy(hb.data(), bs4.p, (nb4 + 1) * sizeof(int), cudaMemcpyDeviceToHost));
+      const int rc_n = gather_tma_item();
+      const long long per = (long long)t4.nbins;
+      std::vector<int2> items;
+      P->gitem_slice.assign(nslice + 1, 0);
+      for (long long bk = 0; bk < nb4; bk++) {
+        if (bk % per == 0) P->gitem_slice[bk / per] = (long long)items.size();
+        for (int p0 = hb[bk]; p0 < hb[bk + 1]; p0 += rc_n) items.push_back(make_int2((int)bk, p0));
+      }
+      P->gitem_slice[nslice] = (long long)items.size();
+      CK(P->gitem.alloc(std::max<size_t>(items.size(), 1) * sizeof(int2)));
+      if (!items.empty())
+        CK(cudaMemcpy(P->gitem.p, items.data(), items.size() * sizeof(int2), cudaMemcpyHostToDevice));
+      P->gbk = GatherBlocks{P->gblk.as<int>(), P->gitem.as<int2>(), gbs, t4.nbin[0], t4.nbin[1]};
+      CK(P->gfault.alloc(sizeof(int)));
+      CK(cudaMemset(P->gfault.p, 0, sizeof(int)));
+      P->gtma = 1;  // the default where it applies; the autotuner times both
+    }
   }
   int rc2 = build_tasks(P, st);
   if (rc2) return rc2;
@@ -842,7 +890,7 @@ int mirt_interp_plan_create(mirt_interp_plan **plan, int32_t D, const int32_t *K
 
 int mirt_interp_plan_forward(mirt_interp_plan *P, const void *ck, void *fm, void *stream) {
   if (!P) return fail(MIRT_ERR_ARG, "plan is NULL");
-  CK(launch_gather(P->ag, P->lg, static_cast<const float2 *>(ck), static_cast<float2 *>(fm),
+  CK(plan_gather(P, static_cast<const float2 *>(ck), static_cast<float2 *>(fm),
                    as_stream(stream)));
   return MIRT_OK;
 }
@@ -1005,9 +1053,12 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
     int rc = build_tasks(P, st);
     if (rc) return rc;
   }
-  // gather candidates: CTA size
+  // gather candidates: CTA size of the plain gather, and the TMA-staged gather
   Launch bestg = P->lg;
   float bestg_ms = 1e30f;
+  const int had_tma = P->gbk.item != nullptr;
+  int best_tma = 0;
+  P->gtma = 0;
   for (int threads : {64, 128, 256}) {
     Launch l = P->lg;
     l.threads = threads;
@@ -1023,6 +1074,19 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
       bestg = l;
     }
   }
+  if (had_tma) {
+    P->gtma = 1;
+    float ms = 0;
+    int rc = time_launch([&]() {
+      return plan_gather(P, grid.as<float2>(), samp.as<float2>(), st);
+    }, st, &ms);
+    if (rc) return rc;
+    if (ms < bestg_ms) {
+      bestg_ms = ms;
+      best_tma = 1;
+    }
+  }
+  P->gtma = best_tma;
   P->lg = bestg;
   CK(cudaStreamSynchronize(st));
   return MIRT_OK;
@@ -1030,11 +1094,32 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
 
 int mirt_interp_plan_config(mirt_interp_plan *P, int32_t *out, int32_t n) {
   if (!P || !out) return fail(MIRT_ERR_ARG, "NULL argument");
-  const int32_t v[20] = {P->t.T[0], P->t.T[1], P->t.T[2], P->ls.threads, P->heavy_first, P->ls.cw,
+  const int32_t v[21] = {P->t.T[0], P->t.T[1], P->t.T[2], P->ls.threads, P->heavy_first, P->ls.cw,
                          P->lg.threads, P->lg.sb, P->lg.grid, P->t.B[0], P->t.B[1], P->t.B[2],
                          P->split_chunk, P->t.ntask, P->t.padc, P->t.nred, P->ls.atomic,
-                         P->t.own, P->t.sweep, P->t.sweep_rows};
-  for (int i = 0; i < n && i < 20; i++) out[i] = v[i];
+                         P->t.own, P->t.sweep, P->t.sweep_rows, P->gtma};
+  for (int i = 0; i < n && i < 21; i++) out[i] = v[i];
+  return MIRT_OK;
+}
+
+int mirt_interp_plan_set_gather(mirt_interp_plan *P, int32_t tma) {
+  if (!P) return fail(MIRT_ERR_ARG, "plan is NULL");
+  if (tma && !P->gbk.item)
+    return fail(MIRT_ERR_ARG, "TMA gather needs 2D, J = 6, an even C >= 32 and K >= 13");
+  P->gtma = tma ? 1 : 0;
+  return MIRT_OK;
+}
+
+int mirt_interp_plan_fault(mirt_interp_plan *P, int32_t *fault) {
+  if (!P || !fault) return fail(MIRT_ERR_ARG, "NULL argument");
+  *fault = 0;
+  if (P->gfault.p) {
+    CK(cudaDeviceSynchronize());
+    int f = 0;
+    CK(cudaMemcpy(&f, P->gfault.p, sizeof(int), cudaMemcpyDeviceToHost));
+    CK(cudaMemset(P->gfault.p, 0, sizeof(int)));
+    *fault = f;
+  }
   return MIRT_OK;
 }
 
@@ -1823,7 +1908,7 @@ int mirt_nufft_forward(mirt_nufft *p, const void *x, void *X, void *stream) {
   if (rc) return rc;
   CK(launch_transpose_cols(p->grid_cm.as<float2>(), p->grid.as<float2>(), p->gg.ngrid, p->C,
                            p->nslice, 1, st, &p->gp));
-  CK(launch_gather(p->ip->ag, p->ip->lg, p->grid.as<float2>(), static_cast<float2 *>(X), st));
+  CK(plan_gather(p->ip, p->grid.as<float2>(), static_cast<float2 *>(X), st));
   return MIRT_OK;
 }
 
@@ -1862,16 +1947,8 @@ int nufft_forward_range(mirt_nufft *p, int s0, int s1, const float2 *x, float2 *
                   CUFFT_FORWARD));
   CK(launch_transpose_cols(gcm, p->grid.as<float2>() + s0 * gi, p->gg.ngrid, C, ns, 1, st,
                            &p->gp));
-  // the gather over the chunk's positions (slice-major in the gather order)
-  mirt_interp_plan *P = p->ip;
-  const long long q0 = P->moff_host[s0], nq = P->moff_host[s1] - q0;
-  InterpArgs ag = P->ag;
-  ag.Mtot = nq;
-  ag.W += q0 * ag.SJ;
-  ag.K0 += q0;
-  if (ag.perm) ag.perm += q0;
-  if (ag.phase) ag.phase += q0;
-  CK(launch_gather(ag, P->lg, p->grid.as<float2>(), X, st));
+  // the gather over the chunk's slices (slice-major in the gather order)
+  CK(plan_gather(p->ip, p->grid.as<float2>(), X, st, s0, s1));
   return MIRT_OK;
 }
 

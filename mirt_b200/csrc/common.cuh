@@ -55,12 +55,17 @@ __device__ __forceinline__ int wrapk(int k, int K) {
   return r < 0 ? r + K : r;
 }
 
+// The roundings are spelled out (one product, then one fused multiply-add per
+// part) so that every kernel computing a product gets the same bits, whatever
+// contraction the compiler would otherwise choose.
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
-  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+  return make_float2(__fmaf_rn(a.x, b.x, -__fmul_rn(a.y, b.y)),
+                     __fmaf_rn(a.x, b.y, __fmul_rn(a.y, b.x)));
 }
 // conj(a) * b
 __device__ __forceinline__ float2 cmulc(float2 a, float2 b) {
-  return make_float2(a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x);
+  return make_float2(__fmaf_rn(a.x, b.x, __fmul_rn(a.y, b.y)),
+                     __fmaf_rn(a.x, b.y, -__fmul_rn(a.y, b.x)));
 }
 
 }  // namespace mirt

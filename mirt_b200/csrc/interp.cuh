@@ -119,6 +119,26 @@ struct Launch {
                  // atomics (not bitwise reproducible); 0: one owner per point
 };
 
+// The gather over TMA-staged grid tiles and records (gather_tma.cu): 2D, J = 6,
+// C even and >= 32, K >= 13 per dimension.  Samples in the gather order are
+// grouped by gb x gb blocks of their first taps; start[b] is the first
+// position of block b = (slice * nby + by) * nbx + bx (start[nblocks] = Mtot);
+// a work item (block, first position) covers up to gather_tma_item() samples
+// of one block, items in block order.
+struct GatherBlocks {
+  const int *start;
+  const int2 *item;
+  int gb, nbx, nby;
+};
+bool gather_tma_ok(const InterpArgs &a);
+int gather_tma_block();
+int gather_tma_item();
+// items [it0, it0 + nit) of a batch of nslice slices; *fault is set when a
+// stage does not arrive within the kernel's wait limit
+cudaError_t launch_gather_tma(const InterpArgs &a, const GatherBlocks &g, int nslice,
+                              long long it0, long long nit, const float2 *ck, float2 *fm,
+                              int *fault, cudaStream_t st);
+
 // Compute the sort key of every sample: slice * nbins + bin of its first tap.
 cudaError_t launch_bin_keys(const InterpArgs &a, const Tiling &t, uint32_t *keys,
                             cudaStream_t st);

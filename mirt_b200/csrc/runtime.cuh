@@ -69,6 +69,12 @@ struct mirt_interp_plan {
   mirt::DMem wtap_g, k0tap_g, perm_g, phase_g;
   mirt::DMem swept;        // row-sweep spread: the samples in plan order, [Mtot][C]
   mirt::DMem sweep_teams;  // row-sweep spread: balanced team list (int4 per team)
+  // TMA gather: first position of each block of the gather order, work items
+  // (block, first position), the first item of each slice, fault flag
+  mirt::DMem gblk, gitem, gfault;
+  std::vector<long long> gitem_slice;
+  mirt::GatherBlocks gbk{};
+  int gtma = 0;            // 1: the gather runs on TMA-staged tiles
   int split_chunk = 1024;  // sample visits per spread task before a tile is split
   int heavy_first = 1;     // spread task order: 1 heaviest first, 0 grid order
   int deterministic = 1;   // 0: the spread may use shared-memory atomics

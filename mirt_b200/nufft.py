@@ -66,14 +66,14 @@ def minmax_kb_scale(N: int, J: int, K: int) -> np.ndarray:
 
 
 def _plan_config(lib, handle) -> dict:
-    v = (C.c_int32 * 20)()
-    check(lib.mirt_interp_plan_config(handle, v, 20))
+    v = (C.c_int32 * 21)()
+    check(lib.mirt_interp_plan_config(handle, v, 21))
     return {"spread_tile": [v[0], v[1], v[2]], "spread_threads": v[3], "spread_heavy_first": v[4],
             "coil_lanes": v[5], "gather_threads": v[6],
             "gather_ctas": v[8], "sort_bin": [v[9], v[10], v[11]], "split_chunk": v[12],
             "spread_tasks": v[13], "spread_padc": v[14], "spread_reductions": v[15],
             "spread_atomic": v[16], "spread_own": v[17], "spread_sweep": v[18],
-            "spread_sweep_rows": v[19]}
+            "spread_sweep_rows": v[19], "gather_tma": v[20]}
 
 
 class InterpPlan:
@@ -172,6 +172,19 @@ class InterpPlan:
         check(self.lib.mirt_interp_plan_set_sweep(self.handle, int(segments), int(rows)))
         return self.config()
 
+    def set_gather(self, tma=True):
+        """TMA-staged gather (2D, J = 6, even C >= 32) or the plain gather
+        (see mirt_interp_plan_set_gather)."""
+        check(self.lib.mirt_interp_plan_set_gather(self.handle, int(bool(tma))))
+        return self.config()
+
+    def fault(self):
+        """1 if an in-kernel wait ran out since the last call (see
+        mirt_interp_plan_fault), else 0."""
+        f = C.c_int32(0)
+        check(self.lib.mirt_interp_plan_fault(self.handle, C.byref(f)))
+        return f.value
+
     def set_spread(self, tile, threads=32, padc=0, stream=None):
         """Fix the spread tiling (tile extents per dimension, CTA size, spare
         tile columns 0 or J1 - 1) instead of autotuning it."""
@@ -267,6 +280,19 @@ class NufftPlan:
         check(self.lib.mirt_interp_plan_set_sweep(
             self.lib.mirt_nufft_interp_plan(self.handle), int(segments), int(rows)))
         return self.config()
+
+    def set_gather(self, tma=True):
+        """See InterpPlan.set_gather."""
+        check(self.lib.mirt_interp_plan_set_gather(self.lib.mirt_nufft_interp_plan(self.handle),
+                                                   int(bool(tma))))
+        return self.config()
+
+    def fault(self):
+        """See InterpPlan.fault."""
+        f = C.c_int32(0)
+        check(self.lib.mirt_interp_plan_fault(self.lib.mirt_nufft_interp_plan(self.handle),
+                                              C.byref(f)))
+        return f.value
 
     def capture(self, x=None, X=None, xa=None):
         """CUDA graph of forward x -> X (if x) then adjoint X -> xa (if xa) on

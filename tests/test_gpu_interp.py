@@ -430,3 +430,63 @@ def test_sweep_spread_refused_where_it_does_not_apply():
     with pytest.raises(mb.MirtError, match="row-sweep"):
         plan.set_sweep(True)
     plan.close()
+
+
+@pytest.mark.parametrize("C,K", [(32, (96, 64)), (40, (13, 27)), (64, (40, 33))])
+def test_tma_gather_matches_plain_gather_and_oracle(C, K):
+    """Gather over TMA-staged tiles and records (2D, J = 6, even C >= 32):
+    bitwise the plain gather (same arithmetic and order), the oracle's
+    forward to FP32 rounding, coil chunks (C = 40, 64), grids from 13 points
+    (where most blocks wrap and read the grid directly), a dense slice (blocks
+    split into several work items), coordinates far outside the grid, three
+    slices; the plan's fault flag stays clear."""
+    import torch
+    rng = np.random.default_rng(11 + C)
+    J, L = [6, 6], [1024, 1024]
+    h = [mb.minmax_kb_table(max(K[0] // 2, 6), 6, K[0], 1024),
+         mb.minmax_kb_table(max(K[1] // 2, 6), 6, K[1], 1024)]
+    tms = [rng.uniform(-40, 40, (2000, 2)), rng.uniform(-3, 3, (3000, 2)),
+           rng.uniform(-300, 300, (700, 2))]
+    moff = np.concatenate([[0], np.cumsum([len(t) for t in tms])])
+    plan = mb.InterpPlan(K, J, L, h, np.concatenate(tms), C, slice_moff=moff)
+    assert plan.config()["gather_tma"] == 1      # the default where it applies
+    ck = (rng.standard_normal((3, K[1], K[0], C)) + 1j * rng.standard_normal((3, K[1], K[0], C)))
+    ckd = torch.from_numpy(ck.astype(np.complex64)).cuda()
+    a = plan.forward(ckd).cpu().numpy()
+    assert plan.fault() == 0
+    plan.set_gather(False)
+    b = plan.forward(ckd).cpu().numpy()
+    assert np.array_equal(a, b)
+    for s in range(3):
+        ref = oracle.interp_for(np.transpose(ck[s], (1, 0, 2)).reshape(-1, C, order="F"), h, J, L,
+                                tms[s], K, 0, impl=ref_impl())
+        assert rel_l2(a[moff[s]:moff[s + 1]], ref) <= FWD_TOL, s
+    plan.close()
+
+
+def test_tma_gather_real_tables_phase_and_refusal():
+    """Real tables, first order, with a per-sample phase: the TMA gather equals
+    the plain gather and the oracle; a plan with C = 8 has no TMA blocks."""
+    import torch
+    rng = np.random.default_rng(3)
+    K, J, L = [48, 40], [6, 6], [256, 256]
+    h = [np.cos(np.linspace(-1.2, 1.2, 6 * 256 + 1)), np.exp(-np.linspace(-2, 2, 6 * 256 + 1) ** 2)]
+    tm = rng.uniform(-30, 30, (4000, 2))
+    ph = np.exp(1j * rng.uniform(-np.pi, np.pi, len(tm)))
+    plan = mb.InterpPlan(K, J, L, h, tm, 32, order=1, phase=ph)
+    plan.set_gather(True)
+    ck = rng.standard_normal((1, K[1], K[0], 32)) + 1j * rng.standard_normal((1, K[1], K[0], 32))
+    ckd = torch.from_numpy(ck.astype(np.complex64)).cuda()
+    a = plan.forward(ckd).cpu().numpy()
+    plan.set_gather(False)
+    assert np.array_equal(a, plan.forward(ckd).cpu().numpy())
+    ref = oracle.interp_for(np.transpose(ck[0], (1, 0, 2)).reshape(-1, 32, order="F"), h, J, L, tm,
+                            K, 1, impl=ref_impl()) * ph[:, None]
+    assert rel_l2(a, ref) <= FWD_TOL
+    assert plan.fault() == 0
+    plan.close()
+    p8 = mb.InterpPlan(K, J, L, h, tm, 8, order=1)
+    assert p8.config()["gather_tma"] == 0
+    with pytest.raises(mb.MirtError, match="TMA gather"):
+        p8.set_gather(True)
+    p8.close()
