@@ -157,11 +157,12 @@ def measured_peak():
 
 def traffic_from_profiles(call, workload, variant):
     """DRAM bytes of one gather or spread call (the sum over its kernels) recorded
-    from an ncu capture (profiles/traffic.json), for the plan's spread variant."""
+    from an ncu capture (profiles/traffic.json), for the plan's gather / spread
+    variant."""
     try:
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
             t = json.load(f)
-        return t.get(workload, {}).get(call if call == "gather" else f"spread_{variant}")
+        return t.get(workload, {}).get(f"{call}_{variant}")
     except (OSError, ValueError):
         return None
 
@@ -414,13 +415,14 @@ def run_gpu(args, w):
     peak, peak_kind = measured_peak()
     dom, tdom = ("spread", t_spread) if t_spread >= t_gather else ("gather", t_gather)
     achieved = B / tdom / 1e9
-    variant = "sweep" if tuned.get("spread_sweep", 0) != 0 else "tiled"
-    kernels = {"gather": "gather_kernel",
-               "spread": ("sweep_order_kernel + spread_sweep_kernel" if variant == "sweep"
+    variant = {"spread": "sweep" if tuned.get("spread_sweep", 0) != 0 else "tiled",
+               "gather": "tma" if tuned.get("gather_tma", 0) else "plain"}
+    kernels = {"gather": ("gather_tma_kernel" if variant["gather"] == "tma" else "gather_kernel"),
+               "spread": ("sweep_order_kernel + spread_sweep_kernel" if variant["spread"] == "sweep"
                           else "spread_kernel (+ spread_reduce_kernel)")}
     roof = {"bound": "hbm", "kernel": kernels[dom], "achieved": achieved, "peak": peak,
             "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
-            "traffic": traffic_from_profiles(dom, args.workload, variant),
+            "traffic": traffic_from_profiles(dom, args.workload, variant[dom]),
             "algorithmic_bytes": B,
             "gather": {"ms": 1e3 * t_gather, "GBps": B / t_gather / 1e9,
                        "frac": B / t_gather / 1e9 / peak},
