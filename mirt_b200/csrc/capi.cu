@@ -213,11 +213,7 @@ int build_sweep_teams(mirt_interp_plan *P, int rows, long long target, cudaStrea
     }
   }
   const double T = std::max(1.0, total / (double)std::max<long long>(target, 1));
-  struct Team {
-    double cost;  // kept for inspection; the list is in grid order
-    int4 k;
-  };
-  std::vector<Team> teams;
+  std::vector<int4> tk;  // (slice, first row, x0, x1), in grid order
   for (int s = 0; s < S; s++)
     for (int bi = 0; bi < nband; bi++) {
       const std::vector<float> &v = vb[(size_t)s * nband + bi];
@@ -233,16 +229,11 @@ int build_sweep_teams(mirt_interp_plan *P, int rows, long long target, cudaStrea
           c += add;
           x1++;
         }
-        if (K1 - x1 < 8) {  // a short tail joins this segment
-          for (int x = x1; x < K1; x++) c += vx(x) + alpha;
-          x1 = K1;
-        }
-        teams.push_back(Team{c, make_int4(s, bi * rows, x0, x1)});
+        if (K1 - x1 < 8) x1 = K1;  // a short tail joins this segment
+        tk.push_back(make_int4(s, bi * rows, x0, x1));
         x0 = x1;
       }
     }
-  std::vector<int4> tk(teams.size());
-  for (size_t i = 0; i < teams.size(); i++) tk[i] = teams[i].k;
   if (P->sweep_teams.bytes < tk.size() * sizeof(int4)) CK(P->sweep_teams.alloc(tk.size() * sizeof(int4)));
   CK(cudaMemcpyAsync(P->sweep_teams.p, tk.data(), tk.size() * sizeof(int4), cudaMemcpyHostToDevice,
                      st));

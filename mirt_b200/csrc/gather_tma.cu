@@ -53,7 +53,7 @@ __device__ __forceinline__ void mbar_expect(uint64_t *bar, unsigned bytes) {
                : "memory");
 }
 
-// 4-D tile copy (no multicast)
+// 4-D tile copy into this CTA's own shared memory
 __device__ __forceinline__ void tile_copy(const CUtensorMap *tm, void *dst, uint64_t *bar, int x,
                                           int y, int z, int w) {
   asm volatile(
