@@ -77,3 +77,27 @@ def test_builder_argument_errors():
         mb.newfft_kb_table(0, 16)
     with pytest.raises(mb.MirtError, match="positive"):
         mb.newfft_kb_scale(0, 6, 12, 0.0)
+
+
+def test_newfft_argument_checks_before_any_device_call():
+    """Mode, phasing, table and scaling-factor arguments are checked on the
+    host first, as newfft.m checks its options."""
+    om = np.zeros((4, 2))
+    with pytest.raises(ValueError, match="table0"):
+        mb.newfft(om, (16, 16), mode="sparse")
+    with pytest.raises(ValueError, match="phasing"):
+        mb.newfft(om, (16, 16), phasing="flipreal")
+    with pytest.raises(ValueError, match="built-in tables"):
+        mb.newfft(om, (16, 16), phasing="complex")
+    with pytest.raises(ValueError, match="sn is required"):
+        mb.newfft(om, (16, 16), tables=[np.ones(6 * 512 + 1)] * 2)
+
+
+def test_newfft_without_gpu_fails_loudly():
+    """No CPU fallback: without a device the plan cannot be made (the device
+    stream or the library's device check refuses)."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises((mb.MirtError, RuntimeError, AssertionError)):
+        mb.newfft(np.zeros((4, 2)), (16, 16))
