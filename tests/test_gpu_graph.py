@@ -12,13 +12,18 @@ from mirt_b200 import workloads as wl
 pytestmark = pytest.mark.gpu
 
 
-def test_graph_replay_matches_eager():
+@pytest.mark.parametrize("C", [8, 32])
+def test_graph_replay_matches_eager(C):
+    """C = 32: the captured step holds the TMA-staged gather (its tensor map a
+    by-value kernel parameter) and the row sweep with its ordering pass."""
     import torch
     rng = np.random.default_rng(11)
     om, moff, _ = wl.batch_ga_radial(3, 20, 40, 128, rng)
-    C = 8
     G = mb.NufftPlan(om, (64, 64), (6, 6), (128, 128), n_shift=(32, 32), Ld=1024, ncol=C,
                      slice_moff=moff)
+    if C == 32:
+        cfg = G.config()
+        assert cfg["gather_tma"] == 1 and cfg["spread_sweep"] != 0
     x = torch.randn(G.image_shape, dtype=torch.complex64, device="cuda")
     X = torch.empty(G.sample_shape, dtype=torch.complex64, device="cuda")
     xa = torch.empty(G.image_shape, dtype=torch.complex64, device="cuda")
