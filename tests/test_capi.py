@@ -111,3 +111,19 @@ def test_valid_call_without_gpu_fails_loudly():
         pytest.skip("a GPU is present")
     with pytest.raises(mb.MirtError, match="no CUDA device"):
         mb.interp2_table_mex(**_args2())
+
+
+def test_plan_setters_reject_null_plans():
+    """The spread / gather selectors, the fault read-out and the newfft
+    constructor check their pointers before touching a device."""
+    import ctypes as C
+    lib = _lib.load()
+    assert lib.mirt_interp_plan_set_sweep(None, 1, 1) == 1
+    assert "plan is NULL" in lib.mirt_last_error().decode()
+    assert lib.mirt_interp_plan_set_gather(None, 1) == 1
+    f = C.c_int32(7)
+    assert lib.mirt_interp_plan_fault(None, C.byref(f)) == 1
+    assert lib.mirt_interp_plan_set_deterministic(None, 1) == 1
+    assert lib.mirt_newfft_create(None, 2, None, None, None, None, None, None, 1, None, None, None,
+                                  None, None, 0, None, 1, 1, None) == 1
+    assert "output pointer is NULL" in lib.mirt_last_error().decode()
