@@ -101,3 +101,23 @@ def test_newfft_without_gpu_fails_loudly():
         pytest.skip("a GPU is present")
     with pytest.raises((mb.MirtError, RuntimeError, AssertionError)):
         mb.newfft(np.zeros((4, 2)), (16, 16))
+
+
+def test_oracle_complex_tables_without_phases_is_nufft():
+    """newfft with the min-max:KB complex tables and sn of nufft_init, no Nmid
+    phases and n_shift applied per sample, is the oracle's nufft (the identity
+    the GPU test checks for mirt_newfft_create against mirt_nufft_create)."""
+    import oracle
+    rng = np.random.default_rng(4)
+    om = rng.uniform(-np.pi, np.pi, (300, 2))
+    Nd, Jd, Kd, ns = (16, 12), (6, 6), (32, 24), np.array([8.0, 6.0])
+    st = nr.nufft_init_table(om, Nd, Jd, Kd, ns, 256)
+    sn = nr.scaling_factors(Nd, Jd, Kd)
+    so = nf.newfft_init(om, Nd, Jd, Kd, n_shift=ns, mode="table0", Ld=256, phasing="complex",
+                        h=st["h"], sn=sn)
+    so["phase_after"] = np.exp(1j * (om @ ns))          # n_shift only (no Nmid)
+    x = rng.standard_normal(Nd) + 1j * rng.standard_normal(Nd)
+    fw = lambda Xk, s: oracle.interp_for(Xk, s["h"], s["Jd"], s["Ld"], s["tm"], s["Kd"], 0)[:, 0]
+    a = nf.newfft_for(x, so)
+    b = nr.nufft(x, st, fw)
+    assert np.max(np.abs(a - b)) <= 1e-12 * np.max(np.abs(b))
