@@ -32,9 +32,17 @@ _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
 
 
+# the reference checkout whose nufft/table sources _ref/ is compiled from
+# (MIRT_REFERENCE overrides it); absent on hosts that only run the prebuilt _ref/
+REF_TREE = os.environ.get("MIRT_REFERENCE", "/root/reference")
+
+
 def build(quiet: bool = True) -> None:
     """Compile liboracle.so and, when the reference sources exist, _ref/libmirt_ref.so."""
-    out = subprocess.run(["make", "-C", HERE], capture_output=True, text=True)
+    cmd = ["make", "-C", HERE]
+    if os.path.isdir(os.path.join(REF_TREE, "nufft", "table")):
+        cmd.append(f"REF={REF_TREE}")
+    out = subprocess.run(cmd, capture_output=True, text=True)
     if out.returncode != 0:
         raise RuntimeError("oracle build failed:\n" + out.stdout + out.stderr)
 

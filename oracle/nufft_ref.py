@@ -274,5 +274,7 @@ def dtft_adj(X, om, Nd, n_shift, chunk=2048):
         elif len(Nd) == 2:
             x += np.einsum('m,ma,mb->ab', w, E[0], E[1], optimize=True)
         else:
-            x += np.einsum('m,ma,mb,mc->abc', w, E[0], E[1], E[2], optimize=True)
+            # separable: x[a, b, c] += sum_m E0[m, a] (w_m E1[m, b] E2[m, c]) as one matmul
+            B = (w[:, None] * E[1])[:, :, None] * E[2][:, None, :]
+            x += (E[0].T @ B.reshape(len(w), -1)).reshape(Nd)
     return x
