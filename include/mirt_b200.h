@@ -248,7 +248,11 @@ int mirt_interp_plan_set_gather(mirt_interp_plan *plan, int32_t tma);
 
 /* Fault flag of the plan's bounded in-kernel waits (TMA stage arrivals):
  * synchronises the device, stores 1 in *fault if a wait ran out since the
- * last call (the affected samples were not computed), else 0, and clears it.
+ * last call, else 0, and clears it.  After a 1, treat the plan as poisoned:
+ * the CTA whose wait ran out returned without computing its samples, and a
+ * copy that was only late may still have landed in shared memory after that
+ * CTA left, so no output of that launch, nor of kernels that ran beside it on
+ * the same GPU, can be trusted.  Destroy the plan and build a new one.
  * No reference counterpart. */
 int mirt_interp_plan_fault(mirt_interp_plan *plan, int32_t *fault);
 
@@ -497,9 +501,12 @@ int mirt_mlp_destroy(mirt_mlp *m);
  * MIRT_NOALLOC_SCRATCH_BYTES inside the library, held by every GPU that loads
  * the library until the process exits.  M is limited to
  * floor((MIRT_NOALLOC_SCRATCH_BYTES - 256) / (8 * (J1 + ... + JD) + 16))
- * samples (299,593 for J = 6 in 2D); larger M is rejected with
- * MIRT_ERR_ARG.  The first call on a device looks up the array's device
- * address, so make that first call before any stream capture.  All calls share
+ * samples (299,590 for J = 6 in 2D, 209,713 for J = 6 in 3D); larger M is
+ * rejected with MIRT_ERR_ARG.  The first call on a device looks up the array's
+ * device address and keeps it for the life of the process, so make that first
+ * call before any stream capture; resetting a device (cudaDeviceReset) while
+ * the library is loaded is not supported, since the kept address would then
+ * be stale.  All calls share
  * the array, which keeps the last call's contents (every call rewrites what it
  * reads, so nothing needs clearing): calls that overlap on the GPU, on any
  * streams, race.

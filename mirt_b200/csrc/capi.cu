@@ -1759,6 +1759,35 @@ int nufft_finish(mirt_nufft *p, int D, const int32_t *Nd, const int32_t *Kd, con
   }
   rc = plan_finish(P, Mtot, moff.data(), nslice, st);
   if (rc) return rc;
+  p->own_fft = ncol > 0;
+  for (int d = 0; d < D; d++)
+    if (!fft_len_ok(Kd[d])) p->own_fft = false;
+  if (p->own_fft) {
+    // fused FFT passes over the interpolation grid: twiddles exp(-2 pi i k / K_d) in FP64
+    std::vector<float2> tw;
+    long long off[3] = {0, 0, 0};
+    for (int d = 0; d < D; d++) {
+      off[d] = (long long)tw.size();
+      for (int k = 0; k < Kd[d]; k++) {
+        const double a = 2 * M_PI * (double)k / Kd[d];
+        tw.push_back(make_float2((float)std::cos(a), (float)-std::sin(a)));
+      }
+    }
+    cudaError_t e = p->twtab.alloc(tw.size() * sizeof(float2));
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(p->twtab.p, tw.data(), tw.size() * sizeof(float2),
+                          cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+      e = p->grid.alloc((size_t)nslice * p->gg.ngrid * ncol * sizeof(float2));
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return fail(MIRT_ERR_ALLOC, "NUFFT grid buffers");
+    p->nf.g = p->gg;
+    p->nf.C = ncol;
+    for (int d = 0; d < 3; d++) p->nf.tw[d] = d < D ? p->twtab.as<float2>() + off[d] : nullptr;
+    p->nf.sn = p->sn.as<float2>();
+    p->nf.gp = &p->gp;
+    return MIRT_OK;
+  }
   {
     cudaError_t e = p->grid.alloc((size_t)nslice * p->gg.ngrid * ncol * sizeof(float2));
     if (e == cudaSuccess) e = p->grid_cm.alloc((size_t)nslice * p->gg.ngrid * ncol * sizeof(float2));
@@ -1893,6 +1922,12 @@ int mirt_nufft_forward(mirt_nufft *p, const void *x, void *X, void *stream) {
   if (!p) return fail(MIRT_ERR_ARG, "nufft is NULL");
   if (p->C == 0) return MIRT_OK;
   cudaStream_t st = as_stream(stream);
+  if (p->own_fft) {
+    CK(fft_nufft_forward(p->nf, static_cast<const float2 *>(x), p->grid.as<float2>(), 0,
+                         p->nslice, st));
+    CK(plan_gather(p->ip, p->grid.as<float2>(), static_cast<float2 *>(X), st));
+    return MIRT_OK;
+  }
   CK(launch_deapod_image_cm(static_cast<const float2 *>(x), p->sn.as<float2>(),
                             p->pad.as<float2>(), p->gg, p->C, p->nslice, st));
   int rc = nufft_fft(p, CUFFT_FORWARD, st);
@@ -1910,6 +1945,10 @@ int mirt_nufft_adjoint(mirt_nufft *p, const void *X, void *x, void *stream) {
   mirt_interp_plan *P = p->ip;
   CK(launch_spread(P->a, P->t, P->ls, P->bin_start.as<int>(), static_cast<const float2 *>(X),
                    p->grid.as<float2>(), st));
+  if (p->own_fft) {
+    CK(fft_nufft_adjoint(p->nf, p->grid.as<float2>(), static_cast<float2 *>(x), 0, p->nslice, st));
+    return MIRT_OK;
+  }
   CK(launch_transpose_cols(p->grid.as<float2>(), p->grid_cm.as<float2>(), p->gg.ngrid, p->C,
                            p->nslice, 0, st, &p->gp));
   int rc = nufft_fft(p, CUFFT_INVERSE, st);
@@ -1930,6 +1969,11 @@ int nufft_forward_range(mirt_nufft *p, int s0, int s1, const float2 *x, float2 *
                         cufftHandle fft, cudaStream_t st) {
   const int ns = s1 - s0, C = p->C;
   const long long gi = p->gg.ngrid * C, xi = p->gg.npix * C;
+  if (p->own_fft) {
+    CK(fft_nufft_forward(p->nf, x, p->grid.as<float2>(), s0, s1, st));
+    CK(plan_gather(p->ip, p->grid.as<float2>(), X, st, s0, s1));
+    return MIRT_OK;
+  }
   float2 *pad = p->pad.as<float2>() + s0 * gi;
   float2 *gcm = p->grid_cm.as<float2>() + s0 * gi;
   CK(launch_deapod_image_cm(x + s0 * xi, p->sn.as<float2>(), pad, p->gg, C, ns, st));
@@ -1957,6 +2001,10 @@ int nufft_adjoint_range(mirt_nufft *p, int s0, int s1, const float2 *X, float2 *
   t.pos0 = P->moff_host[s0];
   t.npos = P->moff_host[s1] - t.pos0;
   CK(launch_spread(P->a, t, P->ls, P->bin_start.as<int>(), X, p->grid.as<float2>(), st));
+  if (p->own_fft) {
+    CK(fft_nufft_adjoint(p->nf, p->grid.as<float2>(), x, s0, s1, st));
+    return MIRT_OK;
+  }
   float2 *gcm = p->grid_cm.as<float2>() + s0 * gi;
   CK(launch_transpose_cols(p->grid.as<float2>() + s0 * gi, gcm, p->gg.ngrid, C, ns, 0, st,
                            &p->gp));
@@ -1985,6 +2033,7 @@ int host_pipeline_setup(mirt_nufft *p) {
     CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     p->ev.push_back(e);
   }
+  if (p->own_fft) return MIRT_OK;  // the FFT passes take slice ranges directly
   const int sizes[2] = {ch, p->nslice - (nch - 1) * ch};
   int n[3];
   for (int d = 0; d < p->gg.D; d++) n[d] = p->gg.K[p->gg.D - 1 - d];

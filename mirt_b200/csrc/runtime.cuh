@@ -9,6 +9,7 @@
 #include <utility>
 #include <vector>
 
+#include "fft.cuh"
 #include "glue.cuh"
 #include "interp.cuh"
 
@@ -94,6 +95,11 @@ struct mirt_nufft {
   mirt::GridPhase gp{};                  // tables into phtab (tab[0] null: no grid phase)
   cufftHandle fft = 0;
   bool fft_ok = false;
+  // power-of-two grids from 64 to 1024 points per dimension: the FFT runs as
+  // fused passes over `grid` itself (fft.cu) and grid_cm / pad / cuFFT are unused
+  bool own_fft = false;
+  mirt::DMem twtab;                      // exp(-2 pi i k / K_d) per dimension, float2 [sum K_d]
+  mirt::NufftFft nf{};
   // host-buffer calls, pipelined by slice chunks: copy streams, per-chunk
   // events and the FFT plans of the chunk sizes (made at the first such call)
   cudaStream_t cs_in = nullptr, cs_out = nullptr;
