@@ -328,6 +328,8 @@ def run_gpu(args, w):
     tuned = plan.autotune() if not args.no_autotune else plan.config()
     if args.spread == "sweep" and tuned.get("spread_sweep", 0) == 0:
         tuned = plan.set_sweep(-1, 1)        # the plan's default: balanced teams of one row
+    elif args.spread == "list" and tuned.get("spread_sweep", 0) != -1:
+        tuned = plan.set_sweep(-1, args.sweep_rows)   # visit-list sweep
     elif args.spread == "tiled" and tuned.get("spread_sweep", 0) != 0:
         tuned = plan.set_sweep(0)
     t_tune = time.perf_counter() - t0
@@ -417,8 +419,10 @@ def run_gpu(args, w):
     achieved = B / tdom / 1e9
     variant = {"spread": "sweep" if tuned.get("spread_sweep", 0) != 0 else "tiled",
                "gather": "tma" if tuned.get("gather_tma", 0) else "plain"}
+    sweep_kernel = ("spread_list_kernel" if tuned.get("spread_sweep", 0) == -1
+                    else "sweep_order_kernel + spread_sweep_kernel")
     kernels = {"gather": ("gather_tma_kernel" if variant["gather"] == "tma" else "gather_kernel"),
-               "spread": ("sweep_order_kernel + spread_sweep_kernel" if variant["spread"] == "sweep"
+               "spread": (sweep_kernel if variant["spread"] == "sweep"
                           else "spread_kernel (+ spread_reduce_kernel)")}
     roof = {"bound": "hbm", "kernel": kernels[dom], "achieved": achieved, "peak": peak,
             "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
@@ -466,14 +470,10 @@ def run_gpu(args, w):
                "sample": f"{ns} of {plan.nslice} slices, forward + adjoint, {C} coils "
                          f"({u:.3g} sample-coils in {tc:.1f} s)"}
 
-    # deapodise, forward transpose, gather, crop (cuFFT not counted), and the spread:
-    # row sweep = sample ordering + sweep into the coil-major grid; tiled = spread
-    # [+ reductions] + the adjoint transpose
-    if tuned.get("spread_sweep", 0) != 0:
-        spread_launches = 2
-    else:
-        spread_launches = 2 + (1 if tuned.get("spread_reductions", 0) > 0 else 0)
-    launches_per_step = 4 + spread_launches
+    # the library's own launches per forward + adjoint (FFT passes or, with cuFFT,
+    # the deapodise / transpose / crop kernels; gather; spread), cuFFT not counted
+    fcfg = plan.fft_config()
+    launches_per_step = fcfg["launches_forward"] + fcfg["launches_adjoint"]
     cg = None
     if rank == 0 and world == 1 and not args.no_cg and w["D"] == 2:
         cg = run_cgsense(args)
@@ -648,7 +648,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
-    ap.add_argument("--spread", default="auto", choices=["auto", "sweep", "tiled"],
+    ap.add_argument("--sweep-rows", type=int, default=1, help="rows per band for --spread list")
+    ap.add_argument("--spread", default="auto", choices=["auto", "sweep", "list", "tiled"],
                     help="spread variant: the autotuner's choice, or the row sweep / tiled spread")
     ap.add_argument("--nondeterministic", action="store_true",
                     help="let the spread add with shared-memory atomics (not bitwise reproducible)")

@@ -300,6 +300,13 @@ mirt_interp_plan *mirt_nufft_interp_plan(mirt_nufft *p);
 /* mirt_interp_plan_autotune on the NUFFT's interpolation plan. */
 int mirt_nufft_autotune(mirt_nufft *p, void *stream);
 
+/* How the NUFFT runs: up to 3 values {1 if the oversampled FFT runs as the
+ * library's fused passes over the interpolation grid (power-of-two K from
+ * 64 to 1024 in every dimension), 0 if through cuFFT with coil-layout
+ * transposes; library kernel launches of one forward; of one adjoint} (cuFFT's
+ * own launches not counted).  No reference counterpart. */
+int mirt_nufft_config(mirt_nufft *p, int32_t *out, int32_t n);
+
 int mirt_nufft_destroy(mirt_nufft *p);
 
 /* ------------------------------------------------------------------------

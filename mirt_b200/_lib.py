@@ -103,6 +103,7 @@ _SIGS = {
     "mirt_nufft_adjoint_host": ([_vp, _fp, _fp, _vp], C.c_int),
     "mirt_nufft_interp_plan": ([_vp], _vp),
     "mirt_nufft_autotune": ([_vp, _vp], C.c_int),
+    "mirt_nufft_config": ([_vp, _i32p, _i32], C.c_int),
     "mirt_nufft_destroy": ([_vp], C.c_int),
     "mirt_interp_gather_noalloc": ([_i32, _i32p, _i32p, _i32p, C.POINTER(_vp), _i32, _i32, _dp,
                                     _i64, _i32, _vp, _vp, _vp], C.c_int),

@@ -9,6 +9,9 @@
 
 #include <cufft.h>
 
+#include <cstdio>
+#include <cstdlib>
+
 #include <cmath>
 #include <complex>
 #include <algorithm>
@@ -185,38 +188,103 @@ int sweep_buffer(mirt_interp_plan *P) {
 // in all, in grid order (neighbouring bands read the same samples, so they
 // run together; heaviest-first order measured slower at full size).  Teams
 // write disjoint points, each summed in the same fixed order.
-int build_sweep_teams(mirt_interp_plan *P, int rows, long long target, cudaStream_t st) {
+// Visits per bin column of every band of `rows` grid rows: vb[(s * nband +
+// band) * K1 + x] = samples in bin column x of the band's rows + 5 bin rows.
+int sweep_band_visits(mirt_interp_plan *P, int rows, cudaStream_t st, std::vector<float> &vb) {
   const InterpArgs &a = P->a;
-  Tiling &t = P->t;
+  const Tiling &t = P->t;
   const int K1 = a.g.K[0], K2 = a.g.K[1], S = t.nslice, NQ = rows + 5;
   const long long nb = (long long)t.nbins * S;
   std::vector<int> bs(nb + 1);
   CK(cudaMemcpyAsync(bs.data(), P->bin_start.p, (nb + 1) * sizeof(int), cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
-  const double alpha = 2.0;
   const int nband = (K2 + rows - 1) / rows;
-  // visits per bin column of every band: v[x] = sum over its NQ bin rows
-  std::vector<std::vector<float>> vb((size_t)S * nband);
-  double total = 0;
+  vb.assign((size_t)S * nband * K1, 0.f);
   for (int s = 0; s < S; s++) {
     const int *b = bs.data() + (size_t)s * t.nbins;
     for (int bi = 0; bi < nband; bi++) {
-      std::vector<float> &v = vb[(size_t)s * nband + bi];
-      v.assign(K1, 0.f);
+      float *v = vb.data() + ((size_t)s * nband + bi) * K1;
       for (int q = 0; q < NQ; q++) {
         int r = (bi * rows - 5 + q) % K2;
         if (r < 0) r += K2;
         const int *br = b + (size_t)r * K1;
         for (int x = 0; x < K1; x++) v[x] += (float)(br[x + 1] - br[x]);
       }
-      for (int x = 0; x < K1; x++) total += v[x] + alpha;
     }
   }
+  return MIRT_OK;
+}
+
+// cost of a team: its visits (five warm-up columns included) + 2 per column step
+constexpr double kSweepColumnCost = 2.0;
+
+double sweep_team_cost(const float *v, int K1, int x0, int x1) {
+  double c = 0;
+  for (int x = x0 - 5; x < x1; x++) c += v[(x % K1 + K1) % K1] + kSweepColumnCost;
+  return c;
+}
+
+// The sweep's work queue: teams heaviest first (ties in index order), and the
+// queue counter.  Teams are the list (t.sweep < 0) or the uniform segments.
+int build_sweep_order(mirt_interp_plan *P, const std::vector<float> &vb, cudaStream_t st) {
+  const InterpArgs &a = P->a;
+  Tiling &t = P->t;
+  const int K1 = a.g.K[0], K2 = a.g.K[1], rows = t.sweep_rows;
+  const int nband = (K2 + rows - 1) / rows;
+  std::vector<int4> tk;
+  if (t.sweep < 0) {
+    tk = P->team_host;
+  } else {
+    const int nseg = t.sweep, sw = (K1 + nseg - 1) / nseg;
+    for (int s = 0; s < t.nslice; s++)
+      for (int bi = 0; bi < nband; bi++)
+        for (int g = 0; g < nseg; g++)
+          tk.push_back(make_int4(s, bi * rows, g * sw, std::min(K1, g * sw + sw)));
+  }
+  std::vector<double> cost(tk.size());
+  for (size_t i = 0; i < tk.size(); i++) {
+    const int4 k = tk[i];
+    cost[i] = k.z < k.w ? sweep_team_cost(vb.data() + ((size_t)k.x * nband + k.y / rows) * K1, K1,
+                                          k.z, k.w)
+                        : 0.0;
+  }
+  std::vector<int> order(tk.size());
+  for (size_t i = 0; i < order.size(); i++) order[i] = (int)i;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cost[x] > cost[y]; });
+  if (P->team_order.bytes < std::max<size_t>(order.size(), 1) * sizeof(int))
+    CK(P->team_order.alloc(std::max<size_t>(order.size(), 1) * sizeof(int)));
+  if (!order.empty())
+    CK(cudaMemcpyAsync(P->team_order.p, order.data(), order.size() * sizeof(int),
+                       cudaMemcpyHostToDevice, st));
+  // one queue counter per coil chunk
+  const size_t nq = (size_t)std::max(1, (a.C + P->ls.cw - 1) / std::max(P->ls.cw, 1));
+  if (P->team_next.bytes < nq * sizeof(int)) CK(P->team_next.alloc(nq * sizeof(int)));
+  CK(cudaStreamSynchronize(st));
+  t.team_order = P->team_order.as<int>();
+  t.team_next = P->team_next.as<int>();
+  return MIRT_OK;
+}
+
+// Balanced row-sweep teams: each band of `rows` grid rows of each slice is
+// cut into column segments of about equal cost (sweep_team_cost), segments of
+// at least 8 columns, about `target` teams in all.  Teams write disjoint
+// points, each summed in the same fixed order.
+int build_sweep_teams(mirt_interp_plan *P, int rows, long long target, cudaStream_t st) {
+  const InterpArgs &a = P->a;
+  Tiling &t = P->t;
+  const int K1 = a.g.K[0], K2 = a.g.K[1], S = t.nslice;
+  std::vector<float> vb;
+  int rc = sweep_band_visits(P, rows, st, vb);
+  if (rc) return rc;
+  const double alpha = kSweepColumnCost;
+  const int nband = (K2 + rows - 1) / rows;
+  double total = 0;
+  for (float v : vb) total += v + alpha;
   const double T = std::max(1.0, total / (double)std::max<long long>(target, 1));
   std::vector<int4> tk;  // (slice, first row, x0, x1), in grid order
   for (int s = 0; s < S; s++)
     for (int bi = 0; bi < nband; bi++) {
-      const std::vector<float> &v = vb[(size_t)s * nband + bi];
+      const float *v = vb.data() + ((size_t)s * nband + bi) * K1;
       auto vx = [&](int x) { return (double)v[(x % K1 + K1) % K1]; };
       int x0 = 0;
       while (x0 < K1) {
@@ -238,11 +306,22 @@ int build_sweep_teams(mirt_interp_plan *P, int rows, long long target, cudaStrea
   CK(cudaMemcpyAsync(P->sweep_teams.p, tk.data(), tk.size() * sizeof(int4), cudaMemcpyHostToDevice,
                      st));
   CK(cudaStreamSynchronize(st));
+  P->team_host = tk;
   t.sweep_team = P->sweep_teams.as<int4>();
   t.nteams = (int)tk.size();
   t.sweep = -1;
   t.sweep_rows = rows;
-  return MIRT_OK;
+  return build_sweep_order(P, vb, st);
+}
+
+// Uniform segments: the work queue of their teams.
+int set_uniform_sweep(mirt_interp_plan *P, int nseg, int rows, cudaStream_t st) {
+  P->t.sweep = nseg;
+  P->t.sweep_rows = rows;
+  std::vector<float> vb;
+  int rc = sweep_band_visits(P, rows, st, vb);
+  if (rc) return rc;
+  return build_sweep_order(P, vb, st);
 }
 
 // The plan's gather over slices [s0, s1) (all: s1 < 0): the TMA-staged tiles
@@ -321,6 +400,8 @@ void choose_config(mirt_interp_plan *P) {
   t.npos = -1;
   t.sweep_team = nullptr;
   t.nteams = 0;
+  t.team_order = nullptr;
+  t.team_next = nullptr;
   t.nbins = 1;
   t.ntiles = 1;
   for (int d = 0; d < MIRT_DMAX; d++) {
@@ -766,6 +847,13 @@ int padc_max(const InterpArgs &a) {
   return 5;
 }
 
+// MIRT_AUTOTUNE_LOG=1 in the environment: the autotuner prints every
+// candidate's time to stderr.
+bool autotune_log() {
+  const char *v = std::getenv("MIRT_AUTOTUNE_LOG");
+  return v && v[0] && v[0] != '0';
+}
+
 // Time `fn` (one launch) on the stream: one warm-up, then the best of 3.
 template <class F>
 int time_launch(F fn, cudaStream_t st, float *ms) {
@@ -969,13 +1057,19 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
                                    nseg, rows});
   SpreadCand best{};
   float best_ms = 1e30f;
+  int built_rows = 0;  // rows of the team list last built
   for (const SpreadCand &c : cands) {
     P->t.own = c.own;
     P->t.sweep = c.sweep;
     P->t.sweep_rows = c.sweep_rows;
-    if (c.sweep < 0) {
+    if (c.sweep < 0 && built_rows != c.sweep_rows) {
       int rc = build_sweep_teams(P, c.sweep_rows, 65536, st);
       if (rc) return rc;
+      built_rows = c.sweep_rows;
+    } else if (c.sweep > 0) {
+      int rc = set_uniform_sweep(P, c.sweep, c.sweep_rows, st);
+      if (rc) return rc;
+      built_rows = 0;  // the work queue now orders uniform segments
     }
     int rc = set_spread_tiles(P, c.T, st);
     if (rc) continue;
@@ -988,6 +1082,12 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
                            grid.as<float2>(), st);
     }, st, &ms);
     if (rc) return rc;
+    if (autotune_log())
+      std::fprintf(stderr,
+                   "mirt autotune spread: tile %dx%dx%d threads %d padc %d atomic %d own %d "
+                   "sweep %d rows %d: %.3f ms\n",
+                   c.T[0], c.T[1], c.T[2], c.threads, c.padc, c.atomic, c.own, c.sweep,
+                   c.sweep_rows, ms);
     if (ms < best_ms) {
       best_ms = ms;
       best = c;
@@ -997,8 +1097,11 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
     P->t.own = best.own;
     P->t.sweep = best.sweep;
     P->t.sweep_rows = best.sweep_rows;
-    if (best.sweep < 0) {
+    if (best.sweep < 0 && built_rows != best.sweep_rows) {
       int rc = build_sweep_teams(P, best.sweep_rows, 65536, st);
+      if (rc) return rc;
+    } else if (best.sweep > 0) {
+      int rc = set_uniform_sweep(P, best.sweep, best.sweep_rows, st);
       if (rc) return rc;
     }
     int rc = set_spread_tiles(P, best.T, st);
@@ -1128,6 +1231,9 @@ int mirt_interp_plan_set_sweep(mirt_interp_plan *P, int32_t segments, int32_t ro
   }
   if (segments < 0) {
     int rc = build_sweep_teams(P, rows, 65536, as_stream(nullptr));
+    if (rc) return rc;
+  } else if (segments > 0) {
+    int rc = set_uniform_sweep(P, segments, rows, as_stream(nullptr));
     if (rc) return rc;
   }
   P->t.sweep = segments;
@@ -1996,6 +2102,7 @@ int nufft_adjoint_range(mirt_nufft *p, int s0, int s1, const float2 *X, float2 *
   mirt_interp_plan *P = p->ip;
   Tiling t = P->t;
   if (t.sweep < 0) t.sweep = 2;  // a chunk: uniform halves of rows (same sums)
+  t.team_order = nullptr;        // the chunk's teams in index order
   t.slice0 = s0;
   t.nslice = ns;
   t.pos0 = P->moff_host[s0];
@@ -2187,6 +2294,27 @@ int mirt_graph_destroy(mirt_graph *g) {
 int mirt_nufft_autotune(mirt_nufft *p, void *stream) {
   if (!p) return fail(MIRT_ERR_ARG, "nufft is NULL");
   return mirt_interp_plan_autotune(p->ip, stream);
+}
+
+int mirt_nufft_config(mirt_nufft *p, int32_t *out, int32_t n) {
+  if (!p || !out) return fail(MIRT_ERR_ARG, "NULL argument");
+  const Tiling &t = p->ip->t;
+  // gather: one launch (TMA-staged or plain)
+  const int fwd = (p->own_fft ? p->gg.D : 2) + 1;
+  int spread = 1;
+  if (t.sweep != 0) {
+    spread = 2;  // ordering pass and sweep (and a memset of the work-queue counters)
+  } else if (t.own) {
+    spread = 1;  // the clearing memset, then per colour a launch and a reduction
+    for (int c = 0; c < 4; c++)
+      spread += (t.color_beg[c + 1] > t.color_beg[c]) + (t.red_beg[c + 1] > t.red_beg[c]);
+  } else {
+    spread = (t.ntask > 0) + (t.nred > 0);
+  }
+  const int adj = spread + (p->own_fft ? p->gg.D : 2);
+  const int32_t v[3] = {p->own_fft ? 1 : 0, fwd, adj};
+  for (int i = 0; i < n && i < 3; i++) out[i] = v[i];
+  return MIRT_OK;
 }
 
 int mirt_nufft_destroy(mirt_nufft *p) {

@@ -11,6 +11,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <utility>
+
 #define MIRT_DMAX 3
 #define MIRT_JMAX 16
 
@@ -66,6 +68,17 @@ __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
 __device__ __forceinline__ float2 cmulc(float2 a, float2 b) {
   return make_float2(__fmaf_rn(a.x, b.x, __fmul_rn(a.y, b.y)),
                      __fmaf_rn(a.x, b.y, -__fmul_rn(a.y, b.x)));
+}
+
+// Static loop: f(std::integral_constant<int, i>{}) for i = 0 .. N-1, so that
+// the index is a compile-time constant inside the body.
+template <class F, int... I>
+__device__ __forceinline__ void sfor_impl(F &f, std::integer_sequence<int, I...>) {
+  (f(std::integral_constant<int, I>{}), ...);
+}
+template <int N, class F>
+__device__ __forceinline__ void sfor(F &&f) {
+  sfor_impl(f, std::make_integer_sequence<int, N>{});
 }
 
 }  // namespace mirt

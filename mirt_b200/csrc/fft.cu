@@ -94,16 +94,6 @@ __device__ __forceinline__ float2 twmul(float2 v) {
   }
 }
 
-// static loop: f(std::integral_constant<int, i>) for i = 0 .. N-1
-template <class F, int... I>
-__device__ __forceinline__ void sfor_(F &f, std::integer_sequence<int, I...>) {
-  (f(std::integral_constant<int, I>{}), ...);
-}
-template <int N, class F>
-__device__ __forceinline__ void sfor(F &&f) {
-  sfor_(f, std::make_integer_sequence<int, N>{});
-}
-
 // In-place DFT of R values in natural order.  R = A * B: A DFTs of length B on
 // the stride-A subsequences, twiddles W_R^{a k1}, then B DFTs of length A.
 template <int R, bool INV>

@@ -72,6 +72,11 @@ struct Tiling {
   // first (segments of about equal visit counts, from the sort's bins).
   const int4 *sweep_team;
   int nteams;
+  // Row sweep work queue: teams are taken by warps in the order team_order
+  // (heaviest first; null: index order) through the counters team_next[coil
+  // chunk], which are cleared before every launch.
+  const int *team_order;
+  int *team_next;
   int color_beg[9];
   int red_beg[9];
   int padc;              // spread: spare columns on each side of a tile row in

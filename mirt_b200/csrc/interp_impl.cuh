@@ -685,17 +685,16 @@ __global__ void __launch_bounds__(256) sweep_order_kernel(InterpArgs a, const fl
   }
 }
 
+// The sweep of one team (see spread_sweep_kernel).
 template <int CW, int R, bool REAL>
-__global__ void __launch_bounds__(256) spread_sweep_kernel(InterpArgs a, Tiling t,
-                                                           const int *__restrict__ bin_start,
-                                                           const float2 *__restrict__ fs,
-                                                           float2 *__restrict__ ck) {
+__device__ __forceinline__ void sweep_team(const InterpArgs &a, const Tiling &t,
+                                           const int *__restrict__ bin_start,
+                                           const float2 *__restrict__ fs,
+                                           float2 *__restrict__ ck, long long team) {
   constexpr int NQ = R + 5;  // bin rows reaching the band
   const int K1 = a.g.K[0], K2 = a.g.K[1];
-  const long long team = ((long long)blockIdx.x * blockDim.x + threadIdx.x) / CW;
   int slice, y0, x0, x1;
   if (t.sweep < 0) {
-    if (team >= t.nteams) return;  // the team's lanes leave together
     const int4 tk = t.sweep_team[team];
     slice = tk.x;
     y0 = tk.y;
@@ -704,7 +703,6 @@ __global__ void __launch_bounds__(256) spread_sweep_kernel(InterpArgs a, Tiling 
   } else {
     const int nseg = t.sweep;
     const int nband = (K2 + R - 1) / R;
-    if (team >= (long long)t.nslice * nband * nseg) return;
     const int seg = (int)(team % nseg);
     const long long bandid = team / nseg;
     const int sl = (int)(bandid / nband);
@@ -781,6 +779,33 @@ __global__ void __launch_bounds__(256) spread_sweep_kernel(InterpArgs a, Tiling 
 #pragma unroll
       for (int j = 0; j < 5; j++) acc[r][j] = acc[r][j + 1];
       acc[r][5] = make_float2(0.f, 0.f);
+    }
+  }
+}
+
+// Persistent row sweep: every warp takes 32 / CW teams at a time from the
+// plan's work queue (heaviest teams first) until the queue is empty, so warps
+// do not sit idle behind a heavy team of their block.  Each team's sums are
+// independent of which warp runs it: deterministic.
+template <int CW, int R, bool REAL>
+__global__ void __launch_bounds__(256) spread_sweep_kernel(InterpArgs a, Tiling t,
+                                                           const int *__restrict__ bin_start,
+                                                           const float2 *__restrict__ fs,
+                                                           float2 *__restrict__ ck) {
+  constexpr int G = 32 / CW;
+  const int lane = threadIdx.x & 31;
+  const long long nteam =
+      t.sweep < 0 ? (long long)t.nteams
+                  : (long long)t.nslice * ((a.g.K[1] + R - 1) / R) * t.sweep;
+  for (;;) {
+    int base = 0;
+    if (lane == 0) base = atomicAdd(t.team_next + blockIdx.y, G);  // queue of this coil chunk
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= nteam) break;
+    const long long qi = (long long)base + lane / CW;
+    if (qi < nteam) {
+      const long long team = t.team_order ? (long long)__ldg(t.team_order + qi) : qi;
+      sweep_team<CW, R, REAL>(a, t, bin_start, fs, ck, team);
     }
   }
 }
@@ -1083,22 +1108,29 @@ cudaError_t run(Req &r) {
           cudaError_t e = cudaGetLastError();
           if (e != cudaSuccess) return e;
         }
-        const dim3 grid((unsigned)((thr + 255) / 256), nchunk);
+        if (!t.team_next) return cudaErrorInvalidValue;
         const float2 *fs = t.sorted;
+        auto go = [&](auto kern) -> cudaError_t {
+          // persistent: the blocks that fit on the GPU at once (per coil chunk)
+          int per_sm = 0, dev = 0, nsm = 0;
+          cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0);
+          if (e != cudaSuccess) return e;
+          cudaGetDevice(&dev);
+          cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+          long long nb = (long long)nsm * (per_sm > 0 ? per_sm : 1);
+          const long long need = (thr + 255) / 256;
+          if (nb > need) nb = need;
+          e = cudaMemsetAsync(t.team_next, 0, nchunk * sizeof(int), r.st);
+          if (e != cudaSuccess) return e;
+          kern<<<dim3((unsigned)nb, nchunk), 256, 0, r.st>>>(a, t, r.bin_start, fs, r.out);
+          return cudaGetLastError();
+        };
         switch (t.sweep_rows) {
-          case 1:
-            spread_sweep_kernel<CW, 1, REAL><<<grid, 256, 0, r.st>>>(a, t, r.bin_start, fs, r.out);
-            break;
-          case 2:
-            spread_sweep_kernel<CW, 2, REAL><<<grid, 256, 0, r.st>>>(a, t, r.bin_start, fs, r.out);
-            break;
-          case 4:
-            spread_sweep_kernel<CW, 4, REAL><<<grid, 256, 0, r.st>>>(a, t, r.bin_start, fs, r.out);
-            break;
-          default:
-            return cudaErrorInvalidValue;
+          case 1: return go(spread_sweep_kernel<CW, 1, REAL>);
+          case 2: return go(spread_sweep_kernel<CW, 2, REAL>);
+          case 4: return go(spread_sweep_kernel<CW, 4, REAL>);
+          default: return cudaErrorInvalidValue;
         }
-        return cudaGetLastError();
       }
       if (t.own) {
         // cleared grid, then one launch (and one reduction) per colour

@@ -70,6 +70,8 @@ struct mirt_interp_plan {
   mirt::DMem wtap_g, k0tap_g, perm_g, phase_g;
   mirt::DMem swept;        // row-sweep spread: the samples in plan order, [Mtot][C]
   mirt::DMem sweep_teams;  // row-sweep spread: balanced team list (int4 per team)
+  std::vector<int4> team_host;  // the same list on the host
+  mirt::DMem team_order, team_next;  // row-sweep work queue: heaviest-first order, counter
   // TMA gather: first position of each block of the gather order, work items
   // (block, first position), the first item of each slice, fault flag
   mirt::DMem gblk, gitem, gfault;

@@ -302,6 +302,13 @@ class NufftPlan:
     def config(self):
         return _plan_config(self.lib, self.lib.mirt_nufft_interp_plan(self.handle))
 
+    def fft_config(self):
+        """{'fused_fft': 1 if the FFT runs as the library's fused passes,
+        'launches_forward', 'launches_adjoint': library kernels per call}."""
+        v = (C.c_int32 * 3)()
+        check(self.lib.mirt_nufft_config(self.handle, v, 3))
+        return {"fused_fft": v[0], "launches_forward": v[1], "launches_adjoint": v[2]}
+
     def forward_host(self, x: np.ndarray, out: np.ndarray | None = None, stream=None):
         """host complex64 image (device layout) -> host complex64 samples."""
         x = np.ascontiguousarray(x, dtype=np.complex64)
