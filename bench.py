@@ -171,7 +171,7 @@ def traffic_from_profiles(call, workload, variant):
 # CPU path of the reference (oracle/_ref kernels + scipy FFT + numpy glue)
 # ---------------------------------------------------------------------------
 class CpuReference:
-    def __init__(self, w, om, moff, n_shift):
+    def __init__(self, w, om, moff, n_shift, threads=None):
         import oracle
         from oracle import nufft_ref as nr
         self.oracle = oracle
@@ -186,7 +186,10 @@ class CpuReference:
         self.h = [nr.table_1d(w["N"], w["J"], w["K"], w["L"])] * D
         self.sn = nr.scaling_factors(self.Nd, self.Jd, self.Kd)
         self.om, self.moff, self.n_shift = om, moff, np.asarray(n_shift, float)
-        self.threads = oracle.ref_max_threads() if self.impl == "ref" else 1
+        allc = oracle.ref_max_threads() if self.impl == "ref" else 1
+        # the reference's own behaviour is one core (no threads in nufft/table/);
+        # threads > 1 runs one coil column per thread
+        self.threads = allc if threads is None else max(1, min(int(threads), allc))
 
     def step(self, s, x):
         """forward + adjoint of slice s; x [N.., C] (MATLAB order).  Returns #sample-coils."""
@@ -469,6 +472,12 @@ def run_gpu(args, w):
         cpu = {"value": v, "unit": UNIT, "cores": ref.threads, "kind": ref.kind,
                "sample": f"{ns} of {plan.nslice} slices, forward + adjoint, {C} coils "
                          f"({u:.3g} sample-coils in {tc:.1f} s)"}
+        # one core: the reference's own behaviour (its table code has no threads)
+        ref1 = CpuReference(w, om, moff, n_shift, threads=1)
+        v1, ns1, u1, tc1 = ref1.timed_sample(img_np, target_s=args.cpu_seconds / 2, max_slices=1)
+        cpu["one_core"] = {"value": v1, "unit": UNIT, "cores": 1,
+                           "sample": f"{ns1} slice, forward + adjoint, {C} coils "
+                                     f"({u1:.3g} sample-coils in {tc1:.1f} s)"}
 
     # the library's own launches per forward + adjoint (FFT passes or, with cuFFT,
     # the deapodise / transpose / crop kernels; gather; spread), cuFFT not counted
@@ -532,7 +541,9 @@ def run_cgsense(args):
       plain             qpwls_pcg1 from zero (precon = 1), NUFFT pair per iteration
       precon_only       the same with the circulant preconditioner
       learned           learned DCF (features + MLP + PSF scale) warm start + preconditioner
-      learned_toeplitz  the same on the Toeplitz normal equations (qpwls_pcg2)
+      precon_toeplitz   circulant preconditioner on the Toeplitz normal equations
+                        (qpwls_pcg2), from zero: the Gram form without the learned part
+      learned_toeplitz  the learned warm start on the Toeplitz normal equations
       pipe              Pipe-Menon DCF (30 updates) warm start + preconditioner"""
     import torch
 
@@ -542,7 +553,7 @@ def run_cgsense(args):
     from mirt_b200 import workloads as wl
 
     tol = 1e-3
-    modes = ("plain", "precon_only", "learned", "learned_toeplitz", "pipe")
+    modes = ("plain", "precon_only", "learned", "precon_toeplitz", "learned_toeplitz", "pipe")
     rng = np.random.default_rng(5)
     probs = wl.cgsense_problems(args.cg_problems, rng)
     groups = {}
@@ -584,34 +595,32 @@ def run_cgsense(args):
             a, b = int(moff[s]), int(moff[s + 1])
             noise[a:b] *= y[a:b].norm() / noise[a:b].norm() * 10 ** (-30 / 20)
         y = (y + noise).contiguous()
-        sid = torch.repeat_interleave(torch.arange(len(idx), device="cuda"),
-                                      torch.from_numpy(np.diff(moff)).cuda())
         om_d = torch.from_numpy(om).cuda()
         xref = torch.zeros(A.image_shape, dtype=torch.complex64, device="cuda")
         A.pcg(xref, y, args.cg_ref, precon=True)
-        # untimed first calls of this group's sizes (device buffers come from
-        # the library's caching allocator afterwards), like the plan set-up
-        model.predict(om_d, G1, moff)
-        mb.dcf_pipe(G1, niter=0, thresh=0.0)
-        A.warm_start(y)
+        # untimed first calls of this group's sizes and of every torch op used
+        # below (device buffers come from the library's caching allocator
+        # afterwards), like the plan set-up
+        A.warm_start(y, W=model.predict(om_d, slice_moff=moff).to(torch.float32))
+        A.warm_start(y, W=mb.dcf_pipe(G1, niter=0, thresh=0.0).to(torch.float32))
+        torch.zeros_like(xref)
         torch.cuda.synchronize()
         res = {"N": N, "coils": C, "problems": len(idx)}
         for mode in modes:
             e0 = ev()
-            if mode in ("plain", "precon_only"):
+            if mode in ("plain", "precon_only", "precon_toeplitz"):
                 x = torch.zeros_like(xref)
             else:
+                # the warm start's per-problem least-squares scale absorbs any
+                # scale of the weights: no PSF scaling or normalisation here
                 if mode == "pipe":
                     w = mb.dcf_pipe(G1, niter=29, thresh=0.0)
                 else:
-                    w = model.predict(om_d, G1, moff)
-                cnt = torch.from_numpy(np.diff(moff)).cuda()
-                sums = torch.zeros(len(idx), dtype=torch.float64, device="cuda").index_add_(0, sid, w)
-                wn = (w / (sums / cnt)[sid]).to(torch.float32)
-                x = A.warm_start(y, W=wn)
+                    w = model.predict(om_d, slice_moff=moff)
+                x = A.warm_start(y, W=w.to(torch.float32))
             e1 = ev()
             nr, tms = A.pcg(x, y, args.cg_iters, precon=(mode != "plain"),
-                            gram=(mode == "learned_toeplitz"), xref=xref, timing=True)
+                            gram=mode.endswith("_toeplitz"), xref=xref, timing=True)
             torch.cuda.synchronize()
             pre = e0.elapsed_time(e1)
             t, it = _first_below(nr, tms, tol)

@@ -229,9 +229,15 @@ int mirt_interp_plan_set_ownership(mirt_interp_plan *plan, int32_t own, void *st
  * segments per row (more segments, more parallel teams, five warm-up columns
  * each); -1 a balanced team list built from the sort's bins (rows cut into
  * segments of about equal visit counts, about 64k teams: the default for
- * 32-coil plans); 0 returns to the tiled spread.  MIRT_ERR_ARG
- * where it does not apply.  The autotuner tries it where it applies.  No
- * reference counterpart. */
+ * 32-coil plans); 0 returns to the tiled spread.  Teams are taken by the
+ * kernel's warps from a work queue, heaviest first.  3D plans (J = 6, K >= 6
+ * per dimension, coil chunks of 8, 16 or 32): the line sweep, in which a
+ * warp owns a block of 2 x 2, 2 x 1 or one grid lines along k1 (lanes = coils
+ * x lines) and `segments` (1..K1) uniform segments of their columns, and
+ * sweeps the bin columns of the bin lines around the block with six columns
+ * of accumulators per line in registers (rows unused; the default there,
+ * two segments).  MIRT_ERR_ARG where it does not apply.  The autotuner tries
+ * it where it applies.  No reference counterpart. */
 int mirt_interp_plan_set_sweep(mirt_interp_plan *plan, int32_t segments, int32_t rows);
 
 /* Gather over TMA-staged tiles and records (2D, J = 6, an even C >= 32,
@@ -255,6 +261,14 @@ int mirt_interp_plan_set_gather(mirt_interp_plan *plan, int32_t tma);
  * the same GPU, can be trusted.  Destroy the plan and build a new one.
  * No reference counterpart. */
 int mirt_interp_plan_fault(mirt_interp_plan *plan, int32_t *fault);
+
+/* Test hook of the bounded waits behind mirt_interp_plan_fault: with on = 1,
+ * the TMA gather arms each stage's barrier for bytes that no copy delivers and
+ * issues no copy at all, with a short wait limit, so every wait runs out with
+ * nothing in flight; the launch computes no sample and sets the fault flag.
+ * on = 0 restores the normal gather.  MIRT_ERR_ARG if the plan's gather is not
+ * the TMA one.  No reference counterpart. */
+int mirt_interp_plan_set_fault_test(mirt_interp_plan *plan, int32_t on);
 
 /* Fix the spread's tiling instead of autotuning it: tile extents T[0..D-1]
  * (multiples of the sort bins B of mirt_interp_plan_config, at most the grid

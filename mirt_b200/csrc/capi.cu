@@ -171,6 +171,15 @@ int sweep_ok(const InterpArgs &a, const Tiling &t) {
   return 1;
 }
 
+// The 3D line sweep needs: 3D, J = 6, one-point bins, K >= 6 per dimension,
+// and coil chunks of 8, 16 or 32 lanes (blocks of 2 x 2, 2 x 1 or 1 lines).
+int sweep3_ok(const InterpArgs &a, const Tiling &t, int cw) {
+  if (a.g.D != 3 || (cw != 8 && cw != 16 && cw != 32)) return 0;
+  for (int d = 0; d < 3; d++)
+    if (a.g.J[d] != 6 || t.B[d] != 1 || a.g.K[d] < 6) return 0;
+  return 1;
+}
+
 // The row sweep's copy of the samples in plan order (allocated when the sweep
 // is first selected, outside any launch).
 int sweep_buffer(mirt_interp_plan *P) {
@@ -314,6 +323,61 @@ int build_sweep_teams(mirt_interp_plan *P, int rows, long long target, cudaStrea
   return build_sweep_order(P, vb, st);
 }
 
+// 3D line sweep with nseg uniform segments per line block: the work queue of
+// its teams, heaviest first (cost: the samples of the block's bin lines in
+// the segment and its warm-up columns + 2 per column step).
+int set_line_sweep3(mirt_interp_plan *P, int nseg, cudaStream_t st) {
+  const InterpArgs &a = P->a;
+  Tiling &t = P->t;
+  const int K1 = a.g.K[0], K2 = a.g.K[1], K3 = a.g.K[2], S = t.nslice;
+  const int nl = 32 / P->ls.cw, B2 = nl >= 2 ? 2 : 1, B3 = nl / B2;
+  const int nby = (K2 + B2 - 1) / B2, nbz = (K3 + B3 - 1) / B3;
+  const long long nb = (long long)t.nbins * S;
+  std::vector<int> bs(nb + 1);
+  CK(cudaMemcpyAsync(bs.data(), P->bin_start.p, (nb + 1) * sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  const int sw = (K1 + nseg - 1) / nseg;
+  const long long nteam = (long long)S * nbz * nby * nseg;
+  std::vector<double> cost(nteam, 0.0);
+  for (long long team = 0; team < nteam; team++) {
+    const int seg = (int)(team % nseg);
+    long long rest = team / nseg;
+    const int by = (int)(rest % nby);
+    rest /= nby;
+    const int bz = (int)(rest % nbz);
+    const int s = (int)(rest / nbz);
+    const int x0 = seg * sw, x1 = std::min(K1, x0 + sw);
+    if (x0 >= x1) continue;
+    double c = kSweepColumnCost * (x1 - x0 + 5);
+    for (int q3 = 0; q3 < B3 + 5; q3++)
+      for (int q2 = 0; q2 < B2 + 5; q2++) {
+        const int r = ((by * B2 - 5 + q2) % K2 + K2) % K2;
+        const int z = ((bz * B3 - 5 + q3) % K3 + K3) % K3;
+        const int *br = bs.data() + (size_t)s * t.nbins + ((size_t)z * K2 + r) * K1;
+        const int xs = x0 - 5;
+        if (xs < 0) c += br[K1] - br[xs + K1];
+        c += br[x1] - br[std::max(xs, 0)];
+      }
+    cost[team] = c;
+  }
+  std::vector<int> order(nteam);
+  for (long long i = 0; i < nteam; i++) order[i] = (int)i;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cost[x] > cost[y]; });
+  if (P->team_order.bytes < std::max<size_t>(order.size(), 1) * sizeof(int))
+    CK(P->team_order.alloc(std::max<size_t>(order.size(), 1) * sizeof(int)));
+  if (!order.empty())
+    CK(cudaMemcpyAsync(P->team_order.p, order.data(), order.size() * sizeof(int),
+                       cudaMemcpyHostToDevice, st));
+  const size_t nq = (size_t)std::max(1, (a.C + P->ls.cw - 1) / std::max(P->ls.cw, 1));
+  if (P->team_next.bytes < nq * sizeof(int)) CK(P->team_next.alloc(nq * sizeof(int)));
+  CK(cudaStreamSynchronize(st));
+  t.team_order = P->team_order.as<int>();
+  t.team_next = P->team_next.as<int>();
+  t.sweep = nseg;
+  t.sweep_rows = 1;
+  return MIRT_OK;
+}
+
 // Uniform segments: the work queue of their teams.
 int set_uniform_sweep(mirt_interp_plan *P, int nseg, int rows, cudaStream_t st) {
   P->t.sweep = nseg;
@@ -332,7 +396,8 @@ cudaError_t plan_gather(mirt_interp_plan *P, const float2 *ck, float2 *fm, cudaS
   if (s1 < 0) s1 = S;
   if (P->gtma) {
     const long long i0 = P->gitem_slice[s0], i1 = P->gitem_slice[s1];
-    return launch_gather_tma(P->ag, P->gbk, S, i0, i1 - i0, ck, fm, P->gfault.as<int>(), st);
+    return launch_gather_tma(P->ag, P->gbk, S, i0, i1 - i0, ck, fm, P->gfault.as<int>(), st,
+                             P->gfault_test);
   }
   InterpArgs ag = P->ag;
   if (s0 > 0 || s1 < S) {
@@ -402,6 +467,7 @@ void choose_config(mirt_interp_plan *P) {
   t.nteams = 0;
   t.team_order = nullptr;
   t.team_next = nullptr;
+  t.sweep_u = 4;
   t.nbins = 1;
   t.ntiles = 1;
   for (int d = 0; d < MIRT_DMAX; d++) {
@@ -813,6 +879,13 @@ int plan_finish(mirt_interp_plan *P, long long Mtot, const long long *moff, int 
     rc3 = build_sweep_teams(P, 1, 65536, st);
     if (rc3) return rc3;
   }
+  // 3D, J = 6, coil chunks of 8, 16 or 32: the line sweep, two segments per line
+  if (sweep3_ok(a, P->t, P->ls.cw)) {
+    int rc3 = sweep_buffer(P);
+    if (rc3) return rc3;
+    rc3 = set_line_sweep3(P, 2, st);
+    if (rc3) return rc3;
+  }
   return MIRT_OK;
 }
 
@@ -837,6 +910,7 @@ int set_spread_tiles(mirt_interp_plan *P, const int *T, cudaStream_t st) {
 struct SpreadCand {
   int T[MIRT_DMAX];
   int threads, padc, atomic, own, sweep, sweep_rows;
+  int sweep_u = 4;  // samples whose loads the sweep issues together
 };
 
 // spare columns the J = 6 row update can use (0 elsewhere)
@@ -1050,11 +1124,18 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
   // row sweep (no tiles): bands of 1, 2 or 4 rows, whole rows or uniform
   // segments of at least 32 columns, or balanced teams (sweep = -1)
   if (sweep_ok(a, P->t) && sweep_buffer(P) == MIRT_OK)
-    for (int rows : {1, 2, 4})
-      for (int nseg = (rows < 4 ? -1 : 1); nseg <= 16 && (nseg <= 1 || a.g.K[0] / nseg >= 32);
-           nseg = nseg < 0 ? 1 : nseg * 2)
+    for (int u : {1, 4})
+      for (int rows : {1, 2, 4})
+        for (int nseg = (rows < 4 ? -1 : 1); nseg <= 16 && (nseg <= 1 || a.g.K[0] / nseg >= 32);
+             nseg = nseg < 0 ? 1 : nseg * 2)
+          cands.push_back(SpreadCand{{P->t.T[0], P->t.T[1], P->t.T[2]}, P->ls.threads, 0, 0, 0,
+                                     nseg, rows, u});
+  // 3D line sweep: 1, 2, 4 or 8 segments per line block
+  if (sweep3_ok(a, P->t, cw) && sweep_buffer(P) == MIRT_OK)
+    for (int u : {1, 4})
+      for (int nseg : {1, 2, 4, 8})
         cands.push_back(SpreadCand{{P->t.T[0], P->t.T[1], P->t.T[2]}, P->ls.threads, 0, 0, 0,
-                                   nseg, rows});
+                                   nseg, 1, u});
   SpreadCand best{};
   float best_ms = 1e30f;
   int built_rows = 0;  // rows of the team list last built
@@ -1062,12 +1143,14 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
     P->t.own = c.own;
     P->t.sweep = c.sweep;
     P->t.sweep_rows = c.sweep_rows;
+    P->t.sweep_u = c.sweep_u;
     if (c.sweep < 0 && built_rows != c.sweep_rows) {
       int rc = build_sweep_teams(P, c.sweep_rows, 65536, st);
       if (rc) return rc;
       built_rows = c.sweep_rows;
     } else if (c.sweep > 0) {
-      int rc = set_uniform_sweep(P, c.sweep, c.sweep_rows, st);
+      int rc = D == 3 ? set_line_sweep3(P, c.sweep, st)
+                      : set_uniform_sweep(P, c.sweep, c.sweep_rows, st);
       if (rc) return rc;
       built_rows = 0;  // the work queue now orders uniform segments
     }
@@ -1085,9 +1168,9 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
     if (autotune_log())
       std::fprintf(stderr,
                    "mirt autotune spread: tile %dx%dx%d threads %d padc %d atomic %d own %d "
-                   "sweep %d rows %d: %.3f ms\n",
+                   "sweep %d rows %d u %d: %.3f ms\n",
                    c.T[0], c.T[1], c.T[2], c.threads, c.padc, c.atomic, c.own, c.sweep,
-                   c.sweep_rows, ms);
+                   c.sweep_rows, c.sweep_u, ms);
     if (ms < best_ms) {
       best_ms = ms;
       best = c;
@@ -1097,11 +1180,13 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
     P->t.own = best.own;
     P->t.sweep = best.sweep;
     P->t.sweep_rows = best.sweep_rows;
+    P->t.sweep_u = best.sweep_u;
     if (best.sweep < 0 && built_rows != best.sweep_rows) {
       int rc = build_sweep_teams(P, best.sweep_rows, 65536, st);
       if (rc) return rc;
     } else if (best.sweep > 0) {
-      int rc = set_uniform_sweep(P, best.sweep, best.sweep_rows, st);
+      int rc = D == 3 ? set_line_sweep3(P, best.sweep, st)
+                      : set_uniform_sweep(P, best.sweep, best.sweep_rows, st);
       if (rc) return rc;
     }
     int rc = set_spread_tiles(P, best.T, st);
@@ -1204,6 +1289,13 @@ int mirt_interp_plan_set_gather(mirt_interp_plan *P, int32_t tma) {
   return MIRT_OK;
 }
 
+int mirt_interp_plan_set_fault_test(mirt_interp_plan *P, int32_t on) {
+  if (!P) return fail(MIRT_ERR_ARG, "plan is NULL");
+  if (on && !P->gtma) return fail(MIRT_ERR_ARG, "the plan's gather does not use TMA stages");
+  P->gfault_test = on ? 1 : 0;
+  return MIRT_OK;
+}
+
 int mirt_interp_plan_fault(mirt_interp_plan *P, int32_t *fault) {
   if (!P || !fault) return fail(MIRT_ERR_ARG, "NULL argument");
   *fault = 0;
@@ -1219,6 +1311,20 @@ int mirt_interp_plan_fault(mirt_interp_plan *P, int32_t *fault) {
 
 int mirt_interp_plan_set_sweep(mirt_interp_plan *P, int32_t segments, int32_t rows) {
   if (!P) return fail(MIRT_ERR_ARG, "plan is NULL");
+  if (P->a.g.D == 3) {
+    if (segments && !sweep3_ok(P->a, P->t, P->ls.cw))
+      return fail(MIRT_ERR_ARG, "3D line sweep needs J = 6, K >= 6 per dimension and coil "
+                                "chunks of 8, 16 or 32");
+    if (segments < 0 || segments > P->a.g.K[0])
+      return fail(MIRT_ERR_ARG, "3D line-sweep segments must be in 1..K1 (0: off)");
+    if (segments) {
+      int rc = sweep_buffer(P);
+      if (rc) return rc;
+      return set_line_sweep3(P, segments, as_stream(nullptr));
+    }
+    P->t.sweep = 0;
+    return MIRT_OK;
+  }
   if (segments && !sweep_ok(P->a, P->t))
     return fail(MIRT_ERR_ARG, "row-sweep spread needs 2D, J = 6 and K >= 6 per dimension");
   if (segments < -1 || (segments > 0 && segments > P->a.g.K[0]))

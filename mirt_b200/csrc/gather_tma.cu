@@ -38,6 +38,7 @@ constexpr unsigned TG_K_BYTES = TG_RC * 16;                     // 1,536
 constexpr unsigned TG_STAGE = TG_TILE_BYTES + TG_W_BYTES + TG_K_BYTES;  // 54,016 = 422 x 128
 constexpr int TG_THREADS = 256;
 constexpr long long TG_WAIT_LIMIT = 1ll << 22;
+constexpr long long TG_TEST_WAIT_LIMIT = 1ll << 12;
 
 __device__ __forceinline__ unsigned smem_addr(const void *p) {
   return (unsigned)__cvta_generic_to_shared(p);
@@ -73,9 +74,9 @@ __device__ __forceinline__ void bulk_copy(void *dst, const void *src, unsigned b
       : "memory");
 }
 
-// wait for phase `parity` of the barrier, at most TG_WAIT_LIMIT polls
-__device__ __forceinline__ bool stage_wait(uint64_t *bar, unsigned parity) {
-  for (long long it = 0; it < TG_WAIT_LIMIT; it++) {
+// wait for phase `parity` of the barrier, at most `limit` polls
+__device__ __forceinline__ bool stage_wait(uint64_t *bar, unsigned parity, long long limit) {
+  for (long long it = 0; it < limit; it++) {
     unsigned ok;
     asm volatile(
         "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
@@ -107,12 +108,18 @@ __device__ __forceinline__ Item item_of(const GatherBlocks &g, const InterpArgs 
   return r;
 }
 
-// one thread: arm the stage's barrier and start its copies
+// one thread: arm the stage's barrier and start its copies.  no_copy (the
+// test of the bounded waits): arm the barrier for bytes that no copy will
+// deliver and issue no copy, so that its wait runs out with nothing in flight.
 __device__ __forceinline__ void stage_issue(const CUtensorMap *tm, const InterpArgs &a,
                                             unsigned char *st, uint64_t *bar, const Item &r,
-                                            int chunk) {
+                                            int chunk, bool no_copy) {
   const unsigned wb = (unsigned)r.n * 96u, kb = (unsigned)r.n * 16u;
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  if (no_copy) {
+    mbar_expect(bar, 16u);
+    return;
+  }
   mbar_expect(bar, (r.interior ? TG_TILE_BYTES : 0u) + wb + kb);
   if (r.interior)
     tile_copy(tm, st, bar, chunk * 2 * TG_CW, r.bx * TG_GB, r.by * TG_GB, r.slice);
@@ -124,7 +131,8 @@ template <bool REAL>
 __global__ void __launch_bounds__(TG_THREADS, 2)
     gather_tma_kernel(const __grid_constant__ CUtensorMap tmap, InterpArgs a, GatherBlocks g,
                       long long it0, long long nit, const float2 *__restrict__ ck,
-                      float2 *__restrict__ fm, int *__restrict__ fault) {
+                      float2 *__restrict__ fm, int *__restrict__ fault, int no_copy,
+                      long long wait_limit) {
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t *bar = reinterpret_cast<uint64_t *>(smem + 2 * TG_STAGE);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -143,14 +151,16 @@ __global__ void __launch_bounds__(TG_THREADS, 2)
   unsigned par0 = 0u, par1 = 0u;  // wait parity of each stage's barrier
   const long long end = it0 + nit;
   long long i = it0 + blockIdx.x;
-  if (threadIdx.x == 0 && i < end) stage_issue(&tmap, a, smem, &bar[0], item_of(g, a, i), chunk);
+  if (threadIdx.x == 0 && i < end)
+    stage_issue(&tmap, a, smem, &bar[0], item_of(g, a, i), chunk, no_copy);
   for (int k = 0; i < end; i += gridDim.x, k++) {
     const int s = k & 1;
     const long long inx = i + gridDim.x;
     if (threadIdx.x == 0 && inx < end)
-      stage_issue(&tmap, a, smem + (s ^ 1) * TG_STAGE, &bar[s ^ 1], item_of(g, a, inx), chunk);
+      stage_issue(&tmap, a, smem + (s ^ 1) * TG_STAGE, &bar[s ^ 1], item_of(g, a, inx), chunk,
+                  no_copy);
     const Item r = item_of(g, a, i);
-    const bool ready = stage_wait(&bar[s], s ? par1 : par0);
+    const bool ready = stage_wait(&bar[s], s ? par1 : par0, wait_limit);
     if (s) par1 ^= 1u;
     else par0 ^= 1u;
     if (__syncthreads_or(!ready)) {
@@ -158,7 +168,7 @@ __global__ void __launch_bounds__(TG_THREADS, 2)
       // (bounded), and stop this CTA
       if (threadIdx.x == 0) {
         atomicExch(fault, 1);
-        if (inx < end) stage_wait(&bar[s ^ 1], s ? par0 : par1);
+        if (inx < end) stage_wait(&bar[s ^ 1], s ? par0 : par1, wait_limit);
       }
       return;
     }
@@ -239,7 +249,7 @@ int gather_tma_item() { return TG_RC; }
 
 cudaError_t launch_gather_tma(const InterpArgs &a, const GatherBlocks &g, int nslice,
                               long long it0, long long nit, const float2 *ck, float2 *fm,
-                              int *fault, cudaStream_t st) {
+                              int *fault, cudaStream_t st, int fault_test) {
   if (a.Mtot == 0 || a.C == 0 || nit <= 0) return cudaSuccess;
   if (!gather_tma_ok(a) || g.gb != TG_GB || a.SJ != 12) return cudaErrorInvalidValue;
   PFN_cuTensorMapEncodeTiled_v12000 enc = encode_fn();
@@ -266,7 +276,10 @@ cudaError_t launch_gather_tma(const InterpArgs &a, const GatherBlocks &g, int ns
   long long ctas = (long long)nsm * 2;
   if (ctas > nit) ctas = nit;
   const unsigned nchunk = (unsigned)((a.C + TG_CW - 1) / TG_CW);
-  kern<<<dim3((unsigned)ctas, nchunk), TG_THREADS, smem, st>>>(tm, a, g, it0, nit, ck, fm, fault);
+  // the test of the bounded waits: no copies, and a short wait limit
+  const long long limit = fault_test ? TG_TEST_WAIT_LIMIT : TG_WAIT_LIMIT;
+  kern<<<dim3((unsigned)ctas, nchunk), TG_THREADS, smem, st>>>(tm, a, g, it0, nit, ck, fm, fault,
+                                                              fault_test ? 1 : 0, limit);
   return cudaGetLastError();
 }
 

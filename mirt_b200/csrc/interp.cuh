@@ -77,6 +77,7 @@ struct Tiling {
   // chunk], which are cleared before every launch.
   const int *team_order;
   int *team_next;
+  int sweep_u;           // samples of a bin whose loads are issued together (1 or 4)
   int color_beg[9];
   int red_beg[9];
   int padc;              // spread: spare columns on each side of a tile row in
@@ -139,10 +140,11 @@ bool gather_tma_ok(const InterpArgs &a);
 int gather_tma_block();
 int gather_tma_item();
 // items [it0, it0 + nit) of a batch of nslice slices; *fault is set when a
-// stage does not arrive within the kernel's wait limit
+// stage does not arrive within the kernel's wait limit.  fault_test: the test
+// of that path (no copies are issued, every wait runs out, nothing computed).
 cudaError_t launch_gather_tma(const InterpArgs &a, const GatherBlocks &g, int nslice,
                               long long it0, long long nit, const float2 *ck, float2 *fm,
-                              int *fault, cudaStream_t st);
+                              int *fault, cudaStream_t st, int fault_test = 0);
 
 // Compute the sort key of every sample: slice * nbins + bin of its first tap.
 cudaError_t launch_bin_keys(const InterpArgs &a, const Tiling &t, uint32_t *keys,

@@ -116,6 +116,18 @@ __device__ __forceinline__ float2 cw_fma(float2 w, float2 v, float2 vs, float2 A
   return A;
 }
 
+// acc += conj(w) * v as four scalar FMAs in the order (re: wr vr, wi vi;
+// im: wr vi, -wi vr) -- the roundings of cw_fma.
+template <bool REAL>
+__device__ __forceinline__ void cmac_conj(float2 &acc, float2 w, float2 v) {
+  acc.x = __fmaf_rn(w.x, v.x, acc.x);
+  acc.y = __fmaf_rn(w.x, v.y, acc.y);
+  if (!REAL) {
+    acc.x = __fmaf_rn(w.y, v.y, acc.x);
+    acc.y = __fmaf_rn(-w.y, v.x, acc.y);
+  }
+}
+
 // *p += (wr, wr) v2 + (wi, -wi) v2s: a read-modify-write by the point's one
 // owner, or (ATOMIC) two shared-memory atomic adds when warps share the tile
 template <bool ATOMIC, bool REAL>
@@ -686,7 +698,7 @@ __global__ void __launch_bounds__(256) sweep_order_kernel(InterpArgs a, const fl
 }
 
 // The sweep of one team (see spread_sweep_kernel).
-template <int CW, int R, bool REAL>
+template <int CW, int R, int U, bool REAL>
 __device__ __forceinline__ void sweep_team(const InterpArgs &a, const Tiling &t,
                                            const int *__restrict__ bin_start,
                                            const float2 *__restrict__ fs,
@@ -745,24 +757,43 @@ __device__ __forceinline__ void sweep_team(const InterpArgs &a, const Tiling &t,
     for (int q = 0; q < NQ; q++) end[q] = __ldg(bs + row[q] + xw + 1);
 #pragma unroll
     for (int q = 0; q < NQ; q++) {
-      for (int p = beg[q]; p < end[q]; p++) {
-        const float2 f = on ? __ldg(fs + (long long)p * C + c) : make_float2(0.f, 0.f);
-        const float2 *Ws = a.W + (long long)p * 12;
-        const float4 *W4 = reinterpret_cast<const float4 *>(Ws);
-        float4 w1[3];
+      // U samples at a time, all their loads issued first; positions past the
+      // bin's end repeat its last sample and are not added
+      const int pe = end[q];
+      for (int p = beg[q]; p < pe; p += U) {
+        float2 f[U], w2[U][R];
+        float4 w1[U][3];
 #pragma unroll
-        for (int h = 0; h < 3; h++) w1[h] = __ldg(W4 + h);
+        for (int u = 0; u < U; u++) {
+          const int pu = U == 1 ? p : min(p + u, pe - 1);
+          f[u] = on ? __ldg(fs + (long long)pu * C + c) : make_float2(0.f, 0.f);
+          const float2 *Ws = a.W + (long long)pu * 12;
+          const float4 *W4 = reinterpret_cast<const float4 *>(Ws);
 #pragma unroll
-        for (int r = 0; r < R; r++) {
-          const int j2 = r - q + 5;  // compile-time after unrolling
-          if (j2 >= 0 && j2 < 6) {
-            const float2 v = cw_mul<REAL>(__ldg(Ws + 6 + j2), f);
-            const float2 vs = make_float2(v.y, v.x);
+          for (int h = 0; h < 3; h++) w1[u][h] = __ldg(W4 + h);
 #pragma unroll
-            for (int h = 0; h < 3; h++) {
-              acc[r][2 * h] = cw_fma<REAL>(make_float2(w1[h].x, w1[h].y), v, vs, acc[r][2 * h]);
-              acc[r][2 * h + 1] =
-                  cw_fma<REAL>(make_float2(w1[h].z, w1[h].w), v, vs, acc[r][2 * h + 1]);
+          for (int r = 0; r < R; r++) {
+            const int j2 = r - q + 5;  // compile-time after unrolling
+            if (j2 >= 0 && j2 < 6) w2[u][r] = __ldg(Ws + 6 + j2);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+          if (U == 1 || p + u < pe) {
+#pragma unroll
+            for (int r = 0; r < R; r++) {
+              const int j2 = r - q + 5;
+              if (j2 >= 0 && j2 < 6) {
+                const float2 v = cw_mul<REAL>(w2[u][r], f[u]);
+                const float2 vs = make_float2(v.y, v.x);
+#pragma unroll
+                for (int h = 0; h < 3; h++) {
+                  acc[r][2 * h] =
+                      cw_fma<REAL>(make_float2(w1[u][h].x, w1[u][h].y), v, vs, acc[r][2 * h]);
+                  acc[r][2 * h + 1] = cw_fma<REAL>(make_float2(w1[u][h].z, w1[u][h].w), v, vs,
+                                                   acc[r][2 * h + 1]);
+                }
+              }
             }
           }
         }
@@ -787,7 +818,7 @@ __device__ __forceinline__ void sweep_team(const InterpArgs &a, const Tiling &t,
 // plan's work queue (heaviest teams first) until the queue is empty, so warps
 // do not sit idle behind a heavy team of their block.  Each team's sums are
 // independent of which warp runs it: deterministic.
-template <int CW, int R, bool REAL>
+template <int CW, int R, int U, bool REAL>
 __global__ void __launch_bounds__(256) spread_sweep_kernel(InterpArgs a, Tiling t,
                                                            const int *__restrict__ bin_start,
                                                            const float2 *__restrict__ fs,
@@ -805,8 +836,167 @@ __global__ void __launch_bounds__(256) spread_sweep_kernel(InterpArgs a, Tiling 
     const long long qi = (long long)base + lane / CW;
     if (qi < nteam) {
       const long long team = t.team_order ? (long long)__ldg(t.team_order + qi) : qi;
-      sweep_team<CW, R, REAL>(a, t, bin_start, fs, ck, team);
+      sweep_team<CW, R, U, REAL>(a, t, bin_start, fs, ck, team);
     }
+  }
+}
+
+// ------------------------------------------------------------------------
+// 3D line sweep (J = 6 in every dimension, one-point bins, K >= 6)
+// ------------------------------------------------------------------------
+// A warp owns a block of B2 x B3 grid lines along k1 (rows y0 .. y0 + B2 - 1
+// of planes z0 .. z0 + B3 - 1; lanes = CW coils x the block's 32 / CW lines:
+// 2 x 2 lines for 8 coils, 2 x 1 for 16, one line for 32) and a segment
+// [x0, x1) of their columns.  The samples with taps in the block are those
+// binned in the Q2 x Q3 = (B2 + 5) x (B3 + 5) bin lines around it; lane l
+// keeps the bin pointers of bin lines l and l + 32.  The warp sweeps bin
+// columns x0 - 5 .. x1 - 1 (wrapped): per column it loads each bin line's end
+// pointer, takes the non-empty lines in a fixed order (ballot), and for each
+// sample every lane adds the sample's six k1 taps into the six-column window
+// of its own line (when the line is within the sample's 6 x 6 tap rows), with
+// the same FP32 operation order per tap as the tiled spread (conj(w3) f, then
+// conj(w2), then conj(w1)).  After bin column x, grid column x of every line
+// is complete and is stored once.  Summation order per grid point: columns,
+// bin lines, samples in sort order -- fixed: bitwise reproducible.
+template <int CW, int U, bool REAL>
+__device__ __forceinline__ void sweep3_team(const InterpArgs &a, const Tiling &t,
+                                            const int *__restrict__ bin_start,
+                                            const float2 *__restrict__ fs,
+                                            float2 *__restrict__ ck, long long team) {
+  constexpr unsigned FULLM = 0xffffffffu;
+  constexpr int NL = 32 / CW;             // lines per warp
+  constexpr int B2 = NL >= 2 ? 2 : 1;
+  constexpr int B3 = NL / B2;
+  constexpr int Q2 = B2 + 5, Q3 = B3 + 5, NBL = Q2 * Q3;  // bin lines, at most 49
+  static_assert(NBL <= 64, "bin lines must fit two per lane");
+  const int K1 = a.g.K[0], K2 = a.g.K[1], K3 = a.g.K[2];
+  const int nseg = t.sweep;
+  const int nby = (K2 + B2 - 1) / B2, nbz = (K3 + B3 - 1) / B3;
+  const int seg = (int)(team % nseg);
+  long long rest = team / nseg;
+  const int by = (int)(rest % nby);
+  rest /= nby;
+  const int bz = (int)(rest % nbz);
+  const int slice = t.slice0 + (int)(rest / nbz);
+  const int y0 = by * B2, z0 = bz * B3;
+  const int sw = (K1 + nseg - 1) / nseg;
+  const int x0 = seg * sw, x1 = min(K1, x0 + sw);
+  if (x0 >= x1) return;
+  const int lane = threadIdx.x & 31;
+  const int li = lane / CW;
+  const int dy = li % B2, dz = li / B2;
+  const int C = a.C;
+  const int c = blockIdx.y * CW + lane % CW;
+  const bool on = c < C;
+  const int *bs = bin_start + (long long)slice * t.nbins;
+  auto line_base = [&](int l) -> long long {
+    int r = (y0 - 5 + l % Q2) % K2;
+    if (r < 0) r += K2;
+    int z = (z0 - 5 + l / Q2) % K3;
+    if (z < 0) z += K3;
+    return ((long long)z * K2 + r) * K1;
+  };
+  const long long base0 = lane < NBL ? line_base(lane) : -1;
+  const long long base1 = lane + 32 < NBL ? line_base(lane + 32) : -1;
+  const int xs = x0 - 5;
+  const int xs_w = xs < 0 ? xs + K1 : xs;
+  int beg0 = base0 >= 0 ? __ldg(bs + base0 + xs_w) : 0;
+  int beg1 = base1 >= 0 ? __ldg(bs + base1 + xs_w) : 0;
+  float2 acc[6];
+#pragma unroll
+  for (int j = 0; j < 6; j++) acc[j] = make_float2(0.f, 0.f);
+  const bool out_ok = on && y0 + dy < K2 && z0 + dz < K3;
+  float2 *out = ck + (long long)slice * a.grid_elems +
+                ((long long)(z0 + dz) * K2 + (y0 + dy)) * K1 * C + c;
+  const int SJ = a.SJ;
+  for (int xb = xs; xb < x1; xb++) {
+    const int xw = xb < 0 ? xb + K1 : xb;
+    if (xb == 0 && xs < 0) {
+      if (base0 >= 0) beg0 = __ldg(bs + base0);
+      if (base1 >= 0) beg1 = __ldg(bs + base1);
+    }
+    const int end0 = base0 >= 0 ? __ldg(bs + base0 + xw + 1) : beg0;
+    const int end1 = base1 >= 0 ? __ldg(bs + base1 + xw + 1) : beg1;
+    unsigned m0 = __ballot_sync(FULLM, end0 > beg0);
+    unsigned m1 = __ballot_sync(FULLM, end1 > beg1);
+    while (m0 | m1) {
+      int L, pb, pe;
+      if (m0) {
+        const int l = __ffs(m0) - 1;
+        m0 &= m0 - 1;
+        pb = __shfl_sync(FULLM, beg0, l);
+        pe = __shfl_sync(FULLM, end0, l);
+        L = l;
+      } else {
+        const int l = __ffs(m1) - 1;
+        m1 &= m1 - 1;
+        pb = __shfl_sync(FULLM, beg1, l);
+        pe = __shfl_sync(FULLM, end1, l);
+        L = l + 32;
+      }
+      const int j2 = dy - L % Q2 + 5, j3 = dz - L / Q2 + 5;
+      const bool hit = j2 >= 0 && j2 < 6 && j3 >= 0 && j3 < 6;
+      const int j2c = hit ? j2 : 0, j3c = hit ? j3 : 0;
+      // U samples at a time: all their loads are issued before any is used
+      // (dense bins at the k-space centre hold thousands of samples); the
+      // positions past the bin's end repeat its last sample and are not added
+      for (int p = pb; p < pe; p += U) {
+        float4 w1[U][3];
+        float2 f[U], w2[U], w3[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+          const int pu = min(p + u, pe - 1);
+          const float2 *Ws = a.W + (long long)pu * SJ;
+          const float4 *W4 = reinterpret_cast<const float4 *>(Ws);
+#pragma unroll
+          for (int h = 0; h < 3; h++) w1[u][h] = __ldg(W4 + h);
+          w2[u] = __ldg(Ws + 6 + j2c);
+          w3[u] = __ldg(Ws + 12 + j3c);
+          f[u] = on ? __ldg(fs + (long long)pu * C + c) : make_float2(0.f, 0.f);
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+          if (hit && p + u < pe) {
+            const float2 v3 = cw_mul<REAL>(w3[u], f[u]);
+            const float2 v = cw_mul<REAL>(w2[u], v3);
+#pragma unroll
+            for (int h = 0; h < 3; h++) {
+              cmac_conj<REAL>(acc[2 * h], make_float2(w1[u][h].x, w1[u][h].y), v);
+              cmac_conj<REAL>(acc[2 * h + 1], make_float2(w1[u][h].z, w1[u][h].w), v);
+            }
+          }
+        }
+      }
+    }
+    beg0 = end0;
+    beg1 = end1;
+    if (xb >= x0 && out_ok) out[(long long)xb * C] = acc[0];
+#pragma unroll
+    for (int j = 0; j < 5; j++) acc[j] = acc[j + 1];
+    acc[5] = make_float2(0.f, 0.f);
+  }
+}
+
+// Persistent 3D line sweep over the plan's heaviest-first work queue (one
+// counter per coil chunk); a warp is one team.
+template <int CW, int U, bool REAL>
+__global__ void __launch_bounds__(256) spread_sweep3_kernel(InterpArgs a, Tiling t,
+                                                            const int *__restrict__ bin_start,
+                                                            const float2 *__restrict__ fs,
+                                                            float2 *__restrict__ ck) {
+  constexpr int NL = 32 / CW;
+  constexpr int B2 = NL >= 2 ? 2 : 1;
+  constexpr int B3 = NL / B2;
+  const int lane = threadIdx.x & 31;
+  const long long nteam = (long long)t.nslice * ((a.g.K[1] + B2 - 1) / B2) *
+                          ((a.g.K[2] + B3 - 1) / B3) * t.sweep;
+  for (;;) {
+    int qi = 0;
+    if (lane == 0) qi = atomicAdd(t.team_next + blockIdx.y, 1);
+    qi = __shfl_sync(0xffffffffu, qi, 0);
+    if (qi >= nteam) break;
+    const long long team = t.team_order ? (long long)__ldg(t.team_order + qi) : qi;
+    sweep3_team<CW, U, REAL>(a, t, bin_start, fs, ck, team);
   }
 }
 
@@ -1088,6 +1278,40 @@ cudaError_t run(Req &r) {
   } else {
     const Tiling &t = *r.t;
     const size_t sm = spread_smem_bytes(a, t, l);
+    if constexpr (D == 3 && JT == 6 && (CW == 8 || CW == 16 || CW == 32)) {
+      if (t.sweep > 0) {
+        const unsigned nchunk = (unsigned)((a.C + CW - 1) / CW);
+        if (!t.sorted || !t.team_next) return cudaErrorInvalidValue;
+        if (a.Mtot > 0) {
+          const long long p0 = t.npos < 0 ? 0 : t.pos0;
+          const long long np = t.npos < 0 ? a.Mtot : t.npos;
+          const long long n = np * (long long)a.C;
+          long long nb = (n + 255) / 256;
+          if (nb > 148 * 16) nb = 148 * 16;
+          if (n > 0)
+            sweep_order_kernel<CW><<<(unsigned)nb, 256, 0, r.st>>>(a, r.in, t.sorted, p0, np);
+          cudaError_t e = cudaGetLastError();
+          if (e != cudaSuccess) return e;
+        }
+        auto kern = t.sweep_u == 4 ? spread_sweep3_kernel<CW, 4, REAL>
+                                   : spread_sweep3_kernel<CW, 1, REAL>;
+        int per_sm = 0, dev = 0, nsm = 0;
+        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0);
+        if (e != cudaSuccess) return e;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        constexpr int NL = 32 / CW, B2 = NL >= 2 ? 2 : 1, B3 = NL / B2;
+        const long long teams = (long long)t.nslice * ((a.g.K[1] + B2 - 1) / B2) *
+                                ((a.g.K[2] + B3 - 1) / B3) * t.sweep;
+        long long nb = (long long)nsm * (per_sm > 0 ? per_sm : 1);
+        if (nb > (teams + 7) / 8) nb = (teams + 7) / 8;
+        if (nb < 1) nb = 1;
+        e = cudaMemsetAsync(t.team_next, 0, nchunk * sizeof(int), r.st);
+        if (e != cudaSuccess) return e;
+        kern<<<dim3((unsigned)nb, nchunk), 256, 0, r.st>>>(a, t, r.bin_start, t.sorted, r.out);
+        return cudaGetLastError();
+      }
+    }
     if constexpr (D == 2 && JT == 6) {
       if (t.sweep != 0) {
         const long long nband = (a.g.K[1] + t.sweep_rows - 1) / max(t.sweep_rows, 1);
@@ -1125,10 +1349,11 @@ cudaError_t run(Req &r) {
           kern<<<dim3((unsigned)nb, nchunk), 256, 0, r.st>>>(a, t, r.bin_start, fs, r.out);
           return cudaGetLastError();
         };
+        const bool u4 = t.sweep_u == 4;
         switch (t.sweep_rows) {
-          case 1: return go(spread_sweep_kernel<CW, 1, REAL>);
-          case 2: return go(spread_sweep_kernel<CW, 2, REAL>);
-          case 4: return go(spread_sweep_kernel<CW, 4, REAL>);
+          case 1: return u4 ? go(spread_sweep_kernel<CW, 1, 4, REAL>) : go(spread_sweep_kernel<CW, 1, 1, REAL>);
+          case 2: return u4 ? go(spread_sweep_kernel<CW, 2, 4, REAL>) : go(spread_sweep_kernel<CW, 2, 1, REAL>);
+          case 4: return u4 ? go(spread_sweep_kernel<CW, 4, 4, REAL>) : go(spread_sweep_kernel<CW, 4, 1, REAL>);
           default: return cudaErrorInvalidValue;
         }
       }

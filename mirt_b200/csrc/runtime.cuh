@@ -78,6 +78,7 @@ struct mirt_interp_plan {
   std::vector<long long> gitem_slice;
   mirt::GatherBlocks gbk{};
   int gtma = 0;            // 1: the gather runs on TMA-staged tiles
+  int gfault_test = 0;     // 1: test of the TMA gather's bounded waits (no copies)
   int split_chunk = 1024;  // sample visits per spread task before a tile is split
   int heavy_first = 1;     // spread task order: 1 heaviest first, 0 grid order
   int deterministic = 1;   // 0: the spread may use shared-memory atomics

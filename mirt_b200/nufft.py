@@ -168,7 +168,9 @@ class InterpPlan:
     def set_sweep(self, segments=1, rows=4):
         """Row-sweep spread (2D, J = 6; see mirt_interp_plan_set_sweep):
         uniform segments per grid row (True = 1; 0 / False = tiled spread;
-        -1 = balanced team list) and grid rows per band (1, 2 or 4)."""
+        -1 = balanced team list) and grid rows per band (1, 2 or 4).  3D
+        plans (J = 6, coil chunks of 8, 16 or 32): the line sweep with
+        `segments` uniform segments per line block (rows unused)."""
         check(self.lib.mirt_interp_plan_set_sweep(self.handle, int(segments), int(rows)))
         return self.config()
 
@@ -184,6 +186,11 @@ class InterpPlan:
         f = C.c_int32(0)
         check(self.lib.mirt_interp_plan_fault(self.handle, C.byref(f)))
         return f.value
+
+    def set_fault_test(self, on=True):
+        """Test hook of the TMA gather's bounded waits (see
+        mirt_interp_plan_set_fault_test): no copies, every wait runs out."""
+        check(self.lib.mirt_interp_plan_set_fault_test(self.handle, int(bool(on))))
 
     def set_spread(self, tile, threads=32, padc=0, stream=None):
         """Fix the spread tiling (tile extents per dimension, CTA size, spare
