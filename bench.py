@@ -331,8 +331,6 @@ def run_gpu(args, w):
     tuned = plan.autotune() if not args.no_autotune else plan.config()
     if args.spread == "sweep" and tuned.get("spread_sweep", 0) == 0:
         tuned = plan.set_sweep(-1, 1)        # the plan's default: balanced teams of one row
-    elif args.spread == "list" and tuned.get("spread_sweep", 0) != -1:
-        tuned = plan.set_sweep(-1, args.sweep_rows)   # visit-list sweep
     elif args.spread == "tiled" and tuned.get("spread_sweep", 0) != 0:
         tuned = plan.set_sweep(0)
     t_tune = time.perf_counter() - t0
@@ -361,12 +359,15 @@ def run_gpu(args, w):
     torch.cuda.synchronize()
     eager_ms = ea.elapsed_time(eb) / args.steps
     # the timed steps replay one captured CUDA graph of the whole batched step
-    graph = plan.capture(x, X, xa)
-    graph.launch(stream)
-    torch.cuda.synchronize()
-
-    def step():  # noqa: F811 -- the graph replay replaces the eager step
+    # (--no-graph: eager steps, for profilers that trace kernel launches)
+    graph = None
+    if not args.no_graph:
+        graph = plan.capture(x, X, xa)
         graph.launch(stream)
+        torch.cuda.synchronize()
+
+        def step():  # noqa: F811 -- the graph replay replaces the eager step
+            graph.launch(stream)
 
     if world > 1:
         dist.barrier()
@@ -496,7 +497,8 @@ def run_gpu(args, w):
                        "coils": C, "slices_per_rank": plan.nslice,
                        "l2": "inputs larger than L2; no flush",
                        "launch": tuned, "autotune_s": round(t_tune, 2),
-                       "step": "one CUDA graph launch (forward + adjoint of the batch)",
+                       "step": ("eager forward + adjoint of the batch" if args.no_graph
+                                else "one CUDA graph launch (forward + adjoint of the batch)"),
                        "adjoint_order": ("shared-memory atomics (not bitwise reproducible)"
                                          if tuned.get("spread_atomic") else
                                          "fixed (bitwise reproducible)"),
@@ -507,7 +509,8 @@ def run_gpu(args, w):
             "cg_sense": cg,
         }
         print(json.dumps(line), flush=True)
-    graph.close()
+    if graph is not None:
+        graph.close()
     plan.close()
     if world > 1:
         dist.barrier()
@@ -657,8 +660,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
-    ap.add_argument("--sweep-rows", type=int, default=1, help="rows per band for --spread list")
-    ap.add_argument("--spread", default="auto", choices=["auto", "sweep", "list", "tiled"],
+    ap.add_argument("--no-graph", action="store_true",
+                    help="time eager steps instead of a CUDA-graph replay (for profiling)")
+    ap.add_argument("--spread", default="auto", choices=["auto", "sweep", "tiled"],
                     help="spread variant: the autotuner's choice, or the row sweep / tiled spread")
     ap.add_argument("--nondeterministic", action="store_true",
                     help="let the spread add with shared-memory atomics (not bitwise reproducible)")

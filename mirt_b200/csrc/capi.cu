@@ -197,6 +197,9 @@ int sweep_buffer(mirt_interp_plan *P) {
 // in all, in grid order (neighbouring bands read the same samples, so they
 // run together; heaviest-first order measured slower at full size).  Teams
 // write disjoint points, each summed in the same fixed order.
+// bins with at least this many samples are summed into patches before a sweep
+constexpr int kDenseBin = 16;
+
 // Visits per bin column of every band of `rows` grid rows: vb[(s * nband +
 // band) * K1 + x] = samples in bin column x of the band's rows + 5 bin rows.
 int sweep_band_visits(mirt_interp_plan *P, int rows, cudaStream_t st, std::vector<float> &vb) {
@@ -217,7 +220,11 @@ int sweep_band_visits(mirt_interp_plan *P, int rows, cudaStream_t st, std::vecto
         int r = (bi * rows - 5 + q) % K2;
         if (r < 0) r += K2;
         const int *br = b + (size_t)r * K1;
-        for (int x = 0; x < K1; x++) v[x] += (float)(br[x + 1] - br[x]);
+        for (int x = 0; x < K1; x++) {
+          const int n = br[x + 1] - br[x];
+          // a dense bin costs its patch rows, not its samples
+          v[x] += (float)(P->t.dense_of && n >= kDenseBin ? 6 : n);
+        }
       }
     }
   }
@@ -321,6 +328,77 @@ int build_sweep_teams(mirt_interp_plan *P, int rows, long long target, cudaStrea
   t.sweep = -1;
   t.sweep_rows = rows;
   return build_sweep_order(P, vb, st);
+}
+
+// The sweeps' dense bins: bins with at least `minc` samples (0: none), their
+// index map and patch buffer (J^D taps x C per dense bin).
+int build_dense(mirt_interp_plan *P, int minc, cudaStream_t st) {
+  const InterpArgs &a = P->a;
+  Tiling &t = P->t;
+  t.dense_of = nullptr;
+  t.dense_bin = nullptr;
+  t.patch = nullptr;
+  t.dense0 = 0;
+  t.ndense = 0;
+  t.dense_min = minc;
+  t.dense_chunk = nullptr;
+  t.dense_part0 = nullptr;
+  t.patch_part = nullptr;
+  t.chunk0 = 0;
+  t.nchunks = 0;
+  P->dense_slice.assign(t.nslice + 1, 0);
+  // (a chunk's sample rows are staged in shared memory: at most 256 columns)
+  if (minc <= 0 || a.C == 0 || a.C > 256) return MIRT_OK;
+  const long long nb = (long long)t.nbins * t.nslice;
+  std::vector<int> bs(nb + 1);
+  CK(cudaMemcpyAsync(bs.data(), P->bin_start.p, (nb + 1) * sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  std::vector<int> db;
+  for (long long b = 0; b < nb; b++) {
+    if (b % t.nbins == 0) P->dense_slice[b / t.nbins] = (int)db.size();
+    if (bs[b + 1] - bs[b] >= minc) db.push_back((int)b);
+  }
+  P->dense_slice[t.nslice] = (int)db.size();
+  if (db.empty()) return MIRT_OK;
+  int taps = 1;
+  for (int d = 0; d < a.g.D; d++) taps *= 6;
+  // chunks of at most 64 samples per dense bin, summed apart, then per bin
+  constexpr int kChunk = 64;
+  std::vector<int4> chunks;
+  std::vector<int> part0(db.size() + 1, 0);
+  for (size_t d = 0; d < db.size(); d++) {
+    part0[d] = (int)chunks.size();
+    for (int p = bs[db[d]]; p < bs[db[d] + 1]; p += kChunk)
+      chunks.push_back(make_int4((int)d, p, std::min(p + kChunk, bs[db[d] + 1]),
+                                 (int)chunks.size()));
+  }
+  part0[db.size()] = (int)chunks.size();
+  CK(P->dense_of.alloc(nb * sizeof(int)));
+  CK(P->dense_bin.alloc(db.size() * sizeof(int)));
+  CK(P->patch.alloc(db.size() * (size_t)taps * a.C * sizeof(float2)));
+  CK(P->dense_chunk.alloc(chunks.size() * sizeof(int4)));
+  CK(P->dense_part0.alloc(part0.size() * sizeof(int)));
+  CK(P->patch_part.alloc(chunks.size() * (size_t)taps * a.C * sizeof(float2)));
+  CK(cudaMemcpyAsync(P->dense_chunk.p, chunks.data(), chunks.size() * sizeof(int4),
+                     cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(P->dense_part0.p, part0.data(), part0.size() * sizeof(int),
+                     cudaMemcpyHostToDevice, st));
+  P->dense_part0_host = part0;
+  CK(cudaMemsetAsync(P->dense_of.p, 0xff, nb * sizeof(int), st));
+  CK(cudaMemcpyAsync(P->dense_bin.p, db.data(), db.size() * sizeof(int), cudaMemcpyHostToDevice,
+                     st));
+  CK(launch_mark_dense(P->dense_bin.as<int>(), (int)db.size(), P->dense_of.as<int>(), st));
+  CK(cudaStreamSynchronize(st));
+  t.dense_of = P->dense_of.as<int>();
+  t.dense_bin = P->dense_bin.as<int>();
+  t.patch = P->patch.as<float2>();
+  t.ndense = (int)db.size();
+  t.dense_chunk = P->dense_chunk.as<int4>();
+  t.dense_part0 = P->dense_part0.as<int>();
+  t.patch_part = P->patch_part.as<float2>();
+  t.chunk0 = 0;
+  t.nchunks = (int)chunks.size();
+  return MIRT_OK;
 }
 
 // 3D line sweep with nseg uniform segments per line block: the work queue of
@@ -467,7 +545,17 @@ void choose_config(mirt_interp_plan *P) {
   t.nteams = 0;
   t.team_order = nullptr;
   t.team_next = nullptr;
-  t.sweep_u = 4;
+  t.dense_of = nullptr;
+  t.dense_bin = nullptr;
+  t.patch = nullptr;
+  t.dense0 = 0;
+  t.ndense = 0;
+  t.dense_min = 0;
+  t.dense_chunk = nullptr;
+  t.dense_part0 = nullptr;
+  t.patch_part = nullptr;
+  t.chunk0 = 0;
+  t.nchunks = 0;
   t.nbins = 1;
   t.ntiles = 1;
   for (int d = 0; d < MIRT_DMAX; d++) {
@@ -873,6 +961,10 @@ int plan_finish(mirt_interp_plan *P, long long Mtot, const long long *moff, int 
   CK(query_gather_grid(a, P->lg));
   // 2D, J = 6, 32-coil chunks: the row sweep by default, one grid row per
   // team, balanced segments (about 64k teams, heaviest first)
+  if (sweep3_ok(a, P->t, P->ls.cw)) {
+    int rc3 = build_dense(P, kDenseBin, st);
+    if (rc3) return rc3;
+  }
   if (sweep_ok(a, P->t) && P->ls.cw == 32) {
     int rc3 = sweep_buffer(P);
     if (rc3) return rc3;
@@ -910,7 +1002,6 @@ int set_spread_tiles(mirt_interp_plan *P, const int *T, cudaStream_t st) {
 struct SpreadCand {
   int T[MIRT_DMAX];
   int threads, padc, atomic, own, sweep, sweep_rows;
-  int sweep_u = 4;  // samples whose loads the sweep issues together
 };
 
 // spare columns the J = 6 row update can use (0 elsewhere)
@@ -1124,18 +1215,16 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
   // row sweep (no tiles): bands of 1, 2 or 4 rows, whole rows or uniform
   // segments of at least 32 columns, or balanced teams (sweep = -1)
   if (sweep_ok(a, P->t) && sweep_buffer(P) == MIRT_OK)
-    for (int u : {1, 4})
-      for (int rows : {1, 2, 4})
-        for (int nseg = (rows < 4 ? -1 : 1); nseg <= 16 && (nseg <= 1 || a.g.K[0] / nseg >= 32);
-             nseg = nseg < 0 ? 1 : nseg * 2)
-          cands.push_back(SpreadCand{{P->t.T[0], P->t.T[1], P->t.T[2]}, P->ls.threads, 0, 0, 0,
-                                     nseg, rows, u});
+    for (int rows : {1, 2, 4})
+      for (int nseg = (rows < 4 ? -1 : 1); nseg <= 16 && (nseg <= 1 || a.g.K[0] / nseg >= 32);
+           nseg = nseg < 0 ? 1 : nseg * 2)
+        cands.push_back(SpreadCand{{P->t.T[0], P->t.T[1], P->t.T[2]}, P->ls.threads, 0, 0, 0,
+                                   nseg, rows});
   // 3D line sweep: 1, 2, 4 or 8 segments per line block
   if (sweep3_ok(a, P->t, cw) && sweep_buffer(P) == MIRT_OK)
-    for (int u : {1, 4})
-      for (int nseg : {1, 2, 4, 8})
-        cands.push_back(SpreadCand{{P->t.T[0], P->t.T[1], P->t.T[2]}, P->ls.threads, 0, 0, 0,
-                                   nseg, 1, u});
+    for (int nseg : {1, 2, 4, 8})
+      cands.push_back(SpreadCand{{P->t.T[0], P->t.T[1], P->t.T[2]}, P->ls.threads, 0, 0, 0,
+                                 nseg, 1});
   SpreadCand best{};
   float best_ms = 1e30f;
   int built_rows = 0;  // rows of the team list last built
@@ -1143,7 +1232,6 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
     P->t.own = c.own;
     P->t.sweep = c.sweep;
     P->t.sweep_rows = c.sweep_rows;
-    P->t.sweep_u = c.sweep_u;
     if (c.sweep < 0 && built_rows != c.sweep_rows) {
       int rc = build_sweep_teams(P, c.sweep_rows, 65536, st);
       if (rc) return rc;
@@ -1168,9 +1256,9 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
     if (autotune_log())
       std::fprintf(stderr,
                    "mirt autotune spread: tile %dx%dx%d threads %d padc %d atomic %d own %d "
-                   "sweep %d rows %d u %d: %.3f ms\n",
+                   "sweep %d rows %d: %.3f ms\n",
                    c.T[0], c.T[1], c.T[2], c.threads, c.padc, c.atomic, c.own, c.sweep,
-                   c.sweep_rows, c.sweep_u, ms);
+                   c.sweep_rows, ms);
     if (ms < best_ms) {
       best_ms = ms;
       best = c;
@@ -1180,7 +1268,6 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
     P->t.own = best.own;
     P->t.sweep = best.sweep;
     P->t.sweep_rows = best.sweep_rows;
-    P->t.sweep_u = best.sweep_u;
     if (best.sweep < 0 && built_rows != best.sweep_rows) {
       int rc = build_sweep_teams(P, best.sweep_rows, 65536, st);
       if (rc) return rc;
@@ -2209,6 +2296,12 @@ int nufft_adjoint_range(mirt_nufft *p, int s0, int s1, const float2 *X, float2 *
   Tiling t = P->t;
   if (t.sweep < 0) t.sweep = 2;  // a chunk: uniform halves of rows (same sums)
   t.team_order = nullptr;        // the chunk's teams in index order
+  if (t.ndense > 0) {            // the chunk's dense bins and their sample chunks
+    t.dense0 = P->dense_slice[s0];
+    t.ndense = P->dense_slice[s1] - t.dense0;
+    t.chunk0 = P->dense_part0_host[t.dense0];
+    t.nchunks = P->dense_part0_host[t.dense0 + t.ndense] - t.chunk0;
+  }
   t.slice0 = s0;
   t.nslice = ns;
   t.pos0 = P->moff_host[s0];
@@ -2409,7 +2502,9 @@ int mirt_nufft_config(mirt_nufft *p, int32_t *out, int32_t n) {
   const int fwd = (p->own_fft ? p->gg.D : 2) + 1;
   int spread = 1;
   if (t.sweep != 0) {
-    spread = 2;  // ordering pass and sweep (and a memset of the work-queue counters)
+    // ordering pass, dense-bin patches (chunk sums, per-bin sums), sweep (and a
+    // memset of the queue counters)
+    spread = 2 + (t.ndense > 0 ? 2 : 0);
   } else if (t.own) {
     spread = 1;  // the clearing memset, then per colour a launch and a reduction
     for (int c = 0; c < 4; c++)

@@ -211,6 +211,19 @@ cudaError_t launch_gather(const InterpArgs &a, const Launch &l, const float2 *ck
   return dispatch(r);
 }
 
+namespace {
+__global__ void mark_dense_kernel(const int *__restrict__ dense_bin, int n, int *dense_of) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dense_of[dense_bin[i]] = i;
+}
+}  // namespace
+
+cudaError_t launch_mark_dense(const int *dense_bin, int n, int *dense_of, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  mark_dense_kernel<<<(n + 255) / 256, 256, 0, st>>>(dense_bin, n, dense_of);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_spread(const InterpArgs &a, const Tiling &t, const Launch &l,
                           const int *bin_start, const float2 *fm, float2 *ck, cudaStream_t st) {
   if (a.C == 0) return cudaSuccess;

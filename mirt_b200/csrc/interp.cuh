@@ -77,7 +77,25 @@ struct Tiling {
   // chunk], which are cleared before every launch.
   const int *team_order;
   int *team_next;
-  int sweep_u;           // samples of a bin whose loads are issued together (1 or 4)
+  // Dense bins (the sweeps): bins holding at least a threshold of samples.
+  // Before a sweep, dense_part/reduce_kernel sum each dense bin's samples into its
+  // patch of J^D taps x C (patch[d][tap][c], tap = (j3 J + j2) J + j1), and
+  // the sweep adds the patch where it meets the bin instead of its samples.
+  // dense_of[global bin] = its dense index or -1; dense_bin[d] = the global
+  // bin; a launch covers dense bins [dense0, dense0 + ndense).
+  const int *dense_of;
+  const int *dense_bin;
+  float2 *patch;
+  int dense0, ndense;
+  int dense_min;         // samples that make a bin dense
+  // the patches are summed in chunks of at most 64 samples: chunk i =
+  // dense_chunk[i] = (dense bin, first position, end position, part index);
+  // dense bin d's chunk sums are patch_part[dense_part0[d] .. dense_part0[d+1]);
+  // a launch covers chunks [chunk0, chunk0 + nchunks)
+  const int4 *dense_chunk;
+  const int *dense_part0;
+  float2 *patch_part;
+  int chunk0, nchunks;
   int color_beg[9];
   int red_beg[9];
   int padc;              // spread: spare columns on each side of a tile row in
@@ -167,6 +185,9 @@ cudaError_t query_gather_grid(const InterpArgs &a, Launch &l);
 // fm[m][c] = sum_taps h * ck   for every sample (forward gather)
 cudaError_t launch_gather(const InterpArgs &a, const Launch &l, const float2 *ck,
                           float2 *fm, cudaStream_t st);
+
+// dense_of[dense_bin[i]] = i for i < n (dense_of cleared to -1 first)
+cudaError_t launch_mark_dense(const int *dense_bin, int n, int *dense_of, cudaStream_t st);
 
 // ck = adjoint of the gather; deterministic owner-computes spread over tiles
 cudaError_t launch_spread(const InterpArgs &a, const Tiling &t, const Launch &l,

@@ -698,7 +698,7 @@ __global__ void __launch_bounds__(256) sweep_order_kernel(InterpArgs a, const fl
 }
 
 // The sweep of one team (see spread_sweep_kernel).
-template <int CW, int R, int U, bool REAL>
+template <int CW, int R, bool REAL>
 __device__ __forceinline__ void sweep_team(const InterpArgs &a, const Tiling &t,
                                            const int *__restrict__ bin_start,
                                            const float2 *__restrict__ fs,
@@ -757,43 +757,25 @@ __device__ __forceinline__ void sweep_team(const InterpArgs &a, const Tiling &t,
     for (int q = 0; q < NQ; q++) end[q] = __ldg(bs + row[q] + xw + 1);
 #pragma unroll
     for (int q = 0; q < NQ; q++) {
-      // U samples at a time, all their loads issued first; positions past the
-      // bin's end repeat its last sample and are not added
       const int pe = end[q];
-      for (int p = beg[q]; p < pe; p += U) {
-        float2 f[U], w2[U][R];
-        float4 w1[U][3];
+      for (int p = beg[q]; p < pe; p++) {
+        const float2 f = on ? __ldg(fs + (long long)p * C + c) : make_float2(0.f, 0.f);
+        const float2 *Ws = a.W + (long long)p * 12;
+        const float4 *W4 = reinterpret_cast<const float4 *>(Ws);
+        float4 w1[3];
 #pragma unroll
-        for (int u = 0; u < U; u++) {
-          const int pu = U == 1 ? p : min(p + u, pe - 1);
-          f[u] = on ? __ldg(fs + (long long)pu * C + c) : make_float2(0.f, 0.f);
-          const float2 *Ws = a.W + (long long)pu * 12;
-          const float4 *W4 = reinterpret_cast<const float4 *>(Ws);
+        for (int h = 0; h < 3; h++) w1[h] = __ldg(W4 + h);
 #pragma unroll
-          for (int h = 0; h < 3; h++) w1[u][h] = __ldg(W4 + h);
+        for (int r = 0; r < R; r++) {
+          const int j2 = r - q + 5;  // compile-time after unrolling
+          if (j2 >= 0 && j2 < 6) {
+            const float2 v = cw_mul<REAL>(__ldg(Ws + 6 + j2), f);
+            const float2 vs = make_float2(v.y, v.x);
 #pragma unroll
-          for (int r = 0; r < R; r++) {
-            const int j2 = r - q + 5;  // compile-time after unrolling
-            if (j2 >= 0 && j2 < 6) w2[u][r] = __ldg(Ws + 6 + j2);
-          }
-        }
-#pragma unroll
-        for (int u = 0; u < U; u++) {
-          if (U == 1 || p + u < pe) {
-#pragma unroll
-            for (int r = 0; r < R; r++) {
-              const int j2 = r - q + 5;
-              if (j2 >= 0 && j2 < 6) {
-                const float2 v = cw_mul<REAL>(w2[u][r], f[u]);
-                const float2 vs = make_float2(v.y, v.x);
-#pragma unroll
-                for (int h = 0; h < 3; h++) {
-                  acc[r][2 * h] =
-                      cw_fma<REAL>(make_float2(w1[u][h].x, w1[u][h].y), v, vs, acc[r][2 * h]);
-                  acc[r][2 * h + 1] = cw_fma<REAL>(make_float2(w1[u][h].z, w1[u][h].w), v, vs,
-                                                   acc[r][2 * h + 1]);
-                }
-              }
+            for (int h = 0; h < 3; h++) {
+              acc[r][2 * h] = cw_fma<REAL>(make_float2(w1[h].x, w1[h].y), v, vs, acc[r][2 * h]);
+              acc[r][2 * h + 1] =
+                  cw_fma<REAL>(make_float2(w1[h].z, w1[h].w), v, vs, acc[r][2 * h + 1]);
             }
           }
         }
@@ -818,7 +800,7 @@ __device__ __forceinline__ void sweep_team(const InterpArgs &a, const Tiling &t,
 // plan's work queue (heaviest teams first) until the queue is empty, so warps
 // do not sit idle behind a heavy team of their block.  Each team's sums are
 // independent of which warp runs it: deterministic.
-template <int CW, int R, int U, bool REAL>
+template <int CW, int R, bool REAL>
 __global__ void __launch_bounds__(256) spread_sweep_kernel(InterpArgs a, Tiling t,
                                                            const int *__restrict__ bin_start,
                                                            const float2 *__restrict__ fs,
@@ -836,39 +818,146 @@ __global__ void __launch_bounds__(256) spread_sweep_kernel(InterpArgs a, Tiling 
     const long long qi = (long long)base + lane / CW;
     if (qi < nteam) {
       const long long team = t.team_order ? (long long)__ldg(t.team_order + qi) : qi;
-      sweep_team<CW, R, U, REAL>(a, t, bin_start, fs, ck, team);
+      sweep_team<CW, R, REAL>(a, t, bin_start, fs, ck, team);
     }
   }
+}
+
+// Dense-bin patches for the sweeps (J = 6, D = 2 or 3), in two launches.
+// dense_part_kernel: block i takes chunk i of a dense bin (up to DP_CH of its
+// samples, plan order, already times conj(phase) in fs), copies their tap
+// records and sample rows into shared memory and sums them, one thread per
+// row (j3, j2, c) of six j1 taps, in the sweeps' per-sample operation order
+// and the samples' sort order, into patch_part[i].  dense_reduce_kernel:
+// block d adds its bin's chunk sums in chunk order into patch[d].
+constexpr int DP_CH = 64;
+template <int D, bool REAL>
+__global__ void __launch_bounds__(256) dense_part_kernel(InterpArgs a, Tiling t,
+                                                         const float2 *__restrict__ fs) {
+  constexpr int NR = D == 3 ? 36 : 6;  // (j3, j2) rows of a patch
+  constexpr int SJ = D == 3 ? 18 : 12;
+  extern __shared__ __align__(16) float2 dsm[];
+  const int4 ch = t.dense_chunk[t.chunk0 + blockIdx.x];  // (dense bin, p0, p1, part)
+  const int n = ch.z - ch.y;
+  const int C = a.C;
+  float2 *sw = dsm;                 // [DP_CH][SJ]
+  float2 *sf = dsm + DP_CH * SJ;    // [DP_CH][C]
+  for (int e = threadIdx.x; e < n * SJ; e += blockDim.x) sw[e] = __ldg(a.W + (long long)ch.y * SJ + e);
+  for (int e = threadIdx.x; e < n * C; e += blockDim.x) sf[e] = __ldg(fs + (long long)ch.y * C + e);
+  __syncthreads();
+  float2 *out = t.patch_part + (long long)ch.w * NR * 6 * C;
+  for (int row = threadIdx.x; row < NR * C; row += blockDim.x) {
+    const int c = row % C, jr = row / C;
+    const int j2 = jr % 6, j3 = jr / 6;
+    float2 acc[6];
+#pragma unroll
+    for (int j = 0; j < 6; j++) acc[j] = make_float2(0.f, 0.f);
+    for (int q = 0; q < n; q++) {
+      const float2 *w = sw + q * SJ;
+      float2 v = sf[q * C + c];
+      if (D == 3) v = cw_mul<REAL>(w[12 + j3], v);
+      v = cw_mul<REAL>(w[6 + j2], v);
+#pragma unroll
+      for (int j = 0; j < 6; j++) cmac_conj<REAL>(acc[j], w[j], v);
+    }
+#pragma unroll
+    for (int j = 0; j < 6; j++) out[((long long)jr * 6 + j) * C + c] = acc[j];
+  }
+}
+
+template <int D>
+__global__ void __launch_bounds__(256) dense_reduce_kernel(InterpArgs a, Tiling t) {
+  constexpr int NP = D == 3 ? 216 : 36;
+  const int d = t.dense0 + blockIdx.x;
+  const int q0 = __ldg(t.dense_part0 + d), q1 = __ldg(t.dense_part0 + d + 1);
+  const long long pn = (long long)NP * a.C;
+  float2 *out = t.patch + (long long)d * pn;
+  for (long long e = threadIdx.x; e < pn; e += blockDim.x) {
+    float2 v = t.patch_part[(long long)q0 * pn + e];
+    for (int q = q0 + 1; q < q1; q++) {
+      const float2 w = t.patch_part[(long long)q * pn + e];
+      v.x += w.x;
+      v.y += w.y;
+    }
+    out[e] = v;
+  }
+}
+
+// the two launches of the patches of dense bins [dense0, dense0 + ndense)
+template <int D, bool REAL>
+cudaError_t launch_dense_patches(const InterpArgs &a, const Tiling &t, const float2 *fs,
+                                 cudaStream_t st) {
+  if (!t.dense_of || t.ndense <= 0 || t.nchunks <= 0) return cudaSuccess;
+  constexpr int SJ = D == 3 ? 18 : 12;
+  const size_t sm = (size_t)DP_CH * (SJ + a.C) * sizeof(float2);
+  auto k1 = dense_part_kernel<D, REAL>;
+  cudaError_t e = cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return e;
+  k1<<<(unsigned)t.nchunks, 256, sm, st>>>(a, t, fs);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  dense_reduce_kernel<D><<<(unsigned)t.ndense, 256, 0, st>>>(a, t);
+  return cudaGetLastError();
 }
 
 // ------------------------------------------------------------------------
 // 3D line sweep (J = 6 in every dimension, one-point bins, K >= 6)
 // ------------------------------------------------------------------------
+// cp.async copies into this thread's CTA's shared memory, and their wait
+__device__ __forceinline__ unsigned smem_u32(const void *p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async8(void *dst, const void *src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
+constexpr int SW3_CAP = 32;  // visits staged per batch and warp
+template <int CW>
+constexpr int sweep3_warp_bytes() {
+  return 2 * SW3_CAP * 4 + SW3_CAP * 18 * 8 + SW3_CAP * CW * 8;
+}
+
 // A warp owns a block of B2 x B3 grid lines along k1 (rows y0 .. y0 + B2 - 1
 // of planes z0 .. z0 + B3 - 1; lanes = CW coils x the block's 32 / CW lines:
 // 2 x 2 lines for 8 coils, 2 x 1 for 16, one line for 32) and a segment
 // [x0, x1) of their columns.  The samples with taps in the block are those
 // binned in the Q2 x Q3 = (B2 + 5) x (B3 + 5) bin lines around it; lane l
-// keeps the bin pointers of bin lines l and l + 32.  The warp sweeps bin
-// columns x0 - 5 .. x1 - 1 (wrapped): per column it loads each bin line's end
-// pointer, takes the non-empty lines in a fixed order (ballot), and for each
-// sample every lane adds the sample's six k1 taps into the six-column window
-// of its own line (when the line is within the sample's 6 x 6 tap rows), with
-// the same FP32 operation order per tap as the tiled spread (conj(w3) f, then
-// conj(w2), then conj(w1)).  After bin column x, grid column x of every line
-// is complete and is stored once.  Summation order per grid point: columns,
-// bin lines, samples in sort order -- fixed: bitwise reproducible.
-template <int CW, int U, bool REAL>
+// keeps the bin pointers of bin lines l and l + 32, and loads those of the
+// next column while the current one is summed.  Per bin column the warp
+// lists the column's samples (bin lines in index order, samples in sort
+// order), copies their tap records and sample rows into its shared-memory
+// stage with cp.async (all in flight at once), and then every lane adds each
+// sample's six k1 taps into the six-column window of its own line (when the
+// line is within the sample's 6 x 6 tap rows), with the same FP32 operation
+// order per tap as the tiled spread (conj(w3) f, then conj(w2), then
+// conj(w1)).  Dense bins (at least dense_min samples) add their patches after
+// the column's samples, in bin-line order.  After bin column x, grid column x
+// of every line is complete and is stored once.  The summation order per
+// grid point is fixed and independent of the segments: bitwise reproducible.
+template <int CW, bool REAL>
 __device__ __forceinline__ void sweep3_team(const InterpArgs &a, const Tiling &t,
                                             const int *__restrict__ bin_start,
                                             const float2 *__restrict__ fs,
-                                            float2 *__restrict__ ck, long long team) {
+                                            float2 *__restrict__ ck, long long team,
+                                            unsigned char *wsm) {
   constexpr unsigned FULLM = 0xffffffffu;
   constexpr int NL = 32 / CW;             // lines per warp
   constexpr int B2 = NL >= 2 ? 2 : 1;
   constexpr int B3 = NL / B2;
   constexpr int Q2 = B2 + 5, Q3 = B3 + 5, NBL = Q2 * Q3;  // bin lines, at most 49
   static_assert(NBL <= 64, "bin lines must fit two per lane");
+  int *spos = reinterpret_cast<int *>(wsm);
+  int *slin = spos + SW3_CAP;
+  float2 *srec = reinterpret_cast<float2 *>(wsm + 2 * SW3_CAP * 4);
+  float2 *sf = srec + SW3_CAP * 18;
   const int K1 = a.g.K[0], K2 = a.g.K[1], K3 = a.g.K[2];
   const int nseg = t.sweep;
   const int nby = (K2 + B2 - 1) / B2, nbz = (K3 + B3 - 1) / B3;
@@ -883,12 +972,14 @@ __device__ __forceinline__ void sweep3_team(const InterpArgs &a, const Tiling &t
   const int x0 = seg * sw, x1 = min(K1, x0 + sw);
   if (x0 >= x1) return;
   const int lane = threadIdx.x & 31;
-  const int li = lane / CW;
+  const int li = lane / CW, cl = lane % CW;
   const int dy = li % B2, dz = li / B2;
   const int C = a.C;
-  const int c = blockIdx.y * CW + lane % CW;
-  const bool on = c < C;
+  const int c0 = blockIdx.y * CW;
+  const bool on = c0 + cl < C;
   const int *bs = bin_start + (long long)slice * t.nbins;
+  const int *dof = t.dense_of ? t.dense_of + (long long)slice * t.nbins : nullptr;
+  const int dmin = t.dense_of ? t.dense_min : 0x7fffffff;
   auto line_base = [&](int l) -> long long {
     int r = (y0 - 5 + l % Q2) % K2;
     if (r < 0) r += K2;
@@ -899,72 +990,115 @@ __device__ __forceinline__ void sweep3_team(const InterpArgs &a, const Tiling &t
   const long long base0 = lane < NBL ? line_base(lane) : -1;
   const long long base1 = lane + 32 < NBL ? line_base(lane + 32) : -1;
   const int xs = x0 - 5;
-  const int xs_w = xs < 0 ? xs + K1 : xs;
-  int beg0 = base0 >= 0 ? __ldg(bs + base0 + xs_w) : 0;
-  int beg1 = base1 >= 0 ? __ldg(bs + base1 + xs_w) : 0;
+  auto wrapx = [&](int x) { return x < 0 ? x + K1 : x; };
+  int beg0 = base0 >= 0 ? __ldg(bs + base0 + wrapx(xs)) : 0;
+  int beg1 = base1 >= 0 ? __ldg(bs + base1 + wrapx(xs)) : 0;
+  // end of each bin line's samples
+  const int rend0 = base0 >= 0 ? __ldg(bs + base0 + K1) : 0;
+  const int rend1 = base1 >= 0 ? __ldg(bs + base1 + K1) : 0;
+  // end pointers of the next column (and the row starts where the sweep wraps)
+  int e0n = base0 >= 0 ? __ldg(bs + base0 + wrapx(xs) + 1) : beg0;
+  int e1n = base1 >= 0 ? __ldg(bs + base1 + wrapx(xs) + 1) : beg1;
+  int r0n = 0, r1n = 0;
   float2 acc[6];
 #pragma unroll
   for (int j = 0; j < 6; j++) acc[j] = make_float2(0.f, 0.f);
   const bool out_ok = on && y0 + dy < K2 && z0 + dz < K3;
   float2 *out = ck + (long long)slice * a.grid_elems +
-                ((long long)(z0 + dz) * K2 + (y0 + dy)) * K1 * C + c;
-  const int SJ = a.SJ;
+                ((long long)(z0 + dz) * K2 + (y0 + dy)) * K1 * C + c0 + cl;
   for (int xb = xs; xb < x1; xb++) {
-    const int xw = xb < 0 ? xb + K1 : xb;
+    const int end0 = e0n, end1 = e1n;
     if (xb == 0 && xs < 0) {
-      if (base0 >= 0) beg0 = __ldg(bs + base0);
-      if (base1 >= 0) beg1 = __ldg(bs + base1);
+      beg0 = r0n;
+      beg1 = r1n;
     }
-    const int end0 = base0 >= 0 ? __ldg(bs + base0 + xw + 1) : beg0;
-    const int end1 = base1 >= 0 ? __ldg(bs + base1 + xw + 1) : beg1;
-    unsigned m0 = __ballot_sync(FULLM, end0 > beg0);
-    unsigned m1 = __ballot_sync(FULLM, end1 > beg1);
-    while (m0 | m1) {
-      int L, pb, pe;
-      if (m0) {
-        const int l = __ffs(m0) - 1;
-        m0 &= m0 - 1;
-        pb = __shfl_sync(FULLM, beg0, l);
-        pe = __shfl_sync(FULLM, end0, l);
-        L = l;
+    if (xb + 1 < x1) {
+      const int xn = wrapx(xb + 1);
+      if (base0 >= 0) e0n = __ldg(bs + base0 + xn + 1);
+      if (base1 >= 0) e1n = __ldg(bs + base1 + xn + 1);
+      if (xb + 1 == 0) {
+        if (base0 >= 0) r0n = __ldg(bs + base0);
+        if (base1 >= 0) r1n = __ldg(bs + base1);
+      }
+    }
+    const int n0 = end0 - beg0, n1 = end1 - beg1;
+    const int s0 = n0 >= dmin ? 0 : n0, s1 = n1 >= dmin ? 0 : n1;
+    // the column's sparse samples: line 0 .. 31, then 32 .. 48, in lane order
+    int i0 = s0, i1 = s1;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int u0 = __shfl_up_sync(FULLM, i0, o), u1 = __shfl_up_sync(FULLM, i1, o);
+      if (lane >= o) {
+        i0 += u0;
+        i1 += u1;
+      }
+    }
+    const int tot0 = __shfl_sync(FULLM, i0, 31);
+    const int V = tot0 + __shfl_sync(FULLM, i1, 31);
+    const int ex0 = i0 - s0, ex1 = tot0 + i1 - s1;
+    for (int vb = 0; vb < V; vb += SW3_CAP) {
+      const int nb = min(SW3_CAP, V - vb);
+      for (int k = max(0, vb - ex0); k < s0 && ex0 + k < vb + SW3_CAP; k++) {
+        spos[ex0 + k - vb] = beg0 + k;
+        slin[ex0 + k - vb] = lane;
+      }
+      for (int k = max(0, vb - ex1); k < s1 && ex1 + k < vb + SW3_CAP; k++) {
+        spos[ex1 + k - vb] = beg1 + k;
+        slin[ex1 + k - vb] = lane + 32;
+      }
+      __syncwarp();
+      for (int ch = lane; ch < nb * 9; ch += 32) {
+        const int v = ch / 9, k = ch - 9 * v;
+        cp_async16(srec + v * 18 + 2 * k, a.W + (long long)spos[v] * 18 + 2 * k);
+      }
+      for (int ch = lane; ch < nb * CW; ch += 32) {
+        const int v = ch / CW, k = ch - CW * v;
+        if (c0 + k < C)
+          cp_async8(sf + v * CW + k, fs + (long long)spos[v] * C + c0 + k);
+        else
+          sf[v * CW + k] = make_float2(0.f, 0.f);
+      }
+      cp_async_wait_all();
+      __syncwarp();
+      for (int v = 0; v < nb; v++) {
+        const int L = slin[v];
+        const int j2 = dy - L % Q2 + 5, j3 = dz - L / Q2 + 5;
+        if (j2 >= 0 && j2 < 6 && j3 >= 0 && j3 < 6) {
+          const float2 *rv = srec + v * 18;
+          const float2 v3 = cw_mul<REAL>(rv[12 + j3], sf[v * CW + cl]);
+          const float2 vv = cw_mul<REAL>(rv[6 + j2], v3);
+#pragma unroll
+          for (int j = 0; j < 6; j++) cmac_conj<REAL>(acc[j], rv[j], vv);
+        }
+      }
+      __syncwarp();  // the stage is read before the next batch refills it
+    }
+    // dense bins: their patches, in bin-line order
+    unsigned md0 = __ballot_sync(FULLM, n0 >= dmin && n0 > 0);
+    unsigned md1 = __ballot_sync(FULLM, n1 >= dmin && n1 > 0);
+    const bool had_dense = (md0 | md1) != 0;
+    while (md0 | md1) {
+      int L;
+      long long bb;
+      if (md0) {
+        L = __ffs(md0) - 1;
+        md0 &= md0 - 1;
+        bb = __shfl_sync(FULLM, base0, L);
       } else {
-        const int l = __ffs(m1) - 1;
-        m1 &= m1 - 1;
-        pb = __shfl_sync(FULLM, beg1, l);
-        pe = __shfl_sync(FULLM, end1, l);
+        const int l = __ffs(md1) - 1;
+        md1 &= md1 - 1;
+        bb = __shfl_sync(FULLM, base1, l);
         L = l + 32;
       }
+      const int dn = __ldg(dof + bb + wrapx(xb));
       const int j2 = dy - L % Q2 + 5, j3 = dz - L / Q2 + 5;
-      const bool hit = j2 >= 0 && j2 < 6 && j3 >= 0 && j3 < 6;
-      const int j2c = hit ? j2 : 0, j3c = hit ? j3 : 0;
-      // U samples at a time: all their loads are issued before any is used
-      // (dense bins at the k-space centre hold thousands of samples); the
-      // positions past the bin's end repeat its last sample and are not added
-      for (int p = pb; p < pe; p += U) {
-        float4 w1[U][3];
-        float2 f[U], w2[U], w3[U];
+      if (on && j2 >= 0 && j2 < 6 && j3 >= 0 && j3 < 6) {
+        const float2 *pp = t.patch + ((long long)dn * 216 + (j3 * 6 + j2) * 6) * C + c0 + cl;
 #pragma unroll
-        for (int u = 0; u < U; u++) {
-          const int pu = min(p + u, pe - 1);
-          const float2 *Ws = a.W + (long long)pu * SJ;
-          const float4 *W4 = reinterpret_cast<const float4 *>(Ws);
-#pragma unroll
-          for (int h = 0; h < 3; h++) w1[u][h] = __ldg(W4 + h);
-          w2[u] = __ldg(Ws + 6 + j2c);
-          w3[u] = __ldg(Ws + 12 + j3c);
-          f[u] = on ? __ldg(fs + (long long)pu * C + c) : make_float2(0.f, 0.f);
-        }
-#pragma unroll
-        for (int u = 0; u < U; u++) {
-          if (hit && p + u < pe) {
-            const float2 v3 = cw_mul<REAL>(w3[u], f[u]);
-            const float2 v = cw_mul<REAL>(w2[u], v3);
-#pragma unroll
-            for (int h = 0; h < 3; h++) {
-              cmac_conj<REAL>(acc[2 * h], make_float2(w1[u][h].x, w1[u][h].y), v);
-              cmac_conj<REAL>(acc[2 * h + 1], make_float2(w1[u][h].z, w1[u][h].w), v);
-            }
-          }
+        for (int j = 0; j < 6; j++) {
+          const float2 v = __ldg(pp + (long long)j * C);
+          acc[j].x += v.x;
+          acc[j].y += v.y;
         }
       }
     }
@@ -974,20 +1108,46 @@ __device__ __forceinline__ void sweep3_team(const InterpArgs &a, const Tiling &t
 #pragma unroll
     for (int j = 0; j < 5; j++) acc[j] = acc[j + 1];
     acc[5] = make_float2(0.f, 0.f);
+    // skip-ahead: after a column with no sample, jump to the next column in
+    // which any of the bin lines holds one (the first tap column of each
+    // line's next sample); the columns in between receive nothing
+    if (V == 0 && !had_dense && xb >= 0 && xb + 1 < x1) {
+      const int nc0 = beg0 < rend0 ? __ldg(&a.K0[beg0].x) : x1;
+      const int nc1 = beg1 < rend1 ? __ldg(&a.K0[beg1].x) : x1;
+      const int xn = min(__reduce_min_sync(FULLM, min(nc0, nc1)), x1);
+      if (xn > xb + 1) {
+        int x = xb + 1;
+        for (int k = 0; k < 6 && x < xn; k++, x++) {
+          if (x >= x0 && out_ok) out[(long long)x * C] = acc[0];
+#pragma unroll
+          for (int j = 0; j < 5; j++) acc[j] = acc[j + 1];
+          acc[5] = make_float2(0.f, 0.f);
+        }
+        for (; x < xn; x++)
+          if (x >= x0 && out_ok) out[(long long)x * C] = make_float2(0.f, 0.f);
+        xb = xn - 1;  // the loop moves on to column xn
+        if (xn < x1) {
+          if (base0 >= 0) e0n = __ldg(bs + base0 + xn + 1);
+          if (base1 >= 0) e1n = __ldg(bs + base1 + xn + 1);
+        }
+      }
+    }
   }
 }
 
 // Persistent 3D line sweep over the plan's heaviest-first work queue (one
-// counter per coil chunk); a warp is one team.
-template <int CW, int U, bool REAL>
+// counter per coil chunk); a warp is one team, with its own shared-memory stage.
+template <int CW, bool REAL>
 __global__ void __launch_bounds__(256) spread_sweep3_kernel(InterpArgs a, Tiling t,
                                                             const int *__restrict__ bin_start,
                                                             const float2 *__restrict__ fs,
                                                             float2 *__restrict__ ck) {
+  extern __shared__ __align__(16) unsigned char sm3[];
   constexpr int NL = 32 / CW;
   constexpr int B2 = NL >= 2 ? 2 : 1;
   constexpr int B3 = NL / B2;
   const int lane = threadIdx.x & 31;
+  unsigned char *wsm = sm3 + (threadIdx.x >> 5) * sweep3_warp_bytes<CW>();
   const long long nteam = (long long)t.nslice * ((a.g.K[1] + B2 - 1) / B2) *
                           ((a.g.K[2] + B3 - 1) / B3) * t.sweep;
   for (;;) {
@@ -996,7 +1156,7 @@ __global__ void __launch_bounds__(256) spread_sweep3_kernel(InterpArgs a, Tiling
     qi = __shfl_sync(0xffffffffu, qi, 0);
     if (qi >= nteam) break;
     const long long team = t.team_order ? (long long)__ldg(t.team_order + qi) : qi;
-    sweep3_team<CW, U, REAL>(a, t, bin_start, fs, ck, team);
+    sweep3_team<CW, REAL>(a, t, bin_start, fs, ck, team, wsm);
   }
 }
 
@@ -1293,10 +1453,17 @@ cudaError_t run(Req &r) {
           cudaError_t e = cudaGetLastError();
           if (e != cudaSuccess) return e;
         }
-        auto kern = t.sweep_u == 4 ? spread_sweep3_kernel<CW, 4, REAL>
-                                   : spread_sweep3_kernel<CW, 1, REAL>;
+        {
+          cudaError_t e = launch_dense_patches<3, REAL>(a, t, t.sorted, r.st);
+          if (e != cudaSuccess) return e;
+        }
+        auto kern = spread_sweep3_kernel<CW, REAL>;
+        const size_t smem3 = 8 * (size_t)sweep3_warp_bytes<CW>();
         int per_sm = 0, dev = 0, nsm = 0;
-        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0);
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem3);
+        if (e != cudaSuccess) return e;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, smem3);
         if (e != cudaSuccess) return e;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -1308,7 +1475,7 @@ cudaError_t run(Req &r) {
         if (nb < 1) nb = 1;
         e = cudaMemsetAsync(t.team_next, 0, nchunk * sizeof(int), r.st);
         if (e != cudaSuccess) return e;
-        kern<<<dim3((unsigned)nb, nchunk), 256, 0, r.st>>>(a, t, r.bin_start, t.sorted, r.out);
+        kern<<<dim3((unsigned)nb, nchunk), 256, smem3, r.st>>>(a, t, r.bin_start, t.sorted, r.out);
         return cudaGetLastError();
       }
     }
@@ -1349,11 +1516,10 @@ cudaError_t run(Req &r) {
           kern<<<dim3((unsigned)nb, nchunk), 256, 0, r.st>>>(a, t, r.bin_start, fs, r.out);
           return cudaGetLastError();
         };
-        const bool u4 = t.sweep_u == 4;
         switch (t.sweep_rows) {
-          case 1: return u4 ? go(spread_sweep_kernel<CW, 1, 4, REAL>) : go(spread_sweep_kernel<CW, 1, 1, REAL>);
-          case 2: return u4 ? go(spread_sweep_kernel<CW, 2, 4, REAL>) : go(spread_sweep_kernel<CW, 2, 1, REAL>);
-          case 4: return u4 ? go(spread_sweep_kernel<CW, 4, 4, REAL>) : go(spread_sweep_kernel<CW, 4, 1, REAL>);
+          case 1: return go(spread_sweep_kernel<CW, 1, REAL>);
+          case 2: return go(spread_sweep_kernel<CW, 2, REAL>);
+          case 4: return go(spread_sweep_kernel<CW, 4, REAL>);
           default: return cudaErrorInvalidValue;
         }
       }

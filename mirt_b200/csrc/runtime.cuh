@@ -72,6 +72,10 @@ struct mirt_interp_plan {
   mirt::DMem sweep_teams;  // row-sweep spread: balanced team list (int4 per team)
   std::vector<int4> team_host;  // the same list on the host
   mirt::DMem team_order, team_next;  // row-sweep work queue: heaviest-first order, counter
+  mirt::DMem dense_of, dense_bin, patch;  // the sweeps' dense bins and their patches
+  mirt::DMem dense_chunk, dense_part0, patch_part;  // chunks of the patch sums
+  std::vector<int> dense_slice;           // first dense bin of each slice (+ total)
+  std::vector<int> dense_part0_host;      // first chunk of each dense bin (+ total)
   // TMA gather: first position of each block of the gather order, work items
   // (block, first position), the first item of each slice, fault flag
   mirt::DMem gblk, gitem, gfault;

@@ -504,7 +504,10 @@ def test_3d_line_sweep_matches_oracle(C):
     rng = np.random.default_rng(300 + C)
     K, J, L = [12, 10, 9], [6, 6, 6], [512, 512, 512]
     h = [mb.minmax_kb_table(k // 2, 6, k, 512) for k in K]
-    tms = [rng.uniform(-3, 3, (900, 3)), rng.uniform(-60, 60, (700, 3))]
+    # slice 0: a cluster of ~100 samples per bin (dense bins, summed into
+    # patches before the sweep) around sparse ones
+    tms = [np.concatenate([rng.uniform(-1.5, 1.5, (3000, 3)), rng.uniform(-3, 3, (900, 3))]),
+           rng.uniform(-60, 60, (700, 3))]
     moff = np.concatenate([[0], np.cumsum([len(t) for t in tms])])
     tm = np.concatenate(tms)
     plan = mb.InterpPlan(K, J, L, h, tm, C, slice_moff=moff)
@@ -541,7 +544,7 @@ def test_3d_line_sweep_real_tables_phase(order):
         h = [np.cos(np.linspace(-1.2, 1.2, 6 * 64 + 1)),
              np.exp(-np.linspace(-2, 2, 6 * 64 + 1) ** 2),
              np.cos(np.linspace(-0.9, 0.9, 6 * 64 + 1))]
-        tm = rng.uniform(-20, 20, (900, 3))
+        tm = np.concatenate([rng.uniform(-20, 20, (900, 3)), rng.uniform(2, 3, (500, 3))])
         ph = np.exp(1j * rng.uniform(-np.pi, np.pi, len(tm)))
         C = 8
         plan = mb.InterpPlan(K, J, L, h, tm, C, order=order, phase=ph)

@@ -189,6 +189,8 @@ def test_host_calls_pipelined_by_slice_chunks(C, nslice):
     counts = rng.integers(300, 1200, nslice)
     moff = np.concatenate([[0], np.cumsum(counts)])
     om = rng.uniform(-np.pi, np.pi, (int(moff[-1]), 2))
+    for s in (0, nslice - 1):                   # dense bins (patches) in the first and last chunk
+        om[moff[s]:moff[s] + 200] = rng.uniform(-0.05, 0.05, (200, 2))
     plan = mb.NufftPlan(om, N, (6, 6), K, n_shift=(16, 20), Ld=1024, ncol=C, slice_moff=moff)
     x = (rng.standard_normal(plan.image_shape) + 1j * rng.standard_normal(plan.image_shape))
     x = x.astype(np.complex64)
