@@ -240,6 +240,18 @@ int mirt_interp_plan_set_ownership(mirt_interp_plan *plan, int32_t own, void *st
  * it where it applies.  No reference counterpart. */
 int mirt_interp_plan_set_sweep(mirt_interp_plan *plan, int32_t segments, int32_t rows);
 
+/* Dense bins of the sweeps: bins holding at least 16 samples (the k-space
+ * centre of radial and kooshball trajectories) are summed, before the sweep,
+ * into patches of J^D taps x C (in chunks of 64 samples, added in a fixed
+ * order), and the sweep adds a bin's patch where it meets the bin instead of
+ * its samples, so that no warp runs through thousands of samples of one bin.
+ * 3D line sweeps always do; for the 2D row sweep on = 1 turns it on (one-row
+ * bands only; the default where dense bins exist) and 0 off.  The sums per
+ * grid point stay in a fixed order (deterministic), with the bins' samples
+ * summed first.  MIRT_ERR_ARG if the plan has no dense bins.  No reference
+ * counterpart. */
+int mirt_interp_plan_set_dense(mirt_interp_plan *plan, int32_t on);
+
 /* Gather over TMA-staged tiles and records (2D, J = 6, an even C >= 32,
  * K >= 13; the default there, and the autotuner times it against the plain
  * gather): the gather order groups samples by 8 x 8 blocks of first taps; for

@@ -551,6 +551,7 @@ void choose_config(mirt_interp_plan *P) {
   t.dense0 = 0;
   t.ndense = 0;
   t.dense_min = 0;
+  t.dense_on = 0;
   t.dense_chunk = nullptr;
   t.dense_part0 = nullptr;
   t.patch_part = nullptr;
@@ -961,9 +962,10 @@ int plan_finish(mirt_interp_plan *P, long long Mtot, const long long *moff, int 
   CK(query_gather_grid(a, P->lg));
   // 2D, J = 6, 32-coil chunks: the row sweep by default, one grid row per
   // team, balanced segments (about 64k teams, heaviest first)
-  if (sweep3_ok(a, P->t, P->ls.cw)) {
+  if (sweep_ok(a, P->t) || sweep3_ok(a, P->t, P->ls.cw)) {
     int rc3 = build_dense(P, kDenseBin, st);
     if (rc3) return rc3;
+    P->t.dense_on = P->t.dense_of ? 1 : 0;
   }
   if (sweep_ok(a, P->t) && P->ls.cw == 32) {
     int rc3 = sweep_buffer(P);
@@ -1002,6 +1004,7 @@ int set_spread_tiles(mirt_interp_plan *P, const int *T, cudaStream_t st) {
 struct SpreadCand {
   int T[MIRT_DMAX];
   int threads, padc, atomic, own, sweep, sweep_rows;
+  int dense = 0;  // 2D row sweep with dense-bin patches (one-row bands)
 };
 
 // spare columns the J = 6 row update can use (0 elsewhere)
@@ -1215,11 +1218,13 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
   // row sweep (no tiles): bands of 1, 2 or 4 rows, whole rows or uniform
   // segments of at least 32 columns, or balanced teams (sweep = -1)
   if (sweep_ok(a, P->t) && sweep_buffer(P) == MIRT_OK)
-    for (int rows : {1, 2, 4})
-      for (int nseg = (rows < 4 ? -1 : 1); nseg <= 16 && (nseg <= 1 || a.g.K[0] / nseg >= 32);
-           nseg = nseg < 0 ? 1 : nseg * 2)
-        cands.push_back(SpreadCand{{P->t.T[0], P->t.T[1], P->t.T[2]}, P->ls.threads, 0, 0, 0,
-                                   nseg, rows});
+    for (int dense : {0, 1})
+      for (int rows : {1, 2, 4})
+        for (int nseg = (rows < 4 ? -1 : 1); nseg <= 16 && (nseg <= 1 || a.g.K[0] / nseg >= 32);
+             nseg = nseg < 0 ? 1 : nseg * 2)
+          if (!dense || (rows == 1 && P->t.dense_of))
+            cands.push_back(SpreadCand{{P->t.T[0], P->t.T[1], P->t.T[2]}, P->ls.threads, 0, 0, 0,
+                                       nseg, rows, dense});
   // 3D line sweep: 1, 2, 4 or 8 segments per line block
   if (sweep3_ok(a, P->t, cw) && sweep_buffer(P) == MIRT_OK)
     for (int nseg : {1, 2, 4, 8})
@@ -1232,6 +1237,7 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
     P->t.own = c.own;
     P->t.sweep = c.sweep;
     P->t.sweep_rows = c.sweep_rows;
+    P->t.dense_on = c.dense;
     if (c.sweep < 0 && built_rows != c.sweep_rows) {
       int rc = build_sweep_teams(P, c.sweep_rows, 65536, st);
       if (rc) return rc;
@@ -1256,9 +1262,9 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
     if (autotune_log())
       std::fprintf(stderr,
                    "mirt autotune spread: tile %dx%dx%d threads %d padc %d atomic %d own %d "
-                   "sweep %d rows %d: %.3f ms\n",
+                   "sweep %d rows %d dense %d: %.3f ms\n",
                    c.T[0], c.T[1], c.T[2], c.threads, c.padc, c.atomic, c.own, c.sweep,
-                   c.sweep_rows, ms);
+                   c.sweep_rows, c.dense, ms);
     if (ms < best_ms) {
       best_ms = ms;
       best = c;
@@ -1268,6 +1274,7 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
     P->t.own = best.own;
     P->t.sweep = best.sweep;
     P->t.sweep_rows = best.sweep_rows;
+    P->t.dense_on = best.dense;
     if (best.sweep < 0 && built_rows != best.sweep_rows) {
       int rc = build_sweep_teams(P, best.sweep_rows, 65536, st);
       if (rc) return rc;
@@ -1435,6 +1442,13 @@ int mirt_interp_plan_set_sweep(mirt_interp_plan *P, int32_t segments, int32_t ro
     P->t.own = 0;
     P->ls.atomic = 0;
   }
+  return MIRT_OK;
+}
+
+int mirt_interp_plan_set_dense(mirt_interp_plan *P, int32_t on) {
+  if (!P) return fail(MIRT_ERR_ARG, "plan is NULL");
+  if (on && !P->t.dense_of) return fail(MIRT_ERR_ARG, "the plan has no dense bins");
+  P->t.dense_on = on ? 1 : 0;
   return MIRT_OK;
 }
 
@@ -2495,6 +2509,8 @@ int mirt_nufft_autotune(mirt_nufft *p, void *stream) {
   return mirt_interp_plan_autotune(p->ip, stream);
 }
 
+static bool a3d(const mirt_nufft *p) { return p->gg.D == 3; }
+
 int mirt_nufft_config(mirt_nufft *p, int32_t *out, int32_t n) {
   if (!p || !out) return fail(MIRT_ERR_ARG, "NULL argument");
   const Tiling &t = p->ip->t;
@@ -2504,7 +2520,8 @@ int mirt_nufft_config(mirt_nufft *p, int32_t *out, int32_t n) {
   if (t.sweep != 0) {
     // ordering pass, dense-bin patches (chunk sums, per-bin sums), sweep (and a
     // memset of the queue counters)
-    spread = 2 + (t.ndense > 0 ? 2 : 0);
+    const bool dense = t.ndense > 0 && (a3d(p) || (t.dense_on && t.sweep_rows == 1));
+    spread = 2 + (dense ? 2 : 0);
   } else if (t.own) {
     spread = 1;  // the clearing memset, then per colour a launch and a reduction
     for (int c = 0; c < 4; c++)

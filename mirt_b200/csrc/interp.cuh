@@ -88,6 +88,7 @@ struct Tiling {
   float2 *patch;
   int dense0, ndense;
   int dense_min;         // samples that make a bin dense
+  int dense_on;          // 2D row sweep: use the patches (one-row bands only)
   // the patches are summed in chunks of at most 64 samples: chunk i =
   // dense_chunk[i] = (dense bin, first position, end position, part index);
   // dense bin d's chunk sums are patch_part[dense_part0[d] .. dense_part0[d+1]);

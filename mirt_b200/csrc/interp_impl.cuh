@@ -697,8 +697,9 @@ __global__ void __launch_bounds__(256) sweep_order_kernel(InterpArgs a, const fl
   }
 }
 
-// The sweep of one team (see spread_sweep_kernel).
-template <int CW, int R, bool REAL>
+// The sweep of one team (see spread_sweep_kernel).  DENSE: bins with at least
+// dense_min samples add their patches (dense_part/reduce_kernel) instead.
+template <int CW, int R, bool REAL, bool DENSE>
 __device__ __forceinline__ void sweep_team(const InterpArgs &a, const Tiling &t,
                                            const int *__restrict__ bin_start,
                                            const float2 *__restrict__ fs,
@@ -758,6 +759,29 @@ __device__ __forceinline__ void sweep_team(const InterpArgs &a, const Tiling &t,
 #pragma unroll
     for (int q = 0; q < NQ; q++) {
       const int pe = end[q];
+      if constexpr (DENSE) {
+        if (pe - beg[q] >= t.dense_min) {
+          // a dense bin: the sums of its samples, from its patch
+          const int dn = __ldg(t.dense_of + (long long)slice * t.nbins + row[q] + xw);
+          if (on) {
+#pragma unroll
+            for (int r = 0; r < R; r++) {
+              const int j2 = r - q + 5;
+              if (j2 >= 0 && j2 < 6) {
+                const float2 *pp = t.patch + ((long long)dn * 36 + j2 * 6) * C + c;
+#pragma unroll
+                for (int j = 0; j < 6; j++) {
+                  const float2 v = __ldg(pp + (long long)j * C);
+                  acc[r][j].x += v.x;
+                  acc[r][j].y += v.y;
+                }
+              }
+            }
+          }
+          beg[q] = pe;
+          continue;
+        }
+      }
       for (int p = beg[q]; p < pe; p++) {
         const float2 f = on ? __ldg(fs + (long long)p * C + c) : make_float2(0.f, 0.f);
         const float2 *Ws = a.W + (long long)p * 12;
@@ -800,7 +824,7 @@ __device__ __forceinline__ void sweep_team(const InterpArgs &a, const Tiling &t,
 // plan's work queue (heaviest teams first) until the queue is empty, so warps
 // do not sit idle behind a heavy team of their block.  Each team's sums are
 // independent of which warp runs it: deterministic.
-template <int CW, int R, bool REAL>
+template <int CW, int R, bool REAL, bool DENSE>
 __global__ void __launch_bounds__(256) spread_sweep_kernel(InterpArgs a, Tiling t,
                                                            const int *__restrict__ bin_start,
                                                            const float2 *__restrict__ fs,
@@ -818,7 +842,7 @@ __global__ void __launch_bounds__(256) spread_sweep_kernel(InterpArgs a, Tiling 
     const long long qi = (long long)base + lane / CW;
     if (qi < nteam) {
       const long long team = t.team_order ? (long long)__ldg(t.team_order + qi) : qi;
-      sweep_team<CW, R, REAL>(a, t, bin_start, fs, ck, team);
+      sweep_team<CW, R, REAL, DENSE>(a, t, bin_start, fs, ck, team);
     }
   }
 }
@@ -1516,10 +1540,16 @@ cudaError_t run(Req &r) {
           kern<<<dim3((unsigned)nb, nchunk), 256, 0, r.st>>>(a, t, r.bin_start, fs, r.out);
           return cudaGetLastError();
         };
+        if (t.dense_on && t.dense_of && t.sweep_rows == 1) {
+          // one-row bands with dense-bin patches
+          cudaError_t e = launch_dense_patches<2, REAL>(a, t, t.sorted, r.st);
+          if (e != cudaSuccess) return e;
+          return go(spread_sweep_kernel<CW, 1, REAL, true>);
+        }
         switch (t.sweep_rows) {
-          case 1: return go(spread_sweep_kernel<CW, 1, REAL>);
-          case 2: return go(spread_sweep_kernel<CW, 2, REAL>);
-          case 4: return go(spread_sweep_kernel<CW, 4, REAL>);
+          case 1: return go(spread_sweep_kernel<CW, 1, REAL, false>);
+          case 2: return go(spread_sweep_kernel<CW, 2, REAL, false>);
+          case 4: return go(spread_sweep_kernel<CW, 4, REAL, false>);
           default: return cudaErrorInvalidValue;
         }
       }

@@ -187,6 +187,10 @@ class InterpPlan:
         check(self.lib.mirt_interp_plan_fault(self.handle, C.byref(f)))
         return f.value
 
+    def set_dense(self, on=True):
+        """Dense-bin patches in the 2D row sweep (see mirt_interp_plan_set_dense)."""
+        check(self.lib.mirt_interp_plan_set_dense(self.handle, int(bool(on))))
+
     def set_fault_test(self, on=True):
         """Test hook of the TMA gather's bounded waits (see
         mirt_interp_plan_set_fault_test): no copies, every wait runs out."""
@@ -287,6 +291,11 @@ class NufftPlan:
         check(self.lib.mirt_interp_plan_set_sweep(
             self.lib.mirt_nufft_interp_plan(self.handle), int(segments), int(rows)))
         return self.config()
+
+    def set_dense(self, on=True):
+        """See InterpPlan.set_dense."""
+        check(self.lib.mirt_interp_plan_set_dense(self.lib.mirt_nufft_interp_plan(self.handle),
+                                                  int(bool(on))))
 
     def set_gather(self, tma=True):
         """See InterpPlan.set_gather."""

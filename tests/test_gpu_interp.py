@@ -375,6 +375,20 @@ def test_sweep_spread_matches_oracle(C):
     fm_d = torch.from_numpy(fm.astype(np.complex64)).cuda()
     cfg = plan.config()                        # the default for 32-coil chunks: balanced teams
     assert (cfg["spread_sweep"], cfg["spread_sweep_rows"]) == ((-1, 1) if C >= 32 else (0, 1))
+    # one-row bands with dense-bin patches (slice 1 is dense): oracle, and the
+    # same bits for every segmentation
+    plan.set_dense(True)
+    dense_first = None
+    for nseg in (-1, 1, 5, 96):
+        plan.set_sweep(nseg, 1)
+        out = plan.adjoint(fm_d).cpu().numpy()
+        for s in range(3):
+            got = np.transpose(out[s], (1, 0, 2)).reshape(-1, C, order="F")
+            assert rel_l2(got, oracle.interp_adj(fm[moff[s]:moff[s + 1]], h, J, L, tms[s], K, 0,
+                                                 impl=ref_impl())) <= ADJ_TOL, (nseg, s)
+        dense_first = out if dense_first is None else dense_first
+        assert np.array_equal(out, dense_first), nseg
+    plan.set_dense(False)
     plan.set_sweep(0)
     tiled = plan.adjoint(fm_d).cpu().numpy()
     refs = [oracle.interp_adj(fm[moff[s]:moff[s + 1]], h, J, L, tms[s], K, 0, impl=ref_impl())
