@@ -155,16 +155,19 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def traffic_from_profiles(call, workload, variant):
-    """DRAM bytes of one gather or spread call (the sum over its kernels) recorded
-    from an ncu capture (profiles/traffic.json), for the plan's gather / spread
-    variant."""
+def traffic_from_profiles(workload, kernel):
+    """(DRAM bytes of one call, where they come from) for the dominant kernel
+    configuration, looked up in profiles/traffic.json (ncu captures, stated
+    there); (None, None) when that configuration was not captured."""
     try:
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
             t = json.load(f)
-        return t.get(workload, {}).get(f"{call}_{variant}")
-    except (OSError, ValueError):
-        return None
+        e = t.get(workload, {}).get(kernel)
+        if e:
+            return e["bytes"], "profiles/traffic.json: " + e["source"]
+    except (OSError, ValueError, KeyError):
+        pass
+    return None, None
 
 
 # ---------------------------------------------------------------------------
@@ -337,6 +340,9 @@ def run_gpu(args, w):
         tuned = plan.set_sweep(-1, 1)        # the plan's default: balanced teams of one row
     elif args.spread == "tiled" and tuned.get("spread_sweep", 0) != 0:
         tuned = plan.set_sweep(0)
+    if args.sweep_config:                       # a fixed row sweep (for captures of one config)
+        seg, rows = (int(v) for v in args.sweep_config.split(","))
+        tuned = plan.set_sweep(seg, rows)
     t_tune = time.perf_counter() - t0
     img_np = make_images(w, np.random.default_rng(99 + rank))
     if img_np.shape[0] != plan.nslice:
@@ -427,14 +433,18 @@ def run_gpu(args, w):
     achieved = B / tdom / 1e9
     variant = {"spread": "sweep" if tuned.get("spread_sweep", 0) != 0 else "tiled",
                "gather": "tma" if tuned.get("gather_tma", 0) else "plain"}
-    sweep_kernel = ("spread_list_kernel" if tuned.get("spread_sweep", 0) == -1
-                    else "sweep_order_kernel + spread_sweep_kernel")
+    if D == 3:
+        sweep_kernel = "spread_sweep3_kernel"
+    else:
+        sweep_kernel = (f"sweep_order_kernel + spread_sweep_kernel "
+                        f"rows={tuned.get('spread_sweep_rows', 1)}")
     kernels = {"gather": ("gather_tma_kernel" if variant["gather"] == "tma" else "gather_kernel"),
                "spread": (sweep_kernel if variant["spread"] == "sweep"
                           else "spread_kernel (+ spread_reduce_kernel)")}
+    traffic, traffic_src = traffic_from_profiles(args.workload, kernels[dom])
     roof = {"bound": "hbm", "kernel": kernels[dom], "achieved": achieved, "peak": peak,
             "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
-            "traffic": traffic_from_profiles(dom, args.workload, variant[dom]),
+            "traffic": traffic, "traffic_source": traffic_src,
             "algorithmic_bytes": B,
             "gather": {"ms": 1e3 * t_gather, "GBps": B / t_gather / 1e9,
                        "frac": B / t_gather / 1e9 / peak},
@@ -666,6 +676,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--sweep-config", default="",
+                    help="SEGMENTS,ROWS: fix the row sweep after autotuning (for captures)")
     ap.add_argument("--no-graph", action="store_true",
                     help="time eager steps instead of a CUDA-graph replay (for profiling)")
     ap.add_argument("--spread", default="auto", choices=["auto", "sweep", "tiled"],
