@@ -193,12 +193,13 @@ int mirt_interp_plan_adjoint(mirt_interp_plan *plan, const void *fm, void *ck, v
  * bitwise deterministic for any choice. */
 int mirt_interp_plan_autotune(mirt_interp_plan *plan, void *stream);
 
-/* Current launch configuration: up to 21 values
+/* Current launch configuration: up to 23 values
  * {T1, T2, T3, spread threads, spread heavy-first order, coil lanes,
  *  gather threads, (unused), gather CTAs, B1, B2, B3, split chunk,
  *  spread tasks, spare tile columns, partial-tile reductions,
  *  spread shared-tile atomics, ownership spread, row-sweep segments (0: off,
- *  -1: balanced team list), row-sweep rows per band, TMA gather}. */
+ *  -1: balanced team list), row-sweep rows per band, TMA gather,
+ *  row-sweep dense-bin patches, staged row sweep mode}. */
 int mirt_interp_plan_config(mirt_interp_plan *plan, int32_t *out, int32_t n);
 
 /* Adjoint accumulation order.  deterministic = 1 (the default): every
@@ -251,6 +252,17 @@ int mirt_interp_plan_set_sweep(mirt_interp_plan *plan, int32_t segments, int32_t
  * summed first.  MIRT_ERR_ARG if the plan has no dense bins.  No reference
  * counterpart. */
 int mirt_interp_plan_set_dense(mirt_interp_plan *plan, int32_t on);
+
+/* The 2D row sweep with 32-coil lanes, staged per bin column: the warp lists
+ * the samples of the column's bin rows, copies their tap records and sample
+ * rows into shared memory (cp.async) and sums them from there, the sums in the
+ * order of the unstaged sweep (the same bits).  mode 0: unstaged; 1: staged,
+ * after the pass that copies the samples into plan order; 2: staged, reading
+ * the caller's samples through the sort permutation (no ordering pass).  Not
+ * with dense-bin patches (set_dense 0 where both would apply); the autotuner
+ * times 1 and 2 beside the unstaged sweep.  MIRT_ERR_ARG for other modes or
+ * when the plan's lanes are not 32 coils wide.  No reference counterpart. */
+int mirt_interp_plan_set_staged(mirt_interp_plan *plan, int32_t mode);
 
 /* Gather over TMA-staged tiles and records (2D, J = 6, an even C >= 32,
  * K >= 13; the default there, and the autotuner times it against the plain

@@ -67,6 +67,7 @@ _SIGS = {
     "mirt_interp_plan_fault": ([_vp, _i32p], C.c_int),
     "mirt_interp_plan_set_fault_test": ([_vp, _i32], C.c_int),
     "mirt_interp_plan_set_dense": ([_vp, _i32], C.c_int),
+    "mirt_interp_plan_set_staged": ([_vp, _i32], C.c_int),
     "mirt_dcf_pipe": ([_vp, _vp, _i32, _i32, C.c_double, _dp, _i32p, _dp, _vp], C.c_int),
     "mirt_dcf_jackson": ([_vp, _vp, _vp], C.c_int),
     "mirt_dcf_scale": ([_vp, _vp, _dp, _vp], C.c_int),

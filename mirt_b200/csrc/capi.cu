@@ -1005,6 +1005,7 @@ struct SpreadCand {
   int T[MIRT_DMAX];
   int threads, padc, atomic, own, sweep, sweep_rows;
   int dense = 0;  // 2D row sweep with dense-bin patches (one-row bands)
+  int staged = 0;  // 2D row sweep staged per column (1), reading the caller's samples (2)
 };
 
 // spare columns the J = 6 row update can use (0 elsewhere)
@@ -1223,8 +1224,10 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
         for (int nseg = (rows < 4 ? -1 : 1); nseg <= 16 && (nseg <= 1 || a.g.K[0] / nseg >= 32);
              nseg = nseg < 0 ? 1 : nseg * 2)
           if (!dense || (rows == 1 && P->t.dense_of))
-            cands.push_back(SpreadCand{{P->t.T[0], P->t.T[1], P->t.T[2]}, P->ls.threads, 0, 0, 0,
-                                       nseg, rows, dense});
+            for (int staged : {0, 1, 2})
+              if (!staged || (cw == 32 && !dense))
+                cands.push_back(SpreadCand{{P->t.T[0], P->t.T[1], P->t.T[2]}, P->ls.threads, 0,
+                                           0, 0, nseg, rows, dense, staged});
   // 3D line sweep: 1, 2, 4 or 8 segments per line block
   if (sweep3_ok(a, P->t, cw) && sweep_buffer(P) == MIRT_OK)
     for (int nseg : {1, 2, 4, 8})
@@ -1238,6 +1241,7 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
     P->t.sweep = c.sweep;
     P->t.sweep_rows = c.sweep_rows;
     P->t.dense_on = c.dense;
+    P->t.sweep_staged = c.staged;
     if (c.sweep < 0 && built_rows != c.sweep_rows) {
       int rc = build_sweep_teams(P, c.sweep_rows, 65536, st);
       if (rc) return rc;
@@ -1262,9 +1266,9 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
     if (autotune_log())
       std::fprintf(stderr,
                    "mirt autotune spread: tile %dx%dx%d threads %d padc %d atomic %d own %d "
-                   "sweep %d rows %d dense %d: %.3f ms\n",
+                   "sweep %d rows %d dense %d staged %d: %.3f ms\n",
                    c.T[0], c.T[1], c.T[2], c.threads, c.padc, c.atomic, c.own, c.sweep,
-                   c.sweep_rows, c.dense, ms);
+                   c.sweep_rows, c.dense, c.staged, ms);
     if (ms < best_ms) {
       best_ms = ms;
       best = c;
@@ -1275,6 +1279,7 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
     P->t.sweep = best.sweep;
     P->t.sweep_rows = best.sweep_rows;
     P->t.dense_on = best.dense;
+    P->t.sweep_staged = best.staged;
     if (best.sweep < 0 && built_rows != best.sweep_rows) {
       int rc = build_sweep_teams(P, best.sweep_rows, 65536, st);
       if (rc) return rc;
@@ -1367,11 +1372,12 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
 
 int mirt_interp_plan_config(mirt_interp_plan *P, int32_t *out, int32_t n) {
   if (!P || !out) return fail(MIRT_ERR_ARG, "NULL argument");
-  const int32_t v[21] = {P->t.T[0], P->t.T[1], P->t.T[2], P->ls.threads, P->heavy_first, P->ls.cw,
+  const int32_t v[23] = {P->t.T[0], P->t.T[1], P->t.T[2], P->ls.threads, P->heavy_first, P->ls.cw,
                          P->lg.threads, P->lg.sb, P->lg.grid, P->t.B[0], P->t.B[1], P->t.B[2],
                          P->split_chunk, P->t.ntask, P->t.padc, P->t.nred, P->ls.atomic,
-                         P->t.own, P->t.sweep, P->t.sweep_rows, P->gtma};
-  for (int i = 0; i < n && i < 21; i++) out[i] = v[i];
+                         P->t.own, P->t.sweep, P->t.sweep_rows, P->gtma, P->t.dense_on,
+                         P->t.sweep_staged};
+  for (int i = 0; i < n && i < 23; i++) out[i] = v[i];
   return MIRT_OK;
 }
 
@@ -1449,6 +1455,15 @@ int mirt_interp_plan_set_dense(mirt_interp_plan *P, int32_t on) {
   if (!P) return fail(MIRT_ERR_ARG, "plan is NULL");
   if (on && !P->t.dense_of) return fail(MIRT_ERR_ARG, "the plan has no dense bins");
   P->t.dense_on = on ? 1 : 0;
+  return MIRT_OK;
+}
+
+int mirt_interp_plan_set_staged(mirt_interp_plan *P, int32_t mode) {
+  if (!P) return fail(MIRT_ERR_ARG, "plan is NULL");
+  if (mode < 0 || mode > 2) return fail(MIRT_ERR_ARG, "staged mode must be 0, 1 or 2");
+  if (mode && P->ls.cw != 32)
+    return fail(MIRT_ERR_ARG, "the staged row sweep needs 32-coil lanes (C >= 32)");
+  P->t.sweep_staged = mode;
   return MIRT_OK;
 }
 
@@ -2522,6 +2537,10 @@ int mirt_nufft_config(mirt_nufft *p, int32_t *out, int32_t n) {
     // memset of the queue counters)
     const bool dense = t.ndense > 0 && (a3d(p) || (t.dense_on && t.sweep_rows == 1));
     spread = 2 + (dense ? 2 : 0);
+    // the staged 2D sweep reading the caller's samples has no ordering pass
+    const bool staged2 = !a3d(p) && t.sweep_staged == 2 && p->ip->ls.cw == 32 &&
+                         !(t.dense_on && t.dense_of && t.sweep_rows == 1);
+    if (staged2) spread = 1;
   } else if (t.own) {
     spread = 1;  // the clearing memset, then per colour a launch and a reduction
     for (int c = 0; c < 4; c++)

@@ -89,6 +89,10 @@ struct Tiling {
   int dense0, ndense;
   int dense_min;         // samples that make a bin dense
   int dense_on;          // 2D row sweep: use the patches (one-row bands only)
+  // 2D row sweep with 32-coil chunks: 0 the classic kernel; 1 staged per column
+  // (spread_sweep2s_kernel) after the ordering pass; 2 staged, reading the
+  // caller's samples directly (no ordering pass)
+  int sweep_staged;
   // the patches are summed in chunks of at most 64 samples: chunk i =
   // dense_chunk[i] = (dense bin, first position, end position, part index);
   // dense bin d's chunk sums are patch_part[dense_part0[d] .. dense_part0[d+1]);

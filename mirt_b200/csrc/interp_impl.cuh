@@ -1184,6 +1184,185 @@ __global__ void __launch_bounds__(256) spread_sweep3_kernel(InterpArgs a, Tiling
   }
 }
 
+// ------------------------------------------------------------------------
+// 2D row sweep with per-column staging (J = 6, one-point bins, 32-coil chunks)
+// ------------------------------------------------------------------------
+// The team of spread_sweep_kernel (one warp, lane = coil; R grid rows, a
+// segment of their columns), with the bin columns' samples staged as in the 3D
+// line sweep: lane q < R + 5 keeps the pointer of bin row q and loads the next
+// column's while the current one is summed; per column the warp lists the
+// samples (bin rows in order, samples in sort order), copies their tap records
+// and the lanes' sample values into its shared-memory stage with cp.async, and
+// adds them from there.  DIRECT: the sample rows are read in the caller's order
+// through perm and times conj(phase) here, so the ordering pass is not needed.
+// Same operations in the same order as spread_sweep_kernel: the same bits.
+constexpr int SW2_CAP = 16;
+template <bool DIRECT>
+constexpr int sweep2_warp_bytes() {
+  return 3 * SW2_CAP * 4 + SW2_CAP * 4 + SW2_CAP * 8 + SW2_CAP * 12 * 8 + SW2_CAP * 32 * 8;
+}
+
+template <int R, bool REAL, bool DIRECT>
+__device__ __forceinline__ void sweep2s_team(const InterpArgs &a, const Tiling &t,
+                                             const int *__restrict__ bin_start,
+                                             const float2 *__restrict__ fs,
+                                             float2 *__restrict__ ck, long long team,
+                                             unsigned char *wsm) {
+  constexpr unsigned FULLM = 0xffffffffu;
+  constexpr int NQ = R + 5;
+  int *spos = reinterpret_cast<int *>(wsm);
+  int *sq = spos + SW2_CAP;
+  int *smi = sq + SW2_CAP;
+  float2 *sph = reinterpret_cast<float2 *>(wsm + 4 * SW2_CAP * 4);
+  float2 *srec = sph + SW2_CAP;
+  float2 *sf = srec + SW2_CAP * 12;
+  const int K1 = a.g.K[0], K2 = a.g.K[1];
+  int slice, y0, x0, x1;
+  if (t.sweep < 0) {
+    const int4 tk = t.sweep_team[team];
+    slice = tk.x;
+    y0 = tk.y;
+    x0 = tk.z;
+    x1 = tk.w;
+  } else {
+    const int nseg = t.sweep;
+    const int nband = (K2 + R - 1) / R;
+    const int seg = (int)(team % nseg);
+    const long long bandid = team / nseg;
+    const int sl = (int)(bandid / nband);
+    y0 = (int)(bandid - (long long)sl * nband) * R;
+    slice = t.slice0 + sl;
+    const int sw = (K1 + nseg - 1) / nseg;
+    x0 = seg * sw;
+    x1 = min(K1, x0 + sw);
+  }
+  if (x0 >= x1) return;
+  const int lane = threadIdx.x & 31;
+  const int C = a.C;
+  const int c0 = blockIdx.y * 32;
+  const bool on = c0 + lane < C;
+  const int *bs = bin_start + (long long)slice * t.nbins;
+  long long rowb = -1;
+  if (lane < NQ) {
+    int b = (y0 - 5 + lane) % K2;
+    if (b < 0) b += K2;
+    rowb = (long long)b * K1;
+  }
+  const int xs = x0 - 5;
+  auto wrapx = [&](int x) { return x < 0 ? x + K1 : x; };
+  int beg = rowb >= 0 ? __ldg(bs + rowb + wrapx(xs)) : 0;
+  int en = rowb >= 0 ? __ldg(bs + rowb + wrapx(xs) + 1) : beg;
+  int rn = 0;
+  float2 acc[R][6];
+#pragma unroll
+  for (int r = 0; r < R; r++)
+#pragma unroll
+    for (int j = 0; j < 6; j++) acc[r][j] = make_float2(0.f, 0.f);
+  float2 *out = ck + (long long)slice * a.grid_elems + (long long)y0 * K1 * C + c0 + lane;
+  // lane's first chunk of the records' 16-byte copies: (visit, chunk) = (lane / 6, lane % 6)
+  const int cv0 = lane / 6, ck0 = lane - 6 * (lane / 6);
+  for (int xb = xs; xb < x1; xb++) {
+    const int end = en;
+    if (xb == 0 && xs < 0) beg = rn;
+    if (xb + 1 < x1 && rowb >= 0) {
+      en = __ldg(bs + rowb + wrapx(xb + 1) + 1);
+      if (xb + 1 == 0) rn = __ldg(bs + rowb);
+    }
+    const int n = end - beg;
+    int inc = n;
+#pragma unroll
+    for (int o = 1; o < 16; o <<= 1) {
+      const int u = __shfl_up_sync(FULLM, inc, o);
+      if (lane >= o) inc += u;
+    }
+    const int V = __shfl_sync(FULLM, inc, 15);
+    const int ex = inc - n;
+    for (int vb = 0; vb < V; vb += SW2_CAP) {
+      const int nb = min(SW2_CAP, V - vb);
+      for (int k = max(0, vb - ex); k < n && ex + k < vb + SW2_CAP; k++) {
+        spos[ex + k - vb] = beg + k;
+        sq[ex + k - vb] = lane;
+      }
+      __syncwarp();
+      if (DIRECT) {
+        if (lane < nb) {
+          const int p = spos[lane];
+          smi[lane] = a.perm ? __ldg(a.perm + p) : p;
+          sph[lane] = a.phase ? __ldg(a.phase + p) : make_float2(1.f, 0.f);
+        }
+        __syncwarp();
+      }
+      for (int v = cv0, kk = ck0; v < nb;) {
+        cp_async16(srec + v * 12 + 2 * kk, a.W + (long long)spos[v] * 12 + 2 * kk);
+        v += 5;
+        kk += 2;
+        if (kk >= 6) {
+          kk -= 6;
+          v++;
+        }
+      }
+      for (int v = 0; v < nb; v++) {
+        const long long row = DIRECT ? (long long)smi[v] : (long long)spos[v];
+        if (on)
+          cp_async8(sf + v * 32 + lane, fs + row * C + c0 + lane);
+        else
+          sf[v * 32 + lane] = make_float2(0.f, 0.f);
+      }
+      cp_async_wait_all();
+      __syncwarp();
+      for (int v = 0; v < nb; v++) {
+        const int q = sq[v];
+        float2 f = sf[v * 32 + lane];
+        if (DIRECT && a.phase) f = cmulc(sph[v], f);
+        const float2 *rv = srec + v * 12;
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+          const int j2 = r - q + 5;
+          if (j2 >= 0 && j2 < 6) {
+            const float2 vv = cw_mul<REAL>(rv[6 + j2], f);
+#pragma unroll
+            for (int j = 0; j < 6; j++) cmac_conj<REAL>(acc[r][j], rv[j], vv);
+          }
+        }
+      }
+      __syncwarp();
+    }
+    beg = end;
+    if (xb >= x0 && on) {
+#pragma unroll
+      for (int r = 0; r < R; r++)
+        if (y0 + r < K2) out[((long long)r * K1 + xb) * C] = acc[r][0];
+    }
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+#pragma unroll
+      for (int j = 0; j < 5; j++) acc[r][j] = acc[r][j + 1];
+      acc[r][5] = make_float2(0.f, 0.f);
+    }
+  }
+}
+
+template <int R, bool REAL, bool DIRECT>
+__global__ void __launch_bounds__(256) spread_sweep2s_kernel(InterpArgs a, Tiling t,
+                                                             const int *__restrict__ bin_start,
+                                                             const float2 *__restrict__ fs,
+                                                             float2 *__restrict__ ck) {
+  extern __shared__ __align__(16) unsigned char sm2[];
+  const int lane = threadIdx.x & 31;
+  unsigned char *wsm = sm2 + (threadIdx.x >> 5) * sweep2_warp_bytes<DIRECT>();
+  const long long nteam =
+      t.sweep < 0 ? (long long)t.nteams
+                  : (long long)t.nslice * ((a.g.K[1] + R - 1) / R) * t.sweep;
+  for (;;) {
+    int qi = 0;
+    if (lane == 0) qi = atomicAdd(t.team_next + blockIdx.y, 1);
+    qi = __shfl_sync(0xffffffffu, qi, 0);
+    if (qi >= nteam) break;
+    const long long team = t.team_order ? (long long)__ldg(t.team_order + qi) : qi;
+    sweep2s_team<R, REAL, DIRECT>(a, t, bin_start, fs, ck, team, wsm);
+  }
+}
+
 // Sum the partial tiles of each split heavy tile, in slot order, into the grid.
 template <int D, int CW>
 __global__ void __launch_bounds__(256) spread_reduce_kernel(InterpArgs a, Tiling t,
@@ -1511,6 +1690,52 @@ cudaError_t run(Req &r) {
         const long long thr = teams * CW;
         const unsigned nchunk = (unsigned)((a.C + CW - 1) / CW);
         if (thr == 0) return cudaSuccess;
+        if (t.sweep_staged && CW == 32 && !(t.dense_on && t.dense_of && t.sweep_rows == 1)) {
+          // staged sweep: reads the plan-order copy (1) or the caller's samples (2)
+          const bool direct = t.sweep_staged == 2;
+          if (!direct) {
+            if (!t.sorted) return cudaErrorInvalidValue;
+            const long long p0 = t.npos < 0 ? 0 : t.pos0;
+            const long long np = t.npos < 0 ? a.Mtot : t.npos;
+            const long long n = np * (long long)a.C;
+            long long nb = (n + 255) / 256;
+            if (nb > 148 * 16) nb = 148 * 16;
+            if (n > 0)
+              sweep_order_kernel<CW><<<(unsigned)nb, 256, 0, r.st>>>(a, r.in, t.sorted, p0, np);
+            cudaError_t e = cudaGetLastError();
+            if (e != cudaSuccess) return e;
+          }
+          if (!t.team_next) return cudaErrorInvalidValue;
+          const float2 *fsrc = direct ? r.in : t.sorted;
+          auto go2 = [&](auto kern, size_t smem) -> cudaError_t {
+            int per_sm = 0, dev = 0, nsm = 0;
+            cudaError_t e =
+                cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return e;
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, smem);
+            if (e != cudaSuccess) return e;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+            long long nb = (long long)nsm * (per_sm > 0 ? per_sm : 1);
+            const long long need = (teams + 7) / 8;
+            if (nb > need) nb = need;
+            e = cudaMemsetAsync(t.team_next, 0, nchunk * sizeof(int), r.st);
+            if (e != cudaSuccess) return e;
+            kern<<<dim3((unsigned)nb, nchunk), 256, smem, r.st>>>(a, t, r.bin_start, fsrc, r.out);
+            return cudaGetLastError();
+          };
+          const size_t smd = 8 * (size_t)sweep2_warp_bytes<true>();
+          const size_t sms = 8 * (size_t)sweep2_warp_bytes<false>();
+          switch (t.sweep_rows) {
+            case 1: return direct ? go2(spread_sweep2s_kernel<1, REAL, true>, smd)
+                                  : go2(spread_sweep2s_kernel<1, REAL, false>, sms);
+            case 2: return direct ? go2(spread_sweep2s_kernel<2, REAL, true>, smd)
+                                  : go2(spread_sweep2s_kernel<2, REAL, false>, sms);
+            case 4: return direct ? go2(spread_sweep2s_kernel<4, REAL, true>, smd)
+                                  : go2(spread_sweep2s_kernel<4, REAL, false>, sms);
+            default: return cudaErrorInvalidValue;
+          }
+        }
         if (!t.sorted) return cudaErrorInvalidValue;
         {
           const long long p0 = t.npos < 0 ? 0 : t.pos0;

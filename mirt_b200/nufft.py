@@ -66,14 +66,15 @@ def minmax_kb_scale(N: int, J: int, K: int) -> np.ndarray:
 
 
 def _plan_config(lib, handle) -> dict:
-    v = (C.c_int32 * 21)()
-    check(lib.mirt_interp_plan_config(handle, v, 21))
+    v = (C.c_int32 * 23)()
+    check(lib.mirt_interp_plan_config(handle, v, 23))
     return {"spread_tile": [v[0], v[1], v[2]], "spread_threads": v[3], "spread_heavy_first": v[4],
             "coil_lanes": v[5], "gather_threads": v[6],
             "gather_ctas": v[8], "sort_bin": [v[9], v[10], v[11]], "split_chunk": v[12],
             "spread_tasks": v[13], "spread_padc": v[14], "spread_reductions": v[15],
             "spread_atomic": v[16], "spread_own": v[17], "spread_sweep": v[18],
-            "spread_sweep_rows": v[19], "gather_tma": v[20]}
+            "spread_sweep_rows": v[19], "gather_tma": v[20], "spread_dense": v[21],
+            "spread_staged": v[22]}
 
 
 class InterpPlan:
@@ -191,6 +192,11 @@ class InterpPlan:
         """Dense-bin patches in the 2D row sweep (see mirt_interp_plan_set_dense)."""
         check(self.lib.mirt_interp_plan_set_dense(self.handle, int(bool(on))))
 
+    def set_staged(self, mode=1):
+        """2D row sweep staged per bin column: 0 off, 1 after the ordering
+        pass, 2 reading the caller's samples (see mirt_interp_plan_set_staged)."""
+        check(self.lib.mirt_interp_plan_set_staged(self.handle, int(mode)))
+
     def set_fault_test(self, on=True):
         """Test hook of the TMA gather's bounded waits (see
         mirt_interp_plan_set_fault_test): no copies, every wait runs out."""
@@ -296,6 +302,11 @@ class NufftPlan:
         """See InterpPlan.set_dense."""
         check(self.lib.mirt_interp_plan_set_dense(self.lib.mirt_nufft_interp_plan(self.handle),
                                                   int(bool(on))))
+
+    def set_staged(self, mode=1):
+        """See InterpPlan.set_staged."""
+        check(self.lib.mirt_interp_plan_set_staged(self.lib.mirt_nufft_interp_plan(self.handle),
+                                                   int(mode)))
 
     def set_gather(self, tma=True):
         """See InterpPlan.set_gather."""

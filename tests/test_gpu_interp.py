@@ -438,6 +438,57 @@ def test_sweep_spread_real_tables_phase_small_grid(order):
         plan.close()
 
 
+@pytest.mark.parametrize("C", [32, 40, 64])
+def test_staged_sweep_same_bits(C):
+    """The row sweep staged per bin column (mirt_interp_plan_set_staged 1: after
+    the ordering pass; 2: reading the caller's samples through the sort
+    permutation) gives the unstaged sweep's bits for bands of 1, 2 and 4 rows,
+    uniform segments and balanced teams, on three slices (a dense one, one
+    wrapping several times) with a per-sample phase, a partial coil chunk at
+    C = 40; and the oracle's adjoint.  Dense-bin patches take precedence over
+    staging (one-row bands): the same bits as without staging."""
+    import torch
+    rng = np.random.default_rng(29 + C)
+    K, J, L = [96, 64], [6, 6], [1024, 1024]
+    h = [mb.minmax_kb_table(48, 6, 96, 1024), mb.minmax_kb_table(32, 6, 64, 1024)]
+    tms = [rng.uniform(-60, 60, (1500, 2)), rng.uniform(-3, 3, (5000, 2)),
+           rng.uniform(-300, 300, (800, 2))]
+    moff = np.concatenate([[0], np.cumsum([len(t) for t in tms])])
+    tm = np.concatenate(tms)
+    ph = np.exp(1j * rng.uniform(-np.pi, np.pi, len(tm)))
+    plan = mb.InterpPlan(K, J, L, h, tm, C, slice_moff=moff, phase=ph)
+    fm = rng.standard_normal((len(tm), C)) + 1j * rng.standard_normal((len(tm), C))
+    fm_d = torch.from_numpy(fm.astype(np.complex64)).cuda()
+    refs = [oracle.interp_adj((fm * np.conj(ph)[:, None])[moff[s]:moff[s + 1]], h, J, L, tms[s],
+                              K, 0, impl=ref_impl()) for s in range(3)]
+    plan.set_dense(False)
+    for nseg, rows in [(1, 1), (5, 2), (16, 4), (-1, 1), (-1, 4)]:
+        plan.set_sweep(nseg, rows)
+        plan.set_staged(0)
+        base = plan.adjoint(fm_d).cpu().numpy()
+        for s in range(3):
+            got = np.transpose(base[s], (1, 0, 2)).reshape(-1, C, order="F")
+            assert rel_l2(got, refs[s]) <= ADJ_TOL, (nseg, rows, s)
+        for mode in (1, 2):
+            plan.set_staged(mode)
+            assert plan.config()["spread_staged"] == mode
+            out = plan.adjoint(fm_d).cpu().numpy()
+            assert np.array_equal(out, base), (nseg, rows, mode)
+    plan.set_dense(True)
+    plan.set_sweep(-1, 1)
+    plan.set_staged(0)
+    dense = plan.adjoint(fm_d).cpu().numpy()
+    plan.set_staged(2)
+    assert np.array_equal(plan.adjoint(fm_d).cpu().numpy(), dense)
+    with pytest.raises(mb.MirtError, match="staged mode"):
+        plan.set_staged(3)
+    plan.close()
+    small = mb.InterpPlan(K, J, L, h, tms[0], 8)
+    with pytest.raises(mb.MirtError, match="32-coil"):
+        small.set_staged(1)
+    small.close()
+
+
 def test_sweep_spread_refused_where_it_does_not_apply():
     h = [mb.minmax_kb_table(8, 4, 16, 64)] * 2
     plan = mb.InterpPlan([16, 16], [4, 4], [64, 64], h, np.zeros((10, 2)), 2)
