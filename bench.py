@@ -341,8 +341,13 @@ def run_gpu(args, w):
     elif args.spread == "tiled" and tuned.get("spread_sweep", 0) != 0:
         tuned = plan.set_sweep(0)
     if args.sweep_config:                       # a fixed row sweep (for captures of one config)
-        seg, rows = (int(v) for v in args.sweep_config.split(","))
-        tuned = plan.set_sweep(seg, rows)
+        v = [int(x) for x in args.sweep_config.split(",")]
+        tuned = plan.set_sweep(v[0], v[1])
+        if len(v) > 3:
+            plan.set_dense(bool(v[3]))
+        if len(v) > 2:
+            plan.set_staged(v[2])
+        tuned = plan.config()
     t_tune = time.perf_counter() - t0
     img_np = make_images(w, np.random.default_rng(99 + rank))
     if img_np.shape[0] != plan.nslice:
@@ -677,7 +682,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--sweep-config", default="",
-                    help="SEGMENTS,ROWS: fix the row sweep after autotuning (for captures)")
+                    help="SEGMENTS,ROWS[,STAGED[,DENSE]]: fix the row sweep after autotuning "
+                         "(for captures)")
     ap.add_argument("--no-graph", action="store_true",
                     help="time eager steps instead of a CUDA-graph replay (for profiling)")
     ap.add_argument("--spread", default="auto", choices=["auto", "sweep", "tiled"],

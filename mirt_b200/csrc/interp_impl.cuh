@@ -116,16 +116,10 @@ __device__ __forceinline__ float2 cw_fma(float2 w, float2 v, float2 vs, float2 A
   return A;
 }
 
-// acc += conj(w) * v as four scalar FMAs in the order (re: wr vr, wi vi;
-// im: wr vi, -wi vr) -- the roundings of cw_fma.
+// acc += conj(w) * v by cw_fma (the swapped v is shared by a row of taps)
 template <bool REAL>
 __device__ __forceinline__ void cmac_conj(float2 &acc, float2 w, float2 v) {
-  acc.x = __fmaf_rn(w.x, v.x, acc.x);
-  acc.y = __fmaf_rn(w.x, v.y, acc.y);
-  if (!REAL) {
-    acc.x = __fmaf_rn(w.y, v.y, acc.x);
-    acc.y = __fmaf_rn(-w.y, v.x, acc.y);
-  }
+  acc = cw_fma<REAL>(w, v, make_float2(v.y, v.x), acc);
 }
 
 // *p += (wr, wr) v2 + (wi, -wi) v2s: a read-modify-write by the point's one
@@ -942,6 +936,17 @@ __device__ __forceinline__ void cp_async8(void *dst, const void *src) {
 __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
 }
+__device__ __forceinline__ void cp_async4(void *dst, const void *src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+// all but the most recent group complete
+__device__ __forceinline__ void cp_async_wait_group1() {
+  asm volatile("cp.async.wait_group 1;" ::: "memory");
+}
 
 constexpr int SW3_CAP = 32;  // visits staged per batch and warp
 template <int CW>
@@ -1188,18 +1193,28 @@ __global__ void __launch_bounds__(256) spread_sweep3_kernel(InterpArgs a, Tiling
 // 2D row sweep with per-column staging (J = 6, one-point bins, 32-coil chunks)
 // ------------------------------------------------------------------------
 // The team of spread_sweep_kernel (one warp, lane = coil; R grid rows, a
-// segment of their columns), with the bin columns' samples staged as in the 3D
-// line sweep: lane q < R + 5 keeps the pointer of bin row q and loads the next
-// column's while the current one is summed; per column the warp lists the
-// samples (bin rows in order, samples in sort order), copies their tap records
-// and the lanes' sample values into its shared-memory stage with cp.async, and
-// adds them from there.  DIRECT: the sample rows are read in the caller's order
-// through perm and times conj(phase) here, so the ordering pass is not needed.
-// Same operations in the same order as spread_sweep_kernel: the same bits.
+// segment of their columns), with the samples of each bin column staged in the
+// warp's shared memory by cp.async, three columns in flight: while column xb
+// is summed, the sample rows of column xb + 1 and the tap records of column
+// xb + 2 are on their way.  Per column, lane q < R + 5 holds the bounds of bin
+// row q (the next column's end loaded a column ahead); the warp lists the
+// column's samples (bin rows in order, samples in sort order; the first
+// SW2_CAP of them staged ahead, the rest of a crowded column staged when it is
+// summed).  DIRECT: the sample rows are read in the caller's order through perm
+// (staged with the records) and times conj(phase) here, so the ordering pass
+// is not needed.  Same operations in the same order as spread_sweep_kernel:
+// the same bits.
 constexpr int SW2_CAP = 16;
+// one column's list: positions, caller rows, phases; lane bounds
+struct Sw2Meta {
+  int pos[SW2_CAP];
+  int row[SW2_CAP];
+  float2 ph[SW2_CAP];
+  int beg[16], ex[16];
+};
 template <bool DIRECT>
 constexpr int sweep2_warp_bytes() {
-  return 3 * SW2_CAP * 4 + SW2_CAP * 4 + SW2_CAP * 8 + SW2_CAP * 12 * 8 + SW2_CAP * 32 * 8;
+  return 3 * (int)sizeof(Sw2Meta) + 3 * SW2_CAP * 12 * 8 + 2 * SW2_CAP * 32 * 8;
 }
 
 template <int R, bool REAL, bool DIRECT>
@@ -1210,12 +1225,9 @@ __device__ __forceinline__ void sweep2s_team(const InterpArgs &a, const Tiling &
                                              unsigned char *wsm) {
   constexpr unsigned FULLM = 0xffffffffu;
   constexpr int NQ = R + 5;
-  int *spos = reinterpret_cast<int *>(wsm);
-  int *sq = spos + SW2_CAP;
-  int *smi = sq + SW2_CAP;
-  float2 *sph = reinterpret_cast<float2 *>(wsm + 4 * SW2_CAP * 4);
-  float2 *srec = sph + SW2_CAP;
-  float2 *sf = srec + SW2_CAP * 12;
+  Sw2Meta *meta = reinterpret_cast<Sw2Meta *>(wsm);
+  float2 *srec = reinterpret_cast<float2 *>(wsm + 3 * sizeof(Sw2Meta));
+  float2 *sf = srec + 3 * SW2_CAP * 12;
   const int K1 = a.g.K[0], K2 = a.g.K[1];
   int slice, y0, x0, x1;
   if (t.sweep < 0) {
@@ -1250,25 +1262,54 @@ __device__ __forceinline__ void sweep2s_team(const InterpArgs &a, const Tiling &
   }
   const int xs = x0 - 5;
   auto wrapx = [&](int x) { return x < 0 ? x + K1 : x; };
-  int beg = rowb >= 0 ? __ldg(bs + rowb + wrapx(xs)) : 0;
-  int en = rowb >= 0 ? __ldg(bs + rowb + wrapx(xs) + 1) : beg;
+  // lane bounds of the next column to list: start lb, end le (loaded ahead)
+  int lb = rowb >= 0 ? __ldg(bs + rowb + wrapx(xs)) : 0;
+  int le = rowb >= 0 ? __ldg(bs + rowb + wrapx(xs) + 1) : lb;
   int rn = 0;
-  float2 acc[R][6];
-#pragma unroll
-  for (int r = 0; r < R; r++)
-#pragma unroll
-    for (int j = 0; j < 6; j++) acc[r][j] = make_float2(0.f, 0.f);
-  float2 *out = ck + (long long)slice * a.grid_elems + (long long)y0 * K1 * C + c0 + lane;
   // lane's first chunk of the records' 16-byte copies: (visit, chunk) = (lane / 6, lane % 6)
   const int cv0 = lane / 6, ck0 = lane - 6 * (lane / 6);
-  for (int xb = xs; xb < x1; xb++) {
-    const int end = en;
-    if (xb == 0 && xs < 0) beg = rn;
-    if (xb + 1 < x1 && rowb >= 0) {
-      en = __ldg(bs + rowb + wrapx(xb + 1) + 1);
-      if (xb + 1 == 0) rn = __ldg(bs + rowb);
+  // records, caller rows and phases of the listed visits [0, nb)
+  auto issue_rec = [&](Sw2Meta &m, float2 *rec, int nb) {
+    for (int v = cv0, kk = ck0; v < nb;) {
+      cp_async16(rec + v * 12 + 2 * kk, a.W + (long long)m.pos[v] * 12 + 2 * kk);
+      v += 5;
+      kk += 2;
+      if (kk >= 6) {
+        kk -= 6;
+        v++;
+      }
     }
-    const int n = end - beg;
+    if (DIRECT && lane < nb) {
+      const int p = m.pos[lane];
+      if (a.perm)
+        cp_async4(&m.row[lane], a.perm + p);
+      else
+        m.row[lane] = p;
+      if (a.phase) cp_async8(&m.ph[lane], a.phase + p);
+    }
+  };
+  auto issue_rows = [&](const Sw2Meta &m, float2 *f, int nb) {
+    for (int v = 0; v < nb; v++) {
+      const long long row = DIRECT ? (long long)m.row[v] : (long long)m.pos[v];
+      if (on)
+        cp_async8(f + v * 32 + lane, fs + row * C + c0 + lane);
+      else
+        f[v * 32 + lane] = make_float2(0.f, 0.f);
+    }
+  };
+  // list visits [vb, vb + SW2_CAP) of a column from the lanes' bounds
+  auto list_part = [&](Sw2Meta &m, int beg, int n, int ex, int vb) {
+    for (int k = max(0, vb - ex); k < n && ex + k < vb + SW2_CAP; k++) m.pos[ex + k - vb] = beg + k;
+  };
+  // list column xc into meta slot m and issue its records; returns its visits
+  auto list_col = [&](int xc, Sw2Meta &m, float2 *rec) -> int {
+    const int end = le;
+    if (xc == 0 && xs < 0) lb = rn;
+    if (xc + 1 < x1 && rowb >= 0) {
+      le = __ldg(bs + rowb + wrapx(xc + 1) + 1);
+      if (xc + 1 == 0) rn = __ldg(bs + rowb);
+    }
+    const int n = end - lb;
     int inc = n;
 #pragma unroll
     for (int o = 1; o < 16; o <<= 1) {
@@ -1276,58 +1317,107 @@ __device__ __forceinline__ void sweep2s_team(const InterpArgs &a, const Tiling &
       if (lane >= o) inc += u;
     }
     const int V = __shfl_sync(FULLM, inc, 15);
-    const int ex = inc - n;
-    for (int vb = 0; vb < V; vb += SW2_CAP) {
-      const int nb = min(SW2_CAP, V - vb);
-      for (int k = max(0, vb - ex); k < n && ex + k < vb + SW2_CAP; k++) {
-        spos[ex + k - vb] = beg + k;
-        sq[ex + k - vb] = lane;
+    if (lane < 16) {
+      m.beg[lane] = lb;
+      m.ex[lane] = inc - n;
+    }
+    list_part(m, lb, n, inc - n, 0);
+    lb = end;
+    __syncwarp();
+    issue_rec(m, rec, min(V, SW2_CAP));
+    cp_async_commit();
+    return V;
+  };
+  // accumulators of grid columns xb .. xb + 5 (slot j: column xb + j)
+  float2 acc[R][6];
+#pragma unroll
+  for (int r = 0; r < R; r++)
+#pragma unroll
+    for (int j = 0; j < 6; j++) acc[r][j] = make_float2(0.f, 0.f);
+  // staged visits [vb, vb + nb) of the column; bin row q's visits are
+  // [ex[q], ex[q + 1]), each reaching band rows r = q - 5 .. q
+  auto sum_chunk = [&](const Sw2Meta &m, const int *exq, const float2 *rec, const float2 *f,
+                       int vb, int nb) {
+    sfor<NQ>([&](auto QQ) {
+      constexpr int Q = decltype(QQ)::value;
+      const int lo = max(exq[Q] - vb, 0), hi = min(exq[Q + 1] - vb, nb);
+      for (int v = lo; v < hi; v++) {
+        float2 fv = f[v * 32 + lane];
+        if (DIRECT && a.phase) fv = cmulc(m.ph[v], fv);
+        const float4 *r4 = reinterpret_cast<const float4 *>(rec + v * 12);
+        const float4 w01 = r4[0], w23 = r4[1], w45 = r4[2];
+        const float2 w1[6] = {make_float2(w01.x, w01.y), make_float2(w01.z, w01.w),
+                              make_float2(w23.x, w23.y), make_float2(w23.z, w23.w),
+                              make_float2(w45.x, w45.y), make_float2(w45.z, w45.w)};
+        sfor<R>([&](auto RR) {
+          constexpr int r = decltype(RR)::value;
+          constexpr int j2 = r - Q + 5;
+          if constexpr (j2 >= 0 && j2 < 6) {
+            const float2 vv = cw_mul<REAL>(rec[v * 12 + 6 + j2], fv);
+            const float2 vsw = make_float2(vv.y, vv.x);
+            sfor<6>([&](auto JJ) {
+              constexpr int j = decltype(JJ)::value;
+              acc[r][j] = cw_fma<REAL>(w1[j], vv, vsw, acc[r][j]);
+            });
+          }
+        });
       }
-      __syncwarp();
-      if (DIRECT) {
-        if (lane < nb) {
-          const int p = spos[lane];
-          smi[lane] = a.perm ? __ldg(a.perm + p) : p;
-          sph[lane] = a.phase ? __ldg(a.phase + p) : make_float2(1.f, 0.f);
+    });
+  };
+  float2 *out = ck + (long long)slice * a.grid_elems + (long long)y0 * K1 * C + c0 + lane;
+  // prologue: records of the first two columns, sample rows of the first
+  int Vc = list_col(xs, meta[0], srec);
+  int Vn = list_col(xs + 1, meta[1], srec + SW2_CAP * 12);
+  cp_async_wait_group1();
+  __syncwarp();
+  issue_rows(meta[0], sf, min(Vc, SW2_CAP));
+  cp_async_commit();
+  int sc = 0, fb = 0;  // list slot (of 3) and row block (of 2) of the column being summed
+  for (int xb = xs; xb < x1; xb++) {
+    const int s1 = sc == 2 ? 0 : sc + 1, s2 = sc == 0 ? 2 : sc - 1;
+    int Vnn = 0;
+    if (xb + 2 < x1)
+      Vnn = list_col(xb + 2, meta[s2], srec + s2 * SW2_CAP * 12);
+    else
+      cp_async_commit();
+    cp_async_wait_group1();  // records of xb + 1, rows of xb
+    __syncwarp();
+    if (xb + 1 < x1) issue_rows(meta[s1], sf + (1 - fb) * SW2_CAP * 32, min(Vn, SW2_CAP));
+    cp_async_commit();
+    Sw2Meta &m = meta[sc];
+    float2 *rec = srec + sc * SW2_CAP * 12;
+    float2 *f = sf + fb * SW2_CAP * 32;
+    int exq[NQ + 1];
+#pragma unroll
+    for (int q = 0; q <= NQ; q++) exq[q] = m.ex[q];
+    // the first SW2_CAP visits are staged; the rest of a crowded column is
+    // staged here, SW2_CAP at a time
+    for (int vb = 0; vb < Vc; vb += SW2_CAP) {
+      const int nb = min(SW2_CAP, Vc - vb);
+      if (vb > 0) {
+        int beg = 0, ex = 0;
+        if (lane < 16) {
+          beg = m.beg[lane];
+          ex = m.ex[lane];
         }
+        const int exn = __shfl_down_sync(FULLM, ex, 1);
+        const int n = lane < 15 ? exn - ex : 0;
+        __syncwarp();
+        list_part(m, beg, n, ex, vb);
+        __syncwarp();
+        issue_rec(m, rec, nb);
+        cp_async_commit();
+        cp_async_wait_all();
+        __syncwarp();
+        issue_rows(m, f, nb);
+        cp_async_commit();
+        cp_async_wait_all();
         __syncwarp();
       }
-      for (int v = cv0, kk = ck0; v < nb;) {
-        cp_async16(srec + v * 12 + 2 * kk, a.W + (long long)spos[v] * 12 + 2 * kk);
-        v += 5;
-        kk += 2;
-        if (kk >= 6) {
-          kk -= 6;
-          v++;
-        }
-      }
-      for (int v = 0; v < nb; v++) {
-        const long long row = DIRECT ? (long long)smi[v] : (long long)spos[v];
-        if (on)
-          cp_async8(sf + v * 32 + lane, fs + row * C + c0 + lane);
-        else
-          sf[v * 32 + lane] = make_float2(0.f, 0.f);
-      }
-      cp_async_wait_all();
-      __syncwarp();
-      for (int v = 0; v < nb; v++) {
-        const int q = sq[v];
-        float2 f = sf[v * 32 + lane];
-        if (DIRECT && a.phase) f = cmulc(sph[v], f);
-        const float2 *rv = srec + v * 12;
-#pragma unroll
-        for (int r = 0; r < R; r++) {
-          const int j2 = r - q + 5;
-          if (j2 >= 0 && j2 < 6) {
-            const float2 vv = cw_mul<REAL>(rv[6 + j2], f);
-#pragma unroll
-            for (int j = 0; j < 6; j++) cmac_conj<REAL>(acc[r][j], rv[j], vv);
-          }
-        }
-      }
+      sum_chunk(m, exq, rec, f, vb, nb);
       __syncwarp();
     }
-    beg = end;
+    // grid column xb is complete
     if (xb >= x0 && on) {
 #pragma unroll
       for (int r = 0; r < R; r++)
@@ -1339,7 +1429,14 @@ __device__ __forceinline__ void sweep2s_team(const InterpArgs &a, const Tiling &
       for (int j = 0; j < 5; j++) acc[r][j] = acc[r][j + 1];
       acc[r][5] = make_float2(0.f, 0.f);
     }
+    __syncwarp();  // list slot sc is listed again two columns on
+    Vc = Vn;
+    Vn = Vnn;
+    sc = s1;
+    fb ^= 1;
   }
+  cp_async_wait_all();
+  __syncwarp();
 }
 
 template <int R, bool REAL, bool DIRECT>

@@ -462,6 +462,7 @@ def test_staged_sweep_same_bits(C):
     refs = [oracle.interp_adj((fm * np.conj(ph)[:, None])[moff[s]:moff[s + 1]], h, J, L, tms[s],
                               K, 0, impl=ref_impl()) for s in range(3)]
     plan.set_dense(False)
+    first = None
     for nseg, rows in [(1, 1), (5, 2), (16, 4), (-1, 1), (-1, 4)]:
         plan.set_sweep(nseg, rows)
         plan.set_staged(0)
@@ -474,6 +475,8 @@ def test_staged_sweep_same_bits(C):
             assert plan.config()["spread_staged"] == mode
             out = plan.adjoint(fm_d).cpu().numpy()
             assert np.array_equal(out, base), (nseg, rows, mode)
+        first = base if first is None else first
+        assert np.array_equal(base, first)
     plan.set_dense(True)
     plan.set_sweep(-1, 1)
     plan.set_staged(0)
