@@ -348,6 +348,8 @@ def run_gpu(args, w):
         if len(v) > 2:
             plan.set_staged(v[2])
         tuned = plan.config()
+    if args.gather_tma is not None:             # a fixed gather (for captures of one form)
+        tuned = plan.set_gather(args.gather_tma)
     t_tune = time.perf_counter() - t0
     img_np = make_images(w, np.random.default_rng(99 + rank))
     if img_np.shape[0] != plan.nslice:
@@ -684,6 +686,9 @@ def main():
     ap.add_argument("--sweep-config", default="",
                     help="SEGMENTS,ROWS[,STAGED[,DENSE]]: fix the row sweep after autotuning "
                          "(for captures)")
+    ap.add_argument("--gather-tma", type=int, default=None, choices=[0, 1, 2],
+                    help="fix the gather after autotuning: 0 plain, 1 TMA tiles of 32 coils, "
+                         "2 of 16 coils (for captures)")
     ap.add_argument("--no-graph", action="store_true",
                     help="time eager steps instead of a CUDA-graph replay (for profiling)")
     ap.add_argument("--spread", default="auto", choices=["auto", "sweep", "tiled"],

@@ -272,8 +272,11 @@ int mirt_interp_plan_set_staged(mirt_interp_plan *plan, int32_t mode);
  * coefficients and first taps (1-D bulk copies) into shared memory, two
  * stages deep, and reads all taps and records from there; blocks whose taps
  * wrap past K read the grid directly.  Same arithmetic and summation order
- * as the plain gather: identical results.  tma = 0 selects the plain gather;
- * MIRT_ERR_ARG where the plan has no TMA blocks.  No reference counterpart. */
+ * as the plain gather: identical results.  tma = 1: tiles of 32 coils (a warp
+ * per sample, two CTAs per SM); 2: tiles of 16 coils (a half-warp per sample,
+ * three CTAs per SM); 0 selects the plain gather.  The autotuner times all
+ * three.  MIRT_ERR_ARG for other modes and where the plan has no TMA blocks.
+ * No reference counterpart. */
 int mirt_interp_plan_set_gather(mirt_interp_plan *plan, int32_t tma);
 
 /* Fault flag of the plan's bounded in-kernel waits (TMA stage arrivals):

@@ -138,6 +138,16 @@ __global__ void gather_records_kernel(const int *__restrict__ gorder, long long 
   if (ph) phg[i] = ph[p];
   for (int j = 0; j < SJ; j++) Wg[i * SJ + j] = W[p * SJ + j];
 }
+
+// Output records of the TMA gather, in the gather order: (caller's sample
+// index, 0, phase re, phase im as bits); phase (1, 0) where there is none.
+__global__ void out_records_kernel(long long M, const int *__restrict__ permg,
+                                   const float2 *__restrict__ phg, int4 *__restrict__ out) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= M) return;
+  const float2 ph = phg ? phg[i] : make_float2(1.f, 0.f);
+  out[i] = make_int4(permg[i], 0, __float_as_int(ph.x), __float_as_int(ph.y));
+}
 }  // namespace mirt_plan_kernels
 
 namespace {
@@ -475,7 +485,7 @@ cudaError_t plan_gather(mirt_interp_plan *P, const float2 *ck, float2 *fm, cudaS
   if (P->gtma) {
     const long long i0 = P->gitem_slice[s0], i1 = P->gitem_slice[s1];
     return launch_gather_tma(P->ag, P->gbk, S, i0, i1 - i0, ck, fm, P->gfault.as<int>(), st,
-                             P->gfault_test);
+                             P->gfault_test, P->gtma == 2 ? 16 : 32);
   }
   InterpArgs ag = P->ag;
   if (s0 > 0 || s1 < S) {
@@ -951,7 +961,13 @@ int plan_finish(mirt_interp_plan *P, long long Mtot, const long long *moff, int 
       CK(P->gitem.alloc(std::max<size_t>(items.size(), 1) * sizeof(int2)));
       if (!items.empty())
         CK(cudaMemcpy(P->gitem.p, items.data(), items.size() * sizeof(int2), cudaMemcpyHostToDevice));
-      P->gbk = GatherBlocks{P->gblk.as<int>(), P->gitem.as<int2>(), gbs, t4.nbin[0], t4.nbin[1]};
+      CK(P->orec_g.alloc(Mtot * sizeof(int4)));
+      mirt_plan_kernels::out_records_kernel<<<(unsigned)((Mtot + 255) / 256), 256, 0, st>>>(
+          Mtot, P->ag.perm, P->ag.phase, P->orec_g.as<int4>());
+      CK(cudaGetLastError());
+      CK(cudaStreamSynchronize(st));
+      P->gbk = GatherBlocks{P->gblk.as<int>(), P->gitem.as<int2>(), P->orec_g.as<int4>(), gbs,
+                            t4.nbin[0], t4.nbin[1]};
       CK(P->gfault.alloc(sizeof(int)));
       CK(cudaMemset(P->gfault.p, 0, sizeof(int)));
       P->gtma = 1;  // the default where it applies; the autotuner times both
@@ -1352,18 +1368,22 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
       bestg = l;
     }
   }
-  if (had_tma) {
-    P->gtma = 1;
-    float ms = 0;
-    int rc = time_launch([&]() {
-      return plan_gather(P, grid.as<float2>(), samp.as<float2>(), st);
-    }, st, &ms);
-    if (rc) return rc;
-    if (ms < bestg_ms) {
-      bestg_ms = ms;
-      best_tma = 1;
+  if (had_tma)
+    for (int mode : {1, 2}) {  // tiles of 32 or 16 coils
+      P->gtma = mode;
+      float ms = 0;
+      int rc = time_launch([&]() {
+        return plan_gather(P, grid.as<float2>(), samp.as<float2>(), st);
+      }, st, &ms);
+      if (rc) return rc;
+      if (autotune_log())
+        std::fprintf(stderr, "mirt autotune gather: TMA tiles of %d coils: %.3f ms\n",
+                     mode == 2 ? 16 : 32, ms);
+      if (ms < bestg_ms) {
+        bestg_ms = ms;
+        best_tma = mode;
+      }
     }
-  }
   P->gtma = best_tma;
   P->lg = bestg;
   CK(cudaStreamSynchronize(st));
@@ -1383,9 +1403,10 @@ int mirt_interp_plan_config(mirt_interp_plan *P, int32_t *out, int32_t n) {
 
 int mirt_interp_plan_set_gather(mirt_interp_plan *P, int32_t tma) {
   if (!P) return fail(MIRT_ERR_ARG, "plan is NULL");
+  if (tma < 0 || tma > 2) return fail(MIRT_ERR_ARG, "gather mode must be 0, 1 or 2");
   if (tma && !P->gbk.item)
     return fail(MIRT_ERR_ARG, "TMA gather needs 2D, J = 6, an even C >= 32 and K >= 13");
-  P->gtma = tma ? 1 : 0;
+  P->gtma = tma;
   return MIRT_OK;
 }
 

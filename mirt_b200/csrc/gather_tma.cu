@@ -4,22 +4,27 @@
 //
 // The gather order groups the samples by 8 x 8 blocks of their first taps
 // (slice-major, then block rows, then block columns); a work item is up to
-// TG_RC consecutive samples of one block.  A CTA takes one item at a time:
-// one thread issues, on one mbarrier, a cp.async.bulk.tensor of the block's
-// 13 x 13 grid points x 32 coils and 1-D bulk copies of the item's tap
-// coefficients and first taps (contiguous in the gather order) into one of
-// two shared-memory stages, and issues the next item's copies into the other
-// stage before the current one is used, so the loads overlap the arithmetic.
-// The CTA's eight warps take the item's samples in turn (lane = coil) and
-// read their records and all 36 taps from shared memory; only the output
-// index and phase come from global memory.  Blocks whose taps wrap past K
-// (the last block row and column) read the grid from global memory instead.
+// TG_RC consecutive samples of one block.  A CTA's items alternate between
+// two shared-memory stages; an item's copies -- on one mbarrier, a
+// cp.async.bulk.tensor of the block's 13 x 13 grid points x 32 (or 16) coils
+// and 1-D bulk copies of the item's tap coefficients and first taps
+// (contiguous in the gather order) -- are issued while the item before it is
+// summed: the first two at the CTA's start, each later one by the last warp to
+// finish the item two before it, into the stage that item frees.  No CTA-wide
+// barrier: warps do not wait for the slowest warp of every item.  The CTA's
+// eight warps take the item's samples in turn (lane = coil; two samples per
+// warp with 16-coil tiles), starting from a warp that rotates from item to
+// item, and read their records, output rows and phases and all 36 taps from
+// shared memory.  Blocks whose taps wrap past
+// K (the last block row and column) read the grid from global memory instead.
 // Per sample the taps are summed in the order of the plain gather (columns
 // inner, rows outer, packed FP32x2 MACs), so the two give identical results.
 //
-// Waits are bounded: when a stage does not arrive within the limit the CTA
-// sets the plan's fault flag, waits (bounded) for its other stage in flight
-// and stops; the host reads the flag (mirt_interp_plan_fault).
+// Waits are bounded: when a stage does not arrive within the limit the warp
+// sets the plan's fault flag, waits (bounded) for the other stage's copy in
+// flight and stops; the stage is then never released, so no further copy is
+// issued, and the other warps' waits run out in turn.  The host reads the
+// flag (mirt_interp_plan_fault).
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
@@ -30,15 +35,22 @@ namespace {
 
 constexpr int TG_GB = 8;               // block of first taps per dimension
 constexpr int TG_TW = TG_GB + 5;       // tile extent per dimension (J = 6)
-constexpr int TG_CW = 32;              // coils per tile (lanes)
-constexpr unsigned TG_TILE_BYTES = TG_TW * TG_TW * TG_CW * 8;   // 43,264
 constexpr int TG_RC = 96;              // samples per work item
 constexpr unsigned TG_W_BYTES = TG_RC * 12 * 8;                 // 9,216
 constexpr unsigned TG_K_BYTES = TG_RC * 16;                     // 1,536
-constexpr unsigned TG_STAGE = TG_TILE_BYTES + TG_W_BYTES + TG_K_BYTES;  // 54,016 = 422 x 128
+constexpr unsigned TG_O_BYTES = TG_RC * 16;                     // 1,536
 constexpr int TG_THREADS = 256;
 constexpr long long TG_WAIT_LIMIT = 1ll << 22;
 constexpr long long TG_TEST_WAIT_LIMIT = 1ll << 12;
+// Tiles of TCW coils: 32 (a warp per sample, lane = coil) or 16 (a half-warp
+// per sample: smaller stages, three CTAs per SM instead of two).
+template <int TCW>
+struct TgShape {
+  static constexpr unsigned TILE = TG_TW * TG_TW * TCW * 8;         // 43,264 / 21,632
+  static constexpr unsigned STAGE = TILE + TG_W_BYTES + TG_K_BYTES + TG_O_BYTES;  // 55,552 / 33,920
+  static constexpr int CTAS_PER_SM = TCW == 32 ? 2 : 3;
+  static_assert(TILE % 128 == 0 && STAGE % 128 == 0, "stages must stay 128-byte aligned");
+};
 
 __device__ __forceinline__ unsigned smem_addr(const void *p) {
   return (unsigned)__cvta_generic_to_shared(p);
@@ -111,78 +123,92 @@ __device__ __forceinline__ Item item_of(const GatherBlocks &g, const InterpArgs 
 // one thread: arm the stage's barrier and start its copies.  no_copy (the
 // test of the bounded waits): arm the barrier for bytes that no copy will
 // deliver and issue no copy, so that its wait runs out with nothing in flight.
+template <int TCW>
 __device__ __forceinline__ void stage_issue(const CUtensorMap *tm, const InterpArgs &a,
-                                            unsigned char *st, uint64_t *bar, const Item &r,
-                                            int chunk, bool no_copy) {
+                                            const int4 *orec, unsigned char *st, uint64_t *bar,
+                                            const Item &r, int chunk, bool no_copy) {
+  constexpr unsigned TILE = TgShape<TCW>::TILE;
   const unsigned wb = (unsigned)r.n * 96u, kb = (unsigned)r.n * 16u;
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   if (no_copy) {
     mbar_expect(bar, 16u);
     return;
   }
-  mbar_expect(bar, (r.interior ? TG_TILE_BYTES : 0u) + wb + kb);
+  mbar_expect(bar, (r.interior ? TILE : 0u) + wb + 2 * kb);
   if (r.interior)
-    tile_copy(tm, st, bar, chunk * 2 * TG_CW, r.bx * TG_GB, r.by * TG_GB, r.slice);
-  bulk_copy(st + TG_TILE_BYTES, a.W + (long long)r.p0 * 12, wb, bar);
-  bulk_copy(st + TG_TILE_BYTES + TG_W_BYTES, a.K0 + r.p0, kb, bar);
+    tile_copy(tm, st, bar, chunk * 2 * TCW, r.bx * TG_GB, r.by * TG_GB, r.slice);
+  bulk_copy(st + TILE, a.W + (long long)r.p0 * 12, wb, bar);
+  bulk_copy(st + TILE + TG_W_BYTES, a.K0 + r.p0, kb, bar);
+  bulk_copy(st + TILE + TG_W_BYTES + TG_K_BYTES, orec + r.p0, kb, bar);
 }
 
-template <bool REAL>
-__global__ void __launch_bounds__(TG_THREADS, 2)
+template <bool REAL, int TCW>
+__global__ void __launch_bounds__(TG_THREADS, TgShape<TCW>::CTAS_PER_SM)
     gather_tma_kernel(const __grid_constant__ CUtensorMap tmap, InterpArgs a, GatherBlocks g,
                       long long it0, long long nit, const float2 *__restrict__ ck,
                       float2 *__restrict__ fm, int *__restrict__ fault, int no_copy,
                       long long wait_limit) {
+  constexpr unsigned TILE = TgShape<TCW>::TILE, STAGE = TgShape<TCW>::STAGE;
+  constexpr int SPW = 32 / TCW;  // samples per warp at a time
+  constexpr int NWARP = TG_THREADS / 32;
   extern __shared__ __align__(128) unsigned char smem[];
-  uint64_t *bar = reinterpret_cast<uint64_t *>(smem + 2 * TG_STAGE);
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smem + 2 * STAGE);
+  int *done = reinterpret_cast<int *>(bar + 2);  // warps finished with each stage's item
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int nwarp = TG_THREADS / 32;
+  const int sub = lane / TCW, cl = lane % TCW;
   const int C = a.C;
   const int chunk = blockIdx.y;
-  const int c = chunk * TG_CW + lane;
+  const int c = chunk * TCW + cl;
   const bool on = c < C;
   const int K1 = a.g.K[0], K2 = a.g.K[1];
+  const long long end = it0 + nit;
   if (threadIdx.x == 0) {
     mbar_init(&bar[0]);
     mbar_init(&bar[1]);
+    done[0] = done[1] = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
-  unsigned par0 = 0u, par1 = 0u;  // wait parity of each stage's barrier
-  const long long end = it0 + nit;
-  long long i = it0 + blockIdx.x;
-  if (threadIdx.x == 0 && i < end)
-    stage_issue(&tmap, a, smem, &bar[0], item_of(g, a, i), chunk, no_copy);
-  for (int k = 0; i < end; i += gridDim.x, k++) {
+  // the CTA's items are it0 + blockIdx.x + k gridDim.x, k = 0, 1, ...; item k
+  // goes to stage k & 1.  The first two are issued here; after that the last
+  // warp to finish item k issues item k + 2 into the stage it frees, so no
+  // warp waits for another except through the two stages.
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 2; k++) {
+      const long long i = it0 + blockIdx.x + (long long)k * gridDim.x;
+      if (i < end)
+        stage_issue<TCW>(&tmap, a, g.orec, smem + k * STAGE, &bar[k], item_of(g, a, i), chunk,
+                         no_copy);
+    }
+  for (int k = 0;; k++) {
+    const long long i = it0 + blockIdx.x + (long long)k * gridDim.x;
+    if (i >= end) break;
     const int s = k & 1;
-    const long long inx = i + gridDim.x;
-    if (threadIdx.x == 0 && inx < end)
-      stage_issue(&tmap, a, smem + (s ^ 1) * TG_STAGE, &bar[s ^ 1], item_of(g, a, inx), chunk,
-                  no_copy);
     const Item r = item_of(g, a, i);
-    const bool ready = stage_wait(&bar[s], s ? par1 : par0, wait_limit);
-    if (s) par1 ^= 1u;
-    else par0 ^= 1u;
-    if (__syncthreads_or(!ready)) {
-      // a stage did not arrive in time: flag it, let the other stage land
-      // (bounded), and stop this CTA
-      if (threadIdx.x == 0) {
+    if (!stage_wait(&bar[s], (unsigned)(k >> 1) & 1u, wait_limit)) {
+      // the stage did not arrive in time: flag it, let the other stage's copy
+      // land (bounded), and stop this warp; the stage is never released, so
+      // no further copy is issued
+      if (lane == 0) {
         atomicExch(fault, 1);
-        if (inx < end) stage_wait(&bar[s ^ 1], s ? par0 : par1, wait_limit);
+        if (i + gridDim.x < end)
+          stage_wait(&bar[s ^ 1], (unsigned)((k + 1) >> 1) & 1u, wait_limit);
       }
       return;
     }
-    const unsigned char *st = smem + s * TG_STAGE;
+    const unsigned char *st = smem + s * STAGE;
     const float2 *tile = reinterpret_cast<const float2 *>(st);
-    const float2 *Wst = reinterpret_cast<const float2 *>(st + TG_TILE_BYTES);
-    const int4 *Kst = reinterpret_cast<const int4 *>(st + TG_TILE_BYTES + TG_W_BYTES);
+    const float2 *Wst = reinterpret_cast<const float2 *>(st + TILE);
+    const int4 *Kst = reinterpret_cast<const int4 *>(st + TILE + TG_W_BYTES);
+    const int4 *Ost = reinterpret_cast<const int4 *>(st + TILE + TG_W_BYTES + TG_K_BYTES);
     const int x0 = r.bx * TG_GB, y0 = r.by * TG_GB;
     const float2 *gs = ck + (long long)r.slice * a.grid_elems + c;
-    for (int q = warp; q < r.n; q += nwarp) {
-      const int pos = r.p0 + q;
-      // output row and phase: global, used last
-      const int m = a.perm ? __ldg(a.perm + pos) : pos;
-      const float2 ph = a.phase ? __ldg(a.phase + pos) : make_float2(1.f, 0.f);
+    // the warps' share of the item rotates from item to item
+    const int wr = (warp + NWARP - (k % NWARP)) % NWARP;
+    for (int q = wr * SPW + sub; q < r.n; q += NWARP * SPW) {
+      const int4 o = Ost[q];  // output row and phase
+      const int m = o.x;
+      const float2 ph = make_float2(__int_as_float(o.z), __int_as_float(o.w));
       const int4 k0 = Kst[q];
       const float2 *Ws = Wst + q * 12;
       float2 w1[6];
@@ -191,14 +217,14 @@ __global__ void __launch_bounds__(TG_THREADS, 2)
       detail::CAcc s2;
       detail::cacc_zero(s2);
       if (r.interior) {
-        const float2 *tl = tile + ((k0.y - y0) * TG_TW + (k0.x - x0)) * TG_CW + lane;
+        const float2 *tl = tile + ((k0.y - y0) * TG_TW + (k0.x - x0)) * TCW + cl;
 #pragma unroll
         for (int j2 = 0; j2 < 6; j2++) {
           detail::CAcc s1;
           detail::cacc_zero(s1);
 #pragma unroll
           for (int j1 = 0; j1 < 6; j1++)
-            detail::cacc_mac<REAL>(s1, w1[j1], tl[(j2 * TG_TW + j1) * TG_CW]);
+            detail::cacc_mac<REAL>(s1, w1[j1], tl[(j2 * TG_TW + j1) * TCW]);
           detail::cacc_mac<false>(s2, Ws[6 + j2], detail::cacc_get<REAL>(s1));
         }
       } else if (on) {
@@ -217,7 +243,19 @@ __global__ void __launch_bounds__(TG_THREADS, 2)
       if (a.phase) out = cmul(out, ph);
       if (on) fm[(long long)m * C + c] = out;
     }
-    __syncthreads();  // the stage is free before the next-but-one item is copied into it
+    // release the stage; the last warp out refills it with item k + 2
+    __syncwarp();
+    if (lane == 0) {
+      __threadfence_block();
+      if (atomicAdd(&done[s], 1) == NWARP - 1) {
+        done[s] = 0;
+        __threadfence_block();
+        const long long i2 = i + 2ll * gridDim.x;
+        if (i2 < end)
+          stage_issue<TCW>(&tmap, a, g.orec, smem + s * STAGE, &bar[s], item_of(g, a, i2),
+                           chunk, no_copy);
+      }
+    }
   }
 }
 
@@ -238,7 +276,7 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 }  // namespace
 
 bool gather_tma_ok(const InterpArgs &a) {
-  if (a.g.D != 2 || a.C < TG_CW || (a.C & 1)) return false;
+  if (a.g.D != 2 || a.C < 32 || (a.C & 1)) return false;
   for (int d = 0; d < 2; d++)
     if (a.g.J[d] != 6 || a.g.K[d] < TG_TW) return false;
   return true;
@@ -249,9 +287,10 @@ int gather_tma_item() { return TG_RC; }
 
 cudaError_t launch_gather_tma(const InterpArgs &a, const GatherBlocks &g, int nslice,
                               long long it0, long long nit, const float2 *ck, float2 *fm,
-                              int *fault, cudaStream_t st, int fault_test) {
+                              int *fault, cudaStream_t st, int fault_test, int tcw) {
   if (a.Mtot == 0 || a.C == 0 || nit <= 0) return cudaSuccess;
-  if (!gather_tma_ok(a) || g.gb != TG_GB || a.SJ != 12) return cudaErrorInvalidValue;
+  if (!gather_tma_ok(a) || g.gb != TG_GB || a.SJ != 12 || (tcw != 32 && tcw != 16))
+    return cudaErrorInvalidValue;
   PFN_cuTensorMapEncodeTiled_v12000 enc = encode_fn();
   if (!enc) return cudaErrorNotSupported;
   // the grid as floats [S][K2][K1][2C]: dims innermost first, strides in bytes
@@ -260,27 +299,34 @@ cudaError_t launch_gather_tma(const InterpArgs &a, const GatherBlocks &g, int ns
                               (cuuint64_t)nslice};
   const cuuint64_t row = (cuuint64_t)2 * a.C * 4;
   const cuuint64_t strides[3] = {row, row * a.g.K[0], row * a.g.K[0] * a.g.K[1]};
-  const cuuint32_t box[4] = {2 * TG_CW, TG_TW, TG_TW, 1};
+  const cuuint32_t box[4] = {(cuuint32_t)(2 * tcw), TG_TW, TG_TW, 1};
   const cuuint32_t estr[4] = {1, 1, 1, 1};
   CUresult r = enc(&tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<float2 *>(ck), dims, strides,
                    box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
-  const size_t smem = 2 * (size_t)TG_STAGE + 2 * sizeof(uint64_t);
-  auto kern = a.real_tab ? gather_tma_kernel<true> : gather_tma_kernel<false>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  int dev = 0, nsm = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  long long ctas = (long long)nsm * 2;
-  if (ctas > nit) ctas = nit;
-  const unsigned nchunk = (unsigned)((a.C + TG_CW - 1) / TG_CW);
-  // the test of the bounded waits: no copies, and a short wait limit
-  const long long limit = fault_test ? TG_TEST_WAIT_LIMIT : TG_WAIT_LIMIT;
-  kern<<<dim3((unsigned)ctas, nchunk), TG_THREADS, smem, st>>>(tm, a, g, it0, nit, ck, fm, fault,
-                                                              fault_test ? 1 : 0, limit);
-  return cudaGetLastError();
+  auto go = [&](auto kern, unsigned stage, int per_sm, int cw) -> cudaError_t {
+    const size_t smem = 2 * (size_t)stage + 2 * sizeof(uint64_t) + 2 * sizeof(int);
+    cudaError_t e =
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int dev = 0, nsm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    long long ctas = (long long)nsm * per_sm;
+    if (ctas > nit) ctas = nit;
+    const unsigned nchunk = (unsigned)((a.C + cw - 1) / cw);
+    // the test of the bounded waits: no copies, and a short wait limit
+    const long long limit = fault_test ? TG_TEST_WAIT_LIMIT : TG_WAIT_LIMIT;
+    kern<<<dim3((unsigned)ctas, nchunk), TG_THREADS, smem, st>>>(tm, a, g, it0, nit, ck, fm, fault,
+                                                                fault_test ? 1 : 0, limit);
+    return cudaGetLastError();
+  };
+  if (tcw == 32)
+    return go(a.real_tab ? gather_tma_kernel<true, 32> : gather_tma_kernel<false, 32>,
+              TgShape<32>::STAGE, TgShape<32>::CTAS_PER_SM, 32);
+  return go(a.real_tab ? gather_tma_kernel<true, 16> : gather_tma_kernel<false, 16>,
+            TgShape<16>::STAGE, TgShape<16>::CTAS_PER_SM, 16);
 }
 
 }  // namespace mirt

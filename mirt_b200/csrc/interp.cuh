@@ -153,10 +153,12 @@ struct Launch {
 // grouped by gb x gb blocks of their first taps; start[b] is the first
 // position of block b = (slice * nby + by) * nbx + bx (start[nblocks] = Mtot);
 // a work item (block, first position) covers up to gather_tma_item() samples
-// of one block, items in block order.
+// of one block, items in block order; orec[pos] = (caller's sample index, 0,
+// phase as float bits), staged with the tap records.
 struct GatherBlocks {
   const int *start;
   const int2 *item;
+  const int4 *orec;
   int gb, nbx, nby;
 };
 bool gather_tma_ok(const InterpArgs &a);
@@ -165,9 +167,10 @@ int gather_tma_item();
 // items [it0, it0 + nit) of a batch of nslice slices; *fault is set when a
 // stage does not arrive within the kernel's wait limit.  fault_test: the test
 // of that path (no copies are issued, every wait runs out, nothing computed).
+// tcw: coils per tile, 32 (a warp per sample) or 16 (a half-warp per sample).
 cudaError_t launch_gather_tma(const InterpArgs &a, const GatherBlocks &g, int nslice,
                               long long it0, long long nit, const float2 *ck, float2 *fm,
-                              int *fault, cudaStream_t st, int fault_test = 0);
+                              int *fault, cudaStream_t st, int fault_test = 0, int tcw = 32);
 
 // Compute the sort key of every sample: slice * nbins + bin of its first tap.
 cudaError_t launch_bin_keys(const InterpArgs &a, const Tiling &t, uint32_t *keys,

@@ -177,8 +177,9 @@ class InterpPlan:
 
     def set_gather(self, tma=True):
         """TMA-staged gather (2D, J = 6, even C >= 32) or the plain gather
-        (see mirt_interp_plan_set_gather)."""
-        check(self.lib.mirt_interp_plan_set_gather(self.handle, int(bool(tma))))
+        (see mirt_interp_plan_set_gather): True / 1 tiles of 32 coils, 2 tiles
+        of 16 coils, False / 0 the plain gather."""
+        check(self.lib.mirt_interp_plan_set_gather(self.handle, int(tma)))
         return self.config()
 
     def fault(self):
@@ -311,7 +312,7 @@ class NufftPlan:
     def set_gather(self, tma=True):
         """See InterpPlan.set_gather."""
         check(self.lib.mirt_interp_plan_set_gather(self.lib.mirt_nufft_interp_plan(self.handle),
-                                                   int(bool(tma))))
+                                                   int(tma)))
         return self.config()
 
     def fault(self):

@@ -81,7 +81,7 @@ def test_c2_interp_full_batch_vs_reference(c2_plan):
     import torch
     plan, cfg, om, moff, spokes = c2_plan
     # the benchmarked path: TMA-staged gather and row-sweep spread
-    assert cfg["gather_tma"] == 1 and cfg["spread_sweep"] != 0, cfg
+    assert cfg["gather_tma"] in (1, 2) and cfg["spread_sweep"] != 0, cfg
     w = fs.C2
     K = w["K"]
     gather, spread = _interp_calls(plan, torch)

@@ -23,7 +23,7 @@ def test_graph_replay_matches_eager(C):
                      slice_moff=moff)
     if C == 32:
         cfg = G.config()
-        assert cfg["gather_tma"] == 1 and cfg["spread_sweep"] != 0
+        assert cfg["gather_tma"] in (1, 2) and cfg["spread_sweep"] != 0
     x = torch.randn(G.image_shape, dtype=torch.complex64, device="cuda")
     X = torch.empty(G.sample_shape, dtype=torch.complex64, device="cuda")
     xa = torch.empty(G.image_shape, dtype=torch.complex64, device="cuda")

@@ -522,9 +522,14 @@ def test_tma_gather_matches_plain_gather_and_oracle(C, K):
     ckd = torch.from_numpy(ck.astype(np.complex64)).cuda()
     a = plan.forward(ckd).cpu().numpy()
     assert plan.fault() == 0
+    assert plan.set_gather(2)["gather_tma"] == 2  # tiles of 16 coils, a half-warp per sample
+    assert np.array_equal(plan.forward(ckd).cpu().numpy(), a)
+    assert plan.fault() == 0
     plan.set_gather(False)
     b = plan.forward(ckd).cpu().numpy()
     assert np.array_equal(a, b)
+    with pytest.raises(mb.MirtError, match="gather mode"):
+        plan.set_gather(3)
     for s in range(3):
         ref = oracle.interp_for(np.transpose(ck[s], (1, 0, 2)).reshape(-1, C, order="F"), h, J, L,
                                 tms[s], K, 0, impl=ref_impl())
@@ -546,6 +551,8 @@ def test_tma_gather_real_tables_phase_and_refusal():
     ck = rng.standard_normal((1, K[1], K[0], 32)) + 1j * rng.standard_normal((1, K[1], K[0], 32))
     ckd = torch.from_numpy(ck.astype(np.complex64)).cuda()
     a = plan.forward(ckd).cpu().numpy()
+    plan.set_gather(2)
+    assert np.array_equal(a, plan.forward(ckd).cpu().numpy())
     plan.set_gather(False)
     assert np.array_equal(a, plan.forward(ckd).cpu().numpy())
     ref = oracle.interp_for(np.transpose(ck[0], (1, 0, 2)).reshape(-1, 32, order="F"), h, J, L, tm,
@@ -640,13 +647,14 @@ def test_tma_gather_bounded_wait_fault_path():
     C = 32
     ck = rng.standard_normal((96 * 64, C)) + 1j * rng.standard_normal((96 * 64, C))
     ck_d = torch.from_numpy(ck.reshape(64, 96, C).astype(np.complex64)).cuda()[None]
-    plan = mb.InterpPlan(K, J, L, h, tm, C)
-    assert plan.config()["gather_tma"] == 1
-    plan.set_fault_test(True)
-    plan.forward(ck_d)
-    assert plan.fault() == 1
-    assert plan.fault() == 0
-    plan.close()                                # a faulted plan is discarded
+    for mode in (1, 2):                         # tiles of 32 and of 16 coils
+        plan = mb.InterpPlan(K, J, L, h, tm, C)
+        plan.set_gather(mode)
+        plan.set_fault_test(True)
+        plan.forward(ck_d)
+        assert plan.fault() == 1
+        assert plan.fault() == 0
+        plan.close()                            # a faulted plan is discarded
     plan = mb.InterpPlan(K, J, L, h, tm, C)
     got = plan.forward(ck_d).cpu().numpy()
     assert plan.fault() == 0
