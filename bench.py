@@ -632,6 +632,23 @@ def run_cgsense(args):
         torch.zeros_like(xref)
         torch.cuda.synchronize()
         res = {"N": N, "coils": C, "problems": len(idx)}
+        # the learned weights' two parts timed apart (CUDA events): features, then
+        # the MLP on the tensor cores and, for comparison, on the FP32 pipes
+        e_a = ev()
+        feat = ld.dcf_features(om_d, (model.K, model.K), moff)
+        e_b = ev()
+        model.mlp.infer(feat, model.mu, model.sigma)
+        e_c = ev()
+        model.mlp.set_tensor_cores(False)
+        e_d = ev()
+        model.mlp.infer(feat, model.mu, model.sigma)
+        e_e = ev()
+        model.mlp.set_tensor_cores(True)
+        torch.cuda.synchronize()
+        res.update({"samples": int(moff[-1]), "dcf_features_ms": e_a.elapsed_time(e_b),
+                    "mlp_tensor_core_ms": e_b.elapsed_time(e_c),
+                    "mlp_fp32_pipes_ms": e_d.elapsed_time(e_e)})
+        del feat
         for mode in modes:
             e0 = ev()
             if mode in ("plain", "precon_only", "precon_toeplitz"):
@@ -666,6 +683,9 @@ def run_cgsense(args):
     for k in modes:
         out[f"{k}_s"] = tot[k] if reached[k] else None
     out.update({
+        "dcf_features_ms": sum(r["dcf_features_ms"] for r in per),
+        "mlp_tensor_core_ms": sum(r["mlp_tensor_core_ms"] for r in per),
+        "mlp_fp32_pipes_ms": sum(r["mlp_fp32_pipes_ms"] for r in per),
         "plan_and_toeplitz_setup_s": setup_s,
         "reference": f"{args.cg_ref} preconditioned CG iterations from zero (FP32 operators, "
                      "FP64 inner products; within 1e-4 of the FP64 solution on the parity cases)",

@@ -524,7 +524,12 @@ int mirt_dcf_features(const double *om, int64_t M, const int64_t *slice_moff, in
  *            `batch` rows drawn by a counter-based hash of (seed, step, row);
  *            loss_hist (host, `steps` floats, or NULL) gets each step's loss
  *   infer    yhat = network output (device FP32 [n], or NULL) and / or
- *            w = exp(sigma * yhat + mu) (device FP64 [n], or NULL); async */
+ *            w = exp(sigma * yhat + mu) (device FP64 [n], or NULL); async.
+ *            On the tensor cores (mma.sync m16n8k16 BF16, FP32 accumulation;
+ *            each FP32 activation enters as three BF16 terms, so the result
+ *            keeps FP32 accuracy: ~3e-8 relative to FP64 on random weights)
+ *   set_tensor_cores  0: inference on the FP32 pipes instead (the training
+ *            kernels' forward), 1 (the default): on the tensor cores */
 #define MIRT_MLP_NPARAM 9601
 typedef struct mirt_mlp mirt_mlp;
 int mirt_mlp_create(mirt_mlp **out, const float *params);
@@ -535,6 +540,7 @@ int mirt_mlp_train(mirt_mlp *m, const float *x, const float *y, int64_t n, int32
 	int32_t steps, float lr, uint64_t seed, float *loss_hist, void *stream);
 int mirt_mlp_infer(mirt_mlp *m, const float *x, int64_t n, float mu, float sigma, float *yhat,
 	double *w, void *stream);
+int mirt_mlp_set_tensor_cores(mirt_mlp *m, int32_t on);
 int mirt_mlp_destroy(mirt_mlp *m);
 
 /* ------------------------------------------------------------------------

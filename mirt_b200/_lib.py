@@ -96,6 +96,7 @@ _SIGS = {
     "mirt_mlp_train": ([_vp, _vp, _vp, _i64, _i32, _i32, C.c_float, C.c_uint64,
                         C.POINTER(C.c_float), _vp], C.c_int),
     "mirt_mlp_infer": ([_vp, _vp, _i64, C.c_float, C.c_float, _vp, _vp, _vp], C.c_int),
+    "mirt_mlp_set_tensor_cores": ([_vp, _i32], C.c_int),
     "mirt_mlp_destroy": ([_vp], C.c_int),
     "mirt_interp_plan_destroy": ([_vp], C.c_int),
     "mirt_nufft_create": ([C.POINTER(_vp), _i32, _i32p, _i32p, _i32p, _i32p, _dp, _dp, _i64,

@@ -1,7 +1,8 @@
 // mlp.cu -- the density-compensation regressor: a multilayer perceptron
 // 18 -> 64 -> 64 -> 64 -> 1 (ReLU), BF16 weights, FP32 activations and
 // accumulation, trained on the device by hand-written forward / backward
-// kernels with Adam on FP32 master weights.
+// kernels with Adam on FP32 master weights; inference on the tensor cores
+// (mlp_infer_mma_kernel).
 //
 // Parameters, one flat FP32 vector (row-major, out x in):
 //   W1[64][18] b1[64] W2[64][64] b2[64] W3[64][64] b3[64] W4[64] b4
@@ -340,6 +341,187 @@ __global__ void __launch_bounds__(NT) mlp_infer_kernel(const float *__restrict__
   }
 }
 
+// ------------------------------------------------------------------------
+// Inference on the tensor cores: mma.sync m16n8k16, BF16 operands, FP32
+// accumulation.  A warp takes 16 samples at a time; the weights are exact
+// BF16 (B operands, row-major W[out][in] is the column-major B the
+// instruction wants), the FP32 activations enter as the sum of NTERM BF16
+// terms (hi, then the BF16 rounding of each remainder), smallest term first,
+// so that the products carry the activations to about 8 NTERM bits.  The D
+// fragments of n-tiles 2k and 2k+1 are the A fragment of k-tile k of the next
+// layer, so the activations stay in registers from layer to layer.
+// Fragment layout (PTX ISA, m16n8k16 .bf16): g = lane / 4, t = lane % 4;
+// A: a0 (row g, cols 2t, 2t+1), a1 (row g + 8), a2 (cols 2t + 8, 2t + 9),
+// a3 (row g + 8, cols 2t + 8, 2t + 9); B: b0 (k 2t, 2t+1; n g), b1 (k 2t + 8,
+// 2t + 9; n g); C/D: c0, c1 (row g, cols 2t, 2t+1), c2, c3 (row g + 8).
+constexpr int MW1 = 40;  // W1 rows in shared memory: 18 inputs, zero-padded to 32, + 8 pad
+constexpr int MWH = 72;  // W2, W3 rows: 64 + 8 pad (conflict-free B loads)
+
+__device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], uint32_t b0,
+                                         uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+      "{%8,%9}, {%0,%1,%2,%3};"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(__nv_bfloat16 lo, __nv_bfloat16 hi) {
+  return (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
+}
+
+// the NTERM BF16 terms of (v0, v1) packed as pairs, term 0 the largest
+template <int NTERM>
+__device__ __forceinline__ void split_pair(float v0, float v1, uint32_t (&t)[NTERM]) {
+#pragma unroll
+  for (int k = 0; k < NTERM; k++) {
+    const __nv_bfloat16 h0 = __float2bfloat16_rn(v0), h1 = __float2bfloat16_rn(v1);
+    t[k] = pack_bf16(h0, h1);
+    v0 -= __bfloat162float(h0);
+    v1 -= __bfloat162float(h1);
+  }
+}
+
+// A fragments (NTERM terms) of k-tile kt from the previous layer's D fragments
+template <int NTERM>
+__device__ __forceinline__ void a_from_d(const float (&h)[8][4], int kt, uint32_t (&a)[NTERM][4]) {
+  uint32_t t0[NTERM], t1[NTERM], t2[NTERM], t3[NTERM];
+  split_pair<NTERM>(h[2 * kt][0], h[2 * kt][1], t0);
+  split_pair<NTERM>(h[2 * kt][2], h[2 * kt][3], t1);
+  split_pair<NTERM>(h[2 * kt + 1][0], h[2 * kt + 1][1], t2);
+  split_pair<NTERM>(h[2 * kt + 1][2], h[2 * kt + 1][3], t3);
+#pragma unroll
+  for (int k = 0; k < NTERM; k++) {
+    a[k][0] = t0[k];
+    a[k][1] = t1[k];
+    a[k][2] = t2[k];
+    a[k][3] = t3[k];
+  }
+}
+
+// out[8][4] = bias + A W^T over KT k-tiles (A given per k-tile by `afrag`)
+template <int NTERM, int KT, int LDW, class AF>
+__device__ __forceinline__ void mma_layer(const __nv_bfloat16 *__restrict__ W, const float *bias,
+                                          AF afrag, float (&out)[8][4]) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+#pragma unroll
+  for (int nt = 0; nt < 8; nt++) {
+    const float b0 = bias[nt * 8 + 2 * t], b1 = bias[nt * 8 + 2 * t + 1];
+    out[nt][0] = b0;
+    out[nt][1] = b1;
+    out[nt][2] = b0;
+    out[nt][3] = b1;
+  }
+#pragma unroll
+  for (int kt = 0; kt < KT; kt++) {
+    uint32_t a[NTERM][4];
+    afrag(kt, a);
+#pragma unroll
+    for (int nt = 0; nt < 8; nt++) {
+      const __nv_bfloat16 *wr = W + (nt * 8 + g) * LDW + kt * 16 + 2 * t;
+      const uint32_t b0 = *reinterpret_cast<const uint32_t *>(wr);
+      const uint32_t b1 = *reinterpret_cast<const uint32_t *>(wr + 8);
+#pragma unroll
+      for (int k = NTERM - 1; k >= 0; k--) mma_bf16(out[nt], a[k], b0, b1);
+    }
+  }
+}
+
+__device__ __forceinline__ void relu8(float (&h)[8][4]) {
+#pragma unroll
+  for (int nt = 0; nt < 8; nt++)
+#pragma unroll
+    for (int e = 0; e < 4; e++) h[nt][e] = fmaxf(h[nt][e], 0.f);
+}
+
+template <int NTERM>
+__global__ void __launch_bounds__(NT, 2) mlp_infer_mma_kernel(const float *__restrict__ x, long long n,
+                                                           const __nv_bfloat16 *__restrict__ wb,
+                                                           float mu, float sigma,
+                                                           float *__restrict__ yhat,
+                                                           double *__restrict__ wout) {
+  __shared__ __align__(16) __nv_bfloat16 sW1[HID * MW1];
+  __shared__ __align__(16) __nv_bfloat16 sW2[HID * MWH];
+  __shared__ __align__(16) __nv_bfloat16 sW3[HID * MWH];
+  __shared__ float sb1[HID], sb2[HID], sb3[HID], sW4[HID];
+  __shared__ float sb4;
+  for (int e = threadIdx.x; e < HID * 32; e += NT) {
+    const int r = e / 32, k = e % 32;
+    sW1[r * MW1 + k] = k < NIN ? wb[P_W1 + r * NIN + k] : __float2bfloat16_rn(0.f);
+  }
+  for (int e = threadIdx.x; e < HID * HID; e += NT) {
+    sW2[(e / HID) * MWH + e % HID] = wb[P_W2 + e];
+    sW3[(e / HID) * MWH + e % HID] = wb[P_W3 + e];
+  }
+  for (int e = threadIdx.x; e < HID; e += NT) {
+    sb1[e] = __bfloat162float(wb[P_B1 + e]);
+    sb2[e] = __bfloat162float(wb[P_B2 + e]);
+    sb3[e] = __bfloat162float(wb[P_B3 + e]);
+    sW4[e] = __bfloat162float(wb[P_W4 + e]);
+  }
+  if (threadIdx.x == 0) sb4 = __bfloat162float(wb[P_B4]);
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  const long long ngrp = (n + 15) / 16;
+  for (long long grp = (long long)blockIdx.x * (NT / 32) + warp; grp < ngrp;
+       grp += (long long)gridDim.x * (NT / 32)) {
+    const long long r0 = grp * 16 + g, r1 = r0 + 8;
+    // the features of rows r0, r1 at this lane's columns (zero past 18 and past n)
+    auto feat = [&](long long r, int k) -> float {
+      return (r < n && k < NIN) ? __ldg(x + r * NIN + k) : 0.f;
+    };
+    float h1[8][4], h2[8][4];
+    mma_layer<NTERM, 2, MW1>(sW1, sb1, [&](int kt, uint32_t (&a)[NTERM][4]) {
+      const int k0 = kt * 16 + 2 * t;
+      uint32_t t0[NTERM], t1[NTERM], t2[NTERM], t3[NTERM];
+      split_pair<NTERM>(feat(r0, k0), feat(r0, k0 + 1), t0);
+      split_pair<NTERM>(feat(r1, k0), feat(r1, k0 + 1), t1);
+      split_pair<NTERM>(feat(r0, k0 + 8), feat(r0, k0 + 9), t2);
+      split_pair<NTERM>(feat(r1, k0 + 8), feat(r1, k0 + 9), t3);
+#pragma unroll
+      for (int k = 0; k < NTERM; k++) {
+        a[k][0] = t0[k];
+        a[k][1] = t1[k];
+        a[k][2] = t2[k];
+        a[k][3] = t3[k];
+      }
+    }, h1);
+    relu8(h1);
+    mma_layer<NTERM, 4, MWH>(sW2, sb2, [&](int kt, uint32_t (&a)[NTERM][4]) {
+      a_from_d<NTERM>(h1, kt, a);
+    }, h2);
+    relu8(h2);
+    mma_layer<NTERM, 4, MWH>(sW3, sb3, [&](int kt, uint32_t (&a)[NTERM][4]) {
+      a_from_d<NTERM>(h2, kt, a);
+    }, h1);
+    relu8(h1);
+    // output unit: the quad of lanes sharing g holds all 64 columns of rows r0, r1
+    float o0 = 0.f, o1 = 0.f;
+#pragma unroll
+    for (int nt = 0; nt < 8; nt++) {
+      const float w0 = sW4[nt * 8 + 2 * t], w1 = sW4[nt * 8 + 2 * t + 1];
+      o0 = fmaf(w0, h1[nt][0], fmaf(w1, h1[nt][1], o0));
+      o1 = fmaf(w0, h1[nt][2], fmaf(w1, h1[nt][3], o1));
+    }
+    o0 += __shfl_xor_sync(0xffffffffu, o0, 1);
+    o1 += __shfl_xor_sync(0xffffffffu, o1, 1);
+    o0 += __shfl_xor_sync(0xffffffffu, o0, 2);
+    o1 += __shfl_xor_sync(0xffffffffu, o1, 2);
+    if (t == 0) {
+      o0 += sb4;
+      o1 += sb4;
+      if (r0 < n) {
+        if (yhat) yhat[r0] = o0;
+        if (wout) wout[r0] = exp((double)sigma * (double)o0 + (double)mu);
+      }
+      if (r1 < n) {
+        if (yhat) yhat[r1] = o1;
+        if (wout) wout[r1] = exp((double)sigma * (double)o1 + (double)mu);
+      }
+    }
+  }
+}
+
 constexpr size_t kGradSmem = sizeof(Weights) + sizeof(Acts) + sizeof(Errs);
 constexpr size_t kInferSmem = sizeof(Weights) + sizeof(Acts);
 
@@ -348,6 +530,7 @@ constexpr size_t kInferSmem = sizeof(Weights) + sizeof(Acts);
 struct mirt_mlp {
   DMem master, m, v, wb, part, loss_part, step, grad, losses, idx;
   int nblk_cap = 0;
+  int tensor_cores = 1;  // inference on mma.sync (1) or on the FP32 pipes (0)
   float lr = 1e-3f, beta1 = 0.9f, beta2 = 0.999f, eps = 1e-8f;
 };
 
@@ -547,11 +730,25 @@ int mirt_mlp_infer(mirt_mlp *q, const float *x, int64_t n, float mu, float sigma
   if (n < 0) return api_fail(MIRT_ERR_ARG, "n must be >= 0");
   if (n == 0) return MIRT_OK;
   cudaStream_t st = as_stream(stream);
-  long long nb = (n + NS - 1) / NS;
-  if (nb > 148 * 8) nb = 148 * 8;
-  mlp_infer_kernel<<<(unsigned)nb, NT, kInferSmem, st>>>(x, n, q->wb.as<__nv_bfloat16>(), mu,
+  if (q->tensor_cores) {
+    // tensor-core inference: 8 warps of 16 samples per CTA and pass
+    long long nb = (n + 127) / 128;
+    if (nb > 148 * 8) nb = 148 * 8;
+    mlp_infer_mma_kernel<3><<<(unsigned)nb, NT, 0, st>>>(x, n, q->wb.as<__nv_bfloat16>(), mu,
                                                           sigma, yhat, w);
+  } else {
+    long long nb = (n + NS - 1) / NS;
+    if (nb > 148 * 8) nb = 148 * 8;
+    mlp_infer_kernel<<<(unsigned)nb, NT, kInferSmem, st>>>(x, n, q->wb.as<__nv_bfloat16>(), mu,
+                                                            sigma, yhat, w);
+  }
   MCK(cudaGetLastError());
+  return MIRT_OK;
+}
+
+int mirt_mlp_set_tensor_cores(mirt_mlp *q, int32_t on) {
+  if (!q) return api_fail(MIRT_ERR_ARG, "NULL argument");
+  q->tensor_cores = on ? 1 : 0;
   return MIRT_OK;
 }
 

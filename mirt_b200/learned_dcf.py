@@ -122,6 +122,10 @@ class DcfMLP:
                                           _stream_ptr(stream)))
         return w
 
+    def set_tensor_cores(self, on=True):
+        """Inference on the tensor cores (the default) or on the FP32 pipes."""
+        check(self.lib.mirt_mlp_set_tensor_cores(self.handle, int(bool(on))))
+
     def close(self):
         if getattr(self, "handle", None):
             self.lib.mirt_mlp_destroy(self.handle)

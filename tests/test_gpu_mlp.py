@@ -49,9 +49,16 @@ def test_forward_and_gradient_match_oracle():
     x = rng.standard_normal((n, mlp_ref.NFEAT)).astype(np.float32)
     y = rng.standard_normal(n).astype(np.float32)
     net = mb.DcfMLP(p)
-    out = net.infer(_dev(x), weights=False).cpu().numpy()
+    out = net.infer(_dev(x), weights=False).cpu().numpy()   # tensor cores (3 BF16 terms)
     ref_out, _ = mlp_ref.forward(p, x)
     assert rel_l2(out, ref_out) <= 1e-5
+    net.set_tensor_cores(False)                             # the FP32 pipes
+    out32 = net.infer(_dev(x), weights=False).cpu().numpy()
+    assert rel_l2(out32, ref_out) <= 1e-5
+    net.set_tensor_cores(True)
+    for n_odd in (1, 15, 17, 129):                          # partial groups of 16 and CTAs of 128
+        o = net.infer(_dev(x[:n_odd]), weights=False).cpu().numpy()
+        assert rel_l2(o, ref_out[:n_odd]) <= 1e-5, n_odd
     loss, g = net.grad(_dev(x), _dev(y))
     ref_loss, ref_g = mlp_ref.grad(p, x, y)
     assert abs(loss - ref_loss) <= 1e-5 * ref_loss
