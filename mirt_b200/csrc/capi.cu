@@ -2112,14 +2112,36 @@ int nufft_finish(mirt_nufft *p, int D, const int32_t *Nd, const int32_t *Kd, con
   for (int d = 0; d < D; d++)
     if (!fft_len_ok(Kd[d])) p->own_fft = false;
   if (p->own_fft) {
-    // fused FFT passes over the interpolation grid: twiddles exp(-2 pi i k / K_d) in FP64
+    // fused FFT passes over the interpolation grid.  Stage-1 twiddles per
+    // dimension and direction, [q][p1], in FP64: forward exp(-2 pi i p1 q / K)
+    // and adjoint exp(+2 pi i p1 q / K); a grid phase of quarter turns i^(k m)
+    // is folded in (forward: times i^(p1 m), adjoint: times i^(-q m))
+    int qm[3] = {0, 0, 0};
+    bool fold = any_mid;
+    for (int d = 0; d < D && fold; d++) {
+      const long long m4 = 4ll * (nmid ? nmid[d] : 0);
+      if (m4 % Kd[d] != 0) fold = false;
+      else qm[d] = (int)(((m4 / Kd[d]) % 4 + 4) % 4);
+    }
     std::vector<float2> tw;
-    long long off[3] = {0, 0, 0};
+    long long offf[3] = {0, 0, 0}, offa[3] = {0, 0, 0};
+    auto rot = [](float2 w, int e) {  // w * i^e, exact
+      for (int r = 0; r < (e & 3); r++) w = make_float2(-w.y, w.x);
+      return w;
+    };
     for (int d = 0; d < D; d++) {
-      off[d] = (long long)tw.size();
-      for (int k = 0; k < Kd[d]; k++) {
-        const double a = 2 * M_PI * (double)k / Kd[d];
-        tw.push_back(make_float2((float)std::cos(a), (float)-std::sin(a)));
+      int r1 = 0, r2 = 0;
+      fft_radix(Kd[d], &r1, &r2);
+      for (int dir = 0; dir < 2; dir++) {
+        (dir ? offa : offf)[d] = (long long)tw.size();
+        for (int q = 0; q < r2; q++)
+          for (int p1 = 0; p1 < r1; p1++) {
+            const long long j = ((long long)p1 * q) % Kd[d];
+            const double a = 2 * M_PI * (double)j / Kd[d];
+            float2 w = make_float2((float)std::cos(a), (float)(dir ? std::sin(a) : -std::sin(a)));
+            if (fold) w = rot(w, dir ? -(q * qm[d]) : p1 * qm[d]);
+            tw.push_back(w);
+          }
       }
     }
     cudaError_t e = p->twtab.alloc(tw.size() * sizeof(float2));
@@ -2132,7 +2154,11 @@ int nufft_finish(mirt_nufft *p, int D, const int32_t *Nd, const int32_t *Kd, con
     if (e != cudaSuccess) return fail(MIRT_ERR_ALLOC, "NUFFT grid buffers");
     p->nf.g = p->gg;
     p->nf.C = ncol;
-    for (int d = 0; d < 3; d++) p->nf.tw[d] = d < D ? p->twtab.as<float2>() + off[d] : nullptr;
+    for (int d = 0; d < 3; d++) {
+      p->nf.twf[d] = d < D ? p->twtab.as<float2>() + offf[d] : nullptr;
+      p->nf.twa[d] = d < D ? p->twtab.as<float2>() + offa[d] : nullptr;
+    }
+    p->nf.phase_folded = fold ? 1 : 0;
     p->nf.sn = p->sn.as<float2>();
     p->nf.gp = &p->gp;
     return MIRT_OK;

@@ -166,15 +166,19 @@ __device__ __forceinline__ void dft_half_out(float2 *x) {
 }
 
 // ---- the pass kernel ---------------------------------------------------------
-// PRUNE: forward with nin <= n/2, or inverse with nout <= n/2.
-template <int R1, int R2, bool INV, bool PRUNE>
-__global__ void __launch_bounds__(kThreads) fft_pass_kernel(FftPass P, int lpb, int pitch) {
-  constexpr int N = R1 * R2;
+// PRUNE: forward with nin <= n/2, or inverse with nout <= n/2.  VW: the vector
+// width at compile time (16) with the element counts exactly the transform's
+// (nin = n/2 pruned or n, nout = n/2 pruned or n: no bounds tests), or 0 (any
+// width and counts, read from the pass).
+template <int R1, int R2, bool INV, bool PRUNE, int VW>
+__global__ void __launch_bounds__(kThreads) fft_pass_kernel(FftPass P, int lpb, int pitch_rt) {
+  constexpr bool EXACT = VW != 0;
   extern __shared__ __align__(16) float2 sm[];
   __shared__ long long base_in[kMaxLpb], base_out[kMaxLpb];
   __shared__ int snrow[kMaxLpb];
-  const int vw = P.vw;
-  const int lvw = __ffs(vw) - 1;
+  const int vw = VW ? VW : P.vw;
+  const int lvw = VW ? (VW == 16 ? 4 : __ffs(VW) - 1) : __ffs(vw) - 1;
+  const int pitch = VW ? R2 * VW : pitch_rt;
   const int nlines = P.nslice * P.nr2 * P.nr1 * P.nvec;
   const int g0 = blockIdx.x * lpb;
   if (threadIdx.x < lpb) {
@@ -201,6 +205,7 @@ __global__ void __launch_bounds__(kThreads) fft_pass_kernel(FftPass P, int lpb, 
   // stage 1
   constexpr int KH = (PRUNE && !INV) ? R1 / 2 : R1;
   const int n1 = (lpb * R2) << lvw;
+#pragma unroll 1
   for (int i = threadIdx.x; i < n1; i += kThreads) {
     const int v = i & (vw - 1);
     const int q = (i >> lvw) % R2;
@@ -213,14 +218,14 @@ __global__ void __launch_bounds__(kThreads) fft_pass_kernel(FftPass P, int lpb, 
     for (int k1 = 0; k1 < R1; k1++) {
       const int k = R2 * k1 + q;
       x[k1] = make_float2(0.f, 0.f);
-      if (k1 < KH && k < P.nin) x[k1] = src[(long long)k * P.es_in];
+      if (k1 < KH && (EXACT || k < P.nin)) x[k1] = src[(long long)k * P.es_in];
     }
     if (P.sn_in) {
-      const float2 *sr = P.sn_in + (long long)snrow[g] * P.nin;
+      const float2 *sr = P.sn_in + (long long)snrow[g] * P.nin + q;
 #pragma unroll
       for (int k1 = 0; k1 < KH; k1++) {
         const int k = R2 * k1 + q;
-        if (k < P.nin) x[k1] = cmul(x[k1], __ldg(sr + k));
+        if (EXACT || k < P.nin) x[k1] = cmul(x[k1], __ldg(sr + R2 * k1));
       }
     }
     if (P.ph_in) {
@@ -232,11 +237,15 @@ __global__ void __launch_bounds__(kThreads) fft_pass_kernel(FftPass P, int lpb, 
     } else {
       Dft<R1, INV>::run(x);
     }
+    {
+      // this column's twiddles, two per 16-byte load
+      const float4 *tw4 = reinterpret_cast<const float4 *>(P.tw) + q * (R1 / 2);
 #pragma unroll
-    for (int p1 = 1; p1 < R1; p1++) {
-      float2 t = __ldg(P.tw + ((p1 * q) & (N - 1)));
-      if (INV) t.y = -t.y;
-      x[p1] = cmul(x[p1], t);
+      for (int j = 0; j < R1 / 2; j++) {
+        const float4 t = __ldg(tw4 + j);
+        if (j > 0 || !P.tw_unit0) x[2 * j] = cmul(x[2 * j], make_float2(t.x, t.y));
+        x[2 * j + 1] = cmul(x[2 * j + 1], make_float2(t.z, t.w));
+      }
     }
     float2 *d = sm + (size_t)(g * R1) * pitch + (q << lvw) + v;
 #pragma unroll
@@ -247,6 +256,7 @@ __global__ void __launch_bounds__(kThreads) fft_pass_kernel(FftPass P, int lpb, 
   // stage 2
   constexpr int PH = (PRUNE && INV) ? R2 / 2 : R2;
   const int n2 = (lpb * R1) << lvw;
+#pragma unroll 1
   for (int i = threadIdx.x; i < n2; i += kThreads) {
     const int v = i & (vw - 1);
     const int p1 = (i >> lvw) % R1;
@@ -264,14 +274,19 @@ __global__ void __launch_bounds__(kThreads) fft_pass_kernel(FftPass P, int lpb, 
     }
     float2 *dst = P.out + bo + v;
     const float2 *sr = P.sn_out ? P.sn_out + (long long)snrow[g] * P.nout : nullptr;
+    if (EXACT && !sr && !P.ph_out) {
 #pragma unroll
-    for (int p2 = 0; p2 < PH; p2++) {
-      const int p = p1 + R1 * p2;
-      if (p < P.nout) {
-        float2 val = y[p2];
-        if (P.ph_out) val = cmul(val, __ldg(P.ph_out + p));
-        if (sr) val = cmulc(__ldg(sr + p), val);
-        dst[(long long)p * P.es_out] = val;
+      for (int p2 = 0; p2 < PH; p2++) dst[(long long)(p1 + R1 * p2) * P.es_out] = y[p2];
+    } else {
+#pragma unroll
+      for (int p2 = 0; p2 < PH; p2++) {
+        const int p = p1 + R1 * p2;
+        if (EXACT || p < P.nout) {
+          float2 val = y[p2];
+          if (P.ph_out) val = cmul(val, __ldg(P.ph_out + p));
+          if (sr) val = cmulc(__ldg(sr + p), val);
+          dst[(long long)p * P.es_out] = val;
+        }
       }
     }
   }
@@ -296,11 +311,21 @@ cudaError_t launch_r(const FftPass &P, cudaStream_t st) {
     kern<<<grid, kThreads, smem, st>>>(P, lpb, pitch);
     return cudaGetLastError();
   };
-  if (P.inverse)
-    return prune ? pick(fft_pass_kernel<R1, R2, true, true>)
-                 : pick(fft_pass_kernel<R1, R2, true, false>);
-  return prune ? pick(fft_pass_kernel<R1, R2, false, true>)
-               : pick(fft_pass_kernel<R1, R2, false, false>);
+  // the exact form: 16-wide vectors, inputs and outputs exactly the (pruned) halves or all n
+  const int hin = prune && !P.inverse ? P.n / 2 : P.n, hout = prune && P.inverse ? P.n / 2 : P.n;
+  const bool exact = vw == 16 && P.nin == hin && P.nout == hout;
+  if (P.inverse) {
+    if (exact)
+      return prune ? pick(fft_pass_kernel<R1, R2, true, true, 16>)
+                   : pick(fft_pass_kernel<R1, R2, true, false, 16>);
+    return prune ? pick(fft_pass_kernel<R1, R2, true, true, 0>)
+                 : pick(fft_pass_kernel<R1, R2, true, false, 0>);
+  }
+  if (exact)
+    return prune ? pick(fft_pass_kernel<R1, R2, false, true, 16>)
+                 : pick(fft_pass_kernel<R1, R2, false, false, 16>);
+  return prune ? pick(fft_pass_kernel<R1, R2, false, true, 0>)
+               : pick(fft_pass_kernel<R1, R2, false, false, 0>);
 }
 
 // largest power of two dividing v, at most 16
@@ -316,8 +341,9 @@ FftPass base_pass(const NufftFft &f, int d, int s0, int s1, bool inverse) {
   p.nr1 = p.nr2 = 1;
   p.n = f.g.K[d];
   p.inverse = inverse ? 1 : 0;
-  p.tw = f.tw[d];
-  const float2 *ph = (f.gp && f.gp->tab[0]) ? f.gp->tab[d] : nullptr;
+  p.tw = inverse ? f.twa[d] : f.twf[d];
+  p.tw_unit0 = !inverse || !f.phase_folded;  // entry p1 = 0 is 1 for every column
+  const float2 *ph = (f.gp && f.gp->tab[0] && !f.phase_folded) ? f.gp->tab[d] : nullptr;
   if (inverse)
     p.ph_in = ph;
   else
@@ -341,6 +367,20 @@ cudaError_t launch_fft_pass(const FftPass &p, cudaStream_t st) {
     case 1024: return launch_r<32, 32>(p, st);
     default: return cudaErrorInvalidValue;
   }
+}
+
+void fft_radix(int n, int *r1, int *r2) {
+  int a = 0, b = 0;
+  switch (n) {
+    case 64: a = 8, b = 8; break;
+    case 128: a = 8, b = 16; break;
+    case 256: a = 16, b = 16; break;
+    case 512: a = 16, b = 32; break;
+    case 1024: a = 32, b = 32; break;
+    default: break;
+  }
+  *r1 = a;
+  *r2 = b;
 }
 
 int fft_nufft_passes(const NufftFft &f) { return f.g.D; }

@@ -34,7 +34,11 @@ struct FftPass {
   long long is[3], os[3], es_in, es_out;
   int n, nin, nout;
   int inverse;               // 0: exp(-2 pi i k p / n); 1: exp(+...), unnormalised
-  const float2 *tw;          // exp(-2 pi i k / n), k < n (FP64-built)
+  // stage-1 twiddles, [q][p1] (q < R2, p1 < R1 for n = R1 R2, fft_radix):
+  // W^{p1 q}, W = exp(-+2 pi i / n) in the pass's direction, times any grid
+  // phase folded in (FP64-built; see NufftFft)
+  const float2 *tw;
+  int tw_unit0;              // 1: the twiddle of p1 = 0 is 1 in every column (skipped)
   // deapodisation: sn_in scales input k of line (r2, r1) by sn[(r2*nr1 + r1)*nin + k];
   // sn_out scales output p by conj(sn[(r2*nr1 + r1)*nout + p])
   const float2 *sn_in, *sn_out;
@@ -42,20 +46,30 @@ struct FftPass {
   const float2 *ph_out, *ph_in;
 };
 
-// Transform lengths the passes handle (powers of two from 64 to 1024).
+// Transform lengths the passes handle (powers of two from 64 to 1024), and
+// the two radices n = R1 R2 of a length.
 bool fft_len_ok(int n);
+void fft_radix(int n, int *r1, int *r2);
 
 cudaError_t launch_fft_pass(const FftPass &p, cudaStream_t st);
 
 // Geometry of the NUFFT's FFT: image N, grid K, C columns, per-dimension
-// twiddle tables (device, FP64-built), the deapodisation sn [npix] and the
-// optional grid phase.
+// stage-1 twiddle tables of the forward and the adjoint passes (device,
+// FP64-built), the deapodisation sn [npix] and the optional grid phase.
+// When the grid phase is a sequence of quarter turns, exp(2 pi i k Nmid / K)
+// = i^(k m) with m = 4 Nmid / K an integer (K = 2N, Nmid = N/2: m = 1), it is
+// folded into the twiddles: the forward pass's output p = p1 + R1 p2 turns by
+// i^(p1 m) (R1 is a multiple of 4), the same for every output of a stage-2
+// thread, and the adjoint pass's input k = R2 k1 + q by i^(-q m), the same for
+// every input of a stage-1 thread; both are exact rotations and pass through
+// the linear DFT stages.  phase_folded = 1: no phase multiplies in the passes.
 struct NufftFft {
   GlueGeom g;
   int C;
-  const float2 *tw[3];
+  const float2 *twf[3], *twa[3];
   const float2 *sn;
   const GridPhase *gp;       // null or tab[0] null: no grid phase
+  int phase_folded;
 };
 
 // fftn(x .* sn, K) of slices [s0, s1): x [s][n][c] -> grid [s][k][c]
