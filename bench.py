@@ -440,12 +440,18 @@ def run_gpu(args, w):
     achieved = B / tdom / 1e9
     variant = {"spread": "sweep" if tuned.get("spread_sweep", 0) != 0 else "tiled",
                "gather": "tma" if tuned.get("gather_tma", 0) else "plain"}
+    rows, staged = tuned.get("spread_sweep_rows", 1), tuned.get("spread_staged", 0)
     if D == 3:
         sweep_kernel = "spread_sweep3_kernel"
+    elif staged == 2:
+        sweep_kernel = f"spread_sweep2s_kernel rows={rows} (caller-order samples)"
+    elif staged == 1:
+        sweep_kernel = f"sweep_order_kernel + spread_sweep2s_kernel rows={rows}"
     else:
-        sweep_kernel = (f"sweep_order_kernel + spread_sweep_kernel "
-                        f"rows={tuned.get('spread_sweep_rows', 1)}")
-    kernels = {"gather": ("gather_tma_kernel" if variant["gather"] == "tma" else "gather_kernel"),
+        sweep_kernel = f"sweep_order_kernel + spread_sweep_kernel rows={rows}"
+    tma_coils = 16 if tuned.get("gather_tma", 0) == 2 else 32
+    kernels = {"gather": (f"gather_tma_kernel ({tma_coils}-coil tiles)" if variant["gather"] == "tma"
+                          else "gather_kernel"),
                "spread": (sweep_kernel if variant["spread"] == "sweep"
                           else "spread_kernel (+ spread_reduce_kernel)")}
     traffic, traffic_src = traffic_from_profiles(args.workload, kernels[dom])

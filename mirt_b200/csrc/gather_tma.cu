@@ -120,15 +120,18 @@ __device__ __forceinline__ Item item_of(const GatherBlocks &g, const InterpArgs 
   return r;
 }
 
-// one thread: arm the stage's barrier and start its copies.  no_copy (the
-// test of the bounded waits): arm the barrier for bytes that no copy will
-// deliver and issue no copy, so that its wait runs out with nothing in flight.
+// one thread: record the item in the stage's header, arm the stage's barrier
+// (its arrival publishes the header to the waiting warps) and start its
+// copies.  no_copy (the test of the bounded waits): arm the barrier for bytes
+// that no copy will deliver and issue no copy, so that its wait runs out with
+// nothing in flight.
 template <int TCW>
 __device__ __forceinline__ void stage_issue(const CUtensorMap *tm, const InterpArgs &a,
                                             const int4 *orec, unsigned char *st, uint64_t *bar,
-                                            const Item &r, int chunk, bool no_copy) {
+                                            Item *hdr, const Item &r, int chunk, bool no_copy) {
   constexpr unsigned TILE = TgShape<TCW>::TILE;
   const unsigned wb = (unsigned)r.n * 96u, kb = (unsigned)r.n * 16u;
+  *hdr = r;
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   if (no_copy) {
     mbar_expect(bar, 16u);
@@ -153,7 +156,8 @@ __global__ void __launch_bounds__(TG_THREADS, TgShape<TCW>::CTAS_PER_SM)
   constexpr int NWARP = TG_THREADS / 32;
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t *bar = reinterpret_cast<uint64_t *>(smem + 2 * STAGE);
-  int *done = reinterpret_cast<int *>(bar + 2);  // warps finished with each stage's item
+  Item *hdr = reinterpret_cast<Item *>(bar + 2);  // each stage's item
+  int *done = reinterpret_cast<int *>(hdr + 2);   // warps finished with each stage's item
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int sub = lane / TCW, cl = lane % TCW;
   const int C = a.C;
@@ -177,14 +181,13 @@ __global__ void __launch_bounds__(TG_THREADS, TgShape<TCW>::CTAS_PER_SM)
     for (int k = 0; k < 2; k++) {
       const long long i = it0 + blockIdx.x + (long long)k * gridDim.x;
       if (i < end)
-        stage_issue<TCW>(&tmap, a, g.orec, smem + k * STAGE, &bar[k], item_of(g, a, i), chunk,
-                         no_copy);
+        stage_issue<TCW>(&tmap, a, g.orec, smem + k * STAGE, &bar[k], &hdr[k], item_of(g, a, i),
+                         chunk, no_copy);
     }
   for (int k = 0;; k++) {
     const long long i = it0 + blockIdx.x + (long long)k * gridDim.x;
     if (i >= end) break;
     const int s = k & 1;
-    const Item r = item_of(g, a, i);
     if (!stage_wait(&bar[s], (unsigned)(k >> 1) & 1u, wait_limit)) {
       // the stage did not arrive in time: flag it, let the other stage's copy
       // land (bounded), and stop this warp; the stage is never released, so
@@ -196,6 +199,7 @@ __global__ void __launch_bounds__(TG_THREADS, TgShape<TCW>::CTAS_PER_SM)
       }
       return;
     }
+    const Item r = hdr[s];
     const unsigned char *st = smem + s * STAGE;
     const float2 *tile = reinterpret_cast<const float2 *>(st);
     const float2 *Wst = reinterpret_cast<const float2 *>(st + TILE);
@@ -252,8 +256,8 @@ __global__ void __launch_bounds__(TG_THREADS, TgShape<TCW>::CTAS_PER_SM)
         __threadfence_block();
         const long long i2 = i + 2ll * gridDim.x;
         if (i2 < end)
-          stage_issue<TCW>(&tmap, a, g.orec, smem + s * STAGE, &bar[s], item_of(g, a, i2),
-                           chunk, no_copy);
+          stage_issue<TCW>(&tmap, a, g.orec, smem + s * STAGE, &bar[s], &hdr[s],
+                           item_of(g, a, i2), chunk, no_copy);
       }
     }
   }
@@ -306,7 +310,8 @@ cudaError_t launch_gather_tma(const InterpArgs &a, const GatherBlocks &g, int ns
                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
   auto go = [&](auto kern, unsigned stage, int per_sm, int cw) -> cudaError_t {
-    const size_t smem = 2 * (size_t)stage + 2 * sizeof(uint64_t) + 2 * sizeof(int);
+    const size_t smem = 2 * (size_t)stage + 2 * sizeof(uint64_t) + 2 * sizeof(Item) +
+                        2 * sizeof(int);
     cudaError_t e =
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
