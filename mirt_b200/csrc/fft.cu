@@ -171,7 +171,8 @@ __device__ __forceinline__ void dft_half_out(float2 *x) {
 // (nin = n/2 pruned or n, nout = n/2 pruned or n: no bounds tests), or 0 (any
 // width and counts, read from the pass).
 template <int R1, int R2, bool INV, bool PRUNE, int VW>
-__global__ void __launch_bounds__(kThreads) fft_pass_kernel(FftPass P, int lpb, int pitch_rt) {
+__global__ void __launch_bounds__(kThreads, VW ? 3 : 1)
+    fft_pass_kernel(FftPass P, int lpb, int pitch_rt) {
   constexpr bool EXACT = VW != 0;
   extern __shared__ __align__(16) float2 sm[];
   __shared__ long long base_in[kMaxLpb], base_out[kMaxLpb];
@@ -214,11 +215,25 @@ __global__ void __launch_bounds__(kThreads) fft_pass_kernel(FftPass P, int lpb, 
     if (bi < 0) continue;
     const float2 *src = P.in + bi + v;
     float2 x[R1];
+    if constexpr (EXACT) {
+      // element k = R2 k1 + q at a running pointer (no hoisted per-element offsets)
+      const float2 *sp = src + (long long)q * P.es_in;
+      const long long st = (long long)R2 * P.es_in;
 #pragma unroll
-    for (int k1 = 0; k1 < R1; k1++) {
-      const int k = R2 * k1 + q;
-      x[k1] = make_float2(0.f, 0.f);
-      if (k1 < KH && (EXACT || k < P.nin)) x[k1] = src[(long long)k * P.es_in];
+      for (int k1 = 0; k1 < R1; k1++) {
+        x[k1] = make_float2(0.f, 0.f);
+        if (k1 < KH) {
+          x[k1] = *sp;
+          sp += st;
+        }
+      }
+    } else {
+#pragma unroll
+      for (int k1 = 0; k1 < R1; k1++) {
+        const int k = R2 * k1 + q;
+        x[k1] = make_float2(0.f, 0.f);
+        if (k1 < KH && k < P.nin) x[k1] = src[(long long)k * P.es_in];
+      }
     }
     if (P.sn_in) {
       const float2 *sr = P.sn_in + (long long)snrow[g] * P.nin + q;
@@ -275,8 +290,13 @@ __global__ void __launch_bounds__(kThreads) fft_pass_kernel(FftPass P, int lpb, 
     float2 *dst = P.out + bo + v;
     const float2 *sr = P.sn_out ? P.sn_out + (long long)snrow[g] * P.nout : nullptr;
     if (EXACT && !sr && !P.ph_out) {
+      float2 *dp = dst + (long long)p1 * P.es_out;
+      const long long st = (long long)R1 * P.es_out;
 #pragma unroll
-      for (int p2 = 0; p2 < PH; p2++) dst[(long long)(p1 + R1 * p2) * P.es_out] = y[p2];
+      for (int p2 = 0; p2 < PH; p2++) {
+        *dp = y[p2];
+        dp += st;
+      }
     } else {
 #pragma unroll
       for (int p2 = 0; p2 < PH; p2++) {
