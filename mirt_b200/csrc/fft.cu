@@ -167,19 +167,19 @@ __device__ __forceinline__ void dft_half_out(float2 *x) {
 
 // ---- the pass kernel ---------------------------------------------------------
 // PRUNE: forward with nin <= n/2, or inverse with nout <= n/2.  VW: the vector
-// width at compile time (16) with the element counts exactly the transform's
+// width at compile time (8 or 16) with the element counts exactly the transform's
 // (nin = n/2 pruned or n, nout = n/2 pruned or n: no bounds tests), or 0 (any
 // width and counts, read from the pass).
 template <int R1, int R2, bool INV, bool PRUNE, int VW>
-__global__ void __launch_bounds__(kThreads, VW ? 3 : 1)
+__global__ void __launch_bounds__(kThreads, VW == 16 ? 3 : VW == 8 ? 2 : 1)
     fft_pass_kernel(FftPass P, int lpb, int pitch_rt) {
   constexpr bool EXACT = VW != 0;
   extern __shared__ __align__(16) float2 sm[];
   __shared__ long long base_in[kMaxLpb], base_out[kMaxLpb];
   __shared__ int snrow[kMaxLpb];
   const int vw = VW ? VW : P.vw;
-  const int lvw = VW ? (VW == 16 ? 4 : __ffs(VW) - 1) : __ffs(vw) - 1;
-  const int pitch = VW ? R2 * VW : pitch_rt;
+  const int lvw = VW ? (VW == 16 ? 4 : 3) : __ffs(vw) - 1;
+  const int pitch = VW ? R2 * VW + (VW < 16 ? VW : 0) : pitch_rt;
   const int nlines = P.nslice * P.nr2 * P.nr1 * P.nvec;
   const int g0 = blockIdx.x * lpb;
   if (threadIdx.x < lpb) {
@@ -331,21 +331,26 @@ cudaError_t launch_r(const FftPass &P, cudaStream_t st) {
     kern<<<grid, kThreads, smem, st>>>(P, lpb, pitch);
     return cudaGetLastError();
   };
-  // the exact form: 16-wide vectors, inputs and outputs exactly the (pruned) halves or all n
+  // the exact forms: 16- or 8-wide vectors, inputs and outputs exactly the
+  // (pruned) halves or all n
   const int hin = prune && !P.inverse ? P.n / 2 : P.n, hout = prune && P.inverse ? P.n / 2 : P.n;
-  const bool exact = vw == 16 && P.nin == hin && P.nout == hout;
-  if (P.inverse) {
-    if (exact)
-      return prune ? pick(fft_pass_kernel<R1, R2, true, true, 16>)
-                   : pick(fft_pass_kernel<R1, R2, true, false, 16>);
-    return prune ? pick(fft_pass_kernel<R1, R2, true, true, 0>)
-                 : pick(fft_pass_kernel<R1, R2, true, false, 0>);
-  }
-  if (exact)
-    return prune ? pick(fft_pass_kernel<R1, R2, false, true, 16>)
-                 : pick(fft_pass_kernel<R1, R2, false, false, 16>);
-  return prune ? pick(fft_pass_kernel<R1, R2, false, true, 0>)
-               : pick(fft_pass_kernel<R1, R2, false, false, 0>);
+  const int exact = (P.nin == hin && P.nout == hout && (vw == 16 || vw == 8)) ? vw : 0;
+  auto by_width = [&](auto k16, auto k8, auto k0) -> cudaError_t {
+    return exact == 16 ? pick(k16) : exact == 8 ? pick(k8) : pick(k0);
+  };
+  if (P.inverse)
+    return prune ? by_width(fft_pass_kernel<R1, R2, true, true, 16>,
+                            fft_pass_kernel<R1, R2, true, true, 8>,
+                            fft_pass_kernel<R1, R2, true, true, 0>)
+                 : by_width(fft_pass_kernel<R1, R2, true, false, 16>,
+                            fft_pass_kernel<R1, R2, true, false, 8>,
+                            fft_pass_kernel<R1, R2, true, false, 0>);
+  return prune ? by_width(fft_pass_kernel<R1, R2, false, true, 16>,
+                          fft_pass_kernel<R1, R2, false, true, 8>,
+                          fft_pass_kernel<R1, R2, false, true, 0>)
+               : by_width(fft_pass_kernel<R1, R2, false, false, 16>,
+                          fft_pass_kernel<R1, R2, false, false, 8>,
+                          fft_pass_kernel<R1, R2, false, false, 0>);
 }
 
 // largest power of two dividing v, at most 16
