@@ -116,10 +116,16 @@ __device__ __forceinline__ float2 cw_fma(float2 w, float2 v, float2 vs, float2 A
   return A;
 }
 
-// acc += conj(w) * v by cw_fma (the swapped v is shared by a row of taps)
+// acc += conj(w) * v as four scalar FMAs in the order (re: wr vr, wi vi;
+// im: wr vi, -wi vr) -- the roundings of cw_fma.
 template <bool REAL>
 __device__ __forceinline__ void cmac_conj(float2 &acc, float2 w, float2 v) {
-  acc = cw_fma<REAL>(w, v, make_float2(v.y, v.x), acc);
+  acc.x = __fmaf_rn(w.x, v.x, acc.x);
+  acc.y = __fmaf_rn(w.x, v.y, acc.y);
+  if (!REAL) {
+    acc.x = __fmaf_rn(w.y, v.y, acc.x);
+    acc.y = __fmaf_rn(-w.y, v.x, acc.y);
+  }
 }
 
 // *p += (wr, wr) v2 + (wi, -wi) v2s: a read-modify-write by the point's one
