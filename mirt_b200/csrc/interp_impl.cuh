@@ -234,12 +234,13 @@ __global__ void __launch_bounds__(256, D == 3 ? 2 : 4) gather_kernel(InterpArgs 
         } else {
           CAcc s3;
           cacc_zero(s3);
-#pragma unroll 1
+#pragma unroll 2
           for (int j3 = 0; j3 < JT; j3++) {
             const float2 *pl = gc + tap_k(k0.z, j3, K3) * pstr;
             CAcc s2;
             cacc_zero(s2);
-#pragma unroll 3
+            // the plane's JT rows at once: all JT x JT tap loads in flight together
+#pragma unroll
             for (int j2 = 0; j2 < JT; j2++)
               cacc_mac<false>(s2, __ldg(Ws + JT + j2), rowsum(pl + tap_k(k0.y, j2, K2) * rstr));
             cacc_mac<false>(s3, __ldg(Ws + 2 * JT + j3), cacc_get<false>(s2));
