@@ -945,11 +945,13 @@ int plan_finish(mirt_interp_plan *P, long long Mtot, const long long *moff, int 
     P->ag.K0 = P->k0tap_g.as<int4>();
     P->ag.perm = P->perm_g.as<int>();
     P->ag.phase = a.phase ? P->phase_g.as<float2>() : nullptr;
-    if (gbs == gather_tma_block() && a.g.D == 2) {
-      // work items: up to gather_tma_item() samples of one non-empty block
+    const bool tma3 = a.g.D == 3 && gather_tma3_ok(a) && gbs == gather_tma3_block();
+    if ((gbs == gather_tma_block() && a.g.D == 2) || tma3) {
+      // work items: up to gather_tma_item() (3D: gather_tma3_item()) samples of
+      // one non-empty block
       std::vector<int> hb(nb4 + 1);
       CK(cudaMemcpy(hb.data(), bs4.p, (nb4 + 1) * sizeof(int), cudaMemcpyDeviceToHost));
-      const int rc_n = gather_tma_item();
+      const int rc_n = tma3 ? gather_tma3_item() : gather_tma_item();
       const long long per = (long long)t4.nbins;
       std::vector<int2> items;
       P->gitem_slice.assign(nslice + 1, 0);
@@ -967,7 +969,7 @@ int plan_finish(mirt_interp_plan *P, long long Mtot, const long long *moff, int 
       CK(cudaGetLastError());
       CK(cudaStreamSynchronize(st));
       P->gbk = GatherBlocks{P->gblk.as<int>(), P->gitem.as<int2>(), P->orec_g.as<int4>(), gbs,
-                            t4.nbin[0], t4.nbin[1]};
+                            t4.nbin[0], t4.nbin[1], t4.nbin[2]};
       CK(P->gfault.alloc(sizeof(int)));
       CK(cudaMemset(P->gfault.p, 0, sizeof(int)));
       P->gtma = 1;  // the default where it applies; the autotuner times both
@@ -1369,7 +1371,8 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
     }
   }
   if (had_tma)
-    for (int mode : {1, 2}) {  // tiles of 32 or 16 coils
+    for (int mode : {1, 2}) {  // tiles of 32 or 16 coils (3D: of 8 coils, mode 1 only)
+      if (mode == 2 && a.g.D == 3) continue;
       P->gtma = mode;
       float ms = 0;
       int rc = time_launch([&]() {
@@ -1378,7 +1381,7 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
       if (rc) return rc;
       if (autotune_log())
         std::fprintf(stderr, "mirt autotune gather: TMA tiles of %d coils: %.3f ms\n",
-                     mode == 2 ? 16 : 32, ms);
+                     a.g.D == 3 ? 8 : mode == 2 ? 16 : 32, ms);
       if (ms < bestg_ms) {
         bestg_ms = ms;
         best_tma = mode;
@@ -1405,7 +1408,10 @@ int mirt_interp_plan_set_gather(mirt_interp_plan *P, int32_t tma) {
   if (!P) return fail(MIRT_ERR_ARG, "plan is NULL");
   if (tma < 0 || tma > 2) return fail(MIRT_ERR_ARG, "gather mode must be 0, 1 or 2");
   if (tma && !P->gbk.item)
-    return fail(MIRT_ERR_ARG, "TMA gather needs 2D, J = 6, an even C >= 32 and K >= 13");
+    return fail(MIRT_ERR_ARG, "TMA gather needs J = 6 and, in 2D, an even C >= 32 and K >= 13, "
+                              "in 3D an even C >= 8 and K >= 9");
+  if (tma == 2 && P->a.g.D == 3)
+    return fail(MIRT_ERR_ARG, "gather mode 2 (16-coil tiles) is 2D only");
   P->gtma = tma;
   return MIRT_OK;
 }

@@ -149,25 +149,31 @@ struct Launch {
 };
 
 // The gather over TMA-staged grid tiles and records (gather_tma.cu): 2D, J = 6,
-// C even and >= 32, K >= 13 per dimension.  Samples in the gather order are
-// grouped by gb x gb blocks of their first taps; start[b] is the first
-// position of block b = (slice * nby + by) * nbx + bx (start[nblocks] = Mtot);
-// a work item (block, first position) covers up to gather_tma_item() samples
-// of one block, items in block order; orec[pos] = (caller's sample index, 0,
-// phase as float bits), staged with the tap records.
+// C even and >= 32, K >= 13 per dimension; or 3D, J = 6, C even and >= 8,
+// K >= 9 per dimension.  Samples in the gather order are grouped by blocks of
+// gb points per dimension of their first taps; start[b] is the first position
+// of block b = ((slice * nbz + bz) * nby + by) * nbx + bx (start[nblocks] =
+// Mtot); a work item (block, first position) covers up to gather_tma_item()
+// (3D: gather_tma3_item()) samples of one block, items in block order;
+// orec[pos] = (caller's sample index, 0, phase as float bits), staged with the
+// tap records.
 struct GatherBlocks {
   const int *start;
   const int2 *item;
   const int4 *orec;
-  int gb, nbx, nby;
+  int gb, nbx, nby, nbz;
 };
 bool gather_tma_ok(const InterpArgs &a);
 int gather_tma_block();
 int gather_tma_item();
+bool gather_tma3_ok(const InterpArgs &a);
+int gather_tma3_block();
+int gather_tma3_item();
 // items [it0, it0 + nit) of a batch of nslice slices; *fault is set when a
 // stage does not arrive within the kernel's wait limit.  fault_test: the test
 // of that path (no copies are issued, every wait runs out, nothing computed).
-// tcw: coils per tile, 32 (a warp per sample) or 16 (a half-warp per sample).
+// tcw: coils per tile, 32 (a warp per sample) or 16 (a half-warp per sample);
+// 3D plans always use tiles of 8 coils (a quarter-warp per sample).
 cudaError_t launch_gather_tma(const InterpArgs &a, const GatherBlocks &g, int nslice,
                               long long it0, long long nit, const float2 *ck, float2 *fm,
                               int *fault, cudaStream_t st, int fault_test = 0, int tcw = 32);

@@ -537,6 +537,48 @@ def test_tma_gather_matches_plain_gather_and_oracle(C, K):
     plan.close()
 
 
+@pytest.mark.parametrize("C,K", [(8, (32, 24, 20)), (10, (12, 9, 16))])
+def test_tma_gather_3d_matches_plain_gather_and_oracle(C, K):
+    """3D gather over TMA-staged 9 x 9 x 9 tiles of 8 coils (4 x 4 x 4 blocks
+    of first taps, items of up to 32 samples): bitwise the plain 3D gather,
+    the oracle's forward to FP32 rounding; a partial coil chunk (C = 10), grids
+    down to K = 9 (most blocks wrap and read the grid directly), a dense slice
+    (blocks split into several items), coordinates far outside the grid, three
+    slices; a per-sample phase; the bounded waits' fault path."""
+    import torch
+    rng = np.random.default_rng(91 + C)
+    J, L = [6, 6, 6], [256, 256, 256]
+    h = [mb.minmax_kb_table(max(k // 2, 6), 6, k, 256) for k in K]
+    tms = [rng.uniform(-20, 20, (1500, 3)), rng.uniform(-2, 2, (3000, 3)),
+           rng.uniform(-100, 100, (500, 3))]
+    moff = np.concatenate([[0], np.cumsum([len(t) for t in tms])])
+    tm = np.concatenate(tms)
+    ph = np.exp(1j * rng.uniform(-np.pi, np.pi, len(tm)))
+    plan = mb.InterpPlan(K, J, L, h, tm, C, slice_moff=moff, phase=ph)
+    assert plan.config()["gather_tma"] == 1      # the default where it applies
+    ck = (rng.standard_normal((3, K[2], K[1], K[0], C)) +
+          1j * rng.standard_normal((3, K[2], K[1], K[0], C)))
+    ckd = torch.from_numpy(ck.astype(np.complex64)).cuda()
+    a = plan.forward(ckd).cpu().numpy()
+    assert plan.fault() == 0
+    plan.set_gather(False)
+    assert np.array_equal(plan.forward(ckd).cpu().numpy(), a)
+    for s in range(3):
+        ref = oracle.interp_for(np.transpose(ck[s], (2, 1, 0, 3)).reshape(-1, C, order="F"), h, J,
+                                L, tms[s], K, 0, impl=ref_impl()) * ph[moff[s]:moff[s + 1], None]
+        assert rel_l2(a[moff[s]:moff[s + 1]], ref) <= FWD_TOL, s
+    with pytest.raises(mb.MirtError, match="2D only"):
+        plan.set_gather(2)
+    plan.set_gather(True)
+    plan.set_fault_test(True)                   # no copies: every wait runs out, nothing in flight
+    plan.forward(ckd)
+    assert plan.fault() == 1
+    plan.close()                                # a faulted plan is discarded
+    p6 = mb.InterpPlan(K, J, L, h, tms[0], 6)   # C < 8: no 3D TMA blocks
+    assert p6.config()["gather_tma"] == 0
+    p6.close()
+
+
 def test_tma_gather_real_tables_phase_and_refusal():
     """Real tables, first order, with a per-sample phase: the TMA gather equals
     the plain gather and the oracle; a plan with C = 8 has no TMA blocks."""
