@@ -265,7 +265,7 @@ int mirt_interp_plan_set_dense(mirt_interp_plan *plan, int32_t on);
 int mirt_interp_plan_set_staged(mirt_interp_plan *plan, int32_t mode);
 
 /* Gather over TMA-staged tiles and records (2D, J = 6, an even C >= 32,
- * K >= 13; the default there, and the autotuner times it against the plain
+ * K >= 13; 3D below; the default there, and the autotuner times it against the plain
  * gather): the gather order groups samples by 8 x 8 blocks of first taps; for
  * each work item (up to 96 samples of one block) a CTA loads the block's
  * 13 x 13 x 32-coil grid tile (cp.async.bulk.tensor) and the item's tap
@@ -274,9 +274,12 @@ int mirt_interp_plan_set_staged(mirt_interp_plan *plan, int32_t mode);
  * wrap past K read the grid directly.  Same arithmetic and summation order
  * as the plain gather: identical results.  tma = 1: tiles of 32 coils (a warp
  * per sample, two CTAs per SM); 2: tiles of 16 coils (a half-warp per sample,
- * three CTAs per SM); 0 selects the plain gather.  The autotuner times all
- * three.  MIRT_ERR_ARG for other modes and where the plan has no TMA blocks.
- * No reference counterpart. */
+ * three CTAs per SM); 0 selects the plain gather.  3D plans (J = 6, an even
+ * C >= 8, K >= 9): tma = 1 stages 9 x 9 x 9 x 8-coil tiles of 4 x 4 x 4
+ * blocks of first taps (items of up to 32 samples, a quarter-warp per
+ * sample); mode 2 is 2D only.  The autotuner times the forms that apply.
+ * MIRT_ERR_ARG for other modes and where the plan has no TMA blocks.  No
+ * reference counterpart. */
 int mirt_interp_plan_set_gather(mirt_interp_plan *plan, int32_t tma);
 
 /* Fault flag of the plan's bounded in-kernel waits (TMA stage arrivals):
