@@ -576,7 +576,11 @@ def run_cgsense(args):
       precon_toeplitz   circulant preconditioner on the Toeplitz normal equations
                         (qpwls_pcg2), from zero: the Gram form without the learned part
       learned_toeplitz  the learned warm start on the Toeplitz normal equations
-      pipe              Pipe-Menon DCF (30 updates) warm start + preconditioner"""
+      pipe              Pipe-Menon DCF (30 updates) warm start + preconditioner
+      learned_precon    from zero, the circulant preconditioner built from the learned DCF
+                        (G' diag(w^2) G, floored; the learned weights and the preconditioner's
+                        kernel built inside the timed region), NUFFT pair per iteration
+      learned_precon_blend  the same, blended half and half with the unweighted one"""
     import torch
 
     import mirt_b200 as mb
@@ -585,7 +589,8 @@ def run_cgsense(args):
     from mirt_b200 import workloads as wl
 
     tol = 1e-3
-    modes = ("plain", "precon_only", "learned", "precon_toeplitz", "learned_toeplitz", "pipe")
+    modes = ("plain", "precon_only", "learned", "precon_toeplitz", "learned_toeplitz", "pipe",
+             "learned_precon", "learned_precon_blend")
     rng = np.random.default_rng(5)
     probs = wl.cgsense_problems(args.cg_problems, rng)
     groups = {}
@@ -635,6 +640,7 @@ def run_cgsense(args):
         # afterwards), like the plan set-up
         A.warm_start(y, W=model.predict(om_d, slice_moff=moff).to(torch.float32))
         A.warm_start(y, W=mb.dcf_pipe(G1, niter=0, thresh=0.0).to(torch.float32))
+        A.precon_dcf(model.predict(om_d, slice_moff=moff), 0.0)
         torch.zeros_like(xref)
         torch.cuda.synchronize()
         res = {"N": N, "coils": C, "problems": len(idx)}
@@ -659,6 +665,12 @@ def run_cgsense(args):
             e0 = ev()
             if mode in ("plain", "precon_only", "precon_toeplitz"):
                 x = torch.zeros_like(xref)
+            elif mode.startswith("learned_precon"):
+                w = model.predict(om_d, slice_moff=moff)
+                e_p = ev()
+                A.precon_dcf(w, 1.0 if mode == "learned_precon" else 0.5)
+                e_q = ev()
+                x = torch.zeros_like(xref)
             else:
                 # the warm start's per-problem least-squares scale absorbs any
                 # scale of the weights: no PSF scaling or normalisation here
@@ -676,6 +688,9 @@ def run_cgsense(args):
             res[mode] = {"s": None if t is None else (pre + t) / 1e3, "setup_s": pre / 1e3,
                          "iters": it, "ms_per_iter": float(tms[-1] / len(tms)),
                          "nrmse_start": float(nr[0].max()), "nrmse_end": float(nr[-1].max())}
+            if mode.startswith("learned_precon"):
+                res[mode]["precon_build_ms"] = e_p.elapsed_time(e_q)
+                A.precon_dcf(w, 0.0)         # the unweighted preconditioner again (untimed)
         for k in modes:
             if res[k]["s"] is None:
                 reached[k] = False

@@ -464,6 +464,20 @@ int mirt_sense_cg(mirt_sense *op, void *x, const void *y, const float *W, int32_
  * [Mtot, 2] column-major trajectory.  Synchronous. */
 int mirt_sense_toeplitz(mirt_sense *op, const double *om, void *stream);
 
+/* The circulant preconditioner from density-compensation weights (the learned
+ * DCF, or any): the spectrum of G' diag(w^2) G -- the inverse sampling density
+ * where the trajectory samples -- floored at 1e-3 of its maximum per problem,
+ * so that the preconditioner stays Hermitian positive definite and the
+ * minimiser is unchanged, and blended with the unweighted spectrum of
+ * mirt_sense_toeplitz: P = blend Pw / mean(Pw) + (1 - blend) P1 / mean(P1)
+ * per problem (blend 0: the unweighted preconditioner again).  Replaces the
+ * attached preconditioner; MIRT_PCG_CIRCULANT then uses it.  om: the plan's
+ * host FP64 trajectory; w: device FP64 [Mtot] in the plan's sample order.
+ * MIRT_ERR_ARG without mirt_sense_toeplitz or with blend outside [0, 1].
+ * Synchronous.  No reference counterpart. */
+int mirt_sense_precon_dcf(mirt_sense *op, const double *om, const double *w, double blend,
+	void *stream);
+
 /* mirt_sense_cg with options (flags, OR of):
  *   MIRT_PCG_CIRCULANT  precondition with the attached circulant
  *                       preconditioner (qpwls_pcg1's `precon`)

@@ -82,6 +82,7 @@ _SIGS = {
     "mirt_sense_warm_start": ([_vp, _vp, _vp, _vp, _vp], C.c_int),
     "mirt_sense_destroy": ([_vp], C.c_int),
     "mirt_sense_toeplitz": ([_vp, _dp, _vp], C.c_int),
+    "mirt_sense_precon_dcf": ([_vp, _dp, _vp, C.c_double, _vp], C.c_int),
     "mirt_sense_pcg": ([_vp, _vp, _vp, _vp, _i32, _i32, _vp, _dp, C.POINTER(C.c_float), _vp],
                        C.c_int),
     "mirt_toeplitz_create": ([C.POINTER(_vp), _dp, _i64, _i64p, _i32, _i32p, _i32p, _i32p,

@@ -478,6 +478,42 @@ int mirt_sense_cg(mirt_sense *op, void *x, const void *y, const float *W, int32_
   return mirt_sense_pcg(op, x, y, W, niter, 0, xref, nrmse, ms, stream);
 }
 
+namespace {
+__global__ void k_square(const double *__restrict__ w, double *__restrict__ w2, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    w2[i] = w[i] * w[i];
+}
+}  // namespace
+
+int mirt_sense_precon_dcf(mirt_sense *op, const double *om, const double *w, double blend,
+                          void *stream) {
+  if (!op || !om || !w) return api_fail(MIRT_ERR_ARG, "NULL argument");
+  if (!op->T) return api_fail(MIRT_ERR_ARG, "mirt_sense_toeplitz must run first");
+  if (!(blend >= 0.0 && blend <= 1.0)) return api_fail(MIRT_ERR_ARG, "blend must be in [0, 1]");
+  cudaStream_t st = as_stream(stream);
+  mirt_interp_plan *P = op->G->ip;
+  const int Nd[2] = {op->N1, op->N2}, Kd[2] = {P->a.g.K[0], P->a.g.K[1]};
+  const int Jd[2] = {P->a.g.J[0], P->a.g.J[1]}, Ld[2] = {P->a.g.L[0], P->a.g.L[1]};
+  DMem w2;
+  cudaError_t e = w2.alloc(std::max<long long>(op->M, 1) * sizeof(double));
+  if (e) return api_fail(MIRT_ERR_ALLOC, "DCF preconditioner weights");
+  if (op->M > 0) {
+    long long nb = (op->M + 255) / 256;
+    if (nb > 148 * 16) nb = 148 * 16;
+    k_square<<<(unsigned)nb, 256, 0, st>>>(w, w2.as<double>(), op->M);
+    e = cudaGetLastError();
+    if (e) return api_fail(MIRT_ERR_CUDA, cudaGetErrorString(e));
+  }
+  mirt_toeplitz *Tw = nullptr;
+  int rc = toep_create(&Tw, om, op->M, P->moff_host.data(), op->S, Nd, Kd, Jd, Ld,
+                       w2.as<double>(), 1, st);
+  if (rc) return rc;
+  rc = toep_precon_dcf(op->T, Tw, blend, st);
+  delete Tw;
+  return rc;
+}
+
 int mirt_sense_toeplitz(mirt_sense *op, const double *om, void *stream) {
   if (!op || !om) return api_fail(MIRT_ERR_ARG, "NULL argument");
   cudaStream_t st = as_stream(stream);

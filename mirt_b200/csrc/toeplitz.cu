@@ -199,6 +199,44 @@ __global__ void k_precon(const float2 *__restrict__ H, const double *__restrict_
   }
 }
 
+// per slice: mean of max(Re Hw, 1e-3 max Re Hw) and of P1
+__global__ void k_dcf_means(const float2 *__restrict__ Hw, const float *__restrict__ mxw,
+                            const float *__restrict__ P1, long long P, double *__restrict__ mean) {
+  __shared__ double pw[256], p1[256];
+  const int s = blockIdx.x;
+  const float fl = 1e-3f * mxw[s];
+  double a = 0, b = 0;
+  for (long long k = threadIdx.x; k < P; k += blockDim.x) {
+    a += (double)fmaxf(Hw[s * P + k].x, fl);
+    b += (double)P1[s * P + k];
+  }
+  pw[threadIdx.x] = a;
+  p1[threadIdx.x] = b;
+  __syncthreads();
+  for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+    if (threadIdx.x < h) {
+      pw[threadIdx.x] += pw[threadIdx.x + h];
+      p1[threadIdx.x] += p1[threadIdx.x + h];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    mean[2 * s] = pw[0] / (double)P;
+    mean[2 * s + 1] = p1[0] / (double)P;
+  }
+}
+
+__global__ void k_dcf_blend(const float2 *__restrict__ Hw, const float *__restrict__ mxw,
+                            const float *__restrict__ P1, const double *__restrict__ mean,
+                            double blend, float *__restrict__ Hp, int S, long long P) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < S * P;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int s = (int)(e / P);
+    const double pw = (double)fmaxf(Hw[e].x, 1e-3f * mxw[s]);
+    Hp[e] = (float)(blend * pw / mean[2 * s] + (1.0 - blend) * (double)P1[e] / mean[2 * s + 1]);
+  }
+}
+
 int make_plan(cufftHandle *h, int N1, int N2, int batch) {
   int n[2] = {2 * N2, 2 * N1};
   const int P = 4 * N1 * N2;
@@ -310,6 +348,31 @@ int toep_precon_build(mirt_toeplitz *T, const double *lam, const double *beta, c
   k_specmax<<<S, 256, 0, st>>>(T->H.as<float2>(), dl.as<double>(), P, mx.as<float>());
   k_precon<<<nblk(S * P), 256, 0, st>>>(T->H.as<float2>(), dl.as<double>(), db.as<double>(),
                                         mx.as<float>(), T->Hp.as<float>(), S, T->N1, T->N2);
+  TCK(cudaGetLastError());
+  TCK(cudaStreamSynchronize(st));
+  return MIRT_OK;
+}
+
+int toep_precon_dcf(mirt_toeplitz *T, const mirt_toeplitz *Tw, double blend, cudaStream_t st) {
+  const int S = T->S;
+  const long long P = 4ll * T->N1 * T->N2;
+  if (!T->Hp.p || !Tw || Tw->S != S || Tw->N1 != T->N1 || Tw->N2 != T->N2)
+    return api_fail(MIRT_ERR_ARG, "preconditioner kernels of different shapes");
+  if (!T->Hp1.p) {  // keep the unweighted spectrum the first time
+    TCK(T->Hp1.alloc(S * P * sizeof(float)));
+    TCK(cudaMemcpyAsync(T->Hp1.p, T->Hp.p, S * P * sizeof(float), cudaMemcpyDeviceToDevice, st));
+  }
+  DMem one, mx, mean;
+  std::vector<double> ones(S, 1.0);
+  TCK(one.alloc(S * sizeof(double)));
+  TCK(mx.alloc(S * sizeof(float)));
+  TCK(mean.alloc(2 * S * sizeof(double)));
+  TCK(cudaMemcpyAsync(one.p, ones.data(), S * sizeof(double), cudaMemcpyHostToDevice, st));
+  k_specmax<<<S, 256, 0, st>>>(Tw->H.as<float2>(), one.as<double>(), P, mx.as<float>());
+  k_dcf_means<<<S, 256, 0, st>>>(Tw->H.as<float2>(), mx.as<float>(), T->Hp1.as<float>(), P,
+                                 mean.as<double>());
+  k_dcf_blend<<<nblk(S * P), 256, 0, st>>>(Tw->H.as<float2>(), mx.as<float>(), T->Hp1.as<float>(),
+                                           mean.as<double>(), blend, T->Hp.as<float>(), S, P);
   TCK(cudaGetLastError());
   TCK(cudaStreamSynchronize(st));
   return MIRT_OK;

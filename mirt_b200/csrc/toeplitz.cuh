@@ -13,6 +13,7 @@ struct mirt_toeplitz {
   int S = 0, N1 = 0, N2 = 0, ncol = 0;
   mirt::DMem H;    // complex64 [S][2N2][2N1]: FFT of the circulant kernel
   mirt::DMem Hp;   // float [S][2N2][2N1]: circulant preconditioner spectrum (or empty)
+  mirt::DMem Hp1;  // float [S][2N2][2N1]: the unweighted spectrum, kept when Hp is blended
   mirt::DMem pad;  // complex64 [S * ncol][2N2][2N1]: work grid
   cufftHandle fft_n = 0, fft_1 = 0;  // batches S * ncol and S
   bool ok_n = false, ok_1 = false;
@@ -36,6 +37,15 @@ int toep_gram_sense(mirt_toeplitz *T, const float2 *x, const float2 *sens, float
 // r_s the spectrum of the quadratic first-order penalty with weight beta_s
 // (host arrays of S values).
 int toep_precon_build(mirt_toeplitz *T, const double *lam, const double *beta, cudaStream_t st);
+
+// Circulant preconditioner spectrum from the learned density compensation:
+// Tw = G' diag(w^2) G (its spectrum approximates the inverse sampling density
+// where the trajectory samples), floored at 1e-3 of its maximum per slice so
+// that it stays positive (a Hermitian positive definite preconditioner keeps
+// the unweighted minimiser), blended with T's unweighted spectrum P1 (kept in
+// Hp1): Hp = blend Pw / mean(Pw) + (1 - blend) P1 / mean(P1).  T's
+// toep_precon_build must have run; blend in [0, 1].
+int toep_precon_dcf(mirt_toeplitz *T, const mirt_toeplitz *Tw, double blend, cudaStream_t st);
 
 // out = crop(IFFT(Hp FFT(pad(x)))) per slice, single column
 int toep_precon_apply(mirt_toeplitz *T, const float2 *x, float2 *out, cudaStream_t st);

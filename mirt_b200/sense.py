@@ -75,6 +75,16 @@ class SenseSystem:
         self.has_toeplitz = True
         return self
 
+    def precon_dcf(self, w, blend=1.0, stream=None):
+        """Replace the circulant preconditioner by the one built from the
+        density-compensation weights w (device FP64 [Mtot], e.g. the learned
+        DCF), blended with the unweighted one (see mirt_sense_precon_dcf);
+        blend=0 restores the unweighted preconditioner.  Needs toeplitz()."""
+        check(self.lib.mirt_sense_precon_dcf(self.handle, self.G.om_f.ctypes.data_as(_dp),
+                                             _ptr(w.to(_torch().float64).contiguous()),
+                                             float(blend), _stream_ptr(stream)))
+        return self
+
     def pcg(self, x, y, niter, W=None, precon=False, gram=False, xref=None, timing=False,
             stream=None):
         """niter iterations of qpwls_pcg1 (NUFFT pair each iteration) or, with

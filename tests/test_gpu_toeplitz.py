@@ -57,6 +57,7 @@ def _sense_batch(seed, N=32, K=64, C=4, spokes=(22, 16)):
     xt = np.stack([wl.ellipses(N, 6, rng).T for _ in oms])
     ys = [R.forward(xt[s]) for s, R in enumerate(refs)]
     y = torch.from_numpy(np.concatenate(ys).astype(np.complex64)).cuda()
+    A.oms, A.moff = oms, moff
     return A, refs, ys, y
 
 
@@ -76,6 +77,40 @@ def test_preconditioned_cg_reaches_fp64_solution_faster():
         h = np.nonzero(np.all(nr <= 1e-3, axis=1))[0]
         return h[0] if len(h) else 10 ** 9
     assert first(nr_pre) < first(nr_plain), (first(nr_pre), first(nr_plain))
+
+
+def test_dcf_preconditioner_keeps_the_minimiser():
+    """The circulant preconditioner built from density-compensation weights
+    (Pipe-Menon weights here; the learned DCF feeds the same call), pure and
+    blended with the unweighted one: PCG with it reaches the FP64 solution of
+    the unweighted problem (a Hermitian positive definite preconditioner keeps
+    the minimiser); blend 0 gives the unweighted preconditioner's iterates
+    again (to FP32 rounding: the spectrum is rescaled); refusals."""
+    import torch
+    A, refs, ys, y = _sense_batch(5)
+    sol = [qpwls_pcg1(np.zeros((32, 32), complex), R, None, ys[s], 400)[-1]
+           for s, R in enumerate(refs)]
+    xref = torch.from_numpy(np.stack(sol).astype(np.complex64)).cuda()
+    x = torch.zeros(A.image_shape, dtype=torch.complex64, device="cuda")
+    nr_u, _ = A.pcg(x, y, 40, precon=True, xref=xref)
+    G1 = mb.NufftPlan(np.concatenate(A.oms), (32, 32), (6, 6), (64, 64), n_shift=(16, 16),
+                      Ld=1024, ncol=1, slice_moff=A.moff)
+    w = mb.dcf_pipe(G1, niter=20)
+    for blend in (1.0, 0.5):
+        A.precon_dcf(w, blend)
+        x = torch.zeros_like(xref)
+        nr, _ = A.pcg(x, y, 200, precon=True, xref=xref)
+        assert np.all(nr[-1] <= 5e-4), (blend, nr[-1])
+    A.precon_dcf(w, 0.0)
+    x = torch.zeros_like(xref)
+    nr0, _ = A.pcg(x, y, 40, precon=True, xref=xref)
+    assert np.allclose(nr0[:16], nr_u[:16], rtol=1e-3, atol=1e-6)
+    assert np.allclose(nr0[-1], nr_u[-1], rtol=0.1)     # rescaled spectrum: FP32 rounding
+    with pytest.raises(mb.MirtError, match="blend"):
+        A.precon_dcf(w, 1.5)
+    B = ms.SenseSystem(A.G, A.sens, A.beta)     # no Toeplitz operator attached
+    with pytest.raises(mb.MirtError, match="toeplitz"):
+        B.precon_dcf(w, 1.0)
 
 
 def test_gram_form_solution_matches_nufft_form():
