@@ -492,6 +492,36 @@ def test_staged_sweep_same_bits(C):
     small.close()
 
 
+@pytest.mark.parametrize("order", [0, 1])
+def test_staged_sweep_real_tables_phase(order):
+    """The staged row sweep with real tables (order 0 and 1) and a per-sample
+    phase, 32 coils, grids down to K = 6 x 7 (every tap row and column wraps):
+    the unstaged sweep's bits for both staged modes, and the oracle's adjoint."""
+    import torch
+    rng = np.random.default_rng(41 + order)
+    for K in ([6, 7], [40, 24]):
+        J, L = [6, 6], [64, 64]
+        h = [np.cos(np.linspace(-1.2, 1.2, 6 * 64 + 1)), np.exp(-np.linspace(-2, 2, 6 * 64 + 1) ** 2)]
+        tm = rng.uniform(-20, 20, (900, 2))
+        ph = np.exp(1j * rng.uniform(-np.pi, np.pi, len(tm)))
+        C = 32
+        plan = mb.InterpPlan(K, J, L, h, tm, C, order=order, phase=ph)
+        plan.set_dense(False)
+        rows = 4 if K[1] > 7 else 2
+        plan.set_sweep(1, rows)
+        plan.set_staged(0)
+        fm = rng.standard_normal((len(tm), C)) + 1j * rng.standard_normal((len(tm), C))
+        fm_d = torch.from_numpy(fm.astype(np.complex64)).cuda()
+        base = plan.adjoint(fm_d).cpu().numpy()
+        for mode in (1, 2):
+            plan.set_staged(mode)
+            assert np.array_equal(plan.adjoint(fm_d).cpu().numpy(), base), (K, mode)
+        got = np.transpose(base[0], (1, 0, 2)).reshape(-1, C, order="F")
+        ref = oracle.interp_adj(fm * np.conj(ph)[:, None], h, J, L, tm, K, order, impl=ref_impl())
+        assert rel_l2(got, ref) <= ADJ_TOL, K
+        plan.close()
+
+
 def test_sweep_spread_refused_where_it_does_not_apply():
     h = [mb.minmax_kb_table(8, 4, 16, 64)] * 2
     plan = mb.InterpPlan([16, 16], [4, 4], [64, 64], h, np.zeros((10, 2)), 2)
