@@ -609,6 +609,31 @@ def test_tma_gather_3d_matches_plain_gather_and_oracle(C, K):
     p6.close()
 
 
+@pytest.mark.parametrize("order", [0, 1])
+def test_tma_gather_3d_real_tables(order):
+    """3D TMA gather with real tables (order 0 and 1): the plain 3D gather's
+    bits and the oracle's forward."""
+    import torch
+    rng = np.random.default_rng(61 + order)
+    K, J, L = [16, 12, 10], [6, 6, 6], [64, 64, 64]
+    t = np.linspace(-2, 2, 6 * 64 + 1)
+    h = [np.exp(-t ** 2), np.cos(0.6 * t), np.exp(-0.5 * t ** 2)]
+    tm = rng.uniform(-12, 12, (2500, 3))
+    C = 8
+    plan = mb.InterpPlan(K, J, L, h, tm, C, order=order)
+    assert plan.config()["gather_tma"] == 1
+    ck = rng.standard_normal((1, K[2], K[1], K[0], C)) + 1j * rng.standard_normal((1, K[2], K[1], K[0], C))
+    ckd = torch.from_numpy(ck.astype(np.complex64)).cuda()
+    a = plan.forward(ckd).cpu().numpy()
+    plan.set_gather(False)
+    assert np.array_equal(plan.forward(ckd).cpu().numpy(), a)
+    ref = oracle.interp_for(np.transpose(ck[0], (2, 1, 0, 3)).reshape(-1, C, order="F"), h, J, L,
+                            tm, K, order, impl=ref_impl())
+    assert rel_l2(a, ref) <= FWD_TOL
+    assert plan.fault() == 0
+    plan.close()
+
+
 def test_tma_gather_real_tables_phase_and_refusal():
     """Real tables, first order, with a per-sample phase: the TMA gather equals
     the plain gather and the oracle; a plan with C = 8 has no TMA blocks."""
