@@ -46,6 +46,7 @@ UNIT = "Msamples/s"
 WORKLOADS = {
     "c2": dict(D=2, N=256, K=512, J=6, L=1024, ncoil=32, nslice=64, spokes=(100, 400), nro=512),
     "c2s": dict(D=2, N=256, K=512, J=6, L=1024, ncoil=32, nslice=4, spokes=(100, 400), nro=512),
+    "c2m": dict(D=2, N=256, K=512, J=6, L=1024, ncoil=32, nslice=16, spokes=(100, 400), nro=512),
     "c1": dict(D=2, N=64, K=128, J=6, L=1024, ncoil=1, nslice=1, spokes=(64, 64), nro=128),
     "c3": dict(D=3, N=128, K=256, J=6, L=512, ncoil=8, nslice=1, spokes=(16384, 16384), nro=256),
     "c3s": dict(D=3, N=128, K=256, J=6, L=512, ncoil=8, nslice=1, spokes=(2048, 2048), nro=256),

@@ -139,6 +139,20 @@ __global__ void gather_records_kernel(const int *__restrict__ gorder, long long 
   for (int j = 0; j < SJ; j++) Wg[i * SJ + j] = W[p * SJ + j];
 }
 
+// Tap records of the staged 2D row sweep (J = 6): per position, the six
+// first-dimension taps as FFMA2 operand pairs (wr, wr, wi, -wi), then the six
+// second-dimension taps two per float4.
+__global__ void sweep_records_kernel(const float2 *__restrict__ W, long long M,
+                                     float4 *__restrict__ out) {
+  const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (p >= M) return;
+  const float2 *w = W + p * 12;
+  float4 *o = out + p * 9;
+  for (int j = 0; j < 6; j++) o[j] = make_float4(w[j].x, w[j].x, w[j].y, -w[j].y);
+  for (int k = 0; k < 3; k++) o[6 + k] = make_float4(w[6 + 2 * k].x, w[6 + 2 * k].y,
+                                                      w[7 + 2 * k].x, w[7 + 2 * k].y);
+}
+
 // Output records of the TMA gather, in the gather order: (caller's sample
 // index, 0, phase re, phase im as bits); phase (1, 0) where there is none.
 __global__ void out_records_kernel(long long M, const int *__restrict__ permg,
@@ -990,6 +1004,14 @@ int plan_finish(mirt_interp_plan *P, long long Mtot, const long long *moff, int 
     if (rc3) return rc3;
     rc3 = build_sweep_teams(P, 1, 65536, st);
     if (rc3) return rc3;
+    // the staged sweep's records (FFMA2 operand pairs of the taps)
+    CK(P->wsw.alloc(std::max<long long>(Mtot, 1) * 9 * sizeof(float4)));
+    if (Mtot > 0)
+      mirt_plan_kernels::sweep_records_kernel<<<(unsigned)((Mtot + 255) / 256), 256, 0, st>>>(
+          a.W, Mtot, P->wsw.as<float4>());
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(st));
+    P->t.wsw = P->wsw.as<float4>();
   }
   // 3D, J = 6, coil chunks of 8, 16 or 32: the line sweep, two segments per line
   if (sweep3_ok(a, P->t, P->ls.cw)) {
@@ -1239,11 +1261,11 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
   if (sweep_ok(a, P->t) && sweep_buffer(P) == MIRT_OK)
     for (int dense : {0, 1})
       for (int rows : {1, 2, 4})
-        for (int nseg = (rows < 4 ? -1 : 1); nseg <= 16 && (nseg <= 1 || a.g.K[0] / nseg >= 32);
+        for (int nseg = -1; nseg <= 16 && (nseg <= 1 || a.g.K[0] / nseg >= 32);
              nseg = nseg < 0 ? 1 : nseg * 2)
           if (!dense || (rows == 1 && P->t.dense_of))
             for (int staged : {0, 1, 2})
-              if (!staged || (cw == 32 && !dense))
+              if (!staged || (cw == 32 && !dense && P->t.wsw))
                 cands.push_back(SpreadCand{{P->t.T[0], P->t.T[1], P->t.T[2]}, P->ls.threads, 0,
                                            0, 0, nseg, rows, dense, staged});
   // 3D line sweep: 1, 2, 4 or 8 segments per line block
@@ -1488,7 +1510,7 @@ int mirt_interp_plan_set_dense(mirt_interp_plan *P, int32_t on) {
 int mirt_interp_plan_set_staged(mirt_interp_plan *P, int32_t mode) {
   if (!P) return fail(MIRT_ERR_ARG, "plan is NULL");
   if (mode < 0 || mode > 2) return fail(MIRT_ERR_ARG, "staged mode must be 0, 1 or 2");
-  if (mode && P->ls.cw != 32)
+  if (mode && (P->ls.cw != 32 || !P->t.wsw))
     return fail(MIRT_ERR_ARG, "the staged row sweep needs 32-coil lanes (C >= 32)");
   P->t.sweep_staged = mode;
   return MIRT_OK;

@@ -93,6 +93,10 @@ struct Tiling {
   // (spread_sweep2s_kernel) after the ordering pass; 2 staged, reading the
   // caller's samples directly (no ordering pass)
   int sweep_staged;
+  // the staged sweep's tap records, 9 float4 per position (plan order): the
+  // six first-dimension taps as FFMA2 operand pairs (wr, wr, wi, -wi), then
+  // the six second-dimension taps (two per float4)
+  const float4 *wsw;
   // the patches are summed in chunks of at most 64 samples: chunk i =
   // dense_chunk[i] = (dense bin, first position, end position, part index);
   // dense bin d's chunk sums are patch_part[dense_part0[d] .. dense_part0[d+1]);

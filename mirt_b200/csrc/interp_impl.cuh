@@ -1219,9 +1219,11 @@ struct Sw2Meta {
   float2 ph[SW2_CAP];
   int beg[16], ex[16];
 };
+// per warp: three lists, two blocks of tap records (9 float4 per visit) and
+// two blocks of sample rows
 template <bool DIRECT>
 constexpr int sweep2_warp_bytes() {
-  return 3 * (int)sizeof(Sw2Meta) + 3 * SW2_CAP * 12 * 8 + 2 * SW2_CAP * 32 * 8;
+  return 3 * (int)sizeof(Sw2Meta) + 2 * SW2_CAP * 9 * 16 + 2 * SW2_CAP * 32 * 8;
 }
 
 template <int R, bool REAL, bool DIRECT>
@@ -1233,8 +1235,8 @@ __device__ __forceinline__ void sweep2s_team(const InterpArgs &a, const Tiling &
   constexpr unsigned FULLM = 0xffffffffu;
   constexpr int NQ = R + 5;
   Sw2Meta *meta = reinterpret_cast<Sw2Meta *>(wsm);
-  float2 *srec = reinterpret_cast<float2 *>(wsm + 3 * sizeof(Sw2Meta));
-  float2 *sf = srec + 3 * SW2_CAP * 12;
+  float4 *srec = reinterpret_cast<float4 *>(wsm + 3 * sizeof(Sw2Meta));
+  float2 *sf = reinterpret_cast<float2 *>(srec + 2 * SW2_CAP * 9);
   const int K1 = a.g.K[0], K2 = a.g.K[1];
   int slice, y0, x0, x1;
   if (t.sweep < 0) {
@@ -1273,19 +1275,8 @@ __device__ __forceinline__ void sweep2s_team(const InterpArgs &a, const Tiling &
   int lb = rowb >= 0 ? __ldg(bs + rowb + wrapx(xs)) : 0;
   int le = rowb >= 0 ? __ldg(bs + rowb + wrapx(xs) + 1) : lb;
   int rn = 0;
-  // lane's first chunk of the records' 16-byte copies: (visit, chunk) = (lane / 6, lane % 6)
-  const int cv0 = lane / 6, ck0 = lane - 6 * (lane / 6);
-  // records, caller rows and phases of the listed visits [0, nb)
-  auto issue_rec = [&](Sw2Meta &m, float2 *rec, int nb) {
-    for (int v = cv0, kk = ck0; v < nb;) {
-      cp_async16(rec + v * 12 + 2 * kk, a.W + (long long)m.pos[v] * 12 + 2 * kk);
-      v += 5;
-      kk += 2;
-      if (kk >= 6) {
-        kk -= 6;
-        v++;
-      }
-    }
+  // caller rows and phases of the listed visits [0, nb) (DIRECT)
+  auto issue_meta = [&](Sw2Meta &m, int nb) {
     if (DIRECT && lane < nb) {
       const int p = m.pos[lane];
       if (a.perm)
@@ -1295,7 +1286,12 @@ __device__ __forceinline__ void sweep2s_team(const InterpArgs &a, const Tiling &
       if (a.phase) cp_async8(&m.ph[lane], a.phase + p);
     }
   };
-  auto issue_rows = [&](const Sw2Meta &m, float2 *f, int nb) {
+  // tap records (9 x 16 bytes each) and sample rows of the listed visits [0, nb)
+  auto issue_data = [&](const Sw2Meta &m, float4 *rec, float2 *f, int nb) {
+    for (int ch = lane; ch < nb * 9; ch += 32) {
+      const int v = ch / 9, k = ch - 9 * v;
+      cp_async16(rec + ch, t.wsw + (long long)m.pos[v] * 9 + k);
+    }
     for (int v = 0; v < nb; v++) {
       const long long row = DIRECT ? (long long)m.row[v] : (long long)m.pos[v];
       if (on)
@@ -1308,8 +1304,9 @@ __device__ __forceinline__ void sweep2s_team(const InterpArgs &a, const Tiling &
   auto list_part = [&](Sw2Meta &m, int beg, int n, int ex, int vb) {
     for (int k = max(0, vb - ex); k < n && ex + k < vb + SW2_CAP; k++) m.pos[ex + k - vb] = beg + k;
   };
-  // list column xc into meta slot m and issue its records; returns its visits
-  auto list_col = [&](int xc, Sw2Meta &m, float2 *rec) -> int {
+  // list column xc into list slot m and issue its caller rows and phases;
+  // returns its visits
+  auto list_col = [&](int xc, Sw2Meta &m) -> int {
     const int end = le;
     if (xc == 0 && xs < 0) lb = rn;
     if (xc + 1 < x1 && rowb >= 0) {
@@ -1331,7 +1328,7 @@ __device__ __forceinline__ void sweep2s_team(const InterpArgs &a, const Tiling &
     list_part(m, lb, n, inc - n, 0);
     lb = end;
     __syncwarp();
-    issue_rec(m, rec, min(V, SW2_CAP));
+    issue_meta(m, min(V, SW2_CAP));
     cp_async_commit();
     return V;
   };
@@ -1342,8 +1339,9 @@ __device__ __forceinline__ void sweep2s_team(const InterpArgs &a, const Tiling &
 #pragma unroll
     for (int j = 0; j < 6; j++) acc[r][j] = make_float2(0.f, 0.f);
   // staged visits [vb, vb + nb) of the column; bin row q's visits are
-  // [ex[q], ex[q + 1]), each reaching band rows r = q - 5 .. q
-  auto sum_chunk = [&](const Sw2Meta &m, const int *exq, const float2 *rec, const float2 *f,
+  // [ex[q], ex[q + 1]), each reaching band rows r = q - 5 .. q.  The records'
+  // operand pairs (wr, wr) and (wi, -wi) feed cw_fma's two FFMA2 directly.
+  auto sum_chunk = [&](const Sw2Meta &m, const int *exq, const float4 *rec, const float2 *f,
                        int vb, int nb) {
     sfor<NQ>([&](auto QQ) {
       constexpr int Q = decltype(QQ)::value;
@@ -1351,20 +1349,23 @@ __device__ __forceinline__ void sweep2s_team(const InterpArgs &a, const Tiling &
       for (int v = lo; v < hi; v++) {
         float2 fv = f[v * 32 + lane];
         if (DIRECT && a.phase) fv = cmulc(m.ph[v], fv);
-        const float4 *r4 = reinterpret_cast<const float4 *>(rec + v * 12);
-        const float4 w01 = r4[0], w23 = r4[1], w45 = r4[2];
-        const float2 w1[6] = {make_float2(w01.x, w01.y), make_float2(w01.z, w01.w),
-                              make_float2(w23.x, w23.y), make_float2(w23.z, w23.w),
-                              make_float2(w45.x, w45.y), make_float2(w45.z, w45.w)};
+        const float4 *r4 = rec + v * 9;
+        float4 wp[6];
+#pragma unroll
+        for (int j = 0; j < 6; j++) wp[j] = r4[j];
         sfor<R>([&](auto RR) {
           constexpr int r = decltype(RR)::value;
           constexpr int j2 = r - Q + 5;
           if constexpr (j2 >= 0 && j2 < 6) {
-            const float2 vv = cw_mul<REAL>(rec[v * 12 + 6 + j2], fv);
+            const float4 w2p = r4[6 + j2 / 2];
+            const float2 w2 = (j2 & 1) ? make_float2(w2p.z, w2p.w) : make_float2(w2p.x, w2p.y);
+            const float2 vv = cw_mul<REAL>(w2, fv);
             const float2 vsw = make_float2(vv.y, vv.x);
             sfor<6>([&](auto JJ) {
               constexpr int j = decltype(JJ)::value;
-              acc[r][j] = cw_fma<REAL>(w1[j], vv, vsw, acc[r][j]);
+              float2 A = __ffma2_rn(make_float2(wp[j].x, wp[j].y), vv, acc[r][j]);
+              if (!REAL) A = __ffma2_rn(make_float2(wp[j].z, wp[j].w), vsw, A);
+              acc[r][j] = A;
             });
           }
         });
@@ -1372,27 +1373,29 @@ __device__ __forceinline__ void sweep2s_team(const InterpArgs &a, const Tiling &
     });
   };
   float2 *out = ck + (long long)slice * a.grid_elems + (long long)y0 * K1 * C + c0 + lane;
-  // prologue: records of the first two columns, sample rows of the first
-  int Vc = list_col(xs, meta[0], srec);
-  int Vn = list_col(xs + 1, meta[1], srec + SW2_CAP * 12);
+  // prologue: lists of the first two columns, records and rows of the first
+  int Vc = list_col(xs, meta[0]);
+  int Vn = list_col(xs + 1, meta[1]);
   cp_async_wait_group1();
   __syncwarp();
-  issue_rows(meta[0], sf, min(Vc, SW2_CAP));
+  issue_data(meta[0], srec, sf, min(Vc, SW2_CAP));
   cp_async_commit();
-  int sc = 0, fb = 0;  // list slot (of 3) and row block (of 2) of the column being summed
+  int sc = 0, fb = 0;  // list slot (of 3) and data block (of 2) of the column being summed
   for (int xb = xs; xb < x1; xb++) {
     const int s1 = sc == 2 ? 0 : sc + 1, s2 = sc == 0 ? 2 : sc - 1;
     int Vnn = 0;
     if (xb + 2 < x1)
-      Vnn = list_col(xb + 2, meta[s2], srec + s2 * SW2_CAP * 12);
+      Vnn = list_col(xb + 2, meta[s2]);
     else
       cp_async_commit();
-    cp_async_wait_group1();  // records of xb + 1, rows of xb
+    cp_async_wait_group1();  // list of xb + 1, records and rows of xb
     __syncwarp();
-    if (xb + 1 < x1) issue_rows(meta[s1], sf + (1 - fb) * SW2_CAP * 32, min(Vn, SW2_CAP));
+    if (xb + 1 < x1)
+      issue_data(meta[s1], srec + (1 - fb) * SW2_CAP * 9, sf + (1 - fb) * SW2_CAP * 32,
+                 min(Vn, SW2_CAP));
     cp_async_commit();
     Sw2Meta &m = meta[sc];
-    float2 *rec = srec + sc * SW2_CAP * 12;
+    float4 *rec = srec + fb * SW2_CAP * 9;
     float2 *f = sf + fb * SW2_CAP * 32;
     int exq[NQ + 1];
 #pragma unroll
@@ -1412,11 +1415,11 @@ __device__ __forceinline__ void sweep2s_team(const InterpArgs &a, const Tiling &
         __syncwarp();
         list_part(m, beg, n, ex, vb);
         __syncwarp();
-        issue_rec(m, rec, nb);
+        issue_meta(m, nb);
         cp_async_commit();
         cp_async_wait_all();
         __syncwarp();
-        issue_rows(m, f, nb);
+        issue_data(m, rec, f, nb);
         cp_async_commit();
         cp_async_wait_all();
         __syncwarp();
@@ -1436,7 +1439,7 @@ __device__ __forceinline__ void sweep2s_team(const InterpArgs &a, const Tiling &
       for (int j = 0; j < 5; j++) acc[r][j] = acc[r][j + 1];
       acc[r][5] = make_float2(0.f, 0.f);
     }
-    __syncwarp();  // list slot sc is listed again two columns on
+    __syncwarp();  // list slot sc is listed again two columns on, data block fb one column on
     Vc = Vn;
     Vn = Vnn;
     sc = s1;
@@ -1796,6 +1799,7 @@ cudaError_t run(Req &r) {
         if (thr == 0) return cudaSuccess;
         if (t.sweep_staged && CW == 32 && !(t.dense_on && t.dense_of && t.sweep_rows == 1)) {
           // staged sweep: reads the plan-order copy (1) or the caller's samples (2)
+          if (!t.wsw) return cudaErrorInvalidValue;
           const bool direct = t.sweep_staged == 2;
           if (!direct) {
             if (!t.sorted) return cudaErrorInvalidValue;

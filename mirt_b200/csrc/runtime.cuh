@@ -69,6 +69,7 @@ struct mirt_interp_plan {
   mirt::InterpArgs ag{};
   mirt::DMem wtap_g, k0tap_g, perm_g, phase_g;
   mirt::DMem orec_g;        // TMA gather: output records (sample index, phase) in gather order
+  mirt::DMem wsw;           // staged 2D row sweep: tap records with FFMA2 operand pairs, plan order
   mirt::DMem swept;        // row-sweep spread: the samples in plan order, [Mtot][C]
   mirt::DMem sweep_teams;  // row-sweep spread: balanced team list (int4 per team)
   std::vector<int4> team_host;  // the same list on the host
