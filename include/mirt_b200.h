@@ -390,6 +390,24 @@ int mirt_newfft_create(mirt_nufft **out, int32_t D, const int32_t *Nd, const int
 int mirt_newfft_kb_table(int32_t J, int32_t L, double *h);
 int mirt_newfft_kb_scale(int32_t N, int32_t J, int32_t K, double nmid, double *sn);
 
+/* newfft's table interpolators by ktype (phasing 'real'; host FP64):
+ *   MIRT_KTYPE_KB_MINMAX  'kb:minmax' (as mirt_newfft_kb_table / _kb_scale)
+ *   MIRT_KTYPE_KB_BEATTY  'kb:beatty': the KB kernel (kb_m = 0) of shape
+ *                         alpha = pi sqrt(J^2 / r^2 (r - 1/2)^2 - 0.8), r = K/N
+ *                         (nufft/newfft.m:275-283), scale 1 / KB-FT((n - nmid) / K)
+ *   MIRT_KTYPE_DIRIC      'diric': N'/K diric(t, N', K) with N' = 2 floor((K+1)/2) - 1
+ *                         (nufft/newfft.m:256-266, nufft/nufft_diric.m), scale 1;
+ *                         exact only when J = K, as the reference warns
+ * table: J*L+1 values at t = -J/2 + i/L; scale: N values (st.sn is their outer
+ * product over dimensions).  MIRT_ERR_ARG for unknown ktypes and for
+ * 'kb:beatty' where its shape is not real. */
+#define MIRT_KTYPE_KB_MINMAX 0
+#define MIRT_KTYPE_KB_BEATTY 1
+#define MIRT_KTYPE_DIRIC 2
+int mirt_newfft_ktype_table(int32_t ktype, int32_t N, int32_t J, int32_t K, int32_t L, double *h);
+int mirt_newfft_ktype_scale(int32_t ktype, int32_t N, int32_t J, int32_t K, double nmid,
+	double *sn);
+
 /* Capture one batched step of the plan -- forward x -> X when x is given,
  * then adjoint X -> xa when xa is given -- into a CUDA graph (on an internal
  * capture stream) and return it instantiated; mirt_graph_launch replays it

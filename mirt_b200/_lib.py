@@ -119,6 +119,8 @@ _SIGS = {
                             _i32, _vp], C.c_int),
     "mirt_newfft_kb_table": ([_i32, _i32, _dp], C.c_int),
     "mirt_newfft_kb_scale": ([_i32, _i32, _i32, C.c_double, _dp], C.c_int),
+    "mirt_newfft_ktype_table": ([_i32, _i32, _i32, _i32, _i32, _dp], C.c_int),
+    "mirt_newfft_ktype_scale": ([_i32, _i32, _i32, _i32, C.c_double, _dp], C.c_int),
 }
 
 _lib: C.CDLL | None = None

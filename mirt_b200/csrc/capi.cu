@@ -33,6 +33,10 @@ std::vector<std::complex<double>> scale1(int N, int K, const std::vector<double>
                                          double beta);
 void kb_table(int J, int L, std::vector<double> &h);
 std::vector<double> kb_scale(int N, int J, int K, double nmid);
+void kb_table_alpha(int J, int L, double alpha_full, std::vector<double> &h);
+std::vector<double> kb_scale_alpha(int N, int J, int K, double nmid, double alpha);
+double kb_beatty_alpha(int N, int J, int K);
+void diric_table(int J, int K, int L, std::vector<double> &h);
 }  // namespace mirt
 
 using namespace mirt;
@@ -2317,6 +2321,47 @@ int mirt_newfft_kb_scale(int32_t N, int32_t J, int32_t K, double nmid, double *s
     return fail(MIRT_ERR_ARG, "N, K must be positive, J in 1..16");
   if (!sn) return fail(MIRT_ERR_ARG, "output pointer is NULL");
   std::vector<double> s = kb_scale(N, J, K, nmid);
+  std::copy(s.begin(), s.end(), sn);
+  return MIRT_OK;
+}
+
+int mirt_newfft_ktype_table(int32_t ktype, int32_t N, int32_t J, int32_t K, int32_t L, double *h) {
+  if (N < 1 || J < 1 || J > MIRT_JMAX || K < 1 || L < 1)
+    return fail(MIRT_ERR_ARG, "N, K, L must be positive, J in 1..16");
+  if (!h) return fail(MIRT_ERR_ARG, "output pointer is NULL");
+  std::vector<double> t;
+  switch (ktype) {
+    case MIRT_KTYPE_KB_MINMAX: kb_table(J, L, t); break;
+    case MIRT_KTYPE_KB_BEATTY: {
+      const double a = kb_beatty_alpha(N, J, K);
+      if (!(a > 0)) return fail(MIRT_ERR_ARG, "kb:beatty has no real shape for this J, K/N");
+      kb_table_alpha(J, L, a, t);
+      break;
+    }
+    case MIRT_KTYPE_DIRIC: diric_table(J, K, L, t); break;
+    default: return fail(MIRT_ERR_ARG, "unknown ktype");
+  }
+  std::copy(t.begin(), t.end(), h);
+  return MIRT_OK;
+}
+
+int mirt_newfft_ktype_scale(int32_t ktype, int32_t N, int32_t J, int32_t K, double nmid,
+                            double *sn) {
+  if (N < 1 || J < 1 || J > MIRT_JMAX || K < 1)
+    return fail(MIRT_ERR_ARG, "N, K must be positive, J in 1..16");
+  if (!sn) return fail(MIRT_ERR_ARG, "output pointer is NULL");
+  std::vector<double> s;
+  switch (ktype) {
+    case MIRT_KTYPE_KB_MINMAX: s = kb_scale(N, J, K, nmid); break;
+    case MIRT_KTYPE_KB_BEATTY: {
+      const double a = kb_beatty_alpha(N, J, K);
+      if (!(a > 0)) return fail(MIRT_ERR_ARG, "kb:beatty has no real shape for this J, K/N");
+      s = kb_scale_alpha(N, J, K, nmid, a);
+      break;
+    }
+    case MIRT_KTYPE_DIRIC: s.assign(N, 1.0); break;
+    default: return fail(MIRT_ERR_ARG, "unknown ktype");
+  }
   std::copy(s.begin(), s.end(), sn);
   return MIRT_OK;
 }

@@ -238,15 +238,16 @@ bool minmax_kb_table(int N, int J, int K, int L, std::vector<cd> &h) {
   return true;
 }
 
-// Real table of newfft's default 'table0' / 'table1' modes (ktype
-// 'kb:minmax', phasing 'real'): the KB kernel sampled at t = -J/2 + i / L,
-// i = 0 .. J*L.  The 'ratio' construction reads the sparse interpolator of a
-// fake N = J problem column by column; for a kernel that depends only on the
-// offset t that is the kernel itself, symmetric, zero at |t| = J/2.  The
-// inline kernel carries alpha printed with %g.
-void kb_table(int J, int L, std::vector<double> &h) {
+// Real table of newfft's KB interpolators (phasing 'real'): the KB kernel
+// (kb_m = 0) of shape alpha sampled at t = -J/2 + i / L, i = 0 .. J*L.  The
+// 'ratio' construction reads the sparse interpolator of a fake N = J problem
+// column by column; for a kernel that depends only on the offset t that is
+// the kernel itself, symmetric, zero at |t| = J/2.  The inline kernel carries
+// alpha printed with %g (nufft/kaiser_bessel.m:80-82).  'kb:minmax' (the
+// default of 'table0' / 'table1'): alpha = 2.34 J; 'kb:beatty': kb_beatty_alpha.
+void kb_table_alpha(int J, int L, double alpha_full, std::vector<double> &h) {
   char buf[64];
-  std::snprintf(buf, sizeof buf, "%g", 2.34 * J);
+  std::snprintf(buf, sizeof buf, "%g", alpha_full);
   const double alpha = std::atof(buf);
   const double i0a = bessel_i0(alpha);
   h.assign((size_t)J * L + 1, 0.0);
@@ -259,12 +260,52 @@ void kb_table(int J, int L, std::vector<double> &h) {
   }
 }
 
-// 1D scaling factors of newfft with ktype 'kb:minmax': 1 / KB-FT((n - Nmid) / K)
-// (alpha = 2.34 J as a number, no %g round trip here).
-std::vector<double> kb_scale(int N, int J, int K, double nmid) {
+void kb_table(int J, int L, std::vector<double> &h) { kb_table_alpha(J, L, 2.34 * J, h); }
+
+// 1D scaling factors of newfft's KB interpolators: 1 / KB-FT((n - Nmid) / K)
+// (alpha as a number, no %g round trip here: st.kb_alf, nufft/newfft.m:352-356).
+std::vector<double> kb_scale_alpha(int N, int J, int K, double nmid, double alpha) {
   std::vector<double> s(N);
-  for (int n = 0; n < N; n++) s[n] = 1.0 / kb_ft((n - nmid) / K, J, 2.34 * J);
+  for (int n = 0; n < N; n++) s[n] = 1.0 / kb_ft((n - nmid) / K, J, alpha);
   return s;
+}
+
+std::vector<double> kb_scale(int N, int J, int K, double nmid) {
+  return kb_scale_alpha(N, J, K, nmid, 2.34 * J);
+}
+
+// KB shape of ktype 'kb:beatty' (Beatty et al.): pi sqrt(J^2 / r^2 (r - 1/2)^2 - 0.8)
+// with r = K / N (nufft/newfft.m:275-283); kb_m = 0.  0 when the root is not real.
+double kb_beatty_alpha(int N, int J, int K) {
+  const double r = (double)K / (double)N;
+  const double a = (double)J * J / (r * r) * (r - 0.5) * (r - 0.5) - 0.8;
+  return a > 0 ? M_PI * std::sqrt(a) : 0.0;
+}
+
+// Table of ktype 'diric' with phasing 'real' (nufft/newfft.m:256-266,
+// nufft/nufft_diric.m:31-36): the kernel N' / K diric(k, N', K) with the odd
+// N' = 2 floor((K + 1) / 2) - 1 and the true Dirichlet function
+// sin(pi k N' / K) / (N' sin(pi k / K)) (sign(cos(pi k (N' - 1) / K)) where
+// |sin(pi k / K)| <= 1e-12), read by the 'fast' construction
+// (nufft/private/newfft_table_init.m:160-169, nufft/private/nufft_coef.m) at
+// t = -J/2 + i / L, i < J L, the last entry repeating the first.
+void diric_table(int J, int K, int L, std::vector<double> &h) {
+  const int Np = 2 * ((K + 1) / 2) - 1;
+  h.assign((size_t)J * L + 1, 0.0);
+  for (size_t i = 0; i + 1 < h.size(); i++) {
+    const double k = -J / 2.0 + (double)i / L;
+    const double t = M_PI / K * k;
+    const double sn = std::sin(t);
+    double f;
+    if (std::fabs(sn) > 1e-12) {
+      f = std::sin(Np * t) / (Np * sn);
+    } else {
+      const double c = std::cos(t * (Np - 1));
+      f = c > 0 ? 1.0 : (c < 0 ? -1.0 : 0.0);
+    }
+    h[i] = (double)Np / K * f;
+  }
+  h[h.size() - 1] = h[0];
 }
 
 }  // namespace mirt

@@ -381,22 +381,48 @@ def newfft_kb_scale(N: int, J: int, K: int, nmid: float) -> np.ndarray:
     return s
 
 
+_KTYPES = {"kb:minmax": 0, "kb:beatty": 1, "diric": 2}
+
+
+def newfft_table(ktype: str, N: int, J: int, K: int, L: int) -> np.ndarray:
+    """Real table of newfft's interpolator `ktype` ('kb:minmax', 'kb:beatty',
+    'diric'; phasing 'real'), [J*L+1] (see mirt_newfft_ktype_table)."""
+    if ktype not in _KTYPES:
+        raise ValueError(f"ktype must be one of {sorted(_KTYPES)}")
+    h = np.empty(int(J) * int(L) + 1)
+    check(load().mirt_newfft_ktype_table(_KTYPES[ktype], int(N), int(J), int(K), int(L),
+                                         h.ctypes.data_as(_dp)))
+    return h
+
+
+def newfft_scale(ktype: str, N: int, J: int, K: int, nmid: float) -> np.ndarray:
+    """1D scaling factors of newfft's interpolator `ktype`, [N]."""
+    if ktype not in _KTYPES:
+        raise ValueError(f"ktype must be one of {sorted(_KTYPES)}")
+    s = np.empty(int(N))
+    check(load().mirt_newfft_ktype_scale(_KTYPES[ktype], int(N), int(J), int(K), float(nmid),
+                                         s.ctypes.data_as(_dp)))
+    return s
+
+
 class NewfftPlan(NufftPlan):
     """st = newfft(om, Nd, 'Jd', Jd, 'Kd', Kd, 'n_shift', n_shift, 'mode',
     'table0' | 'table1', 'oversample', Ld, 'phasing', phasing) on the device
     (nufft/newfft.m, nufft/private/newfft_table_init.m).
 
     phasing 'real' (the reference's default) with ``tables=None`` builds the
-    'kb:minmax' real tables and scaling factors in the library; any other
-    interpolator is given as ``tables`` (one 1D table per dimension, real or
-    complex, J*L+1 values) and ``sn`` ([(Nd)], first index fastest).
+    real tables and scaling factors of ``ktype`` in the library ('kb:minmax',
+    the reference's default, 'kb:beatty' or 'diric'); any other interpolator
+    is given as ``tables`` (one 1D table per dimension, real or complex, J*L+1
+    values) and ``sn`` ([(Nd)], first index fastest).
     phasing 'real' applies phase_before / phase_after with Nmid = floor(N/2);
     'complex' applies only exp(i om . n_shift) per sample.  Layouts and
     methods are those of NufftPlan.
     """
 
     def __init__(self, om, Nd, Jd=None, Kd=None, n_shift=None, mode="table1", Ld=None,
-                 phasing="real", tables=None, sn=None, ncol=1, slice_moff=None, stream=None):
+                 phasing="real", tables=None, sn=None, ncol=1, slice_moff=None, stream=None,
+                 ktype="kb:minmax"):
         om = np.asarray(om, dtype=np.float64)
         D = 1 if om.ndim == 1 else om.shape[1]
         Nd = _i32(Nd)
@@ -414,13 +440,13 @@ class NewfftPlan(NufftPlan):
         self.Nmid = (np.floor(Nd / 2) if phasing == "real" else (Nd - 1) / 2).astype(np.float64)
         if tables is None:
             if phasing != "real":
-                raise ValueError("built-in tables are the 'kb:minmax' real ones; pass tables "
+                raise ValueError("built-in tables are the phasing 'real' ones; pass tables "
                                  "and sn for other phasings")
-            tables = [newfft_kb_table(Jd[d], Ld[d]) for d in range(D)]
+            tables = [newfft_table(ktype, Nd[d], Jd[d], Kd[d], Ld[d]) for d in range(D)]
             s = np.ones(1)
             for d in range(D):
-                s = np.outer(s.ravel(order="F"), newfft_kb_scale(Nd[d], Jd[d], Kd[d],
-                                                                 self.Nmid[d]))
+                s = np.outer(s.ravel(order="F"), newfft_scale(ktype, Nd[d], Jd[d], Kd[d],
+                                                              self.Nmid[d]))
             sn = s.ravel(order="F")
         if sn is None:
             raise ValueError("sn is required with caller tables")

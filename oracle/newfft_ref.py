@@ -17,6 +17,15 @@ What is restated, with the reference lines followed:
   repeats the first (0 at |t| = J/2).
 * ``kb_scale``           1 / kaiser_bessel_ft((n - Nmid) / K, J, alpha, 0, 1),
   nufft/newfft.m:352-356, outer product nufft/newfft.m:366-375
+* ``beatty_alpha``       ktype 'kb:beatty': pi sqrt(J^2 / r^2 (r - 1/2)^2 - 0.8),
+  r = K / N, kb_m = 0 (nufft/newfft.m:275-283); its table and scale are
+  ``kb_table`` / ``kb_scale`` with that alpha
+* ``diric_table``        ktype 'diric' with phasing 'real' (nufft/newfft.m:256-266):
+  N' / K nufft_diric(t, N', K, true) with N' = 2 floor((K + 1) / 2) - 1
+  (nufft/nufft_diric.m:31-36), read by the 'fast' construction of
+  nufft/private/newfft_table_init.m:160-169 through nufft/private/nufft_coef.m
+  (the kernel at t = -J/2 + i/L, i < J L; the last entry repeats the first);
+  its scaling factors are 1 (nufft/newfft.m:354-355)
 * ``phase_before``       nufft/newfft.m:511-520
 * ``phase_after``        nufft/newfft.m:522-527
 * ``newfft_for/adj``     nufft/private/newfft_approx_for.m:15-63,
@@ -45,9 +54,28 @@ def kb_alpha(J):
     return 2.34 * J
 
 
-def kb_table(J: int, L: int) -> np.ndarray:
-    """Real [J*L+1] table of the 'kb:minmax' kernel (alpha printed with %g)."""
-    alpha = float(f"{kb_alpha(J):g}")
+def beatty_alpha(N, J, K):
+    r = K / N
+    return np.pi * np.sqrt(J ** 2 / r ** 2 * (r - 0.5) ** 2 - 0.8)
+
+
+def diric_table(J: int, K: int, L: int) -> np.ndarray:
+    """Real [J*L+1] table of ktype 'diric' with phasing 'real'."""
+    Np = 2 * ((K + 1) // 2) - 1
+    k = -J / 2 + np.arange(J * L) / L
+    t = np.pi / K * k
+    f = np.sin(t)
+    big = np.abs(f) > 1e-12
+    out = np.sign(np.cos(t * (Np - 1)))
+    out[big] = np.sin(Np * t[big]) / (Np * f[big])
+    h = Np / K * out
+    return np.append(h, h[0])
+
+
+def kb_table(J: int, L: int, alpha=None) -> np.ndarray:
+    """Real [J*L+1] table of the KB kernel (kb_m = 0) of shape alpha (default
+    2.34 J: 'kb:minmax'), alpha printed with %g as the inline kernel does."""
+    alpha = float(f"{(kb_alpha(J) if alpha is None else alpha):g}")
     t = (np.arange(J * L + 1) - J * L / 2) / L
     h = np.zeros(J * L + 1)
     inside = np.abs(t) < J / 2
@@ -56,9 +84,29 @@ def kb_table(J: int, L: int) -> np.ndarray:
     return h
 
 
-def kb_scale(N: int, J: int, K: int, Nmid: float) -> np.ndarray:
+def kb_scale(N: int, J: int, K: int, Nmid: float, alpha=None) -> np.ndarray:
     nc = np.arange(N) - Nmid
-    return 1.0 / nr.kaiser_bessel_ft(nc / K, J, kb_alpha(J), 0.0, 1)
+    return 1.0 / nr.kaiser_bessel_ft(nc / K, J, kb_alpha(J) if alpha is None else alpha, 0.0, 1)
+
+
+def ktype_table(ktype, N, J, K, L):
+    if ktype == "kb:minmax":
+        return kb_table(J, L)
+    if ktype == "kb:beatty":
+        return kb_table(J, L, beatty_alpha(N, J, K))
+    if ktype == "diric":
+        return diric_table(J, K, L)
+    raise ValueError(ktype)
+
+
+def ktype_scale(ktype, N, J, K, Nmid):
+    if ktype == "kb:minmax":
+        return kb_scale(N, J, K, Nmid)
+    if ktype == "kb:beatty":
+        return kb_scale(N, J, K, Nmid, beatty_alpha(N, J, K))
+    if ktype == "diric":
+        return np.ones(N)
+    raise ValueError(ktype)
 
 
 def phase_before(Kd, Nmid) -> np.ndarray:
@@ -71,10 +119,10 @@ def phase_before(Kd, Nmid) -> np.ndarray:
 
 
 def newfft_init(om, Nd, Jd=None, Kd=None, n_shift=None, mode="table1", Ld=None,
-                phasing="real", h=None, sn=None) -> dict:
+                phasing="real", h=None, sn=None, ktype="kb:minmax") -> dict:
     """st of newfft(om, Nd, 'Jd', Jd, 'Kd', Kd, 'n_shift', n_shift, 'mode', mode,
-    'oversample', Ld, 'phasing', phasing) with ktype 'kb:minmax' (or the
-    caller's tables h and scaling factors sn)."""
+    'oversample', Ld, 'phasing', phasing, 'ktype', ktype) for ktype 'kb:minmax',
+    'kb:beatty' or 'diric' (or the caller's tables h and scaling factors sn)."""
     om = np.asarray(om, dtype=np.float64)
     if om.ndim == 1:
         om = om[:, None]
@@ -88,11 +136,11 @@ def newfft_init(om, Nd, Jd=None, Kd=None, n_shift=None, mode="table1", Ld=None,
     Ld = tuple(Ld if np.ndim(Ld) else [int(Ld)] * dd)
     Nmid = nmid_of(Nd, phasing)
     if h is None:
-        h = [kb_table(Jd[d], Ld[d]) for d in range(dd)]
+        h = [ktype_table(ktype, Nd[d], Jd[d], Kd[d], Ld[d]) for d in range(dd)]
     if sn is None:
         s = np.ones(1)
         for d in range(dd):
-            s = np.outer(s.ravel(order="F"), kb_scale(Nd[d], Jd[d], Kd[d], Nmid[d]))
+            s = np.outer(s.ravel(order="F"), ktype_scale(ktype, Nd[d], Jd[d], Kd[d], Nmid[d]))
         sn = s.reshape(tuple(Nd), order="F")
     st = dict(om=om, Nd=tuple(Nd), Jd=Jd, Kd=Kd, Ld=Ld, order=order, Nmid=Nmid,
               n_shift=n_shift, h=h, sn=np.asarray(sn).reshape(tuple(Nd), order="F"),

@@ -48,6 +48,30 @@ def test_reference_selftest_setups(Nd, mode):
     assert _mpd(nr.dtft_adj(Xe, om, Nd, ns), st.adj(Xe)) < BOUND[mode]
 
 
+@pytest.mark.parametrize("ktype", ["kb:beatty", "diric"])
+@pytest.mark.parametrize("Nd", [(20,), (6, 5)])
+@pytest.mark.parametrize("mode", ["table0", "table1"])
+def test_other_interpolators(ktype, Nd, mode):
+    """newfft's 'kb:beatty' and 'diric' tables built in the library: the
+    oracle's forward / adjoint and the exact DTFT's bounds."""
+    Jd = tuple(2 * np.asarray(Nd)) if ktype == "diric" else None
+    if Jd is not None and max(Jd) > 16:
+        pytest.skip("J > 16")
+    rng = np.random.default_rng(2)
+    om = 3 * 2 * np.pi * (rng.random((100, len(Nd))) - 0.5)
+    x0 = rng.random(Nd)
+    st = mb.newfft(om, Nd, Jd=Jd, mode=mode, ktype=ktype)
+    so = nf.newfft_init(om, Nd, Jd=Jd, mode=mode, ktype=ktype)
+    X = st.fft(x0)
+    Xo = nf.newfft_for(x0, so)
+    assert rel_l2(X, Xo) <= TOL
+    assert rel_l2(st.adj(Xo), nf.newfft_adj(Xo, so)) <= TOL
+    ns = np.zeros(len(Nd))
+    Xe = nr.dtft(x0, om, ns)
+    assert _mpd(Xe, X) < BOUND[mode]
+    assert _mpd(nr.dtft_adj(Xe, om, Nd, ns), st.adj(Xe)) < BOUND[mode]
+
+
 def test_batched_slices_coils_and_shift():
     """Three trajectories of uneven length, 3 columns, centred image (n_shift =
     N/2), table1: every slice and column against the oracle."""

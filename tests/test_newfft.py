@@ -121,3 +121,44 @@ def test_oracle_complex_tables_without_phases_is_nufft():
     a = nf.newfft_for(x, so)
     b = nr.nufft(x, st, fw)
     assert np.max(np.abs(a - b)) <= 1e-12 * np.max(np.abs(b))
+
+
+@pytest.mark.parametrize("ktype", ["kb:beatty", "diric"])
+@pytest.mark.parametrize("Nd", [(21,), (20,), (20, 10), (6,), (6, 5)])
+@pytest.mark.parametrize("mode", ["table0", "table1"])
+def test_oracle_ktypes_match_exact_dtft(ktype, Nd, mode):
+    """The oracle's 'kb:beatty' and 'diric' interpolators (diric with Jd = 2 Nd
+    = Kd, as the reference's self-test sets it, nufft/newfft.m:629-635) on the
+    self-test set-up, within the same bounds as 'kb:minmax'."""
+    Jd = tuple(2 * np.asarray(Nd)) if ktype == "diric" else None
+    if Jd is not None and max(Jd) > 16:
+        pytest.skip("J > 16")
+    om, x0 = _case(Nd)
+    ns = np.zeros(len(Nd))
+    Xe = nr.dtft(x0, om, ns)
+    st = nf.newfft_init(om, Nd, Jd=Jd, mode=mode, ktype=ktype)
+    assert _mpd(Xe, nf.newfft_for(x0, st)) < BOUND[mode]
+    assert _mpd(nr.dtft_adj(Xe, om, Nd, ns), nf.newfft_adj(Xe, st)) < BOUND[mode]
+
+
+@pytest.mark.parametrize("ktype", ["kb:minmax", "kb:beatty", "diric"])
+@pytest.mark.parametrize("N,J,K,L", [(20, 6, 40, 512), (21, 6, 42, 2048), (6, 12, 12, 512),
+                                     (64, 8, 128, 1024)])
+def test_ktype_table_and_scale_builders(ktype, N, J, K, L):
+    """The library's host builders of the three interpolators against the
+    oracle (FP64 both)."""
+    nmid = np.floor(N / 2)
+    assert np.max(np.abs(mb.newfft_table(ktype, N, J, K, L) - nf.ktype_table(ktype, N, J, K, L))) <= 1e-13
+    s, so = mb.newfft_scale(ktype, N, J, K, nmid), nf.ktype_scale(ktype, N, J, K, nmid)
+    assert np.max(np.abs(s - so) / np.abs(so)) <= 1e-12
+
+
+def test_ktype_errors():
+    with pytest.raises(ValueError, match="ktype"):
+        mb.newfft_table("minmax:tuned", 20, 6, 40, 512)
+    lib = mb.load()
+    h = np.empty(6 * 8 + 1)
+    assert lib.mirt_newfft_ktype_table(7, 20, 6, 40, 8, h.ctypes.data_as(mb._lib._dp)) != 0
+    # kb:beatty's shape is not real for a K/N too close to 1/2
+    with pytest.raises(mb.MirtError, match="beatty"):
+        mb.newfft_table("kb:beatty", 20, 2, 12, 8)
