@@ -398,12 +398,17 @@ int mirt_newfft_kb_scale(int32_t N, int32_t J, int32_t K, double nmid, double *s
  *   MIRT_KTYPE_DIRIC      'diric': N'/K diric(t, N', K) with N' = 2 floor((K+1)/2) - 1
  *                         (nufft/newfft.m:256-266, nufft/nufft_diric.m), scale 1;
  *                         exact only when J = K, as the reference warns
+ *   MIRT_KTYPE_MINMAX_KB  'minmax:kb': the min-max interpolator with KB-fitted
+ *                         scaling (nufft/newfft.m:315-320, 384-395), the fit at
+ *                         Nmid = floor(N/2), no phase; scale the real part of
+ *                         nufft_scale1 at nmid (N <= K)
  * table: J*L+1 values at t = -J/2 + i/L; scale: N values (st.sn is their outer
  * product over dimensions).  MIRT_ERR_ARG for unknown ktypes and for
  * 'kb:beatty' where its shape is not real. */
 #define MIRT_KTYPE_KB_MINMAX 0
 #define MIRT_KTYPE_KB_BEATTY 1
 #define MIRT_KTYPE_DIRIC 2
+#define MIRT_KTYPE_MINMAX_KB 3
 int mirt_newfft_ktype_table(int32_t ktype, int32_t N, int32_t J, int32_t K, int32_t L, double *h);
 int mirt_newfft_ktype_scale(int32_t ktype, int32_t N, int32_t J, int32_t K, double nmid,
 	double *sn);

@@ -37,6 +37,8 @@ void kb_table_alpha(int J, int L, double alpha_full, std::vector<double> &h);
 std::vector<double> kb_scale_alpha(int N, int J, int K, double nmid, double alpha);
 double kb_beatty_alpha(int N, int J, int K);
 void diric_table(int J, int K, int L, std::vector<double> &h);
+bool minmax_kb_table_real(int N, int J, int K, int L, std::vector<double> &h);
+std::vector<double> minmax_kb_scale_real(int N, int J, int K, double Nmid);
 }  // namespace mirt
 
 using namespace mirt;
@@ -2339,6 +2341,11 @@ int mirt_newfft_ktype_table(int32_t ktype, int32_t N, int32_t J, int32_t K, int3
       break;
     }
     case MIRT_KTYPE_DIRIC: diric_table(J, K, L, t); break;
+    case MIRT_KTYPE_MINMAX_KB:
+      if (N > K) return fail(MIRT_ERR_ARG, "minmax:kb needs N <= K");
+      if (!minmax_kb_table_real(N, J, K, L, t))
+        return fail(MIRT_ERR_ARG, "singular min-max matrix for this N, J, K");
+      break;
     default: return fail(MIRT_ERR_ARG, "unknown ktype");
   }
   std::copy(t.begin(), t.end(), h);
@@ -2360,6 +2367,7 @@ int mirt_newfft_ktype_scale(int32_t ktype, int32_t N, int32_t J, int32_t K, doub
       break;
     }
     case MIRT_KTYPE_DIRIC: s.assign(N, 1.0); break;
+    case MIRT_KTYPE_MINMAX_KB: s = minmax_kb_scale_real(N, J, K, nmid); break;
     default: return fail(MIRT_ERR_ARG, "unknown ktype");
   }
   std::copy(s.begin(), s.end(), sn);

@@ -149,10 +149,10 @@ double diric(double k, int N, int K) { return nufft_sinc(k / ((double)K / (doubl
 
 }  // namespace
 
-// alphas (L+1 real coefficients) and beta of nufft_alpha_kb_fit(N, J, K)
-void alpha_kb_fit(int N, int J, int K, std::vector<double> &alphas, double &beta) {
+// alphas (L+1 real coefficients) and beta of nufft_alpha_kb_fit(N, J, K, 'Nmid', Nmid)
+void alpha_kb_fit_nmid(int N, int J, int K, double Nmid, std::vector<double> &alphas,
+                       double &beta) {
   beta = 1.0;
-  const double Nmid = (N - 1) / 2.0;
   const int L = N > 40 ? 13 : (int)std::ceil(N / 3.0);
   double kb_a = kb_alpha_best(J, (double)K / (double)N);
   // kaiser_bessel_ft('inline', ...) prints alpha with %g into its kernel string
@@ -170,6 +170,11 @@ void alpha_kb_fit(int N, int J, int K, std::vector<double> &alphas, double &beta
   alphas.assign(L + 1, 0.0);
   alphas[0] = coef[0];
   for (int l = 1; l <= L; l++) alphas[l] = coef[l] / 2;
+}
+
+// nufft_alpha_kb_fit(N, J, K) (its default Nmid = (N - 1) / 2)
+void alpha_kb_fit(int N, int J, int K, std::vector<double> &alphas, double &beta) {
+  alpha_kb_fit_nmid(N, J, K, (N - 1) / 2.0, alphas, beta);
 }
 
 // 1D scaling factors nufft_scale1(N, K, alpha, beta, (N-1)/2)
@@ -236,6 +241,78 @@ bool minmax_kb_table(int N, int J, int K, int L, std::vector<cd> &h) {
     for (int l = 0; l < L; l++) h[(size_t)blk * L + l] = p[(size_t)l + (size_t)jj * L];
   h[(size_t)J * L] = 0;
   return true;
+}
+
+// newfft's ktype 'minmax:kb' with phasing 'real' (nufft/newfft.m:315-320,
+// 384-395): alphas and beta of nufft_alpha_kb_fit with Nmid = floor(N / 2),
+// T = inv(C'SS'C) and r of nufft/private/nufft_T.m / nufft_r.m (sinc diric,
+// tol 0: the plain inverse), coefficients c = T r without phase (phasing
+// 'real'), read by the 'fast' construction of
+// nufft/private/newfft_table_init.m:160-169 (columns J .. 1 of the sparse
+// interpolator at t1 = J/2 - 1 + i/L, the last entry repeating the first).
+// The coefficients are real.
+bool minmax_kb_table_real(int N, int J, int K, int L, std::vector<double> &h) {
+  std::vector<double> alpha;
+  double beta;
+  alpha_kb_fit_nmid(N, J, K, std::floor(N / 2.0), alpha, beta);
+  const int La = (int)alpha.size() - 1;
+  std::vector<double> T(J * J, 0.0);
+  for (int a = 0; a < J; a++)
+    for (int b = 0; b < J; b++) {
+      double s = 0;
+      for (int l1 = -La; l1 <= La; l1++)
+        for (int l2 = -La; l2 <= La; l2++) {
+          const double tmp = (double)(b - a) + beta * (double)(l1 - l2);
+          s += alpha[std::abs(l1)] * alpha[std::abs(l2)] * diric(tmp, N, K);
+        }
+      T[a * J + b] = s;
+    }
+  if (!invert(T, J)) return false;
+  const double gam = 2 * M_PI / K;
+  std::vector<double> p((size_t)L * J, 0.0);  // used columns 0..J-1 of p [L, K]
+  std::vector<double> r(J), arg(J);
+  for (int l = 0; l < L; l++) {
+    const double t1 = (J / 2.0 - 1) + (double)l / L;
+    const double om = t1 * 2 * M_PI / K;
+    const double koff = std::floor(om / gam - J / 2.0);
+    const double dk = om / gam - koff;
+    for (int j = 0; j < J; j++) {
+      arg[j] = -(double)(j + 1) + dk;
+      double s = 0;
+      for (int l1 = -La; l1 <= La; l1++) s += alpha[std::abs(l1)] * diric(arg[j] + l1 * beta, N, K);
+      r[j] = s;
+    }
+    for (int j = 0; j < J; j++) {
+      double c = 0;
+      for (int i = 0; i < J; i++) c += T[j * J + i] * r[i];
+      long long col = (long long)(koff + (j + 1));
+      col = ((col % K) + K) % K;
+      if (col < J) p[(size_t)l + (size_t)col * L] += c;
+    }
+  }
+  h.assign((size_t)J * L + 1, 0.0);
+  for (int jj = J - 1, blk = 0; jj >= 0; jj--, blk++)
+    for (int l = 0; l < L; l++) h[(size_t)blk * L + l] = p[(size_t)l + (size_t)jj * L];
+  h[(size_t)J * L] = h[0];
+  return true;
+}
+
+// scaling factors of newfft's 'minmax:kb' (phasing 'real'): the real part of
+// nufft_scale1(N, K, alpha, beta, Nmid) with the alphas fitted at Nmid
+// (nufft/newfft.m:360-364: reale)
+std::vector<double> minmax_kb_scale_real(int N, int J, int K, double Nmid) {
+  std::vector<double> alpha;
+  double beta;
+  alpha_kb_fit_nmid(N, J, K, Nmid, alpha, beta);
+  const int L = (int)alpha.size() - 1;
+  std::vector<double> sn(N);
+  for (int n = 0; n < N; n++) {
+    const double g = (2 * M_PI / K) * (n - Nmid) * beta;
+    cd s(0, 0);
+    for (int l1 = -L; l1 <= L; l1++) s += alpha[std::abs(l1)] * std::exp(cd(0, g * l1));
+    sn[n] = s.real();
+  }
+  return sn;
 }
 
 // Real table of newfft's KB interpolators (phasing 'real'): the KB kernel

@@ -20,6 +20,10 @@ What is restated, with the reference lines followed:
 * ``beatty_alpha``       ktype 'kb:beatty': pi sqrt(J^2 / r^2 (r - 1/2)^2 - 0.8),
   r = K / N, kb_m = 0 (nufft/newfft.m:275-283); its table and scale are
   ``kb_table`` / ``kb_scale`` with that alpha
+* ``minmax_kb_table``    ktype 'minmax:kb' with phasing 'real' (nufft/newfft.m:315-320,
+  384-395): alphas / beta of nufft_alpha_kb_fit at Nmid = floor(N/2), c = T r
+  (nufft/private/nufft_T.m, nufft_r.m) without phase, read by the 'fast'
+  construction; scale the real part of nufft_scale1 at Nmid
 * ``diric_table``        ktype 'diric' with phasing 'real' (nufft/newfft.m:256-266):
   N' / K nufft_diric(t, N', K, true) with N' = 2 floor((K + 1) / 2) - 1
   (nufft/nufft_diric.m:31-36), read by the 'fast' construction of
@@ -89,6 +93,30 @@ def kb_scale(N: int, J: int, K: int, Nmid: float, alpha=None) -> np.ndarray:
     return 1.0 / nr.kaiser_bessel_ft(nc / K, J, kb_alpha(J) if alpha is None else alpha, 0.0, 1)
 
 
+def minmax_kb_table(N, J, K, L):
+    """Real [J*L+1] table of ktype 'minmax:kb' with phasing 'real': the min-max
+    coefficients c = T r (alphas fitted at Nmid = floor(N/2), no phase) read
+    by the 'fast' construction, the last entry repeating the first."""
+    alpha, beta = nr.nufft_alpha_kb_fit(N, J, K, Nmid=np.floor(N / 2))
+    T = nr.nufft_T(N, J, K, alpha, beta)
+    t1 = (J / 2 - 1) + np.arange(L, dtype=np.float64) / L
+    om1 = t1 * 2 * np.pi / K
+    r, _ = nr.nufft_r(om1, N, J, K, alpha, beta)
+    c = np.real(T @ r)
+    koff = nr.nufft_offset(om1, J, K)
+    kd = np.mod(np.arange(1, J + 1)[:, None] + koff[None, :], K).astype(np.int64)
+    p = np.zeros((L, K))
+    for j in range(J):
+        np.add.at(p, (np.arange(L), kd[j]), c[j])
+    h = np.concatenate([p[:, jj] for jj in range(J - 1, -1, -1)])
+    return np.append(h, h[0])
+
+
+def minmax_kb_scale(N, J, K, Nmid):
+    alpha, beta = nr.nufft_alpha_kb_fit(N, J, K, Nmid=Nmid)
+    return np.real(nr.nufft_scale1(N, K, alpha, beta, Nmid))
+
+
 def ktype_table(ktype, N, J, K, L):
     if ktype == "kb:minmax":
         return kb_table(J, L)
@@ -96,6 +124,8 @@ def ktype_table(ktype, N, J, K, L):
         return kb_table(J, L, beatty_alpha(N, J, K))
     if ktype == "diric":
         return diric_table(J, K, L)
+    if ktype == "minmax:kb":
+        return minmax_kb_table(N, J, K, L)
     raise ValueError(ktype)
 
 
@@ -106,6 +136,8 @@ def ktype_scale(ktype, N, J, K, Nmid):
         return kb_scale(N, J, K, Nmid, beatty_alpha(N, J, K))
     if ktype == "diric":
         return np.ones(N)
+    if ktype == "minmax:kb":
+        return minmax_kb_scale(N, J, K, Nmid)
     raise ValueError(ktype)
 
 

@@ -63,10 +63,11 @@ def kaiser_bessel_ft(u, J, alpha, kb_m=0.0, d=1):
     return np.real(y)
 
 
-def nufft_alpha_kb_fit(N: int, J: int, K: int):
-    """LS fit of Fourier-series scaling coefficients; nufft_alpha_kb_fit.m:13-54."""
+def nufft_alpha_kb_fit(N: int, J: int, K: int, Nmid=None):
+    """LS fit of Fourier-series scaling coefficients; nufft_alpha_kb_fit.m:13-54
+    (its 'Nmid' option; default (N - 1) / 2)."""
     beta = 1.0
-    Nmid = (N - 1) / 2
+    Nmid = (N - 1) / 2 if Nmid is None else Nmid
     L = 13 if N > 40 else int(np.ceil(N / 3))
     nlist = np.arange(N, dtype=np.float64) - Nmid
     kb_a, kb_m = kb_params_best(J, K / N)

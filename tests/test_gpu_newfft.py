@@ -48,12 +48,14 @@ def test_reference_selftest_setups(Nd, mode):
     assert _mpd(nr.dtft_adj(Xe, om, Nd, ns), st.adj(Xe)) < BOUND[mode]
 
 
-@pytest.mark.parametrize("ktype", ["kb:beatty", "diric"])
+@pytest.mark.parametrize("ktype", ["kb:beatty", "diric", "minmax:kb"])
 @pytest.mark.parametrize("Nd", [(20,), (6, 5)])
 @pytest.mark.parametrize("mode", ["table0", "table1"])
 def test_other_interpolators(ktype, Nd, mode):
-    """newfft's 'kb:beatty' and 'diric' tables built in the library: the
-    oracle's forward / adjoint and the exact DTFT's bounds."""
+    """newfft's 'kb:beatty', 'diric' and 'minmax:kb' tables built in the
+    library: the oracle's forward / adjoint and the exact DTFT's bounds (for
+    'minmax:kb' only where N >= 16: below that the reference's fit of the
+    scaling factors is coarse, about 0.06 % of the DTFT at N = 8)."""
     Jd = tuple(2 * np.asarray(Nd)) if ktype == "diric" else None
     if Jd is not None and max(Jd) > 16:
         pytest.skip("J > 16")
@@ -66,6 +68,8 @@ def test_other_interpolators(ktype, Nd, mode):
     Xo = nf.newfft_for(x0, so)
     assert rel_l2(X, Xo) <= TOL
     assert rel_l2(st.adj(Xo), nf.newfft_adj(Xo, so)) <= TOL
+    if ktype == "minmax:kb" and min(Nd) < 16:
+        return
     ns = np.zeros(len(Nd))
     Xe = nr.dtft(x0, om, ns)
     assert _mpd(Xe, X) < BOUND[mode]

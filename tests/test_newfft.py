@@ -162,3 +162,37 @@ def test_ktype_errors():
     # kb:beatty's shape is not real for a K/N too close to 1/2
     with pytest.raises(mb.MirtError, match="beatty"):
         mb.newfft_table("kb:beatty", 20, 2, 12, 8)
+
+
+@pytest.mark.parametrize("N,J,K,L", [(20, 6, 40, 512), (21, 6, 42, 2048), (64, 8, 128, 1024),
+                                     (10, 5, 20, 256)])
+def test_minmax_kb_builders(N, J, K, L):
+    """newfft's 'minmax:kb' (phasing 'real', the KB fit at Nmid = floor(N/2)):
+    the library's builders against the oracle (the least-squares fit is a QR
+    solve in the library and an SVD one in numpy: tables agree to 1e-10)."""
+    nmid = np.floor(N / 2)
+    h, ho = mb.newfft_table("minmax:kb", N, J, K, L), nf.ktype_table("minmax:kb", N, J, K, L)
+    assert np.max(np.abs(h - ho)) <= 1e-10
+    s, so = mb.newfft_scale("minmax:kb", N, J, K, nmid), nf.ktype_scale("minmax:kb", N, J, K, nmid)
+    assert np.max(np.abs(s - so) / np.abs(so)) <= 1e-12
+
+
+@pytest.mark.parametrize("Nd", [(21,), (9,), (21, 11)])
+def test_minmax_kb_is_nufft_init_interpolator_for_odd_n(Nd):
+    """For odd N, floor(N/2) = (N-1)/2: newfft's 'minmax:kb' with phasing 'real'
+    uses the same min-max coefficients as nufft_init's 'minmax:kb' (the
+    oracle pinned by the reference's golden vectors), only phased differently,
+    so the two transforms agree to their tables' quantisation (order 0,
+    L = 2^13) -- and both sit at the same distance from the exact DTFT."""
+    import oracle
+    rng = np.random.default_rng(3)
+    D = len(Nd)
+    om = 3 * 2 * np.pi * (rng.random((200, D)) - 0.5)
+    x0 = rng.random(Nd) + 1j * rng.random(Nd)
+    Kd, Jd, Ld = tuple(2 * np.asarray(Nd)), (6,) * D, (2 ** 13,) * D
+    so = nf.newfft_init(om, Nd, Jd=Jd, Kd=Kd, mode="table0", Ld=Ld, ktype="minmax:kb")
+    Xn = nf.newfft_for(x0, so)
+    st = nr.nufft_init_table(om, Nd, Jd, Kd, (0,) * D, Ld)
+    Xi = nr.nufft(x0, st, lambda Xk, s: oracle.interp_for(Xk, s["h"], s["Jd"], s["Ld"], s["tm"],
+                                                          s["Kd"], 0)[:, 0])
+    assert np.linalg.norm(Xn - Xi) <= 2e-4 * np.linalg.norm(Xi)
