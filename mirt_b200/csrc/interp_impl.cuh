@@ -898,9 +898,22 @@ __global__ void __launch_bounds__(256) dense_reduce_kernel(InterpArgs a, Tiling 
   const long long pn = (long long)NP * a.C;
   float2 *out = t.patch + (long long)d * pn;
   for (long long e = threadIdx.x; e < pn; e += blockDim.x) {
-    float2 v = t.patch_part[(long long)q0 * pn + e];
-    for (int q = q0 + 1; q < q1; q++) {
-      const float2 w = t.patch_part[(long long)q * pn + e];
+    const float2 *src = t.patch_part + e;
+    float2 v = src[(long long)q0 * pn];
+    int q = q0 + 1;
+    // eight chunk partials loaded ahead, added in chunk order (the same sums)
+    for (; q + 8 <= q1; q += 8) {
+      float2 w[8];
+#pragma unroll
+      for (int u = 0; u < 8; u++) w[u] = src[(long long)(q + u) * pn];
+#pragma unroll
+      for (int u = 0; u < 8; u++) {
+        v.x += w[u].x;
+        v.y += w[u].y;
+      }
+    }
+    for (; q < q1; q++) {
+      const float2 w = src[(long long)q * pn];
       v.x += w.x;
       v.y += w.y;
     }
