@@ -4,7 +4,7 @@
  *
  * Three layers, all plain C types:
  *
- *  1. Drop-ins for the six mex gateways.  Same arguments, in the same order,
+ *  1. Drop-ins for the eight mex gateways.  Same arguments, in the same order,
  *     as the MATLAB calls
  *        fm = interpD_table_mex(ck, h1..hD, J, L, tm, [order, flips])
  *        ck = interpD_table_adj_mex(fm, h1..hD, J, L, tm, K, [order, flips])
@@ -155,6 +155,43 @@ int mirt_interp3_table_adj_mex(
 	const int32_t *flips, int64_t flips_numel,
 	double *ck_re, double *ck_im);
 
+/* fm = interp4_table_mex(ck, h1, h2, h3, h4, J, L, tm, [order, flips])
+ * replaces nufft/table/interp4_table_mex.c:12-163 (gateway :167-184) and the
+ * kernels of nufft/table/interp4_table1_for.c:30,168,325.
+ * ck dimensions [K1 K2 K3 K4 N].  The reference gateway rejects N > 1
+ * ("N=1 done only", :97-98); this drop-in accepts any N.  Its failure text
+ * is the reference gateway's own, "interp3_table_mex failed" (:182).
+ * K1..K3 must be >= J1..J3 (the GPU kernels wrap a tap once); K4 is free. */
+int mirt_interp4_table_mex(
+	const double *ck_re, const double *ck_im, const int64_t *ck_dims, int32_t ck_ndim,
+	const double *h1_re, const double *h1_im, int64_t h1_rows, int64_t h1_cols,
+	const double *h2_re, const double *h2_im, int64_t h2_rows, int64_t h2_cols,
+	const double *h3_re, const double *h3_im, int64_t h3_rows, int64_t h3_cols,
+	const double *h4_re, const double *h4_im, int64_t h4_rows, int64_t h4_cols,
+	const int32_t *J, int64_t J_numel,
+	const int32_t *L, int64_t L_numel,
+	const double *tm, int64_t tm_rows, int64_t tm_cols,
+	const int32_t *order, int64_t order_numel,
+	const int32_t *flips, int64_t flips_numel,
+	double *fm_re, double *fm_im);
+
+/* ck = interp4_table_adj_mex(fm, h1, h2, h3, h4, J, L, tm, K, [order, flips])
+ * replaces nufft/table/interp4_table_adj_mex.c:12-166 (gateway :170-189) and
+ * nufft/table/interp4_table1_adj.c:31,160,306.  ck [K1*K2*K3*K4, N]. */
+int mirt_interp4_table_adj_mex(
+	const double *fm_re, const double *fm_im, int64_t fm_rows, int64_t fm_cols,
+	const double *h1_re, const double *h1_im, int64_t h1_rows, int64_t h1_cols,
+	const double *h2_re, const double *h2_im, int64_t h2_rows, int64_t h2_cols,
+	const double *h3_re, const double *h3_im, int64_t h3_rows, int64_t h3_cols,
+	const double *h4_re, const double *h4_im, int64_t h4_rows, int64_t h4_cols,
+	const int32_t *J, int64_t J_numel,
+	const int32_t *L, int64_t L_numel,
+	const double *tm, int64_t tm_rows, int64_t tm_cols,
+	const int32_t *K, int64_t K_numel,
+	const int32_t *order, int64_t order_numel,
+	const int32_t *flips, int64_t flips_numel,
+	double *ck_re, double *ck_im);
+
 /* ------------------------------------------------------------------------
  * 2. device-resident interpolation plan (no reference counterpart: the
  *    reference re-reads its tables and tm on every mex call)
@@ -167,12 +204,16 @@ int mirt_interp3_table_adj_mex(
  * ---------------------------------------------------------------------- */
 typedef struct mirt_interp_plan mirt_interp_plan;
 
-/* tm: host FP64 [Mtot, D] column-major (t = omega / (2 pi / K)).
+/* D = 1..4.  tm: host FP64 [Mtot, D] column-major (t = omega / (2 pi / K)).
  * h_re[d] / h_im[d]: host FP64 tables of length J[d]*L[d]+1; h_im == NULL or
  * h_im[0] == NULL selects real tables.  slice_moff: nslice+1 offsets
  * (NULL when nslice == 1).  phase_re/phase_im: optional host FP64 per-sample
  * factor applied after the gather and conjugated before the spread (NULL for
- * none).  stream: cudaStream_t used for the set-up work (NULL = default). */
+ * none).  stream: cudaStream_t used for the set-up work (NULL = default).
+ * J[d] <= K[d] in the first three dimensions.  A 4D plan runs as a 3D plan
+ * over the nslice * K4 hyperplanes of its grids, each sample once per
+ * 4th-dimension tap (Mtot * J4 < 2^31), the tap's coefficient as that
+ * sample's phase; the launch setters and the autotuner act on that 3D plan. */
 int mirt_interp_plan_create(mirt_interp_plan **plan, int32_t D,
 	const int32_t *K, const int32_t *J, const int32_t *L,
 	const double *const *h_re, const double *const *h_im, int32_t order,

@@ -2,7 +2,7 @@
 interpolation (JeffFessler/mirt nufft/table/) behind the reference's own
 interfaces.
 
-* ``mirt_b200.mex``: the six mex gateways (interp{1,2,3}_table[_adj]_mex)
+* ``mirt_b200.mex``: the eight mex gateways (interp{1,2,3,4}_table[_adj]_mex)
 * ``mirt_b200.nufft``: device plans, nufft_init / nufft / nufft_adj, newfft (table mode)
 * ``mirt_b200.dcf``: density compensation (ir_mri_density_comp 'pipe', 'jackson')
 * ``mirt_b200.learned_dcf``: the learned density compensation (features, MLP)
@@ -13,7 +13,8 @@ calling any compute function does, and fails loudly if it has not been built.
 """
 from ._lib import MirtError, load
 from .mex import (MexError, interp1_table_adj_mex, interp1_table_mex, interp2_table_adj_mex,
-                  interp2_table_mex, interp3_table_adj_mex, interp3_table_mex)
+                  interp2_table_mex, interp3_table_adj_mex, interp3_table_mex,
+                  interp4_table_adj_mex, interp4_table_mex)
 from .nufft import (InterpPlan, NewfftPlan, NufftPlan, minmax_kb_scale, minmax_kb_table, newfft,
                     newfft_kb_scale, newfft_kb_table, newfft_scale, newfft_table, nufft,
                     nufft_adj, nufft_init)
@@ -22,8 +23,9 @@ from .learned_dcf import DcfMLP, LearnedDCF, dcf_features
 
 __all__ = [
     "MirtError", "MexError", "load",
-    "interp1_table_mex", "interp2_table_mex", "interp3_table_mex",
+    "interp1_table_mex", "interp2_table_mex", "interp3_table_mex", "interp4_table_mex",
     "interp1_table_adj_mex", "interp2_table_adj_mex", "interp3_table_adj_mex",
+    "interp4_table_adj_mex",
     "InterpPlan", "NufftPlan", "minmax_kb_table", "minmax_kb_scale",
     "nufft_init", "nufft", "nufft_adj",
     "NewfftPlan", "newfft", "newfft_kb_table", "newfft_kb_scale", "newfft_table", "newfft_scale",

@@ -46,11 +46,15 @@ _SIGS = {
                                + _INTS * 2 + [_dp, _dp], C.c_int),
     "mirt_interp3_table_mex": ([_dp, _dp, _i64p, _i32] + _TAB * 3 + _INTS * 2 + [_dp, _i64, _i64]
                                + _INTS * 2 + [_dp, _dp], C.c_int),
+    "mirt_interp4_table_mex": ([_dp, _dp, _i64p, _i32] + _TAB * 4 + _INTS * 2 + [_dp, _i64, _i64]
+                               + _INTS * 2 + [_dp, _dp], C.c_int),
     "mirt_interp1_table_adj_mex": ([_dp, _dp, _i64, _i64] + _TAB + _INTS * 2
                                    + [_dp, _i64, _i64] + _INTS * 3 + [_dp, _dp], C.c_int),
     "mirt_interp2_table_adj_mex": ([_dp, _dp, _i64, _i64] + _TAB * 2 + _INTS * 2
                                    + [_dp, _i64, _i64] + _INTS * 3 + [_dp, _dp], C.c_int),
     "mirt_interp3_table_adj_mex": ([_dp, _dp, _i64, _i64] + _TAB * 3 + _INTS * 2
+                                   + [_dp, _i64, _i64] + _INTS * 3 + [_dp, _dp], C.c_int),
+    "mirt_interp4_table_adj_mex": ([_dp, _dp, _i64, _i64] + _TAB * 4 + _INTS * 2
                                    + [_dp, _i64, _i64] + _INTS * 3 + [_dp, _dp], C.c_int),
     "mirt_interp_plan_create": ([C.POINTER(_vp), _i32, _i32p, _i32p, _i32p,
                                  C.POINTER(_dp), C.POINTER(_dp), _i32, _dp, _i64, _i64p, _i32,

@@ -17,6 +17,7 @@
 #include <algorithm>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <set>
 #include <string>
@@ -39,6 +40,12 @@ double kb_beatty_alpha(int N, int J, int K);
 void diric_table(int J, int K, int L, std::vector<double> &h);
 bool minmax_kb_table_real(int N, int J, int K, int L, std::vector<double> &h);
 std::vector<double> minmax_kb_scale_real(int N, int J, int K, double Nmid);
+int plan4_create(mirt_interp_plan **out, const int *K, const int *J, const int *L,
+                 const double *const *h_re, const double *const *h_im, int order,
+                 const double *tm, long long M4, const long long *moff, int nslice, int C,
+                 const double *ph_re, const double *ph_im, cudaStream_t st);
+int plan4_forward(mirt_interp_plan *P, const float2 *ck, float2 *fm, cudaStream_t st);
+int plan4_adjoint(mirt_interp_plan *P, const float2 *fm, float2 *ck, cudaStream_t st);
 }  // namespace mirt
 
 using namespace mirt;
@@ -1104,6 +1111,8 @@ int validate_geometry(int D, const int *K, const int *J, const int *L, int order
     if (J[d] < 1 || J[d] > MIRT_JMAX) return fail(MIRT_ERR_ARG, "J must be in 1..16");
     if (L[d] < 1) return fail(MIRT_ERR_ARG, "L must be positive");
     if ((long long)J[d] * L[d] + 1 > (1ll << 30)) return fail(MIRT_ERR_ARG, "table too long");
+    // the kernels wrap a tap index k0 + j (k0 in [0, K)) at most once
+    if (J[d] > K[d]) return fail(MIRT_ERR_ARG, "J must not exceed K in any dimension");
   }
   if (order != 0 && order != 1) return fail(MIRT_ERR_ARG, "bad order");
   if (cplx && order) return fail(MIRT_ERR_ARG, "only 0th order implemented for complex");
@@ -1116,6 +1125,9 @@ int validate_geometry(int D, const int *K, const int *J, const int *L, int order
 }
 
 }  // namespace
+
+// The plan whose launches a setter tunes: a 4D plan's 3D plan, else the plan.
+static mirt_interp_plan *launch_plan(mirt_interp_plan *P) { return P->sub4 ? P->sub4 : P; }
 
 extern "C" {
 
@@ -1135,7 +1147,16 @@ int mirt_interp_plan_create(mirt_interp_plan **plan, int32_t D, const int32_t *K
   if (rc) return rc;
   const bool cplx = h_im != nullptr && h_im[0] != nullptr;
   if (nslice < 1) return fail(MIRT_ERR_ARG, "nslice must be >= 1");
-  rc = validate_geometry(D, K, J, L, order, cplx, Mtot, ncol);
+  if (D < 1 || D > 4) return fail(MIRT_ERR_ARG, "D must be 1, 2, 3 or 4");
+  if (D == 4) {
+    // the 4th dimension's taps are wrapped on the host by a general modulo
+    if (K[3] < 1) return fail(MIRT_ERR_ARG, "K must be positive");
+    if (J[3] < 1 || J[3] > MIRT_JMAX) return fail(MIRT_ERR_ARG, "J must be in 1..16");
+    if (L[3] < 1) return fail(MIRT_ERR_ARG, "L must be positive");
+    if ((long long)J[3] * L[3] + 1 > (1ll << 30)) return fail(MIRT_ERR_ARG, "table too long");
+    if (!h_re[3] || (cplx && !h_im[3])) return fail(MIRT_ERR_ARG, "NULL table");
+  }
+  rc = validate_geometry(D == 4 ? 3 : D, K, J, L, order, cplx, Mtot, ncol);
   if (rc) return rc;
   std::vector<long long> moff(nslice + 1);
   if (slice_moff) {
@@ -1150,6 +1171,9 @@ int mirt_interp_plan_create(mirt_interp_plan **plan, int32_t D, const int32_t *K
     moff[1] = Mtot;
   }
   cudaStream_t st = as_stream(stream);
+  if (D == 4)
+    return plan4_create(plan, K, J, L, h_re, h_im, order, tm, Mtot, moff.data(), nslice, ncol,
+                        phase_re, phase_im, st);
   auto *P = new mirt_interp_plan();
   rc = plan_geometry(P, D, K, J, L, h_re, h_im, order, ncol, st);
   if (!rc) {
@@ -1184,6 +1208,9 @@ int mirt_interp_plan_create(mirt_interp_plan **plan, int32_t D, const int32_t *K
 
 int mirt_interp_plan_forward(mirt_interp_plan *P, const void *ck, void *fm, void *stream) {
   if (!P) return fail(MIRT_ERR_ARG, "plan is NULL");
+  if (P->sub4)
+    return plan4_forward(P, static_cast<const float2 *>(ck), static_cast<float2 *>(fm),
+                         as_stream(stream));
   CK(plan_gather(P, static_cast<const float2 *>(ck), static_cast<float2 *>(fm),
                    as_stream(stream)));
   return MIRT_OK;
@@ -1191,6 +1218,9 @@ int mirt_interp_plan_forward(mirt_interp_plan *P, const void *ck, void *fm, void
 
 int mirt_interp_plan_adjoint(mirt_interp_plan *P, const void *fm, void *ck, void *stream) {
   if (!P) return fail(MIRT_ERR_ARG, "plan is NULL");
+  if (P->sub4)
+    return plan4_adjoint(P, static_cast<const float2 *>(fm), static_cast<float2 *>(ck),
+                         as_stream(stream));
   CK(launch_spread(P->a, P->t, P->ls, P->bin_start.as<int>(), static_cast<const float2 *>(fm),
                    static_cast<float2 *>(ck), as_stream(stream)));
   return MIRT_OK;
@@ -1198,6 +1228,7 @@ int mirt_interp_plan_adjoint(mirt_interp_plan *P, const void *fm, void *ck, void
 
 int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
   if (!P) return fail(MIRT_ERR_ARG, "plan is NULL");
+  P = launch_plan(P);
   cudaStream_t st = as_stream(stream);
   const InterpArgs &a = P->a;
   const int D = a.g.D, cw = P->ls.cw;
@@ -1423,6 +1454,7 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
 
 int mirt_interp_plan_config(mirt_interp_plan *P, int32_t *out, int32_t n) {
   if (!P || !out) return fail(MIRT_ERR_ARG, "NULL argument");
+  P = launch_plan(P);
   const int32_t v[23] = {P->t.T[0], P->t.T[1], P->t.T[2], P->ls.threads, P->heavy_first, P->ls.cw,
                          P->lg.threads, P->lg.sb, P->lg.grid, P->t.B[0], P->t.B[1], P->t.B[2],
                          P->split_chunk, P->t.ntask, P->t.padc, P->t.nred, P->ls.atomic,
@@ -1434,6 +1466,7 @@ int mirt_interp_plan_config(mirt_interp_plan *P, int32_t *out, int32_t n) {
 
 int mirt_interp_plan_set_gather(mirt_interp_plan *P, int32_t tma) {
   if (!P) return fail(MIRT_ERR_ARG, "plan is NULL");
+  P = launch_plan(P);
   if (tma < 0 || tma > 2) return fail(MIRT_ERR_ARG, "gather mode must be 0, 1 or 2");
   if (tma && !P->gbk.item)
     return fail(MIRT_ERR_ARG, "TMA gather needs J = 6 and, in 2D, an even C >= 32 and K >= 13, "
@@ -1446,6 +1479,7 @@ int mirt_interp_plan_set_gather(mirt_interp_plan *P, int32_t tma) {
 
 int mirt_interp_plan_set_fault_test(mirt_interp_plan *P, int32_t on) {
   if (!P) return fail(MIRT_ERR_ARG, "plan is NULL");
+  P = launch_plan(P);
   if (on && !P->gtma) return fail(MIRT_ERR_ARG, "the plan's gather does not use TMA stages");
   P->gfault_test = on ? 1 : 0;
   return MIRT_OK;
@@ -1453,6 +1487,7 @@ int mirt_interp_plan_set_fault_test(mirt_interp_plan *P, int32_t on) {
 
 int mirt_interp_plan_fault(mirt_interp_plan *P, int32_t *fault) {
   if (!P || !fault) return fail(MIRT_ERR_ARG, "NULL argument");
+  P = launch_plan(P);
   *fault = 0;
   if (P->gfault.p) {
     CK(cudaDeviceSynchronize());
@@ -1466,6 +1501,7 @@ int mirt_interp_plan_fault(mirt_interp_plan *P, int32_t *fault) {
 
 int mirt_interp_plan_set_sweep(mirt_interp_plan *P, int32_t segments, int32_t rows) {
   if (!P) return fail(MIRT_ERR_ARG, "plan is NULL");
+  P = launch_plan(P);
   if (P->a.g.D == 3) {
     if (segments && !sweep3_ok(P->a, P->t, P->ls.cw))
       return fail(MIRT_ERR_ARG, "3D line sweep needs J = 6, K >= 6 per dimension and coil "
@@ -1508,6 +1544,7 @@ int mirt_interp_plan_set_sweep(mirt_interp_plan *P, int32_t segments, int32_t ro
 
 int mirt_interp_plan_set_dense(mirt_interp_plan *P, int32_t on) {
   if (!P) return fail(MIRT_ERR_ARG, "plan is NULL");
+  P = launch_plan(P);
   if (on && !P->t.dense_of) return fail(MIRT_ERR_ARG, "the plan has no dense bins");
   P->t.dense_on = on ? 1 : 0;
   return MIRT_OK;
@@ -1515,6 +1552,7 @@ int mirt_interp_plan_set_dense(mirt_interp_plan *P, int32_t on) {
 
 int mirt_interp_plan_set_staged(mirt_interp_plan *P, int32_t mode) {
   if (!P) return fail(MIRT_ERR_ARG, "plan is NULL");
+  P = launch_plan(P);
   if (mode < 0 || mode > 2) return fail(MIRT_ERR_ARG, "staged mode must be 0, 1 or 2");
   if (mode && (P->ls.cw != 32 || !P->t.wsw))
     return fail(MIRT_ERR_ARG, "the staged row sweep needs 32-coil lanes (C >= 32)");
@@ -1524,6 +1562,7 @@ int mirt_interp_plan_set_staged(mirt_interp_plan *P, int32_t mode) {
 
 int mirt_interp_plan_set_ownership(mirt_interp_plan *P, int32_t own, void *stream) {
   if (!P) return fail(MIRT_ERR_ARG, "plan is NULL");
+  P = launch_plan(P);
   if (own && !own_ok(P->a, P->t))
     return fail(MIRT_ERR_ARG, "ownership spread needs 2D, J = 6, tiles of >= 5 points and an "
                               "even number of tiles (last one >= 5 points) per dimension");
@@ -1541,6 +1580,7 @@ int mirt_interp_plan_set_ownership(mirt_interp_plan *P, int32_t own, void *strea
 
 int mirt_interp_plan_set_deterministic(mirt_interp_plan *P, int32_t deterministic) {
   if (!P) return fail(MIRT_ERR_ARG, "plan is NULL");
+  P = launch_plan(P);
   P->deterministic = deterministic ? 1 : 0;
   if (deterministic) {
     P->ls.atomic = 0;
@@ -1555,6 +1595,7 @@ int mirt_interp_plan_set_deterministic(mirt_interp_plan *P, int32_t deterministi
 int mirt_interp_plan_set_spread(mirt_interp_plan *P, const int32_t *T, int32_t threads,
                                 int32_t padc, void *stream) {
   if (!P || !T) return fail(MIRT_ERR_ARG, "NULL argument");
+  P = launch_plan(P);
   const int D = P->a.g.D;
   if (threads < 32 || threads > 1024 || threads % 32)
     return fail(MIRT_ERR_ARG, "spread threads must be a multiple of 32 in [32, 1024]");
@@ -1606,8 +1647,8 @@ struct MexCall {
   const char *gateway;  // the gateway's mexFail() text
   int D;
   bool adj;
-  int K[MIRT_DMAX], J[MIRT_DMAX], L[MIRT_DMAX];
-  Tab h[MIRT_DMAX];
+  int K[4], J[4], L[4];  // up to the 4D gateways
+  Tab h[4];
   int order;
   long long M;
   int N;
@@ -1646,6 +1687,9 @@ int mex_check_tables(MexCall &c, const int32_t *flips, int64_t flips_numel) {
       return mex_fail(c, "J outside 1..16 is not supported by the GPU kernels");
     if (c.L[d] < 1) return mex_fail(c, "L must be positive");
     if (c.K[d] < 1) return mex_fail(c, "K must be positive");
+    // the first three dimensions run in the GPU kernels, which wrap a tap once
+    if (d < 3 && c.J[d] > c.K[d])
+      return mex_fail(c, "J larger than K is not supported by the GPU kernels");
   }
   return MIRT_OK;
 }
@@ -1667,20 +1711,30 @@ int mex_run(MexCall &c) {
     if (M >= (1ll << 31)) return mex_fail(c, "too many samples");
   }
   const bool cplx = c.h[0].im != nullptr;
-  const double *hr[MIRT_DMAX] = {nullptr, nullptr, nullptr};
-  const double *hi[MIRT_DMAX] = {nullptr, nullptr, nullptr};
+  const double *hr[4] = {nullptr, nullptr, nullptr, nullptr};
+  const double *hi[4] = {nullptr, nullptr, nullptr, nullptr};
   for (int d = 0; d < c.D; d++) {
     hr[d] = c.h[d].re;
     hi[d] = c.h[d].im;
   }
   mirt_interp_plan P;
-  rc = plan_geometry(&P, c.D, c.K, c.J, c.L, hr, cplx ? hi : nullptr, c.order, N, st);
-  if (rc) return rc;
-  CK(P.tm.alloc(std::max<long long>(M, 1) * c.D * sizeof(double)));
-  if (M) CK(cudaMemcpyAsync(P.tm.p, c.tm, M * c.D * sizeof(double), cudaMemcpyHostToDevice, st));
-  const long long moff[2] = {0, M};
-  rc = plan_finish(&P, M, moff, 1, st);
-  if (rc) return rc;
+  // 4D: the 4D plan over its 3D plan of hyperplanes (interp4.cu)
+  std::unique_ptr<mirt_interp_plan> P4;
+  if (c.D == 4) {
+    mirt_interp_plan *p4 = nullptr;
+    rc = mirt_interp_plan_create(&p4, 4, c.K, c.J, c.L, hr, cplx ? hi : nullptr, c.order, c.tm,
+                                 M, nullptr, 1, N, nullptr, nullptr, st);
+    if (rc) return rc;
+    P4.reset(p4);
+  } else {
+    rc = plan_geometry(&P, c.D, c.K, c.J, c.L, hr, cplx ? hi : nullptr, c.order, N, st);
+    if (rc) return rc;
+    CK(P.tm.alloc(std::max<long long>(M, 1) * c.D * sizeof(double)));
+    if (M) CK(cudaMemcpyAsync(P.tm.p, c.tm, M * c.D * sizeof(double), cudaMemcpyHostToDevice, st));
+    const long long moff[2] = {0, M};
+    rc = plan_finish(&P, M, moff, 1, st);
+    if (rc) return rc;
+  }
 
   const long long nin = c.adj ? M : nk;
   const long long nout = c.adj ? nk : M;
@@ -1696,7 +1750,11 @@ int mex_run(MexCall &c) {
     CK(cudaMemcpyAsync(ii, c.in_im, nin * N * sizeof(double), cudaMemcpyHostToDevice, st));
   }
   CK(launch_split_to_il(ir, ii, nin, N, in_il.as<float2>(), st));
-  if (c.adj)
+  if (P4) {
+    rc = c.adj ? mirt_interp_plan_adjoint(P4.get(), in_il.p, out_il.p, st)
+               : mirt_interp_plan_forward(P4.get(), in_il.p, out_il.p, st);
+    if (rc) return rc;
+  } else if (c.adj)
     CK(launch_spread(P.a, P.t, P.ls, P.bin_start.as<int>(), in_il.as<float2>(),
                      out_il.as<float2>(), st));
   else
@@ -1957,6 +2015,109 @@ int mirt_interp3_table_adj_mex(const double *fm_re, const double *fm_im, int64_t
   if (!h2_re || !tab_len_ok(c.h[1], c.J[1], c.L[1])) return mex_fail(c, "h2 size problem");
   if (!h3_re || !tab_len_ok(c.h[2], c.J[2], c.L[2])) return mex_fail(c, "h3 size problem");
   if (fm_rows != tm_rows || tm_cols != 3) return mex_fail(c, "t_m must be Mx3 matrix");
+  c.M = fm_rows;
+  c.N = (int)fm_cols;
+  c.order = order ? order[0] : 0;
+  int rc = mex_check_tables(c, flips, flips_numel);
+  if (rc) return rc;
+  c.tm = tm;
+  c.in_re = fm_re;
+  c.in_im = fm_im;
+  c.out_re = ck_re;
+  c.out_im = ck_im;
+  return mex_run(c);
+}
+
+/* The 4D gateways: nufft/table/interp4_table_mex.c:12-163 and
+ * interp4_table_adj_mex.c:12-166, their checks in order and their texts
+ * (the forward gateway's own failure text names interp3_table_mex,
+ * interp4_table_mex.c:182). */
+int mirt_interp4_table_mex(const double *ck_re, const double *ck_im, const int64_t *ck_dims,
+                           int32_t ck_ndim, const double *h1_re, const double *h1_im,
+                           int64_t h1_rows, int64_t h1_cols, const double *h2_re,
+                           const double *h2_im, int64_t h2_rows, int64_t h2_cols,
+                           const double *h3_re, const double *h3_im, int64_t h3_rows,
+                           int64_t h3_cols, const double *h4_re, const double *h4_im,
+                           int64_t h4_rows, int64_t h4_cols, const int32_t *J, int64_t J_numel,
+                           const int32_t *L, int64_t L_numel, const double *tm, int64_t tm_rows,
+                           int64_t tm_cols, const int32_t *order, int64_t order_numel,
+                           const int32_t *flips, int64_t flips_numel, double *fm_re,
+                           double *fm_im) {
+  MexCall c{};
+  c.gateway = "interp3_table_mex failed";
+  c.D = 4;
+  c.adj = false;
+  if (!ck_re || !ck_im) return mex_fail(c, "mxIsComplexDouble");
+  if (!tm) return mex_fail(c, "mxIsRealDouble");
+  if (!J || J_numel != 4) return mex_fail(c, "J must be [1,4]");
+  if (!L || L_numel != 4) return mex_fail(c, "L must be [1,4]");
+  if (order && order_numel != 1) return mex_fail(c, "order must be scalar int32 (0 | 1)");
+  if (flips && flips_numel != 4) return mex_fail(c, "flips must be [1 4] int32 (0 | 1)");
+  for (int d = 0; d < 4; d++) {
+    c.J[d] = J[d];
+    c.L[d] = L[d];
+  }
+  c.h[0] = Tab{h1_re, h1_im, h1_rows, h1_cols};
+  c.h[1] = Tab{h2_re, h2_im, h2_rows, h2_cols};
+  c.h[2] = Tab{h3_re, h3_im, h3_rows, h3_cols};
+  c.h[3] = Tab{h4_re, h4_im, h4_rows, h4_cols};
+  if (!h1_re || !tab_len_ok(c.h[0], c.J[0], c.L[0])) return mex_fail(c, "h1 size problem");
+  if (!h2_re || !tab_len_ok(c.h[1], c.J[1], c.L[1])) return mex_fail(c, "h2 size problem");
+  if (!h3_re || !tab_len_ok(c.h[2], c.J[2], c.L[2])) return mex_fail(c, "h3 size problem");
+  if (!h4_re || !tab_len_ok(c.h[3], c.J[3], c.L[3])) return mex_fail(c, "h4 size problem");
+  if (tm_cols != 4) return mex_fail(c, "tm must have 4 columns");
+  for (int d = 0; d < 4; d++) c.K[d] = ck_ndim > d ? (int)ck_dims[d] : 1;
+  // the reference gateway stops at N > 1 ("N=1 done only"); this one runs every column
+  c.N = ck_ndim > 4 ? (int)ck_dims[4] : 1;
+  c.M = tm_rows;
+  c.order = order ? order[0] : 0;
+  int rc = mex_check_tables(c, flips, flips_numel);
+  if (rc) return rc;
+  c.tm = tm;
+  c.in_re = ck_re;
+  c.in_im = ck_im;
+  c.out_re = fm_re;
+  c.out_im = fm_im;
+  return mex_run(c);
+}
+
+int mirt_interp4_table_adj_mex(const double *fm_re, const double *fm_im, int64_t fm_rows,
+                               int64_t fm_cols, const double *h1_re, const double *h1_im,
+                               int64_t h1_rows, int64_t h1_cols, const double *h2_re,
+                               const double *h2_im, int64_t h2_rows, int64_t h2_cols,
+                               const double *h3_re, const double *h3_im, int64_t h3_rows,
+                               int64_t h3_cols, const double *h4_re, const double *h4_im,
+                               int64_t h4_rows, int64_t h4_cols, const int32_t *J,
+                               int64_t J_numel, const int32_t *L, int64_t L_numel,
+                               const double *tm, int64_t tm_rows, int64_t tm_cols,
+                               const int32_t *K, int64_t K_numel, const int32_t *order,
+                               int64_t order_numel, const int32_t *flips, int64_t flips_numel,
+                               double *ck_re, double *ck_im) {
+  MexCall c{};
+  c.gateway = "interp4_table_adj_mex() failed";
+  c.D = 4;
+  c.adj = true;
+  if (!fm_re || !fm_im) return mex_fail(c, "mxIsComplexDouble");
+  if (!tm) return mex_fail(c, "mxIsRealDouble");
+  if (!J || J_numel != 4) return mex_fail(c, "J must be int32 [1,4]");
+  if (!L || L_numel != 4) return mex_fail(c, "L must be int32 [1,4]");
+  if (!K || K_numel != 4) return mex_fail(c, "K must be int32 [1,4]");
+  if (order && order_numel != 1) return mex_fail(c, "order must be scalar int32 (0 | 1)");
+  if (flips && flips_numel != 4) return mex_fail(c, "flips must be [1 4] int32 (0 | 1)");
+  for (int d = 0; d < 4; d++) {
+    c.J[d] = J[d];
+    c.L[d] = L[d];
+    c.K[d] = K[d];
+  }
+  c.h[0] = Tab{h1_re, h1_im, h1_rows, h1_cols};
+  c.h[1] = Tab{h2_re, h2_im, h2_rows, h2_cols};
+  c.h[2] = Tab{h3_re, h3_im, h3_rows, h3_cols};
+  c.h[3] = Tab{h4_re, h4_im, h4_rows, h4_cols};
+  if (!h1_re || !tab_len_ok(c.h[0], c.J[0], c.L[0])) return mex_fail(c, "h1 size problem");
+  if (!h2_re || !tab_len_ok(c.h[1], c.J[1], c.L[1])) return mex_fail(c, "h2 size problem");
+  if (!h3_re || !tab_len_ok(c.h[2], c.J[2], c.L[2])) return mex_fail(c, "h3 size problem");
+  if (!h4_re || !tab_len_ok(c.h[3], c.J[3], c.L[3])) return mex_fail(c, "h4 size problem");
+  if (fm_rows != tm_rows || tm_cols != 4) return mex_fail(c, "t_m must be Mx4 matrix");
   c.M = fm_rows;
   c.N = (int)fm_cols;
   c.order = order ? order[0] : 0;

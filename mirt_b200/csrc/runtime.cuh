@@ -89,6 +89,18 @@ struct mirt_interp_plan {
   int heavy_first = 1;     // spread task order: 1 heaviest first, 0 grid order
   int deterministic = 1;   // 0: the spread may use shared-memory atomics
   std::vector<long long> moff_host;
+  // 4D plan (interp4.cu): a 3D plan over the nslice * K4 hyperplanes whose
+  // samples are the (sample, 4th-dimension tap) pairs; x4_pos[m J4 + j4] is
+  // the 3D position of pair (m, j4), x4_src[e] the 4D sample of 3D sample e,
+  // x4_buf the [Me][C] samples of the 3D plan
+  mirt_interp_plan *sub4 = nullptr;
+  int J4 = 0;
+  long long Me = 0;
+  mirt::DMem x4_pos, x4_src, x4_buf;
+  mirt_interp_plan() = default;
+  mirt_interp_plan(const mirt_interp_plan &) = delete;
+  mirt_interp_plan &operator=(const mirt_interp_plan &) = delete;
+  ~mirt_interp_plan() { delete sub4; }
 };
 
 // NUFFT plan: an interpolation plan plus scaling factors, grids and the FFT.

@@ -1,4 +1,4 @@
-"""Python mirror of the six mex gateways of nufft/table/.
+"""Python mirror of the eight mex gateways of nufft/table/.
 
 Same names, argument order and meaning as the MATLAB calls
 
@@ -123,7 +123,8 @@ def _fwd(D, ck, hs, J, L, tm, order, flips, fail, jmsg, lmsg, fmsg):
     if D == 1:
         _call(lib.mirt_interp1_table_mex, _p(re), _p(im), K1, N, *targs, *common)
     else:
-        fn = lib.mirt_interp2_table_mex if D == 2 else lib.mirt_interp3_table_mex
+        fn = {2: lib.mirt_interp2_table_mex, 3: lib.mirt_interp3_table_mex,
+              4: lib.mirt_interp4_table_mex}[D]
         _call(fn, _p(re), _p(im), _p(dims, _i64p), len(dims), *targs, *common)
     return (fm_re + 1j * fm_im).reshape((M, N_out), order="F")
 
@@ -152,7 +153,7 @@ def _adj(D, fm, hs, J, L, tm, K, order, flips, fail, jmsg, lmsg, kmsg, fmsg):
         targs += [_p(r), _p(i), rows, cols]
     lib = load()
     fn = {1: lib.mirt_interp1_table_adj_mex, 2: lib.mirt_interp2_table_adj_mex,
-          3: lib.mirt_interp3_table_adj_mex}[D]
+          3: lib.mirt_interp3_table_adj_mex, 4: lib.mirt_interp4_table_adj_mex}[D]
     _call(fn, _p(re), _p(im), M, N, *targs, _p(Jd, _i32p), D, _p(Ld, _i32p), D,
           _p(tmf), tm2.shape[0], tm2.shape[1], _p(Kd, _i32p), D,
           _p(od, _i32p), on, _p(fd, _i32p), fn_, _p(ck_re), _p(ck_im))
@@ -178,6 +179,13 @@ def interp3_table_mex(ck, h1, h2, h3, J, L, tm, order=None, flips=None):
                 "J must be [1,3]", "L must be [1,3]", "flips must be [1 3] int32 (0 | 1)")
 
 
+def interp4_table_mex(ck, h1, h2, h3, h4, J, L, tm, order=None, flips=None):
+    """fm = interp4_table_mex(ck, h1, h2, h3, h4, J, L, tm, [order, flips]);
+    nufft/table/interp4_table_mex.c (whose failure text names interp3_table_mex)."""
+    return _fwd(4, ck, [h1, h2, h3, h4], J, L, tm, order, flips, "interp3_table_mex failed",
+                "J must be [1,4]", "L must be [1,4]", "flips must be [1 4] int32 (0 | 1)")
+
+
 def interp1_table_adj_mex(fm, h, J, L, tm, K, order=None, flips=None):
     """ck = interp1_table_adj_mex(fm, h, J, L, tm, K, [order, flips])."""
     return _adj(1, fm, [h], J, L, tm, K, order, flips, "interp1_table_adj_mex() failed",
@@ -197,3 +205,10 @@ def interp3_table_adj_mex(fm, h1, h2, h3, J, L, tm, K, order=None, flips=None):
     return _adj(3, fm, [h1, h2, h3], J, L, tm, K, order, flips, "interp3_table_adj_mex() failed",
                 "J must be int32 [1,3]", "L must be int32 [1,3]", "K must be int32 [1,3]",
                 "flips must be [1 3] int32 (0 | 1)")
+
+
+def interp4_table_adj_mex(fm, h1, h2, h3, h4, J, L, tm, K, order=None, flips=None):
+    """ck = interp4_table_adj_mex(fm, h1, h2, h3, h4, J, L, tm, K, [order, flips])."""
+    return _adj(4, fm, [h1, h2, h3, h4], J, L, tm, K, order, flips,
+                "interp4_table_adj_mex() failed", "J must be int32 [1,4]", "L must be int32 [1,4]",
+                "K must be int32 [1,4]", "flips must be [1 4] int32 (0 | 1)")

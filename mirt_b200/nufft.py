@@ -80,9 +80,10 @@ def _plan_config(lib, handle) -> dict:
 class InterpPlan:
     """Plan of the table gather / spread for fixed tables and trajectory.
 
-    tm: [Mtot, D] float64 (t = omega / (2 pi / K)); tables: list of D arrays
-    (complex128 or float64).  Device tensors: grid [nslice, K_D, ..., K_1, ncol]
-    and samples [Mtot, ncol], complex64, contiguous.
+    tm: [Mtot, D] float64 (t = omega / (2 pi / K)), D = 1..4; tables: list of
+    D arrays (complex128 or float64).  Device tensors: grid [nslice, K_D, ...,
+    K_1, ncol] and samples [Mtot, ncol], complex64, contiguous.  A 4D plan
+    runs on a 3D plan of the grids' hyperplanes; its setters tune that plan.
     """
 
     def __init__(self, K, J, L, tables, tm, ncol, order=0, slice_moff=None, phase=None,
@@ -99,8 +100,8 @@ class InterpPlan:
         mo, self.nslice = _moff(slice_moff, self.Mtot)
         is_cx = any(np.iscomplexobj(h) for h in tables)
         self._keep = []
-        hr = (_dp * 3)()
-        hi = (_dp * 3)() if is_cx else None
+        hr = (_dp * max(3, self.D))()
+        hi = (_dp * max(3, self.D))() if is_cx else None
         for d, h in enumerate(tables):
             r = np.ascontiguousarray(np.real(h), dtype=np.float64)
             self._keep.append(r)

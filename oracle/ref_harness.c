@@ -1,6 +1,6 @@
 /*
  * oracle/ref_harness.c -- drives the reference's own, unmodified table
- * interpolation kernels (nufft/table/interp{1,2,3}_table1_{for,adj}.c, built
+ * interpolation kernels (nufft/table/interp{1,2,3,4}_table1_{for,adj}.c, built
  * from the reference sources into oracle/_ref/libmirt_ref.so) with the mex
  * gateways' column semantics.
  *
@@ -10,7 +10,7 @@
  * The gateways run the kernel once per column (coil) serially:
  *   nufft/table/interp2_table_mex.c:87-95 (complex h), :110-121 (real h)
  *   nufft/table/interp2_table_adj_mex.c:90-98, :113-124
- *   nufft/table/interp1_table_mex.c, interp3_table_mex.c (same pattern)
+ *   nufft/table/interp1_table_mex.c, interp3_table_mex.c, interp4_table_mex.c (same pattern)
  * ref_interp_cols() keeps that per-column call and, when nthreads > 1, hands
  * whole columns to POSIX threads; the kernels themselves are unchanged.
  */
@@ -67,6 +67,27 @@ void interp3_table1_real_per_adj(double *, double *, int, int, int,
 	const double *, const double *, const double *,
 	int, int, int, int, int, int, const double *, int, const double *, const double *);
 
+void interp4_table0_complex_per(const double *, const double *, int, int, int, int,
+	const double *, const double *, const double *, const double *, const double *, const double *,
+	const double *, const double *,
+	int, int, int, int, int, int, int, int, const double *, int, double *, double *);
+void interp4_table0_real_per(const double *, const double *, int, int, int, int,
+	const double *, const double *, const double *, const double *,
+	int, int, int, int, int, int, int, int, const double *, int, double *, double *);
+void interp4_table1_real_per(const double *, const double *, int, int, int, int,
+	const double *, const double *, const double *, const double *,
+	int, int, int, int, int, int, int, int, const double *, int, double *, double *);
+void interp4_table0_complex_per_adj(double *, double *, int, int, int, int,
+	const double *, const double *, const double *, const double *, const double *, const double *,
+	const double *, const double *,
+	int, int, int, int, int, int, int, int, const double *, int, const double *, const double *);
+void interp4_table0_real_per_adj(double *, double *, int, int, int, int,
+	const double *, const double *, const double *, const double *,
+	int, int, int, int, int, int, int, int, const double *, int, const double *, const double *);
+void interp4_table1_real_per_adj(double *, double *, int, int, int, int,
+	const double *, const double *, const double *, const double *,
+	int, int, int, int, int, int, int, int, const double *, int, const double *, const double *);
+
 /* One column through the reference kernel that the gateway would pick.
  * Returns 0, or -1 for an unsupported (D, order, complex) combination. */
 static int one_col(int adj, int D, const int *K, const double *const *hr,
@@ -120,6 +141,29 @@ static int one_col(int adj, int D, const int *K, const double *const *hr,
 				hr[0], hr[1], hr[2], J[0], J[1], J[2], L[0], L[1], L[2], tm, M, r_fm, i_fm);
 			else interp3_table1_real_per_adj(r_ck, i_ck, K[0], K[1], K[2],
 				hr[0], hr[1], hr[2], J[0], J[1], J[2], L[0], L[1], L[2], tm, M, r_fm, i_fm);
+		}
+	} else if (D == 4) {
+		/* nufft/table/interp4_table_mex.c:117-160, interp4_table_adj_mex.c:120-160 */
+		if (!adj) {
+			if (cx) interp4_table0_complex_per(r_ck, i_ck, K[0], K[1], K[2], K[3],
+				hr[0], hi[0], hr[1], hi[1], hr[2], hi[2], hr[3], hi[3],
+				J[0], J[1], J[2], J[3], L[0], L[1], L[2], L[3], tm, M, r_fm, i_fm);
+			else if (order == 0) interp4_table0_real_per(r_ck, i_ck, K[0], K[1], K[2], K[3],
+				hr[0], hr[1], hr[2], hr[3],
+				J[0], J[1], J[2], J[3], L[0], L[1], L[2], L[3], tm, M, r_fm, i_fm);
+			else interp4_table1_real_per(r_ck, i_ck, K[0], K[1], K[2], K[3],
+				hr[0], hr[1], hr[2], hr[3],
+				J[0], J[1], J[2], J[3], L[0], L[1], L[2], L[3], tm, M, r_fm, i_fm);
+		} else {
+			if (cx) interp4_table0_complex_per_adj(r_ck, i_ck, K[0], K[1], K[2], K[3],
+				hr[0], hi[0], hr[1], hi[1], hr[2], hi[2], hr[3], hi[3],
+				J[0], J[1], J[2], J[3], L[0], L[1], L[2], L[3], tm, M, r_fm, i_fm);
+			else if (order == 0) interp4_table0_real_per_adj(r_ck, i_ck, K[0], K[1], K[2], K[3],
+				hr[0], hr[1], hr[2], hr[3],
+				J[0], J[1], J[2], J[3], L[0], L[1], L[2], L[3], tm, M, r_fm, i_fm);
+			else interp4_table1_real_per_adj(r_ck, i_ck, K[0], K[1], K[2], K[3],
+				hr[0], hr[1], hr[2], hr[3],
+				J[0], J[1], J[2], J[3], L[0], L[1], L[2], L[3], tm, M, r_fm, i_fm);
 		}
 	} else {
 		return -1;

@@ -7,8 +7,9 @@ compiled unmodified into oracle/_ref/libmirt_ref.so (oracle/Makefile), run
 with the gateways' column loop.  The fixtures pin the oracle restatement and
 the GPU kernels on machines where the reference sources are absent.
 
-Cases cover D = 1, 2, 3; complex order-0, real order-0 and real order-1
-tables; several columns; unequal J and L per dimension; coordinates that are
+Cases cover D = 1, 2, 3, 4; complex order-0, real order-0 and real order-1
+tables; several columns; unequal J and L per dimension; J = K, and K4 < J4
+(a 4th-dimension tap wrapping twice); coordinates that are
 integers, half-integers, tiny negatives and far outside [0, K) (periodic wrap).
 """
 from __future__ import annotations
@@ -34,6 +35,8 @@ def cases():
         (2, [20, 18], [5, 4], [16, 64], 1),
         (3, [10, 12, 8], [6, 6, 6], [32, 16, 16], 2),
         (3, [9, 8, 11], [4, 5, 3], [8, 16, 32], 1),
+        (4, [7, 6, 8, 5], [4, 3, 5, 4], [16, 8, 32, 16], 2),
+        (4, [6, 6, 6, 3], [6, 6, 6, 4], [8, 8, 8, 8], 1),
     ]
     for D, K, J, L, N in specs:
         for variant in ("cx0", "re0", "re1"):

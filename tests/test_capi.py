@@ -105,6 +105,58 @@ def test_adjoint_and_1d_3d_errors():
                                  np.array([8, 8, 8], np.int32))
 
 
+def test_4d_gateway_errors():
+    """interp4_table_mex.c:43-98 and interp4_table_adj_mex.c:46-104: the checks
+    in order, with the gateways' texts (the forward one fails as
+    interp3_table_mex, as the reference's own gateway does)."""
+    h = np.zeros(25)
+    J4, L4, K4 = (np.array([6, 6, 6, 6], np.int32), np.array([4, 4, 4, 4], np.int32),
+                  np.array([8, 8, 8, 8], np.int32))
+    ck = np.zeros((8, 8, 8, 8), complex)
+    tm = np.zeros((3, 4))
+    fm = np.zeros((3, 1), complex)
+    f = "interp3_table_mex failed: "
+    with pytest.raises(mb.MexError, match=re.escape(f + "mxIsComplexDouble")):
+        mb.interp4_table_mex(ck.real, h, h, h, h, J4, L4, tm)
+    with pytest.raises(mb.MexError, match=re.escape(f + "J must be [1,4]")):
+        mb.interp4_table_mex(ck, h, h, h, h, J4[:3], L4, tm)
+    with pytest.raises(mb.MexError, match=re.escape(f + "L must be [1,4]")):
+        mb.interp4_table_mex(ck, h, h, h, h, J4, L4[:2], tm)
+    with pytest.raises(mb.MexError, match=re.escape(f + "flips must be [1 4] int32 (0 | 1)")):
+        mb.interp4_table_mex(ck, h, h, h, h, J4, L4, tm, flips=np.zeros(3, np.int32))
+    with pytest.raises(mb.MexError, match=re.escape(f + "h4 size problem")):
+        mb.interp4_table_mex(ck, h, h, h, np.zeros(24), J4, L4, tm)
+    with pytest.raises(mb.MexError, match=re.escape(f + "tm must have 4 columns")):
+        mb.interp4_table_mex(ck, h, h, h, h, J4, L4, np.zeros((3, 3)))
+    with pytest.raises(mb.MexError, match=re.escape(f + "flip not compiled")):
+        mb.interp4_table_mex(ck, h, h, h, h, J4, L4, tm, flips=np.array([0, 0, 0, 1], np.int32))
+    with pytest.raises(mb.MexError, match="h must be real or complex double"):
+        mb.interp4_table_mex(ck, h, h, h, np.zeros(25, complex), J4, L4, tm)
+    a = "interp4_table_adj_mex() failed: "
+    with pytest.raises(mb.MexError, match=re.escape(a + "K must be int32 [1,4]")):
+        mb.interp4_table_adj_mex(fm, h, h, h, h, J4, L4, tm, K4[:3])
+    with pytest.raises(mb.MexError, match=re.escape(a + "h2 size problem")):
+        mb.interp4_table_adj_mex(fm, h, np.zeros((25, 2)), h, h, J4, L4, tm, K4)
+    with pytest.raises(mb.MexError, match=re.escape(a + "t_m must be Mx4 matrix")):
+        mb.interp4_table_adj_mex(fm, h, h, h, h, J4, L4, np.zeros((4, 4)), K4)
+    with pytest.raises(mb.MexError, match=re.escape(a + "only 0th order implemented for complex")):
+        hc = np.zeros(25, complex)
+        mb.interp4_table_adj_mex(fm, hc, hc, hc, hc, J4, L4, tm, K4, order=np.ones(1, np.int32))
+
+
+def test_j_larger_than_k_is_refused():
+    """The GPU kernels wrap each tap once, so J > K is refused before any
+    device work (the 4th dimension of the 4D gateways wraps on the host)."""
+    h = np.zeros(25)
+    with pytest.raises(mb.MexError, match="J larger than K is not supported"):
+        mb.interp2_table_mex(np.zeros((8, 4), complex), h, h, np.array([6, 6], np.int32),
+                             np.array([4, 4], np.int32), np.zeros((3, 2)))
+    with pytest.raises(mb.MexError, match="J larger than K is not supported"):
+        mb.interp4_table_adj_mex(np.zeros((3, 1), complex), h, h, h, h,
+                                 np.array([6, 6, 6, 6], np.int32), np.array([4, 4, 4, 4], np.int32),
+                                 np.zeros((3, 4)), np.array([8, 5, 8, 2], np.int32))
+
+
 def test_valid_call_without_gpu_fails_loudly():
     import torch
     if torch.cuda.is_available():

@@ -32,7 +32,9 @@ def _fwd(D, ck, h, J, L, tm, K, order):
         return mb.interp1_table_mex(ck, h[0], _i32(J), _i32(L), tm, o)
     if D == 2:
         return mb.interp2_table_mex(ckr, h[0], h[1], _i32(J), _i32(L), tm, o)
-    return mb.interp3_table_mex(ckr, h[0], h[1], h[2], _i32(J), _i32(L), tm, o)
+    if D == 3:
+        return mb.interp3_table_mex(ckr, h[0], h[1], h[2], _i32(J), _i32(L), tm, o)
+    return mb.interp4_table_mex(ckr, h[0], h[1], h[2], h[3], _i32(J), _i32(L), tm, o)
 
 
 def _adj(D, fm, h, J, L, tm, K, order):
@@ -41,10 +43,12 @@ def _adj(D, fm, h, J, L, tm, K, order):
         return mb.interp1_table_adj_mex(fm, h[0], _i32(J), _i32(L), tm, _i32(K), o)
     if D == 2:
         return mb.interp2_table_adj_mex(fm, h[0], h[1], _i32(J), _i32(L), tm, _i32(K), o)
-    return mb.interp3_table_adj_mex(fm, h[0], h[1], h[2], _i32(J), _i32(L), tm, _i32(K), o)
+    if D == 3:
+        return mb.interp3_table_adj_mex(fm, h[0], h[1], h[2], _i32(J), _i32(L), tm, _i32(K), o)
+    return mb.interp4_table_adj_mex(fm, h[0], h[1], h[2], h[3], _i32(J), _i32(L), tm, _i32(K), o)
 
 
-@pytest.mark.parametrize("i", range(18))
+@pytest.mark.parametrize("i", range(24))
 def test_mex_matches_golden(i):
     c = load_golden()[i]
     D = c["D"]
@@ -103,6 +107,77 @@ def test_random_geometry(D, variant):
     ref_a = oracle.interp_adj(fm, h, J, L, tm, K, order, impl=ref_impl())
     assert rel_l2(_fwd(D, ck, h, J, L, tm, K, order), ref_f) <= FWD_TOL
     assert rel_l2(_adj(D, fm, h, J, L, tm, K, order), ref_a) <= ADJ_TOL
+
+
+@pytest.mark.parametrize("variant", ["cx0", "re0", "re1"])
+def test_4d_random_geometry(variant):
+    """4D gateways (interp4_table1_for.c / interp4_table1_adj.c) on the 3D
+    kernels: generic J, K4 < J4 (a 4th-dimension tap wraps twice),
+    coordinates far outside [0, K), several columns."""
+    rng = np.random.default_rng(404)
+    K = [17, 13, 11, 5]
+    J = [5, 6, 4, 6]
+    L = [64, 128, 32, 64]
+    cx = variant == "cx0"
+    order = 1 if variant == "re1" else 0
+    h = [np.exp(-np.linspace(-j / 2, j / 2, j * l + 1) ** 2)
+         * (np.exp(0.4j * np.linspace(-j / 2, j / 2, j * l + 1)) if cx else 1)
+         for j, l in zip(J, L)]
+    M, N = 2000, 3
+    tm = rng.uniform(-3 * max(K), 3 * max(K), (M, 4))
+    tm[:40] = np.round(tm[:40] * 2) / 2
+    nk = int(np.prod(K))
+    ck = rng.standard_normal((nk, N)) + 1j * rng.standard_normal((nk, N))
+    fm = rng.standard_normal((M, N)) + 1j * rng.standard_normal((M, N))
+    ref_f = oracle.interp_for(ck, h, J, L, tm, K, order, impl=ref_impl())
+    ref_a = oracle.interp_adj(fm, h, J, L, tm, K, order, impl=ref_impl())
+    assert rel_l2(_fwd(4, ck, h, J, L, tm, K, order), ref_f) <= FWD_TOL
+    assert rel_l2(_adj(4, fm, h, J, L, tm, K, order), ref_a) <= ADJ_TOL
+
+
+def test_4d_plan_multislice_phase_autotuned():
+    """4D device plan: uneven slices (one empty), 8 coils, a per-sample phase,
+    J = 6 (the 3D plan underneath may pick its line sweep and TMA gather),
+    against the oracle per slice before and after autotuning."""
+    import torch
+    rng = np.random.default_rng(44)
+    K, J, L = [24, 20, 18, 9], [6, 6, 6, 6], [256, 256, 256, 256]
+    h = [np.exp(-np.linspace(-3, 3, 6 * 256 + 1) ** 2 / 2)
+         * np.exp(0.3j * d * np.linspace(-3, 3, 6 * 256 + 1)) for d in range(4)]
+    counts = [1500, 0, 900]
+    moff = np.concatenate([[0], np.cumsum(counts)])
+    tm = np.concatenate([rng.uniform(-30, 30, (c, 4)) for c in counts])
+    ph = np.exp(1j * rng.uniform(0, 2 * np.pi, len(tm)))
+    C, S = 8, len(counts)
+    plan = mb.InterpPlan(K, J, L, h, tm, C, slice_moff=moff, phase=ph)
+    assert plan.grid_shape == (S, 9, 18, 20, 24, C)
+    ck = rng.standard_normal(plan.grid_shape) + 1j * rng.standard_normal(plan.grid_shape)
+    fm = rng.standard_normal((len(tm), C)) + 1j * rng.standard_normal((len(tm), C))
+    ck_d = torch.from_numpy(ck.astype(np.complex64)).cuda()
+    fm_d = torch.from_numpy(fm.astype(np.complex64)).cuda()
+
+    def check():
+        out_f = plan.forward(ck_d).cpu().numpy()
+        out_a = plan.adjoint(fm_d).cpu().numpy()
+        for s in range(S):
+            sl = slice(moff[s], moff[s + 1])
+            got_a = np.transpose(out_a[s], (3, 2, 1, 0, 4)).reshape(-1, C, order="F")
+            if not counts[s]:
+                assert not got_a.any()
+                continue
+            cks = np.transpose(ck[s], (3, 2, 1, 0, 4)).reshape(-1, C, order="F")
+            ref_f = oracle.interp_for(cks, h, J, L, tm[sl], K, 0, impl=ref_impl())
+            assert rel_l2(out_f[sl], ph[sl, None] * ref_f) <= FWD_TOL
+            ref_a = oracle.interp_adj(np.conj(ph[sl, None]) * fm[sl], h, J, L, tm[sl], K, 0,
+                                      impl=ref_impl())
+            assert rel_l2(got_a, ref_a) <= ADJ_TOL
+        return out_a
+
+    before = check()
+    plan.autotune()
+    after = check()
+    assert rel_l2(after, before) <= ADJ_TOL
+    plan.close()
 
 
 def test_3d_minmax_multicolumn():

@@ -20,7 +20,7 @@ from oracle import nufft_ref as nr
 from conftest import load_golden, rel_l2
 
 
-@pytest.mark.parametrize("i", range(18))
+@pytest.mark.parametrize("i", range(24))
 def test_port_matches_golden(i):
     c = load_golden()[i]
     h = c["h"]
@@ -31,13 +31,13 @@ def test_port_matches_golden(i):
 
 
 @pytest.mark.skipif(not oracle.ref_available(), reason="reference kernels not built here")
-@pytest.mark.parametrize("D", [1, 2, 3])
+@pytest.mark.parametrize("D", [1, 2, 3, 4])
 @pytest.mark.parametrize("variant", ["cx0", "re0", "re1"])
 def test_port_matches_reference_kernels(D, variant):
     rng = np.random.default_rng(7 + D)
-    K = [13, 16, 9][:D]
-    J = [6, 5, 4][:D]
-    L = [128, 32, 16][:D]
+    K = [13, 16, 9, 5][:D]
+    J = [6, 5, 4, 3][:D]
+    L = [128, 32, 16, 8][:D]
     cx = variant == "cx0"
     order = 1 if variant == "re1" else 0
     h = [rng.standard_normal(j * l + 1) + (1j * rng.standard_normal(j * l + 1) if cx else 0)
