@@ -443,13 +443,28 @@ int mirt_newfft_kb_scale(int32_t N, int32_t J, int32_t K, double nmid, double *s
  *                         scaling (nufft/newfft.m:315-320, 384-395), the fit at
  *                         Nmid = floor(N/2), no phase; scale the real part of
  *                         nufft_scale1 at nmid (N <= K)
+ *   MIRT_KTYPE_MINMAX_UNIF  'minmax:unif': the min-max interpolator with
+ *                         uniform scaling, alpha = 1, beta = 0
+ *                         (nufft/newfft.m:337-341); scale 1 (N <= K)
+ *   MIRT_KTYPE_MINMAX_TUNED 'minmax:tuned': the min-max interpolator with the
+ *                         tuned coefficients of nufft_best_alpha(J, 0, K/N)
+ *                         (nufft/newfft.m:322-327, nufft/nufft_best_alpha.m):
+ *                         K = 2N needs J in 2..10; other K/N take alpha = 1,
+ *                         beta = 0.5 as the reference does (N <= K)
+ *   MIRT_KTYPE_LINEAR     'linear': the triangle 1 - |t|/(J/2) on |t| < J/2
+ *                         (nufft/newfft.m:268-273); scale newfft_scale_tri
+ *                         (nufft/newfft.m:535-550) at this dimension's nmid
  * table: J*L+1 values at t = -J/2 + i/L; scale: N values (st.sn is their outer
- * product over dimensions).  MIRT_ERR_ARG for unknown ktypes and for
- * 'kb:beatty' where its shape is not real. */
+ * product over dimensions).  MIRT_ERR_ARG for unknown ktypes, for
+ * 'kb:beatty' where its shape is not real and for 'minmax:tuned' where the
+ * reference has no coefficients. */
 #define MIRT_KTYPE_KB_MINMAX 0
 #define MIRT_KTYPE_KB_BEATTY 1
 #define MIRT_KTYPE_DIRIC 2
 #define MIRT_KTYPE_MINMAX_KB 3
+#define MIRT_KTYPE_MINMAX_UNIF 4
+#define MIRT_KTYPE_MINMAX_TUNED 5
+#define MIRT_KTYPE_LINEAR 6
 int mirt_newfft_ktype_table(int32_t ktype, int32_t N, int32_t J, int32_t K, int32_t L, double *h);
 int mirt_newfft_ktype_scale(int32_t ktype, int32_t N, int32_t J, int32_t K, double nmid,
 	double *sn);

@@ -40,6 +40,13 @@ double kb_beatty_alpha(int N, int J, int K);
 void diric_table(int J, int K, int L, std::vector<double> &h);
 bool minmax_kb_table_real(int N, int J, int K, int L, std::vector<double> &h);
 std::vector<double> minmax_kb_scale_real(int N, int J, int K, double Nmid);
+bool minmax_table_real_ab(int N, int J, int K, int L, const std::vector<double> &alpha, double beta,
+                          std::vector<double> &h);
+std::vector<double> minmax_scale_real_ab(int N, int K, const std::vector<double> &alpha,
+                                         double beta, double Nmid);
+bool best_alpha(int J, int N, int K, std::vector<double> &alpha, double &beta);
+void linear_table(int J, int L, std::vector<double> &h);
+std::vector<double> linear_scale(int N, int J, int K, double Nmid);
 int plan4_create(mirt_interp_plan **out, const int *K, const int *J, const int *L,
                  const double *const *h_re, const double *const *h_im, int order,
                  const double *tm, long long M4, const long long *moff, int nslice, int C,
@@ -2507,6 +2514,18 @@ int mirt_newfft_ktype_table(int32_t ktype, int32_t N, int32_t J, int32_t K, int3
       if (!minmax_kb_table_real(N, J, K, L, t))
         return fail(MIRT_ERR_ARG, "singular min-max matrix for this N, J, K");
       break;
+    case MIRT_KTYPE_MINMAX_UNIF:
+    case MIRT_KTYPE_MINMAX_TUNED: {
+      if (N > K) return fail(MIRT_ERR_ARG, "minmax:* needs N <= K");
+      std::vector<double> alpha{1.0};
+      double beta = 0.0;
+      if (ktype == MIRT_KTYPE_MINMAX_TUNED && !best_alpha(J, N, K, alpha, beta))
+        return fail(MIRT_ERR_ARG, "minmax:tuned: unknown J,K/N");
+      if (!minmax_table_real_ab(N, J, K, L, alpha, beta, t))
+        return fail(MIRT_ERR_ARG, "singular min-max matrix for this N, J, K");
+      break;
+    }
+    case MIRT_KTYPE_LINEAR: linear_table(J, L, t); break;
     default: return fail(MIRT_ERR_ARG, "unknown ktype");
   }
   std::copy(t.begin(), t.end(), h);
@@ -2529,6 +2548,16 @@ int mirt_newfft_ktype_scale(int32_t ktype, int32_t N, int32_t J, int32_t K, doub
     }
     case MIRT_KTYPE_DIRIC: s.assign(N, 1.0); break;
     case MIRT_KTYPE_MINMAX_KB: s = minmax_kb_scale_real(N, J, K, nmid); break;
+    case MIRT_KTYPE_MINMAX_UNIF: s = minmax_scale_real_ab(N, K, {1.0}, 0.0, nmid); break;
+    case MIRT_KTYPE_MINMAX_TUNED: {
+      std::vector<double> alpha;
+      double beta;
+      if (!best_alpha(J, N, K, alpha, beta))
+        return fail(MIRT_ERR_ARG, "minmax:tuned: unknown J,K/N");
+      s = minmax_scale_real_ab(N, K, alpha, beta, nmid);
+      break;
+    }
+    case MIRT_KTYPE_LINEAR: s = linear_scale(N, J, K, nmid); break;
     default: return fail(MIRT_ERR_ARG, "unknown ktype");
   }
   std::copy(s.begin(), s.end(), sn);

@@ -243,18 +243,16 @@ bool minmax_kb_table(int N, int J, int K, int L, std::vector<cd> &h) {
   return true;
 }
 
-// newfft's ktype 'minmax:kb' with phasing 'real' (nufft/newfft.m:315-320,
-// 384-395): alphas and beta of nufft_alpha_kb_fit with Nmid = floor(N / 2),
-// T = inv(C'SS'C) and r of nufft/private/nufft_T.m / nufft_r.m (sinc diric,
-// tol 0: the plain inverse), coefficients c = T r without phase (phasing
-// 'real'), read by the 'fast' construction of
+// The real min-max table of newfft's 'minmax:*' interpolators with phasing
+// 'real' (nufft/newfft.m:384-395) for scaling-factor Fourier coefficients
+// alpha[0..La] and beta: T = inv(C'SS'C) and r of nufft/private/nufft_T.m /
+// nufft_r.m (sinc diric, tol 0: the plain inverse), coefficients c = T r
+// without phase, read by the 'fast' construction of
 // nufft/private/newfft_table_init.m:160-169 (columns J .. 1 of the sparse
 // interpolator at t1 = J/2 - 1 + i/L, the last entry repeating the first).
 // The coefficients are real.
-bool minmax_kb_table_real(int N, int J, int K, int L, std::vector<double> &h) {
-  std::vector<double> alpha;
-  double beta;
-  alpha_kb_fit_nmid(N, J, K, std::floor(N / 2.0), alpha, beta);
+bool minmax_table_real_ab(int N, int J, int K, int L, const std::vector<double> &alpha, double beta,
+                          std::vector<double> &h) {
   const int La = (int)alpha.size() - 1;
   std::vector<double> T(J * J, 0.0);
   for (int a = 0; a < J; a++)
@@ -297,20 +295,105 @@ bool minmax_kb_table_real(int N, int J, int K, int L, std::vector<double> &h) {
   return true;
 }
 
-// scaling factors of newfft's 'minmax:kb' (phasing 'real'): the real part of
-// nufft_scale1(N, K, alpha, beta, Nmid) with the alphas fitted at Nmid
-// (nufft/newfft.m:360-364: reale)
-std::vector<double> minmax_kb_scale_real(int N, int J, int K, double Nmid) {
-  std::vector<double> alpha;
-  double beta;
-  alpha_kb_fit_nmid(N, J, K, Nmid, alpha, beta);
+// the real part of nufft_scale1(N, K, alpha, beta, Nmid) (nufft/nufft_scale.m:54-75;
+// nufft/newfft.m:360-364 keeps the real part), alpha real
+std::vector<double> minmax_scale_real_ab(int N, int K, const std::vector<double> &alpha,
+                                         double beta, double Nmid) {
   const int L = (int)alpha.size() - 1;
   std::vector<double> sn(N);
   for (int n = 0; n < N; n++) {
+    if (L == 0) {
+      sn[n] = alpha[0];
+      continue;
+    }
     const double g = (2 * M_PI / K) * (n - Nmid) * beta;
     cd s(0, 0);
     for (int l1 = -L; l1 <= L; l1++) s += alpha[std::abs(l1)] * std::exp(cd(0, g * l1));
     sn[n] = s.real();
+  }
+  return sn;
+}
+
+// newfft's ktype 'minmax:kb' (nufft/newfft.m:315-320): the alphas and beta of
+// nufft_alpha_kb_fit fitted at Nmid = floor(N/2) for the table, at nmid for
+// the scaling factors
+bool minmax_kb_table_real(int N, int J, int K, int L, std::vector<double> &h) {
+  std::vector<double> alpha;
+  double beta;
+  alpha_kb_fit_nmid(N, J, K, std::floor(N / 2.0), alpha, beta);
+  return minmax_table_real_ab(N, J, K, L, alpha, beta, h);
+}
+
+std::vector<double> minmax_kb_scale_real(int N, int J, int K, double Nmid) {
+  std::vector<double> alpha;
+  double beta;
+  alpha_kb_fit_nmid(N, J, K, Nmid, alpha, beta);
+  return minmax_scale_real_ab(N, K, alpha, beta, Nmid);
+}
+
+// nufft_best_alpha(J, 0, K/N) (nufft/nufft_best_alpha.m), ktype 'minmax:tuned'
+// (nufft/newfft.m:322-327): for K/N = 2 the numerically tuned Fourier
+// coefficients of the scaling factors -- three-term sets for J = 4 and 6,
+// two-term sets for J = 2, 3, 5, 7 .. 10 (the reference's tables, data the
+// interpolator's values depend on); for any other K/N alpha = 1, beta = 0.5.
+// False for K/N = 2 with a J outside 2..10 (the reference's 'unknown J,K/N').
+bool best_alpha(int J, int N, int K, std::vector<double> &alpha, double &beta) {
+  if (K != 2 * N) {
+    alpha.assign(1, 1.0);
+    beta = 0.5;
+    return true;
+  }
+  if (J == 4) {
+    alpha = {1, -0.5319, 0.1522, -0.0199};
+    beta = 0.6339;
+    return true;
+  }
+  if (J == 6) {
+    alpha = {1, -0.6903, 0.2138, -0.0191};
+    beta = 0.2254;
+    return true;
+  }
+  static const double two[9][4] = {
+      {1, -0.200, -0.04, 0.34},  {1, -0.485, 0.090, 0.48}, {1, -0.470, 0.085, 0.56},
+      {1, -0.4825, 0.12, 0.495}, {1, -0.57, 0.14, 0.43},   {1, -0.465, 0.07, 0.65},
+      {1, -0.540, 0.16, 0.47},   {1, -0.625, 0.14, 0.325}, {1, -0.57, 0.185, 0.43}};
+  if (J < 2 || J > 10) return false;
+  const double *row = two[J - 2];
+  alpha = {row[0], row[1], row[2]};
+  beta = row[3];
+  return true;
+}
+
+// ktype 'linear' (nufft/newfft.m:268-273): the triangle (1 - |t| / (J/2)) on
+// |t| < J/2, sampled by the 'fast' construction at t = -J/2 + i/L, the last
+// entry repeating the first (0 at |t| = J/2)
+void linear_table(int J, int L, std::vector<double> &h) {
+  h.assign((size_t)J * L + 1, 0.0);
+  for (long long i = 0; i < (long long)J * L; i++) {
+    const double t = -J / 2.0 + (double)i / L;
+    h[i] = std::fabs(t) < J / 2.0 ? 1 - std::fabs(t / (J / 2.0)) : 0.0;
+  }
+  h[(size_t)J * L] = h[0];
+}
+
+// its scaling factors, newfft_scale_tri (nufft/newfft.m:535-550): with
+// f(x) = J sinc^2(J x / K), sn[n] = f(n - Nmid) / sum_{l = -3..3} f(n - Nmid - l K)^2
+// (per dimension: the reference passes the whole Nmid vector, which only
+// works in 1D)
+std::vector<double> linear_scale(int N, int J, int K, double Nmid) {
+  auto f = [&](double x) {
+    const double s = nufft_sinc(J * x / K);
+    return J * s * s;
+  };
+  std::vector<double> sn(N);
+  for (int n = 0; n < N; n++) {
+    const double nc = n - Nmid;
+    double tmp = 0;
+    for (int l = -3; l <= 3; l++) {
+      const double v = f(nc - (double)l * K);
+      tmp += v * v;
+    }
+    sn[n] = f(nc) / tmp;
   }
   return sn;
 }

@@ -382,12 +382,14 @@ def newfft_kb_scale(N: int, J: int, K: int, nmid: float) -> np.ndarray:
     return s
 
 
-_KTYPES = {"kb:minmax": 0, "kb:beatty": 1, "diric": 2, "minmax:kb": 3}
+_KTYPES = {"kb:minmax": 0, "kb:beatty": 1, "diric": 2, "minmax:kb": 3, "minmax:unif": 4,
+           "minmax:tuned": 5, "linear": 6}
 
 
 def newfft_table(ktype: str, N: int, J: int, K: int, L: int) -> np.ndarray:
     """Real table of newfft's interpolator `ktype` ('kb:minmax', 'kb:beatty',
-    'diric', 'minmax:kb'; phasing 'real'), [J*L+1] (see mirt_newfft_ktype_table)."""
+    'diric', 'minmax:kb', 'minmax:unif', 'minmax:tuned', 'linear'; phasing
+    'real'), [J*L+1] (see mirt_newfft_ktype_table)."""
     if ktype not in _KTYPES:
         raise ValueError(f"ktype must be one of {sorted(_KTYPES)}")
     h = np.empty(int(J) * int(L) + 1)
@@ -413,7 +415,8 @@ class NewfftPlan(NufftPlan):
 
     phasing 'real' (the reference's default) with ``tables=None`` builds the
     real tables and scaling factors of ``ktype`` in the library ('kb:minmax',
-    the reference's default, 'kb:beatty', 'diric' or 'minmax:kb'); any other interpolator
+    the reference's default, 'kb:beatty', 'diric', 'minmax:kb', 'minmax:unif',
+    'minmax:tuned' or 'linear'); any other interpolator
     is given as ``tables`` (one 1D table per dimension, real or complex, J*L+1
     values) and ``sn`` ([(Nd)], first index fastest).
     phasing 'real' applies phase_before / phase_after with Nmid = floor(N/2);

@@ -30,6 +30,13 @@ What is restated, with the reference lines followed:
   nufft/private/newfft_table_init.m:160-169 through nufft/private/nufft_coef.m
   (the kernel at t = -J/2 + i/L, i < J L; the last entry repeats the first);
   its scaling factors are 1 (nufft/newfft.m:354-355)
+* ``minmax_table``       ktypes 'minmax:unif' (alpha = 1, beta = 0,
+  nufft/newfft.m:337-341) and 'minmax:tuned' (``best_alpha``: nufft_best_alpha(J,
+  0, K/N), nufft/newfft.m:322-327), the 'minmax:kb' construction with those
+  coefficients; scale the real part of nufft_scale1
+* ``linear_table``       ktype 'linear' (nufft/newfft.m:268-273), the triangle
+  read by the 'fast' construction; ``linear_scale`` newfft_scale_tri
+  (nufft/newfft.m:535-550), evaluated per dimension
 * ``phase_before``       nufft/newfft.m:511-520
 * ``phase_after``        nufft/newfft.m:522-527
 * ``newfft_for/adj``     nufft/private/newfft_approx_for.m:15-63,
@@ -93,11 +100,36 @@ def kb_scale(N: int, J: int, K: int, Nmid: float, alpha=None) -> np.ndarray:
     return 1.0 / nr.kaiser_bessel_ft(nc / K, J, kb_alpha(J) if alpha is None else alpha, 0.0, 1)
 
 
-def minmax_kb_table(N, J, K, L):
-    """Real [J*L+1] table of ktype 'minmax:kb' with phasing 'real': the min-max
-    coefficients c = T r (alphas fitted at Nmid = floor(N/2), no phase) read
+# nufft/nufft_best_alpha.m:13-33: tuned Fourier coefficients of the scaling
+# factors for K/N = 2, J -> (alpha_0 .. alpha_L, beta); the L = 3 sets are the
+# reference's choice for J = 4 and 6 (its "L = 0: best available", :37-43)
+_BEST_ALPHA_L3 = {4: ([1, -0.5319, 0.1522, -0.0199], 0.6339),
+                  6: ([1, -0.6903, 0.2138, -0.0191], 0.2254)}
+_BEST_ALPHA_L2 = {2: ([1, -0.200, -0.04], 0.34), 3: ([1, -0.485, 0.090], 0.48),
+                  4: ([1, -0.470, 0.085], 0.56), 5: ([1, -0.4825, 0.12], 0.495),
+                  6: ([1, -0.57, 0.14], 0.43), 7: ([1, -0.465, 0.07], 0.65),
+                  8: ([1, -0.540, 0.16], 0.47), 9: ([1, -0.625, 0.14], 0.325),
+                  10: ([1, -0.57, 0.185], 0.43)}
+
+
+def best_alpha(J, N, K):
+    """nufft_best_alpha(J, 0, K/N) (nufft/nufft_best_alpha.m:35-77): for K/N = 2
+    the L = 3 set where there is one, else the L = 2 set (ValueError for a J
+    without one: newfft's 'unknown J,K/N'); for any other K/N alpha = 1,
+    beta = 0.5."""
+    if K / N != 2:
+        return np.array([1.0]), 0.5
+    table = _BEST_ALPHA_L3 if J in _BEST_ALPHA_L3 else _BEST_ALPHA_L2
+    if J not in table:
+        raise ValueError("unknown J,K/N")
+    a, b = table[J]
+    return np.asarray(a, dtype=np.float64), b
+
+
+def minmax_table(N, J, K, L, alpha, beta):
+    """Real [J*L+1] table of a 'minmax:*' ktype with phasing 'real': the min-max
+    coefficients c = T r (no phase) for scaling coefficients alpha, beta read
     by the 'fast' construction, the last entry repeating the first."""
-    alpha, beta = nr.nufft_alpha_kb_fit(N, J, K, Nmid=np.floor(N / 2))
     T = nr.nufft_T(N, J, K, alpha, beta)
     t1 = (J / 2 - 1) + np.arange(L, dtype=np.float64) / L
     om1 = t1 * 2 * np.pi / K
@@ -112,9 +144,31 @@ def minmax_kb_table(N, J, K, L):
     return np.append(h, h[0])
 
 
+def minmax_kb_table(N, J, K, L):
+    """ktype 'minmax:kb': the alphas fitted at Nmid = floor(N/2)."""
+    alpha, beta = nr.nufft_alpha_kb_fit(N, J, K, Nmid=np.floor(N / 2))
+    return minmax_table(N, J, K, L, alpha, beta)
+
+
 def minmax_kb_scale(N, J, K, Nmid):
     alpha, beta = nr.nufft_alpha_kb_fit(N, J, K, Nmid=Nmid)
     return np.real(nr.nufft_scale1(N, K, alpha, beta, Nmid))
+
+
+def linear_table(J, L):
+    """ktype 'linear' (nufft/newfft.m:268-273): (1 - |t/(J/2)|) (|t| < J/2) at
+    t = -J/2 + i/L, i < J L, the last entry repeating the first."""
+    t = -J / 2 + np.arange(J * L) / L
+    h = (1 - np.abs(t / (J / 2))) * (np.abs(t) < J / 2)
+    return np.append(h, h[0])
+
+
+def linear_scale(N, J, K, Nmid):
+    """newfft_scale_tri (nufft/newfft.m:535-550) at one dimension's Nmid."""
+    nc = np.arange(N) - Nmid
+    fun = lambda x: J * nr.nufft_sinc(J * x / K) ** 2
+    tmp = sum(np.abs(fun(nc - ll * K)) ** 2 for ll in range(-3, 4))
+    return fun(nc) / tmp
 
 
 def ktype_table(ktype, N, J, K, L):
@@ -126,6 +180,12 @@ def ktype_table(ktype, N, J, K, L):
         return diric_table(J, K, L)
     if ktype == "minmax:kb":
         return minmax_kb_table(N, J, K, L)
+    if ktype == "minmax:unif":
+        return minmax_table(N, J, K, L, np.array([1.0]), 0.0)
+    if ktype == "minmax:tuned":
+        return minmax_table(N, J, K, L, *best_alpha(J, N, K))
+    if ktype == "linear":
+        return linear_table(J, L)
     raise ValueError(ktype)
 
 
@@ -138,6 +198,12 @@ def ktype_scale(ktype, N, J, K, Nmid):
         return np.ones(N)
     if ktype == "minmax:kb":
         return minmax_kb_scale(N, J, K, Nmid)
+    if ktype == "minmax:unif":
+        return np.real(nr.nufft_scale1(N, K, np.array([1.0]), 0.0, Nmid))
+    if ktype == "minmax:tuned":
+        return np.real(nr.nufft_scale1(N, K, *best_alpha(J, N, K), Nmid))
+    if ktype == "linear":
+        return linear_scale(N, J, K, Nmid)
     raise ValueError(ktype)
 
 

@@ -153,9 +153,49 @@ def test_ktype_table_and_scale_builders(ktype, N, J, K, L):
     assert np.max(np.abs(s - so) / np.abs(so)) <= 1e-12
 
 
+@pytest.mark.parametrize("ktype,N,J,K,L", [
+    ("minmax:tuned", 20, 6, 40, 512), ("minmax:tuned", 21, 4, 42, 1024),
+    ("minmax:tuned", 16, 8, 32, 256), ("minmax:tuned", 20, 6, 30, 512),
+    ("minmax:unif", 20, 6, 40, 512), ("minmax:unif", 21, 5, 32, 256),
+    ("linear", 20, 2, 40, 512), ("linear", 21, 4, 42, 256)])
+def test_minmax_tuned_unif_linear_builders(ktype, N, J, K, L):
+    """'minmax:tuned' (the L = 3 sets for J = 4, 6, L = 2 for J = 8, alpha = 1,
+    beta = 0.5 for K/N != 2), 'minmax:unif' and 'linear': the library's builders
+    against the oracle (FP64 both; the min-max inverse is Gauss-Jordan in the
+    library and LAPACK in numpy)."""
+    nmid = np.floor(N / 2)
+    h, ho = mb.newfft_table(ktype, N, J, K, L), nf.ktype_table(ktype, N, J, K, L)
+    assert np.max(np.abs(h - ho)) <= 1e-11 * np.max(np.abs(ho))
+    s, so = mb.newfft_scale(ktype, N, J, K, nmid), nf.ktype_scale(ktype, N, J, K, nmid)
+    assert np.max(np.abs(s - so) / np.abs(so)) <= 1e-12
+
+
+@pytest.mark.parametrize("Nd", [(21,), (20,), (20, 10), (20, 10, 8)])
+@pytest.mark.parametrize("mode", ["table0", "table1"])
+def test_oracle_minmax_tuned_unif_linear_vs_exact_dtft(Nd, mode):
+    """On the reference's self-test set-ups (nufft/newfft.m:599-640):
+    'minmax:tuned' (which the self-test runs) within 0.12 % of the exact DTFT;
+    'minmax:unif' and 'linear' at Jd = 2 (which it lists and skips as poor)
+    within 1 % and 100 %: a wrong phase, Nmid or coefficient set gives errors
+    of order 100 % or more (measured: tuned <= 0.08 %, unif <= 0.58 %, linear
+    37-85 %, the straw man's own error)."""
+    om, x0 = _case(Nd)
+    ns = np.zeros(len(Nd))
+    Xe = nr.dtft(x0, om, ns)
+    xe = nr.dtft_adj(Xe, om, Nd, ns)
+    for ktype, Jd, bound in (("minmax:tuned", None, 0.12), ("minmax:unif", None, 1.0),
+                             ("linear", (2,) * len(Nd), 100.0)):
+        st = nf.newfft_init(om, Nd, Jd=Jd, mode=mode, ktype=ktype)
+        assert _mpd(Xe, nf.newfft_for(x0, st)) < bound, ktype
+        assert _mpd(xe, nf.newfft_adj(Xe, st)) < bound, ktype
+
+
 def test_ktype_errors():
     with pytest.raises(ValueError, match="ktype"):
-        mb.newfft_table("minmax:tuned", 20, 6, 40, 512)
+        mb.newfft_table("kb:user", 20, 6, 40, 512)
+    # K = 2 N with a J the tuned tables do not hold
+    with pytest.raises(mb.MirtError, match="unknown J,K/N"):
+        mb.newfft_table("minmax:tuned", 20, 12, 40, 512)
     lib = mb.load()
     h = np.empty(6 * 8 + 1)
     assert lib.mirt_newfft_ktype_table(7, 20, 6, 40, 8, h.ctypes.data_as(mb._lib._dp)) != 0
