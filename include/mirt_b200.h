@@ -469,6 +469,25 @@ int mirt_newfft_ktype_table(int32_t ktype, int32_t N, int32_t J, int32_t K, int3
 int mirt_newfft_ktype_scale(int32_t ktype, int32_t N, int32_t J, int32_t K, double nmid,
 	double *sn);
 
+/* newfft's interpolators with caller parameters (phasing 'real'; host FP64):
+ *   'kb:user' (nufft/newfft.m:300-313): the KB kernel of shape alpha and
+ *       integer order m in 0..32, f^m I_m(alpha f) / I_m(alpha), f = sqrt(1 -
+ *       (t/(J/2))^2) (nufft/kaiser_bessel.m:106-117; alpha and m printed with
+ *       %g into the kernel as the reference's inline kernel does); scale
+ *       1 / KB-FT((n - nmid) / K, J, alpha, m) (nufft/kaiser_bessel_ft.m:70-73)
+ *   'minmax:user' (nufft/newfft.m:329-335): the min-max interpolator for the
+ *       real Fourier coefficients alpha[0 .. nalpha-1] and beta of its scaling
+ *       factors (nufft/private/nufft_T.m, nufft_r.m); scale the real part of
+ *       nufft_scale1 (N <= K)
+ * One dimension per call, as the reference's st.kb_alf(id) / st.alpha{id}. */
+int mirt_newfft_kb_user_table(int32_t J, int32_t L, double alpha, int32_t m, double *h);
+int mirt_newfft_kb_user_scale(int32_t N, int32_t J, int32_t K, double nmid, double alpha,
+	int32_t m, double *sn);
+int mirt_newfft_minmax_user_table(int32_t N, int32_t J, int32_t K, int32_t L,
+	const double *alpha, int32_t nalpha, double beta, double *h);
+int mirt_newfft_minmax_user_scale(int32_t N, int32_t K, double nmid, const double *alpha,
+	int32_t nalpha, double beta, double *sn);
+
 /* Capture one batched step of the plan -- forward x -> X when x is given,
  * then adjoint X -> xa when xa is given -- into a CUDA graph (on an internal
  * capture stream) and return it instantiated; mirt_graph_launch replays it

@@ -47,6 +47,8 @@ std::vector<double> minmax_scale_real_ab(int N, int K, const std::vector<double>
 bool best_alpha(int J, int N, int K, std::vector<double> &alpha, double &beta);
 void linear_table(int J, int L, std::vector<double> &h);
 std::vector<double> linear_scale(int N, int J, int K, double Nmid);
+void kb_user_table(int J, int L, double alpha_full, int m, std::vector<double> &h);
+std::vector<double> kb_user_scale(int N, int J, int K, double nmid, double alpha, int m);
 int plan4_create(mirt_interp_plan **out, const int *K, const int *J, const int *L,
                  const double *const *h_re, const double *const *h_im, int order,
                  const double *tm, long long M4, const long long *moff, int nslice, int C,
@@ -2560,6 +2562,52 @@ int mirt_newfft_ktype_scale(int32_t ktype, int32_t N, int32_t J, int32_t K, doub
     case MIRT_KTYPE_LINEAR: s = linear_scale(N, J, K, nmid); break;
     default: return fail(MIRT_ERR_ARG, "unknown ktype");
   }
+  std::copy(s.begin(), s.end(), sn);
+  return MIRT_OK;
+}
+
+int mirt_newfft_kb_user_table(int32_t J, int32_t L, double alpha, int32_t m, double *h) {
+  if (J < 1 || J > MIRT_JMAX || L < 1) return fail(MIRT_ERR_ARG, "L must be positive, J in 1..16");
+  if (!h) return fail(MIRT_ERR_ARG, "output pointer is NULL");
+  if (!(alpha >= 0) || m < 0 || m > 32)
+    return fail(MIRT_ERR_ARG, "kb:user needs alpha >= 0 and an integer kb_m in 0..32");
+  std::vector<double> t;
+  kb_user_table(J, L, alpha, m, t);
+  std::copy(t.begin(), t.end(), h);
+  return MIRT_OK;
+}
+
+int mirt_newfft_kb_user_scale(int32_t N, int32_t J, int32_t K, double nmid, double alpha,
+                              int32_t m, double *sn) {
+  if (N < 1 || J < 1 || J > MIRT_JMAX || K < 1)
+    return fail(MIRT_ERR_ARG, "N, K must be positive, J in 1..16");
+  if (!sn) return fail(MIRT_ERR_ARG, "output pointer is NULL");
+  if (!(alpha >= 0) || m < 0 || m > 32)
+    return fail(MIRT_ERR_ARG, "kb:user needs alpha >= 0 and an integer kb_m in 0..32");
+  const std::vector<double> s = kb_user_scale(N, J, K, nmid, alpha, m);
+  std::copy(s.begin(), s.end(), sn);
+  return MIRT_OK;
+}
+
+int mirt_newfft_minmax_user_table(int32_t N, int32_t J, int32_t K, int32_t L,
+                                  const double *alpha, int32_t nalpha, double beta, double *h) {
+  if (N < 1 || J < 1 || J > MIRT_JMAX || K < 1 || L < 1)
+    return fail(MIRT_ERR_ARG, "N, K, L must be positive, J in 1..16");
+  if (!h || !alpha || nalpha < 1) return fail(MIRT_ERR_ARG, "NULL argument or empty alpha");
+  if (N > K) return fail(MIRT_ERR_ARG, "minmax:* needs N <= K");
+  std::vector<double> t;
+  if (!minmax_table_real_ab(N, J, K, L, std::vector<double>(alpha, alpha + nalpha), beta, t))
+    return fail(MIRT_ERR_ARG, "singular min-max matrix for this N, J, K");
+  std::copy(t.begin(), t.end(), h);
+  return MIRT_OK;
+}
+
+int mirt_newfft_minmax_user_scale(int32_t N, int32_t K, double nmid, const double *alpha,
+                                  int32_t nalpha, double beta, double *sn) {
+  if (N < 1 || K < 1) return fail(MIRT_ERR_ARG, "N, K must be positive");
+  if (!sn || !alpha || nalpha < 1) return fail(MIRT_ERR_ARG, "NULL argument or empty alpha");
+  const std::vector<double> s =
+      minmax_scale_real_ab(N, K, std::vector<double>(alpha, alpha + nalpha), beta, nmid);
   std::copy(s.begin(), s.end(), sn);
   return MIRT_OK;
 }

@@ -442,6 +442,83 @@ double kb_beatty_alpha(int N, int J, int K) {
   return a > 0 ? M_PI * std::sqrt(a) : 0.0;
 }
 
+// I_m(x) for an integer order m >= 0 and x >= 0 by its power series
+// sum_k (x/2)^(2k+m) / (k! (k+m)!) (positive terms)
+double bessel_in(int m, double x) {
+  const double q = x * x / 4.0;
+  double term = std::pow(x / 2.0, m) / std::tgamma(m + 1.0), sum = term;
+  for (int k = 1; k < 1000; k++) {
+    term *= q / ((double)k * (double)(k + m));
+    sum += term;
+    if (term < sum * 1e-17) break;
+  }
+  return sum;
+}
+
+// J_nu(z) / z^nu for nu = m + 1/2 (the 1D KB transform), given z^2 (z
+// imaginary when z^2 < 0, where the ratio is I_nu(|z|) / |z|^nu).  Power
+// series sum_k (-z^2/4)^k / (k! Gamma(k + nu + 1)) / 2^nu where its terms do
+// not cancel (z^2 <= 0, or z below m + 1); above, the spherical Bessel
+// function j_m by upward recurrence from sin z / z (J_{m+1/2}(z) =
+// sqrt(2 z / pi) j_m(z)), stable for z > m.
+double jnu_over_znu(int m, double z2) {
+  const double nu = m + 0.5;
+  if (z2 <= (double)(m + 1) * (m + 1)) {
+    double term = 1.0 / std::tgamma(nu + 1.0), sum = term;
+    for (int k = 1; k < 1000; k++) {
+      term *= (-z2 / 4.0) / ((double)k * ((double)k + nu));
+      sum += term;
+      if (std::fabs(term) < std::fabs(sum) * 1e-17) break;
+    }
+    return sum / std::pow(2.0, nu);
+  }
+  const double z = std::sqrt(z2);
+  double jm = std::sin(z) / z;
+  if (m > 0) {
+    double jprev = jm;
+    jm = std::sin(z) / (z * z) - std::cos(z) / z;
+    for (int l = 1; l < m; l++) {
+      const double jn = (2 * l + 1) / z * jm - jprev;
+      jprev = jm;
+      jm = jn;
+    }
+  }
+  return std::sqrt(2 * z / M_PI) * jm / std::pow(z, nu);
+}
+
+// ktype 'kb:user' (nufft/newfft.m:300-313): the KB kernel of shape alpha and
+// integer order m >= 0, f^m I_m(alpha f) / I_m(alpha) with f = sqrt(1 -
+// (t / (J/2))^2) on |t| < J/2 (nufft/kaiser_bessel.m:106-117), both printed
+// with %g into the inline kernel (:80-82), sampled at t = -J/2 + i/L as the
+// 'ratio' construction reads it
+void kb_user_table(int J, int L, double alpha_full, int m, std::vector<double> &h) {
+  char buf[64];
+  std::snprintf(buf, sizeof buf, "%g", alpha_full);
+  const double alpha = std::atof(buf);
+  const double den = bessel_in(m, alpha);
+  h.assign((size_t)J * L + 1, 0.0);
+  for (size_t i = 0; i < h.size(); i++) {
+    const double t = -J / 2.0 + (double)i / L;
+    if (std::fabs(t) < J / 2.0) {
+      const double f = std::sqrt(1 - (t / (J / 2.0)) * (t / (J / 2.0)));
+      h[i] = std::pow(f, m) * bessel_in(m, alpha * f) / den;
+    }
+  }
+}
+
+// its scaling factors 1 / KB-FT((n - nmid) / K) with the 1D transform
+// (2 pi)^(1/2) (J/2) alpha^m / I_m(alpha) J_nu(z) / z^nu, nu = m + 1/2,
+// z = sqrt((2 pi (J/2) u)^2 - alpha^2) (nufft/kaiser_bessel_ft.m:70-73)
+std::vector<double> kb_user_scale(int N, int J, int K, double nmid, double alpha, int m) {
+  const double c = std::sqrt(2 * M_PI) * (J / 2.0) * std::pow(alpha, m) / bessel_in(m, alpha);
+  std::vector<double> s(N);
+  for (int n = 0; n < N; n++) {
+    const double a = 2 * M_PI * (J / 2.0) * ((n - nmid) / K);
+    s[n] = 1.0 / (c * jnu_over_znu(m, a * a - alpha * alpha));
+  }
+  return s;
+}
+
 // Table of ktype 'diric' with phasing 'real' (nufft/newfft.m:256-266,
 // nufft/nufft_diric.m:31-36): the kernel N' / K diric(k, N', K) with the odd
 // N' = 2 floor((K + 1) / 2) - 1 and the true Dirichlet function

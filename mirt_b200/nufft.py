@@ -386,25 +386,66 @@ _KTYPES = {"kb:minmax": 0, "kb:beatty": 1, "diric": 2, "minmax:kb": 3, "minmax:u
            "minmax:tuned": 5, "linear": 6}
 
 
-def newfft_table(ktype: str, N: int, J: int, K: int, L: int) -> np.ndarray:
+_USER_KTYPES = ("kb:user", "minmax:user")
+
+
+def _user_args(ktype, kb_alf, kb_m, alpha, beta):
+    if ktype == "kb:user":
+        if kb_alf is None or kb_m is None:
+            raise ValueError("kb_alf and kb_m required")
+        if float(kb_m) != int(kb_m):
+            raise ValueError("kb:user: kb_m must be an integer")
+        return float(kb_alf), int(kb_m)
+    if alpha is None or beta is None:
+        raise ValueError("user must provide alpha/beta")
+    a = np.ascontiguousarray(np.atleast_1d(np.asarray(alpha, dtype=np.float64)))
+    return a, float(beta)
+
+
+def newfft_table(ktype: str, N: int, J: int, K: int, L: int, kb_alf=None, kb_m=None,
+                 alpha=None, beta=None) -> np.ndarray:
     """Real table of newfft's interpolator `ktype` ('kb:minmax', 'kb:beatty',
-    'diric', 'minmax:kb', 'minmax:unif', 'minmax:tuned', 'linear'; phasing
-    'real'), [J*L+1] (see mirt_newfft_ktype_table)."""
-    if ktype not in _KTYPES:
-        raise ValueError(f"ktype must be one of {sorted(_KTYPES)}")
+    'diric', 'minmax:kb', 'minmax:unif', 'minmax:tuned', 'linear'; 'kb:user'
+    with this dimension's kb_alf and integer kb_m; 'minmax:user' with its real
+    alpha and beta; phasing 'real'), [J*L+1] (see mirt_newfft_ktype_table,
+    mirt_newfft_kb_user_table, mirt_newfft_minmax_user_table)."""
     h = np.empty(int(J) * int(L) + 1)
-    check(load().mirt_newfft_ktype_table(_KTYPES[ktype], int(N), int(J), int(K), int(L),
-                                         h.ctypes.data_as(_dp)))
+    lib = load()
+    if ktype == "kb:user":
+        a, m = _user_args(ktype, kb_alf, kb_m, alpha, beta)
+        check(lib.mirt_newfft_kb_user_table(int(J), int(L), a, m, h.ctypes.data_as(_dp)))
+    elif ktype == "minmax:user":
+        a, b = _user_args(ktype, kb_alf, kb_m, alpha, beta)
+        check(lib.mirt_newfft_minmax_user_table(int(N), int(J), int(K), int(L),
+                                                a.ctypes.data_as(_dp), a.size, b,
+                                                h.ctypes.data_as(_dp)))
+    elif ktype in _KTYPES:
+        check(lib.mirt_newfft_ktype_table(_KTYPES[ktype], int(N), int(J), int(K), int(L),
+                                          h.ctypes.data_as(_dp)))
+    else:
+        raise ValueError(f"ktype must be one of {sorted(_KTYPES) + list(_USER_KTYPES)}")
     return h
 
 
-def newfft_scale(ktype: str, N: int, J: int, K: int, nmid: float) -> np.ndarray:
+def newfft_scale(ktype: str, N: int, J: int, K: int, nmid: float, kb_alf=None, kb_m=None,
+                 alpha=None, beta=None) -> np.ndarray:
     """1D scaling factors of newfft's interpolator `ktype`, [N]."""
-    if ktype not in _KTYPES:
-        raise ValueError(f"ktype must be one of {sorted(_KTYPES)}")
     s = np.empty(int(N))
-    check(load().mirt_newfft_ktype_scale(_KTYPES[ktype], int(N), int(J), int(K), float(nmid),
-                                         s.ctypes.data_as(_dp)))
+    lib = load()
+    if ktype == "kb:user":
+        a, m = _user_args(ktype, kb_alf, kb_m, alpha, beta)
+        check(lib.mirt_newfft_kb_user_scale(int(N), int(J), int(K), float(nmid), a, m,
+                                            s.ctypes.data_as(_dp)))
+    elif ktype == "minmax:user":
+        a, b = _user_args(ktype, kb_alf, kb_m, alpha, beta)
+        check(lib.mirt_newfft_minmax_user_scale(int(N), int(K), float(nmid),
+                                                a.ctypes.data_as(_dp), a.size, b,
+                                                s.ctypes.data_as(_dp)))
+    elif ktype in _KTYPES:
+        check(lib.mirt_newfft_ktype_scale(_KTYPES[ktype], int(N), int(J), int(K), float(nmid),
+                                          s.ctypes.data_as(_dp)))
+    else:
+        raise ValueError(f"ktype must be one of {sorted(_KTYPES) + list(_USER_KTYPES)}")
     return s
 
 
@@ -416,7 +457,9 @@ class NewfftPlan(NufftPlan):
     phasing 'real' (the reference's default) with ``tables=None`` builds the
     real tables and scaling factors of ``ktype`` in the library ('kb:minmax',
     the reference's default, 'kb:beatty', 'diric', 'minmax:kb', 'minmax:unif',
-    'minmax:tuned' or 'linear'); any other interpolator
+    'minmax:tuned', 'linear', 'kb:user' with per-dimension ``kb_alf`` and
+    integer ``kb_m``, or 'minmax:user' with per-dimension ``alpha`` (lists of
+    real coefficients) and ``beta``); any other interpolator
     is given as ``tables`` (one 1D table per dimension, real or complex, J*L+1
     values) and ``sn`` ([(Nd)], first index fastest).
     phasing 'real' applies phase_before / phase_after with Nmid = floor(N/2);
@@ -426,7 +469,7 @@ class NewfftPlan(NufftPlan):
 
     def __init__(self, om, Nd, Jd=None, Kd=None, n_shift=None, mode="table1", Ld=None,
                  phasing="real", tables=None, sn=None, ncol=1, slice_moff=None, stream=None,
-                 ktype="kb:minmax"):
+                 ktype="kb:minmax", kb_alf=None, kb_m=None, alpha=None, beta=None):
         om = np.asarray(om, dtype=np.float64)
         D = 1 if om.ndim == 1 else om.shape[1]
         Nd = _i32(Nd)
@@ -446,11 +489,18 @@ class NewfftPlan(NufftPlan):
             if phasing != "real":
                 raise ValueError("built-in tables are the phasing 'real' ones; pass tables "
                                  "and sn for other phasings")
-            tables = [newfft_table(ktype, Nd[d], Jd[d], Kd[d], Ld[d]) for d in range(D)]
+            # per-dimension user parameters (st.kb_alf(id), st.kb_m(id), st.alpha{id},
+            # st.beta{id}: nufft/private/newfft_table_init.m:88-96)
+            def user(d):
+                pick = lambda v: None if v is None else v[d]
+                return dict(kb_alf=pick(kb_alf), kb_m=pick(kb_m), alpha=pick(alpha),
+                            beta=pick(beta))
+            tables = [newfft_table(ktype, Nd[d], Jd[d], Kd[d], Ld[d], **user(d))
+                      for d in range(D)]
             s = np.ones(1)
             for d in range(D):
                 s = np.outer(s.ravel(order="F"), newfft_scale(ktype, Nd[d], Jd[d], Kd[d],
-                                                              self.Nmid[d]))
+                                                              self.Nmid[d], **user(d)))
             sn = s.ravel(order="F")
         if sn is None:
             raise ValueError("sn is required with caller tables")

@@ -37,6 +37,10 @@ What is restated, with the reference lines followed:
 * ``linear_table``       ktype 'linear' (nufft/newfft.m:268-273), the triangle
   read by the 'fast' construction; ``linear_scale`` newfft_scale_tri
   (nufft/newfft.m:535-550), evaluated per dimension
+* ``kb_table(J, L, alpha, kb_m)`` / ``kb_scale``  ktype 'kb:user' (nufft/newfft.m:300-313):
+  the KB kernel of order kb_m, its transform nufft/kaiser_bessel_ft.m:70-73
+* ``minmax_table`` with the caller's alpha / beta: ktype 'minmax:user'
+  (nufft/newfft.m:329-335)
 * ``phase_before``       nufft/newfft.m:511-520
 * ``phase_after``        nufft/newfft.m:522-527
 * ``newfft_for/adj``     nufft/private/newfft_approx_for.m:15-63,
@@ -83,21 +87,25 @@ def diric_table(J: int, K: int, L: int) -> np.ndarray:
     return np.append(h, h[0])
 
 
-def kb_table(J: int, L: int, alpha=None) -> np.ndarray:
-    """Real [J*L+1] table of the KB kernel (kb_m = 0) of shape alpha (default
-    2.34 J: 'kb:minmax'), alpha printed with %g as the inline kernel does."""
+def kb_table(J: int, L: int, alpha=None, kb_m=0) -> np.ndarray:
+    """Real [J*L+1] table of the KB kernel of shape alpha (default 2.34 J:
+    'kb:minmax') and order kb_m, f^m I_m(alpha f) / I_m(alpha)
+    (nufft/kaiser_bessel.m:106-117), alpha and kb_m printed with %g as the
+    inline kernel does (:80-82)."""
     alpha = float(f"{(kb_alpha(J) if alpha is None else alpha):g}")
+    kb_m = float(f"{kb_m:g}")
     t = (np.arange(J * L + 1) - J * L / 2) / L
     h = np.zeros(J * L + 1)
     inside = np.abs(t) < J / 2
     f = np.sqrt(1 - (t[inside] / (J / 2)) ** 2)
-    h[inside] = special.iv(0, alpha * f) / special.iv(0, alpha)
+    h[inside] = f ** kb_m * special.iv(abs(kb_m), alpha * f) / special.iv(abs(kb_m), alpha)
     return h
 
 
-def kb_scale(N: int, J: int, K: int, Nmid: float, alpha=None) -> np.ndarray:
+def kb_scale(N: int, J: int, K: int, Nmid: float, alpha=None, kb_m=0) -> np.ndarray:
     nc = np.arange(N) - Nmid
-    return 1.0 / nr.kaiser_bessel_ft(nc / K, J, kb_alpha(J) if alpha is None else alpha, 0.0, 1)
+    return 1.0 / nr.kaiser_bessel_ft(nc / K, J, kb_alpha(J) if alpha is None else alpha,
+                                     float(kb_m), 1)
 
 
 # nufft/nufft_best_alpha.m:13-33: tuned Fourier coefficients of the scaling
@@ -171,7 +179,11 @@ def linear_scale(N, J, K, Nmid):
     return fun(nc) / tmp
 
 
-def ktype_table(ktype, N, J, K, L):
+def ktype_table(ktype, N, J, K, L, kb_alf=None, kb_m=None, alpha=None, beta=None):
+    if ktype == "kb:user":
+        return kb_table(J, L, kb_alf, kb_m)
+    if ktype == "minmax:user":
+        return minmax_table(N, J, K, L, np.atleast_1d(np.asarray(alpha, dtype=np.float64)), beta)
     if ktype == "kb:minmax":
         return kb_table(J, L)
     if ktype == "kb:beatty":
@@ -189,7 +201,12 @@ def ktype_table(ktype, N, J, K, L):
     raise ValueError(ktype)
 
 
-def ktype_scale(ktype, N, J, K, Nmid):
+def ktype_scale(ktype, N, J, K, Nmid, kb_alf=None, kb_m=None, alpha=None, beta=None):
+    if ktype == "kb:user":
+        return kb_scale(N, J, K, Nmid, kb_alf, kb_m)
+    if ktype == "minmax:user":
+        return np.real(nr.nufft_scale1(N, K, np.atleast_1d(np.asarray(alpha, dtype=np.float64)),
+                                       beta, Nmid))
     if ktype == "kb:minmax":
         return kb_scale(N, J, K, Nmid)
     if ktype == "kb:beatty":
@@ -217,10 +234,13 @@ def phase_before(Kd, Nmid) -> np.ndarray:
 
 
 def newfft_init(om, Nd, Jd=None, Kd=None, n_shift=None, mode="table1", Ld=None,
-                phasing="real", h=None, sn=None, ktype="kb:minmax") -> dict:
+                phasing="real", h=None, sn=None, ktype="kb:minmax", kb_alf=None, kb_m=None,
+                alpha=None, beta=None) -> dict:
     """st of newfft(om, Nd, 'Jd', Jd, 'Kd', Kd, 'n_shift', n_shift, 'mode', mode,
-    'oversample', Ld, 'phasing', phasing, 'ktype', ktype) for ktype 'kb:minmax',
-    'kb:beatty' or 'diric' (or the caller's tables h and scaling factors sn)."""
+    'oversample', Ld, 'phasing', phasing, 'ktype', ktype[, 'kb_alf', kb_alf,
+    'kb_m', kb_m | 'alpha', alpha, 'beta', beta]) for the built-in ktypes (or
+    the caller's tables h and scaling factors sn); user parameters are given
+    per dimension."""
     om = np.asarray(om, dtype=np.float64)
     if om.ndim == 1:
         om = om[:, None]
@@ -233,12 +253,16 @@ def newfft_init(om, Nd, Jd=None, Kd=None, n_shift=None, mode="table1", Ld=None,
         Ld = 2 ** 11 if order == 0 else 2 ** 9
     Ld = tuple(Ld if np.ndim(Ld) else [int(Ld)] * dd)
     Nmid = nmid_of(Nd, phasing)
+    def user(d):
+        pick = lambda v: None if v is None else v[d]
+        return dict(kb_alf=pick(kb_alf), kb_m=pick(kb_m), alpha=pick(alpha), beta=pick(beta))
     if h is None:
-        h = [ktype_table(ktype, Nd[d], Jd[d], Kd[d], Ld[d]) for d in range(dd)]
+        h = [ktype_table(ktype, Nd[d], Jd[d], Kd[d], Ld[d], **user(d)) for d in range(dd)]
     if sn is None:
         s = np.ones(1)
         for d in range(dd):
-            s = np.outer(s.ravel(order="F"), ktype_scale(ktype, Nd[d], Jd[d], Kd[d], Nmid[d]))
+            s = np.outer(s.ravel(order="F"), ktype_scale(ktype, Nd[d], Jd[d], Kd[d], Nmid[d],
+                                                         **user(d)))
         sn = s.reshape(tuple(Nd), order="F")
     st = dict(om=om, Nd=tuple(Nd), Jd=Jd, Kd=Kd, Ld=Ld, order=order, Nmid=Nmid,
               n_shift=n_shift, h=h, sn=np.asarray(sn).reshape(tuple(Nd), order="F"),

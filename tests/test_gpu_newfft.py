@@ -89,6 +89,30 @@ def test_other_interpolators(ktype, Nd, mode):
     assert _mpd(nr.dtft_adj(Xe, om, Nd, ns), st.adj(Xe)) < bound
 
 
+@pytest.mark.parametrize("kw", [dict(ktype="kb:user", kb_m=1, kb_alf=15.0),
+                                dict(ktype="minmax:user", alpha=[1.0, -0.57, 0.14], beta=0.43)])
+@pytest.mark.parametrize("Nd", [(20,), (6, 5)])
+@pytest.mark.parametrize("mode", ["table0", "table1"])
+def test_user_interpolators(kw, Nd, mode):
+    """'kb:user' (order 1) and 'minmax:user' with per-dimension parameters:
+    the oracle's forward / adjoint, and within 1 % of the exact DTFT."""
+    dd = len(Nd)
+    per_dim = {k: (v if k == "ktype" else [v] * dd) for k, v in kw.items()}
+    rng = np.random.default_rng(2)
+    om = 3 * 2 * np.pi * (rng.random((100, dd)) - 0.5)
+    x0 = rng.random(Nd)
+    st = mb.newfft(om, Nd, mode=mode, **per_dim)
+    so = nf.newfft_init(om, Nd, mode=mode, **per_dim)
+    X = st.fft(x0)
+    Xo = nf.newfft_for(x0, so)
+    assert rel_l2(X, Xo) <= TOL
+    assert rel_l2(st.adj(Xo), nf.newfft_adj(Xo, so)) <= TOL
+    ns = np.zeros(dd)
+    Xe = nr.dtft(x0, om, ns)
+    assert _mpd(Xe, X) < 1.0
+    assert _mpd(nr.dtft_adj(Xe, om, Nd, ns), st.adj(Xe)) < 1.0
+
+
 def test_batched_slices_coils_and_shift():
     """Three trajectories of uneven length, 3 columns, centred image (n_shift =
     N/2), table1: every slice and column against the oracle."""

@@ -190,9 +190,68 @@ def test_oracle_minmax_tuned_unif_linear_vs_exact_dtft(Nd, mode):
         assert _mpd(xe, nf.newfft_adj(Xe, st)) < bound, ktype
 
 
+@pytest.mark.parametrize("J,L,alf,m", [(6, 512, 2.34 * 6, 0), (6, 512, 14.0, 1), (8, 256, 18.5, 2),
+                                       (4, 1024, 5.0, 3), (6, 512, 3.0, 0)])
+def test_kb_user_builders(J, L, alf, m):
+    """'kb:user': the KB kernel of order m and its transform (the library's
+    series / spherical-Bessel evaluation against scipy's iv / jv)."""
+    h = mb.newfft_table("kb:user", 20, J, 40, L, kb_alf=alf, kb_m=m)
+    ho = nf.ktype_table("kb:user", 20, J, 40, L, kb_alf=alf, kb_m=m)
+    assert np.max(np.abs(h - ho)) <= 1e-13 * np.max(np.abs(ho))
+    for N, K in ((20, 40), (21, 32), (64, 128)):
+        nmid = np.floor(N / 2)
+        s = mb.newfft_scale("kb:user", N, J, K, nmid, kb_alf=alf, kb_m=m)
+        so = nf.ktype_scale("kb:user", N, J, K, nmid, kb_alf=alf, kb_m=m)
+        assert np.max(np.abs(s - so) / np.abs(so)) <= 1e-12
+
+
+@pytest.mark.parametrize("alpha,beta", [([1.0], 0.5), ([1, -0.57, 0.14], 0.43), ([1.0], 0.0)])
+def test_minmax_user_builders(alpha, beta):
+    h = mb.newfft_table("minmax:user", 20, 6, 40, 512, alpha=alpha, beta=beta)
+    ho = nf.ktype_table("minmax:user", 20, 6, 40, 512, alpha=alpha, beta=beta)
+    assert np.max(np.abs(h - ho)) <= 1e-11 * np.max(np.abs(ho))
+    s = mb.newfft_scale("minmax:user", 20, 6, 40, 10.0, alpha=alpha, beta=beta)
+    so = nf.ktype_scale("minmax:user", 20, 6, 40, 10.0, alpha=alpha, beta=beta)
+    assert np.max(np.abs(s - so) / np.abs(so)) <= 1e-12
+
+
+@pytest.mark.parametrize("Nd", ND_LIST)
+@pytest.mark.parametrize("mode", ["table0", "table1"])
+def test_oracle_user_ktypes_vs_exact_dtft(Nd, mode):
+    """The self-test's 'kb:user' (kb_m = 0, kb_alf = 2.34 * 6: within the
+    'kb:minmax' bounds) and 'minmax:user' (alpha = 1, beta = 0.5, listed and
+    skipped as poor: within 1 %), nufft/newfft.m:627-632; 'kb:user' of orders
+    1 and 2 (alpha 15, 16) within 1 % (measured <= 0.34 %; scaling factors of
+    the wrong order give about 6 %)."""
+    om, x0 = _case(Nd)
+    dd = len(Nd)
+    ns = np.zeros(dd)
+    Xe = nr.dtft(x0, om, ns)
+    xe = nr.dtft_adj(Xe, om, Nd, ns)
+    cases = ((dict(ktype="kb:user", kb_alf=[2.34 * 6] * dd, kb_m=[0] * dd), BOUND[mode]),
+             (dict(ktype="kb:user", kb_alf=[15.0] * dd, kb_m=[1] * dd), 1.0),
+             (dict(ktype="kb:user", kb_alf=[16.0] * dd, kb_m=[2] * dd), 1.0),
+             (dict(ktype="minmax:user", alpha=[[1.0]] * dd, beta=[0.5] * dd), 1.0))
+    for kw, bound in cases:
+        st = nf.newfft_init(om, Nd, mode=mode, **kw)
+        assert _mpd(Xe, nf.newfft_for(x0, st)) < bound, kw
+        assert _mpd(xe, nf.newfft_adj(Xe, st)) < bound, kw
+
+
+def test_user_ktype_errors():
+    with pytest.raises(ValueError, match="kb_alf and kb_m required"):
+        mb.newfft_table("kb:user", 20, 6, 40, 512, kb_alf=14.0)
+    with pytest.raises(ValueError, match="integer"):
+        mb.newfft_table("kb:user", 20, 6, 40, 512, kb_alf=14.0, kb_m=0.5)
+    with pytest.raises(mb.MirtError, match="alpha >= 0"):
+        mb.newfft_scale("kb:user", 20, 6, 40, 10.0, kb_alf=-1.0, kb_m=0)
+    with pytest.raises(ValueError, match="alpha/beta"):
+        mb.newfft_table("minmax:user", 20, 6, 40, 512, alpha=[1.0])
+
+
 def test_ktype_errors():
     with pytest.raises(ValueError, match="ktype"):
-        mb.newfft_table("kb:user", 20, 6, 40, 512)
+        mb.newfft_table("minmax:other", 20, 6, 40, 512)
     # K = 2 N with a J the tuned tables do not hold
     with pytest.raises(mb.MirtError, match="unknown J,K/N"):
         mb.newfft_table("minmax:tuned", 20, 12, 40, 512)
