@@ -488,6 +488,23 @@ int mirt_newfft_minmax_user_table(int32_t N, int32_t J, int32_t K, int32_t L,
 int mirt_newfft_minmax_user_scale(int32_t N, int32_t K, double nmid, const double *alpha,
 	int32_t nalpha, double beta, double *sn);
 
+/* newfft's tables with phasing 'complex' (host FP64, J*L+1 complex values
+ * split into h_re / h_im) for every ktype above, MIRT_KTYPE_KB_USER (kb_alf,
+ * kb_m) and MIRT_KTYPE_MINMAX_USER (alpha[0 .. nalpha-1], beta); the other
+ * ktypes ignore those arguments.  The sparse interpolator's entries
+ * conj(exp(i gam (N-1)/2 (t - k)) c) (nufft/newfft.m:405-411, 446) read by
+ * the 'fast' construction (nufft/private/newfft_table_init.m:160-169: the
+ * last entry repeats the first; 'diric' without the odd-N trick of phasing
+ * 'real'), or for 'kb:*' by the 'ratio' construction (:173-184: a fake
+ * problem N' = J, K' = J K / N and the phase exp(i pi t (1/K - 1/K'))).
+ * 'minmax:kb' fits its alphas at Nmid = (N-1)/2.  Scaling factors: the
+ * functions above with nmid = (N-1)/2. */
+#define MIRT_KTYPE_KB_USER 7
+#define MIRT_KTYPE_MINMAX_USER 8
+int mirt_newfft_table_complex(int32_t ktype, int32_t N, int32_t J, int32_t K, int32_t L,
+	double kb_alf, int32_t kb_m, const double *alpha, int32_t nalpha, double beta,
+	double *h_re, double *h_im);
+
 /* Capture one batched step of the plan -- forward x -> X when x is given,
  * then adjoint X -> xa when xa is given -- into a CUDA graph (on an internal
  * capture stream) and return it instantiated; mirt_graph_launch replays it

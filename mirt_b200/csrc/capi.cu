@@ -48,6 +48,12 @@ bool best_alpha(int J, int N, int K, std::vector<double> &alpha, double &beta);
 void linear_table(int J, int L, std::vector<double> &h);
 std::vector<double> linear_scale(int N, int J, int K, double Nmid);
 void kb_user_table(int J, int L, double alpha_full, int m, std::vector<double> &h);
+void kb_table_complex(int N, int J, int K, int L, double alpha_full, int m,
+                      std::vector<std::complex<double>> &h);
+bool minmax_table_complex_ab(int N, int J, int K, int L, const std::vector<double> &alpha,
+                             double beta, std::vector<std::complex<double>> &h);
+void diric_table_complex(int N, int J, int K, int L, std::vector<std::complex<double>> &h);
+void linear_table_complex(int N, int J, int K, int L, std::vector<std::complex<double>> &h);
 std::vector<double> kb_user_scale(int N, int J, int K, double nmid, double alpha, int m);
 int plan4_create(mirt_interp_plan **out, const int *K, const int *J, const int *L,
                  const double *const *h_re, const double *const *h_im, int order,
@@ -2563,6 +2569,59 @@ int mirt_newfft_ktype_scale(int32_t ktype, int32_t N, int32_t J, int32_t K, doub
     default: return fail(MIRT_ERR_ARG, "unknown ktype");
   }
   std::copy(s.begin(), s.end(), sn);
+  return MIRT_OK;
+}
+
+int mirt_newfft_table_complex(int32_t ktype, int32_t N, int32_t J, int32_t K, int32_t L,
+                              double kb_alf, int32_t kb_m, const double *alpha, int32_t nalpha,
+                              double beta, double *h_re, double *h_im) {
+  if (N < 1 || J < 1 || J > MIRT_JMAX || K < 1 || L < 1)
+    return fail(MIRT_ERR_ARG, "N, K, L must be positive, J in 1..16");
+  if (!h_re || !h_im) return fail(MIRT_ERR_ARG, "output pointer is NULL");
+  std::vector<std::complex<double>> t;
+  const bool minmax = ktype == MIRT_KTYPE_MINMAX_KB || ktype == MIRT_KTYPE_MINMAX_UNIF ||
+                      ktype == MIRT_KTYPE_MINMAX_TUNED || ktype == MIRT_KTYPE_MINMAX_USER;
+  if (minmax && N > K) return fail(MIRT_ERR_ARG, "minmax:* needs N <= K");
+  switch (ktype) {
+    case MIRT_KTYPE_KB_MINMAX: kb_table_complex(N, J, K, L, 2.34 * J, 0, t); break;
+    case MIRT_KTYPE_KB_BEATTY: {
+      const double a = kb_beatty_alpha(N, J, K);
+      if (!(a > 0)) return fail(MIRT_ERR_ARG, "kb:beatty has no real shape for this J, K/N");
+      kb_table_complex(N, J, K, L, a, 0, t);
+      break;
+    }
+    case MIRT_KTYPE_KB_USER:
+      if (!(kb_alf >= 0) || kb_m < 0 || kb_m > 32)
+        return fail(MIRT_ERR_ARG, "kb:user needs alpha >= 0 and an integer kb_m in 0..32");
+      kb_table_complex(N, J, K, L, kb_alf, kb_m, t);
+      break;
+    case MIRT_KTYPE_DIRIC: diric_table_complex(N, J, K, L, t); break;
+    case MIRT_KTYPE_LINEAR: linear_table_complex(N, J, K, L, t); break;
+    case MIRT_KTYPE_MINMAX_KB:
+    case MIRT_KTYPE_MINMAX_UNIF:
+    case MIRT_KTYPE_MINMAX_TUNED:
+    case MIRT_KTYPE_MINMAX_USER: {
+      std::vector<double> a{1.0};
+      double b = 0.0;
+      if (ktype == MIRT_KTYPE_MINMAX_KB) {
+        alpha_kb_fit(N, J, K, a, b);  // Nmid = (N - 1) / 2 with phasing 'complex'
+      } else if (ktype == MIRT_KTYPE_MINMAX_TUNED) {
+        if (!best_alpha(J, N, K, a, b)) return fail(MIRT_ERR_ARG, "minmax:tuned: unknown J,K/N");
+      } else if (ktype == MIRT_KTYPE_MINMAX_USER) {
+        if (!alpha || nalpha < 1) return fail(MIRT_ERR_ARG, "user must provide alpha/beta");
+        a.assign(alpha, alpha + nalpha);
+        b = beta;
+      }
+      if (!minmax_table_complex_ab(N, J, K, L, a, b, t))
+        return fail(MIRT_ERR_ARG, "singular min-max matrix for this N, J, K");
+      break;
+    }
+    default: return fail(MIRT_ERR_ARG, "unknown ktype");
+  }
+  for (size_t i = 0; i < t.size(); i++) {
+    h_re[i] = t[i].real();
+    h_im[i] = t[i].imag();
+  }
   return MIRT_OK;
 }
 

@@ -519,6 +519,121 @@ std::vector<double> kb_user_scale(int N, int J, int K, double nmid, double alpha
   return s;
 }
 
+// ---------------------------------------------------------------------------
+// newfft's tables for phasing 'complex'
+// ---------------------------------------------------------------------------
+// The 'fast' construction of nufft/private/newfft_table_init.m:160-169 with
+// phasing 'complex': the sparse interpolator of the sample points om = t1 2 pi
+// / K, t1 = J/2 - 1 + l/L, has the entries conj(exp(i gam (N - 1)/2 arg) c)
+// (nufft/newfft.m:405-411, 446) at grid columns mod(koff + j, K), where c is
+// the coefficient of tap j at offset arg = -j + om/gam - koff
+// (nufft/private/nufft_coef.m, nufft_r.m); the table is columns J .. 1 of it,
+// the last entry repeating the first.  K may be fractional (the 'ratio'
+// construction's fake problem).  coef(arg, c) fills the J coefficients of one
+// sample point.
+template <class Coef>
+void table_fast_complex(double N, int J, double K, int L, Coef coef, std::vector<cd> &h) {
+  const double gam = 2 * M_PI / K;
+  std::vector<cd> p((size_t)L * J, cd(0, 0));  // the used columns 0 .. J-1
+  std::vector<double> arg(J), c(J);
+  for (int l = 0; l < L; l++) {
+    const double t1 = (J / 2.0 - 1) + (double)l / L;
+    const double om = t1 * 2 * M_PI / K;
+    const double koff = std::floor(om / gam - J / 2.0);
+    const double dk = om / gam - koff;
+    for (int j = 0; j < J; j++) arg[j] = -(double)(j + 1) + dk;
+    coef(arg.data(), c.data());
+    for (int j = 0; j < J; j++) {
+      const cd ud = std::exp(cd(0, gam * (N - 1) / 2 * arg[j])) * c[j];
+      const double col = std::fmod(std::fmod(koff + (j + 1), K) + K, K);
+      if (col < J && col == std::floor(col)) p[(size_t)l + (size_t)col * L] += std::conj(ud);
+    }
+  }
+  h.assign((size_t)J * L + 1, cd(0, 0));
+  for (int jj = J - 1, blk = 0; jj >= 0; jj--, blk++)
+    for (int l = 0; l < L; l++) h[(size_t)blk * L + l] = p[(size_t)l + (size_t)jj * L];
+  h[(size_t)J * L] = h[0];
+}
+
+// 'kb:*' with phasing 'complex': the 'ratio' construction
+// (nufft/private/newfft_table_init.m:173-184): the fake problem N' = J,
+// K' = J K / N, then the phase exp(i pi t (1/K - 1/K')) at t = -J/2 + i/L
+void kb_table_complex(int N, int J, int K, int L, double alpha_full, int m, std::vector<cd> &h) {
+  char buf[64];
+  std::snprintf(buf, sizeof buf, "%g", alpha_full);
+  const double alpha = std::atof(buf);
+  const double den = bessel_in(m, alpha);
+  const double Kf = (double)J * K / N;
+  table_fast_complex((double)J, J, Kf, L, [&](const double *arg, double *c) {
+    for (int j = 0; j < J; j++) {
+      const double u = arg[j] / (J / 2.0);
+      c[j] = std::fabs(arg[j]) < J / 2.0
+                 ? std::pow(std::sqrt(1 - u * u), m) * bessel_in(m, alpha * std::sqrt(1 - u * u)) / den
+                 : 0.0;
+    }
+  }, h);
+  for (size_t i = 0; i < h.size(); i++) {
+    const double t = -J / 2.0 + (double)i / L;
+    h[i] *= std::exp(cd(0, M_PI * t * (1.0 / K - 1.0 / Kf)));
+  }
+}
+
+// 'minmax:*' with phasing 'complex': T = inv(C'SS'C), c = T r for the
+// scaling-factor coefficients alpha, beta, in the 'fast' construction
+bool minmax_table_complex_ab(int N, int J, int K, int L, const std::vector<double> &alpha,
+                             double beta, std::vector<cd> &h) {
+  const int La = (int)alpha.size() - 1;
+  std::vector<double> T(J * J, 0.0);
+  for (int a = 0; a < J; a++)
+    for (int b = 0; b < J; b++) {
+      double s = 0;
+      for (int l1 = -La; l1 <= La; l1++)
+        for (int l2 = -La; l2 <= La; l2++)
+          s += alpha[std::abs(l1)] * alpha[std::abs(l2)] *
+               diric((double)(b - a) + beta * (double)(l1 - l2), N, K);
+      T[a * J + b] = s;
+    }
+  if (!invert(T, J)) return false;
+  std::vector<double> r(J);
+  table_fast_complex((double)N, J, (double)K, L, [&](const double *arg, double *c) {
+    for (int j = 0; j < J; j++) {
+      double s = 0;
+      for (int l1 = -La; l1 <= La; l1++) s += alpha[std::abs(l1)] * diric(arg[j] + l1 * beta, N, K);
+      r[j] = s;
+    }
+    for (int j = 0; j < J; j++) {
+      double v = 0;
+      for (int i = 0; i < J; i++) v += T[j * J + i] * r[i];
+      c[j] = v;
+    }
+  }, h);
+  return true;
+}
+
+// 'diric' with phasing 'complex' (nufft/newfft.m:256-266 without the odd-N
+// trick of phasing 'real'): N/K diric(t, N, K) with the true Dirichlet kernel
+// sin(pi t N / K) / (N sin(pi t / K)) (nufft/nufft_diric.m:31-36)
+void diric_table_complex(int N, int J, int K, int L, std::vector<cd> &h) {
+  table_fast_complex((double)N, J, (double)K, L, [&](const double *arg, double *c) {
+    for (int j = 0; j < J; j++) {
+      const double t = M_PI / K * arg[j];
+      const double f = std::sin(t);
+      const double cs = std::cos(t * (N - 1));
+      const double d = std::fabs(f) > 1e-12 ? std::sin(N * t) / (N * f)
+                                            : (double)((cs > 0) - (cs < 0));
+      c[j] = (double)N / K * d;
+    }
+  }, h);
+}
+
+// 'linear' with phasing 'complex'
+void linear_table_complex(int N, int J, int K, int L, std::vector<cd> &h) {
+  table_fast_complex((double)N, J, (double)K, L, [&](const double *arg, double *c) {
+    for (int j = 0; j < J; j++)
+      c[j] = std::fabs(arg[j]) < J / 2.0 ? 1 - std::fabs(arg[j] / (J / 2.0)) : 0.0;
+  }, h);
+}
+
 // Table of ktype 'diric' with phasing 'real' (nufft/newfft.m:256-266,
 // nufft/nufft_diric.m:31-36): the kernel N' / K diric(k, N', K) with the odd
 // N' = 2 floor((K + 1) / 2) - 1 and the true Dirichlet function

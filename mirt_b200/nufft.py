@@ -402,13 +402,36 @@ def _user_args(ktype, kb_alf, kb_m, alpha, beta):
     return a, float(beta)
 
 
+def _newfft_table_complex(ktype, N, J, K, L, kb_alf, kb_m, alpha, beta):
+    code = {**_KTYPES, "kb:user": 7, "minmax:user": 8}.get(ktype)
+    if code is None:
+        raise ValueError(f"ktype must be one of {sorted(_KTYPES) + list(_USER_KTYPES)}")
+    a, m, al, b = 0.0, 0, None, 0.0
+    if ktype == "kb:user":
+        a, m = _user_args(ktype, kb_alf, kb_m, alpha, beta)
+    elif ktype == "minmax:user":
+        al, b = _user_args(ktype, kb_alf, kb_m, alpha, beta)
+    hr = np.empty(int(J) * int(L) + 1)
+    hi = np.empty_like(hr)
+    check(load().mirt_newfft_table_complex(
+        code, int(N), int(J), int(K), int(L), a, m,
+        None if al is None else al.ctypes.data_as(_dp), 0 if al is None else al.size, b,
+        hr.ctypes.data_as(_dp), hi.ctypes.data_as(_dp)))
+    return hr + 1j * hi
+
+
 def newfft_table(ktype: str, N: int, J: int, K: int, L: int, kb_alf=None, kb_m=None,
-                 alpha=None, beta=None) -> np.ndarray:
+                 alpha=None, beta=None, phasing="real") -> np.ndarray:
     """Real table of newfft's interpolator `ktype` ('kb:minmax', 'kb:beatty',
     'diric', 'minmax:kb', 'minmax:unif', 'minmax:tuned', 'linear'; 'kb:user'
     with this dimension's kb_alf and integer kb_m; 'minmax:user' with its real
     alpha and beta; phasing 'real'), [J*L+1] (see mirt_newfft_ktype_table,
-    mirt_newfft_kb_user_table, mirt_newfft_minmax_user_table)."""
+    mirt_newfft_kb_user_table, mirt_newfft_minmax_user_table); phasing
+    'complex': the complex table (see mirt_newfft_table_complex)."""
+    if phasing == "complex":
+        return _newfft_table_complex(ktype, N, J, K, L, kb_alf, kb_m, alpha, beta)
+    if phasing != "real":
+        raise ValueError("phasing must be 'real' or 'complex'")
     h = np.empty(int(J) * int(L) + 1)
     lib = load()
     if ktype == "kb:user":
@@ -459,7 +482,9 @@ class NewfftPlan(NufftPlan):
     the reference's default, 'kb:beatty', 'diric', 'minmax:kb', 'minmax:unif',
     'minmax:tuned', 'linear', 'kb:user' with per-dimension ``kb_alf`` and
     integer ``kb_m``, or 'minmax:user' with per-dimension ``alpha`` (lists of
-    real coefficients) and ``beta``); any other interpolator
+    real coefficients) and ``beta``); with phasing 'complex' the complex
+    tables of the same ktypes, with the scaling factors at Nmid = (N-1)/2; any
+    other interpolator
     is given as ``tables`` (one 1D table per dimension, real or complex, J*L+1
     values) and ``sn`` ([(Nd)], first index fastest).
     phasing 'real' applies phase_before / phase_after with Nmid = floor(N/2);
@@ -486,16 +511,13 @@ class NewfftPlan(NufftPlan):
         self.phasing = phasing
         self.Nmid = (np.floor(Nd / 2) if phasing == "real" else (Nd - 1) / 2).astype(np.float64)
         if tables is None:
-            if phasing != "real":
-                raise ValueError("built-in tables are the phasing 'real' ones; pass tables "
-                                 "and sn for other phasings")
             # per-dimension user parameters (st.kb_alf(id), st.kb_m(id), st.alpha{id},
             # st.beta{id}: nufft/private/newfft_table_init.m:88-96)
             def user(d):
                 pick = lambda v: None if v is None else v[d]
                 return dict(kb_alf=pick(kb_alf), kb_m=pick(kb_m), alpha=pick(alpha),
                             beta=pick(beta))
-            tables = [newfft_table(ktype, Nd[d], Jd[d], Kd[d], Ld[d], **user(d))
+            tables = [newfft_table(ktype, Nd[d], Jd[d], Kd[d], Ld[d], phasing=phasing, **user(d))
                       for d in range(D)]
             s = np.ones(1)
             for d in range(D):

@@ -41,6 +41,10 @@ What is restated, with the reference lines followed:
   the KB kernel of order kb_m, its transform nufft/kaiser_bessel_ft.m:70-73
 * ``minmax_table`` with the caller's alpha / beta: ktype 'minmax:user'
   (nufft/newfft.m:329-335)
+* ``ktype_table_complex`` every ktype with phasing 'complex': the sparse
+  interpolator's entries conj(exp(i gam (N-1)/2 arg) c) (nufft/newfft.m:405-411,
+  446) read by the 'fast' construction, or for 'kb:*' by the 'ratio' one with
+  its phase correction (nufft/private/newfft_table_init.m:160-184)
 * ``phase_before``       nufft/newfft.m:511-520
 * ``phase_after``        nufft/newfft.m:522-527
 * ``newfft_for/adj``     nufft/private/newfft_approx_for.m:15-63,
@@ -224,6 +228,87 @@ def ktype_scale(ktype, N, J, K, Nmid, kb_alf=None, kb_m=None, alpha=None, beta=N
     raise ValueError(ktype)
 
 
+def _fast_table_complex(N, J, K, L, coef):
+    """The 'fast' construction (nufft/private/newfft_table_init.m:160-169) with
+    phasing 'complex': sparse-interpolator entries conj(exp(i gam (N-1)/2 arg)
+    c(arg)) (nufft/newfft.m:405-411, 446) at columns mod(koff + j, K), the
+    table columns J .. 1, the last entry repeating the first.  K may be
+    fractional (the 'ratio' construction's fake problem)."""
+    gam = 2 * np.pi / K
+    t1 = (J / 2 - 1) + np.arange(L, dtype=np.float64) / L
+    om1 = t1 * 2 * np.pi / K
+    koff = nr.nufft_offset(om1, J, K)
+    dk = om1 / gam - koff
+    arg = -np.arange(1, J + 1, dtype=np.float64)[:, None] + dk[None, :]      # [J, L]
+    uu = np.conj(np.exp(1j * gam * (N - 1) / 2 * arg) * coef(arg))
+    kd = np.mod(np.arange(1, J + 1)[:, None] + koff[None, :], K)
+    p = np.zeros((L, J), dtype=np.complex128)
+    for j in range(J):
+        use = (kd[j] < J) & (kd[j] == np.floor(kd[j]))
+        np.add.at(p, (np.arange(L)[use], kd[j][use].astype(np.int64)), uu[j][use])
+    h = np.concatenate([p[:, jj] for jj in range(J - 1, -1, -1)])
+    return np.append(h, h[0])
+
+
+def ktype_table_complex(ktype, N, J, K, L, kb_alf=None, kb_m=None, alpha=None, beta=None):
+    """Complex [J*L+1] table of `ktype` with phasing 'complex': the 'ratio'
+    construction for 'kb:*' (nufft/private/newfft_table_init.m:173-184: fake
+    N' = J, K' = J K / N, then exp(i pi t (1/K - 1/K'))), the 'fast' one for
+    the others ('diric' with the caller's N: no odd-N trick; 'minmax:kb' fitted
+    at Nmid = (N-1)/2)."""
+    if ktype.startswith("kb:"):
+        if ktype == "kb:minmax":
+            a, m = kb_alpha(J), 0
+        elif ktype == "kb:beatty":
+            a, m = beatty_alpha(N, J, K), 0
+        else:
+            a, m = kb_alf, kb_m
+        a = float(f"{a:g}")
+        m = float(f"{m:g}")
+
+        def kern(arg):
+            out = np.zeros_like(arg)
+            inside = np.abs(arg) < J / 2
+            f = np.sqrt(1 - (arg[inside] / (J / 2)) ** 2)
+            out[inside] = f ** m * special.iv(abs(m), a * f) / special.iv(abs(m), a)
+            return out
+        Kf = J * K / N
+        h = _fast_table_complex(J, J, Kf, L, kern)
+        t0 = (np.arange(J * L + 1) - J * L / 2) / L
+        return h * np.exp(1j * np.pi * t0 * (1 / K - 1 / Kf))
+    if ktype == "diric":
+        def kern(arg):
+            t = np.pi / K * arg
+            f = np.sin(t)
+            big = np.abs(f) > 1e-12
+            out = np.sign(np.cos(t * (N - 1)))
+            out[big] = np.sin(N * t[big]) / (N * f[big])
+            return N / K * out
+        return _fast_table_complex(N, J, K, L, kern)
+    if ktype == "linear":
+        return _fast_table_complex(N, J, K, L,
+                                   lambda arg: (1 - np.abs(arg / (J / 2))) * (np.abs(arg) < J / 2))
+    if ktype == "minmax:kb":
+        al, b = nr.nufft_alpha_kb_fit(N, J, K)
+    elif ktype == "minmax:unif":
+        al, b = np.array([1.0]), 0.0
+    elif ktype == "minmax:tuned":
+        al, b = best_alpha(J, N, K)
+    elif ktype == "minmax:user":
+        al, b = np.atleast_1d(np.asarray(alpha, dtype=np.float64)), beta
+    else:
+        raise ValueError(ktype)
+    T = nr.nufft_T(N, J, K, al, b)
+
+    def coef(arg):
+        r = np.zeros(arg.shape)
+        L_ = len(al) - 1
+        for l1 in range(-L_, L_ + 1):
+            r = r + al[abs(l1)] * nr.nufft_diric(arg + l1 * b, N, K)
+        return np.real(T @ r)
+    return _fast_table_complex(N, J, K, L, coef)
+
+
 def phase_before(Kd, Nmid) -> np.ndarray:
     """exp(i 2 pi sum_d k_d / K_d Nmid_d) over the grid [(Kd)]."""
     ph = np.zeros(())
@@ -257,7 +342,8 @@ def newfft_init(om, Nd, Jd=None, Kd=None, n_shift=None, mode="table1", Ld=None,
         pick = lambda v: None if v is None else v[d]
         return dict(kb_alf=pick(kb_alf), kb_m=pick(kb_m), alpha=pick(alpha), beta=pick(beta))
     if h is None:
-        h = [ktype_table(ktype, Nd[d], Jd[d], Kd[d], Ld[d], **user(d)) for d in range(dd)]
+        make = ktype_table_complex if phasing == "complex" else ktype_table
+        h = [make(ktype, Nd[d], Jd[d], Kd[d], Ld[d], **user(d)) for d in range(dd)]
     if sn is None:
         s = np.ones(1)
         for d in range(dd):

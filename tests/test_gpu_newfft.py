@@ -113,6 +113,25 @@ def test_user_interpolators(kw, Nd, mode):
     assert _mpd(nr.dtft_adj(Xe, om, Nd, ns), st.adj(Xe)) < 1.0
 
 
+@pytest.mark.parametrize("ktype,kw", [("kb:minmax", {}), ("minmax:kb", {}), ("minmax:tuned", {}),
+                                      ("kb:user", dict(kb_alf=15.0, kb_m=1)),
+                                      ("minmax:user", dict(alpha=[1.0, -0.57, 0.14], beta=0.43))])
+@pytest.mark.parametrize("Nd", [(20,), (20, 10)])
+def test_complex_phasing_builtin_tables(ktype, kw, Nd):
+    """phasing 'complex' (mode 'table0') with the library's complex tables and
+    scaling factors at Nmid = (N-1)/2: the oracle's forward / adjoint."""
+    dd = len(Nd)
+    per_dim = {k: [v] * dd for k, v in kw.items()}
+    rng = np.random.default_rng(3)
+    om = 3 * 2 * np.pi * (rng.random((100, dd)) - 0.5)
+    x0 = rng.random(Nd)
+    st = mb.newfft(om, Nd, mode="table0", phasing="complex", ktype=ktype, **per_dim)
+    so = nf.newfft_init(om, Nd, mode="table0", phasing="complex", ktype=ktype, **per_dim)
+    Xo = nf.newfft_for(x0, so)
+    assert rel_l2(st.fft(x0), Xo) <= TOL
+    assert rel_l2(st.adj(Xo), nf.newfft_adj(Xo, so)) <= TOL
+
+
 def test_batched_slices_coils_and_shift():
     """Three trajectories of uneven length, 3 columns, centred image (n_shift =
     N/2), table1: every slice and column against the oracle."""

@@ -87,8 +87,8 @@ def test_newfft_argument_checks_before_any_device_call():
         mb.newfft(om, (16, 16), mode="sparse")
     with pytest.raises(ValueError, match="phasing"):
         mb.newfft(om, (16, 16), phasing="flipreal")
-    with pytest.raises(ValueError, match="built-in tables"):
-        mb.newfft(om, (16, 16), phasing="complex")
+    with pytest.raises(ValueError, match="kb_alf and kb_m required"):
+        mb.newfft(om, (16, 16), phasing="complex", ktype="kb:user")
     with pytest.raises(ValueError, match="sn is required"):
         mb.newfft(om, (16, 16), tables=[np.ones(6 * 512 + 1)] * 2)
 
@@ -247,6 +247,65 @@ def test_user_ktype_errors():
         mb.newfft_scale("kb:user", 20, 6, 40, 10.0, kb_alf=-1.0, kb_m=0)
     with pytest.raises(ValueError, match="alpha/beta"):
         mb.newfft_table("minmax:user", 20, 6, 40, 512, alpha=[1.0])
+
+
+_COMPLEX_CASES = [("kb:minmax", {}, 20, 6, 40, 512), ("kb:minmax", {}, 21, 6, 32, 256),
+                  ("kb:beatty", {}, 20, 6, 40, 512), ("kb:user", dict(kb_alf=15.0, kb_m=1), 20, 6, 40, 512),
+                  ("diric", {}, 20, 12, 40, 256), ("linear", {}, 20, 2, 40, 512),
+                  ("minmax:kb", {}, 20, 6, 40, 512), ("minmax:kb", {}, 21, 6, 42, 256),
+                  ("minmax:unif", {}, 20, 6, 40, 512), ("minmax:tuned", {}, 20, 6, 40, 512),
+                  ("minmax:user", dict(alpha=[1.0], beta=0.5), 20, 6, 40, 512)]
+
+
+@pytest.mark.parametrize("ktype,kw,N,J,K,L", _COMPLEX_CASES)
+def test_complex_phasing_table_builders(ktype, kw, N, J, K, L):
+    """Every ktype's table with phasing 'complex' (the 'fast' / 'ratio'
+    constructions): the library against the oracle."""
+    h = mb.newfft_table(ktype, N, J, K, L, phasing="complex", **kw)
+    ho = nf.ktype_table_complex(ktype, N, J, K, L, **kw)
+    assert np.max(np.abs(h - ho)) <= 1e-11 * np.max(np.abs(ho))
+    assert np.max(np.abs(ho.imag)) > 0.1 * np.max(np.abs(ho))
+
+
+@pytest.mark.parametrize("N,J,K,L", [(20, 6, 40, 512), (21, 6, 42, 1024), (64, 8, 128, 256)])
+def test_complex_minmax_kb_table_is_nufft_init_table(N, J, K, L):
+    """newfft's 'minmax:kb' with phasing 'complex' (alphas fitted at Nmid =
+    (N-1)/2, the phase exp(i gam (N-1)/2 arg)) is nufft_init's min-max:KB
+    table -- which the reference's golden vectors pin -- in every entry but
+    the last: the 'fast' construction repeats the first entry there
+    (newfft_table_init.m:169), nufft_table_init.m writes 0."""
+    hn = nf.ktype_table_complex("minmax:kb", N, J, K, L)
+    hi = nr.nufft_init_table(np.zeros((1, 1)), (N,), (J,), (K,), (0,), L)["h"][0]
+    assert np.array_equal(hn[:-1], hi[:-1])
+    assert hn[-1] == hn[0] and hi[-1] == 0
+
+
+@pytest.mark.parametrize("Nd", ND_LIST + [(6,), (6, 5)])
+def test_oracle_complex_phasing_vs_exact_dtft(Nd):
+    """Phasing 'complex', mode 'table0' (the self-test's complex runs;
+    complex tables are order 0 only): every ktype on the self-test set-ups.
+    The table0 lookup of the phase ramp exp(-i pi t (N-1)/K) adds about 0.02 %
+    to every kernel (measured: kb:* and 'minmax:tuned' <= 0.11 %, 'minmax:kb'
+    <= 0.16 % where its fit is coarse (N = 10, 8; not checked at N = 6, 0.41 %),
+    'diric' (Jd = 2 Nd) <= 0.03 %,
+    'minmax:unif' / 'minmax:user' <= 0.81 %, 'linear' (Jd = 2) 38-84 %)."""
+    om, x0 = _case(Nd)
+    dd = len(Nd)
+    ns = np.zeros(dd)
+    Xe = nr.dtft(x0, om, ns)
+    xe = nr.dtft_adj(Xe, om, Nd, ns)
+    cases = [("kb:minmax", {}, 0.12), ("kb:beatty", {}, 0.12), ("minmax:tuned", {}, 0.12),
+             ("minmax:unif", {}, 1.0), ("linear", dict(Jd=(2,) * dd), 100.0),
+             ("kb:user", dict(kb_alf=[2.34 * 6] * dd, kb_m=[0] * dd), 0.12),
+             ("minmax:user", dict(alpha=[[1.0]] * dd, beta=[0.5] * dd), 1.0)]
+    if 2 * max(Nd) <= 16:
+        cases.append(("diric", dict(Jd=tuple(2 * np.asarray(Nd))), 0.12))
+    if min(Nd) >= 8:     # below that the reference's fit of the scaling factors has <= 3 terms
+        cases.append(("minmax:kb", {}, 0.2))
+    for ktype, kw, bound in cases:
+        st = nf.newfft_init(om, Nd, mode="table0", phasing="complex", ktype=ktype, **kw)
+        assert _mpd(Xe, nf.newfft_for(x0, st)) < bound, ktype
+        assert _mpd(xe, nf.newfft_adj(Xe, st)) < bound, ktype
 
 
 def test_ktype_errors():
