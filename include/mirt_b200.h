@@ -394,6 +394,30 @@ int mirt_nufft_config(mirt_nufft *p, int32_t *out, int32_t n);
 
 int mirt_nufft_destroy(mirt_nufft *p);
 
+/* nufft_init's other interpolators in table mode (host FP64), for
+ * nufft_init(om, Nd, Jd, Kd, n_shift, 'table', L, ktype, ...): the 1D table
+ * of nufft/nufft_table_init.m:100-116 (J*L+1 complex values split into
+ * h_re / h_im: nufft_init's sparse interpolator read by the 'fast'
+ * construction, the last entry 0) and the 1D factors whose outer product is
+ * st.sn (nufft/nufft_init.m:210-230, conjugated as its st.sn(:) * tmp'
+ * does).  ktype:
+ *   MIRT_KTYPE_KB_MINMAX    'kaiser' (alpha = 2.34 J, m = 0)
+ *   MIRT_KTYPE_KB_USER      'kaiser', alpha, m (kb_alf, integer kb_m)
+ *   MIRT_KTYPE_MINMAX_KB    'minmax:kb' (the tables of mirt_nufft_create)
+ *   MIRT_KTYPE_MINMAX_TUNED 'minmax:tuned'
+ *   MIRT_KTYPE_MINMAX_USER  'minmax:user' (alpha[0 .. nalpha-1], beta)
+ *   MIRT_KTYPE_MINMAX_UNIF  'uniform' (alpha = 1, beta = 0)
+ *   MIRT_KTYPE_LINEAR       'linear' (scale 1 / nufft_interp_zn(0, ...))
+ * A NUFFT with these is mirt_newfft_create with phasing 'complex', mode
+ * 'table0' and the tables and st.sn given (nufft.m / nufft_adj.m apply only
+ * the n_shift phase around the same gather). */
+int mirt_nufft_ktype_table(int32_t ktype, int32_t N, int32_t J, int32_t K, int32_t L,
+	double kb_alf, int32_t kb_m, const double *alpha, int32_t nalpha, double beta,
+	double *h_re, double *h_im);
+int mirt_nufft_ktype_scale(int32_t ktype, int32_t N, int32_t J, int32_t K, double kb_alf,
+	int32_t kb_m, const double *alpha, int32_t nalpha, double beta,
+	double *sn_re, double *sn_im);
+
 /* ------------------------------------------------------------------------
  * 3a. newfft in table mode: st = newfft(om, Nd, 'Jd', Jd, 'Kd', Kd,
  *     'n_shift', n_shift, 'mode', 'table0' | 'table1', 'oversample', Ld,

@@ -17,7 +17,7 @@ from .mex import (MexError, interp1_table_adj_mex, interp1_table_mex, interp2_ta
                   interp4_table_adj_mex, interp4_table_mex)
 from .nufft import (InterpPlan, NewfftPlan, NufftPlan, minmax_kb_scale, minmax_kb_table, newfft,
                     newfft_kb_scale, newfft_kb_table, newfft_scale, newfft_table, nufft,
-                    nufft_adj, nufft_init)
+                    nufft_adj, nufft_init, nufft_scale, nufft_table)
 from .dcf import dcf_jackson, dcf_pipe, ir_mri_density_comp
 from .learned_dcf import DcfMLP, LearnedDCF, dcf_features
 
@@ -27,7 +27,7 @@ __all__ = [
     "interp1_table_adj_mex", "interp2_table_adj_mex", "interp3_table_adj_mex",
     "interp4_table_adj_mex",
     "InterpPlan", "NufftPlan", "minmax_kb_table", "minmax_kb_scale",
-    "nufft_init", "nufft", "nufft_adj",
+    "nufft_init", "nufft", "nufft_adj", "nufft_table", "nufft_scale",
     "NewfftPlan", "newfft", "newfft_kb_table", "newfft_kb_scale", "newfft_table", "newfft_scale",
     "dcf_pipe", "dcf_jackson", "ir_mri_density_comp",
     "dcf_features", "DcfMLP", "LearnedDCF",

@@ -125,6 +125,10 @@ _SIGS = {
     "mirt_newfft_kb_scale": ([_i32, _i32, _i32, C.c_double, _dp], C.c_int),
     "mirt_newfft_ktype_table": ([_i32, _i32, _i32, _i32, _i32, _dp], C.c_int),
     "mirt_newfft_ktype_scale": ([_i32, _i32, _i32, _i32, C.c_double, _dp], C.c_int),
+    "mirt_nufft_ktype_table": ([_i32, _i32, _i32, _i32, _i32, C.c_double, _i32, _dp, _i32,
+                                C.c_double, _dp, _dp], C.c_int),
+    "mirt_nufft_ktype_scale": ([_i32, _i32, _i32, _i32, C.c_double, _i32, _dp, _i32,
+                                C.c_double, _dp, _dp], C.c_int),
     "mirt_newfft_table_complex": ([_i32, _i32, _i32, _i32, _i32, C.c_double, _i32, _dp, _i32,
                                    C.c_double, _dp, _dp], C.c_int),
     "mirt_newfft_kb_user_table": ([_i32, _i32, C.c_double, _i32, _dp], C.c_int),

@@ -54,6 +54,12 @@ bool minmax_table_complex_ab(int N, int J, int K, int L, const std::vector<doubl
                              double beta, std::vector<std::complex<double>> &h);
 void diric_table_complex(int N, int J, int K, int L, std::vector<std::complex<double>> &h);
 void linear_table_complex(int N, int J, int K, int L, std::vector<std::complex<double>> &h);
+bool nufft_table_ktype(int kt, int N, int J, int K, int L, double kb_alf, int kb_m,
+                       const std::vector<double> &alpha, double beta,
+                       std::vector<std::complex<double>> &h);
+bool nufft_scale_ktype(int kt, int N, int J, int K, double kb_alf, int kb_m,
+                       const std::vector<double> &alpha, double beta,
+                       std::vector<std::complex<double>> &sn);
 std::vector<double> kb_user_scale(int N, int J, int K, double nmid, double alpha, int m);
 int plan4_create(mirt_interp_plan **out, const int *K, const int *J, const int *L,
                  const double *const *h_re, const double *const *h_im, int order,
@@ -2621,6 +2627,72 @@ int mirt_newfft_table_complex(int32_t ktype, int32_t N, int32_t J, int32_t K, in
   for (size_t i = 0; i < t.size(); i++) {
     h_re[i] = t[i].real();
     h_im[i] = t[i].imag();
+  }
+  return MIRT_OK;
+}
+
+namespace {
+// the argument checks of mirt_nufft_ktype_table / _scale
+int nufft_ktype_args(int32_t ktype, int32_t N, int32_t J, int32_t K, double kb_alf, int32_t kb_m,
+                     const double *alpha, int32_t nalpha, std::vector<double> &al) {
+  if (N < 1 || J < 1 || J > MIRT_JMAX || K < 1)
+    return fail(MIRT_ERR_ARG, "N, K must be positive, J in 1..16");
+  switch (ktype) {
+    case MIRT_KTYPE_KB_MINMAX:
+    case MIRT_KTYPE_LINEAR:
+      break;
+    case MIRT_KTYPE_KB_USER:
+      if (!(kb_alf >= 0) || kb_m < 0 || kb_m > 32)
+        return fail(MIRT_ERR_ARG, "kaiser needs alpha >= 0 and an integer m in 0..32");
+      break;
+    case MIRT_KTYPE_MINMAX_KB:
+    case MIRT_KTYPE_MINMAX_UNIF:
+    case MIRT_KTYPE_MINMAX_TUNED:
+    case MIRT_KTYPE_MINMAX_USER:
+      if (N > K) return fail(MIRT_ERR_ARG, "N > K");
+      if (ktype == MIRT_KTYPE_MINMAX_USER) {
+        if (!alpha || nalpha < 1) return fail(MIRT_ERR_ARG, "user must provide alpha/beta");
+        al.assign(alpha, alpha + nalpha);
+      }
+      break;
+    default: return fail(MIRT_ERR_ARG, "not an interpolator of nufft_init");
+  }
+  return MIRT_OK;
+}
+}  // namespace
+
+int mirt_nufft_ktype_table(int32_t ktype, int32_t N, int32_t J, int32_t K, int32_t L,
+                           double kb_alf, int32_t kb_m, const double *alpha, int32_t nalpha,
+                           double beta, double *h_re, double *h_im) {
+  if (!h_re || !h_im) return fail(MIRT_ERR_ARG, "output pointer is NULL");
+  if (L < 1) return fail(MIRT_ERR_ARG, "L must be positive");
+  std::vector<double> al;
+  int rc = nufft_ktype_args(ktype, N, J, K, kb_alf, kb_m, alpha, nalpha, al);
+  if (rc) return rc;
+  std::vector<std::complex<double>> t;
+  if (!nufft_table_ktype(ktype, N, J, K, L, kb_alf, kb_m, al, beta, t))
+    return fail(MIRT_ERR_ARG, ktype == MIRT_KTYPE_MINMAX_TUNED ? "unknown J,K/N"
+                                                                : "singular min-max matrix");
+  for (size_t i = 0; i < t.size(); i++) {
+    h_re[i] = t[i].real();
+    h_im[i] = t[i].imag();
+  }
+  return MIRT_OK;
+}
+
+int mirt_nufft_ktype_scale(int32_t ktype, int32_t N, int32_t J, int32_t K, double kb_alf,
+                           int32_t kb_m, const double *alpha, int32_t nalpha, double beta,
+                           double *sn_re, double *sn_im) {
+  if (!sn_re || !sn_im) return fail(MIRT_ERR_ARG, "output pointer is NULL");
+  std::vector<double> al;
+  int rc = nufft_ktype_args(ktype, N, J, K, kb_alf, kb_m, alpha, nalpha, al);
+  if (rc) return rc;
+  std::vector<std::complex<double>> s;
+  if (!nufft_scale_ktype(ktype, N, J, K, kb_alf, kb_m, al, beta, s))
+    return fail(MIRT_ERR_ARG, "unknown J,K/N");
+  for (int n = 0; n < N; n++) {
+    sn_re[n] = s[n].real();
+    sn_im[n] = s[n].imag();
   }
   return MIRT_OK;
 }

@@ -634,6 +634,98 @@ void linear_table_complex(int N, int J, int K, int L, std::vector<cd> &h) {
   }, h);
 }
 
+// ---------------------------------------------------------------------------
+// nufft_init's interpolators in table mode
+// ---------------------------------------------------------------------------
+// nufft/nufft_table_init.m:100-116 reads nufft_init's sparse interpolator
+// (entries conj(exp(i gam (N-1)/2 arg) c), nufft/nufft_init.m:262-290) at
+// t1 = J/2 - 1 + l/L with the 'fast' construction, columns J .. 1, the last
+// entry 0.  kt: 0 'kaiser' (alpha = 2.34 J, m = 0: kaiser_bessel('inline', J),
+// nufft/kaiser_bessel.m:68-69), 7 'kaiser' with the caller's alpha and m,
+// 3 'minmax:kb', 4 'uniform', 5 'minmax:tuned', 8 'minmax:user', 6 'linear'.
+bool nufft_table_ktype(int kt, int N, int J, int K, int L, double kb_alf, int kb_m,
+                       const std::vector<double> &alpha, double beta, std::vector<cd> &h) {
+  if (kt == 0 || kt == 7) {
+    char buf[64];
+    std::snprintf(buf, sizeof buf, "%g", kt == 0 ? 2.34 * J : kb_alf);
+    const double a = std::atof(buf);
+    const int m = kt == 0 ? 0 : kb_m;
+    const double den = bessel_in(m, a);
+    table_fast_complex((double)N, J, (double)K, L, [&](const double *arg, double *c) {
+      for (int j = 0; j < J; j++) {
+        const double u = arg[j] / (J / 2.0);
+        c[j] = std::fabs(arg[j]) < J / 2.0
+                   ? std::pow(std::sqrt(1 - u * u), m) * bessel_in(m, a * std::sqrt(1 - u * u)) / den
+                   : 0.0;
+      }
+    }, h);
+  } else if (kt == 6) {
+    linear_table_complex(N, J, K, L, h);
+  } else {
+    std::vector<double> al{1.0};
+    double b = 0.0;
+    if (kt == 3) {
+      alpha_kb_fit(N, J, K, al, b);
+    } else if (kt == 5) {
+      if (!best_alpha(J, N, K, al, b)) return false;
+    } else if (kt == 8) {
+      al = alpha;
+      b = beta;
+    } else if (kt != 4) {
+      return false;
+    }
+    if (!minmax_table_complex_ab(N, J, K, L, al, b, h)) return false;
+  }
+  h.back() = 0;
+  return true;
+}
+
+// the 1D factors whose outer product is nufft_init's st.sn (st.sn(:) *
+// tmp', nufft/nufft_init.m:210-230, a conjugate transpose): conj of
+// 1 / KB-FT((n - (N-1)/2) / K) for 'kaiser', of nufft_scale(N, K, alpha,
+// beta) for the min-max kinds, of 1 / nufft_interp_zn(0, N, J, K, kernel)
+// (nufft/private/nufft_interp_zn.m) for 'linear'
+bool nufft_scale_ktype(int kt, int N, int J, int K, double kb_alf, int kb_m,
+                       const std::vector<double> &alpha, double beta, std::vector<cd> &sn) {
+  sn.assign(N, cd(0, 0));
+  const double nmid = (N - 1) / 2.0;
+  if (kt == 0 || kt == 7) {
+    const std::vector<double> s =
+        kb_user_scale(N, J, K, nmid, kt == 0 ? 2.34 * J : kb_alf, kt == 0 ? 0 : kb_m);
+    for (int n = 0; n < N; n++) sn[n] = s[n];
+    return true;
+  }
+  if (kt == 6) {
+    const double gam = 2 * M_PI / K;
+    const int j0 = (J % 2 == 0) ? -J / 2 + 1 : -(J - 1) / 2;
+    for (int n = 0; n < N; n++) {
+      cd zn(0, 0);
+      for (int jj = 0; jj < J; jj++) {
+        const double jarg = -(double)(j0 + jj);
+        const double f = std::fabs(jarg) < J / 2.0 ? 1 - std::fabs(jarg / (J / 2.0)) : 0.0;
+        zn += f * std::exp(cd(0, gam * jarg * (n - nmid)));
+      }
+      sn[n] = std::conj(1.0 / zn);
+    }
+    return true;
+  }
+  std::vector<double> al{1.0};
+  double b = 0.0;
+  if (kt == 3) {
+    alpha_kb_fit(N, J, K, al, b);
+  } else if (kt == 5) {
+    if (!best_alpha(J, N, K, al, b)) return false;
+  } else if (kt == 8) {
+    al = alpha;
+    b = beta;
+  } else if (kt != 4) {
+    return false;
+  }
+  const std::vector<cd> s = scale1(N, K, al, b);
+  for (int n = 0; n < N; n++) sn[n] = std::conj(s[n]);
+  return true;
+}
+
 // Table of ktype 'diric' with phasing 'real' (nufft/newfft.m:256-266,
 // nufft/nufft_diric.m:31-36): the kernel N' / K diric(k, N', K) with the odd
 // N' = 2 floor((K + 1) / 2) - 1 and the true Dirichlet function

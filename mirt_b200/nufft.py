@@ -577,23 +577,102 @@ def newfft(om, Nd, **kw) -> NewfftPlan:
 # ---------------------------------------------------------------------------
 # MATLAB-style interface
 # ---------------------------------------------------------------------------
-def nufft_init(om, Nd, Jd, Kd, n_shift=None, *args):
-    """st = nufft_init(om, Nd, Jd, Kd, n_shift, 'table', Ld, 'minmax:kb').
+_NUFFT_KTYPES = {"kaiser": 0, "minmax:kb": 3, "uniform": 4, "minmax:tuned": 5, "linear": 6,
+                 "minmax:user": 8}
 
-    Only the table mode with the min-max:KB interpolator (the reference's
-    default for 'table', nufft/nufft_init.m:93-95) is provided.
+
+def _nufft_ktype_call(fn, ktype, N, J, K, L, params, out_len):
+    code = _NUFFT_KTYPES.get(ktype)
+    if code is None:
+        raise ValueError(f"ktype must be one of {sorted(_NUFFT_KTYPES)}")
+    kb_alf, kb_m, al, beta = 0.0, 0, None, 0.0
+    if ktype == "kaiser" and params:
+        code, kb_alf, kb_m = 7, float(params[0]), int(params[1])
+        if float(params[1]) != kb_m:
+            raise ValueError("kaiser: m must be an integer")
+    elif ktype == "minmax:user":
+        if len(params) != 2:
+            raise ValueError("user must provide alpha/beta")
+        al = np.ascontiguousarray(np.atleast_1d(np.asarray(params[0], dtype=np.float64)))
+        beta = float(params[1])
+    re, im = np.empty(out_len), np.empty(out_len)
+    args = [code, int(N), int(J), int(K)] + ([int(L)] if L is not None else [])
+    check(fn(*args, kb_alf, kb_m, None if al is None else al.ctypes.data_as(_dp),
+             0 if al is None else al.size, beta, re.ctypes.data_as(_dp), im.ctypes.data_as(_dp)))
+    return re + 1j * im
+
+
+def nufft_table(ktype, N, J, K, L, *params) -> np.ndarray:
+    """1D table of nufft_init(..., 'table', L, ktype, params...) (see
+    mirt_nufft_ktype_table): [J*L+1] complex.  params: 'kaiser' [alpha, m]
+    of this dimension, 'minmax:user' alpha (list), beta."""
+    return _nufft_ktype_call(load().mirt_nufft_ktype_table, ktype, N, J, K, L, params,
+                             int(J) * int(L) + 1)
+
+
+def nufft_scale(ktype, N, J, K, *params) -> np.ndarray:
+    """The 1D factors whose outer product is nufft_init's st.sn, [N] complex."""
+    return _nufft_ktype_call(load().mirt_nufft_ktype_scale, ktype, N, J, K, None, params, int(N))
+
+
+def nufft_init(om, Nd, Jd, Kd, n_shift=None, *args, ncol=1, slice_moff=None, stream=None):
+    """st = nufft_init(om, Nd, Jd, Kd, n_shift, 'table', Ld, ktype, ...).
+
+    ktype 'minmax:kb' (the reference's default, nufft/nufft_init.m:83-85) runs
+    the library's NUFFT plan with its fused FFT passes; 'kaiser' [, alpha_list,
+    m_list], 'minmax:tuned', 'minmax:user', alpha_list, beta_list, 'uniform' and
+    'linear' build nufft_init's tables and scaling factors in the library and
+    run them through the newfft plan with phasing 'complex', which is the same
+    nufft / nufft_adj (only the n_shift phase around the gather).  As
+    nufft_table_init.m:86-97 requires, 'kaiser' with parameters must use the
+    same alpha and m in every dimension.
     """
     args = list(args)
     Ld = 1024
     if args and args[0] == "table":
         Ld = args[1] if len(args) > 1 else Ld
-        ktype = args[2] if len(args) > 2 else "minmax:kb"
+        rest = args[2:]
     else:
-        ktype = args[0] if args else "minmax:kb"
-    if ktype != "minmax:kb":
-        raise ValueError(f"only 'minmax:kb' tables are provided, not {ktype!r}")
-    ncol = 1
-    return NufftPlan(om, Nd, Jd, Kd, n_shift=n_shift, Ld=Ld, ncol=ncol)
+        rest = args
+    ktype = rest[0] if rest else "minmax:kb"
+    params = rest[1:]
+    Nd = _i32(Nd)
+    D = len(Nd)
+    Jd, Kd = _i32(Jd), _i32(Kd)
+    Ld = _i32(Ld if np.ndim(Ld) else [Ld] * D)
+    if ktype == "minmax:kb":
+        if params:
+            raise ValueError("minmax:kb takes no parameters")
+        return NufftPlan(om, Nd, Jd, Kd, n_shift=n_shift, Ld=Ld, ncol=ncol,
+                         slice_moff=slice_moff, stream=stream)
+    if ktype not in _NUFFT_KTYPES:
+        raise ValueError(f"unknown kernel type {ktype!r}")
+    if ktype == "kaiser" and params:
+        if len(params) != 2:
+            raise ValueError("kaiser should have no arguments, or both alpha and m")
+        a, m = np.atleast_1d(params[0]), np.atleast_1d(params[1])
+        if len(a) != D or len(m) != D:
+            raise ValueError(f"#alpha={len(a)} #m={len(m)} vs dd={D}")
+        if np.any(a != a[0]) or np.any(m != m[0]):
+            raise ValueError("table based needs identical interpolator for each dimension")
+        per_dim = [(a[d], m[d]) for d in range(D)]
+    elif ktype == "minmax:user":
+        if len(params) != 2:
+            raise ValueError("user must provide alpha/beta")
+        if len(params[0]) != D or len(params[1]) != D:
+            raise ValueError("alpha/beta size mismatch")
+        per_dim = [(params[0][d], params[1][d]) for d in range(D)]
+    else:
+        if params:
+            raise ValueError(f"{ktype} takes no parameters")
+        per_dim = [()] * D
+    tables = [nufft_table(ktype, Nd[d], Jd[d], Kd[d], Ld[d], *per_dim[d]) for d in range(D)]
+    s = np.ones(1, dtype=np.complex128)
+    for d in range(D):
+        s = np.outer(s.ravel(order="F"), nufft_scale(ktype, Nd[d], Jd[d], Kd[d], *per_dim[d]))
+    return NewfftPlan(om, Nd, Jd, Kd, n_shift=n_shift, mode="table0", Ld=Ld, phasing="complex",
+                      tables=tables, sn=s.ravel(order="F"), ncol=ncol, slice_moff=slice_moff,
+                      stream=stream)
 
 
 def _to_device_image(x, D, ncol):

@@ -211,6 +211,91 @@ def nufft_init_table(om, Nd, Jd, Kd, n_shift, Ld) -> dict:
     return st
 
 
+def nufft_ktype_table(ktype, N, J, K, L, *params):
+    """1D table of nufft_init(..., 'table', L, ktype, params...): nufft_init's
+    sparse interpolator (entries conj(exp(i gam (N-1)/2 arg) c),
+    nufft_init.m:262-290) read at t1 = J/2 - 1 + l/L by the 'fast'
+    construction of nufft_table_init.m:100-116, the last entry 0.  'kaiser'
+    [alpha, m]: the KB kernel (alpha 2.34 J, m 0 by default; both printed with
+    %g into the inline kernel); 'linear'; the min-max kinds 'minmax:kb',
+    'minmax:tuned', 'minmax:user' (alpha list, beta), 'uniform'."""
+    from oracle import newfft_ref as nf
+    if ktype == "kaiser":
+        a, m = params if params else (2.34 * J, 0)
+        a, m = float(f"{a:g}"), float(f"{m:g}")
+
+        def coef(arg):
+            out = np.zeros_like(arg)
+            inside = np.abs(arg) < J / 2
+            f = np.sqrt(1 - (arg[inside] / (J / 2)) ** 2)
+            out[inside] = f ** m * special.iv(abs(m), a * f) / special.iv(abs(m), a)
+            return out
+    elif ktype == "linear":
+        coef = lambda arg: (1 - np.abs(arg / (J / 2))) * (np.abs(arg) < J / 2)
+    else:
+        al, b = _nufft_minmax_params(ktype, N, J, K, params)
+        T = nufft_T(N, J, K, al, b)
+
+        def coef(arg):
+            r = np.zeros(arg.shape)
+            for l1 in range(-(len(al) - 1), len(al)):
+                r = r + al[abs(l1)] * nufft_diric(arg + l1 * b, N, K)
+            return np.real(T @ r)
+    h = nf._fast_table_complex(N, J, K, L, coef)
+    h[-1] = 0
+    return h
+
+
+def _nufft_minmax_params(ktype, N, J, K, params):
+    from oracle import newfft_ref as nf
+    if ktype == "minmax:kb":
+        return nufft_alpha_kb_fit(N, J, K)
+    if ktype == "minmax:tuned":
+        return nf.best_alpha(J, N, K)
+    if ktype == "minmax:user":
+        return np.atleast_1d(np.asarray(params[0], dtype=np.float64)), float(params[1])
+    if ktype == "uniform":
+        return np.array([1.0]), 0.0
+    raise ValueError(ktype)
+
+
+def nufft_ktype_scale(ktype, N, J, K, *params):
+    """The 1D factors of nufft_init's st.sn (conj, as st.sn(:) * tmp' makes
+    them; nufft_init.m:210-230): 1 / kaiser_bessel_ft((n - (N-1)/2) / K) for
+    'kaiser', nufft_scale for the min-max kinds, 1 / nufft_interp_zn(0, ...)
+    (nufft/private/nufft_interp_zn.m) for 'linear'."""
+    nc = np.arange(N) - (N - 1) / 2
+    if ktype == "kaiser":
+        a, m = params if params else (2.34 * J, 0)
+        tmp = 1.0 / kaiser_bessel_ft(nc / K, J, a, float(m), 1)
+    elif ktype == "linear":
+        jlist = np.arange(-J // 2 + 1, J // 2 + 1) if J % 2 == 0 else np.arange(-(J - 1) // 2, (J - 1) // 2 + 1)
+        jarg = -jlist[None, :].astype(np.float64)
+        F = (1 - np.abs(jarg / (J / 2))) * (np.abs(jarg) < J / 2)
+        zn = np.sum(F * np.exp(1j * (2 * np.pi / K) * jarg * nc[:, None]), axis=1)
+        tmp = 1.0 / zn
+    else:
+        al, b = _nufft_minmax_params(ktype, N, J, K, params)
+        tmp = nufft_scale1(N, K, al, b)
+    return np.conj(tmp)
+
+
+def nufft_init_table_ktype(om, Nd, Jd, Kd, n_shift, Ld, ktype, *params) -> dict:
+    """st = nufft_init(om, Nd, Jd, Kd, n_shift, 'table', Ld, ktype, params...);
+    per-dimension params ('kaiser': alpha_list, m_list; 'minmax:user':
+    alpha_list, beta_list)."""
+    st = nufft_init_table(om, Nd, Jd, Kd, n_shift, Ld)
+    dd = len(Nd)
+    pd = [tuple(p[d] for p in params) for d in range(dd)] if params else [()] * dd
+    st["h"] = [nufft_ktype_table(ktype, Nd[d], Jd[d], Kd[d], st["Ld"][d], *pd[d])
+               for d in range(dd)]
+    sn = np.ones(1, dtype=np.complex128)
+    for d in range(dd):
+        sn = np.outer(sn.ravel(order='F'), nufft_ktype_scale(ktype, Nd[d], Jd[d], Kd[d], *pd[d]))
+    st["sn"] = sn.reshape(tuple(Nd), order='F')
+    return st
+
+
 def nufft(x, st, interp):
     """X = nufft(x, st); ``interp(Xk_flat_F, st) -> X [M]`` supplies the table gather."""
     Nd, Kd = st['Nd'], st['Kd']

@@ -209,3 +209,24 @@ def test_host_calls_pipelined_by_slice_chunks(C, nslice):
         assert rel_l2(a[sl, C - 1], nr.nufft(x[s, :, :, C - 1].T, st_o, fw)) <= FWD_TOL
         assert rel_l2(y[s, :, :, 0].T, nr.nufft_adj(b[sl, 0], st_o, ad)) <= ADJ_TOL
     plan.close()
+
+
+@pytest.mark.parametrize("ktype,params", [("kaiser", ()), ("kaiser", ([15.0, 15.0], [1, 1])),
+                                          ("minmax:tuned", ()), ("uniform", ()), ("linear", ())])
+def test_nufft_init_other_interpolators(ktype, params):
+    """nufft_init(om, Nd, Jd, Kd, n_shift, 'table', L, ktype, ...) for the
+    interpolators other than 'minmax:kb': the library's tables and scaling
+    factors on the newfft plan with phasing 'complex' against the oracle's
+    nufft / nufft_adj with its own restatement of them."""
+    rng = np.random.default_rng(17)
+    Nd, Jd, Kd = (32, 24), (6, 5), (64, 48)
+    om = rng.uniform(-np.pi, np.pi, (600, 2))
+    ns = np.array([16.0, 12.0])
+    st = mb.nufft_init(om, Nd, Jd, Kd, ns, "table", 2 ** 10, ktype, *params)
+    so = nr.nufft_init_table_ktype(om, Nd, Jd, Kd, ns, 2 ** 10, ktype, *params)
+    fw, ad = _oracle_pair(so)
+    x = rng.standard_normal(Nd) + 1j * rng.standard_normal(Nd)
+    X_o = nr.nufft(x, so, fw)
+    # the newfft plan's tolerance (1e-5 each way, its FP32 FFT included)
+    assert rel_l2(mb.nufft(x, st), X_o) <= 1e-5
+    assert rel_l2(mb.nufft_adj(X_o, st), nr.nufft_adj(X_o, so, ad)) <= 1e-5
