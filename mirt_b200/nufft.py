@@ -472,6 +472,31 @@ def newfft_scale(ktype: str, N: int, J: int, K: int, nmid: float, kb_alf=None, k
     return s
 
 
+def newfft_tables(ktype, Nd, Jd, Kd, Ld, phasing="real", kb_alf=None, kb_m=None, alpha=None,
+                  beta=None):
+    """The 1D tables and st.sn ([(Nd)] flattened, first index fastest) of
+    newfft(..., 'ktype', ktype, 'phasing', phasing) in table mode, built in
+    the library; user parameters per dimension (st.kb_alf(id), st.kb_m(id),
+    st.alpha{id}, st.beta{id}: nufft/private/newfft_table_init.m:88-96).
+    Nmid = floor(N/2) for phasing 'real', (N-1)/2 for 'complex'."""
+    if phasing not in ("real", "complex"):
+        raise ValueError("phasing must be 'real' or 'complex'")
+    Nd = np.asarray(Nd)
+    nmid = np.floor(Nd / 2) if phasing == "real" else (Nd - 1) / 2
+
+    def user(d):
+        pick = lambda v: None if v is None else v[d]
+        return dict(kb_alf=pick(kb_alf), kb_m=pick(kb_m), alpha=pick(alpha), beta=pick(beta))
+    D = len(Nd)
+    tables = [newfft_table(ktype, Nd[d], Jd[d], Kd[d], Ld[d], phasing=phasing, **user(d))
+              for d in range(D)]
+    s = np.ones(1)
+    for d in range(D):
+        s = np.outer(s.ravel(order="F"), newfft_scale(ktype, Nd[d], Jd[d], Kd[d], float(nmid[d]),
+                                                      **user(d)))
+    return tables, s.ravel(order="F")
+
+
 class NewfftPlan(NufftPlan):
     """st = newfft(om, Nd, 'Jd', Jd, 'Kd', Kd, 'n_shift', n_shift, 'mode',
     'table0' | 'table1', 'oversample', Ld, 'phasing', phasing) on the device
@@ -511,19 +536,8 @@ class NewfftPlan(NufftPlan):
         self.phasing = phasing
         self.Nmid = (np.floor(Nd / 2) if phasing == "real" else (Nd - 1) / 2).astype(np.float64)
         if tables is None:
-            # per-dimension user parameters (st.kb_alf(id), st.kb_m(id), st.alpha{id},
-            # st.beta{id}: nufft/private/newfft_table_init.m:88-96)
-            def user(d):
-                pick = lambda v: None if v is None else v[d]
-                return dict(kb_alf=pick(kb_alf), kb_m=pick(kb_m), alpha=pick(alpha),
-                            beta=pick(beta))
-            tables = [newfft_table(ktype, Nd[d], Jd[d], Kd[d], Ld[d], phasing=phasing, **user(d))
-                      for d in range(D)]
-            s = np.ones(1)
-            for d in range(D):
-                s = np.outer(s.ravel(order="F"), newfft_scale(ktype, Nd[d], Jd[d], Kd[d],
-                                                              self.Nmid[d], **user(d)))
-            sn = s.ravel(order="F")
+            tables, sn = newfft_tables(ktype, Nd, Jd, Kd, Ld, phasing, kb_alf=kb_alf, kb_m=kb_m,
+                                       alpha=alpha, beta=beta)
         if sn is None:
             raise ValueError("sn is required with caller tables")
         self._tab = [np.ascontiguousarray(t) for t in tables]
@@ -645,6 +659,18 @@ def nufft_init(om, Nd, Jd, Kd, n_shift=None, *args, ncol=1, slice_moff=None, str
             raise ValueError("minmax:kb takes no parameters")
         return NufftPlan(om, Nd, Jd, Kd, n_shift=n_shift, Ld=Ld, ncol=ncol,
                          slice_moff=slice_moff, stream=stream)
+    tables, sn = nufft_init_tables(ktype, Nd, Jd, Kd, Ld, *params)
+    return NewfftPlan(om, Nd, Jd, Kd, n_shift=n_shift, mode="table0", Ld=Ld, phasing="complex",
+                      tables=tables, sn=sn, ncol=ncol, slice_moff=slice_moff, stream=stream)
+
+
+def nufft_init_tables(ktype, Nd, Jd, Kd, Ld, *params):
+    """The 1D tables and st.sn ([(Nd)] flattened, first index fastest) of
+    nufft_init(..., 'table', Ld, ktype, params...) for the interpolators
+    other than 'minmax:kb', built in the library (params per dimension)."""
+    Nd, Jd, Kd = _i32(Nd), _i32(Jd), _i32(Kd)
+    D = len(Nd)
+    Ld = _i32(Ld if np.ndim(Ld) else [Ld] * D)
     if ktype not in _NUFFT_KTYPES:
         raise ValueError(f"unknown kernel type {ktype!r}")
     if ktype == "kaiser" and params:
@@ -670,9 +696,7 @@ def nufft_init(om, Nd, Jd, Kd, n_shift=None, *args, ncol=1, slice_moff=None, str
     s = np.ones(1, dtype=np.complex128)
     for d in range(D):
         s = np.outer(s.ravel(order="F"), nufft_scale(ktype, Nd[d], Jd[d], Kd[d], *per_dim[d]))
-    return NewfftPlan(om, Nd, Jd, Kd, n_shift=n_shift, mode="table0", Ld=Ld, phasing="complex",
-                      tables=tables, sn=s.ravel(order="F"), ncol=ncol, slice_moff=slice_moff,
-                      stream=stream)
+    return tables, s.ravel(order="F")
 
 
 def _to_device_image(x, D, ncol):

@@ -94,3 +94,48 @@ def test_nufft_init_argument_errors():
         mb.nufft_init(om, (16, 16), (6, 6), (32, 32), (0, 0), "table", 512, "kb:beatty")
     with pytest.raises(mb.MirtError, match="unknown J,K/N"):
         mb.nufft_table("minmax:tuned", 16, 12, 32, 64)
+
+
+@pytest.mark.parametrize("ktype,params", [("kaiser", ()), ("kaiser", ([15.0, 15.0], [1, 1])),
+                                          ("minmax:tuned", ()), ("uniform", ()), ("linear", ())])
+def test_nufft_init_host_tables_match_oracle_st(ktype, params):
+    """The host part of mb.nufft_init for these interpolators (the tables and
+    st.sn handed to the device plan), on the set-up of the GPU test
+    test_nufft_init_other_interpolators, against the oracle's st."""
+    Nd, Jd, Kd = (32, 24), (6, 5), (64, 48)
+    om = np.random.default_rng(17).uniform(-np.pi, np.pi, (600, 2))
+    tables, sn = _nufft_mod().nufft_init_tables(ktype, Nd, Jd, Kd, 2 ** 10, *params)
+    so = nr.nufft_init_table_ktype(om, Nd, Jd, Kd, np.zeros(2), 2 ** 10, ktype, *params)
+    for d in range(2):
+        assert np.max(np.abs(tables[d] - so["h"][d])) <= 1e-11 * np.max(np.abs(so["h"][d]))
+    sno = so["sn"].ravel(order="F")
+    assert np.max(np.abs(sn - sno)) <= 1e-12 * np.max(np.abs(sno))
+
+
+def _nufft_mod():
+    import importlib
+    return importlib.import_module("mirt_b200.nufft")
+
+
+@pytest.mark.parametrize("ktype,kw", [("kb:minmax", {}), ("minmax:kb", {}), ("minmax:tuned", {}),
+                                      ("kb:user", dict(kb_alf=15.0, kb_m=1)),
+                                      ("minmax:user", dict(alpha=[1.0, -0.57, 0.14], beta=0.43))])
+@pytest.mark.parametrize("Nd", [(20,), (20, 10)])
+@pytest.mark.parametrize("phasing", ["real", "complex"])
+def test_newfft_host_tables_match_oracle_st(ktype, kw, Nd, phasing):
+    """The host part of mb.newfft (tables and st.sn with per-dimension user
+    parameters), on the set-ups of the GPU tests test_user_interpolators and
+    test_complex_phasing_builtin_tables, against the oracle's st."""
+    from oracle import newfft_ref as nf
+    dd = len(Nd)
+    per_dim = {k: [v] * dd for k, v in kw.items()}
+    Jd, Kd = (6,) * dd, tuple(2 * np.asarray(Nd))
+    Ld = (2 ** 11,) * dd
+    om = np.zeros((3, dd))
+    tables, sn = _nufft_mod().newfft_tables(ktype, Nd, Jd, Kd, Ld, phasing, **per_dim)
+    so = nf.newfft_init(om, Nd, Jd=Jd, Kd=Kd, mode="table0", Ld=Ld, phasing=phasing,
+                        ktype=ktype, **per_dim)
+    for d in range(dd):
+        assert np.max(np.abs(tables[d] - so["h"][d])) <= 1e-11 * np.max(np.abs(so["h"][d]))
+    sno = so["sn"].ravel(order="F")
+    assert np.max(np.abs(sn - sno)) <= 1e-11 * np.max(np.abs(sno))
