@@ -179,3 +179,36 @@ def test_plan_setters_reject_null_plans():
     assert lib.mirt_newfft_create(None, 2, None, None, None, None, None, None, 1, None, None, None,
                                   None, None, 0, None, 1, 1, None) == 1
     assert "output pointer is NULL" in lib.mirt_last_error().decode()
+
+
+def test_header_builds_and_links_from_c99(tmp_path):
+    """The boundary as a mex gateway sees it: a strict C99 program includes
+    include/mirt_b200.h, links libmirt_b200.so and makes calls that need no
+    GPU (the version, a gateway argument error with its text)."""
+    import os
+    import shutil
+    import subprocess
+    if shutil.which("gcc") is None:
+        pytest.skip("no C compiler")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    libdir = os.path.join(root, "mirt_b200")
+    src = tmp_path / "gateway_check.c"
+    src.write_text(
+        '#include <stdio.h>\n#include <string.h>\n#include "mirt_b200.h"\n'
+        "int main(void) {\n"
+        "  int32_t J[2] = {6, 6}, L[2] = {4, 4};\n"
+        "  if (mirt_version() < 1) return 2;\n"
+        "  int rc = mirt_interp2_table_mex(NULL, NULL, NULL, 0, NULL, NULL, 0, 0, NULL, NULL, 0, 0,\n"
+        "                                  J, 2, L, 2, NULL, 0, 0, NULL, 0, NULL, 0, NULL, NULL);\n"
+        "  printf(\"%d %s\\n\", rc, mirt_last_error());\n"
+        "  return rc == MIRT_ERR_ARG && strstr(mirt_last_error(), \"mxIsComplexDouble\") ? 0 : 3;\n"
+        "}\n")
+    exe = tmp_path / "gateway_check"
+    cc = subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-pedantic",
+                         "-I" + os.path.join(root, "include"), str(src), "-o", str(exe),
+                         "-L" + libdir, "-lmirt_b200", "-Wl,-rpath," + libdir],
+                        capture_output=True, text=True)
+    assert cc.returncode == 0, cc.stderr
+    run = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    assert run.returncode == 0, run.stdout + run.stderr
+    assert "interp2_table_mex failed: mxIsComplexDouble" in run.stdout
