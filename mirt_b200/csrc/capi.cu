@@ -1164,20 +1164,20 @@ int mirt_interp_plan_create(mirt_interp_plan **plan, int32_t D, const int32_t *K
                             void *stream) {
   if (!plan) return fail(MIRT_ERR_ARG, "plan pointer is NULL");
   *plan = nullptr;
-  int rc = device_ok();
-  if (rc) return rc;
-  const bool cplx = h_im != nullptr && h_im[0] != nullptr;
-  if (nslice < 1) return fail(MIRT_ERR_ARG, "nslice must be >= 1");
+  if (!K || !J || !L || !h_re || (Mtot > 0 && !tm)) return fail(MIRT_ERR_ARG, "NULL argument");
   if (D < 1 || D > 4) return fail(MIRT_ERR_ARG, "D must be 1, 2, 3 or 4");
+  const bool cplx = h_im != nullptr && h_im[0] != nullptr;
+  for (int d = 0; d < D; d++)
+    if (!h_re[d] || (cplx && !h_im[d])) return fail(MIRT_ERR_ARG, "NULL table");
+  if (nslice < 1) return fail(MIRT_ERR_ARG, "nslice must be >= 1");
   if (D == 4) {
     // the 4th dimension's taps are wrapped on the host by a general modulo
     if (K[3] < 1) return fail(MIRT_ERR_ARG, "K must be positive");
     if (J[3] < 1 || J[3] > MIRT_JMAX) return fail(MIRT_ERR_ARG, "J must be in 1..16");
     if (L[3] < 1) return fail(MIRT_ERR_ARG, "L must be positive");
     if ((long long)J[3] * L[3] + 1 > (1ll << 30)) return fail(MIRT_ERR_ARG, "table too long");
-    if (!h_re[3] || (cplx && !h_im[3])) return fail(MIRT_ERR_ARG, "NULL table");
   }
-  rc = validate_geometry(D == 4 ? 3 : D, K, J, L, order, cplx, Mtot, ncol);
+  int rc = validate_geometry(D == 4 ? 3 : D, K, J, L, order, cplx, Mtot, ncol);
   if (rc) return rc;
   std::vector<long long> moff(nslice + 1);
   if (slice_moff) {
@@ -1191,6 +1191,8 @@ int mirt_interp_plan_create(mirt_interp_plan **plan, int32_t D, const int32_t *K
     moff[0] = 0;
     moff[1] = Mtot;
   }
+  rc = device_ok();
+  if (rc) return rc;
   cudaStream_t st = as_stream(stream);
   if (D == 4)
     return plan4_create(plan, K, J, L, h_re, h_im, order, tm, Mtot, moff.data(), nslice, ncol,

@@ -212,3 +212,51 @@ def test_header_builds_and_links_from_c99(tmp_path):
     run = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
     assert run.returncode == 0, run.stdout + run.stderr
     assert "interp2_table_mex failed: mxIsComplexDouble" in run.stdout
+
+
+def _plan_create(D, K, J, L, tabs, order=0, M=3, moff=None, nslice=1, ncol=2, cplx=False):
+    import ctypes as C
+    lib = _lib.load()
+    K, J, L = (np.asarray(v, dtype=np.int32) for v in (K, J, L))
+    keep = [np.ascontiguousarray(t, dtype=np.float64) if t is not None else None for t in tabs]
+    dp = C.POINTER(C.c_double)
+    hr = (dp * max(D, 1))(*[t.ctypes.data_as(dp) if t is not None else dp() for t in keep])
+    hi = (dp * max(D, 1))(*[t.ctypes.data_as(dp) if t is not None else dp() for t in keep]) \
+        if cplx else None
+    tm = np.zeros(M * D)
+    mo = None if moff is None else np.asarray(moff, dtype=np.int64)
+    h = C.c_void_p()
+    i32p, i64p = C.POINTER(C.c_int32), C.POINTER(C.c_int64)
+    rc = lib.mirt_interp_plan_create(
+        C.byref(h), D, K.ctypes.data_as(i32p), J.ctypes.data_as(i32p), L.ctypes.data_as(i32p),
+        hr, hi, order, tm.ctypes.data_as(dp), M, None if mo is None else mo.ctypes.data_as(i64p),
+        nslice, ncol, None, None, None)
+    return rc, lib.mirt_last_error().decode()
+
+
+def test_plan_arguments_checked_before_the_device():
+    """mirt_interp_plan_create refuses bad arguments with their own message,
+    before it looks for a device (here: none)."""
+    t = np.zeros(6 * 4 + 1)
+    cases = [
+        (dict(D=5, K=[8] * 5, J=[6] * 5, L=[4] * 5, tabs=[t] * 5), "D must be 1, 2, 3 or 4"),
+        (dict(D=2, K=[8, 5], J=[6, 6], L=[4, 4], tabs=[t, t]), "J must not exceed K"),
+        (dict(D=4, K=[8, 8, 8, 3], J=[6, 6, 6, 17], L=[4] * 4, tabs=[t] * 3 + [np.zeros(69)]),
+         "J must be in 1..16"),
+        (dict(D=3, K=[8] * 3, J=[6] * 3, L=[4] * 3, tabs=[t, None, t]), "NULL table"),
+        (dict(D=2, K=[8, 8], J=[6, 6], L=[4, 4], tabs=[t, t], order=1, cplx=True),
+         "only 0th order implemented for complex"),
+        (dict(D=2, K=[8, 8], J=[6, 6], L=[4, 4], tabs=[t, t], moff=[0, 1, 2], nslice=2),
+         "slice offsets must start at 0 and end at Mtot"),
+        (dict(D=2, K=[8, 8], J=[6, 6], L=[4, 4], tabs=[t, t], nslice=2),
+         "slice offsets required"),
+    ]
+    for kw, msg in cases:
+        rc, err = _plan_create(**kw)
+        assert rc == _lib.MIRT_ERR_ARG and msg in err, (kw, rc, err)
+    import torch
+    if not torch.cuda.is_available():
+        # a 4D plan with K4 < J4 is valid: the 4th dimension wraps on the host
+        rc, err = _plan_create(D=4, K=[8, 8, 8, 3], J=[6, 6, 6, 4], L=[4] * 4,
+                               tabs=[t, t, t, np.zeros(17)])
+        assert "no CUDA device" in err
