@@ -147,6 +147,26 @@ double nufft_sinc(double x) {
 
 double diric(double k, int N, int K) { return nufft_sinc(k / ((double)K / (double)N)); }
 
+// T = inv(C'SS'C) of nufft/private/nufft_T.m (the sinc diric; tol 0, so the
+// plain inverse) for real scaling-factor coefficients alpha[0 .. La] and beta,
+// row-major [J][J]; false when singular
+bool minmax_T(int N, int J, int K, const std::vector<double> &alpha, double beta,
+              std::vector<double> &T) {
+  const int La = (int)alpha.size() - 1;
+  T.assign((size_t)J * J, 0.0);
+  for (int a = 0; a < J; a++)
+    for (int b = 0; b < J; b++) {
+      double s = 0;
+      for (int l1 = -La; l1 <= La; l1++)
+        for (int l2 = -La; l2 <= La; l2++) {
+          const double tmp = (double)(b - a) + beta * (double)(l1 - l2);
+          s += alpha[std::abs(l1)] * alpha[std::abs(l2)] * diric(tmp, N, K);
+        }
+      T[a * J + b] = s;
+    }
+  return invert(T, J);
+}
+
 }  // namespace
 
 // alphas (L+1 real coefficients) and beta of nufft_alpha_kb_fit(N, J, K, 'Nmid', Nmid)
@@ -200,19 +220,8 @@ bool minmax_kb_table(int N, int J, int K, int L, std::vector<cd> &h) {
   double beta;
   alpha_kb_fit(N, J, K, alpha, beta);
   const int La = (int)alpha.size() - 1;
-  // T = inv(C'SS'C)   (tol = 0 in nufft_init)
-  std::vector<double> T(J * J, 0.0);
-  for (int a = 0; a < J; a++)
-    for (int b = 0; b < J; b++) {
-      double s = 0;
-      for (int l1 = -La; l1 <= La; l1++)
-        for (int l2 = -La; l2 <= La; l2++) {
-          const double tmp = (double)(b - a) + beta * (double)(l1 - l2);
-          s += alpha[std::abs(l1)] * alpha[std::abs(l2)] * diric(tmp, N, K);
-        }
-      T[a * J + b] = s;
-    }
-  if (!invert(T, J)) return false;
+  std::vector<double> T;  // tol = 0 in nufft_init
+  if (!minmax_T(N, J, K, alpha, beta, T)) return false;
   const double gam = 2 * M_PI / K;
   std::vector<cd> p((size_t)L * J, cd(0, 0));  // used columns 0..J-1 of p [L, K]
   std::vector<double> r(J), arg(J);
@@ -254,18 +263,8 @@ bool minmax_kb_table(int N, int J, int K, int L, std::vector<cd> &h) {
 bool minmax_table_real_ab(int N, int J, int K, int L, const std::vector<double> &alpha, double beta,
                           std::vector<double> &h) {
   const int La = (int)alpha.size() - 1;
-  std::vector<double> T(J * J, 0.0);
-  for (int a = 0; a < J; a++)
-    for (int b = 0; b < J; b++) {
-      double s = 0;
-      for (int l1 = -La; l1 <= La; l1++)
-        for (int l2 = -La; l2 <= La; l2++) {
-          const double tmp = (double)(b - a) + beta * (double)(l1 - l2);
-          s += alpha[std::abs(l1)] * alpha[std::abs(l2)] * diric(tmp, N, K);
-        }
-      T[a * J + b] = s;
-    }
-  if (!invert(T, J)) return false;
+  std::vector<double> T;
+  if (!minmax_T(N, J, K, alpha, beta, T)) return false;
   const double gam = 2 * M_PI / K;
   std::vector<double> p((size_t)L * J, 0.0);  // used columns 0..J-1 of p [L, K]
   std::vector<double> r(J), arg(J);
@@ -455,6 +454,16 @@ double bessel_in(int m, double x) {
   return sum;
 }
 
+// the KB kernel of order m at offset t: f^m I_m(alpha f) / I_m(alpha) with
+// f = sqrt(1 - (t / (J/2))^2) on |t| < J/2, else 0 (nufft/kaiser_bessel.m:
+// 106-117); den = I_m(alpha)
+static double kb_kernel(double t, int J, double alpha, int m, double den) {
+  if (!(std::fabs(t) < J / 2.0)) return 0.0;
+  const double u = t / (J / 2.0);
+  const double f = std::sqrt(1 - u * u);
+  return std::pow(f, m) * bessel_in(m, alpha * f) / den;
+}
+
 // J_nu(z) / z^nu for nu = m + 1/2 (the 1D KB transform), given z^2 (z
 // imaginary when z^2 < 0, where the ratio is I_nu(|z|) / |z|^nu).  Power
 // series sum_k (-z^2/4)^k / (k! Gamma(k + nu + 1)) / 2^nu where its terms do
@@ -497,13 +506,7 @@ void kb_user_table(int J, int L, double alpha_full, int m, std::vector<double> &
   const double alpha = std::atof(buf);
   const double den = bessel_in(m, alpha);
   h.assign((size_t)J * L + 1, 0.0);
-  for (size_t i = 0; i < h.size(); i++) {
-    const double t = -J / 2.0 + (double)i / L;
-    if (std::fabs(t) < J / 2.0) {
-      const double f = std::sqrt(1 - (t / (J / 2.0)) * (t / (J / 2.0)));
-      h[i] = std::pow(f, m) * bessel_in(m, alpha * f) / den;
-    }
-  }
+  for (size_t i = 0; i < h.size(); i++) h[i] = kb_kernel(-J / 2.0 + (double)i / L, J, alpha, m, den);
 }
 
 // its scaling factors 1 / KB-FT((n - nmid) / K) with the 1D transform
@@ -565,12 +568,7 @@ void kb_table_complex(int N, int J, int K, int L, double alpha_full, int m, std:
   const double den = bessel_in(m, alpha);
   const double Kf = (double)J * K / N;
   table_fast_complex((double)J, J, Kf, L, [&](const double *arg, double *c) {
-    for (int j = 0; j < J; j++) {
-      const double u = arg[j] / (J / 2.0);
-      c[j] = std::fabs(arg[j]) < J / 2.0
-                 ? std::pow(std::sqrt(1 - u * u), m) * bessel_in(m, alpha * std::sqrt(1 - u * u)) / den
-                 : 0.0;
-    }
+    for (int j = 0; j < J; j++) c[j] = kb_kernel(arg[j], J, alpha, m, den);
   }, h);
   for (size_t i = 0; i < h.size(); i++) {
     const double t = -J / 2.0 + (double)i / L;
@@ -583,17 +581,8 @@ void kb_table_complex(int N, int J, int K, int L, double alpha_full, int m, std:
 bool minmax_table_complex_ab(int N, int J, int K, int L, const std::vector<double> &alpha,
                              double beta, std::vector<cd> &h) {
   const int La = (int)alpha.size() - 1;
-  std::vector<double> T(J * J, 0.0);
-  for (int a = 0; a < J; a++)
-    for (int b = 0; b < J; b++) {
-      double s = 0;
-      for (int l1 = -La; l1 <= La; l1++)
-        for (int l2 = -La; l2 <= La; l2++)
-          s += alpha[std::abs(l1)] * alpha[std::abs(l2)] *
-               diric((double)(b - a) + beta * (double)(l1 - l2), N, K);
-      T[a * J + b] = s;
-    }
-  if (!invert(T, J)) return false;
+  std::vector<double> T;
+  if (!minmax_T(N, J, K, alpha, beta, T)) return false;
   std::vector<double> r(J);
   table_fast_complex((double)N, J, (double)K, L, [&](const double *arg, double *c) {
     for (int j = 0; j < J; j++) {
@@ -652,12 +641,7 @@ bool nufft_table_ktype(int kt, int N, int J, int K, int L, double kb_alf, int kb
     const int m = kt == 0 ? 0 : kb_m;
     const double den = bessel_in(m, a);
     table_fast_complex((double)N, J, (double)K, L, [&](const double *arg, double *c) {
-      for (int j = 0; j < J; j++) {
-        const double u = arg[j] / (J / 2.0);
-        c[j] = std::fabs(arg[j]) < J / 2.0
-                   ? std::pow(std::sqrt(1 - u * u), m) * bessel_in(m, a * std::sqrt(1 - u * u)) / den
-                   : 0.0;
-      }
+      for (int j = 0; j < J; j++) c[j] = kb_kernel(arg[j], J, a, m, den);
     }, h);
   } else if (kt == 6) {
     linear_table_complex(N, J, K, L, h);
