@@ -66,6 +66,31 @@ def _radial(nspoke, nread):
     return np.stack([np.outer(np.cos(ang), r).ravel(), np.outer(np.sin(ang), r).ravel()], 1)
 
 
+@pytest.mark.parametrize("case", [0, 1, 2], ids=["1d", "2d", "3d"])
+def test_mex_delta_known_answer(case):
+    """nufft/interp_table_test.m's inputs (a unit grid value, triangle-based
+    complex tables, samples across +-2K) through the drop-ins: the known
+    answer read straight from the tables (FP32 tables: within 1e-6), and the
+    adjoint of single unit samples."""
+    from conftest import delta_known_answer, interp_table_test_cases
+    c = interp_table_test_cases()[case]
+    K, J, L, h, k0, tm = c["K"], c["J"], c["L"], c["h"], c["k0"], c["tm"]
+    D = len(K)
+    ck = np.zeros((int(np.prod(K)), 1), dtype=np.complex128)
+    kk = np.ravel_multi_index(k0, K, order="F")
+    ck[kk, 0] = c["val"]
+    ans = c["val"] * delta_known_answer(K, J, L, h, k0, tm)
+    fm = _fwd(D, ck, h, J, L, tm, K, None)[:, 0]
+    assert np.max(np.abs(fm - ans)) <= 1e-6
+    ms = [0, len(tm) // 3, len(tm) - 1]
+    e = np.zeros((len(tm), len(ms)), dtype=np.complex128)
+    e[ms, range(len(ms))] = 1
+    adj = _adj(D, e, h, J, L, tm, K, None)
+    for i, m in enumerate(ms):
+        want = np.conj(delta_known_answer(K, J, L, h, k0, tm[m:m + 1])[0])
+        assert abs(adj[kk, i] - want) <= 1e-6
+
+
 @pytest.mark.parametrize("N", [1, 3, 8, 32, 40])
 def test_minmax_tables_2d_columns(N):
     """C1 geometry (K=128^2, J=6, L=1024, radial 64x128) with N columns,

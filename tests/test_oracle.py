@@ -17,7 +17,7 @@ import pytest
 
 import oracle
 from oracle import nufft_ref as nr
-from conftest import load_golden, rel_l2
+from conftest import delta_known_answer, interp_table_test_cases, load_golden, rel_l2
 
 
 @pytest.mark.parametrize("i", range(24))
@@ -56,6 +56,25 @@ def test_port_matches_reference_kernels(D, variant):
         a = oracle.interp_adj(fm, h, J, L, tm, K, order, impl="ref", **impl_args)
         b = oracle.interp_adj(fm, h, J, L, tm, K, order, impl="port")
         assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("c", interp_table_test_cases(), ids=["1d", "2d", "3d"])
+def test_port_delta_known_answer(c):
+    """The oracle on interp_table_test.m's inputs equals the known answer of a
+    unit grid value read straight from the tables; and, exactly, the adjoint
+    of one unit sample is the conjugate of the same coefficients."""
+    K, J, L, h, k0 = c["K"], c["J"], c["L"], c["h"], c["k0"]
+    ck = np.zeros(int(np.prod(K)), dtype=np.complex128)
+    ck[np.ravel_multi_index(k0, K, order="F")] = c["val"]
+    ans = c["val"] * delta_known_answer(K, J, L, h, k0, c["tm"])
+    fm = oracle.interp_for(ck, h, J, L, c["tm"], K, 0, impl="port")[:, 0]
+    assert np.max(np.abs(fm - ans)) <= 1e-14
+    for m in (0, len(c["tm"]) // 3, len(c["tm"]) - 1):
+        e = np.zeros(len(c["tm"]), dtype=np.complex128)
+        e[m] = 1
+        adj = oracle.interp_adj(e, h, J, L, c["tm"], K, 0, impl="port")[:, 0]
+        assert abs(adj[np.ravel_multi_index(k0, K, order="F")]
+                   - np.conj(delta_known_answer(K, J, L, h, k0, c["tm"][m:m + 1])[0])) <= 1e-14
 
 
 def _radial(nspoke, nread):
