@@ -230,3 +230,26 @@ def test_nufft_init_other_interpolators(ktype, params):
     # the newfft plan's tolerance (1e-5 each way, its FP32 FFT included)
     assert rel_l2(mb.nufft(x, st), X_o) <= 1e-5
     assert rel_l2(mb.nufft_adj(X_o, st), nr.nufft_adj(X_o, so, ad)) <= 1e-5
+
+
+def test_nufft_init_kaiser_3d_table_test_setup():
+    """nufft/nufft_table_test.m's 3D 'kaiser' set-up (Jd = [3 4 3], odd and
+    even J, n_shift = [3 7 2], Ld = [2^8 2^7 2^7]) on the device against the
+    oracle, forward and adjoint."""
+    Jd, Nd = (3, 4, 3), (10, 8, 9)
+    Kd = tuple(2 * np.asarray(Nd))
+    ns = np.array([3.0, 7.0, 2.0])
+    gam = 2 * np.pi / np.asarray(Kd)
+    g = np.meshgrid(*[np.linspace(-2 * k, 2 * k, n) for k, n in zip(Kd, (21, 18, 23))],
+                    indexing="ij")
+    om = np.stack([gam[d] * g[d].ravel(order="F") for d in range(3)], 1)
+    Ld = (2 ** 8, 2 ** 7, 2 ** 7)
+    st = mb.nufft_init(om, Nd, Jd, Kd, ns, "table", Ld, "kaiser")
+    so = nr.nufft_init_table_ktype(om, Nd, Jd, Kd, ns, Ld, "kaiser")
+    fw, ad = _oracle_pair(so)
+    rng = np.random.default_rng(8)
+    x = rng.standard_normal(Nd) + 1j * rng.standard_normal(Nd)
+    X_o = nr.nufft(x, so, fw)
+    assert rel_l2(mb.nufft(x, st), X_o) <= 1e-5
+    X = np.arange(1, len(om) + 1) + 1j
+    assert rel_l2(mb.nufft_adj(X, st), nr.nufft_adj(X, so, ad)) <= 1e-5

@@ -139,3 +139,84 @@ def test_newfft_host_tables_match_oracle_st(ktype, kw, Nd, phasing):
         assert np.max(np.abs(tables[d] - so["h"][d])) <= 1e-11 * np.max(np.abs(so["h"][d]))
     sno = so["sn"].ravel(order="F")
     assert np.max(np.abs(sn - sno)) <= 1e-11 * np.max(np.abs(sno))
+
+
+def _table_test_3d():
+    """nufft/nufft_table_test.m's 3D set-up: 'kaiser', Jd = [3 4 3],
+    Nd = [10 8 9], Kd = 2 Nd, n_shift = [3 7 2], frequencies on a 21 x 18 x 23
+    grid over +-2K."""
+    Jd, Nd = (3, 4, 3), (10, 8, 9)
+    Kd = tuple(2 * np.asarray(Nd))
+    ns = np.array([3.0, 7.0, 2.0])
+    gam = 2 * np.pi / np.asarray(Kd)
+    g = np.meshgrid(*[np.linspace(-2 * k, 2 * k, n) for k, n in zip(Kd, (21, 18, 23))],
+                    indexing="ij")
+    om = np.stack([gam[d] * g[d].ravel(order="F") for d in range(3)], 1)
+    return om, Nd, Jd, Kd, ns
+
+
+def _fw(Xk, s):
+    return oracle.interp_for(Xk, s["h"], s["Jd"], s["Ld"], s["tm"], s["Kd"], 0)[:, 0]
+
+
+def _ad(X, s):
+    return oracle.interp_adj(X, s["h"], s["Jd"], s["Ld"], s["tm"], s["Kd"], 0)[:, 0]
+
+
+def test_nufft_table_test_3d_kaiser_vs_exact_dtft():
+    """The self-test's inputs (a unit image at (4, 2, 3); the adjoint of
+    X = (1:M) + i) with its Ld = [2^8 2^7 2^7]: the table NUFFT within 1 % /
+    0.5 % of the exact DTFT (measured 0.75 % / 0.34 %: J = 3 and 4)."""
+    om, Nd, Jd, Kd, ns = _table_test_3d()
+    st = nr.nufft_init_table_ktype(om, Nd, Jd, Kd, ns, (2 ** 8, 2 ** 7, 2 ** 7), "kaiser")
+    x = np.zeros(Nd)
+    x[3, 1, 2] = 1
+    Yd = nr.dtft(x, om, ns)
+    assert 100 * np.max(np.abs(nr.nufft(x, st, _fw) - Yd)) / np.max(np.abs(Yd)) < 1.0
+    X = np.arange(1, len(om) + 1) + 1j
+    cd = nr.dtft_adj(X, om, Nd, ns)
+    assert 100 * np.max(np.abs(nr.nufft_adj(X, st, _ad) - cd)) / np.max(np.abs(cd)) < 0.5
+
+
+def test_kaiser_table_converges_to_its_interpolator():
+    """The table NUFFT against the same 'kaiser' interpolator evaluated
+    exactly at every tap (the conjugate of nufft_init's coefficient
+    exp(i gam (N-1)/2 (t - k)) kb(t - k), nufft_init.m:262-290): the relative
+    L2 difference is the table's quantisation and falls as 1/L (measured
+    6.8e-3, 8.3e-4, 1.1e-4 for L = 2^7, 2^10, 2^13), which a wrong index,
+    phase sign or conjugation would not do."""
+    from scipy import special
+    om, Nd, Jd, Kd, ns = _table_test_3d()
+    gam = 2 * np.pi / np.asarray(Kd)
+    om = om + 0.37 * gam[None, :] * np.random.default_rng(5).random(om.shape)
+    rng = np.random.default_rng(1)
+    x = rng.standard_normal(Nd) + 1j * rng.standard_normal(Nd)
+
+    def kb(t, J, a):
+        out = np.zeros_like(t)
+        inside = np.abs(t) < J / 2
+        f = np.sqrt(1 - (t[inside] / (J / 2)) ** 2)
+        out[inside] = special.iv(0, a * f) / special.iv(0, a)
+        return out
+    errs = []
+    for L in (2 ** 7, 2 ** 10):
+        st = nr.nufft_init_table_ktype(om, Nd, Jd, Kd, ns, (L,) * 3, "kaiser")
+        Yt = nr.nufft(x, st, _fw)
+        Xk = np.fft.fftn(x * st["sn"], s=Kd, axes=(0, 1, 2))
+        coef, idx = [], []
+        for d in range(3):
+            t = om[:, d] / gam[d]
+            k = np.floor(t - Jd[d] / 2)[:, None] + np.arange(1, Jd[d] + 1)[None, :]
+            arg = t[:, None] - k
+            a = float(f"{2.34 * Jd[d]:g}")
+            coef.append(np.exp(-1j * gam[d] * (Nd[d] - 1) / 2 * arg) * kb(arg, Jd[d], a))
+            idx.append(np.mod(k, Kd[d]).astype(np.int64))
+        Y = np.zeros(len(om), dtype=np.complex128)
+        for j1 in range(Jd[0]):
+            for j2 in range(Jd[1]):
+                for j3 in range(Jd[2]):
+                    Y += (coef[0][:, j1] * coef[1][:, j2] * coef[2][:, j3]
+                          * Xk[idx[0][:, j1], idx[1][:, j2], idx[2][:, j3]])
+        Y *= np.exp(1j * (om @ ns))
+        errs.append(np.linalg.norm(Yt - Y) / np.linalg.norm(Y))
+    assert errs[1] < 1.5e-3 and errs[0] / errs[1] > 6
