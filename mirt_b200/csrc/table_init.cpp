@@ -140,6 +140,15 @@ bool invert(std::vector<double> &A, int J) {
   return true;
 }
 
+// v as printf's %g prints it (six significant digits): the KB shape that
+// MATLAB's sprintf('%g') writes into the inline kernel strings of
+// nufft/kaiser_bessel.m:80-82 and nufft/kaiser_bessel_ft.m
+double printed_g(double v) {
+  char buf[64];
+  std::snprintf(buf, sizeof buf, "%g", v);
+  return std::atof(buf);
+}
+
 double nufft_sinc(double x) {
   if (x == 0) return 1.0;
   return std::sin(M_PI * x) / (M_PI * x);
@@ -176,9 +185,7 @@ void alpha_kb_fit_nmid(int N, int J, int K, double Nmid, std::vector<double> &al
   const int L = N > 40 ? 13 : (int)std::ceil(N / 3.0);
   double kb_a = kb_alpha_best(J, (double)K / (double)N);
   // kaiser_bessel_ft('inline', ...) prints alpha with %g into its kernel string
-  char buf[64];
-  std::snprintf(buf, sizeof buf, "%g", kb_a);
-  kb_a = std::atof(buf);
+  kb_a = printed_g(kb_a);
   std::vector<double> sn_kaiser(N), X((size_t)N * (L + 1));
   const double gam = 2 * M_PI / K;
   for (int i = 0; i < N; i++) {
@@ -405,9 +412,7 @@ std::vector<double> linear_scale(int N, int J, int K, double Nmid) {
 // alpha printed with %g (nufft/kaiser_bessel.m:80-82).  'kb:minmax' (the
 // default of 'table0' / 'table1'): alpha = 2.34 J; 'kb:beatty': kb_beatty_alpha.
 void kb_table_alpha(int J, int L, double alpha_full, std::vector<double> &h) {
-  char buf[64];
-  std::snprintf(buf, sizeof buf, "%g", alpha_full);
-  const double alpha = std::atof(buf);
+  const double alpha = printed_g(alpha_full);
   const double i0a = bessel_i0(alpha);
   h.assign((size_t)J * L + 1, 0.0);
   for (size_t i = 0; i < h.size(); i++) {
@@ -501,9 +506,7 @@ double jnu_over_znu(int m, double z2) {
 // with %g into the inline kernel (:80-82), sampled at t = -J/2 + i/L as the
 // 'ratio' construction reads it
 void kb_user_table(int J, int L, double alpha_full, int m, std::vector<double> &h) {
-  char buf[64];
-  std::snprintf(buf, sizeof buf, "%g", alpha_full);
-  const double alpha = std::atof(buf);
+  const double alpha = printed_g(alpha_full);
   const double den = bessel_in(m, alpha);
   h.assign((size_t)J * L + 1, 0.0);
   for (size_t i = 0; i < h.size(); i++) h[i] = kb_kernel(-J / 2.0 + (double)i / L, J, alpha, m, den);
@@ -562,9 +565,7 @@ void table_fast_complex(double N, int J, double K, int L, Coef coef, std::vector
 // (nufft/private/newfft_table_init.m:173-184): the fake problem N' = J,
 // K' = J K / N, then the phase exp(i pi t (1/K - 1/K')) at t = -J/2 + i/L
 void kb_table_complex(int N, int J, int K, int L, double alpha_full, int m, std::vector<cd> &h) {
-  char buf[64];
-  std::snprintf(buf, sizeof buf, "%g", alpha_full);
-  const double alpha = std::atof(buf);
+  const double alpha = printed_g(alpha_full);
   const double den = bessel_in(m, alpha);
   const double Kf = (double)J * K / N;
   table_fast_complex((double)J, J, Kf, L, [&](const double *arg, double *c) {
@@ -635,9 +636,7 @@ void linear_table_complex(int N, int J, int K, int L, std::vector<cd> &h) {
 bool nufft_table_ktype(int kt, int N, int J, int K, int L, double kb_alf, int kb_m,
                        const std::vector<double> &alpha, double beta, std::vector<cd> &h) {
   if (kt == 0 || kt == 7) {
-    char buf[64];
-    std::snprintf(buf, sizeof buf, "%g", kt == 0 ? 2.34 * J : kb_alf);
-    const double a = std::atof(buf);
+    const double a = printed_g(kt == 0 ? 2.34 * J : kb_alf);
     const int m = kt == 0 ? 0 : kb_m;
     const double den = bessel_in(m, a);
     table_fast_complex((double)N, J, (double)K, L, [&](const double *arg, double *c) {
