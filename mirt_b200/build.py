@@ -22,7 +22,8 @@ LIB = os.path.join(PKG, "libmirt_b200.so")
 ROOT = os.path.dirname(PKG)
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NVFLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3",
+NVFLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler",
+           "-fPIC,-O3,-Wall,-Wextra,-Wshadow,-Wpointer-arith",
            "--expt-relaxed-constexpr", "-I" + os.path.join(ROOT, "include")]
 
 

@@ -1768,7 +1768,7 @@ int mex_run(MexCall &c) {
   CK(out_split.alloc(std::max<long long>(nout * N, 1) * 2 * sizeof(double)));
   double *ir = in_split.as<double>(), *ii = ir + nin * N;
   double *orr = out_split.as<double>(), *oi = orr + nout * N;
-  if (nin * N) {
+  if (nin > 0 && N > 0) {
     CK(cudaMemcpyAsync(ir, c.in_re, nin * N * sizeof(double), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(ii, c.in_im, nin * N * sizeof(double), cudaMemcpyHostToDevice, st));
   }
@@ -1783,7 +1783,7 @@ int mex_run(MexCall &c) {
   else
     CK(launch_gather(P.ag, P.lg, in_il.as<float2>(), out_il.as<float2>(), st));
   CK(launch_il_to_split(out_il.as<float2>(), nout, N, orr, oi, st));
-  if (nout * N) {
+  if (nout > 0 && N > 0) {
     CK(cudaMemcpyAsync(c.out_re, orr, nout * N * sizeof(double), cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(c.out_im, oi, nout * N * sizeof(double), cudaMemcpyDeviceToHost, st));
   }

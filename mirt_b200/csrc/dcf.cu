@@ -216,7 +216,6 @@ int mirt_dcf_pipe(mirt_nufft *p, double *w, int32_t init_ones, int32_t niter, do
   cudaStream_t st = as_stream(stream);
   const long long M = p->Mtot;
   const int S = p->nslice;
-  const int D = p->gg.D;
   DcfBuffers b;
   rc = b.alloc(p, st);
   if (rc) return rc;

@@ -274,13 +274,6 @@ __global__ void permute_samples_kernel(const double *__restrict__ tm_in,
   if (ph_in) ph_out[pos] = ph_in[m];
 }
 
-static unsigned grid_for(long long n, int thr, int maxb = 148 * 32) {
-  long long b = (n + thr - 1) / thr;
-  if (b > maxb) b = maxb;
-  if (b < 1) b = 1;
-  return (unsigned)b;
-}
-
 namespace {
 dim3 image_grid(const GlueGeom &g, int C, int nslice) {
   return dim3((unsigned)(g.npix / g.N[0] * nslice), (unsigned)((g.N[0] + 31) / 32),
