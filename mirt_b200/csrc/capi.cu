@@ -1718,6 +1718,18 @@ int mex_check_tables(MexCall &c, const int32_t *flips, int64_t flips_numel) {
 }
 
 int mex_run(MexCall &c) {
+  // No samples or no columns: the reference's adjoint returns the zeroed
+  // grid and its forward an empty fm (interp2_table1_adj.c:57-58 clears ck
+  // before the sample loop), with no device work here either.
+  if (c.M == 0 || c.N == 0) {
+    if (c.adj && c.N > 0) {
+      long long nk = 1;
+      for (int d = 0; d < c.D; d++) nk *= c.K[d];
+      std::fill(c.out_re, c.out_re + nk * c.N, 0.0);
+      std::fill(c.out_im, c.out_im + nk * c.N, 0.0);
+    }
+    return MIRT_OK;
+  }
   int rc = device_ok();
   if (rc) return rc;
   std::lock_guard<std::mutex> lk(g_mex_mu);

@@ -260,3 +260,27 @@ def test_plan_arguments_checked_before_the_device():
         rc, err = _plan_create(D=4, K=[8, 8, 8, 3], J=[6, 6, 6, 4], L=[4] * 4,
                                tabs=[t, t, t, np.zeros(17)])
         assert "no CUDA device" in err
+
+
+@pytest.mark.parametrize("D", [1, 2, 3, 4])
+def test_gateways_with_no_samples(D):
+    """M = 0 samples: the adjoint returns the zero grid and the forward an empty
+    fm, as the reference kernels do (interp2_table1_adj.c:57-58 clears ck
+    before its sample loop); no device is needed for that."""
+    h = np.zeros(6 * 4 + 1)
+    J, L = np.full(D, 6, np.int32), np.full(D, 4, np.int32)
+    K = np.full(D, 8, np.int32)
+    tm = np.zeros((0, D))
+    fm = np.zeros((0, 3), complex)
+    hs = [h] * D
+    adj = {1: mb.interp1_table_adj_mex, 2: mb.interp2_table_adj_mex, 3: mb.interp3_table_adj_mex,
+           4: mb.interp4_table_adj_mex}[D]
+    ck = adj(fm, *hs, J if D > 1 else J[:1], L if D > 1 else L[:1], tm, K if D > 1 else K[:1])
+    assert ck.shape == (8 ** D, 3) and not ck.any()
+    fwd = {1: mb.interp1_table_mex, 2: mb.interp2_table_mex, 3: mb.interp3_table_mex,
+           4: mb.interp4_table_mex}[D]
+    grid = np.ones((8,) * D + ((2,) if D > 1 else ()), complex)
+    if D == 1:
+        grid = np.ones((8, 2), complex)
+    out = fwd(grid, *hs, J, L, tm)
+    assert out.shape == (0, 2)
