@@ -20,6 +20,8 @@
 
 #include <cmath>
 #include <complex>
+#include <memory>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -97,12 +99,10 @@ std::complex<double> coef4(double t, int k, const double *hr, const double *hi, 
   return {(1 - alf) * hr[n] + alf * h1, 0.0};
 }
 
-}  // namespace
-
-int plan4_create(mirt_interp_plan **out, const int *K, const int *J, const int *L,
-                 const double *const *h_re, const double *const *h_im, int order,
-                 const double *tm, long long M4, const long long *moff, int nslice, int C,
-                 const double *ph_re, const double *ph_im, cudaStream_t st) {
+int plan4_build(mirt_interp_plan **out, const int *K, const int *J, const int *L,
+                const double *const *h_re, const double *const *h_im, int order,
+                const double *tm, long long M4, const long long *moff, int nslice, int C,
+                const double *ph_re, const double *ph_im, cudaStream_t st) {
   const int K4 = K[3], J4 = J[3], L4 = L[3];
   const long long Me = M4 * J4;
   if (Me >= (1ll << 31)) return api_fail(MIRT_ERR_ARG, "4D plan: samples times J4 must be < 2^31");
@@ -149,8 +149,9 @@ int plan4_create(mirt_interp_plan **out, const int *K, const int *J, const int *
   int rc = mirt_interp_plan_create(&sub, 3, K, J, L, hr3, cplx ? hi3 : nullptr, order, tm3.data(),
                                    Me, moff3.data(), (int32_t)nsub, C, p3r.data(), p3i.data(), st);
   if (rc) return rc;
+  std::unique_ptr<mirt_interp_plan> owned(sub);
   auto *P = new mirt_interp_plan();
-  P->sub4 = sub;
+  P->sub4 = owned.release();
   P->a.g.D = 4;
   P->a.C = C;
   P->a.Mtot = M4;
@@ -171,6 +172,23 @@ int plan4_create(mirt_interp_plan **out, const int *K, const int *J, const int *
   }
   *out = P;
   return MIRT_OK;
+}
+
+}  // namespace
+
+// The host expansion holds 8 * (3 + 2 + 2) bytes per (sample, tap) pair: a
+// failed host allocation returns MIRT_ERR_ALLOC instead of leaving the C ABI
+// as an exception.
+int plan4_create(mirt_interp_plan **out, const int *K, const int *J, const int *L,
+                 const double *const *h_re, const double *const *h_im, int order,
+                 const double *tm, long long M4, const long long *moff, int nslice, int C,
+                 const double *ph_re, const double *ph_im, cudaStream_t st) {
+  try {
+    return plan4_build(out, K, J, L, h_re, h_im, order, tm, M4, moff, nslice, C, ph_re, ph_im,
+                       st);
+  } catch (const std::bad_alloc &) {
+    return api_fail(MIRT_ERR_ALLOC, "4D plan: out of host memory for the expanded samples");
+  }
 }
 
 int plan4_forward(mirt_interp_plan *P, const float2 *ck, float2 *fm, cudaStream_t st) {
