@@ -19,6 +19,7 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <new>
 #include <set>
 #include <string>
 #include <vector>
@@ -1161,7 +1162,7 @@ int mirt_interp_plan_create(mirt_interp_plan **plan, int32_t D, const int32_t *K
                             const double *const *h_im, int32_t order, const double *tm,
                             int64_t Mtot, const int64_t *slice_moff, int32_t nslice,
                             int32_t ncol, const double *phase_re, const double *phase_im,
-                            void *stream) {
+                            void *stream) try {
   if (!plan) return fail(MIRT_ERR_ARG, "plan pointer is NULL");
   *plan = nullptr;
   if (!K || !J || !L || !h_re || (Mtot > 0 && !tm)) return fail(MIRT_ERR_ARG, "NULL argument");
@@ -1227,6 +1228,8 @@ int mirt_interp_plan_create(mirt_interp_plan **plan, int32_t D, const int32_t *K
   }
   *plan = P;
   return MIRT_OK;
+} catch (const std::bad_alloc &) {
+  return fail(MIRT_ERR_ALLOC, "out of host memory");
 }
 
 int mirt_interp_plan_forward(mirt_interp_plan *P, const void *ck, void *fm, void *stream) {
@@ -1249,7 +1252,7 @@ int mirt_interp_plan_adjoint(mirt_interp_plan *P, const void *fm, void *ck, void
   return MIRT_OK;
 }
 
-int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
+int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) try {
   if (!P) return fail(MIRT_ERR_ARG, "plan is NULL");
   P = launch_plan(P);
   cudaStream_t st = as_stream(stream);
@@ -1473,6 +1476,8 @@ int mirt_interp_plan_autotune(mirt_interp_plan *P, void *stream) {
   P->lg = bestg;
   CK(cudaStreamSynchronize(st));
   return MIRT_OK;
+} catch (const std::bad_alloc &) {
+  return fail(MIRT_ERR_ALLOC, "out of host memory");
 }
 
 int mirt_interp_plan_config(mirt_interp_plan *P, int32_t *out, int32_t n) {
@@ -1522,7 +1527,7 @@ int mirt_interp_plan_fault(mirt_interp_plan *P, int32_t *fault) {
   return MIRT_OK;
 }
 
-int mirt_interp_plan_set_sweep(mirt_interp_plan *P, int32_t segments, int32_t rows) {
+int mirt_interp_plan_set_sweep(mirt_interp_plan *P, int32_t segments, int32_t rows) try {
   if (!P) return fail(MIRT_ERR_ARG, "plan is NULL");
   P = launch_plan(P);
   if (P->a.g.D == 3) {
@@ -1563,6 +1568,8 @@ int mirt_interp_plan_set_sweep(mirt_interp_plan *P, int32_t segments, int32_t ro
     P->ls.atomic = 0;
   }
   return MIRT_OK;
+} catch (const std::bad_alloc &) {
+  return fail(MIRT_ERR_ALLOC, "out of host memory");
 }
 
 int mirt_interp_plan_set_dense(mirt_interp_plan *P, int32_t on) {
@@ -1583,7 +1590,7 @@ int mirt_interp_plan_set_staged(mirt_interp_plan *P, int32_t mode) {
   return MIRT_OK;
 }
 
-int mirt_interp_plan_set_ownership(mirt_interp_plan *P, int32_t own, void *stream) {
+int mirt_interp_plan_set_ownership(mirt_interp_plan *P, int32_t own, void *stream) try {
   if (!P) return fail(MIRT_ERR_ARG, "plan is NULL");
   P = launch_plan(P);
   if (own && !own_ok(P->a, P->t))
@@ -1599,6 +1606,8 @@ int mirt_interp_plan_set_ownership(mirt_interp_plan *P, int32_t own, void *strea
   if (rc) return rc;
   CK(cudaStreamSynchronize(as_stream(stream)));
   return MIRT_OK;
+} catch (const std::bad_alloc &) {
+  return fail(MIRT_ERR_ALLOC, "out of host memory");
 }
 
 int mirt_interp_plan_set_deterministic(mirt_interp_plan *P, int32_t deterministic) {
@@ -1616,7 +1625,7 @@ int mirt_interp_plan_set_deterministic(mirt_interp_plan *P, int32_t deterministi
 }
 
 int mirt_interp_plan_set_spread(mirt_interp_plan *P, const int32_t *T, int32_t threads,
-                                int32_t padc, void *stream) {
+                                int32_t padc, void *stream) try {
   if (!P || !T) return fail(MIRT_ERR_ARG, "NULL argument");
   P = launch_plan(P);
   const int D = P->a.g.D;
@@ -1644,6 +1653,8 @@ int mirt_interp_plan_set_spread(mirt_interp_plan *P, const int32_t *T, int32_t t
   if (rc) return rc;
   CK(cudaStreamSynchronize(st));
   return MIRT_OK;
+} catch (const std::bad_alloc &) {
+  return fail(MIRT_ERR_ALLOC, "out of host memory");
 }
 
 int mirt_interp_plan_destroy(mirt_interp_plan *P) {
@@ -2425,7 +2436,7 @@ extern "C" {
 int mirt_nufft_create(mirt_nufft **out, int32_t D, const int32_t *Nd, const int32_t *Kd,
                       const int32_t *Jd, const int32_t *Ld, const double *n_shift,
                       const double *om, int64_t Mtot, const int64_t *slice_moff, int32_t nslice,
-                      int32_t ncol, void *stream) {
+                      int32_t ncol, void *stream) try {
   if (!out) return fail(MIRT_ERR_ARG, "output pointer is NULL");
   *out = nullptr;
   std::vector<long long> moff;
@@ -2468,6 +2479,8 @@ int mirt_nufft_create(mirt_nufft **out, int32_t D, const int32_t *Nd, const int3
   }
   *out = p;
   return MIRT_OK;
+} catch (const std::bad_alloc &) {
+  return fail(MIRT_ERR_ALLOC, "out of host memory");
 }
 
 int mirt_newfft_create(mirt_nufft **out, int32_t D, const int32_t *Nd, const int32_t *Kd,
@@ -2475,7 +2488,7 @@ int mirt_newfft_create(mirt_nufft **out, int32_t D, const int32_t *Nd, const int
                        const double *const *h_im, int32_t order, const double *sn_re,
                        const double *sn_im, const double *nmid, const double *n_shift,
                        const double *om, int64_t Mtot, const int64_t *slice_moff, int32_t nslice,
-                       int32_t ncol, void *stream) {
+                       int32_t ncol, void *stream) try {
   if (!out) return fail(MIRT_ERR_ARG, "output pointer is NULL");
   *out = nullptr;
   if (!h_re || !sn_re) return fail(MIRT_ERR_ARG, "tables and scaling factors are required");
@@ -2503,6 +2516,8 @@ int mirt_newfft_create(mirt_nufft **out, int32_t D, const int32_t *Nd, const int
   }
   *out = p;
   return MIRT_OK;
+} catch (const std::bad_alloc &) {
+  return fail(MIRT_ERR_ALLOC, "out of host memory");
 }
 
 int mirt_newfft_kb_table(int32_t J, int32_t L, double *h) {
@@ -2523,7 +2538,7 @@ int mirt_newfft_kb_scale(int32_t N, int32_t J, int32_t K, double nmid, double *s
   return MIRT_OK;
 }
 
-int mirt_newfft_ktype_table(int32_t ktype, int32_t N, int32_t J, int32_t K, int32_t L, double *h) {
+int mirt_newfft_ktype_table(int32_t ktype, int32_t N, int32_t J, int32_t K, int32_t L, double *h) try {
   if (N < 1 || J < 1 || J > MIRT_JMAX || K < 1 || L < 1)
     return fail(MIRT_ERR_ARG, "N, K, L must be positive, J in 1..16");
   if (!h) return fail(MIRT_ERR_ARG, "output pointer is NULL");
@@ -2558,10 +2573,12 @@ int mirt_newfft_ktype_table(int32_t ktype, int32_t N, int32_t J, int32_t K, int3
   }
   std::copy(t.begin(), t.end(), h);
   return MIRT_OK;
+} catch (const std::bad_alloc &) {
+  return fail(MIRT_ERR_ALLOC, "out of host memory");
 }
 
 int mirt_newfft_ktype_scale(int32_t ktype, int32_t N, int32_t J, int32_t K, double nmid,
-                            double *sn) {
+                            double *sn) try {
   if (N < 1 || J < 1 || J > MIRT_JMAX || K < 1)
     return fail(MIRT_ERR_ARG, "N, K must be positive, J in 1..16");
   if (!sn) return fail(MIRT_ERR_ARG, "output pointer is NULL");
@@ -2590,11 +2607,13 @@ int mirt_newfft_ktype_scale(int32_t ktype, int32_t N, int32_t J, int32_t K, doub
   }
   std::copy(s.begin(), s.end(), sn);
   return MIRT_OK;
+} catch (const std::bad_alloc &) {
+  return fail(MIRT_ERR_ALLOC, "out of host memory");
 }
 
 int mirt_newfft_table_complex(int32_t ktype, int32_t N, int32_t J, int32_t K, int32_t L,
                               double kb_alf, int32_t kb_m, const double *alpha, int32_t nalpha,
-                              double beta, double *h_re, double *h_im) {
+                              double beta, double *h_re, double *h_im) try {
   if (N < 1 || J < 1 || J > MIRT_JMAX || K < 1 || L < 1)
     return fail(MIRT_ERR_ARG, "N, K, L must be positive, J in 1..16");
   if (!h_re || !h_im) return fail(MIRT_ERR_ARG, "output pointer is NULL");
@@ -2643,6 +2662,8 @@ int mirt_newfft_table_complex(int32_t ktype, int32_t N, int32_t J, int32_t K, in
     h_im[i] = t[i].imag();
   }
   return MIRT_OK;
+} catch (const std::bad_alloc &) {
+  return fail(MIRT_ERR_ALLOC, "out of host memory");
 }
 
 namespace {
@@ -2677,7 +2698,7 @@ int nufft_ktype_args(int32_t ktype, int32_t N, int32_t J, int32_t K, double kb_a
 
 int mirt_nufft_ktype_table(int32_t ktype, int32_t N, int32_t J, int32_t K, int32_t L,
                            double kb_alf, int32_t kb_m, const double *alpha, int32_t nalpha,
-                           double beta, double *h_re, double *h_im) {
+                           double beta, double *h_re, double *h_im) try {
   if (!h_re || !h_im) return fail(MIRT_ERR_ARG, "output pointer is NULL");
   if (L < 1) return fail(MIRT_ERR_ARG, "L must be positive");
   std::vector<double> al;
@@ -2692,11 +2713,13 @@ int mirt_nufft_ktype_table(int32_t ktype, int32_t N, int32_t J, int32_t K, int32
     h_im[i] = t[i].imag();
   }
   return MIRT_OK;
+} catch (const std::bad_alloc &) {
+  return fail(MIRT_ERR_ALLOC, "out of host memory");
 }
 
 int mirt_nufft_ktype_scale(int32_t ktype, int32_t N, int32_t J, int32_t K, double kb_alf,
                            int32_t kb_m, const double *alpha, int32_t nalpha, double beta,
-                           double *sn_re, double *sn_im) {
+                           double *sn_re, double *sn_im) try {
   if (!sn_re || !sn_im) return fail(MIRT_ERR_ARG, "output pointer is NULL");
   std::vector<double> al;
   int rc = nufft_ktype_args(ktype, N, J, K, kb_alf, kb_m, alpha, nalpha, al);
@@ -2709,9 +2732,11 @@ int mirt_nufft_ktype_scale(int32_t ktype, int32_t N, int32_t J, int32_t K, doubl
     sn_im[n] = s[n].imag();
   }
   return MIRT_OK;
+} catch (const std::bad_alloc &) {
+  return fail(MIRT_ERR_ALLOC, "out of host memory");
 }
 
-int mirt_newfft_kb_user_table(int32_t J, int32_t L, double alpha, int32_t m, double *h) {
+int mirt_newfft_kb_user_table(int32_t J, int32_t L, double alpha, int32_t m, double *h) try {
   if (J < 1 || J > MIRT_JMAX || L < 1) return fail(MIRT_ERR_ARG, "L must be positive, J in 1..16");
   if (!h) return fail(MIRT_ERR_ARG, "output pointer is NULL");
   if (!(alpha >= 0) || m < 0 || m > 32)
@@ -2720,10 +2745,12 @@ int mirt_newfft_kb_user_table(int32_t J, int32_t L, double alpha, int32_t m, dou
   kb_user_table(J, L, alpha, m, t);
   std::copy(t.begin(), t.end(), h);
   return MIRT_OK;
+} catch (const std::bad_alloc &) {
+  return fail(MIRT_ERR_ALLOC, "out of host memory");
 }
 
 int mirt_newfft_kb_user_scale(int32_t N, int32_t J, int32_t K, double nmid, double alpha,
-                              int32_t m, double *sn) {
+                              int32_t m, double *sn) try {
   if (N < 1 || J < 1 || J > MIRT_JMAX || K < 1)
     return fail(MIRT_ERR_ARG, "N, K must be positive, J in 1..16");
   if (!sn) return fail(MIRT_ERR_ARG, "output pointer is NULL");
@@ -2732,10 +2759,12 @@ int mirt_newfft_kb_user_scale(int32_t N, int32_t J, int32_t K, double nmid, doub
   const std::vector<double> s = kb_user_scale(N, J, K, nmid, alpha, m);
   std::copy(s.begin(), s.end(), sn);
   return MIRT_OK;
+} catch (const std::bad_alloc &) {
+  return fail(MIRT_ERR_ALLOC, "out of host memory");
 }
 
 int mirt_newfft_minmax_user_table(int32_t N, int32_t J, int32_t K, int32_t L,
-                                  const double *alpha, int32_t nalpha, double beta, double *h) {
+                                  const double *alpha, int32_t nalpha, double beta, double *h) try {
   if (N < 1 || J < 1 || J > MIRT_JMAX || K < 1 || L < 1)
     return fail(MIRT_ERR_ARG, "N, K, L must be positive, J in 1..16");
   if (!h || !alpha || nalpha < 1) return fail(MIRT_ERR_ARG, "NULL argument or empty alpha");
@@ -2745,16 +2774,20 @@ int mirt_newfft_minmax_user_table(int32_t N, int32_t J, int32_t K, int32_t L,
     return fail(MIRT_ERR_ARG, "singular min-max matrix for this N, J, K");
   std::copy(t.begin(), t.end(), h);
   return MIRT_OK;
+} catch (const std::bad_alloc &) {
+  return fail(MIRT_ERR_ALLOC, "out of host memory");
 }
 
 int mirt_newfft_minmax_user_scale(int32_t N, int32_t K, double nmid, const double *alpha,
-                                  int32_t nalpha, double beta, double *sn) {
+                                  int32_t nalpha, double beta, double *sn) try {
   if (N < 1 || K < 1) return fail(MIRT_ERR_ARG, "N, K must be positive");
   if (!sn || !alpha || nalpha < 1) return fail(MIRT_ERR_ARG, "NULL argument or empty alpha");
   const std::vector<double> s =
       minmax_scale_real_ab(N, K, std::vector<double>(alpha, alpha + nalpha), beta, nmid);
   std::copy(s.begin(), s.end(), sn);
   return MIRT_OK;
+} catch (const std::bad_alloc &) {
+  return fail(MIRT_ERR_ALLOC, "out of host memory");
 }
 
 int mirt_nufft_forward(mirt_nufft *p, const void *x, void *X, void *stream) {

@@ -13,6 +13,7 @@
 // reproducible bit for bit by an FP64 restatement.
 #include "../../include/mirt_b200.h"
 
+#include <new>
 #include <string>
 
 #include "runtime.cuh"
@@ -111,7 +112,7 @@ __global__ void feat_hist_kernel(const double *__restrict__ om, const double2 *_
 }  // namespace
 
 extern "C" int mirt_dcf_features(const double *om, int64_t M, const int64_t *slice_moff,
-                                 int32_t nslice, const int32_t *K, float *feat, void *stream) {
+                                 int32_t nslice, const int32_t *K, float *feat, void *stream) try {
   if (!om || !K || !feat) return api_fail(MIRT_ERR_ARG, "NULL argument");
   if (M < 0 || nslice < 1) return api_fail(MIRT_ERR_ARG, "need M >= 0 and nslice >= 1");
   if (M >= (1ll << 31)) return api_fail(MIRT_ERR_ARG, "M too large");
@@ -165,4 +166,6 @@ extern "C" int mirt_dcf_features(const double *om, int64_t M, const int64_t *sli
   FCK(cudaGetLastError());
   FCK(cudaStreamSynchronize(st));
   return MIRT_OK;
+} catch (const std::bad_alloc &) {
+  return mirt::api_fail(MIRT_ERR_ALLOC, "out of host memory");
 }

@@ -22,6 +22,7 @@
 
 #include <cmath>
 #include <string>
+#include <new>
 #include <vector>
 
 #include "runtime.cuh"
@@ -633,7 +634,7 @@ int mirt_mlp_params(mirt_mlp *q, float *params) {
 }
 
 int mirt_mlp_grad(mirt_mlp *q, const float *x, const float *y, int64_t n, float *grad,
-                  float *loss, void *stream) {
+                  float *loss, void *stream) try {
   if (!q || !x || !y || !grad) return api_fail(MIRT_ERR_ARG, "NULL argument");
   if (n < 1 || n > (1 << 30)) return api_fail(MIRT_ERR_ARG, "need 1 <= n <= 2^30");
   cudaStream_t st = as_stream(stream);
@@ -664,10 +665,12 @@ int mirt_mlp_grad(mirt_mlp *q, const float *x, const float *y, int64_t n, float 
   MCK(cudaStreamSynchronize(st));
   if (loss) *loss = l;
   return MIRT_OK;
+} catch (const std::bad_alloc &) {
+  return api_fail(MIRT_ERR_ALLOC, "out of host memory");
 }
 
 int mirt_mlp_train(mirt_mlp *q, const float *x, const float *y, int64_t n, int32_t batch,
-                   int32_t steps, float lr, uint64_t seed, float *loss_hist, void *stream) {
+                   int32_t steps, float lr, uint64_t seed, float *loss_hist, void *stream) try {
   if (!q || !x || !y) return api_fail(MIRT_ERR_ARG, "NULL argument");
   if (n < 1 || batch < 1 || batch > (1 << 24) || steps < 0 || !(lr > 0.f))
     return api_fail(MIRT_ERR_ARG, "need n >= 1, 1 <= batch <= 2^24, steps >= 0, lr > 0");
@@ -722,6 +725,8 @@ int mirt_mlp_train(mirt_mlp *q, const float *x, const float *y, int64_t n, int32
                         cudaMemcpyDeviceToHost, st));
   MCK(cudaStreamSynchronize(st));
   return MIRT_OK;
+} catch (const std::bad_alloc &) {
+  return api_fail(MIRT_ERR_ALLOC, "out of host memory");
 }
 
 int mirt_mlp_infer(mirt_mlp *q, const float *x, int64_t n, float mu, float sigma, float *yhat,
