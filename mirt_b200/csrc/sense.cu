@@ -16,6 +16,7 @@
 #include "../../include/mirt_b200.h"
 
 #include <cmath>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -330,7 +331,7 @@ int mirt_sense_reg(mirt_sense *op, const void *x, void *rx, void *stream) {
 }
 
 int mirt_sense_pcg(mirt_sense *op, void *x_, const void *y_, const float *W, int32_t niter,
-                   int32_t flags, const void *xref_, double *nrmse, float *ms, void *stream) {
+                   int32_t flags, const void *xref_, double *nrmse, float *ms, void *stream) try {
   if (!op || !x_ || !y_) return api_fail(MIRT_ERR_ARG, "NULL argument");
   if (niter < 0) return api_fail(MIRT_ERR_ARG, "niter must be >= 0");
   const bool precon = flags & MIRT_PCG_CIRCULANT, gram = flags & MIRT_PCG_TOEPLITZ;
@@ -471,6 +472,8 @@ int mirt_sense_pcg(mirt_sense *op, void *x_, const void *y_, const float *W, int
     }
   }
   return MIRT_OK;
+} catch (const std::bad_alloc &) {
+  return api_fail(MIRT_ERR_ALLOC, "out of host memory");
 }
 
 int mirt_sense_cg(mirt_sense *op, void *x, const void *y, const float *W, int32_t niter,

@@ -19,6 +19,7 @@
 #include "../../include/mirt_b200.h"
 
 #include <cmath>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -257,7 +258,7 @@ namespace mirt {
 
 int toep_create(mirt_toeplitz **out, const double *om, long long M, const long long *moff,
                 int nslice, const int *Nd, const int *Kd, const int *Jd, const int *Ld,
-                const double *w, int ncol, cudaStream_t st) {
+                const double *w, int ncol, cudaStream_t st) try {
   if (!out || !om || !Nd || !Kd || !Jd || !Ld) return api_fail(MIRT_ERR_ARG, "NULL argument");
   *out = nullptr;
   if (ncol < 1 || nslice < 1) return api_fail(MIRT_ERR_ARG, "need ncol >= 1 and nslice >= 1");
@@ -315,6 +316,8 @@ int toep_create(mirt_toeplitz **out, const double *om, long long M, const long l
   if (cudaStreamSynchronize(st) != cudaSuccess) return fin(api_fail(MIRT_ERR_CUDA, "Toeplitz set-up"));
   *out = T;
   return fin(MIRT_OK);
+} catch (const std::bad_alloc &) {
+  return api_fail(MIRT_ERR_ALLOC, "out of host memory");
 }
 
 int toep_gram_sense(mirt_toeplitz *T, const float2 *x, const float2 *sens, float2 *out,
